@@ -1,0 +1,406 @@
+#!/usr/bin/env python
+"""Benchmark: ns/day of full leapfrog steps on the 41,472-atom water box.
+
+A step is one LeapfrogIntegrator iteration (kick + drift, then the periodic
+cutoff LJ(C2) + Coulomb(C1) force with its cell-list rebuild) at dt = 1 fs on
+13,824 TIP3P-geometry waters (24^3 lattice, box 74.496 A, rc 10, C2 from 9).
+
+Default arm (libpmb200 on B200):
+  value  -- device-resident steps (positions/velocities/forces in HBM, one
+            CUDA-graph replay per step), L2 flushed (256 MiB write) before
+            every timed step, each step timed with CUDA events on the stream
+            it runs on; sum over K steps, max over ranks.
+  e2e    -- the same steps through the reference-facing host-buffer C-ABI
+            call (pmb200_eval: positions and forces copied host->device, forces
+            and energies device->host, every step) with the kick/drift done
+            on the host as ProtoMol's integrator does; wall clock per step.
+  fp64   -- the same device-resident steps with the plain FP64 pair kernel.
+  roofline -- the pair kernel (dominant): 81 algorithmic flops per unique
+            in-cutoff pair over its CUDA-event duration, against the FP32 FMA
+            peak measured in-run (the kernel runs on the FP32 pipe; tensor
+            cores and HBM are not its bound); traffic from the committed ncu
+            summary.
+  cpu_baseline -- the reference's own CPU force (oracle/_ref, compiled from
+            the reference sources) driving the same leapfrog on one host core.
+
+--impl reference: the reference CPU implementation alone, one independent
+replica per host core (the reference force is serial), bounded sample.
+
+Multi-GPU (torchrun): independent replicas, one per GPU (the path has no
+exchange step for a single box at this size); value sums ranks' ns/day.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+DT_FS = 1.0
+FLOPS_PER_PAIR = 81          # algorithmic flops per unique in-cutoff pair
+BYTES_PER_ATOM = 84          # algorithmic HBM bytes per atom per evaluation
+KERNELS_PER_STEP = 6         # kick_drift, cell_index, scan, scatter, rank_gather, pair
+WORKLOAD = ("water box: 41,472 atoms (13,824 TIP3P-geometry waters, 24^3 lattice, "
+            "box 74.496 A), LJ C2 switch 9-10 A + Coulomb C1 cutoff 10 A, leapfrog 1 fs")
+METRIC = "ns/day & Gpairs/s, 41k-atom water box: mixed vs FP64 on B200 @<=1e-5 force err"
+
+
+def ns_per_day(sec_per_step):
+    return 0.0864 * DT_FS / sec_per_step
+
+
+def env_int(k, d):
+    try:
+        return int(os.environ.get(k, d))
+    except ValueError:
+        return d
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms in the background."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.p = None
+        self.out = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader",
+                                       "-lms", "200", "-i", str(self.idx)],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.out, _ = self.p.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+                self.out, _ = self.p.communicate()
+
+    def summary(self):
+        if not self.out:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1].split()[0]))
+                mx = float(f[2].split()[0])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+def committed_traffic():
+    """Pair-kernel DRAM bytes per launch from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "pair_mixed_water41k.md")
+    try:
+        txt = open(path).read()
+    except OSError:
+        return None
+    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", txt)
+    return float(m.group(1)) if m else None
+
+
+def cpu_reference_time(sysd, steps):
+    """Seconds per leapfrog step of the reference CPU force on this host, one
+    core; (seconds, kind, detail)."""
+    from oracle import oracle as O
+    if O.ref_available():
+        R = O.RefForce(sysd)
+        t0 = time.perf_counter()
+        R.leapfrog(sysd["pos"], sysd["vel"], DT_FS, steps)
+        dt = time.perf_counter() - t0
+        R.close()
+        kind = "reference"
+    else:
+        t0 = time.perf_counter()
+        O.restate_leapfrog(sysd, sysd["pos"], sysd["vel"], DT_FS, steps)
+        dt = time.perf_counter() - t0
+        kind = "port"
+    return dt / (steps + 1), kind  # steps + 1 force evaluations
+
+
+def _ref_replica(args):
+    steps, seed = args
+    sys.path.insert(0, ROOT)
+    from protomoladdon_b200 import water
+    s = water.medium_41k(seed=seed)
+    t, kind = cpu_reference_time(s, steps)
+    return t, kind
+
+
+def run_reference(args):
+    rank = env_int("RANK", 0)
+    if rank != 0:
+        return 0
+    import multiprocessing as mp
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    steps = max(1, min(args.steps, 3))
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(cores) as pool:
+        res = pool.map(_ref_replica, [(steps, 1234 + r) for r in range(cores)])
+    wall = time.perf_counter() - t0
+    per_step = statistics.mean(t for t, _ in res)
+    kind = res[0][1]
+    value = cores * ns_per_day(per_step)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "ns/day",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": per_step * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "atoms": 41472, "replicas": cores,
+                   "parallelism": f"{cores} independent single-core replicas"},
+        "cpu_baseline": {"value": value, "unit": "ns/day", "cores": cores, "kind": kind,
+                         "sample": f"{steps} leapfrog steps (+1 initial force) per replica, "
+                                   f"{cores} replicas in parallel, wall {wall:.1f} s"},
+        "e2e": {"value": value, "unit": "ns/day", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+    from protomoladdon_b200 import _lib, water
+    from protomoladdon_b200.force import (NonbondedCutoffB200SystemForce, PeriodicTopology,
+                                          ScalarStructure)
+    world = env_int("WORLD_SIZE", 1)
+    rank = env_int("RANK", 0)
+    local = env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    s = water.medium_41k(seed=1234 + rank)
+    n = s["n"]
+    topo = PeriodicTopology.from_dict(s)
+    stream = torch.cuda.Stream(device=dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > L2
+
+    def make(prec):
+        return NonbondedCutoffB200SystemForce(s["ron"], s["rc_lj"], s["rc_coul"], s["rc_alg"],
+                                              precision=prec, device=local)
+
+    def device_run(force):
+        """W warm-up + K timed device-resident steps; returns per-step ms list,
+        pair-kernel ms list, pair count."""
+        pos = torch.tensor(s["pos"], dtype=torch.float64, device=dev)
+        vel = torch.tensor(s["vel"], dtype=torch.float64, device=dev)
+        frc = torch.zeros_like(pos)
+        out = torch.zeros(20, dtype=torch.float64, device=dev)
+        with torch.cuda.stream(stream):
+            force.evaluate_device(topo, pos.data_ptr(), frc.data_ptr(), out.data_ptr(),
+                                  _lib.PMB200_ENERGY, stream.cuda_stream)
+        stream.synchronize()
+        force.sync()
+        pairs = force.last_pair_count()
+        force.set_kernel_timing(True)
+        sp = stream.cuda_stream
+        for _ in range(args.warmup):
+            force.step_device(topo, pos.data_ptr(), vel.data_ptr(), frc.data_ptr(), DT_FS, sp)
+        stream.synchronize()
+        e0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        e1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        kms = []
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        for k in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                e0[k].record(stream)
+            force.step_device(topo, pos.data_ptr(), vel.data_ptr(), frc.data_ptr(), DT_FS, sp)
+            e1[k].record(stream)
+            e1[k].synchronize()
+            kms.append(force.last_kernel_ms())
+        torch.cuda.synchronize(dev)
+        if dist is not None:
+            dist.barrier()
+        force.sync()
+        force.set_kernel_timing(False)
+        step_ms = [a.elapsed_time(b) for a, b in zip(e0, e1)]
+        return step_ms, kms, pairs
+
+    # accuracy of the mixed force vs the FP64 CPU oracle at the start positions
+    acc = {}
+    if rank == 0 and not args.skip_accuracy:
+        from oracle import oracle as O
+        fo, eo, vo, _ = O.restate_eval(s, s["pos"], virial_mode=0)
+        fm = make("mixed")
+        F = np.zeros_like(s["pos"])
+        E = ScalarStructure()
+        fm.evaluate(topo, s["pos"], F, E)
+        fm.close()
+        acc = {"force_rms_rel_err": float(np.sqrt(((F - fo) ** 2).sum() / (fo ** 2).sum())),
+               "energy_rel_err_coulomb": float(abs(E[0] - eo[0]) / abs(eo[0])),
+               "energy_rel_err_lj": float(abs(E[1] - eo[1]) / abs(eo[1]))}
+
+    fmix = make(args.precision)
+    with ClockSampler(local) as clk:
+        step_ms, kms, pairs = device_run(fmix)
+    clocks = clk.summary()
+    fp64 = None
+    if args.precision == "mixed" and not args.skip_fp64:
+        f64 = make("fp64")
+        s64, k64, _ = device_run(f64)
+        f64.close()
+        fp64 = (sum(s64), statistics.mean(k64))
+
+    # end to end through the host-buffer C-ABI call, host kick/drift
+    h = DT_FS * 0.02045482828087295
+    xh = s["pos"].copy()
+    vh = s["vel"].copy()
+    m = s["mass"][:, None]
+    F = np.zeros_like(xh)
+    E = ScalarStructure()
+    fmix.evaluate(topo, xh, F, E)
+    e2e_steps = min(args.steps, 100)
+    e2e_t = []
+    for _ in range(min(args.warmup, 3)):
+        vh += F * h / m
+        xh += vh * h
+        F[:] = 0.0
+        fmix.evaluate(topo, xh, F, E)
+    if dist is not None:
+        dist.barrier()
+    for _ in range(e2e_steps):
+        flush.zero_()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        vh += F * h / m
+        xh += vh * h
+        F[:] = 0.0
+        E.clear()
+        fmix.evaluate(topo, xh, F, E)
+        e2e_t.append(time.perf_counter() - t0)
+    fmix.close()
+
+    tot_ms = sum(step_ms)
+    mean_k = statistics.mean(kms)
+    e2e_s = sum(e2e_t) / len(e2e_t)
+    if dist is not None:
+        t = torch.tensor([tot_ms, e2e_s, mean_k], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tot_ms, e2e_s, mean_k = (float(x) for x in t.tolist())
+    ms_step = tot_ms / args.steps
+    value = world * ns_per_day(ms_step * 1e-3)
+
+    if rank == 0:
+        peak = ctypes_peak(local)
+        achieved = FLOPS_PER_PAIR * pairs / (mean_k * 1e-3) / 1e12
+        traffic = committed_traffic()
+        line = {
+            "metric": METRIC, "value": value, "unit": "ns/day", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if args.precision == "mixed" else "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "atoms": n, "pairs_per_eval": pairs,
+                       "precision": args.precision,
+                       "l2": "flushed before every timed step (256 MiB write)",
+                       "parallelism": f"{world} independent replica(s), one per GPU"},
+            "gpairs_per_s": world * pairs / (ms_step * 1e-3) / 1e9,
+            "pair_kernel_ms": mean_k,
+            "gpairs_per_s_pair_kernel": pairs / (mean_k * 1e-3) / 1e9,
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak,
+                         "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
+                         "traffic": traffic,
+                         "peak_source": "FP32 FMA throughput measured in this run "
+                                        "(pmb200_measure_fp32_peak)",
+                         "hbm": {"achieved_gbs": BYTES_PER_ATOM * n / (mean_k * 1e-3) / 1e9,
+                                 "peak_gbs": measured_hbm()}},
+            "e2e": {"value": world * ns_per_day(e2e_s), "unit": "ns/day",
+                    "ms_per_step": e2e_s * 1e3,
+                    "h2d_bytes_per_step": 2 * 24 * n, "d2h_bytes_per_step": 24 * n + 160},
+            "gpu_launches": KERNELS_PER_STEP * args.steps,
+            "clocks": clocks,
+        }
+        line.update(acc)
+        if fp64 is not None:
+            t64 = fp64[0] / args.steps
+            line["fp64"] = {"ns_per_day": world * ns_per_day(t64 * 1e-3), "ms_per_step": t64,
+                            "pair_kernel_ms": fp64[1],
+                            "mixed_speedup": t64 / ms_step}
+        if world == 1 and not args.skip_cpu:
+            cpu_steps = args.cpu_steps
+            t_cpu, kind = cpu_reference_time(s, cpu_steps)
+            line["cpu_baseline"] = {
+                "value": ns_per_day(t_cpu), "unit": "ns/day", "cores": 1, "kind": kind,
+                "sample": f"{cpu_steps} leapfrog steps (+1 initial force) of the same box, "
+                          f"{t_cpu * 1e3:.0f} ms per step, serial reference force"}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def ctypes_peak(device):
+    import ctypes
+    from protomoladdon_b200 import _lib
+    v = ctypes.c_double()
+    rc = _lib.lib().pmb200_measure_fp32_peak(int(device), ctypes.byref(v))
+    return v.value if rc == 0 else None
+
+
+def measured_hbm():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]
+    except Exception:
+        return 6650.0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--cpu-steps", type=int, default=20)
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-fp64", action="store_true")
+    ap.add_argument("--skip-accuracy", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

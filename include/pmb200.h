@@ -1,0 +1,176 @@
+/* pmb200 -- B200 (sm_100a) periodic cutoff nonbonded system force.
+ *
+ * C ABI of libpmb200.so: plain pointers, sizes and int status codes; no C++
+ * or CUDA types cross it.  It replaces ProtoMol's
+ *
+ *   NonbondedCutoffSystemForce<CubicCellManager,
+ *     OneAtomPairTwo<PeriodicBoundaryConditions, C2SwitchingFunction,
+ *                    LennardJonesForce, C1SwitchingFunction, CoulombForce>>
+ *
+ * registered at protomol/src/protomol/module/NonbondedCutoffForceModule.cpp:
+ * 75-76 and selected in a config by
+ *   force LennardJones Coulomb -algorithm NonbondedCutoff
+ *         -switchingFunction C2 -switchingFunction C1
+ *         -switchon <ron> -cutoff <rc_lj> -cutoff <rc_coul> -cutoff <rc_alg>
+ * (parameter order: OneAtomPairTwo::getParameters,
+ * protomol/src/protomol/force/OneAtomPairTwo.h:127-132, then
+ * NonbondedCutoffForce::getParameters, .../nonbonded/NonbondedCutoffForce.h:
+ * 85-91).  Every function returns 0 on success or a PMB200_E* code; the text
+ * of the last error is available from pmb200_last_error().  Nothing throws
+ * across this boundary.
+ *
+ * Units are ProtoMol's: Angstrom, kcal/mol, amu, charges pre-scaled by
+ * SQRTCOULOMBCONSTANT (Atom::scaledCharge).  Arrays are caller-owned host
+ * memory unless a name says "device".
+ */
+#ifndef PMB200_H
+#define PMB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define PMB200_OK 0
+#define PMB200_EINVAL 1      /* bad argument (message says which) */
+#define PMB200_ECUDA 2       /* CUDA runtime error */
+#define PMB200_ESTATE 3      /* call order: topology/box not set */
+#define PMB200_EUNSUPPORTED 4/* valid in ProtoMol but outside this force */
+#define PMB200_EDEVICE 5     /* device-side check failed (non-finite input) */
+#define PMB200_ENOMEM 6
+
+/* ---- precision of the pair arithmetic ---- */
+#define PMB200_MIXED 0 /* FP32 pair math, int64 fixed-point forces, FP64 totals */
+#define PMB200_FP64 1  /* plain FP64 pair math */
+
+/* ---- what an evaluation produces (bit flags) ---- */
+#define PMB200_ENERGY 1u     /* LENNARDJONES and COULOMB energies */
+#define PMB200_VIRIAL 2u     /* atomic virial (9) */
+#define PMB200_MOLVIRIAL 4u  /* molecular virial (9); needs masses */
+
+typedef struct pmb200_ctx pmb200_ctx;
+
+/* Construction parameters.  Replaces the force-id parse
+ * ForceFactory::make -> NonbondedCutoffForce::doMake -> OneAtomPairTwo::make
+ * -> C2SwitchingFunction::make / C1SwitchingFunction::make
+ * (protomol/src/protomol/factory/ForceFactory.cpp:21-242,
+ *  .../force/nonbonded/NonbondedCutoffForce.h:71-75,
+ *  .../force/OneAtomPairTwo.h:142-155,
+ *  .../switch/C2SwitchingFunction.cpp:30-41, C1SwitchingFunction.cpp:25-27).
+ * C2 validation is the reference's: 0 <= switchon < cutoff_lj. */
+typedef struct {
+  int precision;      /* PMB200_MIXED or PMB200_FP64 */
+  int device;         /* CUDA device ordinal */
+  double switchon;    /* C2 -switchon (Lennard-Jones) */
+  double cutoff_lj;   /* C2 -cutoff */
+  double cutoff_coul; /* C1 -cutoff */
+  double cutoff_alg;  /* algorithm -cutoff; must be >= both switch cutoffs */
+  double cellsize;    /* grid cell edge hint; 0 = max(cutoff_lj, cutoff_coul)/2 */
+} pmb200_params;
+
+/* Replaces constructing the force prototype + ForceGroup ownership
+ * (protomol/src/protomol/force/ForceGroup.cpp:31-52). */
+int pmb200_create(const pmb200_params *params, pmb200_ctx **out);
+int pmb200_destroy(pmb200_ctx *ctx);
+const char *pmb200_last_error(const pmb200_ctx *ctx);
+
+/* Topology the force reads (replaces the per-evaluation reads of
+ * GenericTopology in OneAtomPairTwo::doOneAtomPair,
+ * protomol/src/protomol/force/OneAtomPairTwo.h:57-125):
+ *   type[n]      Atom::type (index into the LJ table)
+ *   q_scaled[n]  Atom::scaledCharge
+ *   molecule[n]  Atom::molecule
+ *   mass[n]      Atom::scaledMass (may be NULL; needed for PMB200_MOLVIRIAL
+ *                and the integrator)
+ *   lj[ntypes*ntypes*4]  LennardJonesParameterTable {A, B, A14, B14}
+ *                (protomol/src/protomol/topology/LennardJonesParameterTable.h:34-36)
+ *   excl[nexcl*3]  ExclusionTable entries {a1, a2, kind}, kind 1 =
+ *                EXCLUSION_MODIFIED, 2 = EXCLUSION_FULL; later duplicates
+ *                override earlier ones like ExclusionTable::add
+ *                (protomol/src/protomol/topology/ExclusionTable.cpp:103-120)
+ *   coulomb_scaling  GenericTopology::coulombScalingFactor
+ * Copies everything to the device. */
+int pmb200_set_topology(pmb200_ctx *ctx, int n, const int *type,
+                        const double *q_scaled, const int *molecule,
+                        const double *mass, int ntypes, const double *lj,
+                        int nexcl, const int *excl, double coulomb_scaling);
+
+/* Periodic cell (replaces PeriodicBoundaryConditions::set,
+ * protomol/src/protomol/topology/PeriodicBoundaryConditions.cpp:32-77).
+ * Only orthogonal boxes; every edge must be >= 2 * max switch cutoff. */
+int pmb200_set_box(pmb200_ctx *ctx, const double e1[3], const double e2[3],
+                   const double e3[3], const double origin[3]);
+
+/* One SystemForce::evaluate
+ * (protomol/src/protomol/force/nonbonded/NonbondedCutoffSystemForce.h:42-53)
+ * on host buffers.  pos[3n] AoS positions (not wrapped).  forces[3n] AoS:
+ * ACCUMULATED into, like the reference.  energies[2] = {COULOMB,
+ * LENNARDJONES}: accumulated into (may be NULL when !(flags&ENERGY)).
+ * virial[9], molvirial[9] row-major xx..zz: accumulated into when the flag is
+ * set (else may be NULL). */
+int pmb200_eval(pmb200_ctx *ctx, const double *pos, double *forces,
+                double *energies, double *virial, double *molvirial,
+                unsigned flags);
+
+/* Same evaluation on device buffers, asynchronous on `stream` (a
+ * cudaStream_t, NULL = the context's stream).  d_pos[3n], d_forces[3n]
+ * (accumulated into), d_out[20] receives {COULOMB, LENNARDJONES, virial[9],
+ * molvirial[9]} (overwritten, FP64) when flags ask for them; may be NULL
+ * when flags == 0.  Errors detected on the device are reported by the next
+ * pmb200_sync(). */
+int pmb200_eval_device(pmb200_ctx *ctx, const double *d_pos, double *d_forces,
+                       double *d_out, unsigned flags, void *stream);
+
+/* Waits for the context's work and reports device-side check failures. */
+int pmb200_sync(pmb200_ctx *ctx);
+
+/* Leapfrog steps on device memory with this force alone, following
+ * LeapfrogIntegrator::run / doKickdoDrift without modifiers
+ * (protomol/src/protomol/integrator/leapfrog/LeapfrogIntegrator.cpp:58-105):
+ * forces at the start, then per step a kick (a half kick on the first step)
+ * and a drift, new forces; a closing half kick.  dt_fs in fs.  d_pos[3n],
+ * d_vel[3n] updated in place; d_forces[3n] holds the final forces.  Steps
+ * after the first run as one captured CUDA graph.  d_out as for
+ * pmb200_eval_device, for the final step's forces. */
+int pmb200_leapfrog_device(pmb200_ctx *ctx, double *d_pos, double *d_vel,
+                           double *d_forces, double *d_out, double dt_fs,
+                           int nsteps, unsigned flags, void *stream);
+
+/* One steady-state leapfrog iteration on device memory: doKickdoDrift()
+ * then calculateForces() (LeapfrogIntegrator::run's loop body,
+ * protomol/src/protomol/integrator/leapfrog/LeapfrogIntegrator.cpp:98-101):
+ * v += F h / m, x += v h, then d_forces is OVERWRITTEN with the forces at the
+ * new positions (StandardIntegrator::calculateForces zeroes forces first,
+ * .../integrator/StandardIntegrator.cpp:48).  Replays a CUDA graph captured on
+ * the first call for the same buffers and stream (the stream must not be the
+ * legacy default stream). */
+int pmb200_step_device(pmb200_ctx *ctx, double *d_pos, double *d_vel,
+                       double *d_forces, double *d_out, double dt_fs,
+                       unsigned flags, void *stream);
+
+/* When on, CUDA events bracket every pair-kernel launch (graph replays
+ * included); pmb200_last_kernel_ms returns the duration of the last one
+ * (valid after the work has completed). */
+int pmb200_set_kernel_timing(pmb200_ctx *ctx, int on);
+int pmb200_last_kernel_ms(pmb200_ctx *ctx, float *ms);
+
+/* Unique in-cutoff pairs found by the last evaluation (the pair count the
+ * Gpairs/s unit counts; fully excluded pairs are not counted).  Requires a
+ * pmb200_sync() after the evaluation. */
+int pmb200_last_pair_count(pmb200_ctx *ctx, long long *pairs);
+
+/* Measurement helper (no counterpart in the reference): FP32 FMA throughput
+ * of `device` in TFLOP/s (2 flops per FMA), from a 148-SM-filling chain of
+ * independent fused multiply-adds timed with CUDA events.  The pair kernels
+ * are bounded by this pipe, not by HBM or tensor cores. */
+int pmb200_measure_fp32_peak(int device, double *tflops);
+
+/* Geometry of the device cell grid chosen for the current box. */
+int pmb200_grid(const pmb200_ctx *ctx, int dims[3], double edge[3]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PMB200_H */

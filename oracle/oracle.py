@@ -1,0 +1,238 @@
+"""ctypes front end for the CPU checkers.  TEST INFRASTRUCTURE ONLY.
+
+Only tests/, ``__graft_entry__.smoke()`` and the CPU-baseline leg of bench.py
+import this module.  It wraps
+
+* ``oracle/_build/libpmoracle.so`` -- pm_oracle.c, the C restatement of
+  ProtoMol's NonbondedCutoffSystemForce<CubicCellManager, OneAtomPairTwo<
+  PeriodicBoundaryConditions, C2, LennardJones, C1, Coulomb>>; and
+* ``oracle/_ref/libpmref.so`` -- the reference's own sources compiled by
+  oracle/Makefile, driven through ref_driver.cpp (present only where the
+  reference tree was available at build time; the file travels with the repo
+  copy).
+
+Parity status: the restatement is pinned bit for bit against the compiled
+reference on seeded water boxes and against the reference's periodic water
+golden (tests/golden/water423.npz, t = 0 energies of
+test/tests/expected/water_CHARMM_PERIODIC_L.energy).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+RESTATE_SO = os.path.join(HERE, "_build", "libpmoracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libpmref.so")
+
+_P = ctypes.c_void_p
+_D = ctypes.c_double
+_I = ctypes.c_int
+
+
+class _PmoSystem(ctypes.Structure):
+    _fields_ = [
+        ("n", _I), ("ntypes", _I),
+        ("type", _P), ("qscaled", _P), ("mol", _P), ("mass", _P), ("lj", _P),
+        ("nexcl", _I), ("excl", _P),
+        ("coulomb_scaling", _D),
+        ("box", _D * 3), ("origin", _D * 3),
+        ("cellsize", _D), ("ron", _D), ("rc_lj", _D), ("rc_coul", _D),
+        ("rc_alg", _D),
+    ]
+
+
+def _ptr(a):
+    return a.ctypes.data_as(_P) if a is not None else None
+
+
+_restate = None
+_ref = None
+
+
+def restate_lib():
+    global _restate
+    if _restate is None:
+        if not os.path.exists(RESTATE_SO):
+            raise RuntimeError(f"oracle restatement not built: {RESTATE_SO} (run make -C oracle restate)")
+        lib = ctypes.CDLL(RESTATE_SO)
+        lib.pmo_eval.argtypes = [ctypes.POINTER(_PmoSystem), _P, _P, _P, _P, _P, _I, _I]
+        lib.pmo_eval.restype = _I
+        lib.pmo_count_pairs.argtypes = [ctypes.POINTER(_PmoSystem), _P]
+        lib.pmo_count_pairs.restype = ctypes.c_longlong
+        lib.pmo_leapfrog.argtypes = [ctypes.POINTER(_PmoSystem), _P, _P, _P, _D, _I, _P]
+        lib.pmo_leapfrog.restype = _I
+        _restate = lib
+    return _restate
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref_lib():
+    global _ref
+    if _ref is None:
+        if not os.path.exists(REF_SO):
+            raise RuntimeError(f"reference oracle not built: {REF_SO} (run make -C oracle ref)")
+        lib = ctypes.CDLL(REF_SO)
+        lib.pmref_create.restype = _P
+        lib.pmref_create.argtypes = [_I, _P, _P, _P, _P, _I, _P, _I, _P, _D, _P, _P,
+                                     _D, _D, _D, _D, _D]
+        lib.pmref_destroy.argtypes = [_P]
+        lib.pmref_eval.argtypes = [_P, _P, _P, _P, _P, _P, _I]
+        lib.pmref_eval.restype = _I
+        lib.pmref_leapfrog.argtypes = [_P, _P, _P, _P, _D, _I, _P]
+        lib.pmref_leapfrog.restype = _I
+        lib.pmref_load_psf.restype = _I
+        _ref = lib
+    return _ref
+
+
+class _Arrays:
+    """Keeps contiguous copies of a system's arrays alive for a C call."""
+
+    def __init__(self, sysd):
+        self.type = np.ascontiguousarray(sysd["type"], dtype=np.int32)
+        self.q = np.ascontiguousarray(sysd["qscaled"], dtype=np.float64)
+        self.mol = np.ascontiguousarray(sysd["mol"], dtype=np.int32)
+        self.mass = np.ascontiguousarray(sysd["mass"], dtype=np.float64)
+        self.lj = np.ascontiguousarray(sysd["lj"], dtype=np.float64).reshape(-1)
+        ex = np.asarray(sysd["excl"], dtype=np.int32).reshape(-1, 3)
+        self.nexcl = ex.shape[0]
+        self.excl = np.ascontiguousarray(ex.reshape(-1)) if self.nexcl else np.zeros(3, np.int32)
+        self.ntypes = int(round(np.sqrt(self.lj.size // 4)))
+        self.n = self.type.size
+
+
+def _pmo_struct(sysd, ar: _Arrays):
+    s = _PmoSystem()
+    s.n = ar.n
+    s.ntypes = ar.ntypes
+    s.type, s.qscaled, s.mol, s.mass, s.lj = (_ptr(ar.type), _ptr(ar.q), _ptr(ar.mol),
+                                              _ptr(ar.mass), _ptr(ar.lj))
+    s.nexcl = ar.nexcl
+    s.excl = _ptr(ar.excl)
+    s.coulomb_scaling = float(sysd.get("coulomb_scaling", 1.0))
+    for k in range(3):
+        s.box[k] = float(sysd["box"][k])
+        s.origin[k] = float(sysd.get("origin", (0.0, 0.0, 0.0))[k])
+    s.cellsize = float(sysd["cellsize"])
+    s.ron, s.rc_lj, s.rc_coul, s.rc_alg = (float(sysd["ron"]), float(sysd["rc_lj"]),
+                                           float(sysd["rc_coul"]), float(sysd["rc_alg"]))
+    return s
+
+
+def restate_eval(sysd, pos, virial_mode=2, brute=False):
+    """Returns (forces[n,3], energies[2] = (coulomb, lj), virial[9], molvirial[9])."""
+    lib = restate_lib()
+    ar = _Arrays(sysd)
+    st = _pmo_struct(sysd, ar)
+    p = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1)
+    f = np.zeros(p.size)
+    e = np.zeros(2)
+    v = np.zeros(9)
+    mv = np.zeros(9)
+    rc = lib.pmo_eval(ctypes.byref(st), _ptr(p), _ptr(f), _ptr(e), _ptr(v), _ptr(mv),
+                      int(virial_mode), int(bool(brute)))
+    if rc:
+        raise RuntimeError(f"pmo_eval failed: {rc}")
+    return f.reshape(-1, 3), e, v, mv
+
+
+def restate_count_pairs(sysd, pos) -> int:
+    lib = restate_lib()
+    ar = _Arrays(sysd)
+    st = _pmo_struct(sysd, ar)
+    p = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1)
+    return int(lib.pmo_count_pairs(ctypes.byref(st), _ptr(p)))
+
+
+def restate_leapfrog(sysd, pos, vel, dt_fs, nsteps):
+    lib = restate_lib()
+    ar = _Arrays(sysd)
+    st = _pmo_struct(sysd, ar)
+    p = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1).copy()
+    v = np.ascontiguousarray(vel, dtype=np.float64).reshape(-1).copy()
+    e = np.zeros(2)
+    rc = lib.pmo_leapfrog(ctypes.byref(st), _ptr(p), _ptr(v), _ptr(ar.mass), float(dt_fs),
+                          int(nsteps), _ptr(e))
+    if rc:
+        raise RuntimeError(f"pmo_leapfrog failed: {rc}")
+    return p.reshape(-1, 3), v.reshape(-1, 3), e
+
+
+class RefForce:
+    """The reference's own NonbondedCutoffSystemForce (compiled from its
+    sources) on one system; evaluate() calls SystemForce::evaluate."""
+
+    def __init__(self, sysd):
+        self.lib = ref_lib()
+        self.ar = _Arrays(sysd)
+        ar = self.ar
+        box = np.ascontiguousarray(sysd["box"], dtype=np.float64)
+        org = np.ascontiguousarray(sysd.get("origin", (0.0, 0.0, 0.0)), dtype=np.float64)
+        self._keep = (box, org)
+        self.n = ar.n
+        self.h = self.lib.pmref_create(
+            ar.n, _ptr(ar.type), _ptr(ar.q), _ptr(ar.mol), _ptr(ar.mass), ar.ntypes,
+            _ptr(ar.lj), ar.nexcl, _ptr(ar.excl), float(sysd.get("coulomb_scaling", 1.0)),
+            _ptr(box), _ptr(org), float(sysd["cellsize"]), float(sysd["ron"]),
+            float(sysd["rc_lj"]), float(sysd["rc_coul"]), float(sysd["rc_alg"]))
+
+    def evaluate(self, pos, virial_mode=2):
+        p = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1)
+        f = np.zeros(p.size)
+        e = np.zeros(2)
+        v = np.zeros(9)
+        mv = np.zeros(9)
+        self.lib.pmref_eval(self.h, _ptr(p), _ptr(f), _ptr(e), _ptr(v), _ptr(mv), int(virial_mode))
+        return f.reshape(-1, 3), e, v, mv
+
+    def leapfrog(self, pos, vel, dt_fs, nsteps):
+        p = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1).copy()
+        v = np.ascontiguousarray(vel, dtype=np.float64).reshape(-1).copy()
+        e = np.zeros(2)
+        self.lib.pmref_leapfrog(self.h, _ptr(p), _ptr(v), _ptr(self.ar.mass), float(dt_fs),
+                                int(nsteps), _ptr(e))
+        return p.reshape(-1, 3), v.reshape(-1, 3), e
+
+    def close(self):
+        if self.h:
+            self.lib.pmref_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def ref_load_psf(psf, par, pdb, exclude="scaled1-4"):
+    """Reads a PSF/PAR/PDB triple with the reference's readers and topology
+    builder; returns a dict of the arrays the nonbonded force consumes."""
+    lib = ref_lib()
+    n, nt, ne = _I(), _I(), _I()
+    args = [psf.encode(), par.encode(), pdb.encode(), exclude.encode()]
+    rc = lib.pmref_load_psf(*args, ctypes.byref(n), ctypes.byref(nt), ctypes.byref(ne),
+                            None, None, None, None, None, None, None)
+    if rc:
+        raise RuntimeError(f"pmref_load_psf failed: {rc}")
+    N, NT, NE = n.value, nt.value, ne.value
+    pos = np.zeros(3 * N)
+    typ = np.zeros(N, np.int32)
+    q = np.zeros(N)
+    mol = np.zeros(N, np.int32)
+    mass = np.zeros(N)
+    lj = np.zeros(4 * NT * NT)
+    ex = np.zeros(3 * max(NE, 1), np.int32)
+    rc = lib.pmref_load_psf(*args, ctypes.byref(n), ctypes.byref(nt), ctypes.byref(ne),
+                            _ptr(pos), _ptr(typ), _ptr(q), _ptr(mol), _ptr(mass), _ptr(lj),
+                            _ptr(ex))
+    if rc:
+        raise RuntimeError(f"pmref_load_psf failed: {rc}")
+    return dict(pos=pos.reshape(N, 3), type=typ, qscaled=q, mol=mol, mass=mass,
+                lj=lj.reshape(NT, NT, 4), excl=ex[:3 * NE].reshape(NE, 3))

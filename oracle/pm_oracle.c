@@ -1,0 +1,583 @@
+/* CPU oracle: C restatement of ProtoMol's periodic cutoff nonbonded system
+ * force (LJ with C2 switching + Coulomb with C1 switching).
+ *
+ * TEST INFRASTRUCTURE ONLY (see pm_oracle.h).  Every function cites the
+ * reference code it restates; paths are relative to protomol/src/protomol/.
+ * The operation order inside each function follows the reference so that the
+ * FP64 results match it bit for bit on orthogonal periodic boxes.
+ */
+#include "pm_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define PMO_EPSILON 1.0e-14                 /* base/PMConstants.cpp:47 */
+#define PMO_INV_TIMEFACTOR 0.02045482828087295 /* base/PMConstants.cpp:51 */
+#define PMO_MAX_INT_2 (2147483647 / 2)       /* base/PMConstants.cpp:44 */
+
+/* ---------------------------------------------------------------------- */
+/* PeriodicBoundaryConditions (topology/PeriodicBoundaryConditions.cpp:32-77,
+ * orthogonal branch only).                                                */
+typedef struct {
+  double e[3];       /* e1.x, e2.y, e3.z */
+  double er[3];      /* reciprocal basis components myE1r.x, ... */
+  double origin[3];
+  double min[3], max[3];
+  double h[3], h2[3]; /* myH, myH2 */
+  double d;           /* myD: squared half of the smallest box length */
+} pbc_t;
+
+static void pbc_set(pbc_t *b, const double box[3], const double origin[3]) {
+  /* e1 = (Lx,0,0), e2 = (0,Ly,0), e3 = (0,0,Lz).
+   * a1 = e2 x e3, myE1r = a1 / e1.a1 (PeriodicBoundaryConditions.cpp:56-61) */
+  const double lx = box[0], ly = box[1], lz = box[2];
+  double a1x = ly * lz - 0.0 * 0.0;
+  double a2y = lz * lx - 0.0 * 0.0;
+  double a3z = lx * ly - 0.0 * 0.0;
+  double d1 = lx * a1x + 0.0 * 0.0 + 0.0 * 0.0;
+  double d2 = 0.0 * 0.0 + ly * a2y + 0.0 * 0.0;
+  double d3 = 0.0 * 0.0 + 0.0 * 0.0 + lz * a3z;
+  int k;
+  b->e[0] = lx; b->e[1] = ly; b->e[2] = lz;
+  b->er[0] = a1x / d1; b->er[1] = a2y / d2; b->er[2] = a3z / d3;
+  for (k = 0; k < 3; k++) {
+    /* a = origin - (e1+e2+e3)*0.5, b = origin + (e1+e2+e3)*0.5 (:63-71) */
+    double s = (k == 0 ? lx + 0.0 + 0.0 : k == 1 ? 0.0 + ly + 0.0 : 0.0 + 0.0 + lz);
+    double a = origin[k] - s * 0.5;
+    double c = origin[k] + s * 0.5;
+    b->origin[k] = origin[k];
+    b->min[k] = a < c ? a : c;
+    b->max[k] = a < c ? c : a;
+  }
+  {
+    double dx = (lx * 0.5) * (lx * 0.5);
+    double dy = (ly * 0.5) * (ly * 0.5);
+    double dz = (lz * 0.5) * (lz * 0.5);
+    double m = dy < dz ? dy : dz;
+    b->d = dx < m ? dx : m; /* myD = min(myDX, min(myDY, myDZ)) (:73-76) */
+  }
+  for (k = 0; k < 3; k++) {
+    b->h[k] = b->max[k] - b->min[k];
+    b->h2[k] = b->h[k] * 0.5;
+  }
+}
+
+static double norm2(const double v[3]) {
+  return v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+}
+
+/* minimalDifference(c1, c2, distSquared)
+ * (topology/PeriodicBoundaryConditions.h:72-110, orthogonal branch). */
+static void pbc_min_diff(const pbc_t *b, const double *c1, const double *c2,
+                         double diff[3], double *dist2) {
+  int k;
+  for (k = 0; k < 3; k++) diff[k] = c2[k] - c1[k];
+  *dist2 = norm2(diff);
+  if (*dist2 > b->d) {
+    for (k = 0; k < 3; k++) {
+      if (diff[k] < -b->h2[k])
+        diff[k] += b->h[k];
+      else if (diff[k] > b->h2[k])
+        diff[k] -= b->h[k];
+    }
+    *dist2 = norm2(diff);
+    if (*dist2 > b->d) {
+      for (k = 0; k < 3; k++) diff[k] -= b->e[k] * rint(b->er[k] * diff[k]);
+      *dist2 = norm2(diff);
+    }
+  }
+}
+
+/* minimalPosition(c) (topology/PeriodicBoundaryConditions.h:113-147). */
+static void pbc_min_pos(const pbc_t *b, const double *c, double out[3]) {
+  int k;
+  for (k = 0; k < 3; k++) out[k] = c[k] - b->origin[k];
+  if (norm2(out) <= b->d) return;
+  for (k = 0; k < 3; k++) {
+    if (out[k] < -b->h2[k])
+      out[k] += b->h[k];
+    else if (out[k] > b->h2[k])
+      out[k] -= b->h[k];
+  }
+  if (norm2(out) <= b->d) return;
+  for (k = 0; k < 3; k++) out[k] = out[k] - b->e[k] * rint(b->er[k] * out[k]);
+}
+
+/* ---------------------------------------------------------------------- */
+/* ExclusionTable::add / check (topology/ExclusionTable.cpp:103-120,
+ * topology/ExclusionTable.h:116-131): pair keyed by (min, max) atom index,
+ * later additions overwrite earlier ones.                                 */
+typedef struct {
+  long long key;
+  int kind;
+  int order;
+} excl_t;
+
+static int excl_cmp(const void *pa, const void *pb) {
+  const excl_t *a = (const excl_t *)pa, *b = (const excl_t *)pb;
+  if (a->key != b->key) return a->key < b->key ? -1 : 1;
+  return a->order < b->order ? -1 : (a->order > b->order);
+}
+
+static int excl_check(const excl_t *t, int m, int i, int j) {
+  long long key;
+  int lo = 0, hi = m - 1, found = 0;
+  if (j < i) { int tmp = i; i = j; j = tmp; }
+  key = ((long long)i << 32) | (unsigned)j;
+  /* last entry with this key wins */
+  while (lo <= hi) {
+    int mid = (lo + hi) / 2;
+    if (t[mid].key <= key) {
+      if (t[mid].key == key) found = t[mid].kind;
+      lo = mid + 1;
+    } else
+      hi = mid - 1;
+  }
+  return found;
+}
+
+/* ---------------------------------------------------------------------- */
+/* Switching functions and potentials.                                      */
+typedef struct {
+  double ron2, rc2, s1, s2, s3; /* C2 (switch/C2SwitchingFunction.cpp:12-18) */
+  double c_rc2, c15_1, c05_3, c15_3; /* C1 (switch/C1SwitchingFunction.cpp:12-16) */
+  double cut2;                  /* OneAtomPairTwo mySquaredCutoff (OneAtomPairTwo.h:38-40) */
+} sw_t;
+
+static void sw_set(sw_t *w, double ron, double rc_lj, double rc_coul) {
+  double t = rc_lj * rc_lj - ron * ron;
+  w->ron2 = ron * ron;
+  w->rc2 = rc_lj * rc_lj;
+  w->s1 = 1.0 / ((t * t) * t);                  /* power<3> = (x*x)*x */
+  w->s2 = rc_lj * rc_lj - 3.0 * ron * ron;
+  w->s3 = 4.0 / ((t * t) * t);
+  w->c_rc2 = rc_coul * rc_coul;
+  w->c15_1 = 1.5 / rc_coul;
+  w->c05_3 = 0.5 / (rc_coul * rc_coul * rc_coul);
+  w->c15_3 = 1.5 / (rc_coul * rc_coul * rc_coul);
+  w->cut2 = w->rc2 > w->c_rc2 ? w->rc2 : w->c_rc2;
+}
+
+/* C2SwitchingFunction::operator() (switch/C2SwitchingFunction.h:42-53). */
+static void c2_switch(const sw_t *w, double d2, double *value, double *deriv) {
+  *deriv = 0.0;
+  if (d2 > w->rc2)
+    *value = 0.0;
+  else if (d2 >= w->ron2) {
+    double c2 = w->rc2 - d2;
+    double c4 = c2 * (w->s2 + 2.0 * d2);
+    *value = w->s1 * (c2 * c4);
+    *deriv = w->s3 * (c2 * c2 - c4);
+  } else
+    *value = 1.0;
+}
+
+/* C1SwitchingFunction::operator() (switch/C1SwitchingFunction.h:41-50). */
+static void c1_switch(const sw_t *w, double d2, double *value, double *deriv) {
+  double dist;
+  if (d2 > w->c_rc2) {
+    *value = 0.0;
+    *deriv = 0.0;
+    return;
+  }
+  dist = sqrt(d2);
+  *value = 1.0 - dist * (w->c15_1 - d2 * w->c05_3);
+  *deriv = -w->c15_1 / dist + dist * w->c15_3;
+}
+
+/* ---------------------------------------------------------------------- */
+typedef struct {
+  const pmo_system *s;
+  const double *pos;
+  double *forces;
+  double e_coul, e_lj;
+  double vir[9], mvir[9];
+  int virial_mode;
+  pbc_t pbc;
+  sw_t sw;
+  excl_t *excl;
+  int nexcl;
+  double *molpos; /* [nmol*3] when virial_mode == 2 */
+  long long pairs;
+  int count_only;
+} ctx_t;
+
+/* ScalarStructure::addVirial(force12, diff) (type/ScalarStructure.cpp:36-54) */
+static void add_virial(double *t, const double f[3], const double d[3]) {
+  double xy = f[0] * d[1];
+  double xz = f[0] * d[2];
+  double yz = f[1] * d[2];
+  t[0] += f[0] * d[0];
+  t[1] += xy;
+  t[2] += xz;
+  t[3] += xy;
+  t[4] += f[1] * d[1];
+  t[5] += yz;
+  t[6] += xz;
+  t[7] += yz;
+  t[8] += f[2] * d[2];
+}
+
+/* OneAtomPairTwo::doOneAtomPair (force/OneAtomPairTwo.h:57-125) with
+ * LennardJonesForce (force/LennardJonesForce.h:29-61) first and
+ * CoulombForce (force/CoulombForce.h:27-38) second. */
+static void one_pair(ctx_t *c, int i, int j) {
+  const pmo_system *s = c->s;
+  double diff[3], d2, r2, e1, f1, e2, f2, sv, sd, fij[3], fs;
+  int mi, mj, same, excl = 0, k;
+  pbc_min_diff(&c->pbc, c->pos + 3 * i, c->pos + 3 * j, diff, &d2);
+  if (d2 > c->sw.cut2) return;
+  mi = s->mol[i];
+  mj = s->mol[j];
+  same = (mi == mj);
+  if (same) excl = excl_check(c->excl, c->nexcl, i, j);
+  if (excl == 2) return;
+  if (c->count_only) {
+    c->pairs++;
+    return;
+  }
+  r2 = 1.0 / d2;
+  { /* Lennard-Jones */
+    const double *p = s->lj + 4 * (s->type[i] * s->ntypes + s->type[j]);
+    double A = excl != 1 ? p[0] : p[2];
+    double B = excl != 1 ? p[1] : p[3];
+    double r6 = r2 * r2 * r2;
+    double r12 = r6 * r6;
+    double r6B = B * r6;
+    double r12A = A * r12;
+    e1 = r12A - r6B;
+    f1 = 12.0 * r12A * r2 - 6.0 * r6B * r2;
+  }
+  { /* Coulomb on pre-scaled charges */
+    e2 = s->qscaled[i] * s->qscaled[j] * sqrt(r2);
+    if (excl == 1) e2 *= s->coulomb_scaling;
+    f2 = e2 * r2;
+  }
+  c2_switch(&c->sw, d2, &sv, &sd);
+  f1 = f1 * sv - e1 * sd;
+  e1 = e1 * sv;
+  c1_switch(&c->sw, d2, &sv, &sd);
+  f2 = f2 * sv - e2 * sd;
+  e2 = e2 * sv;
+  c->e_lj += e1;
+  c->e_coul += e2;
+  fs = f1 + f2;
+  for (k = 0; k < 3; k++) fij[k] = diff[k] * fs;
+  for (k = 0; k < 3; k++) {
+    c->forces[3 * i + k] -= fij[k];
+    c->forces[3 * j + k] += fij[k];
+  }
+  if (!same && c->virial_mode >= 2) {
+    double cd[3], cd2;
+    pbc_min_diff(&c->pbc, c->molpos + 3 * mi, c->molpos + 3 * mj, cd, &cd2);
+    add_virial(c->vir, fij, diff);
+    add_virial(c->mvir, fij, cd);
+  } else if (c->virial_mode >= 1)
+    add_virial(c->vir, fij, diff);
+}
+
+/* molecularCenterOfMass with Kahan summation over the molecule's atoms in
+ * ascending index order (topology/TopologyUtilities.cpp:645-683). */
+static int build_molpos(ctx_t *c) {
+  const pmo_system *s = c->s;
+  int nmol = 0, i, k;
+  double *sum, *comp, *mass;
+  int *seen;
+  for (i = 0; i < s->n; i++)
+    if (s->mol[i] + 1 > nmol) nmol = s->mol[i] + 1;
+  c->molpos = (double *)calloc((size_t)nmol * 3 + 1, sizeof(double));
+  sum = (double *)calloc((size_t)nmol * 3 + 1, sizeof(double));
+  comp = (double *)calloc((size_t)nmol * 3 + 1, sizeof(double));
+  mass = (double *)calloc((size_t)nmol + 1, sizeof(double));
+  seen = (int *)calloc((size_t)nmol + 1, sizeof(int));
+  if (!c->molpos || !sum || !comp || !mass || !seen) {
+    free(sum); free(comp); free(mass); free(seen);
+    return PMO_ENOMEM;
+  }
+  for (i = 0; i < s->n; i++) {
+    int m = s->mol[i];
+    double w = s->mass ? s->mass[i] : 1.0;
+    if (!seen[m]) {
+      seen[m] = 1;
+      mass[m] = w;
+      for (k = 0; k < 3; k++) sum[3 * m + k] = c->pos[3 * i + k] * w;
+    } else {
+      mass[m] += w;
+      for (k = 0; k < 3; k++) {
+        double x = c->pos[3 * i + k] * w;
+        double y = x - comp[3 * m + k];
+        double t = sum[3 * m + k] + y;
+        comp[3 * m + k] = (t - sum[3 * m + k]) - y;
+        sum[3 * m + k] = t;
+      }
+    }
+  }
+  for (i = 0; i < nmol; i++)
+    for (k = 0; k < 3; k++)
+      c->molpos[3 * i + k] = seen[i] ? sum[3 * i + k] / mass[i] : 0.0;
+  free(sum); free(comp); free(mass); free(seen);
+  return PMO_OK;
+}
+
+/* ---------------------------------------------------------------------- */
+/* Cell list + cell-pair walk.
+ *  - CubicCellManager::initialize (topology/CubicCellManager.cpp:46-65):
+ *    cell edge = box / max(1, floor(box / cellsize)) per axis.
+ *  - ArrayCellListStructure::initialize (topology/ArrayCellListStructure.cpp:
+ *    22-128): n = max(1, floor(box / edge + EPSILON)); cells stored x-major,
+ *    z fastest.
+ *  - Topology::updateCellLists (topology/Topology.h:44-86): atoms inserted
+ *    from N-1 down to 0 at the head of their cell's list, cell =
+ *    floor((origin - min + minimalPosition(p)) / edge).
+ *  - CellListEnumerator<Periodic, Cubic>::initialize/next
+ *    (topology/CellListEnumeratorPeriodicBoundaries.h:25-134): neighbour
+ *    deltas with sum(((|k|-1)+ * edge)^2) < cutoff^2, reduced to basis cells,
+ *    de-duplicated, sorted (x, y, z); each cell pair visited from the lower
+ *    array index, self pair first.
+ *  - NonbondedCutoffForce::doEvaluate (force/nonbonded/NonbondedCutoffForce.h:
+ *    37-54): i over cell A, j over cell B (or i's successors in a self cell).
+ */
+typedef struct { int x, y, z; } cell3;
+
+static int cell3_cmp(const void *pa, const void *pb) {
+  const cell3 *a = (const cell3 *)pa, *b = (const cell3 *)pb;
+  if (a->x != b->x) return a->x < b->x ? -1 : 1;
+  if (a->y != b->y) return a->y < b->y ? -1 : 1;
+  if (a->z != b->z) return a->z < b->z ? -1 : 1;
+  return 0;
+}
+
+static int imod(int a, int maxn, int n) { return (a + maxn) % n; }
+
+static int walk_cells(ctx_t *c) {
+  const pmo_system *s = c->s;
+  const pbc_t *b = &c->pbc;
+  double vdiff[3], edge[3], inv[3];
+  int nd[3], maxn[3], n1[3], maxn1[3], k, i;
+  int *head, *next;
+  int ncell, begin, end, ndelta = 0;
+  cell3 *deltas;
+  double cut2 = s->rc_alg * s->rc_alg;
+  for (k = 0; k < 3; k++) {
+    double m = floor((b->max[k] - b->min[k]) / s->cellsize);
+    vdiff[k] = b->max[k] - b->min[k];
+    edge[k] = vdiff[k] / (1.0 > m ? 1.0 : m);
+  }
+  for (k = 0; k < 3; k++) inv[k] = 1.0 / edge[k];
+  for (k = 0; k < 3; k++) {
+    int v = (int)floor(vdiff[k] / edge[k] + PMO_EPSILON);
+    nd[k] = v > 1 ? v : 1;
+    maxn[k] = PMO_MAX_INT_2 - PMO_MAX_INT_2 % nd[k];
+    n1[k] = -nd[k] / 2;
+    maxn1[k] = maxn[k] - n1[k];
+  }
+  ncell = nd[0] * nd[1] * nd[2];
+  head = (int *)malloc(sizeof(int) * (size_t)ncell);
+  next = (int *)malloc(sizeof(int) * (size_t)(s->n > 0 ? s->n : 1));
+  if (!head || !next) { free(head); free(next); return PMO_ENOMEM; }
+  for (i = 0; i < ncell; i++) head[i] = -1;
+  for (i = s->n - 1; i >= 0; i--) {
+    double mp[3];
+    int cc[3], idx;
+    pbc_min_pos(b, c->pos + 3 * i, mp);
+    for (k = 0; k < 3; k++) {
+      double p = (b->origin[k] - b->min[k]) + mp[k];
+      cc[k] = (int)floor(p * inv[k]);
+      /* The reference writes outside its cell array when rounding puts a
+       * coordinate exactly on the upper box face; clamp instead. */
+      if (cc[k] < 0) cc[k] = 0;
+      if (cc[k] >= nd[k]) cc[k] = nd[k] - 1;
+    }
+    idx = (cc[0] * nd[1] + cc[1]) * nd[2] + cc[2];
+    next[i] = head[idx];
+    head[idx] = i;
+  }
+  /* neighbour deltas */
+  {
+    int lim[3];
+    for (k = 0; k < 3; k++) {
+      int v = (int)(s->rc_alg / edge[k] + 1.0 + PMO_EPSILON);
+      lim[k] = v < nd[k] ? v : nd[k];
+    }
+    deltas = (cell3 *)malloc(sizeof(cell3) *
+                             (size_t)((2 * lim[0] + 1) * (2 * lim[1] + 1) * (2 * lim[2] + 1)));
+    if (!deltas) { free(head); free(next); return PMO_ENOMEM; }
+    {
+      double xx = edge[0] * edge[0], yy = edge[1] * edge[1], zz = edge[2] * edge[2];
+      int kx, ly, mz;
+      for (kx = -lim[0]; kx <= lim[0]; kx++) {
+        int x = abs(kx) - 1;
+        double d0;
+        if (x < 0) x = 0;
+        d0 = x * x * xx;
+        for (ly = -lim[1]; ly <= lim[1]; ly++) {
+          int y = abs(ly) - 1;
+          double d1;
+          if (y < 0) y = 0;
+          d1 = d0 + y * y * yy;
+          for (mz = -lim[2]; mz <= lim[2]; mz++) {
+            int z = abs(mz) - 1;
+            if (z < 0) z = 0;
+            if (d1 + z * z * zz < cut2) {
+              cell3 md;
+              int q, dup = 0;
+              md.x = (kx + maxn1[0]) % nd[0] + n1[0];
+              md.y = (ly + maxn1[1]) % nd[1] + n1[1];
+              md.z = (mz + maxn1[2]) % nd[2] + n1[2];
+              if (md.x == 0 && md.y == 0 && md.z == 0) dup = 1;
+              for (q = 0; q < ndelta && !dup; q++)
+                if (deltas[q].x == md.x && deltas[q].y == md.y && deltas[q].z == md.z) dup = 1;
+              if (!dup) deltas[ndelta++] = md;
+            }
+          }
+        }
+      }
+    }
+    qsort(deltas, (size_t)ndelta, sizeof(cell3), cell3_cmp);
+  }
+  /* cell-pair walk */
+  begin = ncell;
+  end = 0;
+  for (i = 0; i < ncell; i++)
+    if (head[i] >= 0) {
+      if (begin == ncell) begin = i;
+      end = i + 1;
+    }
+  if (begin == ncell) begin = end = 0;
+  {
+    int ci = begin, cj = begin, counter = 0;
+    while (ci != end) {
+      int a, bb;
+      for (a = head[ci]; a != -1; a = next[a])
+        for (bb = (ci != cj) ? head[cj] : next[a]; bb != -1; bb = next[bb])
+          one_pair(c, a, bb);
+      /* next() */
+      do {
+        if (ci != end) {
+          cj = end;
+          while (counter != ndelta) {
+            int x = ci / (nd[1] * nd[2]);
+            int y = (ci / nd[2]) % nd[1];
+            int z = ci % nd[2];
+            const cell3 *d = &deltas[counter++];
+            int jx = imod(x + d->x, maxn[0], nd[0]);
+            int jy = imod(y + d->y, maxn[1], nd[1]);
+            int jz = imod(z + d->z, maxn[2], nd[2]);
+            int jdx = (jx * nd[1] + jy) * nd[2] + jz;
+            if (head[jdx] >= 0) { cj = jdx; break; }
+          }
+          if (cj == end) {
+            ++ci;
+            while (ci != end && head[ci] < 0) ++ci;
+            cj = ci;
+            counter = 0;
+          }
+        }
+      } while (ci > cj);
+    }
+  }
+  free(deltas);
+  free(head);
+  free(next);
+  return PMO_OK;
+}
+
+static int ctx_init(ctx_t *c, const pmo_system *s, const double *pos,
+                    double *forces, int virial_mode) {
+  int e;
+  memset(c, 0, sizeof(*c));
+  if (!s || s->n < 0 || !pos || s->ntypes <= 0 || s->cellsize <= 0.0 ||
+      s->rc_lj <= 0.0 || s->rc_coul <= 0.0 || s->rc_alg <= 0.0 ||
+      s->ron < 0.0 || s->ron >= s->rc_lj || s->box[0] <= 0.0 ||
+      s->box[1] <= 0.0 || s->box[2] <= 0.0)
+    return PMO_EBADARG;
+  c->s = s;
+  c->pos = pos;
+  c->forces = forces;
+  c->virial_mode = virial_mode;
+  pbc_set(&c->pbc, s->box, s->origin);
+  sw_set(&c->sw, s->ron, s->rc_lj, s->rc_coul);
+  c->nexcl = s->nexcl;
+  c->excl = (excl_t *)malloc(sizeof(excl_t) * (size_t)(s->nexcl > 0 ? s->nexcl : 1));
+  if (!c->excl) return PMO_ENOMEM;
+  for (e = 0; e < s->nexcl; e++) {
+    int a = s->excl[3 * e], b = s->excl[3 * e + 1];
+    if (b < a) { int t = a; a = b; b = t; }
+    c->excl[e].key = ((long long)a << 32) | (unsigned)b;
+    c->excl[e].kind = s->excl[3 * e + 2];
+    c->excl[e].order = e;
+  }
+  qsort(c->excl, (size_t)s->nexcl, sizeof(excl_t), excl_cmp);
+  if (virial_mode >= 2) return build_molpos(c);
+  return PMO_OK;
+}
+
+static void ctx_free(ctx_t *c) {
+  free(c->excl);
+  free(c->molpos);
+}
+
+int pmo_eval(const pmo_system *s, const double *pos, double *forces,
+             double *energies, double *virial, double *molvirial,
+             int virial_mode, int brute) {
+  ctx_t c;
+  int rc = ctx_init(&c, s, pos, forces, virial_mode), k;
+  if (rc) { ctx_free(&c); return rc; }
+  if (!forces || !energies) { ctx_free(&c); return PMO_EBADARG; }
+  if (brute) {
+    int i, j;
+    for (i = 0; i < s->n; i++)
+      for (j = i + 1; j < s->n; j++) one_pair(&c, i, j);
+  } else {
+    rc = walk_cells(&c);
+  }
+  energies[0] += c.e_coul;
+  energies[1] += c.e_lj;
+  if (virial && virial_mode >= 1)
+    for (k = 0; k < 9; k++) virial[k] += c.vir[k];
+  if (molvirial && virial_mode >= 2)
+    for (k = 0; k < 9; k++) molvirial[k] += c.mvir[k];
+  ctx_free(&c);
+  return rc;
+}
+
+long long pmo_count_pairs(const pmo_system *s, const double *pos) {
+  ctx_t c;
+  long long n;
+  if (ctx_init(&c, s, pos, NULL, 0)) { ctx_free(&c); return -1; }
+  c.count_only = 1;
+  if (walk_cells(&c)) { ctx_free(&c); return -1; }
+  n = c.pairs;
+  ctx_free(&c);
+  return n;
+}
+
+/* LeapfrogIntegrator::run / doKickdoDrift without modifiers
+ * (integrator/leapfrog/LeapfrogIntegrator.cpp:58-105): h = dt *
+ * INV_TIMEFACTOR, v += F h / m, x += v h. */
+int pmo_leapfrog(const pmo_system *s, double *pos, double *vel,
+                 const double *mass, double dt_fs, int nsteps,
+                 double *energies) {
+  const double h = dt_fs * PMO_INV_TIMEFACTOR;
+  const int n = s->n;
+  double *f = (double *)calloc((size_t)3 * (size_t)(n > 0 ? n : 1), sizeof(double));
+  double e[2] = {0.0, 0.0};
+  int step, i, k, rc;
+  if (!f) return PMO_ENOMEM;
+  rc = pmo_eval(s, pos, f, e, NULL, NULL, 0, 0);
+  for (step = 0; step < nsteps && !rc; step++) {
+    double kick = step == 0 ? 0.5 * h : h;
+    for (i = 0; i < n; i++)
+      for (k = 0; k < 3; k++) vel[3 * i + k] += f[3 * i + k] * kick / mass[i];
+    for (i = 0; i < 3 * n; i++) pos[i] += vel[i] * h;
+    for (i = 0; i < 3 * n; i++) f[i] = 0.0;
+    e[0] = e[1] = 0.0;
+    rc = pmo_eval(s, pos, f, e, NULL, NULL, 0, 0);
+  }
+  for (i = 0; i < n; i++)
+    for (k = 0; k < 3; k++) vel[3 * i + k] += f[3 * i + k] * 0.5 * h / mass[i];
+  if (energies) { energies[0] = e[0]; energies[1] = e[1]; }
+  free(f);
+  return rc;
+}

@@ -1,0 +1,74 @@
+/* CPU oracle for the periodic cutoff nonbonded system force.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Tests, the smoke check and the CPU-baseline leg
+ * of bench.py use this as the checker; the product never calls it.
+ *
+ * A plain C restatement of
+ *   NonbondedCutoffSystemForce<CubicCellManager,
+ *     OneAtomPairTwo<PeriodicBoundaryConditions, C2SwitchingFunction,
+ *                    LennardJonesForce, C1SwitchingFunction, CoulombForce>>
+ * from ProtoMol (protomol/src/protomol/...), following the reference's cell
+ * build, cell-pair enumeration order and per-pair arithmetic operation by
+ * operation, so that its FP64 results agree with the reference bit for bit on
+ * the inputs the tests use.  Parity pins: the reference's own code compiled
+ * from its sources (oracle/_ref/libpmref.so, recipe in oracle/Makefile) and
+ * the reference's periodic water golden (test/tests/expected/
+ * water_CHARMM_PERIODIC_L.energy, t = 0 energies), both checked in tests/.
+ */
+#ifndef PM_ORACLE_H
+#define PM_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+  int n;                 /* atoms */
+  int ntypes;            /* LJ atom types */
+  const int *type;       /* [n] LJ type index */
+  const double *qscaled; /* [n] charge * SQRTCOULOMBCONSTANT */
+  const int *mol;        /* [n] molecule id (0..nmol-1) */
+  const double *mass;    /* [n] scaled mass; only for the molecular virial */
+  const double *lj;      /* [ntypes*ntypes*4] {A, B, A14, B14} */
+  int nexcl;             /* exclusion pairs */
+  const int *excl;       /* [nexcl*3] {a1, a2, kind}; kind 1 modified, 2 full */
+  double coulomb_scaling;/* topology coulombScalingFactor (1-4 Coulomb) */
+  double box[3];         /* orthogonal cell basis lengths e1.x, e2.y, e3.z */
+  double origin[3];      /* cellorigin */
+  double cellsize;       /* CubicCellManager cellsize */
+  double ron, rc_lj;     /* C2 switch (Lennard-Jones) */
+  double rc_coul;        /* C1 switch (Coulomb) */
+  double rc_alg;         /* NonbondedCutoff algorithm cutoff */
+} pmo_system;
+
+/* Error codes */
+#define PMO_OK 0
+#define PMO_EBADARG 1
+#define PMO_ENOMEM 2
+
+/* One SystemForce::evaluate.  pos: AoS double[3n] (not wrapped).  forces:
+ * AoS double[3n], accumulated into.  energies[0] = Coulomb, [1] = LJ
+ * (accumulated into).  virial_mode: 0 none, 1 atomic virial, 2 atomic +
+ * molecular virial (virial/molvirial: 9 doubles, accumulated, may be NULL
+ * when not requested).  brute: 0 = cell-list walk exactly as the reference,
+ * 1 = all pairs i<j with the same per-pair code (the reference's
+ * NonbondedSimpleFull cross-check). */
+int pmo_eval(const pmo_system *s, const double *pos, double *forces,
+             double *energies, double *virial, double *molvirial,
+             int virial_mode, int brute);
+
+/* Unique pairs (i<j, not fully excluded) inside max(rc_lj, rc_coul) under
+ * the minimum image; the Gpairs/s unit. */
+long long pmo_count_pairs(const pmo_system *s, const double *pos);
+
+/* Leapfrog with this force alone (LeapfrogIntegrator::run with no
+ * modifiers): initial force, then per step kick (half on the first step) +
+ * drift + force, and a closing half kick.  dt in fs. */
+int pmo_leapfrog(const pmo_system *s, double *pos, double *vel,
+                 const double *mass, double dt_fs, int nsteps,
+                 double *energies);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

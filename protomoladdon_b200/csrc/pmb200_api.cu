@@ -1,0 +1,720 @@
+// libpmb200: host side of the C ABI declared in include/pmb200.h.
+//
+// One context = one periodic system on one GPU: device copies of the
+// topology, the cell grid for the current box, per-evaluation buffers and a
+// CUDA stream.  An evaluation is
+//   k_cell_index -> k_scan -> k_scatter -> k_rank_gather   (counting sort)
+//   k_pair_mixed | k_pair_fp64                            (forces, partials)
+//   [k_com -> k_molvir] -> k_reduce                        (energies, virial)
+// all on the context's stream.
+#include "../../include/pmb200.h"
+#include "pmb200_kernels.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <utility>
+#include <vector>
+
+using namespace pmb200;
+
+struct pmb200_ctx {
+  pmb200_params p{};
+  std::string err;
+  cudaStream_t stream = nullptr;
+  // topology
+  int n = 0, ntypes = 0, nmol = 0;
+  bool have_topo = false, have_box = false, have_mass = false;
+  double csf = 1.0;
+  std::vector<double> h_lj;  // ntypes^2 * 4
+  int *d_type = nullptr, *d_mol = nullptr;
+  double *d_q = nullptr, *d_mass = nullptr;
+  int *d_ex_start = nullptr;
+  int2 *d_ex = nullptr;
+  int *d_mstart = nullptr, *d_matoms = nullptr;
+  float4 *d_lj32 = nullptr;
+  double4 *d_lj64 = nullptr;
+  // grid
+  GridParams g{};
+  MixedConsts mc{};
+  Fp64Consts fc{};
+  std::vector<Row> rows;
+  Stencil stencil{};
+  int ncell_alloc = 0;
+  int *d_count = nullptr, *d_start = nullptr, *d_err = nullptr;
+  double *d_partial = nullptr;
+  // per-atom buffers
+  int n_alloc = 0;
+  int *d_cell_of = nullptr, *d_slot = nullptr, *d_tmp = nullptr, *d_sidx = nullptr;
+  float4 *d_rel32 = nullptr, *d_spos32 = nullptr;
+  double4 *d_rel64 = nullptr, *d_spos64 = nullptr;
+  int2 *d_smeta = nullptr;
+  double *d_finter = nullptr, *d_com = nullptr, *d_mvpart = nullptr;
+  double *d_pairs = nullptr, *d_out = nullptr;
+  // host-buffer evaluation scratch
+  double *d_hpos = nullptr, *d_hfrc = nullptr;
+  // leapfrog graph
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  const void *graph_key[4] = {nullptr, nullptr, nullptr, nullptr};
+  double graph_dt = 0.0;
+  // one-step graph (pmb200_step_device)
+  cudaGraph_t sgraph = nullptr;
+  cudaGraphExec_t sgraph_exec = nullptr;
+  const void *sgraph_key[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  double sgraph_dt = 0.0;
+  unsigned sgraph_flags = 0;
+  int sgraph_timing = -1;
+  // pair-kernel timing
+  int timing = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace {
+
+constexpr int kMolvirBlocks = 64;
+
+int fail(pmb200_ctx *c, int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (c) c->err = buf;
+  return code;
+}
+
+#define CK(call)                                                                 \
+  do {                                                                           \
+    cudaError_t e_ = (call);                                                     \
+    if (e_ != cudaSuccess)                                                       \
+      return fail(c, PMB200_ECUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+template <class T>
+void dfree(T *&p) {
+  if (p) cudaFree((void *)p);
+  p = nullptr;
+}
+
+template <class T>
+cudaError_t dalloc(T *&p, size_t count) {
+  dfree(p);
+  if (count == 0) count = 1;
+  return cudaMalloc((void **)&p, sizeof(T) * count);
+}
+
+void release_graph(pmb200_ctx *c) {
+  if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+  if (c->graph) cudaGraphDestroy(c->graph);
+  c->graph_exec = nullptr;
+  c->graph = nullptr;
+  for (auto &k : c->graph_key) k = nullptr;
+  if (c->sgraph_exec) cudaGraphExecDestroy(c->sgraph_exec);
+  if (c->sgraph) cudaGraphDestroy(c->sgraph);
+  c->sgraph_exec = nullptr;
+  c->sgraph = nullptr;
+  for (auto &k : c->sgraph_key) k = nullptr;
+}
+
+double rc_max(const pmb200_params &p) { return std::max(p.cutoff_lj, p.cutoff_coul); }
+
+// LJ tables: FP64 in Angstrom units, FP32 in cell units (A / u^12, B / u^6).
+int upload_lj(pmb200_ctx *c) {
+  const int t2 = c->ntypes * c->ntypes;
+  std::vector<double4> l64(t2);
+  std::vector<float4> l32(t2);
+  const double u = c->g.unit;
+  const double u6 = std::pow(u, 6.0), u12 = u6 * u6;
+  for (int k = 0; k < t2; k++) {
+    const double *p = &c->h_lj[4 * k];
+    l64[k] = make_double4(p[0], p[1], p[2], p[3]);
+    l32[k] = make_float4((float)(p[0] / u12), (float)(p[1] / u6), (float)(p[2] / u12),
+                         (float)(p[3] / u6));
+  }
+  CK(cudaMemcpyAsync(c->d_lj64, l64.data(), sizeof(double4) * t2, cudaMemcpyHostToDevice,
+                     c->stream));
+  CK(cudaMemcpyAsync(c->d_lj32, l32.data(), sizeof(float4) * t2, cudaMemcpyHostToDevice,
+                     c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return PMB200_OK;
+}
+
+int ensure_atom_buffers(pmb200_ctx *c) {
+  if (c->n_alloc >= c->n && c->d_cell_of) return PMB200_OK;
+  const size_t n = (size_t)std::max(c->n, 1);
+  CK(dalloc(c->d_cell_of, n));
+  CK(dalloc(c->d_slot, n));
+  CK(dalloc(c->d_tmp, n));
+  CK(dalloc(c->d_sidx, n));
+  CK(dalloc(c->d_rel32, n));
+  CK(dalloc(c->d_spos32, n));
+  CK(dalloc(c->d_rel64, n));
+  CK(dalloc(c->d_spos64, n));
+  CK(dalloc(c->d_smeta, n));
+  CK(dalloc(c->d_finter, 3 * n));
+  CK(dalloc(c->d_hpos, 3 * n));
+  CK(dalloc(c->d_hfrc, 3 * n));
+  c->n_alloc = c->n;
+  return PMB200_OK;
+}
+
+// Launch one evaluation on `st`.  accumulate: add into d_forces (1) or
+// overwrite it (0).
+int launch_eval(pmb200_ctx *c, const double *d_pos, double *d_forces, double *d_out,
+                unsigned flags, int accumulate, cudaStream_t st) {
+  const int n = c->n;
+  const bool mixed = c->p.precision == PMB200_MIXED;
+  const bool energy = (flags & PMB200_ENERGY) != 0;
+  const bool virial = (flags & (PMB200_VIRIAL | PMB200_MOLVIRIAL)) != 0;
+  const bool molvir = (flags & PMB200_MOLVIRIAL) != 0;
+  const GridParams &g = c->g;
+  CK(cudaMemsetAsync(c->d_count, 0, sizeof(int) * g.ncell, st));
+  if (n > 0) {
+    const int tb = 256;
+    k_cell_index<<<(n + tb - 1) / tb, tb, 0, st>>>(
+        n, d_pos, g, c->d_cell_of, c->d_count, c->d_slot, mixed ? c->d_rel32 : nullptr,
+        mixed ? nullptr : c->d_rel64, c->d_q, (float)(1.0 / std::sqrt(g.unit)), c->d_err);
+  }
+  k_scan<<<1, 1024, 1024 * sizeof(int), st>>>(g.ncell, c->d_count, c->d_start);
+  if (n > 0) {
+    const int tb = 256;
+    k_scatter<<<(n + tb - 1) / tb, tb, 0, st>>>(n, c->d_cell_of, c->d_slot, c->d_start,
+                                                 c->d_tmp);
+  }
+  const int warps_per_block = 4;
+  const int blocks = (g.ncell + warps_per_block - 1) / warps_per_block;
+  k_rank_gather<<<blocks, 32 * warps_per_block, 0, st>>>(
+      g.ncell, c->d_start, c->d_tmp, mixed ? c->d_rel32 : nullptr,
+      mixed ? nullptr : c->d_rel64, c->d_type, c->d_mol, c->d_sidx,
+      mixed ? c->d_spos32 : nullptr, mixed ? nullptr : c->d_spos64, c->d_smeta);
+  double *finter = molvir ? c->d_finter : nullptr;
+  if (c->timing) CK(cudaEventRecord(c->ev0, st));
+  if (mixed) {
+    const double fscale = 1.0 / g.unit;
+#define PMB_MIXED_LAUNCH(E, V)                                                            \
+  k_pair_mixed<E, V><<<blocks, 128, 0, st>>>(g, c->mc, c->stencil, c->ntypes, c->d_lj32, c->d_start, \
+                                             c->d_spos32, c->d_smeta, c->d_sidx,          \
+                                             c->d_ex_start, c->d_ex, d_forces, accumulate, \
+                                             fscale, c->d_partial, finter)
+    if (energy && virial) PMB_MIXED_LAUNCH(true, true);
+    else if (energy) PMB_MIXED_LAUNCH(true, false);
+    else if (virial) PMB_MIXED_LAUNCH(false, true);
+    else PMB_MIXED_LAUNCH(false, false);
+#undef PMB_MIXED_LAUNCH
+  } else {
+#define PMB_FP64_LAUNCH(E, V)                                                            \
+  k_pair_fp64<E, V><<<blocks, 128, 0, st>>>(g, c->fc, c->stencil, c->ntypes, c->d_lj64, c->d_start, \
+                                            c->d_spos64, c->d_smeta, c->d_sidx,          \
+                                            c->d_ex_start, c->d_ex, d_forces, accumulate, \
+                                            c->d_partial, finter)
+    if (energy && virial) PMB_FP64_LAUNCH(true, true);
+    else if (energy) PMB_FP64_LAUNCH(true, false);
+    else if (virial) PMB_FP64_LAUNCH(false, true);
+    else PMB_FP64_LAUNCH(false, false);
+#undef PMB_FP64_LAUNCH
+  }
+  CK(cudaGetLastError());
+  if (c->timing) CK(cudaEventRecord(c->ev1, st));
+  if (energy || virial) {
+    int nmv = 0;
+    if (molvir) {
+      k_com<<<(c->nmol + 127) / 128, 128, 0, st>>>(c->nmol, c->d_mstart, c->d_matoms,
+                                                    c->d_mass, d_pos, c->d_com);
+      k_molvir<<<kMolvirBlocks, 256, 0, st>>>(n, c->d_mol, d_pos, c->d_com, c->d_finter,
+                                              c->d_mvpart);
+      nmv = kMolvirBlocks;
+    }
+    const double rcc = c->p.cutoff_coul / g.unit;
+    k_reduce<<<1, 256, 0, st>>>(g.ncell, c->d_partial, mixed ? 1 : 0, 1.5 / rcc,
+                                0.5 / (rcc * rcc * rcc), nmv, c->d_mvpart,
+                                d_out ? d_out : c->d_out, c->d_pairs);
+    CK(cudaGetLastError());
+  }
+  return PMB200_OK;
+}
+
+int check_ready(pmb200_ctx *c) {
+  if (!c) return PMB200_EINVAL;
+  if (!c->have_topo) return fail(c, PMB200_ESTATE, "pmb200_set_topology has not been called");
+  if (!c->have_box) return fail(c, PMB200_ESTATE, "pmb200_set_box has not been called");
+  return PMB200_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pmb200_create(const pmb200_params *params, pmb200_ctx **out) {
+  pmb200_ctx *c = nullptr;
+  if (!params || !out) return PMB200_EINVAL;
+  *out = nullptr;
+  const pmb200_params &p = *params;
+  if (p.precision != PMB200_MIXED && p.precision != PMB200_FP64)
+    return PMB200_EINVAL;
+  // C2SwitchingFunction::make validation (C2SwitchingFunction.cpp:30-41)
+  if (!(p.switchon >= 0.0) || !(p.cutoff_lj > 0.0) || !(p.switchon < p.cutoff_lj))
+    return PMB200_EINVAL;
+  if (!(p.cutoff_coul > 0.0) || !(p.cutoff_alg > 0.0)) return PMB200_EINVAL;
+  if (p.cutoff_alg < rc_max(p)) return PMB200_EUNSUPPORTED;
+  if (p.cellsize < 0.0) return PMB200_EINVAL;
+  c = new pmb200_ctx();
+  c->p = p;
+  cudaError_t e = cudaSetDevice(p.device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_err, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(c->d_err, 0, sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_out, sizeof(double) * 20);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_pairs, sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_mvpart, sizeof(double) * 9 * kMolvirBlocks);
+  if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
+  if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
+  if (e != cudaSuccess) {
+    pmb200_destroy(c);
+    return PMB200_ECUDA;
+  }
+  *out = c;
+  return PMB200_OK;
+}
+
+int pmb200_destroy(pmb200_ctx *c) {
+  if (!c) return PMB200_OK;
+  cudaSetDevice(c->p.device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  release_graph(c);
+  dfree(c->d_type); dfree(c->d_mol); dfree(c->d_q); dfree(c->d_mass);
+  dfree(c->d_ex_start); dfree(c->d_ex); dfree(c->d_mstart); dfree(c->d_matoms);
+  dfree(c->d_lj32); dfree(c->d_lj64);
+  dfree(c->d_count); dfree(c->d_start); dfree(c->d_err); dfree(c->d_partial);
+  dfree(c->d_cell_of); dfree(c->d_slot); dfree(c->d_tmp); dfree(c->d_sidx);
+  dfree(c->d_rel32); dfree(c->d_spos32); dfree(c->d_rel64); dfree(c->d_spos64);
+  dfree(c->d_smeta); dfree(c->d_finter); dfree(c->d_com); dfree(c->d_mvpart);
+  dfree(c->d_pairs); dfree(c->d_out); dfree(c->d_hpos); dfree(c->d_hfrc);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return PMB200_OK;
+}
+
+const char *pmb200_last_error(const pmb200_ctx *c) {
+  return c ? c->err.c_str() : "null context";
+}
+
+int pmb200_set_topology(pmb200_ctx *c, int n, const int *type, const double *q_scaled,
+                        const int *molecule, const double *mass, int ntypes,
+                        const double *lj, int nexcl, const int *excl,
+                        double coulomb_scaling) {
+  if (!c) return PMB200_EINVAL;
+  if (n < 0 || ntypes <= 0 || nexcl < 0) return fail(c, PMB200_EINVAL, "negative size");
+  if (n > 0 && (!type || !q_scaled || !molecule)) return fail(c, PMB200_EINVAL, "null array");
+  if (!lj) return fail(c, PMB200_EINVAL, "null LJ table");
+  if (nexcl > 0 && !excl) return fail(c, PMB200_EINVAL, "null exclusion array");
+  if (ntypes > kMaxTypes)
+    return fail(c, PMB200_EUNSUPPORTED, "%d LJ types; at most %d supported", ntypes, kMaxTypes);
+  CK(cudaSetDevice(c->p.device));
+  int nmol = 0;
+  for (int i = 0; i < n; i++) {
+    if (type[i] < 0 || type[i] >= ntypes)
+      return fail(c, PMB200_EINVAL, "atom %d: type %d outside [0, %d)", i, type[i], ntypes);
+    if (molecule[i] < 0) return fail(c, PMB200_EINVAL, "atom %d: negative molecule id", i);
+    if (!std::isfinite(q_scaled[i])) return fail(c, PMB200_EINVAL, "atom %d: charge", i);
+    nmol = std::max(nmol, molecule[i] + 1);
+  }
+  for (int k = 0; k < 4 * ntypes * ntypes; k++)
+    if (!std::isfinite(lj[k])) return fail(c, PMB200_EINVAL, "LJ table entry %d", k);
+  // ExclusionTable::add semantics: keyed by (min, max), later entries win,
+  // EXCLUSION_NONE removes (ExclusionTable.cpp:103-120).
+  std::map<std::pair<int, int>, int> kinds;
+  for (int e = 0; e < nexcl; e++) {
+    int a = excl[3 * e], b = excl[3 * e + 1], k = excl[3 * e + 2];
+    if (a < 0 || b < 0 || a >= n || b >= n)
+      return fail(c, PMB200_EINVAL, "exclusion %d: atom index out of range", e);
+    if (k < 0 || k > 2) return fail(c, PMB200_EINVAL, "exclusion %d: kind %d", e, k);
+    if (a == b) continue;
+    kinds[std::make_pair(std::min(a, b), std::max(a, b))] = k;
+  }
+  std::vector<std::vector<int2>> per(n);
+  for (const auto &kv : kinds) {
+    if (kv.second == 0) continue;
+    per[kv.first.first].push_back(make_int2(kv.first.second, kv.second));
+    per[kv.first.second].push_back(make_int2(kv.first.first, kv.second));
+  }
+  std::vector<int> ex_start(n + 1, 0);
+  std::vector<int2> ex;
+  for (int i = 0; i < n; i++) {
+    std::sort(per[i].begin(), per[i].end(), [](int2 x, int2 y) { return x.x < y.x; });
+    ex_start[i] = (int)ex.size();
+    ex.insert(ex.end(), per[i].begin(), per[i].end());
+  }
+  ex_start[n] = (int)ex.size();
+  std::vector<int> mstart(nmol + 1, 0), matoms(n);
+  for (int i = 0; i < n; i++) mstart[molecule[i] + 1]++;
+  for (int m = 0; m < nmol; m++) mstart[m + 1] += mstart[m];
+  {
+    std::vector<int> fill(mstart.begin(), mstart.end() - 1);
+    for (int i = 0; i < n; i++) matoms[fill[molecule[i]]++] = i;
+  }
+  release_graph(c);
+  c->n = n;
+  c->ntypes = ntypes;
+  c->nmol = nmol;
+  c->csf = coulomb_scaling;
+  c->have_mass = mass != nullptr;
+  c->h_lj.assign(lj, lj + 4 * ntypes * ntypes);
+  const size_t nn = (size_t)std::max(n, 1);
+  CK(dalloc(c->d_type, nn));
+  CK(dalloc(c->d_mol, nn));
+  CK(dalloc(c->d_q, nn));
+  CK(dalloc(c->d_mass, nn));
+  CK(dalloc(c->d_ex_start, nn + 1));
+  CK(dalloc(c->d_ex, std::max<size_t>(ex.size(), 1)));
+  CK(dalloc(c->d_mstart, (size_t)nmol + 1));
+  CK(dalloc(c->d_matoms, nn));
+  CK(dalloc(c->d_com, 3 * (size_t)std::max(nmol, 1)));
+  CK(dalloc(c->d_lj32, (size_t)ntypes * ntypes));
+  CK(dalloc(c->d_lj64, (size_t)ntypes * ntypes));
+  if (n > 0) {
+    CK(cudaMemcpy(c->d_type, type, sizeof(int) * n, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->d_mol, molecule, sizeof(int) * n, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->d_q, q_scaled, sizeof(double) * n, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->d_matoms, matoms.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    if (mass) CK(cudaMemcpy(c->d_mass, mass, sizeof(double) * n, cudaMemcpyHostToDevice));
+  }
+  CK(cudaMemcpy(c->d_ex_start, ex_start.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+  if (!ex.empty())
+    CK(cudaMemcpy(c->d_ex, ex.data(), sizeof(int2) * ex.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->d_mstart, mstart.data(), sizeof(int) * (nmol + 1), cudaMemcpyHostToDevice));
+  int rc = ensure_atom_buffers(c);
+  if (rc) return rc;
+  c->have_topo = true;
+  if (c->have_box) return upload_lj(c);
+  return PMB200_OK;
+}
+
+int pmb200_set_box(pmb200_ctx *c, const double e1[3], const double e2[3], const double e3[3],
+                   const double origin[3]) {
+  if (!c) return PMB200_EINVAL;
+  if (!e1 || !e2 || !e3 || !origin) return fail(c, PMB200_EINVAL, "null box vector");
+  if (e1[1] != 0.0 || e1[2] != 0.0 || e2[0] != 0.0 || e2[2] != 0.0 || e3[0] != 0.0 ||
+      e3[1] != 0.0)
+    return fail(c, PMB200_EUNSUPPORTED, "only orthogonal periodic boxes are supported");
+  const double L[3] = {std::fabs(e1[0]), std::fabs(e2[1]), std::fabs(e3[2])};
+  const double rc = rc_max(c->p);
+  for (int a = 0; a < 3; a++) {
+    if (!(L[a] > 0.0) || !std::isfinite(L[a]))
+      return fail(c, PMB200_EINVAL, "box edge %d is %g", a, L[a]);
+    if (L[a] < 2.0 * rc)
+      return fail(c, PMB200_EUNSUPPORTED,
+                  "box edge %g is below twice the cutoff %g (minimum image would need more "
+                  "than one image per pair)", L[a], rc);
+    if (!std::isfinite(origin[a])) return fail(c, PMB200_EINVAL, "origin");
+  }
+  CK(cudaSetDevice(c->p.device));
+  release_graph(c);
+  GridParams &g = c->g;
+  const double target = c->p.cellsize > 0.0 ? std::max(c->p.cellsize, rc / 3.0) : rc / 2.0;
+  int nd[3];
+  for (int a = 0; a < 3; a++) {
+    nd[a] = std::max(1, (int)std::floor(L[a] / target));
+    g.edge[a] = L[a] / nd[a];
+    g.boxlen[a] = L[a];
+    g.boxmin[a] = origin[a] - 0.5 * L[a];
+  }
+  g.nx = nd[0]; g.ny = nd[1]; g.nz = nd[2];
+  const long long ncell = (long long)nd[0] * nd[1] * nd[2];
+  if (ncell > (1 << 24)) return fail(c, PMB200_EUNSUPPORTED, "%lld cells", ncell);
+  g.ncell = (int)ncell;
+  g.unit = g.edge[0];
+  // stencil: rows (dy, dz) and their dx span, keeping every cell whose
+  // nearest point can lie within the cutoff of the home cell
+  int R[3];
+  for (int a = 0; a < 3; a++) R[a] = (int)std::ceil(rc / g.edge[a] - 1e-12);
+  c->rows.clear();
+  const double rc2 = rc * rc * (1.0 + 1e-12);
+  for (int dz = -R[2]; dz <= R[2]; dz++)
+    for (int dy = -R[1]; dy <= R[1]; dy++) {
+      const double yz = std::pow(std::max(std::abs(dy) - 1, 0) * g.edge[1], 2) +
+                        std::pow(std::max(std::abs(dz) - 1, 0) * g.edge[2], 2);
+      if (yz > rc2) continue;
+      int lo = 0, hi = 0;
+      for (int dx = 0; dx <= R[0]; dx++)
+        if (yz + std::pow(std::max(dx - 1, 0) * g.edge[0], 2) <= rc2) hi = dx;
+      lo = -hi;
+      c->rows.push_back(Row{dy, dz, lo, hi});
+    }
+  if ((int)c->rows.size() > kMaxRows)
+    return fail(c, PMB200_EUNSUPPORTED, "stencil of %d rows (cell size too small)",
+                (int)c->rows.size());
+  g.nrows = (int)c->rows.size();
+  c->stencil = Stencil{};
+  for (size_t r = 0; r < c->rows.size(); r++) c->stencil.rows[r] = c->rows[r];
+  if (c->ncell_alloc < g.ncell) {
+    CK(dalloc(c->d_count, (size_t)g.ncell));
+    CK(dalloc(c->d_start, (size_t)g.ncell + 1));
+    CK(dalloc(c->d_partial, (size_t)g.ncell * kNacc));
+    c->ncell_alloc = g.ncell;
+  }
+  // constants
+  const pmb200_params &p = c->p;
+  const double u = g.unit;
+  const double rl = p.cutoff_lj / u, ro = p.switchon / u, rq = p.cutoff_coul / u;
+  const double t = rl * rl - ro * ro;
+  MixedConsts &m = c->mc;
+  m.cut2 = (float)((rc / u) * (rc / u));
+  m.rclj2 = (float)(rl * rl);
+  m.ron2 = (float)(ro * ro);
+  m.rcc2 = (float)(rq * rq);
+  m.s1 = (float)(1.0 / (t * t * t));
+  m.s2 = (float)(rl * rl - 3.0 * ro * ro);
+  m.s3 = (float)(4.0 / (t * t * t));
+  m.c15_1 = (float)(1.5 / rq);
+  m.c05_3 = (float)(0.5 / (rq * rq * rq));
+  m.c15_3 = (float)(1.5 / (rq * rq * rq));
+  m.csf = (float)c->csf;
+  m.ey = (float)(g.edge[1] / u);
+  m.ez = (float)(g.edge[2] / u);
+  Fp64Consts &f = c->fc;
+  const double tl = p.cutoff_lj * p.cutoff_lj - p.switchon * p.switchon;
+  f.cut2 = rc * rc;
+  f.rclj2 = p.cutoff_lj * p.cutoff_lj;
+  f.ron2 = p.switchon * p.switchon;
+  f.rcc2 = p.cutoff_coul * p.cutoff_coul;
+  f.s1 = 1.0 / ((tl * tl) * tl);
+  f.s2 = p.cutoff_lj * p.cutoff_lj - 3.0 * p.switchon * p.switchon;
+  f.s3 = 4.0 / ((tl * tl) * tl);
+  f.c15_1 = 1.5 / p.cutoff_coul;
+  f.c05_3 = 0.5 / (p.cutoff_coul * p.cutoff_coul * p.cutoff_coul);
+  f.c15_3 = 1.5 / (p.cutoff_coul * p.cutoff_coul * p.cutoff_coul);
+  f.csf = c->csf;
+  c->have_box = true;
+  if (c->have_topo) return upload_lj(c);
+  return PMB200_OK;
+}
+
+int pmb200_eval_device(pmb200_ctx *c, const double *d_pos, double *d_forces, double *d_out,
+                       unsigned flags, void *stream) {
+  int rc = check_ready(c);
+  if (rc) return rc;
+  if ((flags & PMB200_MOLVIRIAL) && !c->have_mass)
+    return fail(c, PMB200_EINVAL, "molecular virial needs masses");
+  if (c->n > 0 && (!d_pos || !d_forces)) return fail(c, PMB200_EINVAL, "null device buffer");
+  CK(cudaSetDevice(c->p.device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  return launch_eval(c, d_pos, d_forces, d_out, flags, 1, st);
+}
+
+int pmb200_sync(pmb200_ctx *c) {
+  if (!c) return PMB200_EINVAL;
+  CK(cudaSetDevice(c->p.device));
+  CK(cudaStreamSynchronize(c->stream));
+  int e = 0;
+  CK(cudaMemcpy(&e, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (e) {
+    CK(cudaMemset(c->d_err, 0, sizeof(int)));
+    return fail(c, PMB200_EDEVICE, "non-finite atom position in an evaluation");
+  }
+  return PMB200_OK;
+}
+
+int pmb200_eval(pmb200_ctx *c, const double *pos, double *forces, double *energies,
+                double *virial, double *molvirial, unsigned flags) {
+  int rc = check_ready(c);
+  if (rc) return rc;
+  if (c->n > 0 && (!pos || !forces)) return fail(c, PMB200_EINVAL, "null host buffer");
+  if ((flags & PMB200_ENERGY) && !energies) return fail(c, PMB200_EINVAL, "null energies");
+  if ((flags & PMB200_VIRIAL) && !virial) return fail(c, PMB200_EINVAL, "null virial");
+  if ((flags & PMB200_MOLVIRIAL) && !molvirial) return fail(c, PMB200_EINVAL, "null molvirial");
+  if ((flags & PMB200_MOLVIRIAL) && !c->have_mass)
+    return fail(c, PMB200_EINVAL, "molecular virial needs masses");
+  CK(cudaSetDevice(c->p.device));
+  const size_t bytes = sizeof(double) * 3 * (size_t)c->n;
+  cudaStream_t st = c->stream;
+  if (c->n > 0) {
+    CK(cudaMemcpyAsync(c->d_hpos, pos, bytes, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(c->d_hfrc, forces, bytes, cudaMemcpyHostToDevice, st));
+  }
+  rc = launch_eval(c, c->d_hpos, c->d_hfrc, c->d_out, flags, 1, st);
+  if (rc) return rc;
+  double out[20];
+  if (c->n > 0) CK(cudaMemcpyAsync(forces, c->d_hfrc, bytes, cudaMemcpyDeviceToHost, st));
+  if (flags) CK(cudaMemcpyAsync(out, c->d_out, sizeof(out), cudaMemcpyDeviceToHost, st));
+  rc = pmb200_sync(c);
+  if (rc) return rc;
+  if (flags & PMB200_ENERGY) {
+    energies[0] += out[0];
+    energies[1] += out[1];
+  }
+  if (flags & PMB200_VIRIAL)
+    for (int k = 0; k < 9; k++) virial[k] += out[2 + k];
+  if (flags & PMB200_MOLVIRIAL)
+    for (int k = 0; k < 9; k++) molvirial[k] += out[11 + k];
+  return PMB200_OK;
+}
+
+int pmb200_leapfrog_device(pmb200_ctx *c, double *d_pos, double *d_vel, double *d_forces,
+                           double *d_out, double dt_fs, int nsteps, unsigned flags,
+                           void *stream) {
+  int rc = check_ready(c);
+  if (rc) return rc;
+  if (!c->have_mass) return fail(c, PMB200_EINVAL, "leapfrog needs masses");
+  if (nsteps < 1) return PMB200_OK;
+  if (!(dt_fs > 0.0)) return fail(c, PMB200_EINVAL, "time step %g", dt_fs);
+  if (c->n > 0 && (!d_pos || !d_vel || !d_forces))
+    return fail(c, PMB200_EINVAL, "null device buffer");
+  CK(cudaSetDevice(c->p.device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  const double h = dt_fs * 0.02045482828087295;  // Constant::INV_TIMEFACTOR
+  const int n = c->n;
+  const int tb = 256, nb = (3 * n + tb - 1) / tb;
+  // initial forces, then the first (half-kick) step
+  rc = launch_eval(c, d_pos, d_forces, nullptr, 0, 0, st);
+  if (rc) return rc;
+  auto step = [&](double kick, unsigned fl) -> int {
+    if (n > 0)
+      k_kick_drift<<<nb, tb, 0, st>>>(n, d_pos, d_vel, d_forces, c->d_mass, kick * h, h, 1);
+    return launch_eval(c, d_pos, d_forces, d_out, fl, 0, st);
+  };
+  rc = step(0.5, nsteps == 1 ? flags : 0);
+  if (rc) return rc;
+  const int middle = nsteps - 2;  // steps 2..nsteps-1 replay one captured graph
+  if (middle > 0) {
+    const void *key[4] = {d_pos, d_vel, d_forces, (const void *)st};
+    bool same = c->graph_exec && c->graph_dt == dt_fs;
+    for (int k = 0; k < 4 && same; k++) same = c->graph_key[k] == key[k];
+    if (!same) {
+      release_graph(c);
+      CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      rc = step(1.0, 0);
+      cudaGraph_t gr = nullptr;
+      cudaError_t e = cudaStreamEndCapture(st, &gr);
+      if (rc) {
+        if (gr) cudaGraphDestroy(gr);
+        return rc;
+      }
+      if (e != cudaSuccess) return fail(c, PMB200_ECUDA, "capture: %s", cudaGetErrorString(e));
+      c->graph = gr;
+      CK(cudaGraphInstantiate(&c->graph_exec, gr, 0));
+      for (int k = 0; k < 4; k++) c->graph_key[k] = key[k];
+      c->graph_dt = dt_fs;
+    }
+    for (int s = 0; s < middle; s++) CK(cudaGraphLaunch(c->graph_exec, st));
+  }
+  if (nsteps >= 2) {
+    rc = step(1.0, flags);
+    if (rc) return rc;
+  }
+  if (n > 0)
+    k_kick_drift<<<nb, tb, 0, st>>>(n, d_pos, d_vel, d_forces, c->d_mass, 0.5 * h, h, 0);
+  CK(cudaGetLastError());
+  return PMB200_OK;
+}
+
+int pmb200_step_device(pmb200_ctx *c, double *d_pos, double *d_vel, double *d_forces,
+                       double *d_out, double dt_fs, unsigned flags, void *stream) {
+  int rc = check_ready(c);
+  if (rc) return rc;
+  if (!c->have_mass) return fail(c, PMB200_EINVAL, "leapfrog needs masses");
+  if (!(dt_fs > 0.0)) return fail(c, PMB200_EINVAL, "time step %g", dt_fs);
+  if (c->n > 0 && (!d_pos || !d_vel || !d_forces))
+    return fail(c, PMB200_EINVAL, "null device buffer");
+  if (!stream) return fail(c, PMB200_EINVAL, "pmb200_step_device needs an explicit stream");
+  if ((flags & PMB200_MOLVIRIAL)) return fail(c, PMB200_EINVAL, "molecular virial in a step");
+  CK(cudaSetDevice(c->p.device));
+  cudaStream_t st = (cudaStream_t)stream;
+  const void *key[5] = {d_pos, d_vel, d_forces, d_out, stream};
+  bool same = c->sgraph_exec && c->sgraph_dt == dt_fs && c->sgraph_flags == flags &&
+              c->sgraph_timing == c->timing;
+  for (int k = 0; k < 5 && same; k++) same = c->sgraph_key[k] == key[k];
+  if (!same) {
+    if (c->sgraph_exec) cudaGraphExecDestroy(c->sgraph_exec);
+    if (c->sgraph) cudaGraphDestroy(c->sgraph);
+    c->sgraph_exec = nullptr;
+    c->sgraph = nullptr;
+    const double h = dt_fs * 0.02045482828087295;  // Constant::INV_TIMEFACTOR
+    const int n = c->n;
+    const int tb = 256, nb = (3 * n + tb - 1) / tb;
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    if (n > 0)
+      k_kick_drift<<<nb, tb, 0, st>>>(n, d_pos, d_vel, d_forces, c->d_mass, h, h, 1);
+    rc = launch_eval(c, d_pos, d_forces, d_out, flags, 0, st);
+    cudaGraph_t gr = nullptr;
+    cudaError_t e = cudaStreamEndCapture(st, &gr);
+    if (rc) {
+      if (gr) cudaGraphDestroy(gr);
+      return rc;
+    }
+    if (e != cudaSuccess) return fail(c, PMB200_ECUDA, "capture: %s", cudaGetErrorString(e));
+    c->sgraph = gr;
+    CK(cudaGraphInstantiate(&c->sgraph_exec, gr, 0));
+    for (int k = 0; k < 5; k++) c->sgraph_key[k] = key[k];
+    c->sgraph_dt = dt_fs;
+    c->sgraph_flags = flags;
+    c->sgraph_timing = c->timing;
+  }
+  CK(cudaGraphLaunch(c->sgraph_exec, st));
+  return PMB200_OK;
+}
+
+int pmb200_set_kernel_timing(pmb200_ctx *c, int on) {
+  if (!c) return PMB200_EINVAL;
+  c->timing = on ? 1 : 0;
+  return PMB200_OK;
+}
+
+int pmb200_last_kernel_ms(pmb200_ctx *c, float *ms) {
+  if (!c || !ms) return PMB200_EINVAL;
+  CK(cudaSetDevice(c->p.device));
+  CK(cudaEventElapsedTime(ms, c->ev0, c->ev1));
+  return PMB200_OK;
+}
+
+int pmb200_last_pair_count(pmb200_ctx *c, long long *pairs) {
+  if (!c || !pairs) return PMB200_EINVAL;
+  double v = 0.0;
+  CK(cudaSetDevice(c->p.device));
+  CK(cudaMemcpy(&v, c->d_pairs, sizeof(double), cudaMemcpyDeviceToHost));
+  *pairs = (long long)llround(v);
+  return PMB200_OK;
+}
+
+int pmb200_measure_fp32_peak(int device, double *tflops) {
+  pmb200_ctx *c = nullptr;
+  if (!tflops) return PMB200_EINVAL;
+  CK(cudaSetDevice(device));
+  int sms = 0;
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  float *sink = nullptr;
+  CK(cudaMalloc((void **)&sink, sizeof(float) * 1024));
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  const int threads = 512, blocks = sms * 4, iters = 4096;
+  k_fma_peak<<<blocks, threads>>>(64, 1.0f, sink);  // warm-up
+  CK(cudaEventRecord(e0));
+  k_fma_peak<<<blocks, threads>>>(iters, 1.0f, sink);
+  CK(cudaEventRecord(e1));
+  CK(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(sink);
+  const double flops = 2.0 * 8.0 * 16.0 * (double)iters * threads * blocks;
+  *tflops = flops / (ms * 1e-3) / 1e12;
+  return PMB200_OK;
+}
+
+int pmb200_grid(const pmb200_ctx *c, int dims[3], double edge[3]) {
+  if (!c || !dims || !edge) return PMB200_EINVAL;
+  if (!c->have_box) return PMB200_ESTATE;
+  dims[0] = c->g.nx; dims[1] = c->g.ny; dims[2] = c->g.nz;
+  for (int a = 0; a < 3; a++) edge[a] = c->g.edge[a];
+  return PMB200_OK;
+}
+
+}  // extern "C"

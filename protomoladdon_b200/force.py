@@ -1,0 +1,282 @@
+"""Host-side mirror of ProtoMol's SystemForce interface for the B200 force.
+
+``NonbondedCutoffB200SystemForce`` stands where the reference registers
+``NonbondedCutoffSystemForce<CubicCellManager, OneAtomPairTwo<
+PeriodicBoundaryConditions, C2SwitchingFunction, LennardJonesForce,
+C1SwitchingFunction, CoulombForce>>``
+(protomol/src/protomol/module/NonbondedCutoffForceModule.cpp:75-76):
+
+* keyword ``NonbondedCutoffB200`` (the reference's ``NonbondedCutoff`` id is
+  taken by the CPU prototype and duplicate ids throw,
+  protomol/src/protomol/base/Factory.h:50-58);
+* ``make(values)`` takes the reference's parameter list in its order
+  (OneAtomPairTwo::getParameters then NonbondedCutoffForce::getParameters):
+  ``[-switchon, C2 -cutoff, C1 -cutoff, algorithm -cutoff]`` and applies
+  C2SwitchingFunction::make's check 0 <= switchon < cutoff
+  (protomol/src/protomol/switch/C2SwitchingFunction.cpp:30-41);
+* ``evaluate(topo, positions, forces, energies)`` is
+  SystemForce::evaluate (protomol/src/protomol/force/system/SystemForce.h:
+  35-38): forces and energies are accumulated into, the virial is added when
+  ``energies.virial`` is on and the molecular virial when
+  ``energies.molecular_virial`` is on.
+
+Every call goes through libpmb200.so; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes
+import re
+
+import numpy as np
+
+from . import _lib
+from ._lib import PmbError
+
+_P = ctypes.c_void_p
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None else None
+
+
+class ScalarStructure:
+    """Energies and virials with the reference's index layout
+    (protomol/src/protomol/type/ScalarStructure.h:26-67)."""
+    COULOMB, LENNARDJONES = 0, 1
+    VIRIALXX = 7
+    MOLVIRIALXX = 16
+    LAST = 36
+
+    def __init__(self, virial=False, molecular_virial=False):
+        self.table = np.zeros(self.LAST)
+        self.virial = virial
+        self.molecular_virial = molecular_virial
+
+    def clear(self):
+        self.table[:] = 0.0
+
+    def __getitem__(self, k):
+        return self.table[k]
+
+    def __setitem__(self, k, v):
+        self.table[k] = v
+
+    def virial_matrix(self):
+        return self.table[self.VIRIALXX:self.VIRIALXX + 9].reshape(3, 3)
+
+    def molvirial_matrix(self):
+        return self.table[self.MOLVIRIALXX:self.MOLVIRIALXX + 9].reshape(3, 3)
+
+
+class PeriodicTopology:
+    """The parts of Topology<PeriodicBoundaryConditions, CubicCellManager> the
+    force reads, as flat arrays (see pmb200_set_topology / pmb200_set_box)."""
+
+    def __init__(self, type, qscaled, mol, lj, excl, box, origin=(0.0, 0.0, 0.0),
+                 mass=None, coulomb_scaling=1.0, cellsize=0.0):
+        self.type = np.ascontiguousarray(type, dtype=np.int32)
+        self.qscaled = np.ascontiguousarray(qscaled, dtype=np.float64)
+        self.mol = np.ascontiguousarray(mol, dtype=np.int32)
+        self.mass = None if mass is None else np.ascontiguousarray(mass, dtype=np.float64)
+        lj = np.asarray(lj, dtype=np.float64)
+        self.ntypes = int(round((lj.size // 4) ** 0.5))
+        self.lj = np.ascontiguousarray(lj.reshape(-1))
+        self.excl = np.ascontiguousarray(np.asarray(excl, dtype=np.int32).reshape(-1, 3))
+        box = np.asarray(box, dtype=np.float64)
+        if box.shape == (3,):
+            box = np.diag(box)
+        self.e = np.ascontiguousarray(box.reshape(3, 3))
+        self.origin = np.ascontiguousarray(origin, dtype=np.float64)
+        self.coulomb_scaling = float(coulomb_scaling)
+        self.cellsize = float(cellsize)
+        self.version = 0
+
+    @property
+    def n(self):
+        return self.type.size
+
+    @classmethod
+    def from_dict(cls, d):
+        return cls(d["type"], d["qscaled"], d["mol"], d["lj"], d["excl"], d["box"],
+                   d.get("origin", (0.0, 0.0, 0.0)), d.get("mass"),
+                   d.get("coulomb_scaling", 1.0), d.get("cellsize_gpu", 0.0))
+
+
+_ID_RE = re.compile(r"-(\w+)\s+([^\s-][^\s]*)")
+
+
+class NonbondedCutoffB200SystemForce:
+    keyword = "NonbondedCutoffB200"
+
+    def __init__(self, switchon, cutoff_lj, cutoff_coul, cutoff_alg, precision="mixed",
+                 device=0, cellsize=0.0):
+        if not (switchon >= 0.0 and cutoff_lj > 0.0 and switchon < cutoff_lj):
+            raise ValueError(
+                f"C2 switching function: 0 <= switchon (={switchon}) < cutoff (={cutoff_lj}).")
+        self.switchon = float(switchon)
+        self.cutoff_lj = float(cutoff_lj)
+        self.cutoff_coul = float(cutoff_coul)
+        self.cutoff_alg = float(cutoff_alg)
+        self.precision = precision
+        self.device = int(device)
+        self.cellsize = float(cellsize)
+        self._ctx = None
+        self._topo_key = None
+        self._box_key = None
+
+    # ---- Makeable -------------------------------------------------------
+    @classmethod
+    def make(cls, values, **kw):
+        """values in the reference's order: switchon, C2 cutoff, C1 cutoff,
+        algorithm cutoff."""
+        if len(values) != 4:
+            raise ValueError(f"{cls.keyword} takes 4 parameters, got {len(values)}")
+        return cls(*[float(v) for v in values], **kw)
+
+    @classmethod
+    def from_id(cls, force_id, **kw):
+        """Parses a config force line such as
+        ``LennardJones Coulomb -algorithm NonbondedCutoffB200
+        -switchingFunction C2 -switchingFunction C1 -switchon 9 -cutoff 10
+        -cutoff 10 -cutoff 10``."""
+        toks = force_id.split()
+        if toks[:2] != ["LennardJones", "Coulomb"]:
+            raise ValueError("expected 'LennardJones Coulomb' potentials")
+        opts = list(zip(toks[2::2], toks[3::2])) if len(toks) % 2 == 0 else None
+        if opts is None:
+            raise ValueError(f"cannot parse force id {force_id!r}")
+        alg = [v for k, v in opts if k == "-algorithm"]
+        if alg != [cls.keyword]:
+            raise ValueError(f"algorithm must be {cls.keyword}")
+        sw = [v for k, v in opts if k == "-switchingFunction"]
+        if sw != ["C2", "C1"]:
+            raise ValueError("switching functions must be C2 (LennardJones) then C1 (Coulomb)")
+        ron = [float(v) for k, v in opts if k == "-switchon"]
+        cut = [float(v) for k, v in opts if k == "-cutoff"]
+        if len(ron) != 1 or len(cut) != 3:
+            raise ValueError("need -switchon and three -cutoff values")
+        return cls(ron[0], cut[0], cut[1], cut[2], **kw)
+
+    def get_id(self):
+        return (f"LennardJones Coulomb -algorithm {self.keyword} -switchingFunction C2 "
+                f"-switchingFunction C1 -switchon {self.switchon:g} -cutoff {self.cutoff_lj:g} "
+                f"-cutoff {self.cutoff_coul:g} -cutoff {self.cutoff_alg:g}")
+
+    # ---- context --------------------------------------------------------
+    def _check(self, rc):
+        if rc != _lib.PMB200_OK:
+            msg = _lib.lib().pmb200_last_error(self._ctx) if self._ctx else b""
+            raise PmbError(rc, (msg or b"").decode())
+
+    def _ensure(self, topo: PeriodicTopology):
+        L = _lib.lib()
+        if self._ctx is None:
+            p = _lib.Params(_lib.PMB200_MIXED if self.precision == "mixed" else _lib.PMB200_FP64,
+                            self.device, self.switchon, self.cutoff_lj, self.cutoff_coul,
+                            self.cutoff_alg, self.cellsize or topo.cellsize)
+            h = _P()
+            rc = L.pmb200_create(ctypes.byref(p), ctypes.byref(h))
+            if rc != _lib.PMB200_OK:
+                raise PmbError(rc, "pmb200_create rejected the parameters")
+            self._ctx = h
+        key = (id(topo), topo.version)
+        if self._topo_key != key:
+            ex = topo.excl.reshape(-1)
+            self._check(L.pmb200_set_topology(
+                self._ctx, topo.n, _ptr(topo.type), _ptr(topo.qscaled), _ptr(topo.mol),
+                _ptr(topo.mass), topo.ntypes, _ptr(topo.lj), topo.excl.shape[0],
+                _ptr(ex) if ex.size else None, topo.coulomb_scaling))
+            self._topo_key = key
+            self._box_key = None
+        bkey = (topo.e.tobytes(), topo.origin.tobytes())
+        if self._box_key != bkey:
+            self._check(L.pmb200_set_box(self._ctx, _ptr(topo.e[0].copy()), _ptr(topo.e[1].copy()),
+                                         _ptr(topo.e[2].copy()), _ptr(topo.origin)))
+            self._box_key = bkey
+
+    def uncache(self):
+        self._topo_key = None
+        self._box_key = None
+
+    # ---- SystemForce ----------------------------------------------------
+    def evaluate(self, topo: PeriodicTopology, positions, forces, energies: ScalarStructure):
+        """Accumulates forces (n,3 float64, C-contiguous, modified in place)
+        and energies like SystemForce::evaluate."""
+        self._ensure(topo)
+        pos = np.ascontiguousarray(positions, dtype=np.float64)
+        if not (isinstance(forces, np.ndarray) and forces.dtype == np.float64
+                and forces.flags.c_contiguous):
+            raise TypeError("forces must be a C-contiguous float64 numpy array")
+        flags = _lib.PMB200_ENERGY
+        vir = np.zeros(9)
+        mvir = np.zeros(9)
+        if energies.virial:
+            flags |= _lib.PMB200_VIRIAL
+        if energies.molecular_virial:
+            flags |= _lib.PMB200_MOLVIRIAL
+        e = np.zeros(2)
+        self._check(_lib.lib().pmb200_eval(self._ctx, _ptr(pos), _ptr(forces), _ptr(e), _ptr(vir),
+                                           _ptr(mvir), flags))
+        energies[ScalarStructure.COULOMB] += e[0]
+        energies[ScalarStructure.LENNARDJONES] += e[1]
+        if energies.virial:
+            energies.table[ScalarStructure.VIRIALXX:ScalarStructure.VIRIALXX + 9] += vir
+        if energies.molecular_virial:
+            energies.table[ScalarStructure.MOLVIRIALXX:ScalarStructure.MOLVIRIALXX + 9] += mvir
+
+    def evaluate_device(self, topo, pos_ptr, force_ptr, out_ptr=None, flags=0, stream=None):
+        """Device-resident evaluation on raw device pointers (ints), e.g.
+        ``tensor.data_ptr()``; forces are accumulated, out (20 doubles) is
+        overwritten.  Asynchronous: call sync()."""
+        self._ensure(topo)
+        self._check(_lib.lib().pmb200_eval_device(
+            self._ctx, _P(pos_ptr), _P(force_ptr), _P(out_ptr) if out_ptr else None,
+            int(flags), _P(stream) if stream else None))
+
+    def leapfrog_device(self, topo, pos_ptr, vel_ptr, force_ptr, dt_fs, nsteps, out_ptr=None,
+                        flags=0, stream=None):
+        self._ensure(topo)
+        self._check(_lib.lib().pmb200_leapfrog_device(
+            self._ctx, _P(pos_ptr), _P(vel_ptr), _P(force_ptr), _P(out_ptr) if out_ptr else None,
+            float(dt_fs), int(nsteps), int(flags), _P(stream) if stream else None))
+
+    def step_device(self, topo, pos_ptr, vel_ptr, force_ptr, dt_fs, stream, out_ptr=None,
+                    flags=0):
+        """One leapfrog iteration (kick + drift, new forces) as a graph replay."""
+        self._ensure(topo)
+        self._check(_lib.lib().pmb200_step_device(
+            self._ctx, _P(pos_ptr), _P(vel_ptr), _P(force_ptr), _P(out_ptr) if out_ptr else None,
+            float(dt_fs), int(flags), _P(stream)))
+
+    def set_kernel_timing(self, on):
+        self._check(_lib.lib().pmb200_set_kernel_timing(self._ctx, 1 if on else 0))
+
+    def last_kernel_ms(self):
+        v = ctypes.c_float()
+        self._check(_lib.lib().pmb200_last_kernel_ms(self._ctx, ctypes.byref(v)))
+        return float(v.value)
+
+    def sync(self):
+        self._check(_lib.lib().pmb200_sync(self._ctx))
+
+    def last_pair_count(self):
+        v = ctypes.c_longlong()
+        self._check(_lib.lib().pmb200_last_pair_count(self._ctx, ctypes.byref(v)))
+        return v.value
+
+    def grid(self):
+        d = (ctypes.c_int * 3)()
+        e = (ctypes.c_double * 3)()
+        self._check(_lib.lib().pmb200_grid(self._ctx, d, e))
+        return tuple(d), tuple(e)
+
+    def close(self):
+        if self._ctx is not None:
+            _lib.lib().pmb200_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

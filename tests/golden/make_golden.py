@@ -1,0 +1,95 @@
+"""Generates the committed golden fixtures from the reference itself.
+
+Run in a tree where the reference sources are available and
+``make -C oracle ref`` has built oracle/_ref/libpmref.so:
+
+    python tests/golden/make_golden.py /root/reference
+
+Fixtures (all inputs and outputs FP64):
+
+* water423.npz -- the reference's periodic water test system
+  (test/tests/data/water_423.{psf,pdb} + par_all27_prot_lipid.inp), read by
+  the reference's own PSF/PAR/PDB readers and topology builder, with the t=0
+  LENNARDJONES and COULOMB energies of its golden
+  test/tests/expected/water_CHARMM_PERIODIC_L.energy (columns 10-11), and the
+  reference's combined LJ(C2, switchon 0.1, cutoff 6.5) + Coulomb(C1, 6.5)
+  forces, energies, atomic and molecular virial on those positions.
+* water648_ref.npz -- the seeded 216-water box (protomoladdon_b200.water.
+  small_648, seed 1234): reference forces, energies, virials, plus 20 FP64
+  leapfrog steps at 1 fs through the reference force.
+* modified_ref.npz -- the same box with every intramolecular O-H pair made
+  EXCLUSION_MODIFIED (1-4 style) and coulombScalingFactor 0.5, exercising
+  A14/B14 and the Coulomb scaling branch.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle import oracle as O  # noqa: E402
+from protomoladdon_b200 import water  # noqa: E402
+
+
+def golden_energy_row(path):
+    with open(path) as fh:
+        cols = fh.readline().split()
+    return float(cols[9]), float(cols[10])  # E_VdW (LJ), E_coulomb
+
+
+def sysd_arrays(s):
+    keys = ("pos", "type", "qscaled", "mol", "mass", "lj", "excl", "box", "origin")
+    out = {k: np.asarray(s[k]) for k in keys}
+    for k in ("coulomb_scaling", "cellsize", "ron", "rc_lj", "rc_coul", "rc_alg"):
+        out[k] = np.float64(s[k])
+    return out
+
+
+def main(ref_root):
+    data = os.path.join(ref_root, "test", "tests", "data")
+    exp = os.path.join(ref_root, "test", "tests", "expected", "water_CHARMM_PERIODIC_L.energy")
+    s = O.ref_load_psf(os.path.join(data, "water_423.psf"),
+                       os.path.join(data, "par_all27_prot_lipid.inp"),
+                       os.path.join(data, "water_423.pos.pdb"), exclude="scaled1-4")
+    # conf: cellBasisVector 28 A cube at origin 0, cellsize 6.5, LJ C2
+    # (switchon 0.1, cutoff 6.5), Coulomb C1 (cutoff 6.5)
+    s.update(box=np.array([28.0, 28.0, 28.0]), origin=np.zeros(3), cellsize=6.5, ron=0.1,
+             rc_lj=6.5, rc_coul=6.5, rc_alg=6.5, coulomb_scaling=1.0)
+    R = O.RefForce(s)
+    f, e, v, mv = R.evaluate(s["pos"], 2)
+    elj, ecoul = golden_energy_row(exp)
+    np.savez_compressed(os.path.join(HERE, "water423.npz"), **sysd_arrays(s),
+                        golden_elj=elj, golden_ecoul=ecoul, ref_forces=f, ref_energies=e,
+                        ref_virial=v, ref_molvirial=mv)
+    R.close()
+
+    w = water.small_648()
+    R = O.RefForce(w)
+    f, e, v, mv = R.evaluate(w["pos"], 2)
+    p20, v20, e20 = R.leapfrog(w["pos"], w["vel"], 1.0, 20)
+    np.savez_compressed(os.path.join(HERE, "water648_ref.npz"), **sysd_arrays(w),
+                        vel=w["vel"], ref_forces=f, ref_energies=e, ref_virial=v,
+                        ref_molvirial=mv, lf20_pos=p20, lf20_vel=v20, lf20_energies=e20)
+    R.close()
+
+    m = dict(w)
+    ex = m["excl"].copy()
+    oh = m["type"][ex[:, 0]] == water.T_O  # the two O-H pairs of each water; H-H stays full
+    ex[oh, 2] = 1
+    m["excl"] = ex
+    m["coulomb_scaling"] = 0.5
+    R = O.RefForce(m)
+    f, e, v, mv = R.evaluate(m["pos"], 2)
+    np.savez_compressed(os.path.join(HERE, "modified_ref.npz"), **sysd_arrays(m),
+                        ref_forces=f, ref_energies=e, ref_virial=v, ref_molvirial=mv)
+    R.close()
+    print("wrote fixtures to", HERE)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

@@ -1,0 +1,92 @@
+"""Host logic without a GPU: parameter parsing/validation, the water
+generator, the C-ABI library's exported symbols and its argument checks."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from protomoladdon_b200 import _lib, water
+from protomoladdon_b200.force import NonbondedCutoffB200SystemForce, PeriodicTopology
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_symbols():
+    txt = open(os.path.join(ROOT, "include", "pmb200.h")).read()
+    return sorted(set(re.findall(r"\b(pmb200_[a-z_0-9]+)\s*\(", txt)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = _lib.lib()
+    syms = header_symbols()
+    assert set(syms) == set(_lib.EXPORTED)
+    for s in syms:
+        assert getattr(L, s) is not None
+
+
+def test_create_validates_before_touching_a_device():
+    L = _lib.lib()
+    h = ctypes.c_void_p()
+    bad = [
+        _lib.Params(0, 0, 10.0, 9.0, 9.0, 9.0, 0.0),   # switchon >= cutoff (C2 make)
+        _lib.Params(0, 0, -1.0, 9.0, 9.0, 9.0, 0.0),   # negative switchon
+        _lib.Params(7, 0, 8.0, 9.0, 9.0, 9.0, 0.0),    # unknown precision
+        _lib.Params(0, 0, 8.0, 9.0, 0.0, 9.0, 0.0),    # zero Coulomb cutoff
+    ]
+    for p in bad:
+        assert L.pmb200_create(ctypes.byref(p), ctypes.byref(h)) == _lib.PMB200_EINVAL
+    p = _lib.Params(0, 0, 8.0, 9.0, 9.0, 8.5, 0.0)     # algorithm cutoff below switch
+    assert L.pmb200_create(ctypes.byref(p), ctypes.byref(h)) == _lib.PMB200_EUNSUPPORTED
+    assert L.pmb200_create(None, ctypes.byref(h)) == _lib.PMB200_EINVAL
+    assert L.pmb200_destroy(None) == 0
+
+
+def test_force_id_parse_and_make():
+    f = NonbondedCutoffB200SystemForce.from_id(
+        "LennardJones Coulomb -algorithm NonbondedCutoffB200 -switchingFunction C2 "
+        "-switchingFunction C1 -switchon 9 -cutoff 10 -cutoff 10 -cutoff 10")
+    assert (f.switchon, f.cutoff_lj, f.cutoff_coul, f.cutoff_alg) == (9, 10, 10, 10)
+    assert NonbondedCutoffB200SystemForce.from_id(f.get_id()).get_id() == f.get_id()
+    with pytest.raises(ValueError):
+        NonbondedCutoffB200SystemForce.make([10, 10, 10, 10])  # switchon == cutoff
+    with pytest.raises(ValueError):
+        NonbondedCutoffB200SystemForce.from_id(
+            "LennardJones Coulomb -algorithm NonbondedCutoff -switchingFunction C2 "
+            "-switchingFunction C1 -switchon 9 -cutoff 10 -cutoff 10 -cutoff 10")
+    with pytest.raises(ValueError):
+        NonbondedCutoffB200SystemForce.make([1, 2, 3])
+
+
+@pytest.mark.parametrize("k,n", [(6, 648), (24, 41472)])
+def test_water_box_recipe(k, n):
+    s = water.water_box(k, rc=10.0, ron=9.0)
+    assert s["n"] == n and s["pos"].shape == (n, 3)
+    assert np.isclose(s["box"][0], k * water.LATTICE)
+    q = s["qscaled"].reshape(-1, 3).sum(1)
+    assert np.abs(q).max() < 1e-12  # neutral molecules
+    d = s["pos"].reshape(-1, 3, 3)
+    oh = np.linalg.norm(d[:, 1] - d[:, 0], axis=1)
+    assert np.allclose(oh, water.R_OH)
+    ang = np.degrees(np.arccos(np.einsum("ij,ij->i", d[:, 1] - d[:, 0], d[:, 2] - d[:, 0])
+                               / water.R_OH ** 2))
+    assert np.allclose(ang, 104.52)
+    assert s["excl"].shape == (3 * n // 3, 3)
+    s2 = water.water_box(k, rc=10.0, ron=9.0)
+    assert np.array_equal(s["pos"], s2["pos"])  # seeded
+
+
+def test_ion_box_and_batch():
+    s = water.water_box(10, rc=9.0, ron=8.0, ion_fraction=0.02)
+    nion = int(np.isin(s["type"], [water.T_NA, water.T_CL]).sum())
+    assert nion == 2 * round(0.02 * 1000 / 2)
+    assert abs(s["qscaled"].sum()) < 1e-9
+    boxes = water.batch_boxes(count=16)
+    for b in boxes:
+        assert 300 - 3 <= b["n"] <= 6000 + 3 and b["box"][0] >= 18.0 - 1e-12
+
+
+def test_topology_wrapper(water648):
+    t = PeriodicTopology.from_dict(water648)
+    assert t.n == 648 and t.ntypes == 2 and t.e.shape == (3, 3)

@@ -1,0 +1,101 @@
+"""The CPU oracle (oracle/pm_oracle.c) against the reference's golden vectors
+and, where it was built, against the reference compiled from its sources."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from protomoladdon_b200 import water
+
+
+def test_golden_water423_energies(water423):
+    """t = 0 energies of test/tests/expected/water_CHARMM_PERIODIC_L.energy
+    (printed to 8 significant digits)."""
+    f, e, v, mv = O.restate_eval(water423, water423["pos"], virial_mode=2)
+    assert abs(e[1] - water423["golden_elj"]) <= 5e-5
+    assert abs(e[0] - water423["golden_ecoul"]) <= 5e-5
+
+
+@pytest.mark.parametrize("fx", ["water423", "water648", "modified648"])
+def test_restatement_bitexact_vs_reference_fixture(fx, request):
+    d = request.getfixturevalue(fx)
+    f, e, v, mv = O.restate_eval(d, d["pos"], virial_mode=2)
+    assert np.array_equal(f, d["ref_forces"])
+    assert np.array_equal(e, d["ref_energies"])
+    assert np.array_equal(v, d["ref_virial"])
+    assert np.array_equal(mv, d["ref_molvirial"])
+
+
+def test_restatement_leapfrog_bitexact(water648):
+    p, v, e = O.restate_leapfrog(water648, water648["pos"], water648["vel"], 1.0, 20)
+    assert np.array_equal(p, water648["lf20_pos"])
+    assert np.array_equal(v, water648["lf20_vel"])
+    assert np.array_equal(e, water648["lf20_energies"])
+
+
+def test_cell_walk_equals_all_pairs(water648):
+    f, e, v, _ = O.restate_eval(water648, water648["pos"], virial_mode=1)
+    fb, eb, vb, _ = O.restate_eval(water648, water648["pos"], virial_mode=1, brute=True)
+    assert np.abs(f - fb).max() < 1e-11
+    assert np.allclose(e, eb, rtol=1e-12, atol=1e-9)
+    assert np.allclose(v, vb, rtol=1e-12, atol=1e-9)
+
+
+def test_newton_third_law(water648):
+    f, _, _, _ = O.restate_eval(water648, water648["pos"], virial_mode=0)
+    assert np.abs(f.sum(0)).max() < 1e-9
+
+
+def test_forces_accumulate(water648):
+    pos = water648["pos"]
+    f1, _, _, _ = O.restate_eval(water648, pos, 0)
+    import ctypes  # noqa: F401
+    # accumulate semantics: a second evaluation into the same buffer doubles
+    lib = O.restate_lib()
+    ar = O._Arrays(water648)
+    st = O._pmo_struct(water648, ar)
+    p = np.ascontiguousarray(pos).reshape(-1)
+    F = f1.reshape(-1).copy()
+    E = np.zeros(2)
+    assert lib.pmo_eval(ctypes.byref(st), O._ptr(p), O._ptr(F), O._ptr(E), None, None, 0, 0) == 0
+    assert np.allclose(F.reshape(-1, 3), 2 * f1, rtol=0, atol=1e-12)
+
+
+def test_translation_invariance_unwrapped(water648):
+    """Positions are not wrapped by the caller; whole-box translations leave
+    forces unchanged up to rounding."""
+    L = water648["box"]
+    shift = np.array([3 * L[0], -2 * L[1], 7 * L[2]])
+    f0, e0, _, _ = O.restate_eval(water648, water648["pos"], 0)
+    f1, e1, _, _ = O.restate_eval(water648, water648["pos"] + shift, 0)
+    assert np.abs(f0 - f1).max() < 1e-8
+    assert np.allclose(e0, e1, rtol=1e-10)
+
+
+def test_empty_and_single_atom():
+    s = water.small_648()
+    for n in (0, 1):
+        d = dict(s)
+        for k in ("type", "qscaled", "mol", "mass"):
+            d[k] = s[k][:n]
+        d["excl"] = np.zeros((0, 3), np.int32)
+        f, e, v, _ = O.restate_eval(d, s["pos"][:n], virial_mode=1)
+        assert f.shape == (n, 3) and not f.any() and not e.any()
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference oracle library not built")
+@pytest.mark.parametrize("seed", [1, 7])
+def test_restatement_bitexact_vs_compiled_reference(seed):
+    s = water.water_box(5, rc=7.0, ron=6.0, seed=seed)
+    s["cellsize"] = 3.1
+    R = O.RefForce(s)
+    f, e, v, mv = R.evaluate(s["pos"], 2)
+    g, ee, vv, mm = O.restate_eval(s, s["pos"], 2)
+    R.close()
+    assert np.array_equal(f, g) and np.array_equal(e, ee)
+    assert np.array_equal(v, vv) and np.array_equal(mv, mm)
+
+
+def test_pair_count_small(water648):
+    n = O.restate_count_pairs(water648, water648["pos"])
+    # ~0.5 * rho * 4/3 pi rc^3 per atom for the 648-atom box at rc 8
+    assert 60_000 < n < 80_000

@@ -1,0 +1,208 @@
+"""GPU parity: libpmb200 (through its C ABI) against the reference's own
+outputs (committed fixtures) and the CPU oracle on the same inputs.
+
+Tolerances (written here, checked below):
+* FP64 kernel: forces RMS relative <= 1e-12, energies/virial relative
+  <= 1e-11 -- only the summation order differs from the reference.
+* mixed kernel: forces RMS relative <= 1e-5;
+  energies: relative <= 1e-6 on the 41,472-atom box; on the small boxes,
+  whose lattice-start Coulomb energy cancels to ~1e-4 of the summed pair
+  magnitudes, |dE| <= 1e-6 * sum over pairs |E_pair| (bounded here by
+  2e-3 kcal/mol); virial relative <= 1e-5.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from protomoladdon_b200 import _lib, water
+from protomoladdon_b200.force import (NonbondedCutoffB200SystemForce, PeriodicTopology,
+                                      ScalarStructure)
+from protomoladdon_b200._lib import PmbError
+
+pytestmark = pytest.mark.gpu
+
+
+def rms_rel(a, b):
+    return float(np.sqrt(((a - b) ** 2).sum() / (b ** 2).sum()))
+
+
+def run(d, precision, virial=True, molvir=True, pos=None, F0=None):
+    topo = PeriodicTopology.from_dict(d)
+    f = NonbondedCutoffB200SystemForce(d["ron"], d["rc_lj"], d["rc_coul"], d["rc_alg"],
+                                       precision=precision)
+    F = np.zeros_like(d["pos"]) if F0 is None else F0.copy()
+    E = ScalarStructure(virial=virial, molecular_virial=molvir)
+    f.evaluate(topo, d["pos"] if pos is None else pos, F, E)
+    pairs = f.last_pair_count()
+    f.close()
+    return F, E, pairs
+
+
+@pytest.mark.parametrize("fx", ["water423", "water648", "modified648"])
+def test_fp64_matches_reference(fx, request):
+    d = request.getfixturevalue(fx)
+    F, E, _ = run(d, "fp64")
+    assert rms_rel(F, d["ref_forces"]) <= 1e-12
+    e = d["ref_energies"]
+    assert abs(E[0] - e[0]) <= 1e-11 * abs(e[0])
+    assert abs(E[1] - e[1]) <= 1e-11 * abs(e[1])
+    assert np.allclose(E.virial_matrix().ravel(), d["ref_virial"], rtol=1e-11, atol=1e-9)
+    assert np.allclose(E.molvirial_matrix().ravel(), d["ref_molvirial"], rtol=1e-11, atol=1e-9)
+
+
+@pytest.mark.parametrize("fx", ["water423", "water648", "modified648"])
+def test_mixed_matches_reference(fx, request):
+    d = request.getfixturevalue(fx)
+    F, E, _ = run(d, "mixed")
+    assert rms_rel(F, d["ref_forces"]) <= 1e-5
+    e = d["ref_energies"]
+    assert abs(E[0] - e[0]) <= 2e-3
+    assert abs(E[1] - e[1]) <= 2e-3
+    v = d["ref_virial"]
+    assert np.abs(E.virial_matrix().ravel() - v).max() <= 1e-5 * np.abs(v).max()
+    mv = d["ref_molvirial"]
+    assert np.abs(E.molvirial_matrix().ravel() - mv).max() <= 1e-5 * np.abs(v).max()
+
+
+def test_golden_energies_through_gpu(water423):
+    """The reference's t = 0 golden energies (8 significant digits)."""
+    for prec in ("fp64", "mixed"):
+        _, E, _ = run(water423, prec, virial=False, molvir=False)
+        assert abs(E[1] - water423["golden_elj"]) <= 5e-4
+        assert abs(E[0] - water423["golden_ecoul"]) <= 5e-4
+
+
+@pytest.fixture(scope="module")
+def medium():
+    s = water.medium_41k()
+    f, e, v, mv = O.restate_eval(s, s["pos"], virial_mode=1)
+    s.update(ref_forces=f, ref_energies=e, ref_virial=v)
+    s["ref_pairs"] = O.restate_count_pairs(s, s["pos"])
+    return s
+
+
+def test_medium_41k_mixed(medium):
+    F, E, pairs = run(medium, "mixed", molvir=False)
+    assert rms_rel(F, medium["ref_forces"]) <= 1e-5
+    e = medium["ref_energies"]
+    assert abs(E[0] - e[0]) <= 1e-6 * abs(e[0])
+    assert abs(E[1] - e[1]) <= 1e-6 * abs(e[1])
+    v = medium["ref_virial"]
+    assert np.abs(E.virial_matrix().ravel() - v).max() <= 1e-5 * np.abs(v).max()
+    assert abs(pairs - medium["ref_pairs"]) <= 1e-6 * medium["ref_pairs"]
+
+
+def test_medium_41k_fp64(medium):
+    F, E, pairs = run(medium, "fp64", molvir=False)
+    assert rms_rel(F, medium["ref_forces"]) <= 1e-12
+    e = medium["ref_energies"]
+    assert np.allclose([E[0], E[1]], e, rtol=1e-11)
+    assert pairs == medium["ref_pairs"]
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_deterministic_and_accumulates(water648, precision):
+    F1, E1, _ = run(water648, precision)
+    F2, E2, _ = run(water648, precision)
+    assert np.array_equal(F1, F2) and np.array_equal(E1.table, E2.table)
+    F3, _, _ = run(water648, precision, F0=F1)
+    assert np.allclose(F3, 2 * F1, rtol=1e-15, atol=1e-12)
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_unwrapped_and_translated_positions(water648, precision):
+    L = water648["box"]
+    shift = np.array([5 * L[0], -3 * L[1], 2 * L[2]])
+    F0, E0, _ = run(water648, precision)
+    F1, E1, _ = run(water648, precision, pos=water648["pos"] + shift)
+    tol = 1e-10 if precision == "fp64" else 1e-5
+    assert rms_rel(F1, F0) <= tol
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_ions_four_types(precision):
+    s = water.water_box(12, rc=12.0, ron=11.0, ion_fraction=0.04, seed=5)
+    f, e, v, _ = O.restate_eval(s, s["pos"], virial_mode=1)
+    F, E, _ = run(s, precision, molvir=False)
+    tol = 1e-12 if precision == "fp64" else 1e-5
+    assert rms_rel(F, f) <= tol
+    assert abs(E[1] - e[1]) <= (1e-11 if precision == "fp64" else 1e-5) * abs(e[1])
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_non_cubic_box(precision):
+    s = water.water_box(8, rc=9.0, ron=8.0, seed=3)
+    s["box"] = s["box"] * np.array([1.0, 1.13, 0.97])
+    s["pos"] = s["pos"] * np.array([1.0, 1.13, 0.97])
+    s["origin"] = 0.5 * s["box"]
+    f, e, v, _ = O.restate_eval(s, s["pos"], virial_mode=1)
+    F, E, _ = run(s, precision, molvir=False)
+    tol = 1e-12 if precision == "fp64" else 1e-5
+    assert rms_rel(F, f) <= tol
+
+
+def test_errors_are_reported(water648):
+    d = dict(water648)
+    pos = d["pos"].copy()
+    pos[5, 1] = np.nan
+    with pytest.raises(PmbError) as ei:
+        run(d, "mixed", pos=pos)
+    assert ei.value.code == _lib.PMB200_EDEVICE
+    small = dict(water648)
+    small["box"] = np.array([15.0, 15.0, 15.0])  # < 2 * cutoff 8
+    with pytest.raises(PmbError) as ei:
+        run(small, "fp64")
+    assert ei.value.code == _lib.PMB200_EUNSUPPORTED
+
+
+def test_empty_system(water648):
+    d = dict(water648)
+    for k in ("type", "qscaled", "mol", "mass"):
+        d[k] = water648[k][:0]
+    d["pos"] = water648["pos"][:0]
+    d["excl"] = np.zeros((0, 3), np.int32)
+    F, E, pairs = run(d, "mixed")
+    assert F.shape == (0, 3) and E[0] == 0.0 and E[1] == 0.0 and pairs == 0
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-9), ("mixed", 2e-5)])
+def test_leapfrog_device_vs_reference(water648, precision, tol):
+    import torch
+    d = water648
+    topo = PeriodicTopology.from_dict(d)
+    f = NonbondedCutoffB200SystemForce(d["ron"], d["rc_lj"], d["rc_coul"], d["rc_alg"],
+                                       precision=precision)
+    dev = torch.device("cuda:0")
+    pos = torch.tensor(d["pos"], dtype=torch.float64, device=dev).contiguous()
+    vel = torch.tensor(d["vel"], dtype=torch.float64, device=dev).contiguous()
+    frc = torch.zeros_like(pos)
+    out = torch.zeros(20, dtype=torch.float64, device=dev)
+    f.leapfrog_device(topo, pos.data_ptr(), vel.data_ptr(), frc.data_ptr(), 1.0, 20,
+                      out.data_ptr(), _lib.PMB200_ENERGY)
+    f.sync()
+    p = pos.cpu().numpy()
+    v = vel.cpu().numpy()
+    f.close()
+    assert np.abs(p - d["lf20_pos"]).max() <= tol * 10
+    assert rms_rel(v, d["lf20_vel"]) <= tol * 10
+    e = out.cpu().numpy()[:2]
+    assert np.allclose(e, d["lf20_energies"], rtol=0, atol=5e-3)
+
+
+def test_device_path_equals_host_path(water648):
+    import torch
+    d = water648
+    topo = PeriodicTopology.from_dict(d)
+    f = NonbondedCutoffB200SystemForce(d["ron"], d["rc_lj"], d["rc_coul"], d["rc_alg"])
+    F, E, _ = run(d, "mixed", molvir=False)
+    pos = torch.tensor(d["pos"], dtype=torch.float64, device="cuda:0")
+    frc = torch.zeros_like(pos)
+    out = torch.zeros(20, dtype=torch.float64, device="cuda:0")
+    f.evaluate_device(topo, pos.data_ptr(), frc.data_ptr(), out.data_ptr(),
+                      _lib.PMB200_ENERGY | _lib.PMB200_VIRIAL)
+    f.sync()
+    f.close()
+    assert np.array_equal(frc.cpu().numpy(), F)
+    o = out.cpu().numpy()
+    assert o[0] == E[0] and o[1] == E[1]
+    assert np.array_equal(o[2:11], E.virial_matrix().ravel())
