@@ -1,9 +1,10 @@
 #!/usr/bin/env python
 """Benchmark: ns/day of full leapfrog steps on the 41,472-atom water box.
 
-A step is one LeapfrogIntegrator iteration (kick + drift, then the periodic
-cutoff LJ(C2) + Coulomb(C1) force with its cell-list rebuild) at dt = 1 fs on
-13,824 TIP3P-geometry waters (24^3 lattice, box 74.496 A, rc 10, C2 from 9).
+A step is one LeapfrogIntegrator iteration (kick + drift with the waters held
+rigid by SETTLE, then the periodic cutoff LJ(C2) + Coulomb(C1) force with its
+cell-list rebuild) at dt = 1 fs on 13,824 rigid TIP3P-geometry waters (24^3
+lattice, box 74.496 A, rc 10, C2 from 9).
 
 Default arm (libpmb200 on B200):
   value  -- device-resident steps (positions/velocities/forces in HBM, one
@@ -48,7 +49,8 @@ sys.path.insert(0, ROOT)
 DT_FS = 1.0
 FLOPS_PER_PAIR = 81          # algorithmic flops per unique in-cutoff pair
 BYTES_PER_ATOM = 84          # algorithmic HBM bytes per atom per evaluation
-KERNELS_PER_STEP = 6         # kick_drift, cell_index, scan, scatter, rank_gather, pair
+KERNELS_PER_STEP = 7         # kick_drift_settle, cell_index, scan, scatter, rank_gather,
+                             # pair, finalize
 WORKLOAD = ("water box: 41,472 atoms (13,824 TIP3P-geometry waters, 24^3 lattice, "
             "box 74.496 A), LJ C2 switch 9-10 A + Coulomb C1 cutoff 10 A, leapfrog 1 fs")
 METRIC = "ns/day & Gpairs/s, 41k-atom water box: mixed vs FP64 on B200 @<=1e-5 force err"
@@ -207,13 +209,16 @@ def run_ours(args):
 
     s = water.medium_41k(seed=1234 + rank)
     n = s["n"]
+    widx = water.rigid_waters(s)
     topo = PeriodicTopology.from_dict(s)
     stream = torch.cuda.Stream(device=dev)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > L2
 
     def make(prec):
-        return NonbondedCutoffB200SystemForce(s["ron"], s["rc_lj"], s["rc_coul"], s["rc_alg"],
-                                              precision=prec, device=local)
+        f = NonbondedCutoffB200SystemForce(s["ron"], s["rc_lj"], s["rc_coul"], s["rc_alg"],
+                                           precision=prec, device=local)
+        f.set_rigid_waters(topo, widx, water.D_OH, water.D_HH)
+        return f
 
     def device_run(force):
         """W warm-up + K timed device-resident steps; returns per-step ms list,
@@ -228,7 +233,6 @@ def run_ours(args):
         stream.synchronize()
         force.sync()
         pairs = force.last_pair_count()
-        force.set_kernel_timing(True)
         sp = stream.cuda_stream
         for _ in range(args.warmup):
             force.step_device(topo, pos.data_ptr(), vel.data_ptr(), frc.data_ptr(), DT_FS, sp)
@@ -245,14 +249,22 @@ def run_ours(args):
                 e0[k].record(stream)
             force.step_device(topo, pos.data_ptr(), vel.data_ptr(), frc.data_ptr(), DT_FS, sp)
             e1[k].record(stream)
-            e1[k].synchronize()
-            kms.append(force.last_kernel_ms())
         torch.cuda.synchronize(dev)
         if dist is not None:
             dist.barrier()
         force.sync()
-        force.set_kernel_timing(False)
         step_ms = [a.elapsed_time(b) for a, b in zip(e0, e1)]
+        # the dominant kernel alone: CUDA events around each directly
+        # launched pair kernel on its stream, L2 flushed before each
+        force.set_kernel_timing(True)
+        for k in range(min(args.steps, 50)):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            force.evaluate_device(topo, pos.data_ptr(), frc.data_ptr(), None, 0, sp)
+            stream.synchronize()
+            kms.append(force.last_kernel_ms())
+        force.set_kernel_timing(False)
+        force.sync()
         return step_ms, kms, pairs
 
     # accuracy of the mixed force vs the FP64 CPU oracle at the start positions
@@ -280,32 +292,33 @@ def run_ours(args):
         f64.close()
         fp64 = (sum(s64), statistics.mean(k64))
 
-    # end to end through the host-buffer C-ABI call, host kick/drift
-    h = DT_FS * 0.02045482828087295
+    # end to end through the host-buffer C-ABI call (SystemForce::evaluate's
+    # replacement): the host integrator does kick + drift + SETTLE, as
+    # ProtoMol's leapfrog with a constraint modifier does, and calls the force
+    from protomoladdon_b200 import rigid
     xh = s["pos"].copy()
     vh = s["vel"].copy()
-    m = s["mass"][:, None]
     F = np.zeros_like(xh)
     E = ScalarStructure()
     fmix.evaluate(topo, xh, F, E)
     e2e_steps = min(args.steps, 100)
     e2e_t = []
-    for _ in range(min(args.warmup, 3)):
-        vh += F * h / m
-        xh += vh * h
+
+    def host_step():
+        rigid.host_kick_drift(xh, vh, F, s["mass"], DT_FS, widx, water.D_OH, water.D_HH)
         F[:] = 0.0
+        E.clear()
         fmix.evaluate(topo, xh, F, E)
+
+    for _ in range(min(args.warmup, 3)):
+        host_step()
     if dist is not None:
         dist.barrier()
     for _ in range(e2e_steps):
         flush.zero_()
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
-        vh += F * h / m
-        xh += vh * h
-        F[:] = 0.0
-        E.clear()
-        fmix.evaluate(topo, xh, F, E)
+        host_step()
         e2e_t.append(time.perf_counter() - t0)
     fmix.close()
 

@@ -150,9 +150,21 @@ int pmb200_step_device(pmb200_ctx *ctx, double *d_pos, double *d_vel,
                        double *d_forces, double *d_out, double dt_fs,
                        unsigned flags, void *stream);
 
-/* When on, CUDA events bracket every pair-kernel launch (graph replays
- * included); pmb200_last_kernel_ms returns the duration of the last one
- * (valid after the work has completed). */
+/* Rigid 3-site waters for the device integrator (pmb200_leapfrog_device,
+ * pmb200_step_device): after each kick + drift the listed waters are put
+ * back on their O-H (d_oh) and H-H (d_hh) lengths by SETTLE and their
+ * velocities become (x_new - x_old) / h, the effect of ProtoMol's SHAKE
+ * position modifier on a water (protomol/src/protomol/modifier/
+ * ModifierShake.cpp, run by LeapfrogIntegrator's postDriftOrNextModify).
+ * widx[3*nwater] = {O, H1, H2} per water; all waters must share the first
+ * one's masses.  nwater = 0 turns the constraints off. */
+int pmb200_set_rigid_waters(pmb200_ctx *ctx, int nwater, const int *widx,
+                            double d_oh, double d_hh);
+
+/* When on, CUDA events bracket every directly launched pair kernel
+ * (pmb200_eval, pmb200_eval_device; not graph replays);
+ * pmb200_last_kernel_ms returns the duration of the last one (valid after
+ * the work has completed). */
 int pmb200_set_kernel_timing(pmb200_ctx *ctx, int on);
 int pmb200_last_kernel_ms(pmb200_ctx *ctx, float *ms);
 
@@ -160,6 +172,18 @@ int pmb200_last_kernel_ms(pmb200_ctx *ctx, float *ms);
  * Gpairs/s unit counts; fully excluded pairs are not counted).  Requires a
  * pmb200_sync() after the evaluation. */
 int pmb200_last_pair_count(pmb200_ctx *ctx, long long *pairs);
+
+/* Host-side integrator helper for callers that keep the state on the host
+ * and call pmb200_eval per step (a ProtoMol integrator driving this force):
+ * one LeapfrogIntegrator::doKickdoDrift (v += F kick h / m, x += v h,
+ * protomol/src/protomol/integrator/leapfrog/LeapfrogIntegrator.cpp:72-85)
+ * followed, for the listed rigid waters, by SETTLE and v = (x_new - x_old)/h
+ * (the role of ProtoMol's SHAKE modifier).  kick is 1 for a full kick, 0.5
+ * for the first half kick.  Runs on the calling thread; no GPU. */
+int pmb200_host_kick_drift(int n, double *pos, double *vel,
+                           const double *forces, const double *mass,
+                           double dt_fs, double kick, int nwater,
+                           const int *widx, double d_oh, double d_hh);
 
 /* Measurement helper (no counterpart in the reference): FP32 FMA throughput
  * of `device` in TFLOP/s (2 flops per FMA), from a 148-SM-filling chain of

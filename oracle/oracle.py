@@ -64,6 +64,11 @@ def restate_lib():
         lib.pmo_count_pairs.restype = ctypes.c_longlong
         lib.pmo_leapfrog.argtypes = [ctypes.POINTER(_PmoSystem), _P, _P, _P, _D, _I, _P]
         lib.pmo_leapfrog.restype = _I
+        lib.pmo_settle.argtypes = [_I, _P, _P, _D, _D, _P, _P]
+        lib.pmo_settle.restype = None
+        lib.pmo_leapfrog_rigid.argtypes = [ctypes.POINTER(_PmoSystem), _P, _P, _P, _D, _I, _I,
+                                           _P, _D, _D, _P]
+        lib.pmo_leapfrog_rigid.restype = _I
         _restate = lib
     return _restate
 
@@ -161,6 +166,33 @@ def restate_leapfrog(sysd, pos, vel, dt_fs, nsteps):
                           int(nsteps), _ptr(e))
     if rc:
         raise RuntimeError(f"pmo_leapfrog failed: {rc}")
+    return p.reshape(-1, 3), v.reshape(-1, 3), e
+
+
+def restate_settle(widx, mass, doh, dhh, old_pos, new_pos):
+    """SETTLE of the listed waters; returns the constrained positions."""
+    lib = restate_lib()
+    w = np.ascontiguousarray(widx, dtype=np.int32).reshape(-1)
+    m = np.ascontiguousarray(mass, dtype=np.float64)
+    o = np.ascontiguousarray(old_pos, dtype=np.float64).reshape(-1)
+    out = np.ascontiguousarray(new_pos, dtype=np.float64).reshape(-1).copy()
+    lib.pmo_settle(w.size // 3, _ptr(w), _ptr(m), float(doh), float(dhh), _ptr(o), _ptr(out))
+    return out.reshape(-1, 3)
+
+
+def restate_leapfrog_rigid(sysd, pos, vel, dt_fs, nsteps, widx, doh, dhh):
+    lib = restate_lib()
+    ar = _Arrays(sysd)
+    st = _pmo_struct(sysd, ar)
+    p = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1).copy()
+    v = np.ascontiguousarray(vel, dtype=np.float64).reshape(-1).copy()
+    w = np.ascontiguousarray(widx, dtype=np.int32).reshape(-1)
+    e = np.zeros(2)
+    rc = lib.pmo_leapfrog_rigid(ctypes.byref(st), _ptr(p), _ptr(v), _ptr(ar.mass), float(dt_fs),
+                                int(nsteps), w.size // 3, _ptr(w), float(doh), float(dhh),
+                                _ptr(e))
+    if rc:
+        raise RuntimeError(f"pmo_leapfrog_rigid failed: {rc}")
     return p.reshape(-1, 3), v.reshape(-1, 3), e
 
 

@@ -581,3 +581,118 @@ int pmo_leapfrog(const pmo_system *s, double *pos, double *vel,
   free(f);
   return rc;
 }
+
+/* ---------------------------------------------------------------------- */
+/* SETTLE for one water: canonical triangle O (0, ra, 0), H1 (-rc, -rb, 0),
+ * H2 (rc, -rb, 0) about the centre of mass; the new orientation is found in
+ * the frame whose z axis is normal to the old molecular plane. */
+static void cross3(const double a[3], const double b[3], double o[3]) {
+  o[0] = a[1] * b[2] - a[2] * b[1];
+  o[1] = a[2] * b[0] - a[0] * b[2];
+  o[2] = a[0] * b[1] - a[1] * b[0];
+}
+static double dot3(const double a[3], const double b[3]) {
+  return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+}
+static void unit3(double a[3]) {
+  double r = sqrt(dot3(a, a));
+  a[0] /= r; a[1] /= r; a[2] /= r;
+}
+
+static void settle_one(double mo, double mh, double doh, double dhh,
+                       const double *A0, const double *B0, const double *C0,
+                       double *A1, double *B1, double *C1) {
+  const double M = mo + 2.0 * mh;
+  const double rc = 0.5 * dhh;
+  const double t = sqrt(doh * doh - rc * rc);
+  const double ra = 2.0 * mh * t / M, rb = t - ra;
+  double com[3], a1[3], b1[3], c1[3], b0[3], c0[3], ex[3], ey[3], ez[3];
+  int k;
+  for (k = 0; k < 3; k++) {
+    com[k] = (mo * A1[k] + mh * B1[k] + mh * C1[k]) / M;
+    a1[k] = A1[k] - com[k];
+    b1[k] = B1[k] - com[k];
+    c1[k] = C1[k] - com[k];
+    b0[k] = B0[k] - A0[k];
+    c0[k] = C0[k] - A0[k];
+  }
+  cross3(b0, c0, ez);
+  cross3(a1, ez, ex);
+  cross3(ez, ex, ey);
+  unit3(ex); unit3(ey); unit3(ez);
+  {
+    const double xb0 = dot3(ex, b0), yb0 = dot3(ey, b0);
+    const double xc0 = dot3(ex, c0), yc0 = dot3(ey, c0);
+    const double za1 = dot3(ez, a1);
+    const double xb1 = dot3(ex, b1), yb1 = dot3(ey, b1), zb1 = dot3(ez, b1);
+    const double xc1 = dot3(ex, c1), yc1 = dot3(ey, c1), zc1 = dot3(ez, c1);
+    const double sphi = za1 / ra, cphi = sqrt(1.0 - sphi * sphi);
+    const double spsi = (zb1 - zc1) / (2.0 * rc * cphi), cpsi = sqrt(1.0 - spsi * spsi);
+    const double ya2 = ra * cphi, xb2 = -rc * cpsi;
+    const double t1 = -rb * cphi, t2 = rc * spsi * sphi;
+    const double yb2 = t1 - t2, yc2 = t1 + t2;
+    /* rotation in the plane that conserves the old orientation's momentum */
+    const double al = xb2 * (xb0 - xc0) + yb0 * yb2 + yc0 * yc2;
+    const double be = xb2 * (yc0 - yb0) + xb0 * yb2 + xc0 * yc2;
+    const double ga = xb0 * yb1 - xb1 * yb0 + xc0 * yc1 - xc1 * yc0;
+    const double ab = al * al + be * be;
+    const double sth = (al * ga - be * sqrt(ab - ga * ga)) / ab, cth = sqrt(1.0 - sth * sth);
+    const double xa3 = -ya2 * sth, ya3 = ya2 * cth, za3 = za1;
+    const double xb3 = xb2 * cth - yb2 * sth, yb3 = xb2 * sth + yb2 * cth, zb3 = zb1;
+    const double xc3 = -xb2 * cth - yc2 * sth, yc3 = -xb2 * sth + yc2 * cth, zc3 = zc1;
+    for (k = 0; k < 3; k++) {
+      A1[k] = com[k] + xa3 * ex[k] + ya3 * ey[k] + za3 * ez[k];
+      B1[k] = com[k] + xb3 * ex[k] + yb3 * ey[k] + zb3 * ez[k];
+      C1[k] = com[k] + xc3 * ex[k] + yc3 * ey[k] + zc3 * ez[k];
+    }
+  }
+}
+
+void pmo_settle(int nwater, const int *widx, const double *mass, double doh,
+                double dhh, const double *old_pos, double *new_pos) {
+  int w;
+  if (nwater <= 0) return;
+  for (w = 0; w < nwater; w++) {
+    const int a = widx[3 * w], b = widx[3 * w + 1], c = widx[3 * w + 2];
+    settle_one(mass[widx[0]], mass[widx[1]], doh, dhh, old_pos + 3 * a, old_pos + 3 * b,
+               old_pos + 3 * c, new_pos + 3 * a, new_pos + 3 * b, new_pos + 3 * c);
+  }
+}
+
+int pmo_leapfrog_rigid(const pmo_system *s, double *pos, double *vel,
+                       const double *mass, double dt_fs, int nsteps, int nwater,
+                       const int *widx, double doh, double dhh,
+                       double *energies) {
+  const double h = dt_fs * PMO_INV_TIMEFACTOR;
+  const int n = s->n;
+  double *f = (double *)calloc((size_t)3 * (size_t)(n > 0 ? n : 1), sizeof(double));
+  double *old = (double *)malloc(sizeof(double) * (size_t)3 * (size_t)(n > 0 ? n : 1));
+  double e[2] = {0.0, 0.0};
+  int step, i, k, rc;
+  if (!f || !old) { free(f); free(old); return PMO_ENOMEM; }
+  rc = pmo_eval(s, pos, f, e, NULL, NULL, 0, 0);
+  for (step = 0; step < nsteps && !rc; step++) {
+    double kick = step == 0 ? 0.5 * h : h;
+    for (i = 0; i < 3 * n; i++) old[i] = pos[i];
+    for (i = 0; i < n; i++)
+      for (k = 0; k < 3; k++) vel[3 * i + k] += f[3 * i + k] * kick / mass[i];
+    for (i = 0; i < 3 * n; i++) pos[i] += vel[i] * h;
+    pmo_settle(nwater, widx, mass, doh, dhh, old, pos);
+    for (i = 0; i < nwater; i++)
+      for (k = 0; k < 3; k++) {
+        const int a = widx[3 * i + k];
+        vel[3 * a] = (pos[3 * a] - old[3 * a]) / h;
+        vel[3 * a + 1] = (pos[3 * a + 1] - old[3 * a + 1]) / h;
+        vel[3 * a + 2] = (pos[3 * a + 2] - old[3 * a + 2]) / h;
+      }
+    for (i = 0; i < 3 * n; i++) f[i] = 0.0;
+    e[0] = e[1] = 0.0;
+    rc = pmo_eval(s, pos, f, e, NULL, NULL, 0, 0);
+  }
+  for (i = 0; i < n; i++)
+    for (k = 0; k < 3; k++) vel[3 * i + k] += f[3 * i + k] * 0.5 * h / mass[i];
+  if (energies) { energies[0] = e[0]; energies[1] = e[1]; }
+  free(f);
+  free(old);
+  return rc;
+}

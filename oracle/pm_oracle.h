@@ -68,6 +68,25 @@ int pmo_leapfrog(const pmo_system *s, double *pos, double *vel,
                  const double *mass, double dt_fs, int nsteps,
                  double *energies);
 
+/* SETTLE (Miyamoto & Kollman, J. Comput. Chem. 13, 952 (1992)): analytic
+ * constraint of rigid 3-site waters.  widx[3*w] = {O, H1, H2}; every water
+ * uses the masses of the first one.  new_pos (3n) holds unconstrained
+ * positions on entry and constrained ones on return; old_pos satisfies the
+ * constraints.  Not part of the reference (which constrains water with
+ * iterative SHAKE, protomol/src/protomol/modifier/ModifierShake.cpp); the
+ * tests check it against a converged SHAKE. */
+void pmo_settle(int nwater, const int *widx, const double *mass, double doh,
+                double dhh, const double *old_pos, double *new_pos);
+
+/* pmo_leapfrog with rigid waters: after each kick + drift the listed waters
+ * are put back on their constraints by SETTLE and their velocities become
+ * (x_new - x_old) / h, as a position-constraint modifier does in ProtoMol's
+ * leapfrog (postDriftOrNextModify).  The closing half kick is unconstrained. */
+int pmo_leapfrog_rigid(const pmo_system *s, double *pos, double *vel,
+                       const double *mass, double dt_fs, int nsteps, int nwater,
+                       const int *widx, double doh, double dhh,
+                       double *energies);
+
 #ifdef __cplusplus
 }
 #endif

@@ -33,7 +33,7 @@ EXPORTED = (
     "pmb200_set_box", "pmb200_eval", "pmb200_eval_device", "pmb200_sync",
     "pmb200_leapfrog_device", "pmb200_last_pair_count", "pmb200_grid",
     "pmb200_step_device", "pmb200_set_kernel_timing", "pmb200_last_kernel_ms",
-    "pmb200_measure_fp32_peak",
+    "pmb200_measure_fp32_peak", "pmb200_set_rigid_waters", "pmb200_host_kick_drift",
 )
 
 _P = ctypes.c_void_p
@@ -81,6 +81,8 @@ def lib():
     L.pmb200_set_kernel_timing.argtypes = [_P, _I]
     L.pmb200_last_kernel_ms.argtypes = [_P, ctypes.POINTER(ctypes.c_float)]
     L.pmb200_measure_fp32_peak.argtypes = [_I, ctypes.POINTER(_D)]
+    L.pmb200_set_rigid_waters.argtypes = [_P, _I, _P, _D, _D]
+    L.pmb200_host_kick_drift.argtypes = [_I, _P, _P, _P, _P, _D, _D, _I, _P, _D, _D]
     for name in EXPORTED:
         getattr(L, name).restype = getattr(L, name).restype or _I
     L.pmb200_last_error.restype = ctypes.c_char_p

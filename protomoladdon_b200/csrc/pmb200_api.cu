@@ -42,8 +42,10 @@ struct pmb200_ctx {
   GridParams g{};
   MixedConsts mc{};
   Fp64Consts fc{};
+  PbcRef pb{};
   std::vector<Row> rows;
-  Stencil stencil{};
+  Stencil stencil{};       // full shell (FP64 kernel)
+  HalfStencil half{};      // half shell by cell (mixed kernel, Newton's third law)
   int ncell_alloc = 0;
   int *d_count = nullptr, *d_start = nullptr, *d_err = nullptr;
   double *d_partial = nullptr;
@@ -53,10 +55,17 @@ struct pmb200_ctx {
   float4 *d_rel32 = nullptr, *d_spos32 = nullptr;
   double4 *d_rel64 = nullptr, *d_spos64 = nullptr;
   int2 *d_smeta = nullptr;
-  double *d_finter = nullptr, *d_com = nullptr, *d_mvpart = nullptr;
-  double *d_pairs = nullptr, *d_out = nullptr;
-  // host-buffer evaluation scratch
+  unsigned long long *d_facc = nullptr;
+  double *d_com = nullptr;
+  double *d_pairs = nullptr, *d_out = nullptr, *d_red = nullptr;
+  // rigid waters (SETTLE) for the device integrator
+  int nwater = 0, nfree = 0;
+  int *d_widx = nullptr, *d_fidx = nullptr;
+  SettleParams sp{};
+  // host-buffer evaluation scratch: device copies and pinned staging
   double *d_hpos = nullptr, *d_hfrc = nullptr;
+  double *h_pin_pos = nullptr, *h_pin_frc = nullptr, *h_pin_out = nullptr;
+  int n_pin = 0;
   // leapfrog graph
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
@@ -68,15 +77,12 @@ struct pmb200_ctx {
   const void *sgraph_key[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   double sgraph_dt = 0.0;
   unsigned sgraph_flags = 0;
-  int sgraph_timing = -1;
   // pair-kernel timing
   int timing = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 
 namespace {
-
-constexpr int kMolvirBlocks = 64;
 
 int fail(pmb200_ctx *c, int code, const char *fmt, ...) {
   char buf[512];
@@ -156,7 +162,7 @@ int ensure_atom_buffers(pmb200_ctx *c) {
   CK(dalloc(c->d_rel64, n));
   CK(dalloc(c->d_spos64, n));
   CK(dalloc(c->d_smeta, n));
-  CK(dalloc(c->d_finter, 3 * n));
+  CK(dalloc(c->d_facc, 3 * n));
   CK(dalloc(c->d_hpos, 3 * n));
   CK(dalloc(c->d_hfrc, 3 * n));
   c->n_alloc = c->n;
@@ -192,50 +198,72 @@ int launch_eval(pmb200_ctx *c, const double *d_pos, double *d_forces, double *d_
       g.ncell, c->d_start, c->d_tmp, mixed ? c->d_rel32 : nullptr,
       mixed ? nullptr : c->d_rel64, c->d_type, c->d_mol, c->d_sidx,
       mixed ? c->d_spos32 : nullptr, mixed ? nullptr : c->d_spos64, c->d_smeta);
-  double *finter = molvir ? c->d_finter : nullptr;
-  if (c->timing) CK(cudaEventRecord(c->ev0, st));
+  if (molvir && c->nmol > 0)
+    k_com<<<(c->nmol + 127) / 128, 128, 0, st>>>(c->nmol, c->d_mstart, c->d_matoms, c->d_mass,
+                                                  d_pos, c->d_com);
+  // pair-kernel timing events are recorded on direct launches only (not
+  // inside a stream capture)
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  CK(cudaStreamIsCapturing(st, &cap));
+  const bool timed = c->timing && cap == cudaStreamCaptureStatusNone;
+  if (timed) CK(cudaEventRecord(c->ev0, st));
   if (mixed) {
     const double fscale = 1.0 / g.unit;
-#define PMB_MIXED_LAUNCH(E, V)                                                            \
-  k_pair_mixed<E, V><<<blocks, 128, 0, st>>>(g, c->mc, c->stencil, c->ntypes, c->d_lj32, c->d_start, \
-                                             c->d_spos32, c->d_smeta, c->d_sidx,          \
-                                             c->d_ex_start, c->d_ex, d_forces, accumulate, \
-                                             fscale, c->d_partial, finter)
-    if (energy && virial) PMB_MIXED_LAUNCH(true, true);
-    else if (energy) PMB_MIXED_LAUNCH(true, false);
-    else if (virial) PMB_MIXED_LAUNCH(false, true);
-    else PMB_MIXED_LAUNCH(false, false);
+#define PMB_MIXED_LAUNCH(E, V, M)                                                          \
+  k_pair_mixed<E, V, M><<<g.ncell, 32 * kWarps, 0, st>>>(                                    \
+      g, c->mc, c->half, c->ntypes, c->d_lj32, c->d_start, c->d_spos32, c->d_smeta,           \
+      c->d_sidx, c->d_ex_start, c->d_ex, c->d_facc, n, c->d_err, c->d_partial, c->pb, c->d_com)
+    if (n > 0) CK(cudaMemsetAsync(c->d_facc, 0, sizeof(unsigned long long) * 3 * (size_t)n, st));
+    if (molvir) PMB_MIXED_LAUNCH(true, true, true);
+    else if (energy && virial) PMB_MIXED_LAUNCH(true, true, false);
+    else if (energy) PMB_MIXED_LAUNCH(true, false, false);
+    else if (virial) PMB_MIXED_LAUNCH(false, true, false);
+    else PMB_MIXED_LAUNCH(false, false, false);
+    if (n > 0)
+      k_finalize<<<(n + 255) / 256, 256, 0, st>>>(n, c->d_facc, c->d_sidx, fscale * kFixInv,
+                                                  accumulate, d_forces);
 #undef PMB_MIXED_LAUNCH
   } else {
-#define PMB_FP64_LAUNCH(E, V)                                                            \
-  k_pair_fp64<E, V><<<blocks, 128, 0, st>>>(g, c->fc, c->stencil, c->ntypes, c->d_lj64, c->d_start, \
-                                            c->d_spos64, c->d_smeta, c->d_sidx,          \
-                                            c->d_ex_start, c->d_ex, d_forces, accumulate, \
-                                            c->d_partial, finter)
-    if (energy && virial) PMB_FP64_LAUNCH(true, true);
-    else if (energy) PMB_FP64_LAUNCH(true, false);
-    else if (virial) PMB_FP64_LAUNCH(false, true);
-    else PMB_FP64_LAUNCH(false, false);
+#define PMB_FP64_LAUNCH(E, V, M)                                                         \
+  k_pair_fp64<E, V, M><<<blocks, 128, 0, st>>>(g, c->fc, c->stencil, c->ntypes, c->d_lj64,  \
+                                               c->d_start, c->d_spos64, c->d_smeta,          \
+                                               c->d_sidx, c->d_ex_start, c->d_ex, d_forces,  \
+                                               accumulate, c->d_partial, c->pb, c->d_com)
+    if (molvir) PMB_FP64_LAUNCH(true, true, true);
+    else if (energy && virial) PMB_FP64_LAUNCH(true, true, false);
+    else if (energy) PMB_FP64_LAUNCH(true, false, false);
+    else if (virial) PMB_FP64_LAUNCH(false, true, false);
+    else PMB_FP64_LAUNCH(false, false, false);
 #undef PMB_FP64_LAUNCH
   }
   CK(cudaGetLastError());
-  if (c->timing) CK(cudaEventRecord(c->ev1, st));
+  if (timed) CK(cudaEventRecord(c->ev1, st));
   if (energy || virial) {
-    int nmv = 0;
-    if (molvir) {
-      k_com<<<(c->nmol + 127) / 128, 128, 0, st>>>(c->nmol, c->d_mstart, c->d_matoms,
-                                                    c->d_mass, d_pos, c->d_com);
-      k_molvir<<<kMolvirBlocks, 256, 0, st>>>(n, c->d_mol, d_pos, c->d_com, c->d_finter,
-                                              c->d_mvpart);
-      nmv = kMolvirBlocks;
-    }
     const double rcc = c->p.cutoff_coul / g.unit;
-    k_reduce<<<1, 256, 0, st>>>(g.ncell, c->d_partial, mixed ? 1 : 0, 1.5 / rcc,
-                                0.5 / (rcc * rcc * rcc), nmv, c->d_mvpart,
-                                d_out ? d_out : c->d_out, c->d_pairs);
+    k_reduce1<<<kRedBlocks, 256, 0, st>>>(g.ncell, c->d_partial, c->d_red);
+    // the mixed kernel visits each pair once, the FP64 kernel twice
+    k_reduce2<<<1, 32, 0, st>>>(kRedBlocks, c->d_red, mixed ? 1 : 0, mixed ? 1.0 : 0.5,
+                                1.5 / rcc, 0.5 / (rcc * rcc * rcc), d_out ? d_out : c->d_out,
+                                c->d_pairs);
     CK(cudaGetLastError());
   }
   return PMB200_OK;
+}
+
+// The integrator's kick + drift: plain, or with SETTLE on the rigid waters.
+void launch_kick_drift(pmb200_ctx *c, double *d_pos, double *d_vel, const double *d_forces,
+                       double kick, double h, cudaStream_t st) {
+  const int n = c->n;
+  if (n <= 0) return;
+  if (c->nwater > 0) {
+    const int units = c->nwater + c->nfree;
+    k_kick_drift_settle<<<(units + 127) / 128, 128, 0, st>>>(
+        c->nwater, c->d_widx, c->nfree, c->d_fidx, d_pos, d_vel, d_forces, c->d_mass, kick, h,
+        c->sp);
+  } else {
+    k_kick_drift<<<(3 * n + 255) / 256, 256, 0, st>>>(n, d_pos, d_vel, d_forces, c->d_mass,
+                                                      kick, h, 1);
+  }
 }
 
 int check_ready(pmb200_ctx *c) {
@@ -270,7 +298,7 @@ int pmb200_create(const pmb200_params *params, pmb200_ctx **out) {
   if (e == cudaSuccess) e = cudaMemset(c->d_err, 0, sizeof(int));
   if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_out, sizeof(double) * 20);
   if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_pairs, sizeof(double));
-  if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_mvpart, sizeof(double) * 9 * kMolvirBlocks);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_red, sizeof(double) * kRedBlocks * ACC_MV);
   if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
   if (e != cudaSuccess) {
@@ -292,8 +320,11 @@ int pmb200_destroy(pmb200_ctx *c) {
   dfree(c->d_count); dfree(c->d_start); dfree(c->d_err); dfree(c->d_partial);
   dfree(c->d_cell_of); dfree(c->d_slot); dfree(c->d_tmp); dfree(c->d_sidx);
   dfree(c->d_rel32); dfree(c->d_spos32); dfree(c->d_rel64); dfree(c->d_spos64);
-  dfree(c->d_smeta); dfree(c->d_finter); dfree(c->d_com); dfree(c->d_mvpart);
-  dfree(c->d_pairs); dfree(c->d_out); dfree(c->d_hpos); dfree(c->d_hfrc);
+  dfree(c->d_smeta); dfree(c->d_com); dfree(c->d_facc);
+  dfree(c->d_pairs); dfree(c->d_out); dfree(c->d_red); dfree(c->d_widx); dfree(c->d_fidx);
+  if (c->h_pin_pos) cudaFreeHost(c->h_pin_pos);
+  if (c->h_pin_frc) cudaFreeHost(c->h_pin_frc);
+  if (c->h_pin_out) cudaFreeHost(c->h_pin_out); dfree(c->d_hpos); dfree(c->d_hfrc);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -360,6 +391,7 @@ int pmb200_set_topology(pmb200_ctx *c, int n, const int *type, const double *q_s
     for (int i = 0; i < n; i++) matoms[fill[molecule[i]]++] = i;
   }
   release_graph(c);
+  c->nwater = c->nfree = 0;  // rigid waters refer to the old atom list
   c->n = n;
   c->ntypes = ntypes;
   c->nmol = nmol;
@@ -453,6 +485,20 @@ int pmb200_set_box(pmb200_ctx *c, const double e1[3], const double e2[3], const 
   g.nrows = (int)c->rows.size();
   c->stencil = Stencil{};
   for (size_t r = 0; r < c->rows.size(); r++) c->stencil.rows[r] = c->rows[r];
+  // half shell by cell: offsets with dz > 0, or dz == 0 and dy > 0, or
+  // dz == dy == 0 and dx >= 0 (dx == 0 is the home cell, pairs i < j)
+  c->half = HalfStencil{};
+  for (const Row &rw : c->rows)
+    for (int dx = rw.dxlo; dx <= rw.dxhi; dx++) {
+      const bool keep = rw.dz > 0 || (rw.dz == 0 && rw.dy > 0) ||
+                        (rw.dz == 0 && rw.dy == 0 && dx >= 0);
+      if (!keep) continue;
+      if (c->half.ncells >= kMaxHalfCells || std::abs(dx) > 8 || std::abs(rw.dy) > 8 ||
+          std::abs(rw.dz) > 8)
+        return fail(c, PMB200_EUNSUPPORTED, "neighbour stencil too large (cell size too small)");
+      c->half.off[c->half.ncells++] =
+          (unsigned short)((dx + 8) | ((rw.dy + 8) << 5) | ((rw.dz + 8) << 10));
+    }
   if (c->ncell_alloc < g.ncell) {
     CK(dalloc(c->d_count, (size_t)g.ncell));
     CK(dalloc(c->d_start, (size_t)g.ncell + 1));
@@ -491,6 +537,20 @@ int pmb200_set_box(pmb200_ctx *c, const double e1[3], const double e2[3], const 
   f.c05_3 = 0.5 / (p.cutoff_coul * p.cutoff_coul * p.cutoff_coul);
   f.c15_3 = 1.5 / (p.cutoff_coul * p.cutoff_coul * p.cutoff_coul);
   f.csf = c->csf;
+  // PeriodicBoundaryConditions::set, orthogonal case (min/max corners,
+  // myH, myH2, reciprocal basis, myD), for the molecule-centre image
+  PbcRef &b = c->pb;
+  for (int a = 0; a < 3; a++) {
+    const double lo = origin[a] - L[a] * 0.5, hi = origin[a] + L[a] * 0.5;
+    b.e[a] = L[a];
+    b.h[a] = std::max(lo, hi) - std::min(lo, hi);
+    b.h2[a] = b.h[a] * 0.5;
+  }
+  b.er[0] = (L[1] * L[2]) / (L[0] * (L[1] * L[2]));
+  b.er[1] = (L[2] * L[0]) / (L[1] * (L[2] * L[0]));
+  b.er[2] = (L[0] * L[1]) / (L[2] * (L[0] * L[1]));
+  b.d = std::min((L[0] * 0.5) * (L[0] * 0.5),
+                 std::min((L[1] * 0.5) * (L[1] * 0.5), (L[2] * 0.5) * (L[2] * 0.5)));
   c->have_box = true;
   if (c->have_topo) return upload_lj(c);
   return PMB200_OK;
@@ -516,7 +576,9 @@ int pmb200_sync(pmb200_ctx *c) {
   CK(cudaMemcpy(&e, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
   if (e) {
     CK(cudaMemset(c->d_err, 0, sizeof(int)));
-    return fail(c, PMB200_EDEVICE, "non-finite atom position in an evaluation");
+    if (e & 1) return fail(c, PMB200_EDEVICE, "non-finite atom position in an evaluation");
+    return fail(c, PMB200_EDEVICE,
+                "a pair force exceeded the mixed kernel's fixed-point range (atoms overlap)");
   }
   return PMB200_OK;
 }
@@ -532,19 +594,34 @@ int pmb200_eval(pmb200_ctx *c, const double *pos, double *forces, double *energi
   if ((flags & PMB200_MOLVIRIAL) && !c->have_mass)
     return fail(c, PMB200_EINVAL, "molecular virial needs masses");
   CK(cudaSetDevice(c->p.device));
-  const size_t bytes = sizeof(double) * 3 * (size_t)c->n;
+  const size_t cnt = 3 * (size_t)c->n;
+  const size_t bytes = sizeof(double) * cnt;
   cudaStream_t st = c->stream;
-  if (c->n > 0) {
-    CK(cudaMemcpyAsync(c->d_hpos, pos, bytes, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(c->d_hfrc, forces, bytes, cudaMemcpyHostToDevice, st));
+  if (c->n_pin < c->n || !c->h_pin_out) {
+    if (c->h_pin_pos) cudaFreeHost(c->h_pin_pos);
+    if (c->h_pin_frc) cudaFreeHost(c->h_pin_frc);
+    if (c->h_pin_out) cudaFreeHost(c->h_pin_out);
+    c->h_pin_pos = c->h_pin_frc = c->h_pin_out = nullptr;
+    CK(cudaMallocHost((void **)&c->h_pin_pos, std::max<size_t>(bytes, 8)));
+    CK(cudaMallocHost((void **)&c->h_pin_frc, std::max<size_t>(bytes, 8)));
+    CK(cudaMallocHost((void **)&c->h_pin_out, sizeof(double) * 20));
+    c->n_pin = c->n;
   }
-  rc = launch_eval(c, c->d_hpos, c->d_hfrc, c->d_out, flags, 1, st);
+  // positions through pinned staging; this evaluation's forces are computed
+  // on the device (overwrite), read back, and added to the caller's array
+  if (c->n > 0) {
+    std::memcpy(c->h_pin_pos, pos, bytes);
+    CK(cudaMemcpyAsync(c->d_hpos, c->h_pin_pos, bytes, cudaMemcpyHostToDevice, st));
+  }
+  rc = launch_eval(c, c->d_hpos, c->d_hfrc, c->d_out, flags, 0, st);
   if (rc) return rc;
-  double out[20];
-  if (c->n > 0) CK(cudaMemcpyAsync(forces, c->d_hfrc, bytes, cudaMemcpyDeviceToHost, st));
-  if (flags) CK(cudaMemcpyAsync(out, c->d_out, sizeof(out), cudaMemcpyDeviceToHost, st));
+  if (c->n > 0) CK(cudaMemcpyAsync(c->h_pin_frc, c->d_hfrc, bytes, cudaMemcpyDeviceToHost, st));
+  if (flags)
+    CK(cudaMemcpyAsync(c->h_pin_out, c->d_out, sizeof(double) * 20, cudaMemcpyDeviceToHost, st));
   rc = pmb200_sync(c);
   if (rc) return rc;
+  for (size_t k = 0; k < cnt; k++) forces[k] += c->h_pin_frc[k];
+  const double *out = c->h_pin_out;
   if (flags & PMB200_ENERGY) {
     energies[0] += out[0];
     energies[1] += out[1];
@@ -575,8 +652,7 @@ int pmb200_leapfrog_device(pmb200_ctx *c, double *d_pos, double *d_vel, double *
   rc = launch_eval(c, d_pos, d_forces, nullptr, 0, 0, st);
   if (rc) return rc;
   auto step = [&](double kick, unsigned fl) -> int {
-    if (n > 0)
-      k_kick_drift<<<nb, tb, 0, st>>>(n, d_pos, d_vel, d_forces, c->d_mass, kick * h, h, 1);
+    launch_kick_drift(c, d_pos, d_vel, d_forces, kick * h, h, st);
     return launch_eval(c, d_pos, d_forces, d_out, fl, 0, st);
   };
   rc = step(0.5, nsteps == 1 ? flags : 0);
@@ -627,8 +703,7 @@ int pmb200_step_device(pmb200_ctx *c, double *d_pos, double *d_vel, double *d_fo
   CK(cudaSetDevice(c->p.device));
   cudaStream_t st = (cudaStream_t)stream;
   const void *key[5] = {d_pos, d_vel, d_forces, d_out, stream};
-  bool same = c->sgraph_exec && c->sgraph_dt == dt_fs && c->sgraph_flags == flags &&
-              c->sgraph_timing == c->timing;
+  bool same = c->sgraph_exec && c->sgraph_dt == dt_fs && c->sgraph_flags == flags;
   for (int k = 0; k < 5 && same; k++) same = c->sgraph_key[k] == key[k];
   if (!same) {
     if (c->sgraph_exec) cudaGraphExecDestroy(c->sgraph_exec);
@@ -636,11 +711,8 @@ int pmb200_step_device(pmb200_ctx *c, double *d_pos, double *d_vel, double *d_fo
     c->sgraph_exec = nullptr;
     c->sgraph = nullptr;
     const double h = dt_fs * 0.02045482828087295;  // Constant::INV_TIMEFACTOR
-    const int n = c->n;
-    const int tb = 256, nb = (3 * n + tb - 1) / tb;
     CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    if (n > 0)
-      k_kick_drift<<<nb, tb, 0, st>>>(n, d_pos, d_vel, d_forces, c->d_mass, h, h, 1);
+    launch_kick_drift(c, d_pos, d_vel, d_forces, h, h, st);
     rc = launch_eval(c, d_pos, d_forces, d_out, flags, 0, st);
     cudaGraph_t gr = nullptr;
     cudaError_t e = cudaStreamEndCapture(st, &gr);
@@ -654,9 +726,55 @@ int pmb200_step_device(pmb200_ctx *c, double *d_pos, double *d_vel, double *d_fo
     for (int k = 0; k < 5; k++) c->sgraph_key[k] = key[k];
     c->sgraph_dt = dt_fs;
     c->sgraph_flags = flags;
-    c->sgraph_timing = c->timing;
   }
   CK(cudaGraphLaunch(c->sgraph_exec, st));
+  return PMB200_OK;
+}
+
+int pmb200_set_rigid_waters(pmb200_ctx *c, int nwater, const int *widx, double d_oh,
+                            double d_hh) {
+  if (!c) return PMB200_EINVAL;
+  if (!c->have_topo) return fail(c, PMB200_ESTATE, "pmb200_set_topology has not been called");
+  if (nwater < 0 || (nwater > 0 && !widx)) return fail(c, PMB200_EINVAL, "water list");
+  if (nwater > 0 && !c->have_mass) return fail(c, PMB200_EINVAL, "rigid waters need masses");
+  if (nwater > 0 && !(d_oh > 0.0 && d_hh > 0.0 && d_hh < 2.0 * d_oh))
+    return fail(c, PMB200_EINVAL, "constraint lengths O-H %g, H-H %g", d_oh, d_hh);
+  CK(cudaSetDevice(c->p.device));
+  release_graph(c);
+  std::vector<char> used(c->n, 0);
+  std::vector<double> mass(c->n);
+  if (c->n > 0 && nwater > 0)
+    CK(cudaMemcpy(mass.data(), c->d_mass, sizeof(double) * c->n, cudaMemcpyDeviceToHost));
+  for (int w = 0; w < 3 * nwater; w++) {
+    const int a = widx[w];
+    if (a < 0 || a >= c->n) return fail(c, PMB200_EINVAL, "water atom index %d", a);
+    if (used[a]) return fail(c, PMB200_EINVAL, "atom %d in two waters", a);
+    used[a] = 1;
+  }
+  for (int w = 0; w < nwater; w++) {  // every water shares the first one's masses
+    if (mass[widx[3 * w]] != mass[widx[0]] || mass[widx[3 * w + 1]] != mass[widx[1]] ||
+        mass[widx[3 * w + 2]] != mass[widx[1]])
+      return fail(c, PMB200_EINVAL, "water %d: masses differ from the first water's", w);
+  }
+  std::vector<int> fidx;
+  for (int i = 0; i < c->n; i++)
+    if (!used[i]) fidx.push_back(i);
+  c->nwater = nwater;
+  c->nfree = (int)fidx.size();
+  if (nwater > 0) {
+    CK(dalloc(c->d_widx, 3 * (size_t)nwater));
+    CK(cudaMemcpy(c->d_widx, widx, sizeof(int) * 3 * nwater, cudaMemcpyHostToDevice));
+    CK(dalloc(c->d_fidx, std::max<size_t>(fidx.size(), 1)));
+    if (!fidx.empty())
+      CK(cudaMemcpy(c->d_fidx, fidx.data(), sizeof(int) * fidx.size(), cudaMemcpyHostToDevice));
+    const double mo = mass[widx[0]], mh = mass[widx[1]];
+    const double rcv = 0.5 * d_hh, t = std::sqrt(d_oh * d_oh - rcv * rcv);
+    c->sp.mo = mo;
+    c->sp.mh = mh;
+    c->sp.rc = rcv;
+    c->sp.ra = 2.0 * mh * t / (mo + 2.0 * mh);
+    c->sp.rb = t - c->sp.ra;
+  }
   return PMB200_OK;
 }
 
@@ -679,6 +797,93 @@ int pmb200_last_pair_count(pmb200_ctx *c, long long *pairs) {
   CK(cudaSetDevice(c->p.device));
   CK(cudaMemcpy(&v, c->d_pairs, sizeof(double), cudaMemcpyDeviceToHost));
   *pairs = (long long)llround(v);
+  return PMB200_OK;
+}
+
+// SETTLE on the host (same algorithm as settle_water on the device).
+static void host_settle(const SettleParams &sp, const double *A0, const double *B0,
+                        const double *C0, double *A1, double *B1, double *C1) {
+  auto cross = [](const double a[3], const double b[3], double o[3]) {
+    o[0] = a[1] * b[2] - a[2] * b[1];
+    o[1] = a[2] * b[0] - a[0] * b[2];
+    o[2] = a[0] * b[1] - a[1] * b[0];
+  };
+  auto dot = [](const double a[3], const double b[3]) {
+    return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+  };
+  auto unit = [&](double a[3]) {
+    const double r = std::sqrt(dot(a, a));
+    a[0] /= r; a[1] /= r; a[2] /= r;
+  };
+  const double M = sp.mo + 2.0 * sp.mh;
+  double com[3], a1[3], b1[3], c1[3], b0[3], c0[3], ex[3], ey[3], ez[3];
+  for (int k = 0; k < 3; k++) {
+    com[k] = (sp.mo * A1[k] + sp.mh * B1[k] + sp.mh * C1[k]) / M;
+    a1[k] = A1[k] - com[k];
+    b1[k] = B1[k] - com[k];
+    c1[k] = C1[k] - com[k];
+    b0[k] = B0[k] - A0[k];
+    c0[k] = C0[k] - A0[k];
+  }
+  cross(b0, c0, ez);
+  cross(a1, ez, ex);
+  cross(ez, ex, ey);
+  unit(ex); unit(ey); unit(ez);
+  const double xb0 = dot(ex, b0), yb0 = dot(ey, b0), xc0 = dot(ex, c0), yc0 = dot(ey, c0);
+  const double za1 = dot(ez, a1);
+  const double xb1 = dot(ex, b1), yb1 = dot(ey, b1), zb1 = dot(ez, b1);
+  const double xc1 = dot(ex, c1), yc1 = dot(ey, c1), zc1 = dot(ez, c1);
+  const double sphi = za1 / sp.ra, cphi = std::sqrt(1.0 - sphi * sphi);
+  const double spsi = (zb1 - zc1) / (2.0 * sp.rc * cphi), cpsi = std::sqrt(1.0 - spsi * spsi);
+  const double ya2 = sp.ra * cphi, xb2 = -sp.rc * cpsi;
+  const double t1 = -sp.rb * cphi, t2 = sp.rc * spsi * sphi;
+  const double yb2 = t1 - t2, yc2 = t1 + t2;
+  const double al = xb2 * (xb0 - xc0) + yb0 * yb2 + yc0 * yc2;
+  const double be = xb2 * (yc0 - yb0) + xb0 * yb2 + xc0 * yc2;
+  const double ga = xb0 * yb1 - xb1 * yb0 + xc0 * yc1 - xc1 * yc0;
+  const double ab = al * al + be * be;
+  const double sth = (al * ga - be * std::sqrt(ab - ga * ga)) / ab;
+  const double cth = std::sqrt(1.0 - sth * sth);
+  const double xa3 = -ya2 * sth, ya3 = ya2 * cth, za3 = za1;
+  const double xb3 = xb2 * cth - yb2 * sth, yb3 = xb2 * sth + yb2 * cth, zb3 = zb1;
+  const double xc3 = -xb2 * cth - yc2 * sth, yc3 = -xb2 * sth + yc2 * cth, zc3 = zc1;
+  for (int k = 0; k < 3; k++) {
+    A1[k] = com[k] + xa3 * ex[k] + ya3 * ey[k] + za3 * ez[k];
+    B1[k] = com[k] + xb3 * ex[k] + yb3 * ey[k] + zb3 * ez[k];
+    C1[k] = com[k] + xc3 * ex[k] + yc3 * ey[k] + zc3 * ez[k];
+  }
+}
+
+int pmb200_host_kick_drift(int n, double *pos, double *vel, const double *forces,
+                           const double *mass, double dt_fs, double kick, int nwater,
+                           const int *widx, double d_oh, double d_hh) {
+  if (n < 0 || (n > 0 && (!pos || !vel || !forces || !mass)) || !(dt_fs > 0.0))
+    return PMB200_EINVAL;
+  if (nwater < 0 || (nwater > 0 && !widx)) return PMB200_EINVAL;
+  const double h = dt_fs * 0.02045482828087295;  // Constant::INV_TIMEFACTOR
+  std::vector<double> old;
+  if (nwater > 0) old.assign(pos, pos + 3 * (size_t)n);
+  for (int i = 0; i < n; i++)
+    for (int k = 0; k < 3; k++) {
+      vel[3 * i + k] += forces[3 * i + k] * (kick * h) / mass[i];
+      pos[3 * i + k] += vel[3 * i + k] * h;
+    }
+  if (nwater > 0) {
+    SettleParams sp{};
+    const double mo = mass[widx[0]], mh = mass[widx[1]];
+    const double rcv = 0.5 * d_hh, t = std::sqrt(d_oh * d_oh - rcv * rcv);
+    sp.mo = mo; sp.mh = mh; sp.rc = rcv;
+    sp.ra = 2.0 * mh * t / (mo + 2.0 * mh);
+    sp.rb = t - sp.ra;
+    for (int w = 0; w < nwater; w++) {
+      const int a = widx[3 * w], b = widx[3 * w + 1], cc = widx[3 * w + 2];
+      if (a < 0 || b < 0 || cc < 0 || a >= n || b >= n || cc >= n) return PMB200_EINVAL;
+      host_settle(sp, &old[3 * a], &old[3 * b], &old[3 * cc], pos + 3 * a, pos + 3 * b,
+                  pos + 3 * cc);
+      for (int at : {a, b, cc})
+        for (int k = 0; k < 3; k++) vel[3 * at + k] = (pos[3 * at + k] - old[3 * at + k]) / h;
+    }
+  }
   return PMB200_OK;
 }
 

@@ -34,9 +34,9 @@ enum {
   ACC_ELJ = 3,  // Lennard-Jones energy
   ACC_ECOUL = 4,// Coulomb energy, direct (FP64 kernel)
   ACC_W = 5,    // 6 virial components xx xy xz yy yz zz (5..10)
-  ACC_WI = 11,  // 6 virial components of same-molecule pairs (11..16)
+  ACC_MW = 11,  // 6 molecular-virial components f_a comDiff_b, a <= b (11..16)
   ACC_PAIRS = 17,
-  ACC_MV = 18,  // 6 components of sum F_i^inter (x) o_i (18..23), finalize
+  ACC_MV = 18,  // number of slots in use
 };
 
 struct Row {        // one (dy, dz) row of the neighbour-cell stencil
@@ -51,6 +51,27 @@ struct GridParams {
   double unit;       // cell-unit length scale (= edge[0])
   int nrows;
 };
+
+// PeriodicBoundaryConditions constants for minimalDifference
+// (protomol/src/protomol/topology/PeriodicBoundaryConditions.cpp:32-77,
+// orthogonal box), used for the molecule-centre differences of the
+// molecular virial.
+struct PbcRef {
+  double e[3], er[3], h[3], h2[3], d;
+};
+
+// PeriodicBoundaryConditions::minimalDifference, orthogonal branch
+// (protomol/src/protomol/topology/PeriodicBoundaryConditions.h:53-70).
+__device__ __forceinline__ void ref_min_image(const PbcRef &b, double v[3]) {
+  if (v[0] * v[0] + v[1] * v[1] + v[2] * v[2] > b.d) {
+    for (int k = 0; k < 3; k++) {
+      if (v[k] < -b.h2[k]) v[k] += b.h[k];
+      else if (v[k] > b.h2[k]) v[k] -= b.h[k];
+    }
+    if (v[0] * v[0] + v[1] * v[1] + v[2] * v[2] > b.d)
+      for (int k = 0; k < 3; k++) v[k] -= b.e[k] * rint(b.er[k] * v[k]);
+  }
+}
 
 struct MixedConsts {   // FP32 constants in cell units
   float cut2, rclj2, ron2, rcc2;
@@ -71,6 +92,14 @@ struct Fp64Consts {
 // contexts with different grids never share it).
 struct Stencil {
   Row rows[kMaxRows];
+};
+
+// Half-shell neighbour cells, one entry per cell offset, packed as
+// (dx + 8) | (dy + 8) << 5 | (dz + 8) << 10 (offsets lie in [-8, 8]).
+constexpr int kMaxHalfCells = 512;
+struct HalfStencil {
+  unsigned short off[kMaxHalfCells];
+  int ncells;
 };
 
 // ---------------------------------------------------------------------------
@@ -208,45 +237,107 @@ __device__ __forceinline__ int lanes_per_atom(int m) {
 }
 
 // ---------------------------------------------------------------------------
-// Mixed-precision pair kernel.  One warp per i-cell; the cell's atoms are
-// taken in chunks of at most 32 / L, each atom served by L lanes that split
-// the j atoms of every neighbour cell by index parity.  Pair arithmetic is
-// FP32 in cell units (positions relative to the cell corner, integer cell
-// shifts, so no per-offset rounding bias); every atom sees the whole stencil
-// (no Newton's-third-law halving, so no write conflicts and no atomics).
-// Per stencil row the FP32 force partial is folded into an int64 fixed-point
-// accumulator (2^-32 force units), giving a deterministic exact sum.  The
-// Coulomb energy is carried as three sums (q q / r, q q, q q r^2) so the C1
-// constants are applied once in FP64.
+// Mixed-precision pair kernel (Newton's third law, half-shell stencil).
+//
+// One 4-warp block per i-cell.  The half-shell stencil rows (every cell pair
+// once; the home cell pairs i < j) are dealt to the block's warps round-robin.
+//
+// Per warp: the cell's atoms are taken in chunks of at most 32 / L, each atom
+// served by L lanes that split the candidates by index.  Candidate j atoms
+// are staged in shared memory in batches of kBatch, already shifted into the
+// i-cell's frame (integer cell offsets in cell units, so no per-offset
+// rounding bias).  Each lane first scans the batch and compacts the indices
+// of its in-range partners into a private list, then walks its list (from a
+// lane-dependent starting point, so lanes rarely hit the same j at once):
+// the pair arithmetic runs on dense lanes instead of under a divergent
+// branch.
+//
+// Forces: the pair force on j is added to a per-batch int32 fixed-point
+// accumulator in shared memory (2^-16 cell-unit force quanta; integer
+// atomics, so the sum is independent of order) and flushed per batch into
+// the global int64 fixed-point accumulator facc (2^-32 quanta, sorted order,
+// [3][n]).  The force on i is summed in FP32 per batch, folded into an int64
+// register, combined over lanes and warps and added to facc once.  Every
+// integer sum is exact, so the result does not depend on scheduling.
+//
+// Pair arithmetic is FP32 in cell units.  The Coulomb energy is carried as
+// three Kahan-compensated sums (q_j / r, q_j, q_j r^2) so that the C1
+// constants are applied once in FP64 at the end.
 // ---------------------------------------------------------------------------
-template <bool kEnergy, bool kVirial>
+constexpr int kWarps = 4;
+constexpr int kBatch = 128;
+
+constexpr float kJScale = 262144.0f; // shared j-force quanta (2^-18) per cell-unit force
+constexpr int kJShift = 14;          // to the global 2^-32 quanta
+constexpr float kJLimit = 6.7e7f;    // per-contribution bound: 32 contributions fit int32
+
+struct __align__(16) MixedWarpSmem {
+  float4 pos[kBatch];                    // staged j atoms, shifted into the i-cell frame
+  int jf[3][kBatch];                     // per-batch j forces, int32 fixed point (2^-16)
+  int2 meta[kBatch];                     // their (LJ type, molecule)
+  int gidx[kBatch];                      // their sorted indices
+  unsigned char list[kBatch / 2][32];    // per-lane in-range candidate indices
+};
+
+struct KahanF {
+  float s = 0.f, c = 0.f;
+  __device__ __forceinline__ void add(float x) {
+    const float y = x - c;
+    const float t = s + y;
+    c = (t - s) - y;
+    s = t;
+  }
+};
+
+// Adds a j-force contribution (cell units) to j's per-batch int32 shared
+// accumulator in 2^-18 quanta.  A batch adds at most 32 contributions to one
+// j, so each must stay within kJLimit quanta (256 cell units); a larger one
+// (close contacts) goes straight to the global int64 accumulator at full
+// 2^-32 resolution instead.  Both sums are exact integer sums.
+__device__ __forceinline__ void jadd(int *sh, unsigned long long *g, float v) {
+  const float q = v * kJScale;
+  if (fabsf(q) <= kJLimit)
+    atomicAdd(sh, __float2int_rn(q));
+  else
+    atomicAdd(g, (unsigned long long)__float2ll_rn(v * 4294967296.0f));
+}
+
+template <bool kEnergy, bool kVirial, bool kMolVir>
 __global__ void __launch_bounds__(128)
-k_pair_mixed(GridParams g, MixedConsts mc, const Stencil st, int ntypes, const float4 *__restrict__ lj32,
+k_pair_mixed(GridParams g, MixedConsts mc, const HalfStencil st, int ntypes, const float4 *__restrict__ lj32,
              const int *__restrict__ start, const float4 *__restrict__ spos,
              const int2 *__restrict__ smeta, const int *__restrict__ sidx,
              const int *__restrict__ ex_start, const int2 *__restrict__ ex,
-             double *__restrict__ forces, int accumulate, double force_scale,
-             double *__restrict__ partial, double *__restrict__ frc_inter) {
+             unsigned long long *__restrict__ facc, int n, int *__restrict__ err,
+             double *__restrict__ partial, const PbcRef pb, const double *__restrict__ com) {
   __shared__ float4 s_lj[kMaxTypes * kMaxTypes];
+  __shared__ MixedWarpSmem s_w[kWarps];
+  __shared__ long long s_f[kWarps][32][3];
+  __shared__ double s_acc[kWarps][ACC_MV];
   for (int k = threadIdx.x; k < ntypes * ntypes; k += blockDim.x) s_lj[k] = lj32[k];
-  __syncthreads();
   const int lane = threadIdx.x & 31;
-  const int cell = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (cell >= g.ncell) return;
+  const int warp = threadIdx.x >> 5;
+  MixedWarpSmem &sm = s_w[warp];
+  for (int t = lane; t < kBatch; t += 32) sm.jf[0][t] = sm.jf[1][t] = sm.jf[2][t] = 0;
+  __syncthreads();
+  const int cell = blockIdx.x;
+  if (cell >= g.ncell) return;  // uniform per block
   const int cx = cell % g.nx;
   const int cy = (cell / g.nx) % g.ny;
   const int cz = cell / (g.nx * g.ny);
   const int cs = start[cell], ce = start[cell + 1];
 
+  KahanF kU, kQ, kR;
   double accU = 0, accQ = 0, accR = 0, accE = 0, accP = 0;
   double w[6] = {0, 0, 0, 0, 0, 0};
-  double wi[6] = {0, 0, 0, 0, 0, 0};
+  double mw[6] = {0, 0, 0, 0, 0, 0};
+  const double inv_unit = 1.0 / g.unit;
 
   for (int c0 = cs; c0 < ce; c0 += 32) {
     const int m = min(32, ce - c0);
     const int L = lanes_per_atom(m);
-    const int ia = lane / L;         // atom within chunk
-    const int sub = lane % L;        // lane within the atom's group
+    const int ia = lane / L;
+    const int sub = lane % L;
     const bool active = ia < m;
     const int i = c0 + (active ? ia : 0);
     const float4 pi = spos[i];
@@ -254,153 +345,259 @@ k_pair_mixed(GridParams g, MixedConsts mc, const Stencil st, int ntypes, const f
     const int oi = sidx[i];
     const int elo = ex_start[oi], ehi = ex_start[oi + 1];
     const int ti = mi.x * ntypes;
+    // a batch holds at most 64 candidates per lane (the list depth)
+    const int batch_cap = min(kBatch, 64 * L);
     long long fx = 0, fy = 0, fz = 0;
-    float fix = 0.f, fiy = 0.f, fiz = 0.f;  // same-molecule force part
+    double Ri[3] = {0.0, 0.0, 0.0};
+    if (kMolVir)
+      for (int k = 0; k < 3; k++) Ri[k] = com[3 * (size_t)mi.y + k];
 
-    for (int r = 0; r < g.nrows; r++) {
-      const Row row = st.rows[r];
-      int jy = cy + row.dy; jy += (jy < 0) ? g.ny : 0; jy -= (jy >= g.ny) ? g.ny : 0;
-      int jz = cz + row.dz; jz += (jz < 0) ? g.nz : 0; jz -= (jz >= g.nz) ? g.nz : 0;
-      // the row's y/z cell distances can exceed one box length only for
-      // grids smaller than the stencil; wrap again to be safe
-      while (jy < 0) jy += g.ny;
-      while (jy >= g.ny) jy -= g.ny;
-      while (jz < 0) jz += g.nz;
-      while (jz >= g.nz) jz -= g.nz;
-      const int rowbase = (jz * g.ny + jy) * g.nx;
-      const float sy = (float)row.dy * mc.ey, sz = (float)row.dz * mc.ez;
-      float px = 0.f, py = 0.f, pz = 0.f;
-      float pU = 0.f, pQ = 0.f, pR = 0.f, pE = 0.f;
+    int nb = 0;          // staged atoms in the current batch
+    int home_lo = 0;     // staged range [home_lo, home_hi) of the home cell,
+    int home_hi = 0;     // whose first entry has sorted index home_base;
+    int home_base = 0;   // home-cell pairs are taken for i < j only
+    auto flush_batch = [&]() {
+      __syncwarp();
+      int cnt = 0;
+      if (active) {
+        // home-cell entries t with ex_lo <= t < ex_lo + ex_n are j <= i
+        const int ex_lo = home_lo;
+        const unsigned ex_n =
+            (unsigned)max(0, min(home_hi - home_lo, i - home_base + 1));
+        const float2 nx = make_float2(-pi.x, -pi.x), ny = make_float2(-pi.y, -pi.y),
+                     nz = make_float2(-pi.z, -pi.z);
+        unsigned char *lst = &sm.list[0][lane];
+        int t = sub;
+        // two candidates per step with packed FP32 (FADD2 / FMUL2 / FFMA2)
+        for (; t + L < nb; t += 2 * L) {
+          const float4 a = sm.pos[t], b = sm.pos[t + L];
+          const float2 dx = __fadd2_rn(make_float2(a.x, b.x), nx);
+          const float2 dy = __fadd2_rn(make_float2(a.y, b.y), ny);
+          const float2 dz = __fadd2_rn(make_float2(a.z, b.z), nz);
+          float2 r2 = __fmul2_rn(dz, dz);
+          r2 = __ffma2_rn(dy, dy, r2);
+          r2 = __ffma2_rn(dx, dx, r2);
+          if (r2.x <= mc.cut2 && (unsigned)(t - ex_lo) >= ex_n) {
+            lst[cnt * 32] = (unsigned char)t;
+            cnt++;
+          }
+          if (r2.y <= mc.cut2 && (unsigned)(t + L - ex_lo) >= ex_n) {
+            lst[cnt * 32] = (unsigned char)(t + L);
+            cnt++;
+          }
+        }
+        if (t < nb) {
+          const float4 a = sm.pos[t];
+          const float dx = a.x - pi.x, dy = a.y - pi.y, dz = a.z - pi.z;
+          const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+          if (r2 <= mc.cut2 && (unsigned)(t - ex_lo) >= ex_n) {
+            lst[cnt * 32] = (unsigned char)t;
+            cnt++;
+          }
+        }
+      }
+      const int maxc = __reduce_max_sync(0xffffffffu, cnt);
+      float px = 0.f, py = 0.f, pz = 0.f, pE = 0.f;
       float pw0 = 0.f, pw1 = 0.f, pw2 = 0.f, pw3 = 0.f, pw4 = 0.f, pw5 = 0.f;
+      float pm0 = 0.f, pm1 = 0.f, pm2 = 0.f, pm3 = 0.f, pm4 = 0.f, pm5 = 0.f;
       int pc = 0;
-      for (int dx = row.dxlo; dx <= row.dxhi; dx++) {
-        int jx = cx + dx;
-        jx %= g.nx;
-        jx += (jx < 0) ? g.nx : 0;
-        const int jc = rowbase + jx;
-        const int js = start[jc], je = start[jc + 1];
-        const float sx = (float)dx;
-        for (int j = js + sub; j < je; j += L) {
-          const float4 pj = spos[j];
-          const float ddx = (pj.x + sx) - pi.x;
-          const float ddy = (pj.y + sy) - pi.y;
-          const float ddz = (pj.z + sz) - pi.z;
-          const float r2 = fmaf(ddx, ddx, fmaf(ddy, ddy, ddz * ddz));
-          if (!(r2 <= mc.cut2) || j == i || !active) continue;
-          const int2 mj = smeta[j];
-          int kind = 0;
-          if (mj.y == mi.y) {
-            kind = excl_kind(ex, elo, ehi, sidx[j]);
-            if (kind == 2) continue;
+      for (int k = 0; k < maxc; k++) {
+        if (k >= cnt) continue;
+        const int t = sm.list[k][lane];
+        const float4 pj = sm.pos[t];
+        const float ddx = pj.x - pi.x, ddy = pj.y - pi.y, ddz = pj.z - pi.z;
+        const float r2 = fmaf(ddx, ddx, fmaf(ddy, ddy, ddz * ddz));
+        const int2 mj = sm.meta[t];
+        int kind = 0;
+        if (mj.y == mi.y) {
+          kind = excl_kind(ex, elo, ehi, sidx[sm.gidx[t]]);
+          if (kind == 2) continue;
+        }
+        // 1/r: hardware reciprocal square root refined by one Newton-Raphson
+        // step for 1/sqrt(x).
+        float rinv = rsqrtf(r2);
+        rinv = fmaf(0.5f * rinv, fmaf(-r2 * rinv, rinv, 1.0f), rinv);
+        const float r2inv = rinv * rinv;
+        const float4 p = s_lj[ti + mj.x];
+        const float A = kind == 1 ? p.z : p.x;
+        const float B = kind == 1 ? p.w : p.y;
+        const float r6 = r2inv * r2inv * r2inv;
+        float elj = fmaf(A, r6, -B) * r6;
+        float flj = fmaf(12.0f * A, r6, -6.0f * B) * r6 * r2inv;
+        {  // C2 switch, branch-free: value 1 below switchon, 0 beyond cutoff
+          const float c2 = mc.rclj2 - r2;
+          const float c4 = c2 * fmaf(2.0f, r2, mc.s2);
+          const bool on = r2 >= mc.ron2;
+          const bool in = r2 <= mc.rclj2;
+          const float sv = in ? (on ? mc.s1 * (c2 * c4) : 1.0f) : 0.0f;
+          const float sd = (in && on) ? mc.s3 * fmaf(c2, c2, -c4) : 0.0f;
+          flj = fmaf(flj, sv, -elj * sd);
+          elj = elj * sv;
+        }
+        float qj = pj.w;
+        if (kind == 1) qj *= mc.csf;
+        float fc = 0.f;
+        if (r2 <= mc.rcc2) {  // C1 switched Coulomb
+          const float ec = pi.w * qj * rinv;
+          const float dist = r2 * rinv;
+          const float sv = 1.0f - dist * fmaf(-r2, mc.c05_3, mc.c15_1);
+          const float sd = fmaf(dist, mc.c15_3, -mc.c15_1 * rinv);
+          fc = fmaf(ec * r2inv, sv, -ec * sd);
+          if (kEnergy) {
+            kU.add(qj * rinv);
+            kQ.add(qj);
+            kR.add(qj * r2);
           }
-          // 1/r: hardware reciprocal square root refined by one
-          // Newton-Raphson step for 1/sqrt(x).
-          float rinv = rsqrtf(r2);
-          rinv = fmaf(0.5f * rinv, fmaf(-r2 * rinv, rinv, 1.0f), rinv);
-          const float r2inv = rinv * rinv;
-          const float4 p = s_lj[ti + mj.x];
-          const float A = kind == 1 ? p.z : p.x;
-          const float B = kind == 1 ? p.w : p.y;
-          const float r6 = r2inv * r2inv * r2inv;
-          float elj = fmaf(A, r6, -B) * r6;
-          float flj = fmaf(12.0f * A, r6, -6.0f * B) * r6 * r2inv;
-          if (r2 > mc.rclj2) {
-            elj = 0.f; flj = 0.f;
-          } else if (r2 >= mc.ron2) {  // C2 switch region
-            const float c2 = mc.rclj2 - r2;
-            const float c4 = c2 * fmaf(2.0f, r2, mc.s2);
-            const float sv = mc.s1 * (c2 * c4);
-            const float sd = mc.s3 * fmaf(c2, c2, -c4);
-            flj = fmaf(flj, sv, -elj * sd);
-            elj = elj * sv;
-          }
-          float qj = pj.w;
-          if (kind == 1) qj *= mc.csf;
-          float fc = 0.f;
-          if (r2 <= mc.rcc2) {  // C1 switched Coulomb
-            const float ec = pi.w * qj * rinv;
-            const float dist = r2 * rinv;
-            const float sv = 1.0f - dist * fmaf(-r2, mc.c05_3, mc.c15_1);
-            const float sd = fmaf(dist, mc.c15_3, -mc.c15_1 * rinv);
-            fc = fmaf(ec * r2inv, sv, -ec * sd);
-            if (kEnergy) {
-              pU = fmaf(qj, rinv, pU);
-              pQ += qj;
-              pR = fmaf(qj, r2, pR);
-            }
-          }
-          const float f = flj + fc;
-          px = fmaf(-ddx, f, px);
-          py = fmaf(-ddy, f, py);
-          pz = fmaf(-ddz, f, pz);
-          if (kEnergy) { pE += elj; pc++; }
-          if (kVirial) {
-            const float fxv = ddx * f, fyv = ddy * f, fzv = ddz * f;
-            pw0 = fmaf(fxv, ddx, pw0); pw1 = fmaf(fxv, ddy, pw1); pw2 = fmaf(fxv, ddz, pw2);
-            pw3 = fmaf(fyv, ddy, pw3); pw4 = fmaf(fyv, ddz, pw4); pw5 = fmaf(fzv, ddz, pw5);
-            if (mj.y == mi.y) {
-              wi[0] += (double)(fxv * ddx); wi[1] += (double)(fxv * ddy); wi[2] += (double)(fxv * ddz);
-              wi[3] += (double)(fyv * ddy); wi[4] += (double)(fyv * ddz); wi[5] += (double)(fzv * ddz);
-              fix -= fxv; fiy -= fyv; fiz -= fzv;
-            }
+        }
+        const float f = flj + fc;
+        const float fxv = ddx * f, fyv = ddy * f, fzv = ddz * f;  // force on j
+        px -= fxv;
+        py -= fyv;
+        pz -= fzv;
+        {
+          const size_t jg = (size_t)sm.gidx[t];
+          jadd(&sm.jf[0][t], &facc[jg], fxv);
+          jadd(&sm.jf[1][t], &facc[(size_t)n + jg], fyv);
+          jadd(&sm.jf[2][t], &facc[2 * (size_t)n + jg], fzv);
+        }
+        if (kEnergy) { pE += elj; pc++; }
+        if (kVirial) {
+          pw0 = fmaf(fxv, ddx, pw0); pw1 = fmaf(fxv, ddy, pw1); pw2 = fmaf(fxv, ddz, pw2);
+          pw3 = fmaf(fyv, ddy, pw3); pw4 = fmaf(fyv, ddz, pw4); pw5 = fmaf(fzv, ddz, pw5);
+          if (kMolVir && mj.y != mi.y) {
+            // ScalarStructure::addVirial(fij, diff, comDiff): comDiff is the
+            // minimal image of the two molecule centres (FP64), in cell units
+            double cd[3];
+            for (int q = 0; q < 3; q++) cd[q] = com[3 * (size_t)mj.y + q] - Ri[q];
+            ref_min_image(pb, cd);
+            const float cx_ = (float)(cd[0] * inv_unit), cy_ = (float)(cd[1] * inv_unit),
+                        cz_ = (float)(cd[2] * inv_unit);
+            pm0 = fmaf(fxv, cx_, pm0); pm1 = fmaf(fxv, cy_, pm1); pm2 = fmaf(fxv, cz_, pm2);
+            pm3 = fmaf(fyv, cy_, pm3); pm4 = fmaf(fyv, cz_, pm4); pm5 = fmaf(fzv, cz_, pm5);
           }
         }
       }
       fx += __float2ll_rn(px * 4294967296.0f);
       fy += __float2ll_rn(py * 4294967296.0f);
       fz += __float2ll_rn(pz * 4294967296.0f);
-      if (kEnergy) {
-        const double qi = (double)pi.w;
-        accU += qi * (double)pU;
-        accQ += qi * (double)pQ;
-        accR += qi * (double)pR;
-        accE += (double)pE;
-        accP += (double)pc;
-      }
+      if (kEnergy) { accE += (double)pE; accP += (double)pc; }
       if (kVirial) {
         w[0] += pw0; w[1] += pw1; w[2] += pw2; w[3] += pw3; w[4] += pw4; w[5] += pw5;
       }
+      if (kMolVir) {
+        mw[0] += pm0; mw[1] += pm1; mw[2] += pm2; mw[3] += pm3; mw[4] += pm4; mw[5] += pm5;
+      }
+      __syncwarp();
+      // flush the batch's j forces to the global accumulator and clear them
+      for (int t = lane; t < nb; t += 32) {
+        const int j = sm.gidx[t];
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+          const int v = sm.jf[q][t];
+          if (v) atomicAdd(&facc[(size_t)q * n + j],
+                           (unsigned long long)((long long)v << kJShift));
+          sm.jf[q][t] = 0;
+        }
+      }
+      nb = 0;
+      home_lo = home_hi = 0;
+      __syncwarp();
+    };
+
+    // this warp's share of the half-shell cells, dealt round-robin
+    for (int q = warp; q < st.ncells; q += kWarps) {
+      const unsigned o = st.off[q];
+      const int dx = (int)(o & 31u) - 8, dy = (int)((o >> 5) & 31u) - 8,
+                dz = (int)((o >> 10) & 31u) - 8;
+      const bool home = (dx | dy | dz) == 0;
+      int jx = (cx + dx) % g.nx; jx += (jx < 0) ? g.nx : 0;
+      int jy = (cy + dy) % g.ny; jy += (jy < 0) ? g.ny : 0;
+      int jz = (cz + dz) % g.nz; jz += (jz < 0) ? g.nz : 0;
+      const int jc = (jz * g.ny + jy) * g.nx + jx;
+      int js = start[jc];
+      const int je = start[jc + 1];
+      const float sx = (float)dx, sy = (float)dy * mc.ey, sz = (float)dz * mc.ez;
+      while (js < je) {
+        const int take = min(je - js, batch_cap - nb);
+        for (int t = lane; t < take; t += 32) {
+          float4 p = spos[js + t];
+          p.x += sx; p.y += sy; p.z += sz;
+          sm.pos[nb + t] = p;
+          sm.meta[nb + t] = smeta[js + t];
+          sm.gidx[nb + t] = js + t;
+        }
+        if (home) {  // staged home-cell atoms: sorted js .. js+take-1
+          home_lo = nb;
+          home_hi = nb + take;
+          home_base = js;
+        }
+        nb += take;
+        js += take;
+        if (nb == batch_cap) flush_batch();
+      }
     }
-    // combine the L lanes of each atom (exact integer sums)
+    if (nb > 0) flush_batch();
+
+    // the i forces: lanes of an atom, then warps, then the global accumulator
     fx = warp_sum_ll(fx, L);
     fy = warp_sum_ll(fy, L);
     fz = warp_sum_ll(fz, L);
-    if (active && sub == 0) {
-      const double sc = force_scale * kFixInv;
-      double *fo = forces + 3 * (size_t)oi;
-      const double gx = (double)fx * sc, gy = (double)fy * sc, gz = (double)fz * sc;
-      if (accumulate) { fo[0] += gx; fo[1] += gy; fo[2] += gz; }
-      else { fo[0] = gx; fo[1] = gy; fo[2] = gz; }
-    }
-    if (kVirial && frc_inter) {
-      // this evaluation's force on the atom from other molecules (Angstrom
-      // units), for the molecular virial
-      float ax = fix, ay = fiy, az = fiz;
-      for (int off = 1; off < L; off <<= 1) {
-        ax += __shfl_xor_sync(0xffffffffu, ax, off);
-        ay += __shfl_xor_sync(0xffffffffu, ay, off);
-        az += __shfl_xor_sync(0xffffffffu, az, off);
+    s_f[warp][lane][0] = fx; s_f[warp][lane][1] = fy; s_f[warp][lane][2] = fz;
+    __syncthreads();
+    if (warp == 0 && active && sub == 0) {
+      long long tx = 0, ty = 0, tz = 0;
+      for (int q = 0; q < kWarps; q++) {
+        tx += s_f[q][lane][0]; ty += s_f[q][lane][1]; tz += s_f[q][lane][2];
       }
-      if (active && sub == 0) {
-        const double sc = force_scale * kFixInv;
-        frc_inter[3 * (size_t)oi] = (double)fx * sc - (double)ax * force_scale;
-        frc_inter[3 * (size_t)oi + 1] = (double)fy * sc - (double)ay * force_scale;
-        frc_inter[3 * (size_t)oi + 2] = (double)fz * sc - (double)az * force_scale;
-      }
+      atomicAdd(&facc[i], (unsigned long long)tx);
+      atomicAdd(&facc[(size_t)n + i], (unsigned long long)ty);
+      atomicAdd(&facc[2 * (size_t)n + i], (unsigned long long)tz);
     }
+    __syncthreads();
+    if (kEnergy && active) {
+      // the three Coulomb sums are per i-atom: weight them by q_i (FP64)
+      const double qi = (double)pi.w;
+      accU += qi * ((double)kU.s - (double)kU.c);
+      accQ += qi * ((double)kQ.s - (double)kQ.c);
+      accR += qi * ((double)kR.s - (double)kR.c);
+    }
+    kU = KahanF(); kQ = KahanF(); kR = KahanF();
   }
   if (kEnergy || kVirial) {
-    double v[kNacc];
+    double v[ACC_MV];
 #pragma unroll
-    for (int k = 0; k < kNacc; k++) v[k] = 0.0;
+    for (int k = 0; k < ACC_MV; k++) v[k] = 0.0;
     v[ACC_U] = accU; v[ACC_Q] = accQ; v[ACC_R] = accR; v[ACC_ELJ] = accE; v[ACC_PAIRS] = accP;
 #pragma unroll
-    for (int k = 0; k < 6; k++) { v[ACC_W + k] = w[k]; v[ACC_WI + k] = wi[k]; }
+    for (int k = 0; k < 6; k++) { v[ACC_W + k] = w[k]; v[ACC_MW + k] = mw[k]; }
 #pragma unroll
     for (int k = 0; k < ACC_MV; k++) {
-      double s = warp_sum_mask(v[k], 32);
-      if (lane == 0) partial[(size_t)cell * kNacc + k] = s;
+      const double sum = warp_sum_mask(v[k], 32);
+      if (lane == 0) s_acc[warp][k] = sum;
     }
+    __syncthreads();
+    if (threadIdx.x < ACC_MV) {
+      double sum = 0.0;
+      for (int q = 0; q < kWarps; q++) sum += s_acc[q][threadIdx.x];
+      partial[(size_t)cell * kNacc + threadIdx.x] = sum;
+    }
+  }
+}
+
+// Fixed-point force accumulator (sorted order, [3][n], 2^-32 quanta in cell
+// units) -> FP64 forces in the caller's atom order, accumulated or
+// overwritten.
+__global__ void k_finalize(int n, const unsigned long long *__restrict__ facc,
+                           const int *__restrict__ sidx, double scale, int accumulate,
+                           double *__restrict__ forces) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const int o = sidx[j];
+  double *fo = forces + 3 * (size_t)o;
+#pragma unroll
+  for (int q = 0; q < 3; q++) {
+    const double v = (double)(long long)facc[(size_t)q * n + j] * scale;
+    fo[q] = accumulate ? fo[q] + v : v;
   }
 }
 
@@ -409,14 +606,14 @@ k_pair_mixed(GridParams g, MixedConsts mc, const Stencil st, int ntypes, const f
 // mixed kernel, with the reference's FP64 per-pair arithmetic
 // (OneAtomPairTwo::doOneAtomPair) in Angstrom, forces summed in FP64.
 // ---------------------------------------------------------------------------
-template <bool kEnergy, bool kVirial>
+template <bool kEnergy, bool kVirial, bool kMolVir>
 __global__ void __launch_bounds__(128)
 k_pair_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes, const double4 *__restrict__ lj64,
             const int *__restrict__ start, const double4 *__restrict__ spos,
             const int2 *__restrict__ smeta, const int *__restrict__ sidx,
             const int *__restrict__ ex_start, const int2 *__restrict__ ex,
             double *__restrict__ forces, int accumulate, double *__restrict__ partial,
-            double *__restrict__ frc_inter) {
+            const PbcRef pb, const double *__restrict__ com) {
   const int lane = threadIdx.x & 31;
   const int cell = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (cell >= g.ncell) return;
@@ -426,7 +623,7 @@ k_pair_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes, const dou
   const int cs = start[cell], ce = start[cell + 1];
   double accC = 0, accE = 0, accP = 0;
   double w[6] = {0, 0, 0, 0, 0, 0};
-  double wi[6] = {0, 0, 0, 0, 0, 0};
+  double mw[6] = {0, 0, 0, 0, 0, 0};
   for (int c0 = cs; c0 < ce; c0 += 32) {
     const int m = min(32, ce - c0);
     const int L = lanes_per_atom(m);
@@ -439,7 +636,10 @@ k_pair_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes, const dou
     const int oi = sidx[i];
     const int elo = ex_start[oi], ehi = ex_start[oi + 1];
     const int ti = mi.x * ntypes;
-    double fx = 0, fy = 0, fz = 0, fix = 0, fiy = 0, fiz = 0;
+    double fx = 0, fy = 0, fz = 0;
+    double Ri[3] = {0.0, 0.0, 0.0};
+    if (kMolVir)
+      for (int k = 0; k < 3; k++) Ri[k] = com[3 * (size_t)mi.y + k];
     for (int r = 0; r < g.nrows; r++) {
       const Row row = st.rows[r];
       int jy = cy + row.dy, jz = cz + row.dz;
@@ -506,10 +706,12 @@ k_pair_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes, const dou
             const double fxv = ddx * f, fyv = ddy * f, fzv = ddz * f;
             w[0] += fxv * ddx; w[1] += fxv * ddy; w[2] += fxv * ddz;
             w[3] += fyv * ddy; w[4] += fyv * ddz; w[5] += fzv * ddz;
-            if (mj.y == mi.y) {
-              wi[0] += fxv * ddx; wi[1] += fxv * ddy; wi[2] += fxv * ddz;
-              wi[3] += fyv * ddy; wi[4] += fyv * ddz; wi[5] += fzv * ddz;
-              fix -= fxv; fiy -= fyv; fiz -= fzv;
+            if (kMolVir && mj.y != mi.y) {
+              double cd[3];
+              for (int q = 0; q < 3; q++) cd[q] = com[3 * (size_t)mj.y + q] - Ri[q];
+              ref_min_image(pb, cd);
+              mw[0] += fxv * cd[0]; mw[1] += fxv * cd[1]; mw[2] += fxv * cd[2];
+              mw[3] += fyv * cd[1]; mw[4] += fyv * cd[2]; mw[5] += fzv * cd[2];
             }
           }
         }
@@ -519,21 +721,11 @@ k_pair_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes, const dou
       fx += __shfl_xor_sync(0xffffffffu, fx, off);
       fy += __shfl_xor_sync(0xffffffffu, fy, off);
       fz += __shfl_xor_sync(0xffffffffu, fz, off);
-      if (kVirial) {
-        fix += __shfl_xor_sync(0xffffffffu, fix, off);
-        fiy += __shfl_xor_sync(0xffffffffu, fiy, off);
-        fiz += __shfl_xor_sync(0xffffffffu, fiz, off);
-      }
     }
     if (active && sub == 0) {
       double *fo = forces + 3 * (size_t)oi;
       if (accumulate) { fo[0] += fx; fo[1] += fy; fo[2] += fz; }
       else { fo[0] = fx; fo[1] = fy; fo[2] = fz; }
-      if (kVirial && frc_inter) {
-        frc_inter[3 * (size_t)oi] = fx - fix;
-        frc_inter[3 * (size_t)oi + 1] = fy - fiy;
-        frc_inter[3 * (size_t)oi + 2] = fz - fiz;
-      }
     }
   }
   if (kEnergy || kVirial) {
@@ -542,7 +734,7 @@ k_pair_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes, const dou
     for (int k = 0; k < ACC_MV; k++) v[k] = 0.0;
     v[ACC_ECOUL] = accC; v[ACC_ELJ] = accE; v[ACC_PAIRS] = accP;
 #pragma unroll
-    for (int k = 0; k < 6; k++) { v[ACC_W + k] = w[k]; v[ACC_WI + k] = wi[k]; }
+    for (int k = 0; k < 6; k++) { v[ACC_W + k] = w[k]; v[ACC_MW + k] = mw[k]; }
 #pragma unroll
     for (int k = 0; k < ACC_MV; k++) {
       double s = warp_sum_mask(v[k], 32);
@@ -554,8 +746,7 @@ k_pair_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes, const dou
 // ---------------------------------------------------------------------------
 // Molecular virial support: molecule centres of mass from the raw positions
 // (mass-weighted, Kahan-compensated like molecularCenterOfMass,
-// protomol/src/protomol/topology/TopologyUtilities.cpp:645-672), then
-// sum_i F_i^inter (x) (r_i - R_mol(i)) per block (9 components, not symmetric).
+// protomol/src/protomol/topology/TopologyUtilities.cpp:645-672).
 // ---------------------------------------------------------------------------
 __global__ void k_com(int nmol, const int *__restrict__ mstart, const int *__restrict__ matoms,
                       const double *__restrict__ mass, const double *__restrict__ pos,
@@ -583,46 +774,23 @@ __global__ void k_com(int nmol, const int *__restrict__ mstart, const int *__res
   for (int k = 0; k < 3; k++) com[3 * m + k] = c[k] / sw;
 }
 
-__global__ void k_molvir(int n, const int *__restrict__ mol, const double *__restrict__ pos,
-                         const double *__restrict__ com, const double *__restrict__ finter,
-                         double *__restrict__ part) {
-  __shared__ double sh[9][256];
-  const int t = threadIdx.x;
-  double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-  for (int i = blockIdx.x * blockDim.x + t; i < n; i += gridDim.x * blockDim.x) {
-    const int m = mol[i];
-    double o[3], f[3];
-    for (int k = 0; k < 3; k++) {
-      o[k] = pos[3 * i + k] - com[3 * m + k];
-      f[k] = finter[3 * i + k];
-    }
-    for (int a = 0; a < 3; a++)
-      for (int b = 0; b < 3; b++) v[3 * a + b] += f[a] * o[b];
-  }
-  for (int k = 0; k < 9; k++) sh[k][t] = v[k];
-  __syncthreads();
-  for (int off = blockDim.x / 2; off > 0; off >>= 1) {
-    if (t < off)
-      for (int k = 0; k < 9; k++) sh[k][t] += sh[k][t + off];
-    __syncthreads();
-  }
-  if (t == 0)
-    for (int k = 0; k < 9; k++) part[blockIdx.x * 9 + k] = sh[k][0];
-}
+// Deterministic two-stage reduction of the per-cell partials.  Stage 1:
+// block b sums cells [b*span, (b+1)*span) in a fixed tree order into
+// red[b][ACC_MV]; stage 2 (one block) sums the blocks in order and forms
+// out[20] = {COULOMB, LENNARDJONES, virial[9], molvirial[9]} and the unique
+// pair count.  mixed != 0: the Coulomb energy comes from the three-sum form
+// with the C1 constants (cell units) applied here in FP64.
+constexpr int kRedBlocks = 64;
 
-// Deterministic final reduction (one block, fixed order) of the per-cell
-// partials into out[20] = {COULOMB, LENNARDJONES, virial[9], molvirial[9]}
-// and the unique pair count.  mixed != 0: the Coulomb energy comes from the
-// three-sum form with the C1 constants (cell units) applied here in FP64.
-__global__ void k_reduce(int ncell, const double *__restrict__ partial, int mixed,
-                         double c15_1, double c05_3, int nmv,
-                         const double *__restrict__ mvpart, double *__restrict__ out,
-                         double *__restrict__ pairs_out) {
+__global__ void k_reduce1(int ncell, const double *__restrict__ partial,
+                          double *__restrict__ red) {
   __shared__ double sh[ACC_MV][256];
   const int t = threadIdx.x;
+  const int span = (ncell + gridDim.x - 1) / gridDim.x;
+  const int lo = blockIdx.x * span, hi = min(ncell, lo + span);
   double v[ACC_MV];
   for (int k = 0; k < ACC_MV; k++) v[k] = 0.0;
-  for (int c = t; c < ncell; c += blockDim.x)
+  for (int c = lo + t; c < hi; c += blockDim.x)
     for (int k = 0; k < ACC_MV; k++) v[k] += partial[(size_t)c * kNacc + k];
   for (int k = 0; k < ACC_MV; k++) sh[k][t] = v[k];
   __syncthreads();
@@ -631,23 +799,33 @@ __global__ void k_reduce(int ncell, const double *__restrict__ partial, int mixe
       for (int k = 0; k < ACC_MV; k++) sh[k][t] += sh[k][t + off];
     __syncthreads();
   }
-  if (t != 0) return;
+  if (t < ACC_MV) red[blockIdx.x * ACC_MV + t] = sh[t][0];
+}
+
+__global__ void k_reduce2(int nred, const double *__restrict__ red, int mixed, double visit,
+                          double c15_1, double c05_3, double *__restrict__ out,
+                          double *__restrict__ pairs_out) {
+  if (threadIdx.x != 0) return;
   double r[ACC_MV];
-  for (int k = 0; k < ACC_MV; k++) r[k] = sh[k][0];
-  const double ec = mixed ? 0.5 * (r[ACC_U] - c15_1 * r[ACC_Q] + c05_3 * r[ACC_R])
-                          : 0.5 * r[ACC_ECOUL];
+  for (int k = 0; k < ACC_MV; k++) r[k] = 0.0;
+  for (int b = 0; b < nred; b++)
+    for (int k = 0; k < ACC_MV; k++) r[k] += red[b * ACC_MV + k];
+  // visit = 1 / (times each pair was evaluated)
+  const double ec = mixed ? visit * (r[ACC_U] - c15_1 * r[ACC_Q] + c05_3 * r[ACC_R])
+                          : visit * r[ACC_ECOUL];
   out[0] = ec;
-  out[1] = 0.5 * r[ACC_ELJ];
+  out[1] = visit * r[ACC_ELJ];
   // symmetric atomic virial from xx xy xz yy yz zz
+  // Both tables hold xx xy xz yy yz zz.  The reference stores the molecular
+  // virial symmetrised from the upper triangle too (ScalarStructure::
+  // addVirial(f, diff, comDiff) adds f_x c_y to both XY and YX,
+  // protomol/src/protomol/type/ScalarStructure.cpp:77-110).
   const int map[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
-  double mv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-  for (int b = 0; b < nmv; b++)
-    for (int k = 0; k < 9; k++) mv[k] += mvpart[b * 9 + k];
   for (int k = 0; k < 9; k++) {
-    out[2 + k] = 0.5 * r[ACC_W + map[k]];
-    out[11 + k] = 0.5 * (r[ACC_W + map[k]] - r[ACC_WI + map[k]]) - mv[k];
+    out[2 + k] = visit * r[ACC_W + map[k]];
+    out[11 + k] = visit * r[ACC_MW + map[k]];
   }
-  if (pairs_out) *pairs_out = 0.5 * r[ACC_PAIRS];
+  if (pairs_out) *pairs_out = visit * r[ACC_PAIRS];
 }
 
 // Leapfrog kick + drift (LeapfrogIntegrator::doKickdoDrift without modifiers,
@@ -662,6 +840,110 @@ __global__ void k_kick_drift(int n, double *__restrict__ pos, double *__restrict
   double v = vel[t] + frc[t] * kick / mass[i];
   vel[t] = v;
   if (drift) pos[t] += v * h;
+}
+
+// ---------------------------------------------------------------------------
+// Rigid water: SETTLE (Miyamoto & Kollman, J. Comput. Chem. 13, 952 (1992)),
+// the analytic constraint of a 3-site water, in FP64.  Canonical triangle
+// about the centre of mass: O (0, ra, 0), H1 (-rc, -rb, 0), H2 (rc, -rb, 0);
+// the new orientation is solved in the frame whose z axis is normal to the
+// old molecular plane.
+// ---------------------------------------------------------------------------
+struct SettleParams {
+  double mo, mh, ra, rb, rc;
+};
+
+__device__ __forceinline__ void d_cross(const double a[3], const double b[3], double o[3]) {
+  o[0] = a[1] * b[2] - a[2] * b[1];
+  o[1] = a[2] * b[0] - a[0] * b[2];
+  o[2] = a[0] * b[1] - a[1] * b[0];
+}
+__device__ __forceinline__ double d_dot(const double a[3], const double b[3]) {
+  return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+}
+__device__ __forceinline__ void d_unit(double a[3]) {
+  const double r = sqrt(d_dot(a, a));
+  a[0] /= r; a[1] /= r; a[2] /= r;
+}
+
+// old: A0 B0 C0 (constrained); in/out: A1 B1 C1 (unconstrained -> constrained)
+__device__ void settle_water(const SettleParams &sp, const double *A0, const double *B0,
+                             const double *C0, double *A1, double *B1, double *C1) {
+  const double M = sp.mo + 2.0 * sp.mh;
+  double com[3], a1[3], b1[3], c1[3], b0[3], c0[3], ex[3], ey[3], ez[3];
+  for (int k = 0; k < 3; k++) {
+    com[k] = (sp.mo * A1[k] + sp.mh * B1[k] + sp.mh * C1[k]) / M;
+    a1[k] = A1[k] - com[k];
+    b1[k] = B1[k] - com[k];
+    c1[k] = C1[k] - com[k];
+    b0[k] = B0[k] - A0[k];
+    c0[k] = C0[k] - A0[k];
+  }
+  d_cross(b0, c0, ez);
+  d_cross(a1, ez, ex);
+  d_cross(ez, ex, ey);
+  d_unit(ex); d_unit(ey); d_unit(ez);
+  const double xb0 = d_dot(ex, b0), yb0 = d_dot(ey, b0);
+  const double xc0 = d_dot(ex, c0), yc0 = d_dot(ey, c0);
+  const double za1 = d_dot(ez, a1);
+  const double xb1 = d_dot(ex, b1), yb1 = d_dot(ey, b1), zb1 = d_dot(ez, b1);
+  const double xc1 = d_dot(ex, c1), yc1 = d_dot(ey, c1), zc1 = d_dot(ez, c1);
+  const double sphi = za1 / sp.ra, cphi = sqrt(1.0 - sphi * sphi);
+  const double spsi = (zb1 - zc1) / (2.0 * sp.rc * cphi), cpsi = sqrt(1.0 - spsi * spsi);
+  const double ya2 = sp.ra * cphi, xb2 = -sp.rc * cpsi;
+  const double t1 = -sp.rb * cphi, t2 = sp.rc * spsi * sphi;
+  const double yb2 = t1 - t2, yc2 = t1 + t2;
+  const double al = xb2 * (xb0 - xc0) + yb0 * yb2 + yc0 * yc2;
+  const double be = xb2 * (yc0 - yb0) + xb0 * yb2 + xc0 * yc2;
+  const double ga = xb0 * yb1 - xb1 * yb0 + xc0 * yc1 - xc1 * yc0;
+  const double ab = al * al + be * be;
+  const double sth = (al * ga - be * sqrt(ab - ga * ga)) / ab, cth = sqrt(1.0 - sth * sth);
+  const double xa3 = -ya2 * sth, ya3 = ya2 * cth, za3 = za1;
+  const double xb3 = xb2 * cth - yb2 * sth, yb3 = xb2 * sth + yb2 * cth, zb3 = zb1;
+  const double xc3 = -xb2 * cth - yc2 * sth, yc3 = -xb2 * sth + yc2 * cth, zc3 = zc1;
+  for (int k = 0; k < 3; k++) {
+    A1[k] = com[k] + xa3 * ex[k] + ya3 * ey[k] + za3 * ez[k];
+    B1[k] = com[k] + xb3 * ex[k] + yb3 * ey[k] + zb3 * ez[k];
+    C1[k] = com[k] + xc3 * ex[k] + yc3 * ey[k] + zc3 * ez[k];
+  }
+}
+
+// Kick + drift with rigid waters: unit u < nwater is a water (one thread:
+// kick, drift, SETTLE, v = (x_new - x_old) / h); the rest are free atoms.
+__global__ void k_kick_drift_settle(int nwater, const int *__restrict__ widx, int nfree,
+                                    const int *__restrict__ fidx, double *__restrict__ pos,
+                                    double *__restrict__ vel, const double *__restrict__ frc,
+                                    const double *__restrict__ mass, double kick, double h,
+                                    SettleParams sp) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u < nwater) {
+    int at[3] = {widx[3 * u], widx[3 * u + 1], widx[3 * u + 2]};
+    double x0[3][3], x1[3][3];
+    for (int a = 0; a < 3; a++) {
+      const int i = at[a];
+      for (int k = 0; k < 3; k++) {
+        const double x = pos[3 * i + k];
+        const double v = vel[3 * i + k] + frc[3 * i + k] * kick / mass[i];
+        x0[a][k] = x;
+        x1[a][k] = x + v * h;
+      }
+    }
+    settle_water(sp, x0[0], x0[1], x0[2], x1[0], x1[1], x1[2]);
+    for (int a = 0; a < 3; a++) {
+      const int i = at[a];
+      for (int k = 0; k < 3; k++) {
+        pos[3 * i + k] = x1[a][k];
+        vel[3 * i + k] = (x1[a][k] - x0[a][k]) / h;
+      }
+    }
+  } else if (u < nwater + nfree) {
+    const int i = fidx[u - nwater];
+    for (int k = 0; k < 3; k++) {
+      const double v = vel[3 * i + k] + frc[3 * i + k] * kick / mass[i];
+      vel[3 * i + k] = v;
+      pos[3 * i + k] += v * h;
+    }
+  }
 }
 
 // FP32 FMA throughput probe: 8 independent FMA chains per thread.

@@ -190,8 +190,9 @@ class NonbondedCutoffB200SystemForce:
             self._box_key = None
         bkey = (topo.e.tobytes(), topo.origin.tobytes())
         if self._box_key != bkey:
-            self._check(L.pmb200_set_box(self._ctx, _ptr(topo.e[0].copy()), _ptr(topo.e[1].copy()),
-                                         _ptr(topo.e[2].copy()), _ptr(topo.origin)))
+            e1, e2, e3 = (np.ascontiguousarray(topo.e[k]) for k in range(3))
+            self._check(L.pmb200_set_box(self._ctx, _ptr(e1), _ptr(e2), _ptr(e3),
+                                         _ptr(topo.origin)))
             self._box_key = bkey
 
     def uncache(self):
@@ -247,6 +248,14 @@ class NonbondedCutoffB200SystemForce:
         self._check(_lib.lib().pmb200_step_device(
             self._ctx, _P(pos_ptr), _P(vel_ptr), _P(force_ptr), _P(out_ptr) if out_ptr else None,
             float(dt_fs), int(flags), _P(stream)))
+
+    def set_rigid_waters(self, topo, widx, d_oh, d_hh):
+        """SETTLE constraints for the device integrator (see pmb200.h)."""
+        self._ensure(topo)
+        w = np.ascontiguousarray(widx, dtype=np.int32).reshape(-1)
+        self._check(_lib.lib().pmb200_set_rigid_waters(self._ctx, w.size // 3,
+                                                       _ptr(w) if w.size else None,
+                                                       float(d_oh), float(d_hh)))
 
     def set_kernel_timing(self, on):
         self._check(_lib.lib().pmb200_set_kernel_timing(self._ctx, 1 if on else 0))

@@ -155,6 +155,25 @@ def water_box(k: int, *, rc: float, ron: float, seed: int = 1234,
     )
 
 
+D_OH = R_OH
+D_HH = 2.0 * R_OH * math.sin(0.5 * THETA_HOH)
+
+
+def rigid_waters(sysd) -> np.ndarray:
+    """(O, H1, H2) atom triples of every 3-atom O-H-H molecule, for the
+    rigid-water (SETTLE) integrator; constraint lengths D_OH and D_HH."""
+    mol = np.asarray(sysd["mol"])
+    typ = np.asarray(sysd["type"])
+    order = np.argsort(mol, kind="stable")
+    bounds = np.flatnonzero(np.diff(np.r_[-1, mol[order], mol.max() + 1 if mol.size else 0]))
+    out = []
+    for a, b in zip(bounds[:-1], bounds[1:]):
+        atoms = order[a:b]
+        if len(atoms) == 3 and typ[atoms[0]] == T_O and (typ[atoms[1:]] == T_H).all():
+            out.append(atoms)
+    return np.asarray(out, dtype=np.int32).reshape(-1, 3)
+
+
 # Named workloads (sizes from the reference-facing benchmark definitions).
 def small_648(seed=1234):
     """216 waters, 6^3 lattice, box 18.624 A, rc 8, C2 from 7."""

@@ -90,3 +90,16 @@ def test_ion_box_and_batch():
 def test_topology_wrapper(water648):
     t = PeriodicTopology.from_dict(water648)
     assert t.n == 648 and t.ntypes == 2 and t.e.shape == (3, 3)
+
+
+def test_host_kick_drift_matches_numpy_settle():
+    from protomoladdon_b200 import rigid
+    s = water.small_648()
+    w = water.rigid_waters(s)
+    rng = np.random.default_rng(1)
+    F = rng.normal(0, 20, s["pos"].shape)
+    p1, v1 = s["pos"].copy(), s["vel"].copy()
+    p2, v2 = s["pos"].copy(), s["vel"].copy()
+    rigid.kick_drift_settle(p1, v1, F, s["mass"], 1.0, w, water.D_OH, water.D_HH)
+    rigid.host_kick_drift(p2, v2, F, s["mass"], 1.0, w, water.D_OH, water.D_HH)
+    assert np.abs(p1 - p2).max() < 1e-12 and np.abs(v1 - v2).max() < 1e-9

@@ -99,3 +99,43 @@ def test_pair_count_small(water648):
     n = O.restate_count_pairs(water648, water648["pos"])
     # ~0.5 * rho * 4/3 pi rc^3 per atom for the 648-atom box at rc 8
     assert 60_000 < n < 80_000
+
+
+def test_settle_constraints_and_shake_agreement():
+    from protomoladdon_b200 import rigid
+    s = water.small_648()
+    w = water.rigid_waters(s)
+    assert w.shape == (216, 3)
+    rng = np.random.default_rng(0)
+    old = s["pos"]
+    new = old + rng.normal(0, 0.02, old.shape)
+    out = O.restate_settle(w, s["mass"], water.D_OH, water.D_HH, old, new)
+    d = out[w]
+    assert np.abs(np.linalg.norm(d[:, 1] - d[:, 0], axis=1) - water.D_OH).max() < 1e-12
+    assert np.abs(np.linalg.norm(d[:, 2] - d[:, 0], axis=1) - water.D_OH).max() < 1e-12
+    assert np.abs(np.linalg.norm(d[:, 2] - d[:, 1], axis=1) - water.D_HH).max() < 1e-12
+    m = s["mass"][w][..., None]
+    assert np.abs((m * (out[w] - new[w])).sum(1)).max() < 1e-12  # momentum kept
+    # an iterative SHAKE on the same three constraints converges to SETTLE's answer
+    x = new.copy()
+    for _ in range(400):
+        for a, b, d0 in ((0, 1, water.D_OH), (0, 2, water.D_OH), (1, 2, water.D_HH)):
+            ia, ib = w[:, a], w[:, b]
+            r, r0 = x[ib] - x[ia], old[ib] - old[ia]
+            ma, mb = s["mass"][ia], s["mass"][ib]
+            g = (d0 * d0 - (r * r).sum(1)) / (2 * (r * r0).sum(1) * (1 / ma + 1 / mb))
+            x[ia] -= (g / ma)[:, None] * r0
+            x[ib] += (g / mb)[:, None] * r0
+    assert np.abs(x[w] - out[w]).max() < 1e-10
+    # the host copy used by host-side integrators agrees
+    host = rigid.settle(w, s["mass"], water.D_OH, water.D_HH, old, new.copy())
+    assert np.abs(host - out).max() < 1e-12
+
+
+def test_rigid_leapfrog_keeps_geometry(water648):
+    w = water.rigid_waters(water648)
+    p, v, e = O.restate_leapfrog_rigid(water648, water648["pos"], water648["vel"], 1.0, 10, w,
+                                       water.D_OH, water.D_HH)
+    d = p[w]
+    assert np.abs(np.linalg.norm(d[:, 1] - d[:, 0], axis=1) - water.D_OH).max() < 1e-10
+    assert np.isfinite(e).all()

@@ -206,3 +206,60 @@ def test_device_path_equals_host_path(water648):
     o = out.cpu().numpy()
     assert o[0] == E[0] and o[1] == E[1]
     assert np.array_equal(o[2:11], E.virial_matrix().ravel())
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-9), ("mixed", 1e-5)])
+def test_rigid_leapfrog_device_vs_oracle(water648, precision, tol):
+    """SETTLE-constrained leapfrog on the device against the oracle's."""
+    import torch
+    d = water648
+    w = water.rigid_waters(d)
+    p_ref, v_ref, e_ref = O.restate_leapfrog_rigid(d, d["pos"], d["vel"], 1.0, 20, w,
+                                                   water.D_OH, water.D_HH)
+    topo = PeriodicTopology.from_dict(d)
+    f = NonbondedCutoffB200SystemForce(d["ron"], d["rc_lj"], d["rc_coul"], d["rc_alg"],
+                                       precision=precision)
+    f.set_rigid_waters(topo, w, water.D_OH, water.D_HH)
+    dev = torch.device("cuda:0")
+    pos = torch.tensor(d["pos"], dtype=torch.float64, device=dev)
+    vel = torch.tensor(d["vel"], dtype=torch.float64, device=dev)
+    frc = torch.zeros_like(pos)
+    out = torch.zeros(20, dtype=torch.float64, device=dev)
+    f.leapfrog_device(topo, pos.data_ptr(), vel.data_ptr(), frc.data_ptr(), 1.0, 20,
+                      out.data_ptr(), _lib.PMB200_ENERGY)
+    f.sync()
+    p, v = pos.cpu().numpy(), vel.cpu().numpy()
+    f.close()
+    x = p[w]
+    assert np.abs(np.linalg.norm(x[:, 1] - x[:, 0], axis=1) - water.D_OH).max() < 1e-10
+    assert np.abs(np.linalg.norm(x[:, 2] - x[:, 1], axis=1) - water.D_HH).max() < 1e-10
+    assert np.abs(p - p_ref).max() <= tol
+    assert rms_rel(v, v_ref) <= 10 * tol
+    assert np.allclose(out.cpu().numpy()[:2], e_ref, rtol=0, atol=5e-3)
+
+
+def test_step_device_matches_leapfrog_body(water648):
+    """pmb200_step_device (graph replay) equals kick + drift + SETTLE + force."""
+    import torch
+    d = water648
+    w = water.rigid_waters(d)
+    topo = PeriodicTopology.from_dict(d)
+    f = NonbondedCutoffB200SystemForce(d["ron"], d["rc_lj"], d["rc_coul"], d["rc_alg"],
+                                       precision="fp64")
+    f.set_rigid_waters(topo, w, water.D_OH, water.D_HH)
+    st = torch.cuda.Stream()
+    pos = torch.tensor(d["pos"], dtype=torch.float64, device="cuda:0")
+    vel = torch.tensor(d["vel"], dtype=torch.float64, device="cuda:0")
+    frc = torch.tensor(d["ref_forces"], dtype=torch.float64, device="cuda:0")
+    for _ in range(3):
+        f.step_device(topo, pos.data_ptr(), vel.data_ptr(), frc.data_ptr(), 1.0, st.cuda_stream)
+    st.synchronize()
+    f.sync()
+    from protomoladdon_b200 import rigid
+    P, V, F = d["pos"].copy(), d["vel"].copy(), d["ref_forces"].copy()
+    for _ in range(3):
+        rigid.kick_drift_settle(P, V, F, d["mass"], 1.0, w, water.D_OH, water.D_HH)
+        F, _, _, _ = O.restate_eval(d, P, 0)
+    f.close()
+    assert np.abs(pos.cpu().numpy() - P).max() < 1e-10
+    assert rms_rel(frc.cpu().numpy(), F) < 1e-11
