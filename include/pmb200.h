@@ -191,6 +191,37 @@ int pmb200_host_kick_drift(int n, double *pos, double *vel,
  * are bounded by this pipe, not by HBM or tensor cores. */
 int pmb200_measure_fp32_peak(int device, double *tflops);
 
+/* Mixed-precision evaluation that allocates no memory (no counterpart in the
+ * reference: ProtoMol's force owns heap-allocated cell lists).  For callers
+ * that must not allocate device memory -- hosts that give all device memory
+ * to their own pool allocator and forbid libraries to take more, or that
+ * cannot afford cudaFree's implicit device synchronisation inside a time
+ * step.  It needs no pmb200_ctx: every input and output is the caller's,
+ * and the scratch (cell lists, sorted copies, fixed-point accumulators,
+ * partial sums) lives in one statically sized device array inside the
+ * library, held on every device that loads it until the process exits.
+ *
+ * Limits: n <= 32768 atoms and at most 8192 grid cells (PMB200_ENOMEM
+ * beyond either), at most 16 LJ types, precision PMB200_MIXED only.
+ * Inputs: device arrays d_pos[3n], d_type[n], d_q[n] (scaledCharge),
+ * d_mol[n], and the exclusions as per-atom lists sorted by partner:
+ * d_ex_start[n+1] offsets into d_ex, which holds int pairs {partner atom,
+ * kind} (kind 1 = modified, 2 = full; each pair listed under both of its
+ * atoms; 8-byte aligned); host arrays lj[ntypes^2*4]
+ * {A, B, A14, B14}, box[3] (orthogonal edges), origin[3].  Outputs:
+ * d_forces[3n] is OVERWRITTEN with this evaluation's forces; d_energy[2]
+ * (may be NULL) receives {COULOMB, LENNARDJONES}.  Work is queued on
+ * `stream`; the first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) and should come before any stream capture.  Every
+ * call shares the one array, so calls whose GPU work overlaps (different
+ * streams, threads or processes sharing a context) race; serialise them. */
+int pmb200_eval_noalloc(const pmb200_params *params, int n, const double *d_pos,
+                        const int *d_type, const double *d_q, const int *d_mol,
+                        const int *d_ex_start, const int *d_ex, int ntypes,
+                        const double *lj, double coulomb_scaling,
+                        const double box[3], const double origin[3],
+                        double *d_forces, double *d_energy, void *stream);
+
 /* Geometry of the device cell grid chosen for the current box. */
 int pmb200_grid(const pmb200_ctx *ctx, int dims[3], double edge[3]);
 

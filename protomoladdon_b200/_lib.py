@@ -34,6 +34,7 @@ EXPORTED = (
     "pmb200_leapfrog_device", "pmb200_last_pair_count", "pmb200_grid",
     "pmb200_step_device", "pmb200_set_kernel_timing", "pmb200_last_kernel_ms",
     "pmb200_measure_fp32_peak", "pmb200_set_rigid_waters", "pmb200_host_kick_drift",
+    "pmb200_eval_noalloc",
 )
 
 _P = ctypes.c_void_p
@@ -83,6 +84,8 @@ def lib():
     L.pmb200_measure_fp32_peak.argtypes = [_I, ctypes.POINTER(_D)]
     L.pmb200_set_rigid_waters.argtypes = [_P, _I, _P, _D, _D]
     L.pmb200_host_kick_drift.argtypes = [_I, _P, _P, _P, _P, _D, _D, _I, _P, _D, _D]
+    L.pmb200_eval_noalloc.argtypes = [ctypes.POINTER(Params), _I, _P, _P, _P, _P, _P, _P, _I, _P,
+                                      _D, _P, _P, _P, _P, _P]
     for name in EXPORTED:
         getattr(L, name).restype = getattr(L, name).restype or _I
     L.pmb200_last_error.restype = ctypes.c_char_p

@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <utility>
 #include <vector>
@@ -911,6 +912,211 @@ int pmb200_measure_fp32_peak(int device, double *tflops) {
   cudaFree(sink);
   const double flops = 2.0 * 8.0 * 16.0 * (double)iters * threads * blocks;
   *tflops = flops / (ms * 1e-3) / 1e12;
+  return PMB200_OK;
+}
+
+// ---------------------------------------------------------------------------
+// pmb200_eval_noalloc: the mixed-precision evaluation with every piece of
+// scratch memory in one file-scope device array instead of cudaMalloc'd
+// context buffers.  It exists for callers that must not allocate device
+// memory: hosts that hand all device memory to their own pool allocator and
+// forbid libraries to take more, or that cannot afford cudaFree's implicit
+// device synchronisation inside their time step.  The array is sized for at
+// most kNoAllocAtoms atoms and kNoAllocCells cells and stays resident on
+// every device that loads this library until the process exits.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kNoAllocAtoms = 32768;
+constexpr int kNoAllocCells = 8192;
+
+constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+struct NoAllocLayout {  // byte offsets inside the scratch array
+  static constexpr size_t count = 0;
+  static constexpr size_t start = align256(count + sizeof(int) * kNoAllocCells);
+  static constexpr size_t partial = align256(start + sizeof(int) * (kNoAllocCells + 1));
+  static constexpr size_t cell_of = align256(partial + sizeof(double) * kNoAllocCells * kNacc);
+  static constexpr size_t slot = align256(cell_of + sizeof(int) * kNoAllocAtoms);
+  static constexpr size_t tmp = align256(slot + sizeof(int) * kNoAllocAtoms);
+  static constexpr size_t sidx = align256(tmp + sizeof(int) * kNoAllocAtoms);
+  static constexpr size_t rel32 = align256(sidx + sizeof(int) * kNoAllocAtoms);
+  static constexpr size_t spos32 = align256(rel32 + sizeof(float4) * kNoAllocAtoms);
+  static constexpr size_t smeta = align256(spos32 + sizeof(float4) * kNoAllocAtoms);
+  static constexpr size_t facc = align256(smeta + sizeof(int2) * kNoAllocAtoms);
+  static constexpr size_t red = align256(facc + sizeof(unsigned long long) * 3 * kNoAllocAtoms);
+  static constexpr size_t lj32 = align256(red + sizeof(double) * kRedBlocks * ACC_MV);
+  static constexpr size_t pairs = align256(lj32 + sizeof(float4) * kMaxTypes * kMaxTypes);
+  static constexpr size_t err = align256(pairs + sizeof(double));
+  static constexpr size_t total = align256(err + sizeof(int));
+};
+
+// The scratch array itself.  Host code must not pass its name to a kernel
+// (on the host it names a stand-in, not device memory); the device address
+// comes from cudaGetSymbolAddress below.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NoAllocLayout::total];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void *g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on the current device, looked up once
+// per device.
+cudaError_t noalloc_scratch(unsigned char **out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_addr[dev]) {
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    g_noalloc_addr[dev] = p;
+  }
+  *out = (unsigned char *)g_noalloc_addr[dev];
+  return cudaSuccess;
+}
+
+}  // namespace
+
+extern "C" int pmb200_eval_noalloc(const pmb200_params *p, int n, const double *d_pos,
+                                   const int *d_type, const double *d_q, const int *d_mol,
+                                   const int *d_ex_start, const int *d_ex_pairs, int ntypes,
+                                   const double *lj, double coulomb_scaling, const double box[3],
+                                   const double origin[3], double *d_forces, double *d_energy,
+                                   void *stream) {
+  // argument checks first: nothing reaches the device for a rejected call
+  if (!p || !box || !origin || !lj) return PMB200_EINVAL;
+  if (p->precision != PMB200_MIXED) return PMB200_EUNSUPPORTED;
+  if (!(p->switchon >= 0.0) || !(p->cutoff_lj > 0.0) || !(p->switchon < p->cutoff_lj) ||
+      !(p->cutoff_coul > 0.0) || !(p->cutoff_alg > 0.0))
+    return PMB200_EINVAL;
+  if (p->cutoff_alg < rc_max(*p)) return PMB200_EUNSUPPORTED;
+  if (n < 0 || n > kNoAllocAtoms) return PMB200_ENOMEM;  // beyond the fixed scratch
+  if (ntypes <= 0 || ntypes > kMaxTypes) return PMB200_EUNSUPPORTED;
+  if (n > 0 && (!d_pos || !d_type || !d_q || !d_mol || !d_ex_start || !d_ex_pairs || !d_forces))
+    return PMB200_EINVAL;
+  if (((uintptr_t)d_ex_pairs & 7u) != 0) return PMB200_EINVAL;  // read as int2
+  const int2 *d_ex = (const int2 *)d_ex_pairs;
+  const double rc = rc_max(*p);
+  double L[3], edge[3];
+  int nd[3];
+  const double target = p->cellsize > 0.0 ? std::max(p->cellsize, rc / 3.0) : rc / 2.0;
+  for (int a = 0; a < 3; a++) {
+    L[a] = box[a];
+    if (!(L[a] > 0.0) || !std::isfinite(L[a]) || !std::isfinite(origin[a])) return PMB200_EINVAL;
+    if (L[a] < 2.0 * rc) return PMB200_EUNSUPPORTED;
+    nd[a] = std::max(1, (int)std::floor(L[a] / target));
+    edge[a] = L[a] / nd[a];
+  }
+  const long long ncell = (long long)nd[0] * nd[1] * nd[2];
+  if (ncell > kNoAllocCells) return PMB200_ENOMEM;  // beyond the fixed scratch
+  GridParams g{};
+  g.nx = nd[0]; g.ny = nd[1]; g.nz = nd[2];
+  g.ncell = (int)ncell;
+  for (int a = 0; a < 3; a++) {
+    g.edge[a] = edge[a];
+    g.boxlen[a] = L[a];
+    g.boxmin[a] = origin[a] - 0.5 * L[a];
+  }
+  g.unit = edge[0];
+  // half-shell neighbour cells (same rule as pmb200_set_box)
+  HalfStencil half{};
+  {
+    int R[3];
+    for (int a = 0; a < 3; a++) R[a] = (int)std::ceil(rc / edge[a] - 1e-12);
+    const double rc2 = rc * rc * (1.0 + 1e-12);
+    for (int dz = 0; dz <= R[2]; dz++)
+      for (int dy = (dz == 0 ? 0 : -R[1]); dy <= R[1]; dy++) {
+        const double yz = std::pow(std::max(std::abs(dy) - 1, 0) * edge[1], 2) +
+                          std::pow(std::max(std::abs(dz) - 1, 0) * edge[2], 2);
+        if (yz > rc2) continue;
+        int hi = 0;
+        for (int dx = 0; dx <= R[0]; dx++)
+          if (yz + std::pow(std::max(dx - 1, 0) * edge[0], 2) <= rc2) hi = dx;
+        for (int dx = (dz == 0 && dy == 0) ? 0 : -hi; dx <= hi; dx++) {
+          if (half.ncells >= kMaxHalfCells || hi > 8 || std::abs(dy) > 8 || dz > 8)
+            return PMB200_EUNSUPPORTED;
+          half.off[half.ncells++] = (unsigned short)((dx + 8) | ((dy + 8) << 5) | ((dz + 8) << 10));
+        }
+      }
+  }
+  const double u = g.unit;
+  const double rl = p->cutoff_lj / u, ro = p->switchon / u, rq = p->cutoff_coul / u;
+  const double t = rl * rl - ro * ro;
+  MixedConsts mc{};
+  mc.cut2 = (float)((rc / u) * (rc / u));
+  mc.rclj2 = (float)(rl * rl);
+  mc.ron2 = (float)(ro * ro);
+  mc.rcc2 = (float)(rq * rq);
+  mc.s1 = (float)(1.0 / (t * t * t));
+  mc.s2 = (float)(rl * rl - 3.0 * ro * ro);
+  mc.s3 = (float)(4.0 / (t * t * t));
+  mc.c15_1 = (float)(1.5 / rq);
+  mc.c05_3 = (float)(0.5 / (rq * rq * rq));
+  mc.c15_3 = (float)(1.5 / (rq * rq * rq));
+  mc.csf = (float)coulomb_scaling;
+  mc.ey = (float)(edge[1] / u);
+  mc.ez = (float)(edge[2] / u);
+  float4 lj32[kMaxTypes * kMaxTypes];
+  const double u6 = std::pow(u, 6.0), u12 = u6 * u6;
+  for (int k = 0; k < ntypes * ntypes; k++)
+    lj32[k] = make_float4((float)(lj[4 * k] / u12), (float)(lj[4 * k + 1] / u6),
+                          (float)(lj[4 * k + 2] / u12), (float)(lj[4 * k + 3] / u6));
+
+  cudaError_t e = cudaSuccess;
+  unsigned char *base = nullptr;
+  if ((e = noalloc_scratch(&base)) != cudaSuccess) return PMB200_ECUDA;
+  using Lo = NoAllocLayout;
+  int *count = (int *)(base + Lo::count);
+  int *start = (int *)(base + Lo::start);
+  double *partial = (double *)(base + Lo::partial);
+  int *cell_of = (int *)(base + Lo::cell_of);
+  int *slot = (int *)(base + Lo::slot);
+  int *tmp = (int *)(base + Lo::tmp);
+  int *sidx = (int *)(base + Lo::sidx);
+  float4 *rel32 = (float4 *)(base + Lo::rel32);
+  float4 *spos32 = (float4 *)(base + Lo::spos32);
+  int2 *smeta = (int2 *)(base + Lo::smeta);
+  unsigned long long *facc = (unsigned long long *)(base + Lo::facc);
+  double *red = (double *)(base + Lo::red);
+  float4 *dlj = (float4 *)(base + Lo::lj32);
+  double *pairs = (double *)(base + Lo::pairs);
+  int *err = (int *)(base + Lo::err);
+  cudaStream_t st = (cudaStream_t)stream;
+  // the array keeps the previous call's contents: zero what accumulates
+  e = cudaMemcpyAsync(dlj, lj32, sizeof(float4) * ntypes * ntypes, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(count, 0, sizeof(int) * g.ncell, st);
+  if (e == cudaSuccess && n > 0)
+    e = cudaMemsetAsync(facc, 0, sizeof(unsigned long long) * 3 * (size_t)n, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, sizeof(int), st);
+  if (e != cudaSuccess) return PMB200_ECUDA;
+  const PbcRef pb{};
+  if (n > 0)
+    k_cell_index<<<(n + 255) / 256, 256, 0, st>>>(n, d_pos, g, cell_of, count, slot, rel32,
+                                                   nullptr, d_q, (float)(1.0 / std::sqrt(u)),
+                                                   err);
+  k_scan<<<1, 1024, 1024 * sizeof(int), st>>>(g.ncell, count, start);
+  if (n > 0) k_scatter<<<(n + 255) / 256, 256, 0, st>>>(n, cell_of, slot, start, tmp);
+  k_rank_gather<<<(g.ncell + 3) / 4, 128, 0, st>>>(g.ncell, start, tmp, rel32, nullptr, d_type,
+                                                    d_mol, sidx, spos32, nullptr, smeta);
+  if (d_energy)
+    k_pair_mixed<true, false, false><<<g.ncell, 32 * kWarps, 0, st>>>(
+        g, mc, half, ntypes, dlj, start, spos32, smeta, sidx, d_ex_start, d_ex, facc, n, err,
+        partial, pb, nullptr);
+  else
+    k_pair_mixed<false, false, false><<<g.ncell, 32 * kWarps, 0, st>>>(
+        g, mc, half, ntypes, dlj, start, spos32, smeta, sidx, d_ex_start, d_ex, facc, n, err,
+        partial, pb, nullptr);
+  if (n > 0)
+    k_finalize<<<(n + 255) / 256, 256, 0, st>>>(n, facc, sidx, kFixInv / u, 0, d_forces);
+  if (d_energy) {
+    k_reduce1<<<kRedBlocks, 256, 0, st>>>(g.ncell, partial, red);
+    k_reduce2<<<1, 32, 0, st>>>(kRedBlocks, red, 1, 1.0, 1.5 / rq, 0.5 / (rq * rq * rq),
+                                d_energy, pairs);
+  }
+  if (cudaGetLastError() != cudaSuccess) return PMB200_ECUDA;
   return PMB200_OK;
 }
 
