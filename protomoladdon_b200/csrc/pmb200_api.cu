@@ -500,6 +500,17 @@ int pmb200_set_box(pmb200_ctx *c, const double e1[3], const double e2[3], const 
       c->half.off[c->half.ncells++] =
           (unsigned short)((dx + 8) | ((rw.dy + 8) << 5) | ((rw.dz + 8) << 10));
     }
+  // Fixed pseudo-random order: consecutive cells of a warp's share then lie
+  // in different directions, so each staged batch holds a similar number of
+  // in-range partners for every i atom and the per-lane lists stay balanced.
+  {
+    unsigned long long x = 0x9E3779B97F4A7C15ull;
+    for (int k = c->half.ncells - 1; k > 0; k--) {
+      x = x * 6364136223846793005ull + 1442695040888963407ull;
+      const int r = (int)((x >> 33) % (unsigned long long)(k + 1));
+      std::swap(c->half.off[k], c->half.off[r]);
+    }
+  }
   if (c->ncell_alloc < g.ncell) {
     CK(dalloc(c->d_count, (size_t)g.ncell));
     CK(dalloc(c->d_start, (size_t)g.ncell + 1));

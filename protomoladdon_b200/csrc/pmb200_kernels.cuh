@@ -504,35 +504,79 @@ k_pair_mixed(GridParams g, MixedConsts mc, const HalfStencil st, int ntypes, con
       __syncwarp();
     };
 
-    // this warp's share of the half-shell cells, dealt round-robin
-    for (int q = warp; q < st.ncells; q += kWarps) {
-      const unsigned o = st.off[q];
-      const int dx = (int)(o & 31u) - 8, dy = (int)((o >> 5) & 31u) - 8,
-                dz = (int)((o >> 10) & 31u) - 8;
-      const bool home = (dx | dy | dz) == 0;
-      int jx = (cx + dx) % g.nx; jx += (jx < 0) ? g.nx : 0;
-      int jy = (cy + dy) % g.ny; jy += (jy < 0) ? g.ny : 0;
-      int jz = (cz + dz) % g.nz; jz += (jz < 0) ? g.nz : 0;
-      const int jc = (jz * g.ny + jy) * g.nx + jx;
-      int js = start[jc];
-      const int je = start[jc + 1];
-      const float sx = (float)dx, sy = (float)dy * mc.ey, sz = (float)dz * mc.ez;
-      while (js < je) {
-        const int take = min(je - js, batch_cap - nb);
-        for (int t = lane; t < take; t += 32) {
-          float4 p = spos[js + t];
-          p.x += sx; p.y += sy; p.z += sz;
-          sm.pos[nb + t] = p;
-          sm.meta[nb + t] = smeta[js + t];
-          sm.gidx[nb + t] = js + t;
+    // This warp's share of the half-shell cells (dealt round-robin), taken
+    // 32 at a time: each lane fetches one cell's atom range, a warp prefix sum
+    // lays the cells end to end, and every batch is loaded with independent
+    // loads (a binary search over the prefix finds each entry's cell), so the
+    // L2 latency is paid once per batch rather than once per cell.
+    const int nmine = warp < st.ncells ? (st.ncells - warp + kWarps - 1) / kWarps : 0;
+    for (int g0 = 0; g0 < nmine; g0 += 32) {
+      const int myq = g0 + lane;
+      int cjs = 0, ccnt = 0;
+      float csx = 0.f, csy = 0.f, csz = 0.f;
+      bool chome = false;
+      if (myq < nmine) {
+        const unsigned o = st.off[warp + myq * kWarps];
+        const int dx = (int)(o & 31u) - 8, dy = (int)((o >> 5) & 31u) - 8,
+                  dz = (int)((o >> 10) & 31u) - 8;
+        chome = (dx | dy | dz) == 0;
+        int jx = (cx + dx) % g.nx; jx += (jx < 0) ? g.nx : 0;
+        int jy = (cy + dy) % g.ny; jy += (jy < 0) ? g.ny : 0;
+        int jz = (cz + dz) % g.nz; jz += (jz < 0) ? g.nz : 0;
+        const int jc = (jz * g.ny + jy) * g.nx + jx;
+        cjs = start[jc];
+        ccnt = start[jc + 1] - cjs;
+        csx = (float)dx; csy = (float)dy * mc.ey; csz = (float)dz * mc.ez;
+      }
+      int incl = ccnt;  // inclusive prefix of the cells' atom counts
+      for (int off = 1; off < 32; off <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) incl += v;
+      }
+      const int total = __shfl_sync(0xffffffffu, incl, 31);
+      const int excl = incl - ccnt;
+      const unsigned hmask = __ballot_sync(0xffffffffu, chome && ccnt > 0);
+      int h_excl = 0, h_cnt = 0, h_js = 0;
+      if (hmask) {
+        const int hl = __ffs(hmask) - 1;
+        h_excl = __shfl_sync(0xffffffffu, excl, hl);
+        h_cnt = __shfl_sync(0xffffffffu, ccnt, hl);
+        h_js = __shfl_sync(0xffffffffu, cjs, hl);
+      }
+      for (int f0 = 0; f0 < total;) {
+        const int take = min(total - f0, batch_cap - nb);
+        for (int r = 0; r < take; r += 32) {
+          const int t = r + lane;
+          const int f = f0 + t;
+          int c = 0;  // number of cells ending at or before f = f's cell
+          for (int step = 16; step > 0; step >>= 1) {
+            const int v = __shfl_sync(0xffffffffu, incl, c + step - 1);
+            if (v <= f) c += step;
+          }
+          const int js_c = __shfl_sync(0xffffffffu, cjs, c);
+          const int ex_c = __shfl_sync(0xffffffffu, excl, c);
+          const float sx = __shfl_sync(0xffffffffu, csx, c);
+          const float sy = __shfl_sync(0xffffffffu, csy, c);
+          const float sz = __shfl_sync(0xffffffffu, csz, c);
+          if (t < take) {
+            const int jg = js_c + (f - ex_c);
+            float4 p = spos[jg];
+            p.x += sx; p.y += sy; p.z += sz;
+            sm.pos[nb + t] = p;
+            sm.meta[nb + t] = smeta[jg];
+            sm.gidx[nb + t] = jg;
+          }
         }
-        if (home) {  // staged home-cell atoms: sorted js .. js+take-1
-          home_lo = nb;
-          home_hi = nb + take;
-          home_base = js;
+        if (hmask) {  // the part of the home cell staged in this batch
+          const int a = max(h_excl, f0), b = min(h_excl + h_cnt, f0 + take);
+          if (a < b) {
+            home_lo = nb + (a - f0);
+            home_hi = nb + (b - f0);
+            home_base = h_js + (a - h_excl);
+          }
         }
         nb += take;
-        js += take;
+        f0 += take;
         if (nb == batch_cap) flush_batch();
       }
     }

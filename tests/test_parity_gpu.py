@@ -186,7 +186,10 @@ def test_leapfrog_device_vs_reference(water648, precision, tol):
     assert np.abs(p - d["lf20_pos"]).max() <= tol * 10
     assert rms_rel(v, d["lf20_vel"]) <= tol * 10
     e = out.cpu().numpy()[:2]
-    assert np.allclose(e, d["lf20_energies"], rtol=0, atol=5e-3)
+    # unconstrained hydrogens collapse onto neighbouring oxygens in 20 fs, so
+    # the final Coulomb energy is ~1e4; mixed: 2e-6 relative, FP64: 5e-3 abs
+    rtol = 2e-6 if precision == "mixed" else 0.0
+    assert np.allclose(e, d["lf20_energies"], rtol=rtol, atol=5e-3)
 
 
 def test_device_path_equals_host_path(water648):
