@@ -193,7 +193,7 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 def run_ours(args):
     import torch
-    from protomoladdon_b200 import _lib, water
+    from protomoladdon_b200 import _lib, replicas, water
     from protomoladdon_b200.force import (NonbondedCutoffB200SystemForce, PeriodicTopology,
                                           ScalarStructure)
     world = env_int("WORLD_SIZE", 1)
@@ -207,7 +207,7 @@ def run_ours(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    s = water.medium_41k(seed=1234 + rank)
+    s = water.medium_41k(seed=replicas.replica_seed(1234, rank))
     n = s["n"]
     widx = water.rigid_waters(s)
     topo = PeriodicTopology.from_dict(s)
@@ -325,12 +325,9 @@ def run_ours(args):
     tot_ms = sum(step_ms)
     mean_k = statistics.mean(kms)
     e2e_s = sum(e2e_t) / len(e2e_t)
-    if dist is not None:
-        t = torch.tensor([tot_ms, e2e_s, mean_k], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tot_ms, e2e_s, mean_k = (float(x) for x in t.tolist())
+    tot_ms, e2e_s, mean_k = replicas.max_over_ranks([tot_ms, e2e_s, mean_k], dist, dev)
     ms_step = tot_ms / args.steps
-    value = world * ns_per_day(ms_step * 1e-3)
+    value = replicas.aggregate_ns_per_day(ms_step, world, DT_FS)
 
     if rank == 0:
         peak = ctypes_peak(local)
@@ -357,7 +354,7 @@ def run_ours(args):
                                  "peak_gbs": measured_hbm()}},
             "e2e": {"value": world * ns_per_day(e2e_s), "unit": "ns/day",
                     "ms_per_step": e2e_s * 1e3,
-                    "h2d_bytes_per_step": 2 * 24 * n, "d2h_bytes_per_step": 24 * n + 160},
+                    "h2d_bytes_per_step": 24 * n, "d2h_bytes_per_step": 24 * n + 160},
             "gpu_launches": KERNELS_PER_STEP * args.steps,
             "clocks": clocks,
         }
