@@ -114,6 +114,10 @@ void *pmref_create(int n, const int *type, const double *qscaled,
   return s;
 }
 
+// The Topology<PeriodicBoundaryConditions, CubicCellManager> built by
+// pmref_create (for test harnesses that evaluate other forces on it).
+void *pmref_topology(void *h) { return ((pmref_sys *)h)->topo; }
+
 void pmref_destroy(void *h) {
   pmref_sys *s = (pmref_sys *)h;
   delete s->force;

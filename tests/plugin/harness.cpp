@@ -1,0 +1,98 @@
+// Test harness: the B200 plugin force inside the reference's own
+// ForceFactory, next to the reference prototype, on a reference-built
+// Topology.  Built by tests/plugin/Makefile against the reference library
+// compiled under oracle/_ref; used only by tests/test_plugin_gpu.py.
+#include "B200CutoffSystemForce.h"
+#include "B200ForceModule.h"
+
+#include <protomol/factory/ForceFactory.h>
+#include <protomol/force/nonbonded/NonbondedCutoffSystemForce.h>
+#include <protomol/force/OneAtomPairTwo.h>
+#include <protomol/force/LennardJonesForce.h>
+#include <protomol/force/CoulombForce.h>
+#include <protomol/switch/C1SwitchingFunction.h>
+#include <protomol/switch/C2SwitchingFunction.h>
+#include <protomol/topology/CellListEnumeratorPeriodicBoundaries.h>
+#include <protomol/topology/TopologyUtilities.h>
+#include <protomol/config/Value.h>
+
+#include <cstring>
+#include <exception>
+#include <string>
+
+using namespace ProtoMol;
+
+extern "C" void *pmref_topology(void *h);
+
+typedef Topology<PeriodicBoundaryConditions, CubicCellManager> PTopo;
+typedef NonbondedCutoffSystemForce<
+    CubicCellManager, OneAtomPairTwo<PeriodicBoundaryConditions, C2SwitchingFunction,
+                                     LennardJonesForce, C1SwitchingFunction, CoulombForce> >
+    RefForce;
+
+static char g_msg[1024];
+
+extern "C" const char *harness_message() { return g_msg; }
+
+static Force *make_force(ForceFactory &f, const std::string &id, double ron, double rclj,
+                         double rcc, double rc) {
+  std::vector<Value> v;
+  v.push_back(Value(ron));
+  v.push_back(Value(rclj));
+  v.push_back(Value(rcc));
+  v.push_back(Value(rc));
+  return f.make(id, v);
+}
+
+static void eval_force(Force *force, PTopo *t, const double *pos, int n, double *f, double *e,
+                       double *vir, double *mvir) {
+  Vector3DBlock p(n), fr(n);
+  std::memcpy(p.c, pos, sizeof(double) * 3 * n);
+  fr.zero();
+  ScalarStructure en;
+  en.clear();
+  en.virial(true);
+  en.molecularVirial(true);
+  buildMolecularCenterOfMass(&p, t);
+  dynamic_cast<SystemForce *>(force)->evaluate(t, &p, &fr, &en);
+  std::memcpy(f, fr.c, sizeof(double) * 3 * n);
+  e[0] = en[ScalarStructure::COULOMB];
+  e[1] = en[ScalarStructure::LENNARDJONES];
+  for (int k = 0; k < 9; k++) {
+    vir[k] = en[(ScalarStructure::Index)(ScalarStructure::VIRIALXX + k)];
+    mvir[k] = en[(ScalarStructure::Index)(ScalarStructure::MOLVIRIALXX + k)];
+  }
+}
+
+// which: 0 = the reference prototype, 1 = the B200 plugin, 2 = the B200
+// plugin through the reference's "time" decorator.  Forces are made by the
+// factory from the config-file id and the four parameter values.
+// Returns 0, or 1 with harness_message() set (factory / plugin exceptions).
+extern "C" int harness_eval(void *ref_handle, int which, int n, const double *pos, double ron,
+                            double rclj, double rcc, double rc, double *forces,
+                            double *energies, double *virial, double *molvirial) {
+  g_msg[0] = 0;
+  try {
+    PTopo *t = (PTopo *)pmref_topology(ref_handle);
+    ForceFactory factory;
+    factory.reg(new RefForce());
+    registerB200CutoffForce(factory);
+    const char *base = "LennardJones Coulomb -switchingFunction C2 -switchingFunction C1 -algorithm ";
+    std::string id = std::string(base) + (which == 0 ? "NonbondedCutoff" : "NonbondedCutoffB200");
+    if (which == 2) id = "time " + id;
+    Force *force = make_force(factory, id, ron, rclj, rcc, rc);
+    if (!force) {
+      std::strncpy(g_msg, ("factory could not make '" + id + "'").c_str(), sizeof(g_msg) - 1);
+      return 1;
+    }
+    std::strncpy(g_msg, force->getId().c_str(), sizeof(g_msg) - 1);
+    eval_force(force, t, pos, n, forces, energies, virial, molvirial);
+    delete force;
+    return 0;
+  } catch (const std::exception &e) {
+    std::strncpy(g_msg, e.what(), sizeof(g_msg) - 1);
+  } catch (...) {
+    std::strncpy(g_msg, "unknown exception", sizeof(g_msg) - 1);
+  }
+  return 1;
+}
