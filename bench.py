@@ -121,7 +121,7 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 def committed_traffic():
     """Pair-kernel DRAM bytes per launch from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "pair_mixed_water41k.md")
+    path = os.path.join(ROOT, "profiles", "pair_mixed_water41k.md")  # ncu summary
     try:
         txt = open(path).read()
     except OSError:

@@ -243,7 +243,7 @@ int launch_eval(pmb200_ctx *c, const double *d_pos, double *d_forces, double *d_
     const double rcc = c->p.cutoff_coul / g.unit;
     k_reduce1<<<kRedBlocks, 256, 0, st>>>(g.ncell, c->d_partial, c->d_red);
     // the mixed kernel visits each pair once, the FP64 kernel twice
-    k_reduce2<<<1, 32, 0, st>>>(kRedBlocks, c->d_red, mixed ? 1 : 0, mixed ? 1.0 : 0.5,
+    k_reduce2<<<1, 256, 0, st>>>(kRedBlocks, c->d_red, mixed ? 1 : 0, mixed ? 1.0 : 0.5,
                                 1.5 / rcc, 0.5 / (rcc * rcc * rcc), d_out ? d_out : c->d_out,
                                 c->d_pairs);
     CK(cudaGetLastError());
@@ -1124,7 +1124,7 @@ extern "C" int pmb200_eval_noalloc(const pmb200_params *p, int n, const double *
     k_finalize<<<(n + 255) / 256, 256, 0, st>>>(n, facc, sidx, kFixInv / u, 0, d_forces);
   if (d_energy) {
     k_reduce1<<<kRedBlocks, 256, 0, st>>>(g.ncell, partial, red);
-    k_reduce2<<<1, 32, 0, st>>>(kRedBlocks, red, 1, 1.0, 1.5 / rq, 0.5 / (rq * rq * rq),
+    k_reduce2<<<1, 256, 0, st>>>(kRedBlocks, red, 1, 1.0, 1.5 / rq, 0.5 / (rq * rq * rq),
                                 d_energy, pairs);
   }
   if (cudaGetLastError() != cudaSuccess) return PMB200_ECUDA;

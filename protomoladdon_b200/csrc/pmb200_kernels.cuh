@@ -849,11 +849,21 @@ __global__ void k_reduce1(int ncell, const double *__restrict__ partial,
 __global__ void k_reduce2(int nred, const double *__restrict__ red, int mixed, double visit,
                           double c15_1, double c05_3, double *__restrict__ out,
                           double *__restrict__ pairs_out) {
+  // all threads stage the block sums; then each of ACC_MV threads adds one
+  // column in block order (fixed order: deterministic)
+  __shared__ double sh[kRedBlocks * ACC_MV];
+  __shared__ double col[ACC_MV];
+  for (int k = threadIdx.x; k < nred * ACC_MV; k += blockDim.x) sh[k] = red[k];
+  __syncthreads();
+  if (threadIdx.x < ACC_MV) {
+    double acc = 0.0;
+    for (int b = 0; b < nred; b++) acc += sh[b * ACC_MV + threadIdx.x];
+    col[threadIdx.x] = acc;
+  }
+  __syncthreads();
   if (threadIdx.x != 0) return;
   double r[ACC_MV];
-  for (int k = 0; k < ACC_MV; k++) r[k] = 0.0;
-  for (int b = 0; b < nred; b++)
-    for (int k = 0; k < ACC_MV; k++) r[k] += red[b * ACC_MV + k];
+  for (int k = 0; k < ACC_MV; k++) r[k] = col[k];
   // visit = 1 / (times each pair was evaluated)
   const double ec = mixed ? visit * (r[ACC_U] - c15_1 * r[ACC_Q] + c05_3 * r[ACC_R])
                           : visit * r[ACC_ECOUL];
