@@ -7,9 +7,14 @@ import this module.  It wraps
   ProtoMol's NonbondedCutoffSystemForce<CubicCellManager, OneAtomPairTwo<
   PeriodicBoundaryConditions, C2, LennardJones, C1, Coulomb>>; and
 * ``oracle/_ref/libpmref.so`` -- the reference's own sources compiled by
-  oracle/Makefile, driven through ref_driver.cpp (present only where the
-  reference tree was available at build time; the file travels with the repo
-  copy).
+  oracle/Makefile, driven through ref_driver.cpp and ref_ewald.cpp (present
+  only where the reference tree was available at build time; the file
+  travels with the repo copy); ``libpmref_exacterf.so`` is the same with the
+  Ewald force built with -DUSE_EWALD_EXACT_ERF.
+
+The real-space Ewald term (NonbondedFullEwaldSystemForce<PBC, CubicCellManager,
+real only, CutoffSwitchingFunction>) is restated in pm_oracle.c as well and
+pinned against both reference builds.
 
 Parity status: the restatement is pinned bit for bit against the compiled
 reference on seeded water boxes and against the reference's periodic water
@@ -26,6 +31,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 RESTATE_SO = os.path.join(HERE, "_build", "libpmoracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libpmref.so")
+REF_EXACT_SO = os.path.join(HERE, "_ref", "libpmref_exacterf.so")
 
 _P = ctypes.c_void_p
 _D = ctypes.c_double
@@ -69,20 +75,34 @@ def restate_lib():
         lib.pmo_leapfrog_rigid.argtypes = [ctypes.POINTER(_PmoSystem), _P, _P, _P, _D, _I, _I,
                                            _P, _D, _D, _P]
         lib.pmo_leapfrog_rigid.restype = _I
+        lib.pmo_eval_ewald_real.argtypes = [ctypes.POINTER(_PmoSystem), _D, _D, _I, _P, _P, _P,
+                                            _P, _P, _I, _I]
+        lib.pmo_eval_ewald_real.restype = _I
+        lib.pmo_ewald_constants.argtypes = [ctypes.POINTER(_PmoSystem), _D, _D, _P]
+        lib.pmo_ewald_constants.restype = _I
+        lib.pmo_count_pairs_ewald.argtypes = [ctypes.POINTER(_PmoSystem), _D, _D, _P]
+        lib.pmo_count_pairs_ewald.restype = ctypes.c_longlong
         _restate = lib
     return _restate
 
 
-def ref_available() -> bool:
-    return os.path.exists(REF_SO)
+_ref_exact = None
 
 
-def ref_lib():
-    global _ref
-    if _ref is None:
-        if not os.path.exists(REF_SO):
-            raise RuntimeError(f"reference oracle not built: {REF_SO} (run make -C oracle ref)")
-        lib = ctypes.CDLL(REF_SO)
+def ref_available(exact_erfc: bool = False) -> bool:
+    return os.path.exists(REF_EXACT_SO if exact_erfc else REF_SO)
+
+
+def ref_lib(exact_erfc: bool = False):
+    """The compiled reference; exact_erfc selects the build whose Ewald force
+    uses libm erfc."""
+    global _ref, _ref_exact
+    lib = _ref_exact if exact_erfc else _ref
+    if lib is None:
+        path = REF_EXACT_SO if exact_erfc else REF_SO
+        if not os.path.exists(path):
+            raise RuntimeError(f"reference oracle not built: {path} (run make -C oracle ref)")
+        lib = ctypes.CDLL(path)
         lib.pmref_create.restype = _P
         lib.pmref_create.argtypes = [_I, _P, _P, _P, _P, _I, _P, _I, _P, _D, _P, _P,
                                      _D, _D, _D, _D, _D]
@@ -92,8 +112,14 @@ def ref_lib():
         lib.pmref_leapfrog.argtypes = [_P, _P, _P, _P, _D, _I, _P]
         lib.pmref_leapfrog.restype = _I
         lib.pmref_load_psf.restype = _I
-        _ref = lib
-    return _ref
+        lib.pmref_ewald_eval.argtypes = [_P, _D, _D, _P, _P, _P, _P, _P, _I]
+        lib.pmref_ewald_eval.restype = _I
+        lib.pmref_ewald_exact_erfc.restype = _I
+        if exact_erfc:
+            _ref_exact = lib
+        else:
+            _ref = lib
+    return lib
 
 
 class _Arrays:
@@ -145,6 +171,46 @@ def restate_eval(sysd, pos, virial_mode=2, brute=False):
     if rc:
         raise RuntimeError(f"pmo_eval failed: {rc}")
     return f.reshape(-1, 3), e, v, mv
+
+
+def restate_ewald_real(sysd, pos, alpha, accuracy, exact_erfc=False, virial_mode=2,
+                       brute=False):
+    """The real-space Ewald term; returns (forces[n,3], coulomb energy,
+    virial[9], molvirial[9])."""
+    lib = restate_lib()
+    ar = _Arrays(sysd)
+    st = _pmo_struct(sysd, ar)
+    p = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1)
+    f = np.zeros(p.size)
+    e = np.zeros(2)
+    v = np.zeros(9)
+    mv = np.zeros(9)
+    rc = lib.pmo_eval_ewald_real(ctypes.byref(st), float(alpha), float(accuracy),
+                                 int(bool(exact_erfc)), _ptr(p), _ptr(f), _ptr(e), _ptr(v),
+                                 _ptr(mv), int(virial_mode), int(bool(brute)))
+    if rc:
+        raise RuntimeError(f"pmo_eval_ewald_real failed: {rc}")
+    return f.reshape(-1, 3), float(e[0]), v, mv
+
+
+def ewald_constants(sysd, alpha, accuracy):
+    """(alpha, rc, 2 alpha / sqrt(pi), alpha^2) as the reference derives them."""
+    lib = restate_lib()
+    ar = _Arrays(sysd)
+    st = _pmo_struct(sysd, ar)
+    out = np.zeros(4)
+    if lib.pmo_ewald_constants(ctypes.byref(st), float(alpha), float(accuracy), _ptr(out)):
+        raise RuntimeError("bad Ewald parameters")
+    return tuple(float(x) for x in out)
+
+
+def restate_count_pairs_ewald(sysd, pos, alpha, accuracy) -> int:
+    lib = restate_lib()
+    ar = _Arrays(sysd)
+    st = _pmo_struct(sysd, ar)
+    p = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1)
+    return int(lib.pmo_count_pairs_ewald(ctypes.byref(st), float(alpha), float(accuracy),
+                                         _ptr(p)))
 
 
 def restate_count_pairs(sysd, pos) -> int:
@@ -200,8 +266,8 @@ class RefForce:
     """The reference's own NonbondedCutoffSystemForce (compiled from its
     sources) on one system; evaluate() calls SystemForce::evaluate."""
 
-    def __init__(self, sysd):
-        self.lib = ref_lib()
+    def __init__(self, sysd, exact_erfc=False):
+        self.lib = ref_lib(exact_erfc)
         self.ar = _Arrays(sysd)
         ar = self.ar
         box = np.ascontiguousarray(sysd["box"], dtype=np.float64)
@@ -222,6 +288,18 @@ class RefForce:
         mv = np.zeros(9)
         self.lib.pmref_eval(self.h, _ptr(p), _ptr(f), _ptr(e), _ptr(v), _ptr(mv), int(virial_mode))
         return f.reshape(-1, 3), e, v, mv
+
+    def ewald_real(self, pos, alpha, accuracy, virial_mode=2):
+        """The reference's real-space Ewald force on this topology: (forces,
+        coulomb energy, virial, molvirial)."""
+        p = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1)
+        f = np.zeros(p.size)
+        e = np.zeros(2)
+        v = np.zeros(9)
+        mv = np.zeros(9)
+        self.lib.pmref_ewald_eval(self.h, float(alpha), float(accuracy), _ptr(p), _ptr(f),
+                                  _ptr(e), _ptr(v), _ptr(mv), int(virial_mode))
+        return f.reshape(-1, 3), float(e[0]), v, mv
 
     def leapfrog(self, pos, vel, dt_fs, nsteps):
         p = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1).copy()

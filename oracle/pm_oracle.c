@@ -1,5 +1,6 @@
 /* CPU oracle: C restatement of ProtoMol's periodic cutoff nonbonded system
- * force (LJ with C2 switching + Coulomb with C1 switching).
+ * force (LJ with C2 switching + Coulomb with C1 switching) and of the
+ * real-space term of its Ewald sum.
  *
  * TEST INFRASTRUCTURE ONLY (see pm_oracle.h).  Every function cites the
  * reference code it restates; paths are relative to protomol/src/protomol/.
@@ -10,6 +11,9 @@
 
 #include <math.h>
 #include <stdlib.h>
+#ifndef M_PI
+#define M_PI 3.14159265358979323846
+#endif
 #include <string.h>
 
 #define PMO_EPSILON 1.0e-14                 /* base/PMConstants.cpp:47 */
@@ -201,6 +205,11 @@ typedef struct {
   double *molpos; /* [nmol*3] when virial_mode == 2 */
   long long pairs;
   int count_only;
+  /* Ewald real-space term (form 1 = A&S poly5 erfc, the reference's default
+   * build; form 2 = libm erfc, its -DUSE_EWALD_EXACT_ERF build) */
+  int form;
+  double ew_alpha, ew_alpha2, ew_2api, ew_rc2;
+  double walk_cut;   /* cutoff of the cell enumerator */
 } ctx_t;
 
 /* ScalarStructure::addVirial(force12, diff) (type/ScalarStructure.cpp:36-54) */
@@ -275,6 +284,80 @@ static void one_pair(ctx_t *c, int i, int j) {
     add_virial(c->mvir, fij, cd);
   } else if (c->virial_mode >= 1)
     add_virial(c->vir, fij, diff);
+}
+
+/* Abramowitz & Stegun 7.1.26 polynomial for erfc(x) e^{x^2}
+ * (base/MathUtilities.cpp:39-49): t = 1 / (1 + p x), t (a1 + t (a2 + ...)). */
+static double ew_poly5(double ar) {
+  const double a1 = 0.254829592, a2 = -0.284496736, a3 = 1.421413741,
+               a4 = -1.453152027, a5 = 1.061405429, p = 0.3275911;
+  double t = 1.0 / (1.0 + p * ar);
+  return (t) * (a1 + (t) * (a2 + (t) * (a3 + (t) * (a4 + (t) * a5))));
+}
+
+/* One (i, j) visit of NonbondedFullEwaldSystemForce::realTerm
+ * (force/nonbonded/NonbondedFullEwaldSystemForce.h:776-851) with the
+ * CutoffSwitchingFunction (switch/CutoffSwitchingFunction.h:41-44) and only
+ * the zero lattice vector (every box edge >= 2 rc, so buildLatticeVectors,
+ * topology/PeriodicBoundaryConditions.cpp:80-104, adds no image within rc).
+ * The force on i is summed into fi; the caller adds fi to forces[i] after
+ * its j loop, as the reference does. */
+static void ewald_pair(ctx_t *c, int i, int j, double fi[3]) {
+  const pmo_system *s = c->s;
+  double rij[3], r2, r, qq, energy, force, fij[3];
+  int mi = s->mol[i], mj = s->mol[j], same = (mi == mj), excl = 0, k;
+  pbc_min_diff(&c->pbc, c->pos + 3 * i, c->pos + 3 * j, rij, &r2);
+  if (same) excl = excl_check(c->excl, c->nexcl, i, j);
+  if (i == j) excl = 2;
+  if (excl == 2) return;
+  r2 = rij[0] * rij[0] + rij[1] * rij[1] + rij[2] * rij[2];
+  if (r2 > c->ew_rc2) return;
+  if (c->count_only) {
+    c->pairs++;
+    return;
+  }
+  r = sqrt(r2);
+  qq = s->qscaled[i] * s->qscaled[j];
+  if (excl == 1) qq *= s->coulomb_scaling;
+  if (c->form == 1) {
+    double rr = 1.0 / r;
+    double ar = c->ew_alpha * r;
+    double e = qq * exp(-ar * ar);
+    energy = ew_poly5(ar) * e * rr;
+    force = ((energy + c->ew_2api * e) * rr * rr);
+  } else {
+    double a = erfc(c->ew_alpha * r) / r;
+    energy = qq * a;
+    force = qq * (a + c->ew_2api * exp(-c->ew_alpha2 * r2)) / r2;
+  }
+  /* switching value 1, derivative 0 inside the cutoff */
+  force = force * 1.0 - energy * 0.0;
+  energy = energy * 1.0;
+  c->e_coul += energy;
+  for (k = 0; k < 3; k++) fij[k] = rij[k] * force;
+  for (k = 0; k < 3; k++) {
+    fi[k] -= fij[k];
+    c->forces[3 * j + k] += fij[k];
+  }
+  if (!same && c->virial_mode >= 2) {
+    double cd[3], cd2;
+    pbc_min_diff(&c->pbc, c->molpos + 3 * mi, c->molpos + 3 * mj, cd, &cd2);
+    add_virial(c->vir, fij, rij);
+    add_virial(c->mvir, fij, cd);
+  } else if (c->virial_mode >= 1)
+    add_virial(c->vir, fij, rij);
+}
+
+/* All j of one i for the Ewald walk: j over cell B, or from i itself in a
+ * self cell (NonbondedFullEwaldSystemForce.h:776-853).  next == NULL walks
+ * j = bfirst .. n-1 (the all-pairs cross-check). */
+static void ewald_atom(ctx_t *c, int a, int bfirst, const int *next) {
+  double fi[3] = {0.0, 0.0, 0.0};
+  int bb, k;
+  for (bb = bfirst; bb != -1; bb = next ? next[bb] : (bb + 1 < c->s->n ? bb + 1 : -1))
+    ewald_pair(c, a, bb, fi);
+  if (!c->count_only)
+    for (k = 0; k < 3; k++) c->forces[3 * a + k] += fi[k];
 }
 
 /* molecularCenterOfMass with Kahan summation over the molecule's atoms in
@@ -358,7 +441,7 @@ static int walk_cells(ctx_t *c) {
   int *head, *next;
   int ncell, begin, end, ndelta = 0;
   cell3 *deltas;
-  double cut2 = s->rc_alg * s->rc_alg;
+  double cut2 = c->walk_cut * c->walk_cut;
   for (k = 0; k < 3; k++) {
     double m = floor((b->max[k] - b->min[k]) / s->cellsize);
     vdiff[k] = b->max[k] - b->min[k];
@@ -397,7 +480,7 @@ static int walk_cells(ctx_t *c) {
   {
     int lim[3];
     for (k = 0; k < 3; k++) {
-      int v = (int)(s->rc_alg / edge[k] + 1.0 + PMO_EPSILON);
+      int v = (int)(c->walk_cut / edge[k] + 1.0 + PMO_EPSILON);
       lim[k] = v < nd[k] ? v : nd[k];
     }
     deltas = (cell3 *)malloc(sizeof(cell3) *
@@ -449,9 +532,13 @@ static int walk_cells(ctx_t *c) {
     int ci = begin, cj = begin, counter = 0;
     while (ci != end) {
       int a, bb;
-      for (a = head[ci]; a != -1; a = next[a])
-        for (bb = (ci != cj) ? head[cj] : next[a]; bb != -1; bb = next[bb])
-          one_pair(c, a, bb);
+      if (c->form)
+        for (a = head[ci]; a != -1; a = next[a])
+          ewald_atom(c, a, (ci != cj) ? head[cj] : a, next);
+      else
+        for (a = head[ci]; a != -1; a = next[a])
+          for (bb = (ci != cj) ? head[cj] : next[a]; bb != -1; bb = next[bb])
+            one_pair(c, a, bb);
       /* next() */
       do {
         if (ci != end) {
@@ -496,6 +583,7 @@ static int ctx_init(ctx_t *c, const pmo_system *s, const double *pos,
   c->pos = pos;
   c->forces = forces;
   c->virial_mode = virial_mode;
+  c->walk_cut = s->rc_alg;
   pbc_set(&c->pbc, s->box, s->origin);
   sw_set(&c->sw, s->ron, s->rc_lj, s->rc_coul);
   c->nexcl = s->nexcl;
@@ -540,6 +628,80 @@ int pmo_eval(const pmo_system *s, const double *pos, double *forces,
     for (k = 0; k < 9; k++) molvirial[k] += c.mvir[k];
   ctx_free(&c);
   return rc;
+}
+
+/* NonbondedFullEwaldSystemForce::initialize, the constants the real-space
+ * term uses (force/nonbonded/NonbondedFullEwaldSystemForce.h:586-598):
+ * default alpha sqrt(pi) (5.5 N / V^2)^(1/6), V = |(e1 x e2) . e3|
+ * (topology/PeriodicBoundaryConditions.cpp:40), rc = sqrt(-log(accuracy)) /
+ * alpha, 2 alpha / sqrt(pi). */
+int pmo_ewald_constants(const pmo_system *s, double alpha, double accuracy,
+                        double out[4]) {
+  double v, p;
+  if (!s || !out || !(accuracy > 0.0) || !(accuracy < 1.0)) return PMO_EBADARG;
+  v = fabs((s->box[0] * s->box[1]) * s->box[2]);
+  if (alpha <= 0.0) alpha = sqrt(M_PI) * pow(5.5 * (unsigned)s->n / (v * v), 1.0 / 6.0);
+  p = -log(accuracy);
+  out[0] = alpha;
+  out[1] = sqrt(p) / alpha;
+  out[2] = 2.0 * alpha / sqrt(M_PI);
+  out[3] = alpha * alpha;
+  return PMO_OK;
+}
+
+static int ewald_setup(ctx_t *c, const pmo_system *s, double alpha, double accuracy,
+                       int exact_erfc) {
+  double k[4];
+  int a;
+  if (pmo_ewald_constants(s, alpha, accuracy, k)) return PMO_EBADARG;
+  for (a = 0; a < 3; a++)
+    if (fabs(s->box[a]) < 2.0 * k[1]) return PMO_EBADARG; /* lattice images */
+  c->form = exact_erfc ? 2 : 1;
+  c->ew_alpha = k[0];
+  c->ew_rc2 = k[1] * k[1];
+  c->ew_2api = k[2];
+  c->ew_alpha2 = k[3];
+  c->walk_cut = k[1];
+  return PMO_OK;
+}
+
+int pmo_eval_ewald_real(const pmo_system *s, double alpha, double accuracy,
+                        int exact_erfc, const double *pos, double *forces,
+                        double *energies, double *virial, double *molvirial,
+                        int virial_mode, int brute) {
+  ctx_t c;
+  int rc = ctx_init(&c, s, pos, forces, virial_mode), k;
+  if (!rc) rc = ewald_setup(&c, s, alpha, accuracy, exact_erfc);
+  if (rc) { ctx_free(&c); return rc; }
+  if (!forces || !energies) { ctx_free(&c); return PMO_EBADARG; }
+  if (brute) {
+    int i;
+    for (i = 0; i < s->n; i++) ewald_atom(&c, i, i + 1 < s->n ? i + 1 : -1, NULL);
+  } else {
+    rc = walk_cells(&c);
+  }
+  energies[0] += c.e_coul;
+  if (virial && virial_mode >= 1)
+    for (k = 0; k < 9; k++) virial[k] += c.vir[k];
+  if (molvirial && virial_mode >= 2)
+    for (k = 0; k < 9; k++) molvirial[k] += c.mvir[k];
+  ctx_free(&c);
+  return rc;
+}
+
+long long pmo_count_pairs_ewald(const pmo_system *s, double alpha, double accuracy,
+                                const double *pos) {
+  ctx_t c;
+  long long n;
+  if (ctx_init(&c, s, pos, NULL, 0) || ewald_setup(&c, s, alpha, accuracy, 1)) {
+    ctx_free(&c);
+    return -1;
+  }
+  c.count_only = 1;
+  if (walk_cells(&c)) { ctx_free(&c); return -1; }
+  n = c.pairs;
+  ctx_free(&c);
+  return n;
 }
 
 long long pmo_count_pairs(const pmo_system *s, const double *pos) {

@@ -61,6 +61,34 @@ int pmo_eval(const pmo_system *s, const double *pos, double *forces,
  * the minimum image; the Gpairs/s unit. */
 long long pmo_count_pairs(const pmo_system *s, const double *pos);
 
+/* The real-space term of ProtoMol's Ewald sum,
+ *   NonbondedFullEwaldSystemForce<PeriodicBoundaryConditions,
+ *     CubicCellManager, real = true, reciprocal = false, correction = false,
+ *     CutoffSwitchingFunction>
+ * (registered in module/NonbondedFullElectrostaticForceModule.cpp:34 as
+ * "Coulomb -algorithm FullEwald -real"): qq erfc(alpha r) / r for every pair
+ * within rc = sqrt(-log(accuracy)) / alpha, MODIFIED pairs scaled by
+ * coulomb_scaling, FULL pairs skipped.  alpha <= 0 selects the reference's
+ * default.  exact_erfc 0 evaluates erfc with the Abramowitz & Stegun
+ * polynomial of the reference's default build, 1 with libm erfc (the
+ * reference built with -DUSE_EWALD_EXACT_ERF).  The cell walk uses the
+ * system's cellsize and the cutoff rc; rc_lj/rc_coul/ron/rc_alg are ignored.
+ * Every box edge must be >= 2 rc (no lattice images).  energies[0] (Coulomb)
+ * is accumulated into; energies[1] is untouched. */
+int pmo_eval_ewald_real(const pmo_system *s, double alpha, double accuracy,
+                        int exact_erfc, const double *pos, double *forces,
+                        double *energies, double *virial, double *molvirial,
+                        int virial_mode, int brute);
+
+/* out = {alpha, rc, 2 alpha / sqrt(pi), alpha^2} as the Ewald force derives
+ * them (alpha <= 0: the reference's default from N and the volume). */
+int pmo_ewald_constants(const pmo_system *s, double alpha, double accuracy,
+                        double out[4]);
+
+/* Unique pairs within the Ewald real-space cutoff (not fully excluded). */
+long long pmo_count_pairs_ewald(const pmo_system *s, double alpha, double accuracy,
+                                const double *pos);
+
 /* Leapfrog with this force alone (LeapfrogIntegrator::run with no
  * modifiers): initial force, then per step kick (half on the first step) +
  * drift + force, and a closing half kick.  dt in fs. */

@@ -20,6 +20,14 @@ Fixtures (all inputs and outputs FP64):
 * modified_ref.npz -- the same box with every intramolecular O-H pair made
   EXCLUSION_MODIFIED (1-4 style) and coulombScalingFactor 0.5, exercising
   A14/B14 and the Coulomb scaling branch.
+* ewald_{water,modified,ions}_ref.npz -- the reference's real-space Ewald
+  force (NonbondedFullEwaldSystemForce<PBC, CubicCellManager, real only,
+  Cutoff>) on the 648-atom box (alpha 0.30, rc 8), on the modified box
+  (default alpha, accuracy 1e-5) and on a box with 10% of the waters
+  replaced by Na+/Cl- (alpha 0.30, rc 9): forces, Coulomb energy, atomic and
+  molecular virial from the reference as shipped (``poly5_*``, erfc by the
+  Abramowitz & Stegun polynomial) and built with -DUSE_EWALD_EXACT_ERF
+  (``exact_*``).  ``--ewald-only`` writes just these.
 """
 from __future__ import annotations
 
@@ -91,5 +99,31 @@ def main(ref_root):
     print("wrote fixtures to", HERE)
 
 
+def ewald_fixtures():
+    w = water.small_648()
+    m = dict(w)
+    ex = m["excl"].copy()
+    ex[m["type"][ex[:, 0]] == water.T_O, 2] = 1
+    m["excl"] = ex
+    m["coulomb_scaling"] = 0.5
+    ions = water.water_box(6, rc=9.0, ron=8.0, seed=77, ion_fraction=0.1)
+    cases = [("ewald_water_ref.npz", w, 0.30, float(np.exp(-(0.30 * 8.0) ** 2))),
+             ("ewald_modified_ref.npz", m, -1.0, 1e-5),
+             ("ewald_ions_ref.npz", ions, 0.30, float(np.exp(-(0.30 * 9.0) ** 2)))]
+    for name, sysd, alpha, acc in cases:
+        out = dict(sysd_arrays(sysd), alpha=np.float64(alpha), accuracy=np.float64(acc))
+        for tag, exact in (("poly5", False), ("exact", True)):
+            R = O.RefForce(sysd, exact_erfc=exact)
+            f, e, v, mv = R.ewald_real(sysd["pos"], alpha, acc, 2)
+            R.close()
+            out.update({f"{tag}_forces": f, f"{tag}_energy": np.float64(e),
+                        f"{tag}_virial": v, f"{tag}_molvirial": mv})
+        np.savez_compressed(os.path.join(HERE, name), **out)
+    print("wrote Ewald fixtures to", HERE)
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    if "--ewald-only" not in sys.argv:
+        main(args[0] if args else "/root/reference")
+    ewald_fixtures()

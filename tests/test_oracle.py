@@ -139,3 +139,71 @@ def test_rigid_leapfrog_keeps_geometry(water648):
     d = p[w]
     assert np.abs(np.linalg.norm(d[:, 1] - d[:, 0], axis=1) - water.D_OH).max() < 1e-10
     assert np.isfinite(e).all()
+
+
+# ---- Ewald real-space term --------------------------------------------------
+EWALD_FIXTURES = ["ewald_water_ref.npz", "ewald_modified_ref.npz", "ewald_ions_ref.npz"]
+
+
+@pytest.mark.parametrize("name", EWALD_FIXTURES)
+@pytest.mark.parametrize("tag", ["poly5", "exact"])
+def test_ewald_restatement_bitexact_vs_reference_fixture(name, tag):
+    """Both reference builds (A&S polynomial as shipped; -DUSE_EWALD_EXACT_ERF)
+    against the restatement, bit for bit."""
+    from tests.conftest import load_fixture
+    d = load_fixture(name)
+    f, e, v, mv = O.restate_ewald_real(d, d["pos"], float(d["alpha"]), float(d["accuracy"]),
+                                       exact_erfc=(tag == "exact"), virial_mode=2)
+    assert np.array_equal(f, d[f"{tag}_forces"])
+    assert e == float(d[f"{tag}_energy"])
+    assert np.array_equal(v, d[f"{tag}_virial"])
+    assert np.array_equal(mv, d[f"{tag}_molvirial"])
+
+
+def test_ewald_cell_walk_equals_all_pairs():
+    from tests.conftest import load_fixture
+    d = load_fixture("ewald_ions_ref.npz")
+    a, acc = float(d["alpha"]), float(d["accuracy"])
+    f, e, v, _ = O.restate_ewald_real(d, d["pos"], a, acc, True, 1)
+    fb, eb, vb, _ = O.restate_ewald_real(d, d["pos"], a, acc, True, 1, brute=True)
+    assert np.abs(f - fb).max() < 1e-11 * np.abs(f).max()
+    assert abs(e - eb) <= 1e-12 * abs(e)
+    assert np.allclose(v, vb, rtol=1e-12, atol=1e-9)
+    assert np.abs(f.sum(axis=0)).max() < 1e-9 * np.abs(f).max()  # Newton's third law
+
+
+def test_ewald_constants_and_limits(water648):
+    """rc = sqrt(-log(accuracy)) / alpha; the default alpha; a box below 2 rc
+    is refused (the reference would add lattice images there)."""
+    a, rc, a2pi, a2 = O.ewald_constants(water648, 0.30, float(np.exp(-(0.30 * 8.0) ** 2)))
+    assert a == 0.30 and abs(rc - 8.0) < 1e-12 and abs(a2pi - 0.6 / np.sqrt(np.pi)) < 1e-15
+    n = water648["n"]
+    v = float(np.prod(water648["box"]))
+    a, rc, _, _ = O.ewald_constants(water648, -1.0, 1e-5)
+    assert abs(a - np.sqrt(np.pi) * (5.5 * n / v ** 2) ** (1.0 / 6.0)) < 1e-15
+    with pytest.raises(RuntimeError):
+        O.restate_ewald_real(water648, water648["pos"], 0.2, 1e-5)  # rc 17 > L / 2
+
+
+def test_ewald_erfc_forms_agree_to_polynomial_error(water648):
+    """The A&S polynomial (|error| <= 1.5e-7 in erfc) and libm erfc agree to
+    that order, per pair and in total."""
+    acc = float(np.exp(-(0.30 * 8.0) ** 2))
+    f1, e1, _, _ = O.restate_ewald_real(water648, water648["pos"], 0.30, acc, False, 0)
+    f2, e2, _, _ = O.restate_ewald_real(water648, water648["pos"], 0.30, acc, True, 0)
+    assert 0 < abs(e1 - e2) < 1e-3 * abs(e2)
+    assert np.sqrt(((f1 - f2) ** 2).sum() / (f2 ** 2).sum()) < 1e-5
+
+
+@pytest.mark.skipif(not O.ref_available(True), reason="reference oracle library not built")
+@pytest.mark.parametrize("seed,exact", [(3, False), (11, True)])
+def test_ewald_restatement_bitexact_vs_compiled_reference(seed, exact):
+    s = water.water_box(6, rc=8.0, ron=7.0, seed=seed, ion_fraction=0.06)
+    s["cellsize"] = 2.9
+    R = O.RefForce(s, exact_erfc=exact)
+    acc = float(np.exp(-(0.33 * 8.5) ** 2))  # rc 8.5
+    f, e, v, mv = R.ewald_real(s["pos"], 0.33, acc, 2)
+    R.close()
+    g, ee, vv, mm = O.restate_ewald_real(s, s["pos"], 0.33, acc, exact, 2)
+    assert np.array_equal(f, g) and e == ee
+    assert np.array_equal(v, vv) and np.array_equal(mv, mm)
