@@ -225,6 +225,46 @@ int pmb200_eval_noalloc(const pmb200_params *params, int n, const double *d_pos,
 /* Geometry of the device cell grid chosen for the current box. */
 int pmb200_grid(const pmb200_ctx *ctx, int dims[3], double edge[3]);
 
+/* ---- Ewald real-space term ----
+ * A context of the second kind replaces the real-space part of ProtoMol's
+ * Ewald sum,
+ *   NonbondedFullEwaldSystemForce<PeriodicBoundaryConditions,
+ *     CubicCellManager, real = true, reciprocal = false, correction = false,
+ *     CutoffSwitchingFunction>
+ * (protomol/src/protomol/module/NonbondedFullElectrostaticForceModule.cpp:34;
+ * config "force Coulomb -algorithm FullEwald -real -alpha <a> -accuracy
+ * <acc>"; pair term .../force/nonbonded/NonbondedFullEwaldSystemForce.h:
+ * 776-851): E = sum over pairs within rc of q_i q_j erfc(alpha r) / r,
+ * modified (1-4) pairs scaled by coulombScalingFactor, full exclusions
+ * skipped.  rc = sqrt(-log(accuracy)) / alpha and, for alpha <= 0, the
+ * reference's default alpha = sqrt(pi) (5.5 N / V^2)^(1/6) are derived as
+ * in NonbondedFullEwaldSystemForce::initialize (same header, 586-598), once
+ * the topology and the box are both set.  Every box edge must be >= 2 rc
+ * (the reference then adds no lattice image, PeriodicBoundaryConditions::
+ * buildLatticeVectors, .../topology/PeriodicBoundaryConditions.cpp:80-104).
+ * All other calls (set_topology, set_box, eval, eval_device, leapfrog_device,
+ * step_device, ...) work on it unchanged; the energy goes to COULOMB and
+ * LENNARDJONES receives 0.  The LJ table passed to set_topology is not used. */
+#define PMB200_ERFC_POLY5 0 /* Abramowitz & Stegun 7.1.26, the reference's default build */
+#define PMB200_ERFC_EXACT 1 /* erfc() itself: the reference built with -DUSE_EWALD_EXACT_ERF */
+
+typedef struct {
+  int precision;   /* PMB200_MIXED or PMB200_FP64 */
+  int device;      /* CUDA device ordinal */
+  int erfc;        /* PMB200_ERFC_POLY5 or PMB200_ERFC_EXACT */
+  double alpha;    /* -alpha (1/Angstrom); <= 0 selects the reference's default */
+  double accuracy; /* -accuracy, in (0, 1) */
+  double cellsize; /* grid cell edge hint; 0 = rc / 2 */
+} pmb200_ewald_params;
+
+/* Replaces constructing NonbondedFullEwaldSystemForce(alpha, accuracy, 3.0)
+ * through its doMake (NonbondedFullEwaldSystemForce.h:118-142). */
+int pmb200_create_ewald_real(const pmb200_ewald_params *params, pmb200_ctx **out);
+
+/* The alpha and real-space cutoff in use (PMB200_ESTATE until the topology
+ * and the box are set, or for a context of the first kind). */
+int pmb200_ewald_info(const pmb200_ctx *ctx, double *alpha, double *rc);
+
 #ifdef __cplusplus
 }
 #endif

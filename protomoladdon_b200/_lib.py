@@ -27,6 +27,9 @@ PMB200_ENERGY = 1
 PMB200_VIRIAL = 2
 PMB200_MOLVIRIAL = 4
 
+PMB200_ERFC_POLY5 = 0
+PMB200_ERFC_EXACT = 1
+
 # Every symbol include/pmb200.h declares.
 EXPORTED = (
     "pmb200_create", "pmb200_destroy", "pmb200_last_error", "pmb200_set_topology",
@@ -34,7 +37,7 @@ EXPORTED = (
     "pmb200_leapfrog_device", "pmb200_last_pair_count", "pmb200_grid",
     "pmb200_step_device", "pmb200_set_kernel_timing", "pmb200_last_kernel_ms",
     "pmb200_measure_fp32_peak", "pmb200_set_rigid_waters", "pmb200_host_kick_drift",
-    "pmb200_eval_noalloc",
+    "pmb200_eval_noalloc", "pmb200_create_ewald_real", "pmb200_ewald_info",
 )
 
 _P = ctypes.c_void_p
@@ -45,6 +48,11 @@ _I = ctypes.c_int
 class Params(ctypes.Structure):
     _fields_ = [("precision", _I), ("device", _I), ("switchon", _D), ("cutoff_lj", _D),
                 ("cutoff_coul", _D), ("cutoff_alg", _D), ("cellsize", _D)]
+
+
+class EwaldParams(ctypes.Structure):
+    _fields_ = [("precision", _I), ("device", _I), ("erfc", _I), ("alpha", _D),
+                ("accuracy", _D), ("cellsize", _D)]
 
 
 class PmbError(RuntimeError):
@@ -86,6 +94,8 @@ def lib():
     L.pmb200_host_kick_drift.argtypes = [_I, _P, _P, _P, _P, _D, _D, _I, _P, _D, _D]
     L.pmb200_eval_noalloc.argtypes = [ctypes.POINTER(Params), _I, _P, _P, _P, _P, _P, _P, _I, _P,
                                       _D, _P, _P, _P, _P, _P]
+    L.pmb200_create_ewald_real.argtypes = [ctypes.POINTER(EwaldParams), ctypes.POINTER(_P)]
+    L.pmb200_ewald_info.argtypes = [_P, ctypes.POINTER(_D), ctypes.POINTER(_D)]
     for name in EXPORTED:
         getattr(L, name).restype = getattr(L, name).restype or _I
     L.pmb200_last_error.restype = ctypes.c_char_p

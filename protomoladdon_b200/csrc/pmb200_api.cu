@@ -26,6 +26,14 @@ using namespace pmb200;
 struct pmb200_ctx {
   pmb200_params p{};
   std::string err;
+  // pair potential: FORM_CUTOFF, or the Ewald real-space term with its
+  // parameters and the alpha / cutoff derived from them
+  int form = FORM_CUTOFF;
+  double ew_alpha_in = 0.0, ew_accuracy = 0.0;
+  double ew_alpha = 0.0, ew_rc = 0.0;
+  // the box as last given (re-applied when an Ewald default alpha changes)
+  bool box_given = false;
+  double box_e[3][3] = {}, box_origin[3] = {};
   cudaStream_t stream = nullptr;
   // topology
   int n = 0, ntypes = 0, nmol = 0;
@@ -130,6 +138,23 @@ void release_graph(pmb200_ctx *c) {
 
 double rc_max(const pmb200_params &p) { return std::max(p.cutoff_lj, p.cutoff_coul); }
 
+// Pair cutoff of the context's potential.
+double ctx_rc(const pmb200_ctx *c) { return c->form == FORM_CUTOFF ? rc_max(c->p) : c->ew_rc; }
+
+// NonbondedFullEwaldSystemForce::initialize
+// (protomol/src/protomol/force/nonbonded/NonbondedFullEwaldSystemForce.h:
+// 586-598): alpha (default sqrt(pi) (5.5 N / V^2)^(1/6), V = |(e1 x e2) . e3|)
+// and rc = sqrt(-log(accuracy)) / alpha.
+void ewald_derive(pmb200_ctx *c, const double L[3]) {
+  double alpha = c->ew_alpha_in;
+  if (alpha <= 0.0) {
+    const double v = std::fabs((L[0] * L[1]) * L[2]);
+    alpha = std::sqrt(M_PI) * std::pow(5.5 * (unsigned)c->n / (v * v), 1.0 / 6.0);
+  }
+  c->ew_alpha = alpha;
+  c->ew_rc = std::sqrt(-std::log(c->ew_accuracy)) / alpha;
+}
+
 // LJ tables: FP64 in Angstrom units, FP32 in cell units (A / u^12, B / u^6).
 int upload_lj(pmb200_ctx *c) {
   const int t2 = c->ntypes * c->ntypes;
@@ -168,6 +193,47 @@ int ensure_atom_buffers(pmb200_ctx *c) {
   CK(dalloc(c->d_hfrc, 3 * n));
   c->n_alloc = c->n;
   return PMB200_OK;
+}
+
+// The pair kernels for the flags asked for (template instances per form).
+template <int F>
+void launch_pair_mixed(pmb200_ctx *c, unsigned flags, cudaStream_t st) {
+  const GridParams &g = c->g;
+  const bool energy = (flags & PMB200_ENERGY) != 0;
+  const bool virial = (flags & (PMB200_VIRIAL | PMB200_MOLVIRIAL)) != 0;
+  const bool molvir = (flags & PMB200_MOLVIRIAL) != 0;
+#define PMB_MIXED_LAUNCH(E, V, M)                                                          \
+  k_pair_mixed<F, E, V, M><<<g.ncell, 32 * kWarps, 0, st>>>(                                 \
+      g, c->mc, c->half, c->ntypes, c->d_lj32, c->d_start, c->d_spos32, c->d_smeta,         \
+      c->d_sidx, c->d_ex_start, c->d_ex, c->d_facc, c->n, c->d_err, c->d_partial, c->pb,    \
+      c->d_com)
+  if (molvir) PMB_MIXED_LAUNCH(true, true, true);
+  else if (energy && virial) PMB_MIXED_LAUNCH(true, true, false);
+  else if (energy) PMB_MIXED_LAUNCH(true, false, false);
+  else if (virial) PMB_MIXED_LAUNCH(false, true, false);
+  else PMB_MIXED_LAUNCH(false, false, false);
+#undef PMB_MIXED_LAUNCH
+}
+
+template <int F>
+void launch_pair_fp64(pmb200_ctx *c, unsigned flags, double *d_forces, int accumulate,
+                      int blocks, cudaStream_t st) {
+  const GridParams &g = c->g;
+  const bool energy = (flags & PMB200_ENERGY) != 0;
+  const bool virial = (flags & (PMB200_VIRIAL | PMB200_MOLVIRIAL)) != 0;
+  const bool molvir = (flags & PMB200_MOLVIRIAL) != 0;
+#define PMB_FP64_LAUNCH(E, V, M)                                                           \
+  k_pair_fp64<F, E, V, M><<<blocks, 128, 0, st>>>(g, c->fc, c->stencil, c->ntypes,          \
+                                                  c->d_lj64, c->d_start, c->d_spos64,       \
+                                                  c->d_smeta, c->d_sidx, c->d_ex_start,     \
+                                                  c->d_ex, d_forces, accumulate,            \
+                                                  c->d_partial, c->pb, c->d_com)
+  if (molvir) PMB_FP64_LAUNCH(true, true, true);
+  else if (energy && virial) PMB_FP64_LAUNCH(true, true, false);
+  else if (energy) PMB_FP64_LAUNCH(true, false, false);
+  else if (virial) PMB_FP64_LAUNCH(false, true, false);
+  else PMB_FP64_LAUNCH(false, false, false);
+#undef PMB_FP64_LAUNCH
 }
 
 // Launch one evaluation on `st`.  accumulate: add into d_forces (1) or
@@ -210,42 +276,32 @@ int launch_eval(pmb200_ctx *c, const double *d_pos, double *d_forces, double *d_
   if (timed) CK(cudaEventRecord(c->ev0, st));
   if (mixed) {
     const double fscale = 1.0 / g.unit;
-#define PMB_MIXED_LAUNCH(E, V, M)                                                          \
-  k_pair_mixed<E, V, M><<<g.ncell, 32 * kWarps, 0, st>>>(                                    \
-      g, c->mc, c->half, c->ntypes, c->d_lj32, c->d_start, c->d_spos32, c->d_smeta,           \
-      c->d_sidx, c->d_ex_start, c->d_ex, c->d_facc, n, c->d_err, c->d_partial, c->pb, c->d_com)
     if (n > 0) CK(cudaMemsetAsync(c->d_facc, 0, sizeof(unsigned long long) * 3 * (size_t)n, st));
-    if (molvir) PMB_MIXED_LAUNCH(true, true, true);
-    else if (energy && virial) PMB_MIXED_LAUNCH(true, true, false);
-    else if (energy) PMB_MIXED_LAUNCH(true, false, false);
-    else if (virial) PMB_MIXED_LAUNCH(false, true, false);
-    else PMB_MIXED_LAUNCH(false, false, false);
+    if (c->form == FORM_EWALD_POLY5) launch_pair_mixed<FORM_EWALD_POLY5>(c, flags, st);
+    else if (c->form == FORM_EWALD_EXACT) launch_pair_mixed<FORM_EWALD_EXACT>(c, flags, st);
+    else launch_pair_mixed<FORM_CUTOFF>(c, flags, st);
     if (n > 0)
       k_finalize<<<(n + 255) / 256, 256, 0, st>>>(n, c->d_facc, c->d_sidx, fscale * kFixInv,
                                                   accumulate, d_forces);
-#undef PMB_MIXED_LAUNCH
   } else {
-#define PMB_FP64_LAUNCH(E, V, M)                                                         \
-  k_pair_fp64<E, V, M><<<blocks, 128, 0, st>>>(g, c->fc, c->stencil, c->ntypes, c->d_lj64,  \
-                                               c->d_start, c->d_spos64, c->d_smeta,          \
-                                               c->d_sidx, c->d_ex_start, c->d_ex, d_forces,  \
-                                               accumulate, c->d_partial, c->pb, c->d_com)
-    if (molvir) PMB_FP64_LAUNCH(true, true, true);
-    else if (energy && virial) PMB_FP64_LAUNCH(true, true, false);
-    else if (energy) PMB_FP64_LAUNCH(true, false, false);
-    else if (virial) PMB_FP64_LAUNCH(false, true, false);
-    else PMB_FP64_LAUNCH(false, false, false);
-#undef PMB_FP64_LAUNCH
+    if (c->form == FORM_EWALD_POLY5)
+      launch_pair_fp64<FORM_EWALD_POLY5>(c, flags, d_forces, accumulate, blocks, st);
+    else if (c->form == FORM_EWALD_EXACT)
+      launch_pair_fp64<FORM_EWALD_EXACT>(c, flags, d_forces, accumulate, blocks, st);
+    else
+      launch_pair_fp64<FORM_CUTOFF>(c, flags, d_forces, accumulate, blocks, st);
   }
   CK(cudaGetLastError());
   if (timed) CK(cudaEventRecord(c->ev1, st));
   if (energy || virial) {
+    // C1 constants for the mixed Coulomb sums (the Ewald term has none)
     const double rcc = c->p.cutoff_coul / g.unit;
+    const bool c1 = c->form == FORM_CUTOFF;
     k_reduce1<<<kRedBlocks, 256, 0, st>>>(g.ncell, c->d_partial, c->d_red);
     // the mixed kernel visits each pair once, the FP64 kernel twice
     k_reduce2<<<1, 256, 0, st>>>(kRedBlocks, c->d_red, mixed ? 1 : 0, mixed ? 1.0 : 0.5,
-                                1.5 / rcc, 0.5 / (rcc * rcc * rcc), d_out ? d_out : c->d_out,
-                                c->d_pairs);
+                                c1 ? 1.5 / rcc : 0.0, c1 ? 0.5 / (rcc * rcc * rcc) : 0.0,
+                                d_out ? d_out : c->d_out, c->d_pairs);
     CK(cudaGetLastError());
   }
   return PMB200_OK;
@@ -307,6 +363,39 @@ int pmb200_create(const pmb200_params *params, pmb200_ctx **out) {
     return PMB200_ECUDA;
   }
   *out = c;
+  return PMB200_OK;
+}
+
+int pmb200_create_ewald_real(const pmb200_ewald_params *params, pmb200_ctx **out) {
+  if (!params || !out) return PMB200_EINVAL;
+  *out = nullptr;
+  const pmb200_ewald_params &e = *params;
+  if (e.erfc != PMB200_ERFC_POLY5 && e.erfc != PMB200_ERFC_EXACT) return PMB200_EINVAL;
+  if (!(e.accuracy > 0.0) || !(e.accuracy < 1.0) || !std::isfinite(e.alpha))
+    return PMB200_EINVAL;
+  if (e.cellsize < 0.0) return PMB200_EINVAL;
+  // the shared construction path, with placeholder switch cutoffs
+  pmb200_params p{};
+  p.precision = e.precision;
+  p.device = e.device;
+  p.switchon = 0.0;
+  p.cutoff_lj = p.cutoff_coul = p.cutoff_alg = 1.0;
+  p.cellsize = e.cellsize;
+  pmb200_ctx *c = nullptr;
+  const int rc = pmb200_create(&p, &c);
+  if (rc) return rc;
+  c->form = e.erfc == PMB200_ERFC_EXACT ? FORM_EWALD_EXACT : FORM_EWALD_POLY5;
+  c->ew_alpha_in = e.alpha;
+  c->ew_accuracy = e.accuracy;
+  *out = c;
+  return PMB200_OK;
+}
+
+int pmb200_ewald_info(const pmb200_ctx *c, double *alpha, double *rc) {
+  if (!c || !alpha || !rc) return PMB200_EINVAL;
+  if (c->form == FORM_CUTOFF || !c->have_box || !c->have_topo) return PMB200_ESTATE;
+  *alpha = c->ew_alpha;
+  *rc = c->ew_rc;
   return PMB200_OK;
 }
 
@@ -425,6 +514,9 @@ int pmb200_set_topology(pmb200_ctx *c, int n, const int *type, const double *q_s
   int rc = ensure_atom_buffers(c);
   if (rc) return rc;
   c->have_topo = true;
+  // an Ewald context's cutoff may depend on N (default alpha): rebuild the grid
+  if (c->form != FORM_CUTOFF && c->box_given)
+    return pmb200_set_box(c, c->box_e[0], c->box_e[1], c->box_e[2], c->box_origin);
   if (c->have_box) return upload_lj(c);
   return PMB200_OK;
 }
@@ -437,15 +529,29 @@ int pmb200_set_box(pmb200_ctx *c, const double e1[3], const double e2[3], const 
       e3[1] != 0.0)
     return fail(c, PMB200_EUNSUPPORTED, "only orthogonal periodic boxes are supported");
   const double L[3] = {std::fabs(e1[0]), std::fabs(e2[1]), std::fabs(e3[2])};
-  const double rc = rc_max(c->p);
   for (int a = 0; a < 3; a++) {
     if (!(L[a] > 0.0) || !std::isfinite(L[a]))
       return fail(c, PMB200_EINVAL, "box edge %d is %g", a, L[a]);
+    if (!std::isfinite(origin[a])) return fail(c, PMB200_EINVAL, "origin");
+  }
+  if (c->form != FORM_CUTOFF) {
+    for (int k = 0; k < 3; k++) {
+      c->box_e[0][k] = e1[k]; c->box_e[1][k] = e2[k]; c->box_e[2][k] = e3[k];
+      c->box_origin[k] = origin[k];
+    }
+    c->box_given = true;
+    if (!c->have_topo) {  // alpha may need N: finish when the topology arrives
+      c->have_box = false;
+      return PMB200_OK;
+    }
+    ewald_derive(c, L);
+  }
+  const double rc = ctx_rc(c);
+  for (int a = 0; a < 3; a++) {
     if (L[a] < 2.0 * rc)
       return fail(c, PMB200_EUNSUPPORTED,
                   "box edge %g is below twice the cutoff %g (minimum image would need more "
                   "than one image per pair)", L[a], rc);
-    if (!std::isfinite(origin[a])) return fail(c, PMB200_EINVAL, "origin");
   }
   CK(cudaSetDevice(c->p.device));
   release_graph(c);
@@ -536,6 +642,8 @@ int pmb200_set_box(pmb200_ctx *c, const double e1[3], const double e2[3], const 
   m.csf = (float)c->csf;
   m.ey = (float)(g.edge[1] / u);
   m.ez = (float)(g.edge[2] / u);
+  m.ea = (float)(c->ew_alpha * u);
+  m.ea2pi = (float)(2.0 * c->ew_alpha * u / std::sqrt(M_PI));
   Fp64Consts &f = c->fc;
   const double tl = p.cutoff_lj * p.cutoff_lj - p.switchon * p.switchon;
   f.cut2 = rc * rc;
@@ -549,6 +657,9 @@ int pmb200_set_box(pmb200_ctx *c, const double e1[3], const double e2[3], const 
   f.c05_3 = 0.5 / (p.cutoff_coul * p.cutoff_coul * p.cutoff_coul);
   f.c15_3 = 1.5 / (p.cutoff_coul * p.cutoff_coul * p.cutoff_coul);
   f.csf = c->csf;
+  f.ea = c->ew_alpha;
+  f.ea2 = c->ew_alpha * c->ew_alpha;
+  f.ea2pi = 2.0 * c->ew_alpha / std::sqrt(M_PI);
   // PeriodicBoundaryConditions::set, orthogonal case (min/max corners,
   // myH, myH2, reciprocal basis, myD), for the molecule-centre image
   PbcRef &b = c->pb;
@@ -1113,11 +1224,11 @@ extern "C" int pmb200_eval_noalloc(const pmb200_params *p, int n, const double *
   k_rank_gather<<<(g.ncell + 3) / 4, 128, 0, st>>>(g.ncell, start, tmp, rel32, nullptr, d_type,
                                                     d_mol, sidx, spos32, nullptr, smeta);
   if (d_energy)
-    k_pair_mixed<true, false, false><<<g.ncell, 32 * kWarps, 0, st>>>(
+    k_pair_mixed<FORM_CUTOFF, true, false, false><<<g.ncell, 32 * kWarps, 0, st>>>(
         g, mc, half, ntypes, dlj, start, spos32, smeta, sidx, d_ex_start, d_ex, facc, n, err,
         partial, pb, nullptr);
   else
-    k_pair_mixed<false, false, false><<<g.ncell, 32 * kWarps, 0, st>>>(
+    k_pair_mixed<FORM_CUTOFF, false, false, false><<<g.ncell, 32 * kWarps, 0, st>>>(
         g, mc, half, ntypes, dlj, start, spos32, smeta, sidx, d_ex_start, d_ex, facc, n, err,
         partial, pb, nullptr);
   if (n > 0)

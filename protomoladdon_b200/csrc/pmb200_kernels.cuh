@@ -73,12 +73,26 @@ __device__ __forceinline__ void ref_min_image(const PbcRef &b, double v[3]) {
   }
 }
 
+// Pair potential of a context: ProtoMol's cutoff LJ (C2) + Coulomb (C1)
+// force, or the real-space Ewald term with erfc from the Abramowitz & Stegun
+// polynomial (the reference's default build) or from erfc itself.
+enum PairForm { FORM_CUTOFF = 0, FORM_EWALD_POLY5 = 1, FORM_EWALD_EXACT = 2 };
+
+// Abramowitz & Stegun, Handbook of Mathematical Functions, 7.1.26:
+// erfc(x) ~ t (a1 + t (a2 + t (a3 + t (a4 + t a5)))) exp(-x^2),
+// t = 1 / (1 + p x), |error| <= 1.5e-7 (the reference's poly5,
+// protomol/src/protomol/base/MathUtilities.cpp:39-49).
+constexpr double kAsP = 0.3275911;
+constexpr double kAsA1 = 0.254829592, kAsA2 = -0.284496736, kAsA3 = 1.421413741,
+                 kAsA4 = -1.453152027, kAsA5 = 1.061405429;
+
 struct MixedConsts {   // FP32 constants in cell units
   float cut2, rclj2, ron2, rcc2;
   float s1, s2, s3;          // C2
   float c15_1, c05_3, c15_3; // C1 (force path)
   float csf;                 // coulombScalingFactor
   float ey, ez;              // edge[1] / unit, edge[2] / unit (1 for cubic cells)
+  float ea, ea2pi;           // Ewald alpha and 2 alpha / sqrt(pi), per cell unit
 };
 
 struct Fp64Consts {
@@ -86,6 +100,7 @@ struct Fp64Consts {
   double s1, s2, s3;
   double c15_1, c05_3, c15_3;
   double csf;
+  double ea, ea2, ea2pi;     // Ewald alpha, alpha^2, 2 alpha / sqrt(pi) (1/A)
 };
 
 // The stencil travels by value in the kernel parameters (per launch, so
@@ -302,7 +317,7 @@ __device__ __forceinline__ void jadd(int *sh, unsigned long long *g, float v) {
     atomicAdd(g, (unsigned long long)__float2ll_rn(v * 4294967296.0f));
 }
 
-template <bool kEnergy, bool kVirial, bool kMolVir>
+template <int kForm, bool kEnergy, bool kVirial, bool kMolVir>
 __global__ void __launch_bounds__(128)
 k_pair_mixed(GridParams g, MixedConsts mc, const HalfStencil st, int ntypes, const float4 *__restrict__ lj32,
              const int *__restrict__ start, const float4 *__restrict__ spos,
@@ -314,7 +329,8 @@ k_pair_mixed(GridParams g, MixedConsts mc, const HalfStencil st, int ntypes, con
   __shared__ MixedWarpSmem s_w[kWarps];
   __shared__ long long s_f[kWarps][32][3];
   __shared__ double s_acc[kWarps][ACC_MV];
-  for (int k = threadIdx.x; k < ntypes * ntypes; k += blockDim.x) s_lj[k] = lj32[k];
+  if (kForm == FORM_CUTOFF)
+    for (int k = threadIdx.x; k < ntypes * ntypes; k += blockDim.x) s_lj[k] = lj32[k];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   MixedWarpSmem &sm = s_w[warp];
@@ -418,6 +434,28 @@ k_pair_mixed(GridParams g, MixedConsts mc, const HalfStencil st, int ntypes, con
         float rinv = rsqrtf(r2);
         rinv = fmaf(0.5f * rinv, fmaf(-r2 * rinv, rinv, 1.0f), rinv);
         const float r2inv = rinv * rinv;
+        float f;
+        if constexpr (kForm != FORM_CUTOFF) {
+          // real-space Ewald (NonbondedFullEwaldSystemForce.h:803-823):
+          // g = erfc(a r) / r, F / r = q_i q_j (g + 2a/sqrt(pi) e^{-a^2 r^2}) / r^2
+          float qj = pj.w;
+          if (kind == 1) qj *= mc.csf;
+          const float x = mc.ea * (r2 * rinv);
+          const float ex = expf(-x * x);
+          float g;
+          if constexpr (kForm == FORM_EWALD_POLY5) {
+            const float t = __fdividef(1.0f, fmaf((float)kAsP, x, 1.0f));
+            const float poly =
+                t * fmaf(t, fmaf(t, fmaf(t, fmaf(t, (float)kAsA5, (float)kAsA4), (float)kAsA3),
+                                 (float)kAsA2),
+                         (float)kAsA1);
+            g = poly * ex * rinv;
+          } else {
+            g = erfcf(x) * rinv;
+          }
+          f = pi.w * qj * fmaf(mc.ea2pi, ex, g) * r2inv;
+          if (kEnergy) kU.add(qj * g);
+        } else {
         const float4 p = s_lj[ti + mj.x];
         const float A = kind == 1 ? p.z : p.x;
         const float B = kind == 1 ? p.w : p.y;
@@ -449,7 +487,9 @@ k_pair_mixed(GridParams g, MixedConsts mc, const HalfStencil st, int ntypes, con
             kR.add(qj * r2);
           }
         }
-        const float f = flj + fc;
+        f = flj + fc;
+        if (kEnergy) pE += elj;
+        }
         const float fxv = ddx * f, fyv = ddy * f, fzv = ddz * f;  // force on j
         px -= fxv;
         py -= fyv;
@@ -460,7 +500,7 @@ k_pair_mixed(GridParams g, MixedConsts mc, const HalfStencil st, int ntypes, con
           jadd(&sm.jf[1][t], &facc[(size_t)n + jg], fyv);
           jadd(&sm.jf[2][t], &facc[2 * (size_t)n + jg], fzv);
         }
-        if (kEnergy) { pE += elj; pc++; }
+        if (kEnergy) pc++;
         if (kVirial) {
           pw0 = fmaf(fxv, ddx, pw0); pw1 = fmaf(fxv, ddy, pw1); pw2 = fmaf(fxv, ddz, pw2);
           pw3 = fmaf(fyv, ddy, pw3); pw4 = fmaf(fyv, ddz, pw4); pw5 = fmaf(fzv, ddz, pw5);
@@ -650,7 +690,7 @@ __global__ void k_finalize(int n, const unsigned long long *__restrict__ facc,
 // mixed kernel, with the reference's FP64 per-pair arithmetic
 // (OneAtomPairTwo::doOneAtomPair) in Angstrom, forces summed in FP64.
 // ---------------------------------------------------------------------------
-template <bool kEnergy, bool kVirial, bool kMolVir>
+template <int kForm, bool kEnergy, bool kVirial, bool kMolVir>
 __global__ void __launch_bounds__(128)
 k_pair_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes, const double4 *__restrict__ lj64,
             const int *__restrict__ start, const double4 *__restrict__ spos,
@@ -713,6 +753,28 @@ k_pair_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes, const dou
             kind = excl_kind(ex, elo, ehi, sidx[j]);
             if (kind == 2) continue;
           }
+          double f, e1 = 0.0, e2;
+          if constexpr (kForm != FORM_CUTOFF) {
+            // NonbondedFullEwaldSystemForce::realTerm's pair arithmetic
+            // (NonbondedFullEwaldSystemForce.h:803-823)
+            const double r = sqrt(r2);
+            double qq = pi.w * pj.w;
+            if (kind == 1) qq *= mc.csf;
+            if constexpr (kForm == FORM_EWALD_POLY5) {
+              const double rr = 1.0 / r;
+              const double ar = mc.ea * r;
+              const double e = qq * exp(-ar * ar);
+              const double t = 1.0 / (1.0 + kAsP * ar);
+              const double poly =
+                  (t) * (kAsA1 + (t) * (kAsA2 + (t) * (kAsA3 + (t) * (kAsA4 + (t) * kAsA5))));
+              e2 = poly * e * rr;
+              f = ((e2 + mc.ea2pi * e) * rr * rr);
+            } else {
+              const double a = erfc(mc.ea * r) / r;
+              e2 = qq * a;
+              f = qq * (a + mc.ea2pi * exp(-mc.ea2 * r2)) / r2;
+            }
+          } else {
           const double rd2 = 1.0 / r2;
           const double4 p = lj64[ti + mj.x];
           const double A = kind == 1 ? p.z : p.x;
@@ -720,7 +782,7 @@ k_pair_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes, const dou
           const double r6 = rd2 * rd2 * rd2;
           const double r12 = r6 * r6;
           const double r6B = B * r6, r12A = A * r12;
-          double e1 = r12A - r6B;
+          e1 = r12A - r6B;
           double f1 = 12.0 * r12A * rd2 - 6.0 * r6B * rd2;
           double sv = 1.0, sd = 0.0;
           if (r2 > mc.rclj2) sv = 0.0;
@@ -732,7 +794,7 @@ k_pair_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes, const dou
           }
           f1 = f1 * sv - e1 * sd;
           e1 = e1 * sv;
-          double e2 = pi.w * pj.w * sqrt(rd2);
+          e2 = pi.w * pj.w * sqrt(rd2);
           if (kind == 1) e2 *= mc.csf;
           double f2 = e2 * rd2;
           if (r2 > mc.rcc2) { e2 = 0.0; f2 = 0.0; }
@@ -743,7 +805,8 @@ k_pair_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes, const dou
             f2 = f2 * v - e2 * dv;
             e2 = e2 * v;
           }
-          const double f = f1 + f2;
+          f = f1 + f2;
+          }
           fx -= ddx * f; fy -= ddy * f; fz -= ddz * f;
           if (kEnergy) { accE += e1; accC += e2; accP += 1.0; }
           if (kVirial) {

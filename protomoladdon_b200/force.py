@@ -171,14 +171,7 @@ class NonbondedCutoffB200SystemForce:
     def _ensure(self, topo: PeriodicTopology):
         L = _lib.lib()
         if self._ctx is None:
-            p = _lib.Params(_lib.PMB200_MIXED if self.precision == "mixed" else _lib.PMB200_FP64,
-                            self.device, self.switchon, self.cutoff_lj, self.cutoff_coul,
-                            self.cutoff_alg, self.cellsize or topo.cellsize)
-            h = _P()
-            rc = L.pmb200_create(ctypes.byref(p), ctypes.byref(h))
-            if rc != _lib.PMB200_OK:
-                raise PmbError(rc, "pmb200_create rejected the parameters")
-            self._ctx = h
+            self._ctx = self._create(topo)
         key = (id(topo), topo.version)
         if self._topo_key != key:
             ex = topo.excl.reshape(-1)
@@ -194,6 +187,16 @@ class NonbondedCutoffB200SystemForce:
             self._check(L.pmb200_set_box(self._ctx, _ptr(e1), _ptr(e2), _ptr(e3),
                                          _ptr(topo.origin)))
             self._box_key = bkey
+
+    def _create(self, topo):
+        p = _lib.Params(_lib.PMB200_MIXED if self.precision == "mixed" else _lib.PMB200_FP64,
+                        self.device, self.switchon, self.cutoff_lj, self.cutoff_coul,
+                        self.cutoff_alg, self.cellsize or topo.cellsize)
+        h = _P()
+        rc = _lib.lib().pmb200_create(ctypes.byref(p), ctypes.byref(h))
+        if rc != _lib.PMB200_OK:
+            raise PmbError(rc, "pmb200_create rejected the parameters")
+        return h
 
     def uncache(self):
         self._topo_key = None
@@ -289,3 +292,81 @@ class NonbondedCutoffB200SystemForce:
             self.close()
         except Exception:
             pass
+
+
+class EwaldRealB200SystemForce(NonbondedCutoffB200SystemForce):
+    """The real-space term of ProtoMol's Ewald sum on the B200: stands where
+    the reference registers ``NonbondedFullEwaldSystemForce<
+    PeriodicBoundaryConditions, CubicCellManager, true, false, false,
+    CutoffSwitchingFunction>``
+    (protomol/src/protomol/module/NonbondedFullElectrostaticForceModule.cpp:34,
+    id ``Coulomb -algorithm FullEwald -real``), under its own algorithm
+    keyword ``FullEwaldB200``.  Parameters in the reference's order
+    (NonbondedFullEwaldSystemForce::getParameters): ``-alpha`` (<= 0: the
+    reference's default from N and the volume) and ``-accuracy`` (> 0);
+    rc = sqrt(-log(accuracy)) / alpha.  ``erfc`` picks the Abramowitz & Stegun
+    polynomial of the reference's default build ("poly5") or erfc itself
+    ("exact", the reference built with -DUSE_EWALD_EXACT_ERF).  The energy
+    goes to COULOMB; everything else is inherited."""
+
+    keyword = "FullEwaldB200"
+
+    def __init__(self, alpha=-1.0, accuracy=1e-5, precision="mixed", device=0, cellsize=0.0,
+                 erfc="poly5"):
+        if not accuracy > 0.0:
+            raise ValueError(f"accuracy (={accuracy}) must be positive")
+        if erfc not in ("poly5", "exact"):
+            raise ValueError("erfc must be 'poly5' or 'exact'")
+        self.alpha = float(alpha)
+        self.accuracy = float(accuracy)
+        self.erfc = erfc
+        self.precision = precision
+        self.device = int(device)
+        self.cellsize = float(cellsize)
+        self._ctx = None
+        self._topo_key = None
+        self._box_key = None
+
+    @classmethod
+    def make(cls, values, **kw):
+        """values in the reference's order: alpha, accuracy."""
+        if len(values) != 2:
+            raise ValueError(f"{cls.keyword} takes 2 parameters, got {len(values)}")
+        return cls(float(values[0]), float(values[1]), **kw)
+
+    @classmethod
+    def from_id(cls, force_id, **kw):
+        """Parses ``Coulomb -algorithm FullEwaldB200 -real -alpha 0.3
+        -accuracy 1e-6`` (-alpha and -accuracy may be left out: -1 and 1e-5,
+        the reference's defaults)."""
+        toks = force_id.split()
+        if not toks or toks[0] != "Coulomb":
+            raise ValueError("expected the 'Coulomb' potential")
+        if "-real" not in toks or "-reciprocal" in toks or "-correction" in toks:
+            raise ValueError("only the real-space term (-real) is offered")
+        rest = [t for t in toks[1:] if t != "-real"]
+        opts = dict(zip(rest[0::2], rest[1::2]))
+        if len(rest) % 2 or opts.get("-algorithm") != cls.keyword:
+            raise ValueError(f"cannot parse force id {force_id!r}")
+        return cls(float(opts.get("-alpha", -1.0)), float(opts.get("-accuracy", 1e-5)), **kw)
+
+    def get_id(self):
+        return (f"Coulomb -algorithm {self.keyword} -real -alpha {self.alpha:g} "
+                f"-accuracy {self.accuracy:g}")
+
+    def _create(self, topo):
+        p = _lib.EwaldParams(
+            _lib.PMB200_MIXED if self.precision == "mixed" else _lib.PMB200_FP64, self.device,
+            _lib.PMB200_ERFC_EXACT if self.erfc == "exact" else _lib.PMB200_ERFC_POLY5,
+            self.alpha, self.accuracy, self.cellsize or topo.cellsize)
+        h = _P()
+        rc = _lib.lib().pmb200_create_ewald_real(ctypes.byref(p), ctypes.byref(h))
+        if rc != _lib.PMB200_OK:
+            raise PmbError(rc, "pmb200_create_ewald_real rejected the parameters")
+        return h
+
+    def ewald_info(self):
+        """(alpha, rc) in use, once the topology and box are set."""
+        a, r = ctypes.c_double(), ctypes.c_double()
+        self._check(_lib.lib().pmb200_ewald_info(self._ctx, ctypes.byref(a), ctypes.byref(r)))
+        return a.value, r.value

@@ -8,7 +8,8 @@ import numpy as np
 import pytest
 
 from protomoladdon_b200 import _lib, water
-from protomoladdon_b200.force import NonbondedCutoffB200SystemForce, PeriodicTopology
+from protomoladdon_b200.force import (EwaldRealB200SystemForce, NonbondedCutoffB200SystemForce,
+                                      PeriodicTopology)
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -57,6 +58,41 @@ def test_force_id_parse_and_make():
             "-switchingFunction C1 -switchon 9 -cutoff 10 -cutoff 10 -cutoff 10")
     with pytest.raises(ValueError):
         NonbondedCutoffB200SystemForce.make([1, 2, 3])
+
+
+def test_ewald_create_validates_before_touching_a_device():
+    L = _lib.lib()
+    h = ctypes.c_void_p()
+    bad = [
+        _lib.EwaldParams(0, 0, 0, 0.3, 0.0, 0.0),   # accuracy must be > 0
+        _lib.EwaldParams(0, 0, 0, 0.3, 1.0, 0.0),   # and < 1 (rc = 0)
+        _lib.EwaldParams(0, 0, 5, 0.3, 1e-6, 0.0),  # unknown erfc form
+        _lib.EwaldParams(0, 0, 0, float("nan"), 1e-6, 0.0),
+        _lib.EwaldParams(0, 0, 0, 0.3, 1e-6, -1.0),  # negative cell size
+    ]
+    for p in bad:
+        assert L.pmb200_create_ewald_real(ctypes.byref(p), ctypes.byref(h)) == _lib.PMB200_EINVAL
+    assert L.pmb200_create_ewald_real(None, ctypes.byref(h)) == _lib.PMB200_EINVAL
+    a, r = ctypes.c_double(), ctypes.c_double()
+    assert L.pmb200_ewald_info(None, ctypes.byref(a), ctypes.byref(r)) == _lib.PMB200_EINVAL
+
+
+def test_ewald_force_id_parse_and_make():
+    f = EwaldRealB200SystemForce.from_id(
+        "Coulomb -algorithm FullEwaldB200 -real -alpha 0.3 -accuracy 2.35e-6")
+    assert (f.alpha, f.accuracy, f.erfc) == (0.3, 2.35e-6, "poly5")
+    assert EwaldRealB200SystemForce.from_id(f.get_id()).get_id() == f.get_id()
+    d = EwaldRealB200SystemForce.from_id("Coulomb -algorithm FullEwaldB200 -real")
+    assert (d.alpha, d.accuracy) == (-1.0, 1e-5)  # the reference's defaults
+    assert EwaldRealB200SystemForce.make([0.25, 1e-6], erfc="exact").erfc == "exact"
+    for bad in ("Coulomb -algorithm FullEwaldB200 -real -reciprocal",
+                "Coulomb -algorithm FullEwald -real", "LennardJones -algorithm FullEwaldB200"):
+        with pytest.raises(ValueError):
+            EwaldRealB200SystemForce.from_id(bad)
+    with pytest.raises(ValueError):
+        EwaldRealB200SystemForce.make([0.3, 0.0])
+    with pytest.raises(ValueError):
+        EwaldRealB200SystemForce.make([0.3])
 
 
 @pytest.mark.parametrize("k,n", [(6, 648), (24, 41472)])
