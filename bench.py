@@ -24,6 +24,10 @@ Default arm (libpmb200 on B200):
   cpu_baseline -- the reference's own CPU force (oracle/_ref, compiled from
             the reference sources) driving the same leapfrog on one host core.
 
+--workload large: the 327,352-atom ion box (one force evaluation per step)
+with both pair kernels, LJ+C1 and the real-space Ewald term; its line's
+value is Gpairs/s of whole LJ+C1 evaluations.
+
 --impl reference: the reference CPU implementation alone, one independent
 replica per host core (the reference force is serial), bounded sample.
 
@@ -378,6 +382,169 @@ def run_ours(args):
     return 0
 
 
+LARGE_WORKLOAD = ("ion water box: 327,352 atoms (110,592 lattice sites, 48^3 lattice, box "
+                  "148.992 A, 2% of waters replaced by Na+/Cl-), rc 12: LJ C2 11-12 A + "
+                  "Coulomb C1 12 A, and the Ewald real-space term erfc(0.30 r)/r")
+LARGE_METRIC = "Gpairs/s, 331k-atom ion box: LJ+C1 and Ewald real-space kernels, mixed vs FP64"
+
+
+def run_large(args):
+    """The large system's two pair kernels, one evaluation per step.  value =
+    unique in-cutoff pairs per second of whole device-resident evaluations
+    (cell build + pair kernel + fixed-point finalize) of the LJ+C1 force;
+    the Ewald real-space kernel, the FP64 kernels, the pair kernels alone and
+    the host-buffer C-ABI call (e2e) are reported beside it."""
+    import torch
+    from protomoladdon_b200 import water
+    from protomoladdon_b200.force import (EwaldRealB200SystemForce,
+                                          NonbondedCutoffB200SystemForce, PeriodicTopology,
+                                          ScalarStructure)
+    if env_int("WORLD_SIZE", 1) > 1 and env_int("RANK", 0) != 0:
+        return 0  # one box, one GPU: replicas are the medium workload's business
+    dev = torch.device("cuda", env_int("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    s = water.large_331k()
+    n = s["n"]
+    topo = PeriodicTopology.from_dict(s)
+    acc = float(np.exp(-(0.30 * 12.0) ** 2))  # rc = sqrt(-log acc) / alpha = 12 A
+    makers = {
+        "cutoff": lambda p: NonbondedCutoffB200SystemForce(s["ron"], s["rc_lj"], s["rc_coul"],
+                                                           s["rc_alg"], precision=p),
+        "ewald_real": lambda p: EwaldRealB200SystemForce(0.30, acc, precision=p),
+    }
+    stream = torch.cuda.Stream(device=dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    pos = torch.tensor(s["pos"], dtype=torch.float64, device=dev)
+    frc = torch.zeros_like(pos)
+    out = torch.zeros(20, dtype=torch.float64, device=dev)
+    sp = stream.cuda_stream
+
+    def device_times(f):
+        f.evaluate_device(topo, pos.data_ptr(), frc.data_ptr(), out.data_ptr(), 1, sp)
+        stream.synchronize()
+        f.sync()
+        pairs = f.last_pair_count()
+        for _ in range(args.warmup):
+            f.evaluate_device(topo, pos.data_ptr(), frc.data_ptr(), None, 0, sp)
+        e0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        e1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        torch.cuda.synchronize(dev)
+        for k in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                e0[k].record(stream)
+            f.evaluate_device(topo, pos.data_ptr(), frc.data_ptr(), None, 0, sp)
+            e1[k].record(stream)
+        torch.cuda.synchronize(dev)
+        f.sync()
+        eval_ms = statistics.mean(a.elapsed_time(b) for a, b in zip(e0, e1))
+        f.set_kernel_timing(True)
+        kms = []
+        for _ in range(min(args.steps, 20)):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            f.evaluate_device(topo, pos.data_ptr(), frc.data_ptr(), None, 0, sp)
+            stream.synchronize()
+            kms.append(f.last_kernel_ms())
+        f.set_kernel_timing(False)
+        f.sync()
+        return eval_ms, statistics.mean(kms), pairs
+
+    def host_eval(f, reps):
+        F = np.zeros_like(s["pos"])
+        E = ScalarStructure()
+        f.evaluate(topo, s["pos"], F, E)
+        ts = []
+        for _ in range(reps):
+            F[:] = 0.0
+            E.clear()
+            flush.zero_()
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            f.evaluate(topo, s["pos"], F, E)
+            ts.append(time.perf_counter() - t0)
+        return statistics.mean(ts), F, E
+
+    peak = ctypes_peak(dev.index)
+    res = {}
+    with ClockSampler(dev.index) as clk:
+        for name, mk in makers.items():
+            for prec in ("mixed", "fp64"):
+                f = mk(prec)
+                eval_ms, k_ms, pairs = device_times(f)
+                e2e_s, F, E = host_eval(f, min(args.steps, 20))
+                f.close()
+                res[(name, prec)] = dict(eval_ms=eval_ms, pair_kernel_ms=k_ms, pairs=pairs,
+                                         e2e_ms=e2e_s * 1e3, F=F, E=E)
+    clocks = clk.summary()
+
+    def kernel_obj(name, prec):
+        r = res[(name, prec)]
+        achieved = FLOPS_PER_PAIR * r["pairs"] / (r["pair_kernel_ms"] * 1e-3) / 1e12
+        o = {"eval_ms": r["eval_ms"], "pair_kernel_ms": r["pair_kernel_ms"],
+             "pairs_per_eval": r["pairs"],
+             "gpairs_per_s": r["pairs"] / (r["eval_ms"] * 1e-3) / 1e9,
+             "gpairs_per_s_pair_kernel": r["pairs"] / (r["pair_kernel_ms"] * 1e-3) / 1e9,
+             "e2e_ms": r["e2e_ms"],
+             "roofline": {"bound": "fp32" if prec == "mixed" else "fp64",
+                          "achieved": achieved,
+                          "peak": peak if prec == "mixed" else None, "unit": "TFLOP/s",
+                          "frac": achieved / peak if (peak and prec == "mixed") else None}}
+        return o
+
+    line = {
+        "metric": LARGE_METRIC, "unit": "Gpairs/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": LARGE_WORKLOAD, "atoms": n,
+                   "l2": "flushed before every timed evaluation (256 MiB write)",
+                   "step": "one force evaluation (cell build + pair kernel + finalize)"},
+    }
+    cut = kernel_obj("cutoff", "mixed")
+    line["value"] = cut["gpairs_per_s"]
+    line["ms_per_step"] = cut["eval_ms"]
+    line["roofline"] = dict(cut["roofline"], traffic=None,
+                            peak_source="FP32 FMA throughput measured in this run")
+    line["kernels"] = {f"{nm}_{p}": kernel_obj(nm, p) for nm in makers for p in ("mixed", "fp64")}
+    line["mixed_speedup_vs_fp64"] = {
+        nm: res[(nm, "fp64")]["eval_ms"] / res[(nm, "mixed")]["eval_ms"] for nm in makers}
+    line["e2e"] = {"value": cut["pairs_per_eval"] / (cut["e2e_ms"] * 1e-3) / 1e9,
+                   "unit": "Gpairs/s", "ms_per_step": cut["e2e_ms"],
+                   "h2d_bytes_per_step": 24 * n, "d2h_bytes_per_step": 24 * n + 160}
+    line["gpu_launches"] = 6 * args.steps  # cell_index, scan, scatter, rank_gather, pair, finalize
+    line["clocks"] = clocks
+    if not args.skip_accuracy:
+        from oracle import oracle as O
+        fo, eo, _, _ = O.restate_eval(s, s["pos"], virial_mode=0)
+        fe, ee, _, _ = O.restate_ewald_real(s, s["pos"], 0.30, acc, False, virial_mode=0)
+        acc_o = {}
+        for nm, (fref, eref) in (("cutoff", (fo, eo[0] + eo[1])), ("ewald_real", (fe, ee))):
+            for p in ("mixed", "fp64"):
+                r = res[(nm, p)]
+                acc_o[f"{nm}_{p}"] = {
+                    "force_rms_rel_err": float(np.sqrt(((r["F"] - fref) ** 2).sum()
+                                                       / (fref ** 2).sum())),
+                    "energy_abs_err": float(abs(r["E"][0] + r["E"][1] - eref))}
+        line["accuracy_vs_fp64_oracle"] = acc_o
+    if not args.skip_cpu:
+        from oracle import oracle as O
+        t0 = time.perf_counter()
+        if O.ref_available():
+            R = O.RefForce(s)
+            R.evaluate(s["pos"], 0)
+            R.close()
+            kind = "reference"
+        else:
+            O.restate_eval(s, s["pos"], virial_mode=0)
+            kind = "port"
+        t_cpu = time.perf_counter() - t0
+        line["cpu_baseline"] = {
+            "value": cut["pairs_per_eval"] / t_cpu / 1e9, "unit": "Gpairs/s", "cores": 1,
+            "kind": kind, "sample": f"one LJ+C1 evaluation of the same box, {t_cpu:.1f} s"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def ctypes_peak(device):
     import ctypes
     from protomoladdon_b200 import _lib
@@ -404,11 +571,16 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--skip-accuracy", action="store_true")
+    ap.add_argument("--workload", default="medium", choices=["medium", "large"],
+                    help="medium: the 41,472-atom water box (the headline); large: the "
+                         "327,352-atom ion box's LJ+C1 and Ewald real-space kernels")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "large":
+        return run_large(args)
     return run_ours(args)
 
 
