@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "pmb200.h"
+#include "B200TopologyUpload.h"
 
 namespace ProtoMol {
 
@@ -135,36 +136,9 @@ private:
     if (rc) THROW(std::string("B200 cutoff force: ") + pmb200_last_error(myCtx));
   }
 
-  // Copies the arrays OneAtomPairTwo::doOneAtomPair reads
-  // (protomol/src/protomol/force/OneAtomPairTwo.h:57-125) and the box.
+  // Copies the topology arrays the pair function reads and the box.
   void upload(const RealTopologyType &t) {
-    const int n = (int)t.atoms.size();
-    const int nt = t.lennardJonesParameters.size();
-    std::vector<int> type(n > 0 ? n : 1), mol(n > 0 ? n : 1);
-    std::vector<double> q(n > 0 ? n : 1), mass(n > 0 ? n : 1), lj(4 * nt * nt > 0 ? 4 * nt * nt : 4);
-    for (int i = 0; i < n; i++) {
-      type[i] = t.atoms[i].type;
-      q[i] = t.atoms[i].scaledCharge;
-      mol[i] = t.atoms[i].molecule;
-      mass[i] = t.atoms[i].scaledMass;
-    }
-    for (int a = 0; a < nt; a++)
-      for (int b = 0; b < nt; b++) {
-        const LennardJonesParameters &l = t.lennardJonesParameters(a, b);
-        double *o = &lj[4 * (a * nt + b)];
-        o[0] = l.A; o[1] = l.B; o[2] = l.A14; o[3] = l.B14;
-      }
-    const std::vector<ExclusionPair> &table = t.exclusions.getTable();
-    std::vector<int> ex(3 * table.size() + 3);
-    for (size_t k = 0; k < table.size(); k++) {
-      ex[3 * k] = table[k].a1;
-      ex[3 * k + 1] = table[k].a2;
-      ex[3 * k + 2] = (int)table[k].excl;
-    }
-    check(pmb200_set_topology(myCtx, n, &type[0], &q[0], &mol[0], &mass[0], nt, &lj[0],
-                              (int)table.size(), &ex[0], t.coulombScalingFactor));
-    const PeriodicBoundaryConditions &bc = t.boundaryConditions;
-    check(pmb200_set_box(myCtx, bc.e1().c, bc.e2().c, bc.e3().c, bc.origin().c));
+    check(b200UploadTopology(myCtx, t));
     myCached = &t;
   }
 

@@ -1,6 +1,6 @@
 /* -*- c++ -*- */
-// ProtoMol module that registers the B200 cutoff force with the app's
-// ForceFactory, following the module hooks of
+// ProtoMol module that registers the B200 forces (the cutoff LJ + Coulomb
+// force and the Ewald real-space term) with the app's ForceFactory, following the module hooks of
 // protomol/src/protomol/base/Module.h (registerForces) and the periodic-only
 // registration of NonbondedCutoffForceModule::registerForces
 // (protomol/src/protomol/module/NonbondedCutoffForceModule.cpp:38-76).
@@ -17,13 +17,14 @@ class ForceFactory;
 
 class B200ForceModule : public Module {
 public:
-  const std::string getName() const { return "B200CutoffForce"; }
+  const std::string getName() const { return "B200Forces"; }
   void registerForces(ProtoMolApp *app);
 };
 
-// Registers the prototype with a factory directly (what registerForces does
+// Register the prototypes with a factory directly (what registerForces does
 // for a periodic configuration); for hosts that build their own factory.
 void registerB200CutoffForce(ForceFactory &factory);
+void registerB200EwaldRealForce(ForceFactory &factory);
 }  // namespace ProtoMol
 
 #endif

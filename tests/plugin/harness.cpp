@@ -3,10 +3,13 @@
 // Topology.  Built by tests/plugin/Makefile against the reference library
 // compiled under oracle/_ref; used only by tests/test_plugin_gpu.py.
 #include "B200CutoffSystemForce.h"
+#include "B200EwaldRealSystemForce.h"
 #include "B200ForceModule.h"
 
 #include <protomol/factory/ForceFactory.h>
 #include <protomol/force/nonbonded/NonbondedCutoffSystemForce.h>
+#include <protomol/force/nonbonded/NonbondedFullEwaldSystemForce.h>
+#include <protomol/switch/CutoffSwitchingFunction.h>
 #include <protomol/force/OneAtomPairTwo.h>
 #include <protomol/force/LennardJonesForce.h>
 #include <protomol/force/CoulombForce.h>
@@ -29,6 +32,9 @@ typedef NonbondedCutoffSystemForce<
     CubicCellManager, OneAtomPairTwo<PeriodicBoundaryConditions, C2SwitchingFunction,
                                      LennardJonesForce, C1SwitchingFunction, CoulombForce> >
     RefForce;
+typedef NonbondedFullEwaldSystemForce<PeriodicBoundaryConditions, CubicCellManager, true, false,
+                                      false, CutoffSwitchingFunction>
+    RefEwaldReal;
 
 static char g_msg[1024];
 
@@ -81,6 +87,41 @@ extern "C" int harness_eval(void *ref_handle, int which, int n, const double *po
     std::string id = std::string(base) + (which == 0 ? "NonbondedCutoff" : "NonbondedCutoffB200");
     if (which == 2) id = "time " + id;
     Force *force = make_force(factory, id, ron, rclj, rcc, rc);
+    if (!force) {
+      std::strncpy(g_msg, ("factory could not make '" + id + "'").c_str(), sizeof(g_msg) - 1);
+      return 1;
+    }
+    std::strncpy(g_msg, force->getId().c_str(), sizeof(g_msg) - 1);
+    eval_force(force, t, pos, n, forces, energies, virial, molvirial);
+    delete force;
+    return 0;
+  } catch (const std::exception &e) {
+    std::strncpy(g_msg, e.what(), sizeof(g_msg) - 1);
+  } catch (...) {
+    std::strncpy(g_msg, "unknown exception", sizeof(g_msg) - 1);
+  }
+  return 1;
+}
+
+// The Ewald real-space term: which 0 = the reference prototype
+// ("Coulomb -algorithm FullEwald -real"), 1 = the B200 plugin
+// ("Coulomb -algorithm FullEwaldB200 -real"); made by the factory from the id
+// and the values {alpha, accuracy}.
+extern "C" int harness_ewald_eval(void *ref_handle, int which, int n, const double *pos,
+                                  double alpha, double accuracy, double *forces,
+                                  double *energies, double *virial, double *molvirial) {
+  g_msg[0] = 0;
+  try {
+    PTopo *t = (PTopo *)pmref_topology(ref_handle);
+    ForceFactory factory;
+    factory.reg(new RefEwaldReal());
+    registerB200EwaldRealForce(factory);
+    std::string id = which == 0 ? "Coulomb -algorithm FullEwald -real"
+                                : "Coulomb -algorithm FullEwaldB200 -real";
+    std::vector<Value> v;
+    v.push_back(Value(alpha));
+    v.push_back(Value(accuracy));
+    Force *force = factory.make(id, v);
     if (!force) {
       std::strncpy(g_msg, ("factory could not make '" + id + "'").c_str(), sizeof(g_msg) - 1);
       return 1;

@@ -37,3 +37,22 @@ def evaluate(ref_force, which, sysd, pos):
                         float(sysd["rc_lj"]), float(sysd["rc_coul"]), float(sysd["rc_alg"]),
                         f.ctypes.data, e.ctypes.data, v.ctypes.data, mv.ctypes.data)
     return rc, L.harness_message().decode(), f, e, v, mv
+
+
+def evaluate_ewald(ref_force, which, sysd, pos, alpha, accuracy):
+    """The Ewald real-space term through the factory: which 0 reference
+    prototype ("Coulomb -algorithm FullEwald -real"), 1 B200 plugin.
+    Returns (rc, message, forces, energies, virial, molvirial)."""
+    L = lib()
+    L.harness_ewald_eval.argtypes = [_P, _I, _I, _P, _D, _D, _P, _P, _P, _P]
+    L.harness_ewald_eval.restype = _I
+    p = np.ascontiguousarray(pos, dtype=np.float64)
+    n = p.shape[0]
+    f = np.zeros((n, 3))
+    e = np.zeros(2)
+    v = np.zeros(9)
+    mv = np.zeros(9)
+    rc = L.harness_ewald_eval(ref_force.h, which, n, p.ctypes.data, float(alpha),
+                              float(accuracy), f.ctypes.data, e.ctypes.data, v.ctypes.data,
+                              mv.ctypes.data)
+    return rc, L.harness_message().decode(), f, e, v, mv

@@ -56,3 +56,52 @@ def test_plugin_matches_reference_through_factory(water648, which):
     vr = water648["ref_virial"]
     assert np.abs(v - vr).max() <= 1e-5 * np.abs(vr).max()
     assert np.abs(mv - water648["ref_molvirial"]).max() <= 1e-5 * np.abs(vr).max()
+
+
+def _ewald_fixture():
+    from .conftest import load_fixture
+    return load_fixture("ewald_water_ref.npz")
+
+
+def test_factory_resolves_reference_ewald_real_id():
+    d = _ewald_fixture()
+    R = O.RefForce(d)
+    rc, msg, f, e, v, mv = H.evaluate_ewald(R, 0, d, d["pos"], float(d["alpha"]),
+                                            float(d["accuracy"]))
+    R.close()
+    assert rc == 0, msg
+    assert "FullEwald -real" in msg
+    np.testing.assert_allclose(f, d["poly5_forces"], rtol=0, atol=1e-11)
+    assert abs(e[0] - float(d["poly5_energy"])) <= 1e-11 * abs(float(d["poly5_energy"]))
+
+
+def test_plugin_ewald_id_resolves_to_b200_force():
+    d = _ewald_fixture()
+    R = O.RefForce(d)
+    rc, msg, *_ = H.evaluate_ewald(R, 1, d, d["pos"], float(d["alpha"]), float(d["accuracy"]))
+    R.close()
+    assert (rc == 0 and "FullEwaldB200 -real" in msg) or "B200 Ewald real-space force" in msg
+
+
+def test_plugin_ewald_rejects_bad_accuracy():
+    d = _ewald_fixture()
+    R = O.RefForce(d)
+    rc, msg, *_ = H.evaluate_ewald(R, 1, d, d["pos"], 0.3, -1.0)
+    R.close()
+    assert rc == 1
+
+
+@pytest.mark.gpu
+def test_plugin_ewald_matches_reference_through_factory():
+    d = _ewald_fixture()
+    R = O.RefForce(d)
+    rc, msg, f, e, v, mv = H.evaluate_ewald(R, 1, d, d["pos"], float(d["alpha"]),
+                                            float(d["accuracy"]))
+    R.close()
+    assert rc == 0, msg
+    fr = d["poly5_forces"]
+    assert np.sqrt(((f - fr) ** 2).sum() / (fr ** 2).sum()) <= 1e-5
+    # |dE| <= 1e-6 of the pair magnitudes (64,495 kcal/mol on this box)
+    assert abs(e[0] - float(d["poly5_energy"])) <= 0.065 and e[1] == 0.0
+    vr = d["poly5_virial"]
+    assert np.abs(v - vr).max() <= 1e-5 * np.abs(vr).max()
