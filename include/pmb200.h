@@ -225,6 +225,38 @@ int pmb200_eval_noalloc(const pmb200_params *params, int n, const double *d_pos,
 /* Geometry of the device cell grid chosen for the current box. */
 int pmb200_grid(const pmb200_ctx *ctx, int dims[3], double edge[3]);
 
+/* ---- derivatives (the differentiable form) ----
+ * FP64 pair arithmetic whatever the context's precision; contexts of the
+ * cutoff kind only (PMB200_EUNSUPPORTED otherwise).  Units and tables are the
+ * ones set_topology takes: q_scaled, and the LJ table entries
+ * {A, B, A14, B14} per ordered type pair (a, b) as the pair loop reads them
+ * (an unordered pair's derivative is split half to (a, b), half to (b, a)).
+ * Work is queued on `stream` (NULL: the context's stream).
+ *
+ * Parameter gradients: d_dq[n] = dE/dq_scaled per atom, d_dlj[ntypes^2 * 4]
+ * = dE/d{A, B, A14, B14}, both overwritten (E = LJ + Coulomb energy).  The
+ * reference has no such entry: it replaces finite differences of
+ * SystemForce::evaluate over its parameters.  */
+int pmb200_param_grad_device(pmb200_ctx *ctx, const double *d_pos, double *d_dq,
+                             double *d_dlj, void *stream);
+
+/* Hessian-vector product and the mixed second derivatives for a direction
+ * w[3n]: d_hv[3n] = H w (H = d^2 E / dx dx), and, for w . grad_x E, its
+ * derivatives d_dq[n] (per q_scaled) and d_dlj[ntypes^2 * 4] (per table
+ * entry); all overwritten; d_dq / d_dlj may be NULL.  Replaces forming the
+ * dense pair Hessian of Hessian::evaluate
+ * (protomol/src/protomol/integrator/hessian/Hessian.cpp:353-568, pair blocks
+ * 581-691 with ReducedHessLennardJones / ReducedHessCoulomb and the switch
+ * Hessians) and multiplying by w. */
+int pmb200_hvp_device(pmb200_ctx *ctx, const double *d_pos, const double *d_w, double *d_hv,
+                      double *d_dq, double *d_dlj, void *stream);
+
+/* New charges (q_scaled[n]) and/or LJ table (lj[ntypes^2 * 4]) for the same
+ * topology; either may be NULL.  Host arrays; the copy is synchronous, so
+ * call it when no evaluation of this context is in flight (pmb200_sync).
+ * Replaces rebuilding the topology to change force-field parameters. */
+int pmb200_update_params(pmb200_ctx *ctx, const double *q_scaled, const double *lj);
+
 /* ---- Ewald real-space term ----
  * A context of the second kind replaces the real-space part of ProtoMol's
  * Ewald sum,

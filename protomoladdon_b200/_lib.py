@@ -38,6 +38,7 @@ EXPORTED = (
     "pmb200_step_device", "pmb200_set_kernel_timing", "pmb200_last_kernel_ms",
     "pmb200_measure_fp32_peak", "pmb200_set_rigid_waters", "pmb200_host_kick_drift",
     "pmb200_eval_noalloc", "pmb200_create_ewald_real", "pmb200_ewald_info",
+    "pmb200_param_grad_device", "pmb200_hvp_device", "pmb200_update_params",
 )
 
 _P = ctypes.c_void_p
@@ -96,6 +97,9 @@ def lib():
                                       _D, _P, _P, _P, _P, _P]
     L.pmb200_create_ewald_real.argtypes = [ctypes.POINTER(EwaldParams), ctypes.POINTER(_P)]
     L.pmb200_ewald_info.argtypes = [_P, ctypes.POINTER(_D), ctypes.POINTER(_D)]
+    L.pmb200_param_grad_device.argtypes = [_P, _P, _P, _P, _P]
+    L.pmb200_hvp_device.argtypes = [_P, _P, _P, _P, _P, _P, _P]
+    L.pmb200_update_params.argtypes = [_P, _P, _P]
     for name in EXPORTED:
         getattr(L, name).restype = getattr(L, name).restype or _I
     L.pmb200_last_error.restype = ctypes.c_char_p

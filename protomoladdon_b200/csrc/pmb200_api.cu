@@ -66,6 +66,9 @@ struct pmb200_ctx {
   int2 *d_smeta = nullptr;
   unsigned long long *d_facc = nullptr;
   double *d_com = nullptr;
+  // derivative kernels: per-block table rows and scratch outputs
+  double *d_tpart = nullptr, *d_gq = nullptr, *d_glj = nullptr;
+  size_t tpart_alloc = 0, gq_alloc = 0, glj_alloc = 0;
   double *d_pairs = nullptr, *d_out = nullptr, *d_red = nullptr;
   // rigid waters (SETTLE) for the device integrator
   int nwater = 0, nfree = 0;
@@ -238,15 +241,13 @@ void launch_pair_fp64(pmb200_ctx *c, unsigned flags, double *d_forces, int accum
 
 // Launch one evaluation on `st`.  accumulate: add into d_forces (1) or
 // overwrite it (0).
-int launch_eval(pmb200_ctx *c, const double *d_pos, double *d_forces, double *d_out,
-                unsigned flags, int accumulate, cudaStream_t st) {
+// Counting sort of the atoms into the grid cells (cell index, scan,
+// scatter, in-cell rank order), producing the cell-unit FP32 copies (mixed)
+// or the Angstrom FP64 copies of the sorted positions.
+void launch_cell_build(pmb200_ctx *c, const double *d_pos, bool mixed, cudaStream_t st) {
   const int n = c->n;
-  const bool mixed = c->p.precision == PMB200_MIXED;
-  const bool energy = (flags & PMB200_ENERGY) != 0;
-  const bool virial = (flags & (PMB200_VIRIAL | PMB200_MOLVIRIAL)) != 0;
-  const bool molvir = (flags & PMB200_MOLVIRIAL) != 0;
   const GridParams &g = c->g;
-  CK(cudaMemsetAsync(c->d_count, 0, sizeof(int) * g.ncell, st));
+  cudaMemsetAsync(c->d_count, 0, sizeof(int) * g.ncell, st);
   if (n > 0) {
     const int tb = 256;
     k_cell_index<<<(n + tb - 1) / tb, tb, 0, st>>>(
@@ -259,12 +260,24 @@ int launch_eval(pmb200_ctx *c, const double *d_pos, double *d_forces, double *d_
     k_scatter<<<(n + tb - 1) / tb, tb, 0, st>>>(n, c->d_cell_of, c->d_slot, c->d_start,
                                                  c->d_tmp);
   }
-  const int warps_per_block = 4;
-  const int blocks = (g.ncell + warps_per_block - 1) / warps_per_block;
-  k_rank_gather<<<blocks, 32 * warps_per_block, 0, st>>>(
+  const int blocks = (g.ncell + 3) / 4;
+  k_rank_gather<<<blocks, 128, 0, st>>>(
       g.ncell, c->d_start, c->d_tmp, mixed ? c->d_rel32 : nullptr,
       mixed ? nullptr : c->d_rel64, c->d_type, c->d_mol, c->d_sidx,
       mixed ? c->d_spos32 : nullptr, mixed ? nullptr : c->d_spos64, c->d_smeta);
+}
+
+int launch_eval(pmb200_ctx *c, const double *d_pos, double *d_forces, double *d_out,
+                unsigned flags, int accumulate, cudaStream_t st) {
+  const int n = c->n;
+  const bool mixed = c->p.precision == PMB200_MIXED;
+  const bool energy = (flags & PMB200_ENERGY) != 0;
+  const bool virial = (flags & (PMB200_VIRIAL | PMB200_MOLVIRIAL)) != 0;
+  const bool molvir = (flags & PMB200_MOLVIRIAL) != 0;
+  const GridParams &g = c->g;
+  launch_cell_build(c, d_pos, mixed, st);
+  CK(cudaGetLastError());
+  const int blocks = (g.ncell + 3) / 4;
   if (molvir && c->nmol > 0)
     k_com<<<(c->nmol + 127) / 128, 128, 0, st>>>(c->nmol, c->d_mstart, c->d_matoms, c->d_mass,
                                                   d_pos, c->d_com);
@@ -411,6 +424,7 @@ int pmb200_destroy(pmb200_ctx *c) {
   dfree(c->d_cell_of); dfree(c->d_slot); dfree(c->d_tmp); dfree(c->d_sidx);
   dfree(c->d_rel32); dfree(c->d_spos32); dfree(c->d_rel64); dfree(c->d_spos64);
   dfree(c->d_smeta); dfree(c->d_com); dfree(c->d_facc);
+  dfree(c->d_tpart); dfree(c->d_gq); dfree(c->d_glj);
   dfree(c->d_pairs); dfree(c->d_out); dfree(c->d_red); dfree(c->d_widx); dfree(c->d_fidx);
   if (c->h_pin_pos) cudaFreeHost(c->h_pin_pos);
   if (c->h_pin_frc) cudaFreeHost(c->h_pin_frc);
@@ -689,6 +703,96 @@ int pmb200_eval_device(pmb200_ctx *c, const double *d_pos, double *d_forces, dou
   CK(cudaSetDevice(c->p.device));
   cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
   return launch_eval(c, d_pos, d_forces, d_out, flags, 1, st);
+}
+
+// Derivative kernels (FP64 pair arithmetic whatever the context's
+// precision; cutoff form only).
+static int launch_deriv(pmb200_ctx *c, int mode, const double *d_pos, const double *d_w,
+                        double *d_hv, double *d_dq, double *d_dlj, cudaStream_t st) {
+  const GridParams &g = c->g;
+  const int blocks = (g.ncell + 3) / 4;
+  const size_t nt4 = (size_t)c->ntypes * c->ntypes * 4;
+  if (c->tpart_alloc < (size_t)blocks * nt4) {
+    CK(dalloc(c->d_tpart, (size_t)blocks * nt4));
+    c->tpart_alloc = (size_t)blocks * nt4;
+  }
+  if (!d_dq) {
+    if (c->gq_alloc < (size_t)std::max(c->n, 1)) {
+      CK(dalloc(c->d_gq, (size_t)std::max(c->n, 1)));
+      c->gq_alloc = (size_t)std::max(c->n, 1);
+    }
+    d_dq = c->d_gq;
+  }
+  if (!d_dlj) {
+    if (c->glj_alloc < nt4) {
+      CK(dalloc(c->d_glj, nt4));
+      c->glj_alloc = nt4;
+    }
+    d_dlj = c->d_glj;
+  }
+  launch_cell_build(c, d_pos, false, st);
+  const size_t smem = sizeof(double) * nt4;
+  if (mode == DERIV_PARAMS)
+    k_deriv_fp64<DERIV_PARAMS><<<blocks, 128, smem, st>>>(
+        g, c->fc, c->stencil, c->ntypes, c->d_lj64, c->d_start, c->d_spos64, c->d_smeta,
+        c->d_sidx, c->d_ex_start, c->d_ex, nullptr, nullptr, d_dq, c->d_tpart);
+  else
+    k_deriv_fp64<DERIV_VJP><<<blocks, 128, smem, st>>>(
+        g, c->fc, c->stencil, c->ntypes, c->d_lj64, c->d_start, c->d_spos64, c->d_smeta,
+        c->d_sidx, c->d_ex_start, c->d_ex, d_w, d_hv, d_dq, c->d_tpart);
+  k_reduce_columns<<<(int)((nt4 + 127) / 128), 128, 0, st>>>(blocks, (int)nt4, c->d_tpart,
+                                                               d_dlj);
+  CK(cudaGetLastError());
+  return PMB200_OK;
+}
+
+static int deriv_ready(pmb200_ctx *c) {
+  int rc = check_ready(c);
+  if (rc) return rc;
+  if (c->form != FORM_CUTOFF)
+    return fail(c, PMB200_EUNSUPPORTED, "derivative kernels cover the cutoff LJ + Coulomb force");
+  return PMB200_OK;
+}
+
+int pmb200_param_grad_device(pmb200_ctx *c, const double *d_pos, double *d_dq, double *d_dlj,
+                             void *stream) {
+  int rc = deriv_ready(c);
+  if (rc) return rc;
+  if (c->n > 0 && (!d_pos || !d_dq)) return fail(c, PMB200_EINVAL, "null device buffer");
+  if (!d_dlj) return fail(c, PMB200_EINVAL, "null device buffer");
+  CK(cudaSetDevice(c->p.device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  return launch_deriv(c, DERIV_PARAMS, d_pos, nullptr, nullptr, d_dq, d_dlj, st);
+}
+
+int pmb200_hvp_device(pmb200_ctx *c, const double *d_pos, const double *d_w, double *d_hv,
+                      double *d_dq, double *d_dlj, void *stream) {
+  int rc = deriv_ready(c);
+  if (rc) return rc;
+  if (c->n > 0 && (!d_pos || !d_w || !d_hv)) return fail(c, PMB200_EINVAL, "null device buffer");
+  CK(cudaSetDevice(c->p.device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  return launch_deriv(c, DERIV_VJP, d_pos, d_w, d_hv, d_dq, d_dlj, st);
+}
+
+int pmb200_update_params(pmb200_ctx *c, const double *q_scaled, const double *lj) {
+  if (!c) return PMB200_EINVAL;
+  if (!c->have_topo) return fail(c, PMB200_ESTATE, "pmb200_set_topology has not been called");
+  CK(cudaSetDevice(c->p.device));
+  if (q_scaled) {
+    for (int i = 0; i < c->n; i++)
+      if (!std::isfinite(q_scaled[i])) return fail(c, PMB200_EINVAL, "atom %d: charge", i);
+    if (c->n > 0)
+      CK(cudaMemcpy(c->d_q, q_scaled, sizeof(double) * c->n, cudaMemcpyHostToDevice));
+  }
+  if (lj) {
+    const int t4 = 4 * c->ntypes * c->ntypes;
+    for (int k = 0; k < t4; k++)
+      if (!std::isfinite(lj[k])) return fail(c, PMB200_EINVAL, "LJ table entry %d", k);
+    c->h_lj.assign(lj, lj + t4);
+    if (c->have_box) return upload_lj(c);
+  }
+  return PMB200_OK;
 }
 
 int pmb200_sync(pmb200_ctx *c) {

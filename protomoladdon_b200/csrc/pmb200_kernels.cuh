@@ -851,6 +851,177 @@ k_pair_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes, const dou
 }
 
 // ---------------------------------------------------------------------------
+// FP64 derivative kernel of the cutoff LJ(C2) + Coulomb(C1) energy for the
+// differentiable form.  Same full-shell cell walk and lane mapping as
+// k_pair_fp64 (every pair is visited from both of its atoms).  Per pair, in
+// the variable s = r^2 (d = x_j - x_i, minimum image):
+//   U(s) = S(s) (A s^-6 - B s^-3) + f q_i q_j phi(s),
+//   phi = s^-1/2 - 1.5/rc + 0.5 s/rc^3 (C1-shifted Coulomb), S the C2 switch
+//   (C2SwitchingFunction.h:42-53 as a function of s), f = coulombScalingFactor
+//   for modified pairs (A14/B14 then too), 1 otherwise.
+// Gradient of U with respect to x_j: 2 U_s d; Hessian block
+// K = 2 U_s I + 4 U_ss d d^T.
+//
+// DERIV_PARAMS: dq[i] = dE/dq_i = sum_j f q_j phi; per LJ table entry (a, b)
+//   dE/dA = sum S s^-6, dE/dB = -sum S s^-3 (entries 2, 3: the modified
+//   pairs' A14, B14), each unordered pair split half to (a, b), half to
+//   (b, a) -- the derivative with respect to the table as the pair loop reads
+//   it.
+// DERIV_VJP: for a direction w (3n), hv = H w (hv_i = sum_j K (w_i - w_j)),
+//   and the derivatives of w . grad E = sum_pairs 2 U_s d.(w_j - w_i) with
+//   respect to q_i (dq) and to the table entries (tpart), as above.
+// Table sums go through shared memory to per-block rows of tpart
+// ([gridDim.x][ntypes^2 * 4]); k_reduce_columns adds the rows in order.
+// ---------------------------------------------------------------------------
+enum DerivMode { DERIV_PARAMS = 0, DERIV_VJP = 1 };
+
+template <int kMode>
+__global__ void __launch_bounds__(128)
+k_deriv_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes,
+             const double4 *__restrict__ lj64, const int *__restrict__ start,
+             const double4 *__restrict__ spos, const int2 *__restrict__ smeta,
+             const int *__restrict__ sidx, const int *__restrict__ ex_start,
+             const int2 *__restrict__ ex, const double *__restrict__ w, double *__restrict__ hv,
+             double *__restrict__ dq, double *__restrict__ tpart) {
+  extern __shared__ double s_tab[];  // ntypes^2 * 4
+  const int nt4 = ntypes * ntypes * 4;
+  for (int k = threadIdx.x; k < nt4; k += blockDim.x) s_tab[k] = 0.0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int cell = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (cell < g.ncell) {
+    const int cx = cell % g.nx;
+    const int cy = (cell / g.nx) % g.ny;
+    const int cz = cell / (g.nx * g.ny);
+    const int cs = start[cell], ce = start[cell + 1];
+    for (int c0 = cs; c0 < ce; c0 += 32) {
+      const int m = min(32, ce - c0);
+      const int L = lanes_per_atom(m);
+      const int ia = lane / L;
+      const int sub = lane % L;
+      const bool active = ia < m;
+      const int i = c0 + (active ? ia : 0);
+      const double4 pi = spos[i];
+      const int2 mi = smeta[i];
+      const int oi = sidx[i];
+      const int elo = ex_start[oi], ehi = ex_start[oi + 1];
+      const int ti = mi.x * ntypes;
+      double wi[3] = {0.0, 0.0, 0.0};
+      if (kMode == DERIV_VJP)
+        for (int k = 0; k < 3; k++) wi[k] = w[3 * (size_t)oi + k];
+      double hx = 0, hy = 0, hz = 0, gq = 0;
+      for (int r = 0; r < g.nrows; r++) {
+        const Row row = st.rows[r];
+        int jy = cy + row.dy, jz = cz + row.dz;
+        while (jy < 0) jy += g.ny;
+        while (jy >= g.ny) jy -= g.ny;
+        while (jz < 0) jz += g.nz;
+        while (jz >= g.nz) jz -= g.nz;
+        const int rowbase = (jz * g.ny + jy) * g.nx;
+        const double sy = row.dy * g.edge[1], sz = row.dz * g.edge[2];
+        for (int dx = row.dxlo; dx <= row.dxhi; dx++) {
+          int jx = cx + dx;
+          jx %= g.nx;
+          jx += (jx < 0) ? g.nx : 0;
+          const int jc = rowbase + jx;
+          const int js = start[jc], je = start[jc + 1];
+          const double sx = dx * g.edge[0];
+          for (int j = js + sub; j < je; j += L) {
+            const double4 pj = spos[j];
+            const double ddx = (pj.x + sx) - pi.x;
+            const double ddy = (pj.y + sy) - pi.y;
+            const double ddz = (pj.z + sz) - pi.z;
+            const double s = ddx * ddx + ddy * ddy + ddz * ddz;
+            if (!(s <= mc.cut2) || !(s > 0.0) || j == i || !active) continue;
+            const int2 mj = smeta[j];
+            int kind = 0;
+            if (mj.y == mi.y) {
+              kind = excl_kind(ex, elo, ehi, sidx[j]);
+              if (kind == 2) continue;
+            }
+            const double4 p = lj64[ti + mj.x];
+            const double A = kind == 1 ? p.z : p.x;
+            const double B = kind == 1 ? p.w : p.y;
+            const double is = 1.0 / s;
+            const double is3 = is * is * is, is6 = is3 * is3;
+            const double E = A * is6 - B * is3;
+            const double Es = (-6.0 * A * is6 + 3.0 * B * is3) * is;
+            const double Ess = (42.0 * A * is6 - 12.0 * B * is3) * is * is;
+            double S = 1.0, Ss = 0.0, Sss = 0.0;
+            if (s > mc.rclj2) {
+              S = 0.0;
+            } else if (s >= mc.ron2) {
+              const double c2 = mc.rclj2 - s;
+              S = mc.s1 * c2 * c2 * (mc.s2 + 2.0 * s);
+              Ss = 2.0 * mc.s1 * c2 * (c2 - mc.s2 - 2.0 * s);
+              Sss = 2.0 * mc.s1 * (mc.s2 + 2.0 * s - 4.0 * c2);
+            }
+            const double qf = pj.w * (kind == 1 ? mc.csf : 1.0);  // f q_j
+            double phi = 0.0, phis = 0.0, phiss = 0.0;
+            if (s <= mc.rcc2) {
+              const double ir = 1.0 / sqrt(s);
+              phi = ir - mc.c15_1 + mc.c05_3 * s;
+              phis = -0.5 * ir * is + mc.c05_3;
+              phiss = 0.75 * ir * is * is;
+            }
+            const int tab = (ti + mj.x) * 4 + (kind == 1 ? 2 : 0);
+            if (kMode == DERIV_PARAMS) {
+              gq += qf * phi;
+              atomicAdd(&s_tab[tab], 0.5 * S * is6);
+              atomicAdd(&s_tab[tab + 1], -0.5 * S * is3);
+            } else {
+              const double wj0 = w[3 * (size_t)sidx[j]], wj1 = w[3 * (size_t)sidx[j] + 1],
+                           wj2 = w[3 * (size_t)sidx[j] + 2];
+              const double dl0 = wi[0] - wj0, dl1 = wi[1] - wj1, dl2 = wi[2] - wj2;
+              const double dd = ddx * dl0 + ddy * dl1 + ddz * dl2;  // d . (w_i - w_j)
+              const double Us = Ss * E + S * Es + pi.w * qf * phis;
+              const double Uss = Sss * E + 2.0 * Ss * Es + S * Ess + pi.w * qf * phiss;
+              const double a = 2.0 * Us, b = 4.0 * Uss * dd;
+              hx += a * dl0 + b * ddx;
+              hy += a * dl1 + b * ddy;
+              hz += a * dl2 + b * ddz;
+              const double T = -2.0 * dd;  // 2 d . (w_j - w_i)
+              gq += qf * phis * T;
+              atomicAdd(&s_tab[tab], 0.5 * T * (Ss * is6 - 6.0 * S * is6 * is));
+              atomicAdd(&s_tab[tab + 1], 0.5 * T * (-Ss * is3 + 3.0 * S * is3 * is));
+            }
+          }
+        }
+      }
+      for (int off = 1; off < L; off <<= 1) {
+        gq += __shfl_xor_sync(0xffffffffu, gq, off);
+        if (kMode == DERIV_VJP) {
+          hx += __shfl_xor_sync(0xffffffffu, hx, off);
+          hy += __shfl_xor_sync(0xffffffffu, hy, off);
+          hz += __shfl_xor_sync(0xffffffffu, hz, off);
+        }
+      }
+      if (active && sub == 0) {
+        dq[oi] = gq;
+        if (kMode == DERIV_VJP) {
+          hv[3 * (size_t)oi] = hx;
+          hv[3 * (size_t)oi + 1] = hy;
+          hv[3 * (size_t)oi + 2] = hz;
+        }
+      }
+    }
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < nt4; k += blockDim.x)
+    tpart[(size_t)blockIdx.x * nt4 + k] = s_tab[k];
+}
+
+// out[k] = sum over rows r of part[r][k], rows added in order (deterministic).
+__global__ void k_reduce_columns(int rows, int cols, const double *__restrict__ part,
+                                 double *__restrict__ out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= cols) return;
+  double acc = 0.0;
+  for (int r = 0; r < rows; r++) acc += part[(size_t)r * cols + k];
+  out[k] = acc;
+}
+
+// ---------------------------------------------------------------------------
 // Molecular virial support: molecule centres of mass from the raw positions
 // (mass-weighted, Kahan-compensated like molecularCenterOfMass,
 // protomol/src/protomol/topology/TopologyUtilities.cpp:645-672).

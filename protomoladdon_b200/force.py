@@ -252,6 +252,33 @@ class NonbondedCutoffB200SystemForce:
             self._ctx, _P(pos_ptr), _P(vel_ptr), _P(force_ptr), _P(out_ptr) if out_ptr else None,
             float(dt_fs), int(flags), _P(stream)))
 
+    def param_grad_device(self, topo, pos_ptr, dq_ptr, dlj_ptr, stream=None):
+        """dE/dq_scaled per atom and dE/d{A, B, A14, B14} per table entry
+        (FP64 kernel; see pmb200_param_grad_device)."""
+        self._ensure(topo)
+        self._check(_lib.lib().pmb200_param_grad_device(
+            self._ctx, _P(pos_ptr), _P(dq_ptr), _P(dlj_ptr), _P(stream) if stream else None))
+
+    def hvp_device(self, topo, pos_ptr, w_ptr, hv_ptr, dq_ptr=None, dlj_ptr=None, stream=None):
+        """hv = H w and the derivatives of w . grad E with respect to the
+        charges and the table (FP64 kernel; see pmb200_hvp_device)."""
+        self._ensure(topo)
+        self._check(_lib.lib().pmb200_hvp_device(
+            self._ctx, _P(pos_ptr), _P(w_ptr), _P(hv_ptr), _P(dq_ptr) if dq_ptr else None,
+            _P(dlj_ptr) if dlj_ptr else None, _P(stream) if stream else None))
+
+    def update_params(self, topo, q_scaled=None, lj=None):
+        """New charges and/or LJ table (host arrays) for the same topology;
+        the topology object's arrays are updated too."""
+        self._ensure(topo)
+        q = None if q_scaled is None else np.ascontiguousarray(q_scaled, dtype=np.float64)
+        t = None if lj is None else np.ascontiguousarray(lj, dtype=np.float64).reshape(-1)
+        self._check(_lib.lib().pmb200_update_params(self._ctx, _ptr(q), _ptr(t)))
+        if q is not None:
+            topo.qscaled = q.copy()
+        if t is not None:
+            topo.lj = t.copy()
+
     def set_rigid_waters(self, topo, widx, d_oh, d_hh):
         """SETTLE constraints for the device integrator (see pmb200.h)."""
         self._ensure(topo)
