@@ -115,6 +115,8 @@ def ref_lib(exact_erfc: bool = False):
         lib.pmref_ewald_eval.argtypes = [_P, _D, _D, _P, _P, _P, _P, _P, _I]
         lib.pmref_ewald_eval.restype = _I
         lib.pmref_ewald_exact_erfc.restype = _I
+        lib.pmref_hessian.argtypes = [_P, _P, _P, _D, _D, _D, _D]
+        lib.pmref_hessian.restype = _I
         if exact_erfc:
             _ref_exact = lib
         else:
@@ -268,6 +270,7 @@ class RefForce:
 
     def __init__(self, sysd, exact_erfc=False):
         self.lib = ref_lib(exact_erfc)
+        self._sys = {k: sysd[k] for k in ("ron", "rc_lj", "rc_coul", "rc_alg")}
         self.ar = _Arrays(sysd)
         ar = self.ar
         box = np.ascontiguousarray(sysd["box"], dtype=np.float64)
@@ -300,6 +303,17 @@ class RefForce:
         self.lib.pmref_ewald_eval(self.h, float(alpha), float(accuracy), _ptr(p), _ptr(f),
                                   _ptr(e), _ptr(v), _ptr(mv), int(virial_mode))
         return f.reshape(-1, 3), float(e[0]), v, mv
+
+    def hessian(self, pos):
+        """The reference's analytic Hessian of the LJ(C2) + Coulomb(C1) energy
+        (Hessian::evaluate, not mass-weighted) as a dense (3n, 3n) array."""
+        p = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1)
+        n3 = p.size
+        h = np.zeros(n3 * n3)
+        s = self._sys
+        self.lib.pmref_hessian(self.h, _ptr(p), _ptr(h), float(s["ron"]), float(s["rc_lj"]),
+                               float(s["rc_coul"]), float(s["rc_alg"]))
+        return h.reshape(n3, n3).T  # column-major -> [row, col]
 
     def leapfrog(self, pos, vel, dt_fs, nsteps):
         p = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1).copy()

@@ -139,3 +139,20 @@ def test_host_kick_drift_matches_numpy_settle():
     rigid.kick_drift_settle(p1, v1, F, s["mass"], 1.0, w, water.D_OH, water.D_HH)
     rigid.host_kick_drift(p2, v2, F, s["mass"], 1.0, w, water.D_OH, water.D_HH)
     assert np.abs(p1 - p2).max() < 1e-12 and np.abs(v1 - v2).max() < 1e-9
+
+
+def test_lj_table_mixing_matches_the_generator():
+    """autograd.lj_table (torch, differentiable) reproduces the water
+    generator's table, ions included."""
+    import torch
+    from protomoladdon_b200.autograd import lj_table
+    for ions in (False, True):
+        ref = water._lj_table(ions)
+        sig = [water.SIG_O, 0.0] + ([water.SIG_NA, water.SIG_CL] if ions else [])
+        eps = [water.EPS_O, 0.0] + ([water.EPS_NA, water.EPS_CL] if ions else [])
+        t = lj_table(torch.tensor(sig, dtype=torch.float64), torch.tensor(eps, dtype=torch.float64))
+        np.testing.assert_allclose(t.numpy(), ref, rtol=1e-13, atol=0)
+    s = torch.tensor([3.0, 0.0], dtype=torch.float64, requires_grad=True)
+    e = torch.tensor([0.2, 0.0], dtype=torch.float64, requires_grad=True)
+    lj_table(s, e).sum().backward()
+    assert torch.isfinite(s.grad).all() and torch.isfinite(e.grad).all()
