@@ -257,6 +257,45 @@ int pmb200_hvp_device(pmb200_ctx *ctx, const double *d_pos, const double *d_w, d
  * Replaces rebuilding the topology to change force-field parameters. */
 int pmb200_update_params(pmb200_ctx *ctx, const double *q_scaled, const double *lj);
 
+/* ---- batches of independent systems ----
+ * Many periodic systems of uneven size evaluated together: one counting sort
+ * over all their atoms, one persistent pair kernel that takes (system,
+ * cell, part of the cell's stencil) tasks from a global counter, one
+ * fixed-point finalize, one per-system reduction; with a stream the
+ * sequence is captured once as a CUDA graph and replayed.  The reference
+ * evaluates one system per force object; a batch replaces a loop of
+ * SystemForce::evaluate over such objects
+ * (protomol/src/protomol/force/system/SystemForce.h:32-35).
+ *
+ * pmb200_batch_create builds a batch from nsys contexts of precision
+ * PMB200_MIXED and the same kind (cutoff or Ewald real-space), each holding
+ * its topology and box; it copies what it needs (the contexts stay usable
+ * and independent).  Positions and forces are the systems' arrays back to
+ * back in system order, [3 * sum n_s]; forces are accumulated into;
+ * d_out[nsys][20] receives each system's {COULOMB, LENNARDJONES, virial 9,
+ * molecular virial 9 (zero: not offered)}.  The schedule (stencil parts per
+ * cell 1..8, task order 0 = by system / 1 = largest estimated cost first,
+ * persistent blocks per SM, 0 = as many as fit) is set directly or chosen
+ * by pmb200_batch_autotune, which times every candidate on the given
+ * positions (reps timed launches each) and keeps the fastest; sched[4] =
+ * {parts, order, blocks per SM, tasks}. */
+typedef struct pmb200_batch pmb200_batch;
+int pmb200_batch_create(pmb200_ctx *const *systems, int nsys, pmb200_batch **out);
+int pmb200_batch_destroy(pmb200_batch *batch);
+const char *pmb200_batch_last_error(const pmb200_batch *batch);
+int pmb200_batch_eval_device(pmb200_batch *batch, const double *d_pos, double *d_forces,
+                             double *d_out, unsigned flags, void *stream);
+int pmb200_batch_set_schedule(pmb200_batch *batch, int parts, int order, int blocks_per_sm);
+int pmb200_batch_get_schedule(const pmb200_batch *batch, int sched[4]);
+int pmb200_batch_autotune(pmb200_batch *batch, const double *d_pos, void *stream, int reps,
+                          int sched[4], float *best_ms);
+/* CUDA-event time of the last directly launched pair kernel (timing on:
+ * launches are direct, not graph replays). */
+int pmb200_batch_set_kernel_timing(pmb200_batch *batch, int on);
+int pmb200_batch_last_kernel_ms(pmb200_batch *batch, float *ms);
+/* In-cutoff pair count per system of the last evaluation with energies. */
+int pmb200_batch_pair_counts(pmb200_batch *batch, long long *counts);
+
 /* ---- Ewald real-space term ----
  * A context of the second kind replaces the real-space part of ProtoMol's
  * Ewald sum,

@@ -39,6 +39,10 @@ EXPORTED = (
     "pmb200_measure_fp32_peak", "pmb200_set_rigid_waters", "pmb200_host_kick_drift",
     "pmb200_eval_noalloc", "pmb200_create_ewald_real", "pmb200_ewald_info",
     "pmb200_param_grad_device", "pmb200_hvp_device", "pmb200_update_params",
+    "pmb200_batch_create", "pmb200_batch_destroy", "pmb200_batch_last_error",
+    "pmb200_batch_eval_device", "pmb200_batch_set_schedule", "pmb200_batch_get_schedule",
+    "pmb200_batch_autotune", "pmb200_batch_set_kernel_timing", "pmb200_batch_last_kernel_ms",
+    "pmb200_batch_pair_counts",
 )
 
 _P = ctypes.c_void_p
@@ -100,8 +104,21 @@ def lib():
     L.pmb200_param_grad_device.argtypes = [_P, _P, _P, _P, _P]
     L.pmb200_hvp_device.argtypes = [_P, _P, _P, _P, _P, _P, _P]
     L.pmb200_update_params.argtypes = [_P, _P, _P]
+    L.pmb200_batch_create.argtypes = [ctypes.POINTER(_P), _I, ctypes.POINTER(_P)]
+    L.pmb200_batch_destroy.argtypes = [_P]
+    L.pmb200_batch_last_error.argtypes = [_P]
+    L.pmb200_batch_last_error.restype = ctypes.c_char_p
+    L.pmb200_batch_eval_device.argtypes = [_P, _P, _P, _P, ctypes.c_uint, _P]
+    L.pmb200_batch_set_schedule.argtypes = [_P, _I, _I, _I]
+    L.pmb200_batch_get_schedule.argtypes = [_P, ctypes.POINTER(_I)]
+    L.pmb200_batch_autotune.argtypes = [_P, _P, _P, _I, ctypes.POINTER(_I),
+                                        ctypes.POINTER(ctypes.c_float)]
+    L.pmb200_batch_set_kernel_timing.argtypes = [_P, _I]
+    L.pmb200_batch_last_kernel_ms.argtypes = [_P, ctypes.POINTER(ctypes.c_float)]
+    L.pmb200_batch_pair_counts.argtypes = [_P, ctypes.POINTER(ctypes.c_longlong)]
     for name in EXPORTED:
         getattr(L, name).restype = getattr(L, name).restype or _I
     L.pmb200_last_error.restype = ctypes.c_char_p
+    L.pmb200_batch_last_error.restype = ctypes.c_char_p
     _lib = L
     return L

@@ -1355,3 +1355,439 @@ int pmb200_grid(const pmb200_ctx *c, int dims[3], double edge[3]) {
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Batches of independent systems (pmb200_batch_*): see pmb200_batch.cuh for
+// the device layout.
+// ===========================================================================
+#include "pmb200_batch.cuh"
+
+struct pmb200_batch {
+  std::string err;
+  int device = 0;
+  int form = FORM_CUTOFF;
+  int nsys = 0, N = 0, C = 0, ntasks = 0;
+  std::vector<BatchSys> h_sys;
+  std::vector<double> cost;  // per system: estimated work of one cell task
+  BatchSys *d_sys = nullptr;
+  int *d_atom_sys = nullptr, *d_type = nullptr, *d_mol = nullptr;
+  double *d_q = nullptr;
+  int *d_ex_start = nullptr;
+  int2 *d_ex = nullptr;
+  unsigned short *d_st = nullptr;
+  float4 *d_lj32 = nullptr;
+  int *d_cell_of = nullptr, *d_count = nullptr, *d_start = nullptr, *d_slot = nullptr;
+  int *d_tmp = nullptr, *d_sidx = nullptr, *d_err = nullptr, *d_counter = nullptr;
+  float4 *d_rel32 = nullptr, *d_spos32 = nullptr;
+  int2 *d_smeta = nullptr;
+  unsigned long long *d_facc = nullptr;
+  double *d_partial = nullptr, *d_pairs = nullptr, *d_scratch_f = nullptr;
+  int4 *d_tasks = nullptr;
+  int *d_rows_start = nullptr, *d_rows = nullptr;
+  // schedule: stencil parts per cell, task order (0 as built, 1 by cost,
+  // largest first), persistent blocks per SM
+  int parts = 1, order = 1, bpsm = 0, max_bpsm = 1, nsm = 1;
+  // graph of one evaluation (pmb200_batch_eval_device with a stream)
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  const void *gkey[4] = {nullptr, nullptr, nullptr, nullptr};
+  unsigned gflags = 0;
+  int timing = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace {
+
+int bfail(pmb200_batch *b, int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (b) b->err = buf;
+  return code;
+}
+
+#define BCK(call)                                                                 \
+  do {                                                                            \
+    cudaError_t e_ = (call);                                                      \
+    if (e_ != cudaSuccess)                                                        \
+      return bfail(b, PMB200_ECUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+void batch_release_graph(pmb200_batch *b) {
+  if (b->graph_exec) cudaGraphExecDestroy(b->graph_exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->graph_exec = nullptr;
+  b->graph = nullptr;
+  for (auto &k : b->gkey) k = nullptr;
+}
+
+// The task list for the current schedule: every (system, cell, part), in
+// system order or by estimated cost (largest first, stable), and each
+// system's rows in list order.
+int batch_build_tasks(pmb200_batch *b) {
+  std::vector<int4> tasks;
+  tasks.reserve((size_t)b->C * b->parts);
+  for (int s = 0; s < b->nsys; s++)
+    for (int c = 0; c < b->h_sys[s].g.ncell; c++)
+      for (int p = 0; p < b->parts; p++) tasks.push_back(make_int4(s, c, p, b->parts));
+  if (b->order == 1)
+    std::stable_sort(tasks.begin(), tasks.end(), [&](const int4 &x, const int4 &y) {
+      return b->cost[x.x] > b->cost[y.x];
+    });
+  const int T = (int)tasks.size();
+  std::vector<int> rs(b->nsys + 1, 0), rows(std::max(T, 1));
+  for (const int4 &t : tasks) rs[t.x + 1]++;
+  for (int s = 0; s < b->nsys; s++) rs[s + 1] += rs[s];
+  {
+    std::vector<int> fill(rs.begin(), rs.end() - 1);
+    for (int t = 0; t < T; t++) rows[fill[tasks[t].x]++] = t;
+  }
+  if (b->ntasks < T || !b->d_tasks) {
+    BCK(dalloc(b->d_tasks, (size_t)std::max(T, 1)));
+    BCK(dalloc(b->d_rows, (size_t)std::max(T, 1)));
+    BCK(dalloc(b->d_partial, (size_t)std::max(T, 1) * kNacc));
+  }
+  b->ntasks = T;
+  if (T > 0) {
+    BCK(cudaMemcpy(b->d_tasks, tasks.data(), sizeof(int4) * T, cudaMemcpyHostToDevice));
+    BCK(cudaMemcpy(b->d_rows, rows.data(), sizeof(int) * T, cudaMemcpyHostToDevice));
+  }
+  BCK(cudaMemcpy(b->d_rows_start, rs.data(), sizeof(int) * (b->nsys + 1),
+                 cudaMemcpyHostToDevice));
+  batch_release_graph(b);
+  return PMB200_OK;
+}
+
+template <int F>
+void batch_launch_pair(pmb200_batch *b, bool energy, bool virial, int grid, cudaStream_t st) {
+#define PMB_BATCH_LAUNCH(E, V)                                                           \
+  k_pair_mixed_batch<F, E, V><<<grid, 32 * kWarps, 0, st>>>(                               \
+      b->d_sys, b->d_tasks, b->ntasks, b->d_counter, b->d_st, b->d_lj32, b->d_start,       \
+      b->d_spos32, b->d_smeta, b->d_sidx, b->d_ex_start, b->d_ex, b->d_facc, b->N,         \
+      b->d_partial)
+  if (energy && virial) PMB_BATCH_LAUNCH(true, true);
+  else if (energy) PMB_BATCH_LAUNCH(true, false);
+  else if (virial) PMB_BATCH_LAUNCH(false, true);
+  else PMB_BATCH_LAUNCH(false, false);
+#undef PMB_BATCH_LAUNCH
+}
+
+// One evaluation of every system on `st` (forces accumulated into d_forces,
+// or overwritten when accumulate is 0).
+int batch_launch_eval(pmb200_batch *b, const double *d_pos, double *d_forces, double *d_out,
+                      unsigned flags, int accumulate, cudaStream_t st, bool timed) {
+  const int N = b->N;
+  const bool energy = (flags & PMB200_ENERGY) != 0;
+  const bool virial = (flags & PMB200_VIRIAL) != 0;
+  BCK(cudaMemsetAsync(b->d_count, 0, sizeof(int) * b->C, st));
+  if (N > 0)
+    k_cell_index_batch<<<(N + 255) / 256, 256, 0, st>>>(N, d_pos, b->d_sys, b->d_atom_sys,
+                                                        b->d_cell_of, b->d_count, b->d_slot,
+                                                        b->d_rel32, b->d_q, b->d_err);
+  k_scan<<<1, 1024, 1024 * sizeof(int), st>>>(b->C, b->d_count, b->d_start);
+  if (N > 0)
+    k_scatter<<<(N + 255) / 256, 256, 0, st>>>(N, b->d_cell_of, b->d_slot, b->d_start,
+                                                 b->d_tmp);
+  k_rank_gather<<<(b->C + 3) / 4, 128, 0, st>>>(b->C, b->d_start, b->d_tmp, b->d_rel32,
+                                                  nullptr, b->d_type, b->d_mol, b->d_sidx,
+                                                  b->d_spos32, nullptr, b->d_smeta);
+  if (N > 0)
+    BCK(cudaMemsetAsync(b->d_facc, 0, sizeof(unsigned long long) * 3 * (size_t)N, st));
+  BCK(cudaMemsetAsync(b->d_counter, 0, sizeof(int), st));
+  const int bpsm = b->bpsm > 0 ? std::min(b->bpsm, b->max_bpsm) : b->max_bpsm;
+  const int grid = std::max(1, std::min(b->ntasks, bpsm * b->nsm));
+  if (timed) BCK(cudaEventRecord(b->ev0, st));
+  if (b->form == FORM_EWALD_POLY5) batch_launch_pair<FORM_EWALD_POLY5>(b, energy, virial, grid, st);
+  else if (b->form == FORM_EWALD_EXACT) batch_launch_pair<FORM_EWALD_EXACT>(b, energy, virial, grid, st);
+  else batch_launch_pair<FORM_CUTOFF>(b, energy, virial, grid, st);
+  if (timed) BCK(cudaEventRecord(b->ev1, st));
+  if (N > 0)
+    k_finalize_batch<<<(N + 255) / 256, 256, 0, st>>>(N, b->d_facc, b->d_sidx, b->d_atom_sys,
+                                                      b->d_sys, accumulate, d_forces);
+  if ((energy || virial) && d_out)
+    k_reduce_batch<<<(b->nsys + 3) / 4, 128, 0, st>>>(b->nsys, b->d_rows_start, b->d_rows,
+                                                       b->d_partial, b->d_sys, d_out, b->d_pairs);
+  BCK(cudaGetLastError());
+  return PMB200_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pmb200_batch_destroy(pmb200_batch *b) {
+  if (!b) return PMB200_OK;
+  cudaSetDevice(b->device);
+  batch_release_graph(b);
+  dfree(b->d_sys); dfree(b->d_atom_sys); dfree(b->d_type); dfree(b->d_mol); dfree(b->d_q);
+  dfree(b->d_ex_start); dfree(b->d_ex); dfree(b->d_st); dfree(b->d_lj32);
+  dfree(b->d_cell_of); dfree(b->d_count); dfree(b->d_start); dfree(b->d_slot);
+  dfree(b->d_tmp); dfree(b->d_sidx); dfree(b->d_err); dfree(b->d_counter);
+  dfree(b->d_rel32); dfree(b->d_spos32); dfree(b->d_smeta); dfree(b->d_facc);
+  dfree(b->d_partial); dfree(b->d_pairs); dfree(b->d_scratch_f); dfree(b->d_tasks);
+  dfree(b->d_rows_start); dfree(b->d_rows);
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  delete b;
+  return PMB200_OK;
+}
+
+const char *pmb200_batch_last_error(const pmb200_batch *b) { return b ? b->err.c_str() : ""; }
+
+int pmb200_batch_create(pmb200_ctx *const *systems, int nsys, pmb200_batch **out) {
+  if (!out || nsys <= 0 || !systems) return PMB200_EINVAL;
+  *out = nullptr;
+  for (int s = 0; s < nsys; s++) {
+    const pmb200_ctx *c = systems[s];
+    if (!c) return PMB200_EINVAL;
+    if (!c->have_topo || !c->have_box) return PMB200_ESTATE;
+    if (c->p.precision != PMB200_MIXED) return PMB200_EUNSUPPORTED;
+    if (c->form != systems[0]->form || c->p.device != systems[0]->p.device)
+      return PMB200_EINVAL;
+  }
+  pmb200_batch *b = new pmb200_batch();
+  b->nsys = nsys;
+  b->device = systems[0]->p.device;
+  b->form = systems[0]->form;
+  int rc = PMB200_OK;
+  auto done = [&](int code) {
+    if (code) pmb200_batch_destroy(b);
+    else *out = b;
+    return code;
+  };
+  if (cudaSetDevice(b->device) != cudaSuccess) return done(PMB200_ECUDA);
+  // offsets and per-system parameters
+  std::vector<unsigned short> st;
+  std::vector<float4> lj;
+  std::vector<int> atom_sys;
+  long long N = 0, C = 0;
+  for (int s = 0; s < nsys; s++) {
+    const pmb200_ctx *c = systems[s];
+    BatchSys y{};
+    y.g = c->g;
+    y.mc = c->mc;
+    y.pb = c->pb;
+    y.fscale = kFixInv / c->g.unit;
+    const double rcc = c->p.cutoff_coul / c->g.unit;
+    y.c15_1 = c->form == FORM_CUTOFF ? 1.5 / rcc : 0.0;
+    y.c05_3 = c->form == FORM_CUTOFF ? 0.5 / (rcc * rcc * rcc) : 0.0;
+    y.qscale32 = (float)(1.0 / std::sqrt(c->g.unit));
+    y.cell0 = (int)C;
+    y.atom0 = (int)N;
+    y.natoms = c->n;
+    y.st0 = (int)st.size();
+    y.st_n = c->half.ncells;
+    st.insert(st.end(), c->half.off, c->half.off + c->half.ncells);
+    y.lj0 = (int)lj.size();
+    y.ntypes = c->ntypes;
+    const double u = c->g.unit, u6 = std::pow(u, 6.0), u12 = u6 * u6;
+    for (int k = 0; k < c->ntypes * c->ntypes; k++) {
+      const double *p = &c->h_lj[4 * k];
+      lj.push_back(make_float4((float)(p[0] / u12), (float)(p[1] / u6), (float)(p[2] / u12),
+                               (float)(p[3] / u6)));
+    }
+    b->h_sys.push_back(y);
+    const double per_cell = c->g.ncell > 0 ? (double)c->n / c->g.ncell : 0.0;
+    b->cost.push_back(per_cell * per_cell * c->half.ncells);
+    atom_sys.insert(atom_sys.end(), c->n, s);
+    N += c->n;
+    C += c->g.ncell;
+  }
+  if (N > (1LL << 30) || C > (1LL << 28)) return done(bfail(b, PMB200_EUNSUPPORTED, "batch too large"));
+  b->N = (int)N;
+  b->C = (int)C;
+  const size_t n1 = (size_t)std::max<long long>(N, 1);
+  // per-atom data gathered from the contexts (exclusions re-indexed)
+  std::vector<int> ex_start(N + 1, 0);
+  std::vector<int2> ex;
+  auto cuda = [&](cudaError_t e) { if (e != cudaSuccess && !rc) rc = bfail(b, PMB200_ECUDA, "%s", cudaGetErrorString(e)); };
+  cuda(dalloc(b->d_type, n1));
+  cuda(dalloc(b->d_mol, n1));
+  cuda(dalloc(b->d_q, n1));
+  if (rc) return done(rc);
+  for (int s = 0; s < nsys; s++) {
+    const pmb200_ctx *c = systems[s];
+    const int a0 = b->h_sys[s].atom0, n = c->n;
+    if (n == 0) continue;
+    cuda(cudaMemcpy(b->d_type + a0, c->d_type, sizeof(int) * n, cudaMemcpyDeviceToDevice));
+    cuda(cudaMemcpy(b->d_mol + a0, c->d_mol, sizeof(int) * n, cudaMemcpyDeviceToDevice));
+    cuda(cudaMemcpy(b->d_q + a0, c->d_q, sizeof(double) * n, cudaMemcpyDeviceToDevice));
+    std::vector<int> es(n + 1);
+    cuda(cudaMemcpy(es.data(), c->d_ex_start, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost));
+    std::vector<int2> e(std::max(es[n], 1));
+    if (es[n] > 0)
+      cuda(cudaMemcpy(e.data(), c->d_ex, sizeof(int2) * es[n], cudaMemcpyDeviceToHost));
+    const int base = (int)ex.size();
+    for (int i = 0; i < n; i++) ex_start[a0 + i] = base + es[i];
+    for (int k = 0; k < es[n]; k++) ex.push_back(make_int2(e[k].x + a0, e[k].y));
+  }
+  ex_start[N] = (int)ex.size();
+  if (rc) return done(rc);
+  cuda(dalloc(b->d_sys, (size_t)nsys));
+  cuda(dalloc(b->d_atom_sys, n1));
+  cuda(dalloc(b->d_ex_start, n1 + 1));
+  cuda(dalloc(b->d_ex, std::max<size_t>(ex.size(), 1)));
+  cuda(dalloc(b->d_st, std::max<size_t>(st.size(), 1)));
+  cuda(dalloc(b->d_lj32, std::max<size_t>(lj.size(), 1)));
+  cuda(dalloc(b->d_cell_of, n1));
+  cuda(dalloc(b->d_slot, n1));
+  cuda(dalloc(b->d_tmp, n1));
+  cuda(dalloc(b->d_sidx, n1));
+  cuda(dalloc(b->d_rel32, n1));
+  cuda(dalloc(b->d_spos32, n1));
+  cuda(dalloc(b->d_smeta, n1));
+  cuda(dalloc(b->d_facc, 3 * n1));
+  cuda(dalloc(b->d_scratch_f, 3 * n1));
+  cuda(dalloc(b->d_count, (size_t)std::max<long long>(C, 1)));
+  cuda(dalloc(b->d_start, (size_t)C + 1));
+  cuda(dalloc(b->d_err, 1));
+  cuda(dalloc(b->d_counter, 1));
+  cuda(dalloc(b->d_pairs, (size_t)nsys));
+  cuda(dalloc(b->d_rows_start, (size_t)nsys + 1));
+  cuda(cudaEventCreate(&b->ev0));
+  cuda(cudaEventCreate(&b->ev1));
+  if (rc) return done(rc);
+  cuda(cudaMemcpy(b->d_sys, b->h_sys.data(), sizeof(BatchSys) * nsys, cudaMemcpyHostToDevice));
+  if (N > 0)
+    cuda(cudaMemcpy(b->d_atom_sys, atom_sys.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
+  cuda(cudaMemcpy(b->d_ex_start, ex_start.data(), sizeof(int) * (N + 1), cudaMemcpyHostToDevice));
+  if (!ex.empty())
+    cuda(cudaMemcpy(b->d_ex, ex.data(), sizeof(int2) * ex.size(), cudaMemcpyHostToDevice));
+  if (!st.empty())
+    cuda(cudaMemcpy(b->d_st, st.data(), sizeof(unsigned short) * st.size(), cudaMemcpyHostToDevice));
+  if (!lj.empty())
+    cuda(cudaMemcpy(b->d_lj32, lj.data(), sizeof(float4) * lj.size(), cudaMemcpyHostToDevice));
+  cuda(cudaMemset(b->d_err, 0, sizeof(int)));
+  if (rc) return done(rc);
+  // persistent grid: resident blocks per SM of the pair kernel
+  int dev_sm = 1, occ = 1;
+  cuda(cudaDeviceGetAttribute(&dev_sm, cudaDevAttrMultiProcessorCount, b->device));
+  cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &occ, k_pair_mixed_batch<FORM_CUTOFF, true, true>, 32 * kWarps, 0));
+  if (rc) return done(rc);
+  b->nsm = dev_sm;
+  b->max_bpsm = std::max(1, occ);
+  return done(batch_build_tasks(b));
+}
+
+int pmb200_batch_set_schedule(pmb200_batch *b, int parts, int order, int blocks_per_sm) {
+  if (!b) return PMB200_EINVAL;
+  if (parts < 1 || parts > 8 || order < 0 || order > 1 || blocks_per_sm < 0)
+    return bfail(b, PMB200_EINVAL, "schedule parts %d order %d blocks/SM %d", parts, order,
+                 blocks_per_sm);
+  BCK(cudaSetDevice(b->device));
+  b->parts = parts;
+  b->order = order;
+  b->bpsm = blocks_per_sm;
+  return batch_build_tasks(b);
+}
+
+int pmb200_batch_get_schedule(const pmb200_batch *b, int sched[4]) {
+  if (!b || !sched) return PMB200_EINVAL;
+  sched[0] = b->parts;
+  sched[1] = b->order;
+  sched[2] = b->bpsm > 0 ? std::min(b->bpsm, b->max_bpsm) : b->max_bpsm;
+  sched[3] = b->ntasks;
+  return PMB200_OK;
+}
+
+int pmb200_batch_eval_device(pmb200_batch *b, const double *d_pos, double *d_forces,
+                             double *d_out, unsigned flags, void *stream) {
+  if (!b) return PMB200_EINVAL;
+  if (flags & PMB200_MOLVIRIAL)
+    return bfail(b, PMB200_EUNSUPPORTED, "molecular virial is not offered for batches");
+  if (b->N > 0 && (!d_pos || !d_forces)) return bfail(b, PMB200_EINVAL, "null device buffer");
+  if ((flags & (PMB200_ENERGY | PMB200_VIRIAL)) && !d_out)
+    return bfail(b, PMB200_EINVAL, "null output buffer");
+  BCK(cudaSetDevice(b->device));
+  cudaStream_t st = (cudaStream_t)stream;
+  if (!stream || b->timing) return batch_launch_eval(b, d_pos, d_forces, d_out, flags, 1, st, b->timing != 0);
+  const void *key[4] = {d_pos, d_forces, d_out, stream};
+  bool same = b->graph_exec && b->gflags == flags;
+  for (int k = 0; k < 4 && same; k++) same = b->gkey[k] == key[k];
+  if (!same) {
+    batch_release_graph(b);
+    BCK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    int rc = batch_launch_eval(b, d_pos, d_forces, d_out, flags, 1, st, false);
+    cudaGraph_t gr = nullptr;
+    cudaError_t e = cudaStreamEndCapture(st, &gr);
+    if (rc) {
+      if (gr) cudaGraphDestroy(gr);
+      return rc;
+    }
+    if (e != cudaSuccess) return bfail(b, PMB200_ECUDA, "capture: %s", cudaGetErrorString(e));
+    b->graph = gr;
+    BCK(cudaGraphInstantiate(&b->graph_exec, gr, 0));
+    for (int k = 0; k < 4; k++) b->gkey[k] = key[k];
+    b->gflags = flags;
+  }
+  BCK(cudaGraphLaunch(b->graph_exec, st));
+  return PMB200_OK;
+}
+
+int pmb200_batch_set_kernel_timing(pmb200_batch *b, int on) {
+  if (!b) return PMB200_EINVAL;
+  b->timing = on ? 1 : 0;
+  return PMB200_OK;
+}
+
+int pmb200_batch_last_kernel_ms(pmb200_batch *b, float *ms) {
+  if (!b || !ms) return PMB200_EINVAL;
+  BCK(cudaSetDevice(b->device));
+  BCK(cudaEventSynchronize(b->ev1));
+  BCK(cudaEventElapsedTime(ms, b->ev0, b->ev1));
+  return PMB200_OK;
+}
+
+int pmb200_batch_pair_counts(pmb200_batch *b, long long *counts) {
+  if (!b || !counts) return PMB200_EINVAL;
+  BCK(cudaSetDevice(b->device));
+  std::vector<double> v(b->nsys);
+  BCK(cudaDeviceSynchronize());
+  BCK(cudaMemcpy(v.data(), b->d_pairs, sizeof(double) * b->nsys, cudaMemcpyDeviceToHost));
+  for (int s = 0; s < b->nsys; s++) counts[s] = (long long)llround(v[s]);
+  return PMB200_OK;
+}
+
+int pmb200_batch_autotune(pmb200_batch *b, const double *d_pos, void *stream, int reps,
+                          int sched[4], float *best_ms) {
+  if (!b || !sched || !best_ms) return PMB200_EINVAL;
+  if (b->N > 0 && !d_pos) return bfail(b, PMB200_EINVAL, "null device buffer");
+  if (reps < 1) reps = 5;
+  BCK(cudaSetDevice(b->device));
+  cudaStream_t st = (cudaStream_t)stream;
+  const int parts_c[3] = {1, 2, 4};
+  const int bpsm_c[2] = {b->max_bpsm, std::max(1, b->max_bpsm / 2)};
+  float best = -1.0f;
+  int bp = 1, bo = 1, bb = 0;
+  for (int pi = 0; pi < 3; pi++)
+    for (int order = 0; order < 2; order++)
+      for (int bi = 0; bi < (bpsm_c[1] != bpsm_c[0] ? 2 : 1); bi++) {
+        int rc = pmb200_batch_set_schedule(b, parts_c[pi], order, bpsm_c[bi]);
+        if (rc) return rc;
+        float tot = 0.0f;
+        for (int r = 0; r < reps + 2; r++) {
+          rc = batch_launch_eval(b, d_pos, b->d_scratch_f, nullptr, 0, 0, st, true);
+          if (rc) return rc;
+          float ms = 0.0f;
+          BCK(cudaEventSynchronize(b->ev1));
+          BCK(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+          if (r >= 2) tot += ms;
+        }
+        const float mean = tot / reps;
+        if (best < 0.0f || mean < best) {
+          best = mean;
+          bp = parts_c[pi];
+          bo = order;
+          bb = bpsm_c[bi];
+        }
+      }
+  int rc = pmb200_batch_set_schedule(b, bp, bo, bb);
+  if (rc) return rc;
+  *best_ms = best;
+  return pmb200_batch_get_schedule(b, sched);
+}
+
+}  // extern "C"

@@ -124,6 +124,26 @@ struct HalfStencil {
 // Wrap each position into the box in FP64, find its cell (x fastest), count
 // cell occupancy, and keep the coordinates relative to the cell's lower
 // corner.  Non-finite coordinates raise err bit 1 and are binned at cell 0.
+// The cell of one position: wrapped into the box in FP64, the cell
+// coordinates c and the offset r from the cell's lower corner (Angstrom).
+// Returns false for a non-finite coordinate (binned at the box corner).
+__device__ __forceinline__ bool locate_cell(const double *xin, const GridParams &g, int c[3],
+                                            double r[3]) {
+  const int nd[3] = {g.nx, g.ny, g.nz};
+  bool ok = true;
+  for (int a = 0; a < 3; a++) {
+    double x = xin[a];
+    if (!isfinite(x)) { ok = false; x = g.boxmin[a]; }
+    double w = x - g.boxmin[a];
+    w -= g.boxlen[a] * floor(w / g.boxlen[a]);
+    int ca = (int)floor(w / g.edge[a]);
+    ca = ca < 0 ? 0 : (ca >= nd[a] ? nd[a] - 1 : ca);
+    c[a] = ca;
+    r[a] = w - ca * g.edge[a];
+  }
+  return ok;
+}
+
 __global__ void k_cell_index(int n, const double *__restrict__ pos, GridParams g,
                              int *__restrict__ cell_of, int *__restrict__ cell_count,
                              int *__restrict__ slot, float4 *__restrict__ rel32,
@@ -131,21 +151,9 @@ __global__ void k_cell_index(int n, const double *__restrict__ pos, GridParams g
                              float qscale32, int *__restrict__ err) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  double x[3] = {pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
   int c[3];
   double r[3];
-  const int nd[3] = {g.nx, g.ny, g.nz};
-  bool bad = false;
-  for (int a = 0; a < 3; a++) {
-    if (!isfinite(x[a])) { bad = true; x[a] = g.boxmin[a]; }
-    double w = x[a] - g.boxmin[a];
-    w -= g.boxlen[a] * floor(w / g.boxlen[a]);
-    int ca = (int)floor(w / g.edge[a]);
-    ca = ca < 0 ? 0 : (ca >= nd[a] ? nd[a] - 1 : ca);
-    c[a] = ca;
-    r[a] = w - ca * g.edge[a];
-  }
-  if (bad) atomicOr(err, 1);
+  if (!locate_cell(pos + 3 * (size_t)i, g, c, r)) atomicOr(err, 1);
   int cid = (c[2] * g.ny + c[1]) * g.nx + c[0];
   cell_of[i] = cid;
   slot[i] = atomicAdd(&cell_count[cid], 1);
@@ -317,27 +325,24 @@ __device__ __forceinline__ void jadd(int *sh, unsigned long long *g, float v) {
     atomicAdd(g, (unsigned long long)__float2ll_rn(v * 4294967296.0f));
 }
 
+// One task of the mixed pair kernel for a whole block (kWarps warps): i-cell
+// `cell` and the stencil entries part * kWarps + warp + k * kWarps * nparts
+// (nparts = 1: the cell's whole half shell).  The stencil offsets and the LJ
+// table are read from shared memory; partial_row receives the task's energy
+// and virial partials.  Every thread of the block must call it (it
+// synchronises the block).
 template <int kForm, bool kEnergy, bool kVirial, bool kMolVir>
-__global__ void __launch_bounds__(128)
-k_pair_mixed(GridParams g, MixedConsts mc, const HalfStencil st, int ntypes, const float4 *__restrict__ lj32,
-             const int *__restrict__ start, const float4 *__restrict__ spos,
-             const int2 *__restrict__ smeta, const int *__restrict__ sidx,
-             const int *__restrict__ ex_start, const int2 *__restrict__ ex,
-             unsigned long long *__restrict__ facc, int n, int *__restrict__ err,
-             double *__restrict__ partial, const PbcRef pb, const double *__restrict__ com) {
-  __shared__ float4 s_lj[kMaxTypes * kMaxTypes];
-  __shared__ MixedWarpSmem s_w[kWarps];
-  __shared__ long long s_f[kWarps][32][3];
-  __shared__ double s_acc[kWarps][ACC_MV];
-  if (kForm == FORM_CUTOFF)
-    for (int k = threadIdx.x; k < ntypes * ntypes; k += blockDim.x) s_lj[k] = lj32[k];
+__device__ __forceinline__ void mixed_task(
+    const GridParams &g, const MixedConsts &mc, const unsigned short *st_off, int st_ncells,
+    int part, int nparts, int ntypes, const float4 *s_lj, int cell,
+    const int *__restrict__ start, const float4 *__restrict__ spos,
+    const int2 *__restrict__ smeta, const int *__restrict__ sidx,
+    const int *__restrict__ ex_start, const int2 *__restrict__ ex,
+    unsigned long long *__restrict__ facc, int n, double *__restrict__ partial_row,
+    const PbcRef &pb, const double *__restrict__ com, MixedWarpSmem &sm,
+    long long (*s_f)[32][3], double (*s_acc)[ACC_MV]) {
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
-  MixedWarpSmem &sm = s_w[warp];
-  for (int t = lane; t < kBatch; t += 32) sm.jf[0][t] = sm.jf[1][t] = sm.jf[2][t] = 0;
-  __syncthreads();
-  const int cell = blockIdx.x;
-  if (cell >= g.ncell) return;  // uniform per block
   const int cx = cell % g.nx;
   const int cy = (cell / g.nx) % g.ny;
   const int cz = cell / (g.nx * g.ny);
@@ -549,14 +554,15 @@ k_pair_mixed(GridParams g, MixedConsts mc, const HalfStencil st, int ntypes, con
     // lays the cells end to end, and every batch is loaded with independent
     // loads (a binary search over the prefix finds each entry's cell), so the
     // L2 latency is paid once per batch rather than once per cell.
-    const int nmine = warp < st.ncells ? (st.ncells - warp + kWarps - 1) / kWarps : 0;
+    const int first = part * kWarps + warp, stride = kWarps * nparts;
+    const int nmine = first < st_ncells ? (st_ncells - first + stride - 1) / stride : 0;
     for (int g0 = 0; g0 < nmine; g0 += 32) {
       const int myq = g0 + lane;
       int cjs = 0, ccnt = 0;
       float csx = 0.f, csy = 0.f, csz = 0.f;
       bool chome = false;
       if (myq < nmine) {
-        const unsigned o = st.off[warp + myq * kWarps];
+        const unsigned o = st_off[first + myq * stride];
         const int dx = (int)(o & 31u) - 8, dy = (int)((o >> 5) & 31u) - 8,
                   dz = (int)((o >> 10) & 31u) - 8;
         chome = (dx | dy | dz) == 0;
@@ -663,9 +669,36 @@ k_pair_mixed(GridParams g, MixedConsts mc, const HalfStencil st, int ntypes, con
     if (threadIdx.x < ACC_MV) {
       double sum = 0.0;
       for (int q = 0; q < kWarps; q++) sum += s_acc[q][threadIdx.x];
-      partial[(size_t)cell * kNacc + threadIdx.x] = sum;
+      partial_row[threadIdx.x] = sum;
     }
   }
+}
+
+template <int kForm, bool kEnergy, bool kVirial, bool kMolVir>
+__global__ void __launch_bounds__(128)
+k_pair_mixed(GridParams g, MixedConsts mc, const HalfStencil st, int ntypes, const float4 *__restrict__ lj32,
+             const int *__restrict__ start, const float4 *__restrict__ spos,
+             const int2 *__restrict__ smeta, const int *__restrict__ sidx,
+             const int *__restrict__ ex_start, const int2 *__restrict__ ex,
+             unsigned long long *__restrict__ facc, int n, int *__restrict__ err,
+             double *__restrict__ partial, const PbcRef pb, const double *__restrict__ com) {
+  __shared__ float4 s_lj[kMaxTypes * kMaxTypes];
+  __shared__ MixedWarpSmem s_w[kWarps];
+  __shared__ long long s_f[kWarps][32][3];
+  __shared__ double s_acc[kWarps][ACC_MV];
+  __shared__ unsigned short s_st[kMaxHalfCells];
+  if (kForm == FORM_CUTOFF)
+    for (int k = threadIdx.x; k < ntypes * ntypes; k += blockDim.x) s_lj[k] = lj32[k];
+  for (int k = threadIdx.x; k < st.ncells; k += blockDim.x) s_st[k] = st.off[k];
+  const int lane = threadIdx.x & 31;
+  MixedWarpSmem &sm = s_w[threadIdx.x >> 5];
+  for (int t = lane; t < kBatch; t += 32) sm.jf[0][t] = sm.jf[1][t] = sm.jf[2][t] = 0;
+  __syncthreads();
+  const int cell = blockIdx.x;
+  if (cell >= g.ncell) return;  // uniform per block
+  mixed_task<kForm, kEnergy, kVirial, kMolVir>(
+      g, mc, s_st, st.ncells, 0, 1, ntypes, s_lj, cell, start, spos, smeta, sidx, ex_start, ex,
+      facc, n, partial + (size_t)cell * kNacc, pb, com, sm, s_f, s_acc);
 }
 
 // Fixed-point force accumulator (sorted order, [3][n], 2^-32 quanta in cell
