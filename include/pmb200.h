@@ -225,6 +225,43 @@ int pmb200_eval_noalloc(const pmb200_params *params, int n, const double *d_pos,
 /* Geometry of the device cell grid chosen for the current box. */
 int pmb200_grid(const pmb200_ctx *ctx, int dims[3], double edge[3]);
 
+/* ---- other switching functions ----
+ * A context of the third kind covers the other registrations of
+ * NonbondedCutoffForceModule for periodic boundaries
+ * (protomol/src/protomol/module/NonbondedCutoffForceModule.cpp:53-82):
+ * OneAtomPair<PBC, S, LennardJonesForce>, OneAtomPair<PBC, S, CoulombForce>
+ * (a single potential: the other switch PMB200_SW_NONE) and
+ * OneAtomPairTwo<PBC, S1, LennardJonesForce, S2, CoulombForce>, with S from
+ * C1 (.../switch/C1SwitchingFunction.h), C2 (C2SwitchingFunction.h) and Cn
+ * (CnSwitchingFunction.cpp, orders 2, 3, 4 and 6; the reference's order 5
+ * has an all-zero coefficient table and is refused with
+ * PMB200_EUNSUPPORTED).  Each potential is multiplied by its own switch,
+ * F' = F S - E dS, E' = E S (OneAtomPair.h:80-88).  Per switch the array
+ * holds {switchon, cutoff, order, switchoff}: C1 reads the cutoff only, C2
+ * switchon and cutoff, Cn all four (switchoff 0 or equal to the cutoff, as
+ * CnSwitchingFunction::make requires).  The CmpCnCn switch is not offered.
+ * Energies: LENNARDJONES and COULOMB as for the first kind. */
+#define PMB200_SW_NONE 0
+#define PMB200_SW_C1 1
+#define PMB200_SW_C2 2
+#define PMB200_SW_CN 3
+
+typedef struct {
+  int precision;       /* PMB200_MIXED or PMB200_FP64 */
+  int device;
+  int lj_switch;       /* PMB200_SW_*; NONE: no Lennard-Jones term */
+  double lj[4];        /* {switchon, cutoff, order, switchoff} */
+  int coulomb_switch;  /* PMB200_SW_*; NONE: no Coulomb term */
+  double coulomb[4];
+  double cutoff_alg;   /* algorithm -cutoff; >= both switch cutoffs */
+  double cellsize;     /* grid cell edge hint; 0 = largest cutoff / 2 */
+} pmb200_pair_params;
+
+/* Replaces constructing those NonbondedCutoffSystemForce prototypes through
+ * the factory (NonbondedCutoffForce::doMake, .../force/nonbonded/
+ * NonbondedCutoffForce.h:71-75, with the switch's make). */
+int pmb200_create_pair(const pmb200_pair_params *params, pmb200_ctx **out);
+
 /* ---- derivatives (the differentiable form) ----
  * FP64 pair arithmetic whatever the context's precision; contexts of the
  * cutoff kind only (PMB200_EUNSUPPORTED otherwise).  Units and tables are the

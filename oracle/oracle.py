@@ -117,6 +117,8 @@ def ref_lib(exact_erfc: bool = False):
         lib.pmref_ewald_exact_erfc.restype = _I
         lib.pmref_hessian.argtypes = [_P, _P, _P, _D, _D, _D, _D]
         lib.pmref_hessian.restype = _I
+        lib.pmref_pair_eval.argtypes = [_P, _I, _P, _I, _P, _D, _P, _P, _P, _P, _P, _I]
+        lib.pmref_pair_eval.restype = _I
         if exact_erfc:
             _ref_exact = lib
         else:
@@ -303,6 +305,30 @@ class RefForce:
         self.lib.pmref_ewald_eval(self.h, float(alpha), float(accuracy), _ptr(p), _ptr(f),
                                   _ptr(e), _ptr(v), _ptr(mv), int(virial_mode))
         return f.reshape(-1, 3), float(e[0]), v, mv
+
+    SWITCH_KINDS = {None: 0, "C1": 1, "C2": 2, "Cn": 3}
+
+    def pair_eval(self, pos, lj, coulomb, rc_alg, virial_mode=2):
+        """The reference's NonbondedCutoffSystemForce with OneAtomPair /
+        OneAtomPairTwo and the given switches: lj / coulomb are None or
+        (kind, switchon, cutoff, order, switchoff) with kind C1, C2 or Cn.
+        Returns (forces, energies (coulomb, lj), virial, molvirial)."""
+        def spec(x):
+            if x is None:
+                return 0, np.zeros(4)
+            return self.SWITCH_KINDS[x[0]], np.asarray(x[1:5], dtype=np.float64)
+        kl, pl = spec(lj)
+        kc, pc = spec(coulomb)
+        p = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1)
+        f = np.zeros(p.size)
+        e = np.zeros(2)
+        v = np.zeros(9)
+        mv = np.zeros(9)
+        rc = self.lib.pmref_pair_eval(self.h, kl, _ptr(pl), kc, _ptr(pc), float(rc_alg), _ptr(p),
+                                      _ptr(f), _ptr(e), _ptr(v), _ptr(mv), int(virial_mode))
+        if rc:
+            raise RuntimeError("pmref_pair_eval failed")
+        return f.reshape(-1, 3), e, v, mv
 
     def hessian(self, pos):
         """The reference's analytic Hessian of the LJ(C2) + Coulomb(C1) energy

@@ -27,6 +27,11 @@ PMB200_ENERGY = 1
 PMB200_VIRIAL = 2
 PMB200_MOLVIRIAL = 4
 
+PMB200_SW_NONE = 0
+PMB200_SW_C1 = 1
+PMB200_SW_C2 = 2
+PMB200_SW_CN = 3
+
 PMB200_ERFC_POLY5 = 0
 PMB200_ERFC_EXACT = 1
 
@@ -42,7 +47,7 @@ EXPORTED = (
     "pmb200_batch_create", "pmb200_batch_destroy", "pmb200_batch_last_error",
     "pmb200_batch_eval_device", "pmb200_batch_set_schedule", "pmb200_batch_get_schedule",
     "pmb200_batch_autotune", "pmb200_batch_set_kernel_timing", "pmb200_batch_last_kernel_ms",
-    "pmb200_batch_pair_counts",
+    "pmb200_batch_pair_counts", "pmb200_create_pair",
 )
 
 _P = ctypes.c_void_p
@@ -58,6 +63,12 @@ class Params(ctypes.Structure):
 class EwaldParams(ctypes.Structure):
     _fields_ = [("precision", _I), ("device", _I), ("erfc", _I), ("alpha", _D),
                 ("accuracy", _D), ("cellsize", _D)]
+
+
+class PairParams(ctypes.Structure):
+    _fields_ = [("precision", _I), ("device", _I), ("lj_switch", _I), ("lj", _D * 4),
+                ("coulomb_switch", _I), ("coulomb", _D * 4), ("cutoff_alg", _D),
+                ("cellsize", _D)]
 
 
 class PmbError(RuntimeError):
@@ -104,6 +115,7 @@ def lib():
     L.pmb200_param_grad_device.argtypes = [_P, _P, _P, _P, _P]
     L.pmb200_hvp_device.argtypes = [_P, _P, _P, _P, _P, _P, _P]
     L.pmb200_update_params.argtypes = [_P, _P, _P]
+    L.pmb200_create_pair.argtypes = [ctypes.POINTER(PairParams), ctypes.POINTER(_P)]
     L.pmb200_batch_create.argtypes = [ctypes.POINTER(_P), _I, ctypes.POINTER(_P)]
     L.pmb200_batch_destroy.argtypes = [_P]
     L.pmb200_batch_last_error.argtypes = [_P]

@@ -31,6 +31,10 @@ struct pmb200_ctx {
   int form = FORM_CUTOFF;
   double ew_alpha_in = 0.0, ew_accuracy = 0.0;
   double ew_alpha = 0.0, ew_rc = 0.0;
+  // generic form: switch kind and {switchon, cutoff, order, switchoff} per
+  // potential (LJ, Coulomb)
+  int sw_kind[2] = {0, 0};
+  double sw_par[2][4] = {};
   // the box as last given (re-applied when an Ewald default alpha changes)
   bool box_given = false;
   double box_e[3][3] = {}, box_origin[3] = {};
@@ -142,7 +146,82 @@ void release_graph(pmb200_ctx *c) {
 double rc_max(const pmb200_params &p) { return std::max(p.cutoff_lj, p.cutoff_coul); }
 
 // Pair cutoff of the context's potential.
-double ctx_rc(const pmb200_ctx *c) { return c->form == FORM_CUTOFF ? rc_max(c->p) : c->ew_rc; }
+double ctx_rc(const pmb200_ctx *c) {
+  if (c->form == FORM_GENERIC) {
+    double r = 0.0;
+    for (int k = 0; k < 2; k++)
+      if (c->sw_kind[k] != SW_OFF) r = std::max(r, c->sw_par[k][1]);
+    return r;
+  }
+  return c->form == FORM_CUTOFF ? rc_max(c->p) : c->ew_rc;
+}
+
+// Cn polynomial coefficients (CnSwitchingFunction.cpp:9-31), rows by order
+// 2, 3, 4, (5: all zero in the reference), 6.
+const double kCnValue[5][7] = {{10., -15., 6., 0, 0, 0, 0},
+                               {35., -84., 70., -20., 0, 0, 0},
+                               {126., -420., 540., -315., 70., 0, 0},
+                               {0, 0, 0, 0, 0, 0, 0},
+                               {1716., -9009., 20020., -24024., 16380., -6006., 924.0}};
+const double kCnDeriv[5][7] = {{30., -60., 30., 0, 0, 0, 0},
+                               {140., -420., 420., -140., 0, 0, 0},
+                               {630., -2520., 3780., -2520., 630., 0, 0},
+                               {0, 0, 0, 0, 0, 0, 0},
+                               {12012., -72072., 180180., -240240., 180180., -72072., 12012.0}};
+
+double binomial(int n, int k) {
+  double b = 1.0;
+  for (int i = 1; i <= k; i++) b = b * (n - k + i) / i;
+  return b;
+}
+
+// The Bernstein form used on the device reproduces the reference's power
+// tables: expanding sum_j binom(2n+1, n+1+j) t^(n+1+j) (1-t)^(n-j) gives
+// kCnValue's row (checked once per process, on the host).
+bool cn_tables_agree() {
+  for (int n : {2, 3, 4, 6}) {
+    double poly[14] = {0};
+    for (int j = 0; j <= n; j++) {
+      const double b = binomial(2 * n + 1, n + 1 + j);
+      for (int m = 0; m <= n - j; m++)  // (1-t)^(n-j) = sum_m binom(n-j, m) (-t)^m
+        poly[n + 1 + j + m] += b * binomial(n - j, m) * ((m & 1) ? -1.0 : 1.0);
+    }
+    for (int i = 0; i <= n; i++)
+      if (std::fabs(poly[n + 1 + i] - kCnValue[n - 2][i]) > 1e-9) return false;
+  }
+  return true;
+}
+
+// A switch's constants with lengths divided by u (1 for Angstrom).
+template <class T>
+SwitchSpec<T> make_switch(int kind, const double par[4], double u) {
+  SwitchSpec<T> w{};
+  w.kind = kind;
+  if (kind == SW_OFF) return w;
+  const double ron = par[0] / u, rc = par[1] / u;
+  w.rc2 = (T)(rc * rc);
+  w.rc = (T)rc;
+  if (kind == SW_C1) {  // C1SwitchingFunction.cpp:12-16
+    w.a = (T)(1.5 / rc);
+    w.b = (T)(0.5 / (rc * rc * rc));
+    w.c = (T)(1.5 / (rc * rc * rc));
+  } else if (kind == SW_C2) {  // C2SwitchingFunction.cpp:12-18
+    const double t = rc * rc - ron * ron;
+    w.ron2 = (T)(ron * ron);
+    w.a = (T)(1.0 / ((t * t) * t));
+    w.b = (T)(rc * rc - 3.0 * ron * ron);
+    w.c = (T)(4.0 / ((t * t) * t));
+  } else if (kind == SW_CN) {  // CnSwitchingFunction.cpp:38-60
+    const int n = (int)par[2];
+    w.nord = n;
+    w.ron2 = (T)(ron * ron);
+    w.ron = (T)ron;
+    w.inv_range = (T)(1.0 / (ron - rc));
+    for (int j = 0; j <= n; j++) w.vcoef[j] = (T)binomial(2 * n + 1, n + 1 + j);
+    w.dpeak = (T)kCnDeriv[n - 2][0];
+  }
+  return w;
+}
 
 // NonbondedFullEwaldSystemForce::initialize
 // (protomol/src/protomol/force/nonbonded/NonbondedFullEwaldSystemForce.h:
@@ -290,14 +369,17 @@ int launch_eval(pmb200_ctx *c, const double *d_pos, double *d_forces, double *d_
   if (mixed) {
     const double fscale = 1.0 / g.unit;
     if (n > 0) CK(cudaMemsetAsync(c->d_facc, 0, sizeof(unsigned long long) * 3 * (size_t)n, st));
-    if (c->form == FORM_EWALD_POLY5) launch_pair_mixed<FORM_EWALD_POLY5>(c, flags, st);
+    if (c->form == FORM_GENERIC) launch_pair_mixed<FORM_GENERIC>(c, flags, st);
+    else if (c->form == FORM_EWALD_POLY5) launch_pair_mixed<FORM_EWALD_POLY5>(c, flags, st);
     else if (c->form == FORM_EWALD_EXACT) launch_pair_mixed<FORM_EWALD_EXACT>(c, flags, st);
     else launch_pair_mixed<FORM_CUTOFF>(c, flags, st);
     if (n > 0)
       k_finalize<<<(n + 255) / 256, 256, 0, st>>>(n, c->d_facc, c->d_sidx, fscale * kFixInv,
                                                   accumulate, d_forces);
   } else {
-    if (c->form == FORM_EWALD_POLY5)
+    if (c->form == FORM_GENERIC)
+      launch_pair_fp64<FORM_GENERIC>(c, flags, d_forces, accumulate, blocks, st);
+    else if (c->form == FORM_EWALD_POLY5)
       launch_pair_fp64<FORM_EWALD_POLY5>(c, flags, d_forces, accumulate, blocks, st);
     else if (c->form == FORM_EWALD_EXACT)
       launch_pair_fp64<FORM_EWALD_EXACT>(c, flags, d_forces, accumulate, blocks, st);
@@ -400,6 +482,57 @@ int pmb200_create_ewald_real(const pmb200_ewald_params *params, pmb200_ctx **out
   c->form = e.erfc == PMB200_ERFC_EXACT ? FORM_EWALD_EXACT : FORM_EWALD_POLY5;
   c->ew_alpha_in = e.alpha;
   c->ew_accuracy = e.accuracy;
+  *out = c;
+  return PMB200_OK;
+}
+
+int pmb200_create_pair(const pmb200_pair_params *params, pmb200_ctx **out) {
+  if (!params || !out) return PMB200_EINVAL;
+  *out = nullptr;
+  const pmb200_pair_params &q = *params;
+  const int kinds[2] = {q.lj_switch, q.coulomb_switch};
+  const double *pars[2] = {q.lj, q.coulomb};
+  double rcmax = 0.0;
+  if (kinds[0] == PMB200_SW_NONE && kinds[1] == PMB200_SW_NONE) return PMB200_EINVAL;
+  for (int k = 0; k < 2; k++) {
+    const int kd = kinds[k];
+    const double *pr = pars[k];
+    if (kd == PMB200_SW_NONE) continue;
+    if (kd != PMB200_SW_C1 && kd != PMB200_SW_C2 && kd != PMB200_SW_CN) return PMB200_EINVAL;
+    const double ron = pr[0], rc = pr[1], order = pr[2], roff = pr[3];
+    if (!(rc > 0.0) || !std::isfinite(rc)) return PMB200_EINVAL;
+    if (kd == PMB200_SW_C2 && !(ron >= 0.0 && ron < rc)) return PMB200_EINVAL;
+    if (kd == PMB200_SW_CN) {
+      // CnSwitchingFunction::make (CnSwitchingFunction.cpp:84-112)
+      if (!(ron >= 0.0 && ron < rc) || (roff > 0.0 && roff != rc) || order < 2.0 || order > 6.0)
+        return PMB200_EINVAL;
+      // the reference's order 5 has an all-zero coefficient row
+      if ((int)order == 5 || order != std::floor(order)) return PMB200_EUNSUPPORTED;
+      static const bool agree = cn_tables_agree();
+      if (!agree) return PMB200_EUNSUPPORTED;
+    }
+    rcmax = std::max(rcmax, rc);
+  }
+  if (!(q.cutoff_alg > 0.0) || q.cellsize < 0.0) return PMB200_EINVAL;
+  if (q.cutoff_alg < rcmax) return PMB200_EUNSUPPORTED;
+  pmb200_params p{};
+  p.precision = q.precision;
+  p.device = q.device;
+  p.switchon = 0.0;
+  p.cutoff_lj = p.cutoff_coul = rcmax;
+  p.cutoff_alg = q.cutoff_alg;
+  p.cellsize = q.cellsize;
+  pmb200_ctx *c = nullptr;
+  const int rc = pmb200_create(&p, &c);
+  if (rc) return rc;
+  c->form = FORM_GENERIC;
+  for (int k = 0; k < 2; k++) {
+    c->sw_kind[k] = kinds[k] == PMB200_SW_C1   ? SW_C1
+                    : kinds[k] == PMB200_SW_C2 ? SW_C2
+                    : kinds[k] == PMB200_SW_CN ? SW_CN
+                                               : SW_OFF;
+    for (int j = 0; j < 4; j++) c->sw_par[k][j] = pars[k][j];
+  }
   *out = c;
   return PMB200_OK;
 }
@@ -656,6 +789,8 @@ int pmb200_set_box(pmb200_ctx *c, const double e1[3], const double e2[3], const 
   m.csf = (float)c->csf;
   m.ey = (float)(g.edge[1] / u);
   m.ez = (float)(g.edge[2] / u);
+  m.swl = make_switch<float>(c->sw_kind[0], c->sw_par[0], u);
+  m.swc = make_switch<float>(c->sw_kind[1], c->sw_par[1], u);
   m.ea = (float)(c->ew_alpha * u);
   m.ea2pi = (float)(2.0 * c->ew_alpha * u / std::sqrt(M_PI));
   Fp64Consts &f = c->fc;
@@ -671,6 +806,8 @@ int pmb200_set_box(pmb200_ctx *c, const double e1[3], const double e2[3], const 
   f.c05_3 = 0.5 / (p.cutoff_coul * p.cutoff_coul * p.cutoff_coul);
   f.c15_3 = 1.5 / (p.cutoff_coul * p.cutoff_coul * p.cutoff_coul);
   f.csf = c->csf;
+  f.swl = make_switch<double>(c->sw_kind[0], c->sw_par[0], 1.0);
+  f.swc = make_switch<double>(c->sw_kind[1], c->sw_par[1], 1.0);
   f.ea = c->ew_alpha;
   f.ea2 = c->ew_alpha * c->ew_alpha;
   f.ea2pi = 2.0 * c->ew_alpha / std::sqrt(M_PI);
@@ -1499,7 +1636,8 @@ int batch_launch_eval(pmb200_batch *b, const double *d_pos, double *d_forces, do
   const int bpsm = b->bpsm > 0 ? std::min(b->bpsm, b->max_bpsm) : b->max_bpsm;
   const int grid = std::max(1, std::min(b->ntasks, bpsm * b->nsm));
   if (timed) BCK(cudaEventRecord(b->ev0, st));
-  if (b->form == FORM_EWALD_POLY5) batch_launch_pair<FORM_EWALD_POLY5>(b, energy, virial, grid, st);
+  if (b->form == FORM_GENERIC) batch_launch_pair<FORM_GENERIC>(b, energy, virial, grid, st);
+  else if (b->form == FORM_EWALD_POLY5) batch_launch_pair<FORM_EWALD_POLY5>(b, energy, virial, grid, st);
   else if (b->form == FORM_EWALD_EXACT) batch_launch_pair<FORM_EWALD_EXACT>(b, energy, virial, grid, st);
   else batch_launch_pair<FORM_CUTOFF>(b, energy, virial, grid, st);
   if (timed) BCK(cudaEventRecord(b->ev1, st));

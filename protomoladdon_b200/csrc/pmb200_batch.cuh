@@ -88,7 +88,7 @@ k_pair_mixed_batch(const BatchSys *__restrict__ sys, const int4 *__restrict__ ta
         dst[k] = src[k];
       const BatchSys &gs = sys[tk.x];
       for (int k = threadIdx.x; k < gs.st_n; k += blockDim.x) s_st[k] = stencils[gs.st0 + k];
-      if (kForm == FORM_CUTOFF)
+      if (kForm == FORM_CUTOFF || kForm == FORM_GENERIC)
         for (int k = threadIdx.x; k < gs.ntypes * gs.ntypes; k += blockDim.x)
           s_lj[k] = lj32[gs.lj0 + k];
       loaded = tk.x;

@@ -76,7 +76,63 @@ __device__ __forceinline__ void ref_min_image(const PbcRef &b, double v[3]) {
 // Pair potential of a context: ProtoMol's cutoff LJ (C2) + Coulomb (C1)
 // force, or the real-space Ewald term with erfc from the Abramowitz & Stegun
 // polynomial (the reference's default build) or from erfc itself.
-enum PairForm { FORM_CUTOFF = 0, FORM_EWALD_POLY5 = 1, FORM_EWALD_EXACT = 2 };
+enum PairForm { FORM_CUTOFF = 0, FORM_EWALD_POLY5 = 1, FORM_EWALD_EXACT = 2, FORM_GENERIC = 3 };
+
+// Switching functions of the generic form (each potential its own; SW_OFF:
+// the potential is absent).  dS is ProtoMol's "deriv": dS/dr / r.
+enum SwitchKind { SW_OFF = 0, SW_C1 = 1, SW_C2 = 2, SW_CN = 3 };
+
+template <class T>
+struct SwitchSpec {
+  int kind, nord;    // SwitchKind; Cn: integer order
+  T rc2, ron2, rc;   // cutoff^2, switchon^2, cutoff
+  T a, b, c;         // C1: 1.5/rc, 0.5/rc^3, 1.5/rc^3; C2: s1, s2, s3 (C2SwitchingFunction.cpp)
+  T ron, inv_range;  // Cn: switchon, 1 / (switchon - cutoff)
+  T vcoef[7];        // Cn: binom(2n+1, n+1+j), j = 0..n
+  T dpeak;           // Cn: (2n+1)! / (n!)^2
+};
+
+// Value S and deriv dS (= dS/dr / r) at r^2 (rinv = 1/r), following
+// C1SwitchingFunction.h:41-50, C2SwitchingFunction.h:42-53 and
+// CnSwitchingFunction.cpp:149-172.  Cn: the reference sums
+// swcoef_i t^(n+1+i) with t = (r - rc)/(switchon - rc); its tables are the
+// smoothstep polynomials, evaluated here in their Bernstein form
+//   S = sum_{k=n+1}^{2n+1} binom(2n+1, k) t^k u^(2n+1-k),  u = 1 - t,
+//   dS/dt = (2n+1)!/(n!)^2 t^n u^n,
+// whose terms are all positive (the power form cancels to ~1e-4 of its
+// terms at order 6, too much for FP32); t and u are both taken from r.
+template <class T>
+__device__ __forceinline__ void switch_eval(const SwitchSpec<T> &w, T r2, T rinv, T &S, T &dS) {
+  S = T(0);
+  dS = T(0);
+  if (r2 > w.rc2) return;
+  if (w.kind == SW_C1) {
+    const T dist = r2 * rinv;
+    S = T(1) - dist * (w.a - r2 * w.b);
+    dS = -w.a * rinv + dist * w.c;
+  } else if (w.kind == SW_C2) {
+    if (r2 < w.ron2) { S = T(1); return; }
+    const T c2 = w.rc2 - r2;
+    const T c4 = c2 * (w.b + T(2) * r2);
+    S = w.a * (c2 * c4);
+    dS = w.c * (c2 * c2 - c4);
+  } else if (w.kind == SW_CN) {
+    if (r2 < w.ron2) { S = T(1); return; }
+    const T r = r2 * rinv;
+    const T t = (r - w.rc) * w.inv_range;
+    const T u = (w.ron - r) * w.inv_range;
+    T tn = T(1), un = T(1);
+    for (int k = 0; k < w.nord; k++) { tn *= t; un *= u; }
+    // sum_j vcoef_j t^j u^(n-j), by Horner in t/u homogeneous form
+    T acc = w.vcoef[w.nord], up = T(1);
+    for (int j = w.nord - 1; j >= 0; j--) {
+      up *= u;
+      acc = acc * t + w.vcoef[j] * up;
+    }
+    S = tn * t * acc;
+    dS = w.dpeak * tn * un * w.inv_range * rinv;
+  }
+}
 
 // Abramowitz & Stegun, Handbook of Mathematical Functions, 7.1.26:
 // erfc(x) ~ t (a1 + t (a2 + t (a3 + t (a4 + t a5)))) exp(-x^2),
@@ -93,6 +149,7 @@ struct MixedConsts {   // FP32 constants in cell units
   float csf;                 // coulombScalingFactor
   float ey, ez;              // edge[1] / unit, edge[2] / unit (1 for cubic cells)
   float ea, ea2pi;           // Ewald alpha and 2 alpha / sqrt(pi), per cell unit
+  SwitchSpec<float> swl, swc;  // generic form: LJ and Coulomb switches
 };
 
 struct Fp64Consts {
@@ -101,6 +158,7 @@ struct Fp64Consts {
   double c15_1, c05_3, c15_3;
   double csf;
   double ea, ea2, ea2pi;     // Ewald alpha, alpha^2, 2 alpha / sqrt(pi) (1/A)
+  SwitchSpec<double> swl, swc;  // generic form: LJ and Coulomb switches
 };
 
 // The stencil travels by value in the kernel parameters (per launch, so
@@ -440,7 +498,32 @@ __device__ __forceinline__ void mixed_task(
         rinv = fmaf(0.5f * rinv, fmaf(-r2 * rinv, rinv, 1.0f), rinv);
         const float r2inv = rinv * rinv;
         float f;
-        if constexpr (kForm != FORM_CUTOFF) {
+        if constexpr (kForm == FORM_GENERIC) {
+          // OneAtomPair / OneAtomPairTwo with any of the C1, C2, Cn switches
+          // (OneAtomPair.h:62-105, OneAtomPairTwo.h:57-125)
+          f = 0.0f;
+          if (mc.swl.kind != SW_OFF) {
+            const float4 p = s_lj[ti + mj.x];
+            const float A = kind == 1 ? p.z : p.x;
+            const float B = kind == 1 ? p.w : p.y;
+            const float r6 = r2inv * r2inv * r2inv;
+            float elj = fmaf(A, r6, -B) * r6;
+            float flj = fmaf(12.0f * A, r6, -6.0f * B) * r6 * r2inv;
+            float S, dS;
+            switch_eval(mc.swl, r2, rinv, S, dS);
+            f = fmaf(flj, S, -elj * dS);
+            if (kEnergy) pE += elj * S;
+          }
+          if (mc.swc.kind != SW_OFF) {
+            float qj = pj.w;
+            if (kind == 1) qj *= mc.csf;
+            const float ec = pi.w * qj * rinv;
+            float S, dS;
+            switch_eval(mc.swc, r2, rinv, S, dS);
+            f += fmaf(ec * r2inv, S, -ec * dS);
+            if (kEnergy) kU.add(qj * rinv * S);
+          }
+        } else if constexpr (kForm != FORM_CUTOFF) {
           // real-space Ewald (NonbondedFullEwaldSystemForce.h:803-823):
           // g = erfc(a r) / r, F / r = q_i q_j (g + 2a/sqrt(pi) e^{-a^2 r^2}) / r^2
           float qj = pj.w;
@@ -687,7 +770,7 @@ k_pair_mixed(GridParams g, MixedConsts mc, const HalfStencil st, int ntypes, con
   __shared__ long long s_f[kWarps][32][3];
   __shared__ double s_acc[kWarps][ACC_MV];
   __shared__ unsigned short s_st[kMaxHalfCells];
-  if (kForm == FORM_CUTOFF)
+  if (kForm == FORM_CUTOFF || kForm == FORM_GENERIC)
     for (int k = threadIdx.x; k < ntypes * ntypes; k += blockDim.x) s_lj[k] = lj32[k];
   for (int k = threadIdx.x; k < st.ncells; k += blockDim.x) s_st[k] = st.off[k];
   const int lane = threadIdx.x & 31;
@@ -786,8 +869,37 @@ k_pair_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes, const dou
             kind = excl_kind(ex, elo, ehi, sidx[j]);
             if (kind == 2) continue;
           }
-          double f, e1 = 0.0, e2;
-          if constexpr (kForm != FORM_CUTOFF) {
+          double f, e1 = 0.0, e2 = 0.0;
+          if constexpr (kForm == FORM_GENERIC) {
+            f = 0.0;
+            const double rd2 = 1.0 / r2;
+            const double rinv = sqrt(rd2);
+            if (mc.swl.kind != SW_OFF) {
+              const double4 p = lj64[ti + mj.x];
+              const double A = kind == 1 ? p.z : p.x;
+              const double B = kind == 1 ? p.w : p.y;
+              const double r6 = rd2 * rd2 * rd2;
+              const double r12 = r6 * r6;
+              const double r6B = B * r6, r12A = A * r12;
+              e1 = r12A - r6B;
+              double f1 = 12.0 * r12A * rd2 - 6.0 * r6B * rd2;
+              double S, dS;
+              switch_eval(mc.swl, r2, rinv, S, dS);
+              f1 = f1 * S - e1 * dS;
+              e1 = e1 * S;
+              f += f1;
+            }
+            if (mc.swc.kind != SW_OFF) {
+              e2 = pi.w * pj.w * rinv;
+              if (kind == 1) e2 *= mc.csf;
+              double f2 = e2 * rd2;
+              double S, dS;
+              switch_eval(mc.swc, r2, rinv, S, dS);
+              f2 = f2 * S - e2 * dS;
+              e2 = e2 * S;
+              f += f2;
+            }
+          } else if constexpr (kForm != FORM_CUTOFF) {
             // NonbondedFullEwaldSystemForce::realTerm's pair arithmetic
             // (NonbondedFullEwaldSystemForce.h:803-823)
             const double r = sqrt(r2);

@@ -397,3 +397,104 @@ class EwaldRealB200SystemForce(NonbondedCutoffB200SystemForce):
         a, r = ctypes.c_double(), ctypes.c_double()
         self._check(_lib.lib().pmb200_ewald_info(self._ctx, ctypes.byref(a), ctypes.byref(r)))
         return a.value, r.value
+
+
+class NonbondedCutoffB200PairForce(NonbondedCutoffB200SystemForce):
+    """The other periodic cutoff registrations of NonbondedCutoffForceModule
+    (protomol/src/protomol/module/NonbondedCutoffForceModule.cpp:53-82):
+    OneAtomPair<PBC, S, LennardJonesForce>, OneAtomPair<PBC, S, CoulombForce>
+    and OneAtomPairTwo<PBC, S1, LennardJonesForce, S2, CoulombForce> with S
+    among C1, C2, Cn.  ``lj`` / ``coulomb``: None (term absent) or a tuple
+    (kind, switchon, cutoff, order, switchoff); C1 reads the cutoff, C2
+    switchon and cutoff, Cn all four (see pmb200_create_pair)."""
+
+    keyword = "NonbondedCutoffB200"
+    _KIND = {None: _lib.PMB200_SW_NONE, "C1": _lib.PMB200_SW_C1, "C2": _lib.PMB200_SW_C2,
+             "Cn": _lib.PMB200_SW_CN}
+    # switch parameters as the reference lists them (getParameters)
+    _PARAMS = {"C1": ["-cutoff"], "C2": ["-switchon", "-cutoff"],
+               "Cn": ["-n", "-switchon", "-switchoff", "-cutoff"]}
+
+    def __init__(self, lj=None, coulomb=None, cutoff_alg=None, precision="mixed", device=0,
+                 cellsize=0.0):
+        def norm(sw):
+            if sw is None:
+                return None
+            sw = tuple(sw) + (0.0,) * (5 - len(sw))
+            if sw[0] not in ("C1", "C2", "Cn"):
+                raise ValueError(f"switching function {sw[0]!r}: C1, C2 or Cn")
+            return (sw[0],) + tuple(float(x) for x in sw[1:5])
+        self.lj = norm(lj)
+        self.coulomb = norm(coulomb)
+        if self.lj is None and self.coulomb is None:
+            raise ValueError("need a Lennard-Jones or a Coulomb term")
+        rcs = [s[2] for s in (self.lj, self.coulomb) if s is not None]
+        self.cutoff_alg = float(cutoff_alg if cutoff_alg is not None else max(rcs))
+        self.precision = precision
+        self.device = int(device)
+        self.cellsize = float(cellsize)
+        self._ctx = None
+        self._topo_key = None
+        self._box_key = None
+
+    def _create(self, topo):
+        def arr(sw):
+            return (ctypes.c_double * 4)(*(sw[1:5] if sw else (0.0,) * 4))
+        p = _lib.PairParams(
+            _lib.PMB200_MIXED if self.precision == "mixed" else _lib.PMB200_FP64, self.device,
+            self._KIND[self.lj[0] if self.lj else None], arr(self.lj),
+            self._KIND[self.coulomb[0] if self.coulomb else None], arr(self.coulomb),
+            self.cutoff_alg, self.cellsize or topo.cellsize)
+        h = _P()
+        rc = _lib.lib().pmb200_create_pair(ctypes.byref(p), ctypes.byref(h))
+        if rc != _lib.PMB200_OK:
+            raise PmbError(rc, "pmb200_create_pair rejected the parameters")
+        return h
+
+    @classmethod
+    def _switch_args(cls, sw):
+        kind, ron, rc, order, roff = sw
+        vals = {"-cutoff": rc, "-switchon": ron, "-n": order, "-switchoff": roff}
+        return " ".join(f"{k} {vals[k]:g}" for k in cls._PARAMS[kind])
+
+    def get_id(self):
+        pots = [n for n, s in (("LennardJones", self.lj), ("Coulomb", self.coulomb)) if s]
+        sws = [s for s in (self.lj, self.coulomb) if s]
+        head = " ".join(pots) + f" -algorithm {self.keyword} " + " ".join(
+            f"-switchingFunction {s[0]}" for s in sws)
+        return head + " " + " ".join(self._switch_args(s) for s in sws) + \
+            f" -cutoff {self.cutoff_alg:g}"
+
+    @classmethod
+    def from_id(cls, force_id, **kw):
+        toks = force_id.split()
+        pots = []
+        while toks and not toks[0].startswith("-"):
+            pots.append(toks.pop(0))
+        if pots not in (["LennardJones"], ["Coulomb"], ["LennardJones", "Coulomb"]):
+            raise ValueError(f"potentials {pots}: LennardJones and/or Coulomb")
+        pairs = list(zip(toks[0::2], toks[1::2]))
+        if len(toks) % 2:
+            raise ValueError(f"cannot parse force id {force_id!r}")
+        if [v for k, v in pairs if k == "-algorithm"] != [cls.keyword]:
+            raise ValueError(f"algorithm must be {cls.keyword}")
+        sws = [v for k, v in pairs if k == "-switchingFunction"]
+        if len(sws) != len(pots):
+            raise ValueError("one switching function per potential")
+        params = [(k, float(v)) for k, v in pairs if k not in ("-algorithm", "-switchingFunction")]
+        specs = []
+        for sw in sws:
+            if sw not in cls._PARAMS:
+                raise ValueError(f"switching function {sw!r}: C1, C2 or Cn")
+            vals = {}
+            for key in cls._PARAMS[sw]:
+                if not params or params[0][0] != key:
+                    raise ValueError(f"{sw}: expected {key}")
+                vals[key] = params.pop(0)[1]
+            specs.append((sw, vals.get("-switchon", 0.0), vals["-cutoff"], vals.get("-n", 0.0),
+                          vals.get("-switchoff", 0.0)))
+        if len(params) != 1 or params[0][0] != "-cutoff":
+            raise ValueError("expected the algorithm -cutoff last")
+        lj = specs[0] if pots[0] == "LennardJones" else None
+        co = specs[-1] if pots[-1] == "Coulomb" else None
+        return cls(lj, co, params[0][1], **kw)

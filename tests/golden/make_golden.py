@@ -28,6 +28,11 @@ Fixtures (all inputs and outputs FP64):
   molecular virial from the reference as shipped (``poly5_*``, erfc by the
   Abramowitz & Stegun polynomial) and built with -DUSE_EWALD_EXACT_ERF
   (``exact_*``).  ``--ewald-only`` writes just these.
+* pairs_ref.npz -- the reference's other periodic cutoff registrations
+  (OneAtomPair / OneAtomPairTwo with C1, C2, Cn switches) on the 648-atom
+  box: per case ``<case>_{forces,energies,virial,molvirial}`` and the switch
+  specs ``<case>_lj`` / ``<case>_coul`` ({kind code, switchon, cutoff,
+  order, switchoff}, kind 0 = absent).  ``--pairs-only`` writes just this.
 """
 from __future__ import annotations
 
@@ -122,8 +127,40 @@ def ewald_fixtures():
     print("wrote Ewald fixtures to", HERE)
 
 
+PAIR_CASES = {
+    # name: (LJ switch, Coulomb switch), each (kind, switchon, cutoff, order, switchoff)
+    "c2_c2": (("C2", 6.5, 8.0, 0, 0), ("C2", 0.0, 8.0, 0, 0)),
+    "c2_cn": (("C2", 6.5, 8.0, 0, 0), ("Cn", 5.0, 8.0, 4, 0)),
+    "cn_cn": (("Cn", 6.0, 8.0, 3, 8.0), ("Cn", 4.0, 8.0, 6, 0)),
+    "lj_c1": (("C1", 0.0, 8.0, 0, 0), None),
+    "lj_cn": (("Cn", 6.5, 8.0, 2, 0), None),
+    "coul_c2": (None, ("C2", 3.0, 8.0, 0, 0)),
+    "coul_cn": (None, ("Cn", 5.0, 8.0, 4, 0)),
+}
+
+
+def pair_fixtures():
+    w = water.small_648()
+    out = dict(sysd_arrays(w))
+    codes = {"C1": 1, "C2": 2, "Cn": 3}
+    R = O.RefForce(w)
+    for name, (lj, co) in PAIR_CASES.items():
+        f, e, v, mv = R.pair_eval(w["pos"], lj, co, 8.0, 2)
+        out.update({f"{name}_forces": f, f"{name}_energies": e, f"{name}_virial": v,
+                    f"{name}_molvirial": mv})
+        for tag, sw in (("lj", lj), ("coul", co)):
+            out[f"{name}_{tag}"] = (np.zeros(5) if sw is None else
+                                    np.array([codes[sw[0]], *sw[1:]], dtype=np.float64))
+    R.close()
+    np.savez_compressed(os.path.join(HERE, "pairs_ref.npz"), **out)
+    print("wrote switch-policy fixtures to", HERE)
+
+
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
-    if "--ewald-only" not in sys.argv:
+    if "--ewald-only" not in sys.argv and "--pairs-only" not in sys.argv:
         main(args[0] if args else "/root/reference")
-    ewald_fixtures()
+    if "--pairs-only" not in sys.argv:
+        ewald_fixtures()
+    if "--ewald-only" not in sys.argv:
+        pair_fixtures()

@@ -156,3 +156,40 @@ def test_lj_table_mixing_matches_the_generator():
     e = torch.tensor([0.2, 0.0], dtype=torch.float64, requires_grad=True)
     lj_table(s, e).sum().backward()
     assert torch.isfinite(s.grad).all() and torch.isfinite(e.grad).all()
+
+
+def test_pair_form_create_validates_before_touching_a_device():
+    L = _lib.lib()
+    h = ctypes.c_void_p()
+    D4 = ctypes.c_double * 4
+
+    def P(lk, lp, ck, cp, alg=10.0):
+        return _lib.PairParams(0, 0, lk, D4(*lp), ck, D4(*cp), alg, 0.0)
+    C2, CN, C1, NO = _lib.PMB200_SW_C2, _lib.PMB200_SW_CN, _lib.PMB200_SW_C1, _lib.PMB200_SW_NONE
+    z = (0, 0, 0, 0)
+    bad = [P(NO, z, NO, z),                          # no term at all
+           P(C2, (9, 9, 0, 0), NO, z),               # C2 switchon == cutoff
+           P(CN, (5, 8, 7, 0), NO, z),               # Cn order above 6
+           P(CN, (5, 8, 4, 9), NO, z),               # switchoff neither 0 nor the cutoff
+           P(C1, (0, -1, 0, 0), NO, z),              # negative cutoff
+           P(9, (0, 8, 0, 0), NO, z)]                # unknown switch
+    for p in bad:
+        assert L.pmb200_create_pair(ctypes.byref(p), ctypes.byref(h)) == _lib.PMB200_EINVAL
+    p = P(CN, (5, 8, 5, 0), NO, z)                   # order 5: the reference's zero table
+    assert L.pmb200_create_pair(ctypes.byref(p), ctypes.byref(h)) == _lib.PMB200_EUNSUPPORTED
+    p = P(C1, (0, 9, 0, 0), C1, (0, 9, 0, 0), alg=8.0)  # algorithm cutoff below a switch
+    assert L.pmb200_create_pair(ctypes.byref(p), ctypes.byref(h)) == _lib.PMB200_EUNSUPPORTED
+
+
+def test_pair_form_ids_round_trip():
+    from protomoladdon_b200.force import NonbondedCutoffB200PairForce as P
+    for lj, co in ((("C2", 6.5, 8.0), ("Cn", 5.0, 8.0, 4, 0)), (None, ("C1", 0, 9.0)),
+                   (("Cn", 6, 8, 3, 8), None), (("C2", 7, 9), ("C2", 0, 9))):
+        f = P(lj, co)
+        g = P.from_id(f.get_id())
+        assert g.get_id() == f.get_id() and g.lj == f.lj and g.coulomb == f.coulomb
+    with pytest.raises(ValueError):
+        P.from_id("LennardJones -algorithm NonbondedCutoffB200 -switchingFunction C2 -cutoff 8 "
+                  "-cutoff 8")  # C2 wants -switchon first
+    with pytest.raises(ValueError):
+        P(("C3", 1, 2), None)
