@@ -262,6 +262,20 @@ typedef struct {
  * NonbondedCutoffForce.h:71-75, with the switch's make). */
 int pmb200_create_pair(const pmb200_pair_params *params, pmb200_ctx **out);
 
+/* Vacuum boundaries, in place of pmb200_set_box: the force with
+ * VacuumBoundaryConditions (plain differences, no images,
+ * protomol/src/protomol/topology/VacuumBoundaryConditions.h) as the
+ * vacuum registrations of NonbondedCutoffForceModule build it
+ * (NonbondedCutoffForceModule.cpp:84-134, cells walked by
+ * CellListEnumeratorStandard.h).  [lo, hi] is the cell-grid domain (any size;
+ * edges need not exceed the cutoff).  Atoms outside it are binned into its
+ * boundary cells with their true coordinates, so every pair is still found,
+ * but FP32 cell-relative coordinates lose precision far outside: keep the
+ * domain around the atoms (e.g. their bounding box plus a margin).  Any
+ * context kind except the Ewald term; pmb200_set_box makes it periodic
+ * again. */
+int pmb200_set_vacuum_domain(pmb200_ctx *ctx, const double lo[3], const double hi[3]);
+
 /* ---- derivatives (the differentiable form) ----
  * FP64 pair arithmetic whatever the context's precision; contexts of the
  * cutoff kind only (PMB200_EUNSUPPORTED otherwise).  Units and tables are the

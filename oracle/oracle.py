@@ -361,6 +361,29 @@ class RefForce:
             pass
 
 
+def ref_vacuum_eval(sysd, pos, virial_mode=2):
+    """The reference's vacuum cutoff force (OneAtomPairTwo<VacuumBoundary
+    Conditions, C2, LJ, C1, Coulomb>) on the system's arrays and cutoffs:
+    (forces, energies (coulomb, lj), virial, molvirial)."""
+    lib = ref_lib()
+    lib.pmref_vacuum_eval.argtypes = [_I, _P, _P, _P, _P, _I, _P, _I, _P, _D, _D, _D, _D, _D,
+                                      _D, _P, _P, _P, _P, _P, _I]
+    lib.pmref_vacuum_eval.restype = _I
+    ar = _Arrays(sysd)
+    p = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1)
+    f = np.zeros(p.size)
+    e = np.zeros(2)
+    v = np.zeros(9)
+    mv = np.zeros(9)
+    lib.pmref_vacuum_eval(ar.n, _ptr(ar.type), _ptr(ar.q), _ptr(ar.mol), _ptr(ar.mass), ar.ntypes,
+                          _ptr(ar.lj), ar.nexcl, _ptr(ar.excl),
+                          float(sysd.get("coulomb_scaling", 1.0)), float(sysd["cellsize"]),
+                          float(sysd["ron"]), float(sysd["rc_lj"]), float(sysd["rc_coul"]),
+                          float(sysd["rc_alg"]), _ptr(p), _ptr(f), _ptr(e), _ptr(v), _ptr(mv),
+                          int(virial_mode))
+    return f.reshape(-1, 3), e, v, mv
+
+
 def ref_load_psf(psf, par, pdb, exclude="scaled1-4"):
     """Reads a PSF/PAR/PDB triple with the reference's readers and topology
     builder; returns a dict of the arrays the nonbonded force consumes."""

@@ -47,7 +47,7 @@ EXPORTED = (
     "pmb200_batch_create", "pmb200_batch_destroy", "pmb200_batch_last_error",
     "pmb200_batch_eval_device", "pmb200_batch_set_schedule", "pmb200_batch_get_schedule",
     "pmb200_batch_autotune", "pmb200_batch_set_kernel_timing", "pmb200_batch_last_kernel_ms",
-    "pmb200_batch_pair_counts", "pmb200_create_pair",
+    "pmb200_batch_pair_counts", "pmb200_create_pair", "pmb200_set_vacuum_domain",
 )
 
 _P = ctypes.c_void_p
@@ -115,6 +115,7 @@ def lib():
     L.pmb200_param_grad_device.argtypes = [_P, _P, _P, _P, _P]
     L.pmb200_hvp_device.argtypes = [_P, _P, _P, _P, _P, _P, _P]
     L.pmb200_update_params.argtypes = [_P, _P, _P]
+    L.pmb200_set_vacuum_domain.argtypes = [_P, _P, _P]
     L.pmb200_create_pair.argtypes = [ctypes.POINTER(PairParams), ctypes.POINTER(_P)]
     L.pmb200_batch_create.argtypes = [ctypes.POINTER(_P), _I, ctypes.POINTER(_P)]
     L.pmb200_batch_destroy.argtypes = [_P]

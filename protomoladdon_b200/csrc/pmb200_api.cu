@@ -12,6 +12,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <limits>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -35,6 +36,8 @@ struct pmb200_ctx {
   // potential (LJ, Coulomb)
   int sw_kind[2] = {0, 0};
   double sw_par[2][4] = {};
+  // vacuum boundaries: the box is only the cell domain (no wrap, no images)
+  bool vacuum = false, vacuum_pending = false;
   // the box as last given (re-applied when an Ewald default alpha changes)
   bool box_given = false;
   double box_e[3][3] = {}, box_origin[3] = {};
@@ -537,6 +540,22 @@ int pmb200_create_pair(const pmb200_pair_params *params, pmb200_ctx **out) {
   return PMB200_OK;
 }
 
+int pmb200_set_vacuum_domain(pmb200_ctx *c, const double lo[3], const double hi[3]) {
+  if (!c) return PMB200_EINVAL;
+  if (!lo || !hi) return fail(c, PMB200_EINVAL, "null domain corner");
+  if (c->form == FORM_EWALD_POLY5 || c->form == FORM_EWALD_EXACT)
+    return fail(c, PMB200_EUNSUPPORTED, "the Ewald term needs periodic boundaries");
+  double e1[3] = {hi[0] - lo[0], 0, 0}, e2[3] = {0, hi[1] - lo[1], 0},
+         e3[3] = {0, 0, hi[2] - lo[2]}, org[3];
+  for (int a = 0; a < 3; a++) {
+    if (!(hi[a] > lo[a]) || !std::isfinite(lo[a]) || !std::isfinite(hi[a]))
+      return fail(c, PMB200_EINVAL, "domain axis %d: [%g, %g]", a, lo[a], hi[a]);
+    org[a] = 0.5 * (lo[a] + hi[a]);
+  }
+  c->vacuum_pending = true;
+  return pmb200_set_box(c, e1, e2, e3, org);
+}
+
 int pmb200_ewald_info(const pmb200_ctx *c, double *alpha, double *rc) {
   if (!c || !alpha || !rc) return PMB200_EINVAL;
   if (c->form == FORM_CUTOFF || !c->have_box || !c->have_topo) return PMB200_ESTATE;
@@ -671,7 +690,11 @@ int pmb200_set_topology(pmb200_ctx *c, int n, const int *type, const double *q_s
 int pmb200_set_box(pmb200_ctx *c, const double e1[3], const double e2[3], const double e3[3],
                    const double origin[3]) {
   if (!c) return PMB200_EINVAL;
+  // a box is periodic unless it comes from pmb200_set_vacuum_domain
+  const bool vacuum = c->vacuum_pending;
+  c->vacuum_pending = false;
   if (!e1 || !e2 || !e3 || !origin) return fail(c, PMB200_EINVAL, "null box vector");
+  c->vacuum = vacuum;
   if (e1[1] != 0.0 || e1[2] != 0.0 || e2[0] != 0.0 || e2[2] != 0.0 || e3[0] != 0.0 ||
       e3[1] != 0.0)
     return fail(c, PMB200_EUNSUPPORTED, "only orthogonal periodic boxes are supported");
@@ -695,7 +718,7 @@ int pmb200_set_box(pmb200_ctx *c, const double e1[3], const double e2[3], const 
   }
   const double rc = ctx_rc(c);
   for (int a = 0; a < 3; a++) {
-    if (L[a] < 2.0 * rc)
+    if (L[a] < 2.0 * rc && !c->vacuum)
       return fail(c, PMB200_EUNSUPPORTED,
                   "box edge %g is below twice the cutoff %g (minimum image would need more "
                   "than one image per pair)", L[a], rc);
@@ -712,6 +735,7 @@ int pmb200_set_box(pmb200_ctx *c, const double e1[3], const double e2[3], const 
     g.boxmin[a] = origin[a] - 0.5 * L[a];
   }
   g.nx = nd[0]; g.ny = nd[1]; g.nz = nd[2];
+  g.periodic = c->vacuum ? 0 : 1;
   const long long ncell = (long long)nd[0] * nd[1] * nd[2];
   if (ncell > (1 << 24)) return fail(c, PMB200_EUNSUPPORTED, "%lld cells", ncell);
   g.ncell = (int)ncell;
@@ -825,6 +849,7 @@ int pmb200_set_box(pmb200_ctx *c, const double e1[3], const double e2[3], const 
   b.er[2] = (L[0] * L[1]) / (L[2] * (L[0] * L[1]));
   b.d = std::min((L[0] * 0.5) * (L[0] * 0.5),
                  std::min((L[1] * 0.5) * (L[1] * 0.5), (L[2] * 0.5) * (L[2] * 0.5)));
+  if (c->vacuum) b.d = std::numeric_limits<double>::infinity();  // no images
   c->have_box = true;
   if (c->have_topo) return upload_lj(c);
   return PMB200_OK;
@@ -1376,6 +1401,7 @@ extern "C" int pmb200_eval_noalloc(const pmb200_params *p, int n, const double *
   const long long ncell = (long long)nd[0] * nd[1] * nd[2];
   if (ncell > kNoAllocCells) return PMB200_ENOMEM;  // beyond the fixed scratch
   GridParams g{};
+  g.periodic = 1;
   g.nx = nd[0]; g.ny = nd[1]; g.nz = nd[2];
   g.ncell = (int)ncell;
   for (int a = 0; a < 3; a++) {

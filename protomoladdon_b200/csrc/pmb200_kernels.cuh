@@ -50,6 +50,7 @@ struct GridParams {
   double boxlen[3];  // box edges
   double unit;       // cell-unit length scale (= edge[0])
   int nrows;
+  int periodic;      // 1: periodic box (wrap, minimum image); 0: vacuum domain
 };
 
 // PeriodicBoundaryConditions constants for minimalDifference
@@ -193,7 +194,10 @@ __device__ __forceinline__ bool locate_cell(const double *xin, const GridParams 
     double x = xin[a];
     if (!isfinite(x)) { ok = false; x = g.boxmin[a]; }
     double w = x - g.boxmin[a];
-    w -= g.boxlen[a] * floor(w / g.boxlen[a]);
+    if (g.periodic) w -= g.boxlen[a] * floor(w / g.boxlen[a]);
+    // vacuum: atoms outside the domain are clamped into its boundary cells;
+    // r keeps their true offset, so no pair is lost (the cell-index map
+    // stays 1-Lipschitz)
     int ca = (int)floor(w / g.edge[a]);
     ca = ca < 0 ? 0 : (ca >= nd[a] ? nd[a] - 1 : ca);
     c[a] = ca;
@@ -649,12 +653,20 @@ __device__ __forceinline__ void mixed_task(
         const int dx = (int)(o & 31u) - 8, dy = (int)((o >> 5) & 31u) - 8,
                   dz = (int)((o >> 10) & 31u) - 8;
         chome = (dx | dy | dz) == 0;
-        int jx = (cx + dx) % g.nx; jx += (jx < 0) ? g.nx : 0;
-        int jy = (cy + dy) % g.ny; jy += (jy < 0) ? g.ny : 0;
-        int jz = (cz + dz) % g.nz; jz += (jz < 0) ? g.nz : 0;
-        const int jc = (jz * g.ny + jy) * g.nx + jx;
-        cjs = start[jc];
-        ccnt = start[jc + 1] - cjs;
+        int jx = cx + dx, jy = cy + dy, jz = cz + dz;
+        bool inside = true;
+        if (g.periodic) {
+          jx %= g.nx; jx += (jx < 0) ? g.nx : 0;
+          jy %= g.ny; jy += (jy < 0) ? g.ny : 0;
+          jz %= g.nz; jz += (jz < 0) ? g.nz : 0;
+        } else {
+          inside = jx >= 0 && jx < g.nx && jy >= 0 && jy < g.ny && jz >= 0 && jz < g.nz;
+        }
+        if (inside) {
+          const int jc = (jz * g.ny + jy) * g.nx + jx;
+          cjs = start[jc];
+          ccnt = start[jc + 1] - cjs;
+        }
         csx = (float)dx; csy = (float)dy * mc.ey; csz = (float)dz * mc.ez;
       }
       int incl = ccnt;  // inclusive prefix of the cells' atom counts
@@ -843,6 +855,7 @@ k_pair_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes, const dou
     for (int r = 0; r < g.nrows; r++) {
       const Row row = st.rows[r];
       int jy = cy + row.dy, jz = cz + row.dz;
+      if (!g.periodic && (jy < 0 || jy >= g.ny || jz < 0 || jz >= g.nz)) continue;
       while (jy < 0) jy += g.ny;
       while (jy >= g.ny) jy -= g.ny;
       while (jz < 0) jz += g.nz;
@@ -851,6 +864,7 @@ k_pair_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes, const dou
       const double sy = row.dy * g.edge[1], sz = row.dz * g.edge[2];
       for (int dx = row.dxlo; dx <= row.dxhi; dx++) {
         int jx = cx + dx;
+        if (!g.periodic && (jx < 0 || jx >= g.nx)) continue;
         jx %= g.nx;
         jx += (jx < 0) ? g.nx : 0;
         const int jc = rowbase + jx;
@@ -1058,6 +1072,7 @@ k_deriv_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes,
       for (int r = 0; r < g.nrows; r++) {
         const Row row = st.rows[r];
         int jy = cy + row.dy, jz = cz + row.dz;
+        if (!g.periodic && (jy < 0 || jy >= g.ny || jz < 0 || jz >= g.nz)) continue;
         while (jy < 0) jy += g.ny;
         while (jy >= g.ny) jy -= g.ny;
         while (jz < 0) jz += g.nz;
@@ -1066,6 +1081,7 @@ k_deriv_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes,
         const double sy = row.dy * g.edge[1], sz = row.dz * g.edge[2];
         for (int dx = row.dxlo; dx <= row.dxhi; dx++) {
           int jx = cx + dx;
+          if (!g.periodic && (jx < 0 || jx >= g.nx)) continue;
           jx %= g.nx;
           jx += (jx < 0) ? g.nx : 0;
           const int jc = rowbase + jx;

@@ -90,6 +90,8 @@ class PeriodicTopology:
         self.coulomb_scaling = float(coulomb_scaling)
         self.cellsize = float(cellsize)
         self.version = 0
+        # vacuum boundaries: (lo[3], hi[3]) of the cell domain; None = periodic
+        self.domain = None
 
     @property
     def n(self):
@@ -181,11 +183,17 @@ class NonbondedCutoffB200SystemForce:
                 _ptr(ex) if ex.size else None, topo.coulomb_scaling))
             self._topo_key = key
             self._box_key = None
-        bkey = (topo.e.tobytes(), topo.origin.tobytes())
+        dom = None if topo.domain is None else tuple(
+            np.ascontiguousarray(x, dtype=np.float64) for x in topo.domain)
+        bkey = (topo.e.tobytes(), topo.origin.tobytes(),
+                None if dom is None else (dom[0].tobytes(), dom[1].tobytes()))
         if self._box_key != bkey:
-            e1, e2, e3 = (np.ascontiguousarray(topo.e[k]) for k in range(3))
-            self._check(L.pmb200_set_box(self._ctx, _ptr(e1), _ptr(e2), _ptr(e3),
-                                         _ptr(topo.origin)))
+            if dom is not None:
+                self._check(L.pmb200_set_vacuum_domain(self._ctx, _ptr(dom[0]), _ptr(dom[1])))
+            else:
+                e1, e2, e3 = (np.ascontiguousarray(topo.e[k]) for k in range(3))
+                self._check(L.pmb200_set_box(self._ctx, _ptr(e1), _ptr(e2), _ptr(e3),
+                                             _ptr(topo.origin)))
             self._box_key = bkey
 
     def _create(self, topo):

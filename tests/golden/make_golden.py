@@ -33,6 +33,11 @@ Fixtures (all inputs and outputs FP64):
   box: per case ``<case>_{forces,energies,virial,molvirial}`` and the switch
   specs ``<case>_lj`` / ``<case>_coul`` ({kind code, switchon, cutoff,
   order, switchoff}, kind 0 = absent).  ``--pairs-only`` writes just this.
+* vacuum_ref.npz -- the reference's vacuum cutoff force (OneAtomPairTwo<
+  VacuumBoundaryConditions, C2, LJ, C1, Coulomb>) on a water droplet (the
+  whole molecules of the 648-atom box within 8.5 A of its centre, unwrapped
+  around it), rc 8 / C2 from 7: forces, energies, virials.
+  ``--vacuum-only`` writes just this.
 """
 from __future__ import annotations
 
@@ -156,11 +161,55 @@ def pair_fixtures():
     print("wrote switch-policy fixtures to", HERE)
 
 
+def droplet():
+    """Whole waters of the 648-atom box within 8.5 A of its centre, as a
+    non-periodic cluster (positions unwrapped around the centre)."""
+    w = water.small_648()
+    box = np.asarray(w["box"], float)
+    c = np.zeros(3)
+    pos = w["pos"] - c
+    pos -= box * np.rint(pos / box)
+    mol = w["mol"]
+    nmol = mol.max() + 1
+    keep_mol = np.zeros(nmol, bool)
+    for m in range(nmol):
+        at = np.nonzero(mol == m)[0]
+        com = pos[at[0]]  # the oxygen
+        # whole molecule on the same side as its oxygen
+        pos[at] = com + (pos[at] - com) - box * np.rint((pos[at] - com) / box)
+        keep_mol[m] = np.linalg.norm(com) <= 8.5
+    keep = keep_mol[mol]
+    idx = np.nonzero(keep)[0]
+    remap = -np.ones(len(mol), int)
+    remap[idx] = np.arange(len(idx))
+    mol_new = np.unique(mol[idx], return_inverse=True)[1]
+    ex = np.asarray(w["excl"]).reshape(-1, 3)
+    ex = ex[keep[ex[:, 0]] & keep[ex[:, 1]]].copy()
+    ex[:, 0] = remap[ex[:, 0]]
+    ex[:, 1] = remap[ex[:, 1]]
+    d = dict(w)
+    d.update(pos=pos[idx], type=w["type"][idx], qscaled=w["qscaled"][idx], mol=mol_new,
+             mass=w["mass"][idx], excl=ex, n=len(idx), ron=7.0, rc_lj=8.0, rc_coul=8.0,
+             rc_alg=8.0, cellsize=4.0)
+    return d
+
+
+def vacuum_fixture():
+    d = droplet()
+    f, e, v, mv = O.ref_vacuum_eval(d, d["pos"], 2)
+    np.savez_compressed(os.path.join(HERE, "vacuum_ref.npz"), **sysd_arrays(d),
+                        ref_forces=f, ref_energies=e, ref_virial=v, ref_molvirial=mv)
+    print("wrote the vacuum fixture to", HERE)
+
+
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
-    if "--ewald-only" not in sys.argv and "--pairs-only" not in sys.argv:
+    only = [a for a in sys.argv[1:] if a.endswith("-only")]
+    if not only:
         main(args[0] if args else "/root/reference")
-    if "--pairs-only" not in sys.argv:
+    if not only or "--ewald-only" in only:
         ewald_fixtures()
-    if "--ewald-only" not in sys.argv:
+    if not only or "--pairs-only" in only:
         pair_fixtures()
+    if not only or "--vacuum-only" in only:
+        vacuum_fixture()
