@@ -2,6 +2,7 @@
 #include "B200ForceModule.h"
 #include "B200CutoffSystemForce.h"
 #include "B200EwaldRealSystemForce.h"
+#include "B200PairSystemForce.h"
 
 #include <protomol/ProtoMolApp.h>
 #include <protomol/factory/ForceFactory.h>
@@ -18,12 +19,34 @@ void ProtoMol::registerB200EwaldRealForce(ForceFactory &factory) {
   factory.reg(new B200EwaldRealSystemForce());
 }
 
+// The switch combinations NonbondedCutoffForceModule registers for the
+// plain LJ / Coulomb potentials (NonbondedCutoffForceModule.cpp:55-82 and
+// 98-125), CmpCnCn aside; the periodic (C2, C1) pair has its own class.
+template <class TBC>
+static void registerPairs(ForceFactory &f, bool withC2C1) {
+  const int C1 = PMB200_SW_C1, C2 = PMB200_SW_C2, CN = PMB200_SW_CN, NO = PMB200_SW_NONE;
+  const int combos[][2] = {{NO, C1}, {NO, C2}, {NO, CN}, {C1, NO}, {C2, NO}, {CN, NO},
+                           {C2, C2}, {C2, CN}, {CN, CN}, {C2, C1}};
+  const int count = withC2C1 ? 10 : 9;
+  for (int k = 0; k < count; k++)
+    f.reg(new B200PairSystemForce<TBC>(combos[k][0], combos[k][1]));
+}
+
+void ProtoMol::registerB200PairForces(ForceFactory &factory, bool vacuum) {
+  if (vacuum) registerPairs<VacuumBoundaryConditions>(factory, true);
+  else registerPairs<PeriodicBoundaryConditions>(factory, false);
+}
+
 void B200ForceModule::registerForces(ProtoMolApp *app) {
-  // periodic boundaries only, like the CPU prototypes they stand beside
-  // (NonbondedCutoffForceModule.cpp:54, NonbondedFullElectrostaticForceModule.cpp:31)
+  // the same split by boundary conditions as the CPU prototypes they stand
+  // beside (NonbondedCutoffForceModule.cpp:53, 96;
+  // NonbondedFullElectrostaticForceModule.cpp:31)
   const std::string bc = app->config[InputBoundaryConditions::keyword];
   if (equalNocase(bc, PeriodicBoundaryConditions::keyword)) {
     registerB200CutoffForce(app->forceFactory);
     registerB200EwaldRealForce(app->forceFactory);
+    registerB200PairForces(app->forceFactory, false);
+  } else if (equalNocase(bc, VacuumBoundaryConditions::keyword)) {
+    registerB200PairForces(app->forceFactory, true);
   }
 }

@@ -25,6 +25,8 @@ public:
 // for a periodic configuration); for hosts that build their own factory.
 void registerB200CutoffForce(ForceFactory &factory);
 void registerB200EwaldRealForce(ForceFactory &factory);
+// The other switch combinations (B200PairSystemForce), periodic or vacuum.
+void registerB200PairForces(ForceFactory &factory, bool vacuum);
 }  // namespace ProtoMol
 
 #endif

@@ -19,9 +19,11 @@
 
 namespace ProtoMol {
 
-// Returns the first non-zero libpmb200 status, or PMB200_OK.
-inline int b200UploadTopology(pmb200_ctx *ctx,
-                              const Topology<PeriodicBoundaryConditions, CubicCellManager> &t) {
+// The atoms, LJ table, exclusions and coulombScalingFactor of any topology
+// with the cubic cell manager.  Returns the first non-zero libpmb200 status,
+// or PMB200_OK.
+template <class TBC>
+int b200UploadAtoms(pmb200_ctx *ctx, const Topology<TBC, CubicCellManager> &t) {
   const int n = (int)t.atoms.size();
   const int nt = t.lennardJonesParameters.size();
   std::vector<int> type(n > 0 ? n : 1), mol(n > 0 ? n : 1);
@@ -45,8 +47,14 @@ inline int b200UploadTopology(pmb200_ctx *ctx,
     ex[3 * k + 1] = table[k].a2;
     ex[3 * k + 2] = (int)table[k].excl;
   }
-  int rc = pmb200_set_topology(ctx, n, &type[0], &q[0], &mol[0], &mass[0], nt > 0 ? nt : 1,
-                               &lj[0], (int)table.size(), &ex[0], t.coulombScalingFactor);
+  return pmb200_set_topology(ctx, n, &type[0], &q[0], &mol[0], &mass[0], nt > 0 ? nt : 1,
+                             &lj[0], (int)table.size(), &ex[0], t.coulombScalingFactor);
+}
+
+// The same and the periodic box.
+inline int b200UploadTopology(pmb200_ctx *ctx,
+                              const Topology<PeriodicBoundaryConditions, CubicCellManager> &t) {
+  int rc = b200UploadAtoms(ctx, t);
   if (rc) return rc;
   const PeriodicBoundaryConditions &bc = t.boundaryConditions;
   return pmb200_set_box(ctx, bc.e1().c, bc.e2().c, bc.e3().c, bc.origin().c);

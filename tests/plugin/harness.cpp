@@ -4,6 +4,7 @@
 // compiled under oracle/_ref; used only by tests/test_plugin_gpu.py.
 #include "B200CutoffSystemForce.h"
 #include "B200EwaldRealSystemForce.h"
+#include "B200PairSystemForce.h"
 #include "B200ForceModule.h"
 
 #include <protomol/factory/ForceFactory.h>
@@ -16,6 +17,10 @@
 #include <protomol/switch/C1SwitchingFunction.h>
 #include <protomol/switch/C2SwitchingFunction.h>
 #include <protomol/topology/CellListEnumeratorPeriodicBoundaries.h>
+#include <protomol/topology/CellListEnumeratorStandard.h>
+#include <protomol/topology/VacuumBoundaryConditions.h>
+#include <protomol/switch/CnSwitchingFunction.h>
+#include <protomol/force/OneAtomPair.h>
 #include <protomol/topology/TopologyUtilities.h>
 #include <protomol/config/Value.h>
 
@@ -130,6 +135,81 @@ extern "C" int harness_ewald_eval(void *ref_handle, int which, int n, const doub
     eval_force(force, t, pos, n, forces, energies, virial, molvirial);
     delete force;
     return 0;
+  } catch (const std::exception &e) {
+    std::strncpy(g_msg, e.what(), sizeof(g_msg) - 1);
+  } catch (...) {
+    std::strncpy(g_msg, "unknown exception", sizeof(g_msg) - 1);
+  }
+  return 1;
+}
+
+// The other switch combinations through the factory: the id (e.g.
+// "LennardJones Coulomb -switchingFunction C2 -switchingFunction Cn
+// -algorithm NonbondedCutoffB200") and its parameter values in order.
+// vacuum = 0: on the periodic topology of ref_handle; 1: on a vacuum
+// topology built here from that topology's atoms and tables.
+template <class TBC>
+static int pair_eval_on(Topology<TBC, CubicCellManager> *t, bool vacuum, const char *id,
+                        int nvalues, const double *values, const double *pos, int n,
+                        double *forces, double *energies, double *virial, double *molvirial) {
+  ForceFactory factory;
+  registerB200PairForces(factory, vacuum);
+  std::vector<Value> v;
+  for (int k = 0; k < nvalues; k++) v.push_back(Value(values[k]));
+  Force *force = factory.make(id, v);
+  if (!force) {
+    std::strncpy(g_msg, (std::string("factory could not make '") + id + "'").c_str(),
+                 sizeof(g_msg) - 1);
+    return 1;
+  }
+  std::strncpy(g_msg, force->getId().c_str(), sizeof(g_msg) - 1);
+  Vector3DBlock p(n), fr(n);
+  std::memcpy(p.c, pos, sizeof(double) * 3 * n);
+  fr.zero();
+  ScalarStructure en;
+  en.clear();
+  en.virial(true);
+  en.molecularVirial(true);
+  buildMolecularCenterOfMass(&p, t);
+  dynamic_cast<SystemForce *>(force)->evaluate(t, &p, &fr, &en);
+  std::memcpy(forces, fr.c, sizeof(double) * 3 * n);
+  energies[0] = en[ScalarStructure::COULOMB];
+  energies[1] = en[ScalarStructure::LENNARDJONES];
+  for (int k = 0; k < 9; k++) {
+    virial[k] = en[(ScalarStructure::Index)(ScalarStructure::VIRIALXX + k)];
+    molvirial[k] = en[(ScalarStructure::Index)(ScalarStructure::MOLVIRIALXX + k)];
+  }
+  delete force;
+  return 0;
+}
+
+extern "C" int harness_pair_eval(void *ref_handle, int vacuum, const char *id, int nvalues,
+                                 const double *values, int n, const double *pos, double *forces,
+                                 double *energies, double *virial, double *molvirial) {
+  g_msg[0] = 0;
+  try {
+    PTopo *t = (PTopo *)pmref_topology(ref_handle);
+    if (!vacuum)
+      return pair_eval_on(t, false, id, nvalues, values, pos, n, forces, energies, virial,
+                          molvirial);
+    typedef Topology<VacuumBoundaryConditions, CubicCellManager> VTopo;
+    VTopo v(t->coulombScalingFactor, ExclusionType(ExclusionType::ONE2),
+            VacuumBoundaryConditions(), CubicCellManager(4.0), 16.0f);
+    // element-wise copies: the LJ and exclusion tables own raw arrays
+    v.atoms = t->atoms;
+    v.atomTypes = t->atomTypes;
+    v.molecules = t->molecules;
+    const int nt = (int)t->lennardJonesParameters.size();
+    v.lennardJonesParameters.resize(nt);
+    for (int a = 0; a < nt; a++)
+      for (int b = 0; b < nt; b++)
+        v.lennardJonesParameters.set(a, b, t->lennardJonesParameters(a, b));
+    v.exclusions.resize(n);
+    const std::vector<ExclusionPair> &tab = t->exclusions.getTable();
+    for (size_t k = 0; k < tab.size(); k++) v.exclusions.add(tab[k].a1, tab[k].a2, tab[k].excl);
+    v.exclusions.optimize();
+    return pair_eval_on(&v, true, id, nvalues, values, pos, n, forces, energies, virial,
+                        molvirial);
   } catch (const std::exception &e) {
     std::strncpy(g_msg, e.what(), sizeof(g_msg) - 1);
   } catch (...) {

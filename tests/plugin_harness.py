@@ -56,3 +56,24 @@ def evaluate_ewald(ref_force, which, sysd, pos, alpha, accuracy):
                               float(accuracy), f.ctypes.data, e.ctypes.data, v.ctypes.data,
                               mv.ctypes.data)
     return rc, L.harness_message().decode(), f, e, v, mv
+
+
+def evaluate_pair(ref_force, vacuum, force_id, values, pos):
+    """A switch-policy force made by the factory from its config id and
+    values: on the reference topology of ref_force (vacuum 0) or on a vacuum
+    copy of it (1).  Returns (rc, message, forces, energies, virial,
+    molvirial)."""
+    L = lib()
+    L.harness_pair_eval.argtypes = [_P, _I, ctypes.c_char_p, _I, _P, _I, _P, _P, _P, _P, _P]
+    L.harness_pair_eval.restype = _I
+    p = np.ascontiguousarray(pos, dtype=np.float64)
+    n = p.shape[0]
+    vals = np.ascontiguousarray(values, dtype=np.float64)
+    f = np.zeros((n, 3))
+    e = np.zeros(2)
+    v = np.zeros(9)
+    mv = np.zeros(9)
+    rc = L.harness_pair_eval(ref_force.h, int(vacuum), force_id.encode(), vals.size,
+                             vals.ctypes.data, n, p.ctypes.data, f.ctypes.data, e.ctypes.data,
+                             v.ctypes.data, mv.ctypes.data)
+    return rc, L.harness_message().decode(), f, e, v, mv

@@ -105,3 +105,61 @@ def test_plugin_ewald_matches_reference_through_factory():
     assert abs(e[0] - float(d["poly5_energy"])) <= 0.065 and e[1] == 0.0
     vr = d["poly5_virial"]
     assert np.abs(v - vr).max() <= 1e-5 * np.abs(vr).max()
+
+
+# ---- the other switch combinations and vacuum boundaries -------------------
+def _pair_case(name):
+    """(force id, values) of a switch-policy fixture case, as a config gives them."""
+    from .conftest import load_fixture
+    d = load_fixture("pairs_ref.npz")
+    names = {1: "C1", 2: "C2", 3: "Cn"}
+    pots, sws, vals = [], [], []
+    for pot, key in (("LennardJones", f"{name}_lj"), ("Coulomb", f"{name}_coul")):
+        a = d[key]
+        if a[0] == 0:
+            continue
+        kind = names[int(a[0])]
+        pots.append(pot)
+        sws.append(kind)
+        ron, rc, order, roff = (float(x) for x in a[1:])
+        vals += {"C1": [rc], "C2": [ron, rc], "Cn": [order, ron, roff, rc]}[kind]
+    vals.append(8.0)  # algorithm cutoff
+    fid = " ".join(pots) + "".join(f" -switchingFunction {k}" for k in sws) + \
+        " -algorithm NonbondedCutoffB200"
+    return d, fid, vals
+
+
+def test_factory_resolves_switch_policy_ids():
+    for case in ("c2_cn", "lj_c1", "coul_cn"):
+        d, fid, vals = _pair_case(case)
+        R = O.RefForce(d)
+        rc, msg, *_ = H.evaluate_pair(R, 0, fid, vals, d["pos"])
+        R.close()
+        assert (rc == 0 and fid in msg) or "B200 cutoff force" in msg, (case, msg)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["c2_c2", "c2_cn", "cn_cn", "lj_c1", "coul_c2"])
+def test_switch_policy_plugin_matches_reference(case):
+    d, fid, vals = _pair_case(case)
+    R = O.RefForce(d)
+    rc, msg, f, e, v, mv = H.evaluate_pair(R, 0, fid, vals, d["pos"])
+    R.close()
+    assert rc == 0, msg
+    fr = d[f"{case}_forces"]
+    assert np.sqrt(((f - fr) ** 2).sum() / (fr ** 2).sum()) <= 1e-5
+
+
+@pytest.mark.gpu
+def test_vacuum_plugin_matches_reference():
+    from .conftest import load_fixture
+    d = load_fixture("vacuum_ref.npz")
+    R = O.RefForce(d)
+    fid = ("LennardJones Coulomb -switchingFunction C2 -switchingFunction C1 "
+           "-algorithm NonbondedCutoffB200")
+    rc, msg, f, e, v, mv = H.evaluate_pair(R, 1, fid, [7.0, 8.0, 8.0, 8.0], d["pos"])
+    R.close()
+    assert rc == 0, msg
+    fr = d["ref_forces"]
+    assert np.sqrt(((f - fr) ** 2).sum() / (fr ** 2).sum()) <= 1e-5
+    assert np.abs(e - d["ref_energies"]).max() <= 2e-3
