@@ -1550,6 +1550,7 @@ struct pmb200_batch {
   // schedule: stencil parts per cell, task order (0 as built, 1 by cost,
   // largest first), persistent blocks per SM
   int parts = 1, order = 1, bpsm = 0, max_bpsm = 1, nsm = 1;
+  int occ[4] = {1, 1, 1, 1};  // resident blocks per SM per variant (energy | virial << 1)
   // graph of one evaluation (pmb200_batch_eval_device with a stream)
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
@@ -1659,7 +1660,9 @@ int batch_launch_eval(pmb200_batch *b, const double *d_pos, double *d_forces, do
   if (N > 0)
     BCK(cudaMemsetAsync(b->d_facc, 0, sizeof(unsigned long long) * 3 * (size_t)N, st));
   BCK(cudaMemsetAsync(b->d_counter, 0, sizeof(int), st));
-  const int bpsm = b->bpsm > 0 ? std::min(b->bpsm, b->max_bpsm) : b->max_bpsm;
+  // resident blocks per SM of the variant launched (registers differ)
+  const int fit = b->occ[(energy ? 1 : 0) | (virial ? 2 : 0)];
+  const int bpsm = b->bpsm > 0 ? std::min(b->bpsm, fit) : fit;
   const int grid = std::max(1, std::min(b->ntasks, bpsm * b->nsm));
   if (timed) BCK(cudaEventRecord(b->ev0, st));
   if (b->form == FORM_GENERIC) batch_launch_pair<FORM_GENERIC>(b, energy, virial, grid, st);
@@ -1826,13 +1829,38 @@ int pmb200_batch_create(pmb200_ctx *const *systems, int nsys, pmb200_batch **out
   cuda(cudaMemset(b->d_err, 0, sizeof(int)));
   if (rc) return done(rc);
   // persistent grid: resident blocks per SM of the pair kernel
-  int dev_sm = 1, occ = 1;
+  int dev_sm = 1;
   cuda(cudaDeviceGetAttribute(&dev_sm, cudaDevAttrMultiProcessorCount, b->device));
-  cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      &occ, k_pair_mixed_batch<FORM_CUTOFF, true, true>, 32 * kWarps, 0));
+  auto fits = [&](auto kernel, int &out) {
+    int o = 1;
+    cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kernel, 32 * kWarps, 0));
+    out = std::max(1, o);
+  };
+  // per (energy, virial) variant of the batch's form
+  if (b->form == FORM_GENERIC) {
+    fits(k_pair_mixed_batch<FORM_GENERIC, false, false>, b->occ[0]);
+    fits(k_pair_mixed_batch<FORM_GENERIC, true, false>, b->occ[1]);
+    fits(k_pair_mixed_batch<FORM_GENERIC, false, true>, b->occ[2]);
+    fits(k_pair_mixed_batch<FORM_GENERIC, true, true>, b->occ[3]);
+  } else if (b->form == FORM_EWALD_POLY5) {
+    fits(k_pair_mixed_batch<FORM_EWALD_POLY5, false, false>, b->occ[0]);
+    fits(k_pair_mixed_batch<FORM_EWALD_POLY5, true, false>, b->occ[1]);
+    fits(k_pair_mixed_batch<FORM_EWALD_POLY5, false, true>, b->occ[2]);
+    fits(k_pair_mixed_batch<FORM_EWALD_POLY5, true, true>, b->occ[3]);
+  } else if (b->form == FORM_EWALD_EXACT) {
+    fits(k_pair_mixed_batch<FORM_EWALD_EXACT, false, false>, b->occ[0]);
+    fits(k_pair_mixed_batch<FORM_EWALD_EXACT, true, false>, b->occ[1]);
+    fits(k_pair_mixed_batch<FORM_EWALD_EXACT, false, true>, b->occ[2]);
+    fits(k_pair_mixed_batch<FORM_EWALD_EXACT, true, true>, b->occ[3]);
+  } else {
+    fits(k_pair_mixed_batch<FORM_CUTOFF, false, false>, b->occ[0]);
+    fits(k_pair_mixed_batch<FORM_CUTOFF, true, false>, b->occ[1]);
+    fits(k_pair_mixed_batch<FORM_CUTOFF, false, true>, b->occ[2]);
+    fits(k_pair_mixed_batch<FORM_CUTOFF, true, true>, b->occ[3]);
+  }
   if (rc) return done(rc);
   b->nsm = dev_sm;
-  b->max_bpsm = std::max(1, occ);
+  b->max_bpsm = std::max(std::max(b->occ[0], b->occ[1]), std::max(b->occ[2], b->occ[3]));
   return done(batch_build_tasks(b));
 }
 
@@ -1852,7 +1880,7 @@ int pmb200_batch_get_schedule(const pmb200_batch *b, int sched[4]) {
   if (!b || !sched) return PMB200_EINVAL;
   sched[0] = b->parts;
   sched[1] = b->order;
-  sched[2] = b->bpsm > 0 ? std::min(b->bpsm, b->max_bpsm) : b->max_bpsm;
+  sched[2] = b->bpsm > 0 ? std::min(b->bpsm, b->occ[0]) : b->occ[0];
   sched[3] = b->ntasks;
   return PMB200_OK;
 }
@@ -1923,7 +1951,7 @@ int pmb200_batch_autotune(pmb200_batch *b, const double *d_pos, void *stream, in
   BCK(cudaSetDevice(b->device));
   cudaStream_t st = (cudaStream_t)stream;
   const int parts_c[3] = {1, 2, 4};
-  const int bpsm_c[2] = {b->max_bpsm, std::max(1, b->max_bpsm / 2)};
+  const int bpsm_c[2] = {b->occ[0], std::max(1, b->occ[0] / 2)};
   float best = -1.0f;
   int bp = 1, bo = 1, bb = 0;
   for (int pi = 0; pi < 3; pi++)
