@@ -287,8 +287,10 @@ void launch_pair_mixed(pmb200_ctx *c, unsigned flags, cudaStream_t st) {
   const bool energy = (flags & PMB200_ENERGY) != 0;
   const bool virial = (flags & (PMB200_VIRIAL | PMB200_MOLVIRIAL)) != 0;
   const bool molvir = (flags & PMB200_MOLVIRIAL) != 0;
+  const size_t smem =
+      (F == FORM_CUTOFF || F == FORM_GENERIC) ? sizeof(float4) * c->ntypes * c->ntypes : 0;
 #define PMB_MIXED_LAUNCH(E, V, M)                                                          \
-  k_pair_mixed<F, E, V, M><<<g.ncell, 32 * kWarps, 0, st>>>(                                 \
+  k_pair_mixed<F, E, V, M><<<g.ncell, 32 * kWarps, smem, st>>>(                              \
       g, c->mc, c->half, c->ntypes, c->d_lj32, c->d_start, c->d_spos32, c->d_smeta,         \
       c->d_sidx, c->d_ex_start, c->d_ex, c->d_facc, c->n, c->d_err, c->d_partial, c->pb,    \
       c->d_com)
@@ -1491,11 +1493,11 @@ extern "C" int pmb200_eval_noalloc(const pmb200_params *p, int n, const double *
   k_rank_gather<<<(g.ncell + 3) / 4, 128, 0, st>>>(g.ncell, start, tmp, rel32, nullptr, d_type,
                                                     d_mol, sidx, spos32, nullptr, smeta);
   if (d_energy)
-    k_pair_mixed<FORM_CUTOFF, true, false, false><<<g.ncell, 32 * kWarps, 0, st>>>(
+    k_pair_mixed<FORM_CUTOFF, true, false, false><<<g.ncell, 32 * kWarps, sizeof(float4) * ntypes * ntypes, st>>>(
         g, mc, half, ntypes, dlj, start, spos32, smeta, sidx, d_ex_start, d_ex, facc, n, err,
         partial, pb, nullptr);
   else
-    k_pair_mixed<FORM_CUTOFF, false, false, false><<<g.ncell, 32 * kWarps, 0, st>>>(
+    k_pair_mixed<FORM_CUTOFF, false, false, false><<<g.ncell, 32 * kWarps, sizeof(float4) * ntypes * ntypes, st>>>(
         g, mc, half, ntypes, dlj, start, spos32, smeta, sidx, d_ex_start, d_ex, facc, n, err,
         partial, pb, nullptr);
   if (n > 0)

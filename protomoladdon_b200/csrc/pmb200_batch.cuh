@@ -65,7 +65,6 @@ k_pair_mixed_batch(const BatchSys *__restrict__ sys, const int4 *__restrict__ ta
                    double *__restrict__ partial) {
   __shared__ float4 s_lj[kMaxTypes * kMaxTypes];
   __shared__ MixedWarpSmem s_w[kWarps];
-  __shared__ long long s_f[kWarps][32][3];
   __shared__ double s_acc[kWarps][ACC_MV];
   __shared__ unsigned short s_st[kMaxHalfCells];
   __shared__ BatchSys s_sys;
@@ -97,7 +96,7 @@ k_pair_mixed_batch(const BatchSys *__restrict__ sys, const int4 *__restrict__ ta
     mixed_task<kForm, kEnergy, kVirial, false>(
         s_sys.g, s_sys.mc, s_st, s_sys.st_n, tk.z, tk.w, s_sys.ntypes, s_lj, tk.y,
         start + s_sys.cell0, spos, smeta, sidx, ex_start, ex, facc, N,
-        partial + (size_t)t * kNacc, s_sys.pb, nullptr, sm, s_f, s_acc);
+        partial + (size_t)t * kNacc, s_sys.pb, nullptr, s_w, s_acc);
     __syncthreads();  // s_task and the staged system are reused
   }
 }
