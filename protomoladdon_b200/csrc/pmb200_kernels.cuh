@@ -355,6 +355,7 @@ constexpr int kBatch = 128;
 constexpr float kJScale = 262144.0f; // shared j-force quanta (2^-18) per cell-unit force
 constexpr int kJShift = 14;          // to the global 2^-32 quanta
 constexpr float kJLimit = 6.7e7f;    // per-contribution bound: 32 contributions fit int32
+constexpr float kJToGlobal = 16384.0f;  // 2^-18 quanta -> the accumulator's 2^-32 quanta
 
 struct __align__(16) MixedWarpSmem {
   float4 pos[kBatch];                    // staged j atoms, shifted into the i-cell frame
@@ -374,18 +375,12 @@ struct KahanF {
   }
 };
 
-// Adds a j-force contribution (cell units) to j's per-batch int32 shared
-// accumulator in 2^-18 quanta.  A batch adds at most 32 contributions to one
-// j, so each must stay within kJLimit quanta (256 cell units); a larger one
-// (close contacts) goes straight to the global int64 accumulator at full
-// 2^-32 resolution instead.  Both sums are exact integer sums.
-__device__ __forceinline__ void jadd(int *sh, unsigned long long *g, float v) {
-  const float q = v * kJScale;
-  if (fabsf(q) <= kJLimit)
-    atomicAdd(sh, __float2int_rn(q));
-  else
-    atomicAdd(g, (unsigned long long)__float2ll_rn(v * 4294967296.0f));
-}
+// j forces: each contribution, in 2^-18 quanta of cell-unit force, goes to
+// j's per-batch int32 shared accumulator.  A batch adds at most 32
+// contributions to one j, so each must stay within kJLimit quanta (256 cell
+// units); a pair with a larger component (close contacts) adds all three
+// straight to the global int64 accumulator at 2^-32 resolution instead.
+// Both sums are exact integer sums.
 
 // One task of the mixed pair kernel for a whole block (kWarps warps): i-cell
 // `cell` and the stencil entries part * kWarps + warp + k * kWarps * nparts
@@ -573,7 +568,7 @@ __device__ __forceinline__ void mixed_task(
           const float dist = r2 * rinv;
           const float sv = 1.0f - dist * fmaf(-r2, mc.c05_3, mc.c15_1);
           const float sd = fmaf(dist, mc.c15_3, -mc.c15_1 * rinv);
-          fc = fmaf(ec * r2inv, sv, -ec * sd);
+          fc = ec * fmaf(r2inv, sv, -sd);
           if (kEnergy) {
             kU.add(qj * rinv);
             kQ.add(qj);
@@ -583,15 +578,25 @@ __device__ __forceinline__ void mixed_task(
         f = flj + fc;
         if (kEnergy) pE += elj;
         }
-        const float fxv = ddx * f, fyv = ddy * f, fzv = ddz * f;  // force on j
+        // force on j in 2^-18 quanta (power-of-two scale: exact); the i
+        // force, virial and molecular virial sums run in the same units
+        const float fq = f * kJScale;
+        const float fxv = ddx * fq, fyv = ddy * fq, fzv = ddz * fq;
         px -= fxv;
         py -= fyv;
         pz -= fzv;
-        {
+        // j force: int32 shared-memory quanta, or, for a contribution too
+        // large for 32 of them to fit, straight into the int64 accumulator
+        if (fmaxf(fabsf(fxv), fmaxf(fabsf(fyv), fabsf(fzv))) <= kJLimit) {
+          atomicAdd(&sm.jf[0][t], __float2int_rn(fxv));
+          atomicAdd(&sm.jf[1][t], __float2int_rn(fyv));
+          atomicAdd(&sm.jf[2][t], __float2int_rn(fzv));
+        } else {
           const size_t jg = (size_t)sm.gidx[t];
-          jadd(&sm.jf[0][t], &facc[jg], fxv);
-          jadd(&sm.jf[1][t], &facc[(size_t)n + jg], fyv);
-          jadd(&sm.jf[2][t], &facc[2 * (size_t)n + jg], fzv);
+          atomicAdd(&facc[jg], (unsigned long long)__float2ll_rn(fxv * kJToGlobal));
+          atomicAdd(&facc[(size_t)n + jg], (unsigned long long)__float2ll_rn(fyv * kJToGlobal));
+          atomicAdd(&facc[2 * (size_t)n + jg],
+                    (unsigned long long)__float2ll_rn(fzv * kJToGlobal));
         }
         if (kEnergy) pc++;
         if (kVirial) {
@@ -610,15 +615,18 @@ __device__ __forceinline__ void mixed_task(
           }
         }
       }
-      fx += __float2ll_rn(px * 4294967296.0f);
-      fy += __float2ll_rn(py * 4294967296.0f);
-      fz += __float2ll_rn(pz * 4294967296.0f);
+      fx += __float2ll_rn(px * kJToGlobal);
+      fy += __float2ll_rn(py * kJToGlobal);
+      fz += __float2ll_rn(pz * kJToGlobal);
       if (kEnergy) { accE += (double)pE; accP += (double)pc; }
+      constexpr double kInvJ = 1.0 / (double)kJScale;  // quanta -> cell-unit forces
       if (kVirial) {
-        w[0] += pw0; w[1] += pw1; w[2] += pw2; w[3] += pw3; w[4] += pw4; w[5] += pw5;
+        w[0] += pw0 * kInvJ; w[1] += pw1 * kInvJ; w[2] += pw2 * kInvJ;
+        w[3] += pw3 * kInvJ; w[4] += pw4 * kInvJ; w[5] += pw5 * kInvJ;
       }
       if (kMolVir) {
-        mw[0] += pm0; mw[1] += pm1; mw[2] += pm2; mw[3] += pm3; mw[4] += pm4; mw[5] += pm5;
+        mw[0] += pm0 * kInvJ; mw[1] += pm1 * kInvJ; mw[2] += pm2 * kInvJ;
+        mw[3] += pm3 * kInvJ; mw[4] += pm4 * kInvJ; mw[5] += pm5 * kInvJ;
       }
       __syncwarp();
       // flush the batch's j forces to the global accumulator and clear them
