@@ -13,7 +13,8 @@ DEPS = SOURCES + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(
     os.path.join(HERE, "..", "include", "pmb200.h")]
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
-              "-Xcompiler", "-fPIC", "-shared", "-cudart", "static"]
+              "-Xcompiler", "-fPIC", "-Xcompiler", "-fopenmp", "-shared", "-cudart", "static",
+              "-lgomp"]
 
 
 def nvcc():

@@ -1001,7 +1001,13 @@ int pmb200_eval(pmb200_ctx *c, const double *pos, double *forces, double *energi
   // positions through pinned staging; this evaluation's forces are computed
   // on the device (overwrite), read back, and added to the caller's array
   if (c->n > 0) {
-    std::memcpy(c->h_pin_pos, pos, bytes);
+    // staging copy on the host's cores (large systems), then one transfer
+    const long long chunks = (long long)((cnt + 8191) / 8192);
+#pragma omp parallel for schedule(static) if (chunks > 8)
+    for (long long b = 0; b < chunks; b++) {
+      const size_t lo = (size_t)b * 8192, m = std::min<size_t>(8192, cnt - lo);
+      std::memcpy(c->h_pin_pos + lo, pos + lo, sizeof(double) * m);
+    }
     CK(cudaMemcpyAsync(c->d_hpos, c->h_pin_pos, bytes, cudaMemcpyHostToDevice, st));
   }
   rc = launch_eval(c, c->d_hpos, c->d_hfrc, c->d_out, flags, 0, st);
@@ -1011,7 +1017,12 @@ int pmb200_eval(pmb200_ctx *c, const double *pos, double *forces, double *energi
     CK(cudaMemcpyAsync(c->h_pin_out, c->d_out, sizeof(double) * 20, cudaMemcpyDeviceToHost, st));
   rc = pmb200_sync(c);
   if (rc) return rc;
-  for (size_t k = 0; k < cnt; k++) forces[k] += c->h_pin_frc[k];
+  {
+    const double *src = c->h_pin_frc;
+    const long long m = (long long)cnt;
+#pragma omp parallel for schedule(static) if (m > 65536)
+    for (long long k = 0; k < m; k++) forces[k] += src[k];
+  }
   const double *out = c->h_pin_out;
   if (flags & PMB200_ENERGY) {
     energies[0] += out[0];
@@ -1252,13 +1263,24 @@ int pmb200_host_kick_drift(int n, double *pos, double *vel, const double *forces
     return PMB200_EINVAL;
   if (nwater < 0 || (nwater > 0 && !widx)) return PMB200_EINVAL;
   const double h = dt_fs * 0.02045482828087295;  // Constant::INV_TIMEFACTOR
-  std::vector<double> old;
-  if (nwater > 0) old.assign(pos, pos + 3 * (size_t)n);
-  for (int i = 0; i < n; i++)
+  for (int w = 0; w < 3 * nwater; w++)
+    if (widx[w] < 0 || widx[w] >= n) return PMB200_EINVAL;
+  // the host's cores share the atoms and the waters (independent per atom /
+  // per water); the pre-step positions live in a per-thread-reused buffer
+  static thread_local std::vector<double> old;
+  if (nwater > 0) old.resize(3 * (size_t)n);
+  const double kh = kick * h, inv_h = 1.0 / h;
+  double *op = nwater > 0 ? old.data() : nullptr;
+#pragma omp parallel for schedule(static) if (n > 4096)
+  for (int i = 0; i < n; i++) {
+    const double s = kh / mass[i];
     for (int k = 0; k < 3; k++) {
-      vel[3 * i + k] += forces[3 * i + k] * (kick * h) / mass[i];
-      pos[3 * i + k] += vel[3 * i + k] * h;
+      const size_t q = 3 * (size_t)i + k;
+      if (op) op[q] = pos[q];
+      vel[q] += forces[q] * s;
+      pos[q] += vel[q] * h;
     }
+  }
   if (nwater > 0) {
     SettleParams sp{};
     const double mo = mass[widx[0]], mh = mass[widx[1]];
@@ -1266,13 +1288,17 @@ int pmb200_host_kick_drift(int n, double *pos, double *vel, const double *forces
     sp.mo = mo; sp.mh = mh; sp.rc = rcv;
     sp.ra = 2.0 * mh * t / (mo + 2.0 * mh);
     sp.rb = t - sp.ra;
+#pragma omp parallel for schedule(static) if (nwater > 1024)
     for (int w = 0; w < nwater; w++) {
       const int a = widx[3 * w], b = widx[3 * w + 1], cc = widx[3 * w + 2];
-      if (a < 0 || b < 0 || cc < 0 || a >= n || b >= n || cc >= n) return PMB200_EINVAL;
-      host_settle(sp, &old[3 * a], &old[3 * b], &old[3 * cc], pos + 3 * a, pos + 3 * b,
-                  pos + 3 * cc);
-      for (int at : {a, b, cc})
-        for (int k = 0; k < 3; k++) vel[3 * at + k] = (pos[3 * at + k] - old[3 * at + k]) / h;
+      host_settle(sp, op + 3 * (size_t)a, op + 3 * (size_t)b, op + 3 * (size_t)cc,
+                  pos + 3 * (size_t)a, pos + 3 * (size_t)b, pos + 3 * (size_t)cc);
+      const int at3[3] = {a, b, cc};
+      for (int m = 0; m < 3; m++)
+        for (int k = 0; k < 3; k++) {
+          const size_t q = 3 * (size_t)at3[m] + k;
+          vel[q] = (pos[q] - op[q]) * inv_h;
+        }
     }
   }
   return PMB200_OK;
