@@ -304,9 +304,16 @@ def run_ours(args):
     # replacement): the host integrator does kick + drift + SETTLE, as
     # ProtoMol's leapfrog with a constraint modifier does, and calls the force
     from protomoladdon_b200 import rigid
-    xh = s["pos"].copy()
-    vh = s["vel"].copy()
-    F = np.zeros_like(xh)
+    # the integrator's arrays in page-locked host memory (the library then
+    # transfers positions without a staging copy)
+    def pinned_copy(a):
+        t = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
+        v = t.numpy()
+        v[...] = a
+        return t, v
+    _xt, xh = pinned_copy(s["pos"])
+    _vt, vh = pinned_copy(s["vel"])
+    _ft, F = pinned_copy(np.zeros_like(s["pos"]))
     E = ScalarStructure()
     fmix.evaluate(topo, xh, F, E)
     e2e_steps = min(args.steps, 100)

@@ -1001,14 +1001,23 @@ int pmb200_eval(pmb200_ctx *c, const double *pos, double *forces, double *energi
   // positions through pinned staging; this evaluation's forces are computed
   // on the device (overwrite), read back, and added to the caller's array
   if (c->n > 0) {
-    // staging copy on the host's cores (large systems), then one transfer
-    const long long chunks = (long long)((cnt + 8191) / 8192);
+    // page-locked caller arrays are transferred directly; pageable ones go
+    // through the pinned staging copy, made on the host's cores
+    cudaPointerAttributes attr{};
+    const bool pinned = cudaPointerGetAttributes(&attr, pos) == cudaSuccess &&
+                        attr.type == cudaMemoryTypeHost;
+    cudaGetLastError();  // a pageable pointer may leave an error behind
+    const double *src = pos;
+    if (!pinned) {
+      const long long chunks = (long long)((cnt + 8191) / 8192);
 #pragma omp parallel for schedule(static) if (chunks > 8)
-    for (long long b = 0; b < chunks; b++) {
-      const size_t lo = (size_t)b * 8192, m = std::min<size_t>(8192, cnt - lo);
-      std::memcpy(c->h_pin_pos + lo, pos + lo, sizeof(double) * m);
+      for (long long b = 0; b < chunks; b++) {
+        const size_t lo = (size_t)b * 8192, m = std::min<size_t>(8192, cnt - lo);
+        std::memcpy(c->h_pin_pos + lo, pos + lo, sizeof(double) * m);
+      }
+      src = c->h_pin_pos;
     }
-    CK(cudaMemcpyAsync(c->d_hpos, c->h_pin_pos, bytes, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(c->d_hpos, src, bytes, cudaMemcpyHostToDevice, st));
   }
   rc = launch_eval(c, c->d_hpos, c->d_hfrc, c->d_out, flags, 0, st);
   if (rc) return rc;

@@ -266,3 +266,23 @@ def test_step_device_matches_leapfrog_body(water648):
     f.close()
     assert np.abs(pos.cpu().numpy() - P).max() < 1e-10
     assert rms_rel(frc.cpu().numpy(), F) < 1e-11
+
+
+def test_pinned_host_positions_equal_pageable(water648):
+    """pmb200_eval transfers page-locked positions directly and pageable ones
+    through its staging copy: the same forces and energies either way."""
+    import torch
+    d = water648
+    topo = PeriodicTopology.from_dict(d)
+    f = NonbondedCutoffB200SystemForce(d["ron"], d["rc_lj"], d["rc_coul"], d["rc_alg"])
+    pinned = torch.empty(d["pos"].shape, dtype=torch.float64, pin_memory=True).numpy()
+    pinned[...] = d["pos"]
+    out = []
+    for pos in (np.ascontiguousarray(d["pos"]), pinned):
+        F = np.zeros_like(d["pos"])
+        E = ScalarStructure()
+        f.evaluate(topo, pos, F, E)
+        out.append((F, E[0], E[1]))
+    f.close()
+    assert np.array_equal(out[0][0], out[1][0])
+    assert out[0][1:] == out[1][1:]
