@@ -32,6 +32,10 @@ value is Gpairs/s of whole LJ+C1 evaluations.
 persistent, graph-captured batched launch with the autotuned schedule,
 against one launch sequence per system.
 
+--workload diff: the differentiable form -- Hessian-vector products by
+double backward, parameter gradients and a force-matching loss gradient on
+the 648- and 41,472-atom boxes.
+
 --impl reference: the reference CPU implementation alone, one independent
 replica per host core (the reference force is serial), bounded sample.
 
@@ -708,6 +712,100 @@ def run_batch(args):
     return 0
 
 
+DIFF_WORKLOAD = ("differentiable form on the 648- and 41,472-atom water boxes: 32 seeded unit "
+                 "Hessian-vector products by double backward, dE/dq and dE/dsigma, dE/depsilon "
+                 "per type, and the force-matching loss sum |F(theta) - F_target|^2 "
+                 "(targets from 5% seeded Gaussian parameter perturbations) with its gradient")
+DIFF_METRIC = "Hessian-vector products per second, 41k-atom water box (FP64 derivative kernel)"
+
+
+def run_diff(args):
+    """The differentiable form, timed with CUDA events through the torch
+    autograd API (positions resident on the device): Hessian-vector products
+    (value, on the 41k box), parameter gradients and the force-matching loss
+    gradient, with the accuracy of one product against central differences
+    of the FP64 oracle."""
+    import torch
+    from protomoladdon_b200 import water
+    from protomoladdon_b200.autograd import NonbondedEnergy, lj_table
+    if env_int("WORLD_SIZE", 1) > 1 and env_int("RANK", 0) != 0:
+        return 0
+    dev = torch.device("cuda", env_int("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    res = {}
+    with ClockSampler(dev.index) as clk:
+        for name, s in (("water648", water.small_648()), ("water41k", water.medium_41k())):
+            m = NonbondedEnergy.from_system(s, precision="fp64")
+            q, t = m.initial_params(device=dev)
+            pos = torch.tensor(s["pos"], dtype=torch.float64, device=dev, requires_grad=True)
+            rng = np.random.default_rng(2024)
+            vs = []
+            for _ in range(32):
+                v = rng.standard_normal(s["pos"].shape)
+                vs.append(torch.tensor(v / np.linalg.norm(v), device=dev))
+            E = m.energy(pos, q, t)
+            (g,) = torch.autograd.grad(E, pos, create_graph=True)
+
+            def timed(fn, reps):
+                for _ in range(max(args.warmup, 3)):
+                    fn(0)
+                torch.cuda.synchronize(dev)
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record()
+                for k in range(reps):
+                    fn(k)
+                e1.record()
+                torch.cuda.synchronize(dev)
+                return e0.elapsed_time(e1) / reps
+
+            hv_ms = timed(lambda k: torch.autograd.grad(g, pos, grad_outputs=vs[k % 32],
+                                                        retain_graph=True), 32)
+            sig = torch.tensor([3.1507, 0.0], dtype=torch.float64, device=dev, requires_grad=True)
+            eps = torch.tensor([0.1521, 0.0], dtype=torch.float64, device=dev, requires_grad=True)
+            qq = q.clone().requires_grad_(True)
+
+            def param_grad(k):
+                torch.autograd.grad(m.energy(pos.detach(), qq, lj_table(sig, eps)), (qq, sig, eps))
+            pg_ms = timed(param_grad, 10)
+            F_t = (-m.gradient(pos.detach(), q * 1.03, lj_table(sig * 1.02, eps * 0.97))).detach()
+
+            def loss_grad(k):
+                F = m.forces(pos.detach(), qq, lj_table(sig, eps))
+                torch.autograd.grad(((F - F_t) ** 2).sum(), (qq, sig, eps))
+            lg_ms = timed(loss_grad, 10)
+            acc = None
+            if not args.skip_accuracy:
+                from oracle import oracle as O
+                v = vs[0].cpu().numpy()
+                (hv,) = torch.autograd.grad(g, pos, grad_outputs=vs[0], retain_graph=True)
+                h = 1e-4
+                fp, _, _, _ = O.restate_eval(s, s["pos"] + h * v, virial_mode=0)
+                fm, _, _, _ = O.restate_eval(s, s["pos"] - h * v, virial_mode=0)
+                fd = -(fp - fm) / (2 * h)
+                acc = float(np.linalg.norm(hv.cpu().numpy() - fd) / np.linalg.norm(fd))
+            m.close()
+            res[name] = {"atoms": s["n"], "hvp_ms": hv_ms, "hvp_per_s": 1e3 / hv_ms,
+                         "param_grad_ms": pg_ms, "loss_grad_ms": lg_ms,
+                         "hvp_rel_err_vs_fd": acc}
+    clocks = clk.summary()
+    big = res["water41k"]
+    line = {
+        "metric": DIFF_METRIC, "value": big["hvp_per_s"], "unit": "HVP/s", "n_gpus": 1,
+        "steps": 32, "warmup": max(args.warmup, 3), "ms_per_step": big["hvp_ms"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": DIFF_WORKLOAD, "step": "one Hessian-vector product (41k box)",
+                   "l2": "not flushed: derivative passes run back to back as in an "
+                         "optimizer loop, the ~6 MB working set staying in L2"},
+        "systems": res, "gpu_launches": 32 * 6, "clocks": clocks,
+        "e2e": {"value": big["hvp_per_s"], "unit": "HVP/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def ctypes_peak(device):
     import ctypes
     from protomoladdon_b200 import _lib
@@ -734,10 +832,12 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--skip-accuracy", action="store_true")
-    ap.add_argument("--workload", default="medium", choices=["medium", "large", "batch"],
+    ap.add_argument("--workload", default="medium",
+                    choices=["medium", "large", "batch", "diff"],
                     help="medium: the 41,472-atom water box (the headline); large: the "
                          "327,352-atom ion box's LJ+C1 and Ewald real-space kernels; batch: "
-                         "512 uneven boxes in one batched launch")
+                         "512 uneven boxes in one batched launch; diff: the differentiable "
+                         "form (Hessian-vector products, parameter gradients)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -747,6 +847,8 @@ def main():
         return run_large(args)
     if args.workload == "batch":
         return run_batch(args)
+    if args.workload == "diff":
+        return run_diff(args)
     return run_ours(args)
 
 
