@@ -346,6 +346,10 @@ int pmb200_batch_set_kernel_timing(pmb200_batch *batch, int on);
 int pmb200_batch_last_kernel_ms(pmb200_batch *batch, float *ms);
 /* In-cutoff pair count per system of the last evaluation with energies. */
 int pmb200_batch_pair_counts(pmb200_batch *batch, long long *counts);
+/* Waits for `stream` (NULL: the whole device) and reports a device-side
+ * error of the batch's evaluations since the last call (PMB200_EDEVICE:
+ * a non-finite position, or a pair force beyond the fixed-point range). */
+int pmb200_batch_sync(pmb200_batch *batch, void *stream);
 
 /* ---- Ewald real-space term ----
  * A context of the second kind replaces the real-space part of ProtoMol's

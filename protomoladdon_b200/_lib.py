@@ -48,6 +48,7 @@ EXPORTED = (
     "pmb200_batch_eval_device", "pmb200_batch_set_schedule", "pmb200_batch_get_schedule",
     "pmb200_batch_autotune", "pmb200_batch_set_kernel_timing", "pmb200_batch_last_kernel_ms",
     "pmb200_batch_pair_counts", "pmb200_create_pair", "pmb200_set_vacuum_domain",
+    "pmb200_batch_sync",
 )
 
 _P = ctypes.c_void_p
@@ -128,6 +129,7 @@ def lib():
                                         ctypes.POINTER(ctypes.c_float)]
     L.pmb200_batch_set_kernel_timing.argtypes = [_P, _I]
     L.pmb200_batch_last_kernel_ms.argtypes = [_P, ctypes.POINTER(ctypes.c_float)]
+    L.pmb200_batch_sync.argtypes = [_P, _P]
     L.pmb200_batch_pair_counts.argtypes = [_P, ctypes.POINTER(ctypes.c_longlong)]
     for name in EXPORTED:
         getattr(L, name).restype = getattr(L, name).restype or _I

@@ -50,6 +50,11 @@ class SystemBatch:
             self._b, _P(pos_ptr), _P(force_ptr), _P(out_ptr) if out_ptr else None, int(flags),
             _P(stream) if stream else None))
 
+    def sync(self, stream=None):
+        """Waits for the stream (None: the device) and raises PmbError for a
+        device-side error of the batch's evaluations."""
+        self._check(_lib.lib().pmb200_batch_sync(self._b, _P(stream) if stream else None))
+
     def set_schedule(self, parts=1, order=1, blocks_per_sm=0):
         self._check(_lib.lib().pmb200_batch_set_schedule(self._b, parts, order, blocks_per_sm))
 

@@ -1667,7 +1667,7 @@ void batch_launch_pair(pmb200_batch *b, bool energy, bool virial, int grid, cuda
   k_pair_mixed_batch<F, E, V><<<grid, 32 * kWarps, 0, st>>>(                               \
       b->d_sys, b->d_tasks, b->ntasks, b->d_counter, b->d_st, b->d_lj32, b->d_start,       \
       b->d_spos32, b->d_smeta, b->d_sidx, b->d_ex_start, b->d_ex, b->d_facc, b->N,         \
-      b->d_partial)
+      b->d_partial, b->d_err)
   if (energy && virial) PMB_BATCH_LAUNCH(true, true);
   else if (energy) PMB_BATCH_LAUNCH(true, false);
   else if (virial) PMB_BATCH_LAUNCH(false, true);
@@ -1953,6 +1953,22 @@ int pmb200_batch_eval_device(pmb200_batch *b, const double *d_pos, double *d_for
     b->gflags = flags;
   }
   BCK(cudaGraphLaunch(b->graph_exec, st));
+  return PMB200_OK;
+}
+
+int pmb200_batch_sync(pmb200_batch *b, void *stream) {
+  if (!b) return PMB200_EINVAL;
+  BCK(cudaSetDevice(b->device));
+  if (stream) BCK(cudaStreamSynchronize((cudaStream_t)stream));
+  else BCK(cudaDeviceSynchronize());
+  int e = 0;
+  BCK(cudaMemcpy(&e, b->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (e) {
+    BCK(cudaMemset(b->d_err, 0, sizeof(int)));
+    if (e & 1) return bfail(b, PMB200_EDEVICE, "non-finite atom position in a batch evaluation");
+    return bfail(b, PMB200_EDEVICE,
+                 "a pair force exceeded the fixed-point range in a batch evaluation (atoms overlap)");
+  }
   return PMB200_OK;
 }
 

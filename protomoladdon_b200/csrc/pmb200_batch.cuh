@@ -62,7 +62,7 @@ k_pair_mixed_batch(const BatchSys *__restrict__ sys, const int4 *__restrict__ ta
                    const float4 *__restrict__ spos, const int2 *__restrict__ smeta,
                    const int *__restrict__ sidx, const int *__restrict__ ex_start,
                    const int2 *__restrict__ ex, unsigned long long *__restrict__ facc, int N,
-                   double *__restrict__ partial) {
+                   double *__restrict__ partial, int *__restrict__ err) {
   __shared__ float4 s_lj[kMaxTypes * kMaxTypes];
   __shared__ MixedWarpSmem s_w[kWarps];
   __shared__ double s_acc[kWarps][ACC_MV];
@@ -96,7 +96,7 @@ k_pair_mixed_batch(const BatchSys *__restrict__ sys, const int4 *__restrict__ ta
     mixed_task<kForm, kEnergy, kVirial, false>(
         s_sys.g, s_sys.mc, s_st, s_sys.st_n, tk.z, tk.w, s_sys.ntypes, s_lj, tk.y,
         start + s_sys.cell0, spos, smeta, sidx, ex_start, ex, facc, N,
-        partial + (size_t)t * kNacc, s_sys.pb, nullptr, s_w, s_acc);
+        partial + (size_t)t * kNacc, s_sys.pb, nullptr, s_w, s_acc, err);
     __syncthreads();  // s_task and the staged system are reused
   }
 }

@@ -397,7 +397,7 @@ __device__ __forceinline__ void mixed_task(
     const int *__restrict__ ex_start, const int2 *__restrict__ ex,
     unsigned long long *__restrict__ facc, int n, double *__restrict__ partial_row,
     const PbcRef &pb, const double *__restrict__ com, MixedWarpSmem *s_w,
-    double (*s_acc)[ACC_MV]) {
+    double (*s_acc)[ACC_MV], int *__restrict__ err) {
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   MixedWarpSmem &sm = s_w[warp];
@@ -592,6 +592,9 @@ __device__ __forceinline__ void mixed_task(
           atomicAdd(&sm.jf[1][t], __float2int_rn(fyv));
           atomicAdd(&sm.jf[2][t], __float2int_rn(fzv));
         } else {
+          // beyond the int64 accumulator's range (~2^31 cell units), or not
+          // finite: the evaluation reports a device error
+          if (!(fmaxf(fabsf(fxv), fmaxf(fabsf(fyv), fabsf(fzv))) < 2.8e14f)) atomicOr(err, 2);
           const size_t jg = (size_t)sm.gidx[t];
           atomicAdd(&facc[jg], (unsigned long long)__float2ll_rn(fxv * kJToGlobal));
           atomicAdd(&facc[(size_t)n + jg], (unsigned long long)__float2ll_rn(fyv * kJToGlobal));
@@ -810,7 +813,7 @@ k_pair_mixed(GridParams g, MixedConsts mc, const HalfStencil st, int ntypes, con
   if (cell >= g.ncell) return;  // uniform per block
   mixed_task<kForm, kEnergy, kVirial, kMolVir>(
       g, mc, s_st, st.ncells, 0, 1, ntypes, s_lj, cell, start, spos, smeta, sidx, ex_start, ex,
-      facc, n, partial + (size_t)cell * kNacc, pb, com, s_w, s_acc);
+      facc, n, partial + (size_t)cell * kNacc, pb, com, s_w, s_acc, err);
 }
 
 // Fixed-point force accumulator (sorted order, [3][n], 2^-32 quanta in cell

@@ -64,6 +64,7 @@ def batch_eval(batch, boxes, flags=_lib.PMB200_ENERGY | _lib.PMB200_VIRIAL, stre
     out = torch.zeros((len(boxes), 20), dtype=torch.float64, device="cuda")
     for _ in range(times):
         batch.eval_device(pos.data_ptr(), frc.data_ptr(), out.data_ptr(), flags, stream)
+    batch.sync()  # raises on a device-side error
     torch.cuda.synchronize()
     return frc.cpu().numpy(), out.cpu().numpy()
 
@@ -134,3 +135,19 @@ def test_batch_rejects_mixed_kinds_and_fp64(boxes):
     with pytest.raises(PmbError) as ei:
         SystemBatch([(f64, PeriodicTopology.from_dict(s))])
     assert ei.value.code == _lib.PMB200_EUNSUPPORTED
+
+
+def test_batch_reports_non_finite_positions(boxes):
+    from protomoladdon_b200._lib import PmbError
+    mem = make_members(boxes[:3])
+    b = SystemBatch(mem)
+    pos = torch.tensor(np.concatenate([s["pos"] for s in boxes[:3]]), dtype=torch.float64,
+                       device="cuda")
+    pos[5, 1] = float("nan")
+    frc = torch.zeros_like(pos)
+    b.eval_device(pos.data_ptr(), frc.data_ptr(), None, 0, None)
+    with pytest.raises(PmbError) as ei:
+        b.sync()
+    assert ei.value.code == _lib.PMB200_EDEVICE
+    b.sync()  # the flag is cleared once reported
+    b.close()
