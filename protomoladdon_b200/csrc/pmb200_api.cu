@@ -24,6 +24,10 @@
 
 using namespace pmb200;
 
+// page-locked result words of a host-buffer evaluation: 20 doubles (energies,
+// virial, molecular virial) and the device error flag behind them
+constexpr int kPinOut = 21;
+
 struct pmb200_ctx {
   pmb200_params p{};
   std::string err;
@@ -96,6 +100,11 @@ struct pmb200_ctx {
   const void *sgraph_key[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   double sgraph_dt = 0.0;
   unsigned sgraph_flags = 0;
+  // host-buffer evaluation graph (pmb200_eval): copy in, evaluate, copy out
+  cudaGraph_t hgraph = nullptr;
+  cudaGraphExec_t hgraph_exec = nullptr;
+  const void *hgraph_src = nullptr;
+  unsigned hgraph_flags = 0;
   // pair-kernel timing
   int timing = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -144,6 +153,11 @@ void release_graph(pmb200_ctx *c) {
   c->sgraph_exec = nullptr;
   c->sgraph = nullptr;
   for (auto &k : c->sgraph_key) k = nullptr;
+  if (c->hgraph_exec) cudaGraphExecDestroy(c->hgraph_exec);
+  if (c->hgraph) cudaGraphDestroy(c->hgraph);
+  c->hgraph_exec = nullptr;
+  c->hgraph = nullptr;
+  c->hgraph_src = nullptr;
 }
 
 double rc_max(const pmb200_params &p) { return std::max(p.cutoff_lj, p.cutoff_coul); }
@@ -959,19 +973,23 @@ int pmb200_update_params(pmb200_ctx *c, const double *q_scaled, const double *lj
   return PMB200_OK;
 }
 
+// The device error flag's value e (read after the work that set it has
+// finished): clears the flag and reports.
+static int device_error(pmb200_ctx *c, int e) {
+  if (!e) return PMB200_OK;
+  CK(cudaMemset(c->d_err, 0, sizeof(int)));
+  if (e & 1) return fail(c, PMB200_EDEVICE, "non-finite atom position in an evaluation");
+  return fail(c, PMB200_EDEVICE,
+              "a pair force exceeded the mixed kernel's fixed-point range (atoms overlap)");
+}
+
 int pmb200_sync(pmb200_ctx *c) {
   if (!c) return PMB200_EINVAL;
   CK(cudaSetDevice(c->p.device));
   CK(cudaStreamSynchronize(c->stream));
   int e = 0;
   CK(cudaMemcpy(&e, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
-  if (e) {
-    CK(cudaMemset(c->d_err, 0, sizeof(int)));
-    if (e & 1) return fail(c, PMB200_EDEVICE, "non-finite atom position in an evaluation");
-    return fail(c, PMB200_EDEVICE,
-                "a pair force exceeded the mixed kernel's fixed-point range (atoms overlap)");
-  }
-  return PMB200_OK;
+  return device_error(c, e);
 }
 
 int pmb200_eval(pmb200_ctx *c, const double *pos, double *forces, double *energies,
@@ -989,15 +1007,18 @@ int pmb200_eval(pmb200_ctx *c, const double *pos, double *forces, double *energi
   const size_t bytes = sizeof(double) * cnt;
   cudaStream_t st = c->stream;
   if (c->n_pin < c->n || !c->h_pin_out) {
+    release_graph(c);  // the evaluation graph copies through these buffers
     if (c->h_pin_pos) cudaFreeHost(c->h_pin_pos);
     if (c->h_pin_frc) cudaFreeHost(c->h_pin_frc);
     if (c->h_pin_out) cudaFreeHost(c->h_pin_out);
     c->h_pin_pos = c->h_pin_frc = c->h_pin_out = nullptr;
     CK(cudaMallocHost((void **)&c->h_pin_pos, std::max<size_t>(bytes, 8)));
     CK(cudaMallocHost((void **)&c->h_pin_frc, std::max<size_t>(bytes, 8)));
-    CK(cudaMallocHost((void **)&c->h_pin_out, sizeof(double) * 20));
+    CK(cudaMallocHost((void **)&c->h_pin_out, sizeof(double) * kPinOut));
     c->n_pin = c->n;
   }
+  // the device error flag's page-locked copy, behind the 20 result words
+  int *h_err = reinterpret_cast<int *>(c->h_pin_out + 20);
   // positions through pinned staging; this evaluation's forces are computed
   // on the device (overwrite), read back, and added to the caller's array
   if (c->n > 0) {
@@ -1017,14 +1038,64 @@ int pmb200_eval(pmb200_ctx *c, const double *pos, double *forces, double *energi
       }
       src = c->h_pin_pos;
     }
-    CK(cudaMemcpyAsync(c->d_hpos, src, bytes, cudaMemcpyHostToDevice, st));
+    // copy in, evaluate, copy out: one graph per (source array, flags),
+    // replayed while the context's box and topology stay the same (the
+    // pair-kernel timing mode launches directly)
+    if (c->timing) {
+      CK(cudaMemcpyAsync(c->d_hpos, src, bytes, cudaMemcpyHostToDevice, st));
+      rc = launch_eval(c, c->d_hpos, c->d_hfrc, c->d_out, flags, 0, st);
+      if (rc) return rc;
+      CK(cudaMemcpyAsync(c->h_pin_frc, c->d_hfrc, bytes, cudaMemcpyDeviceToHost, st));
+      if (flags)
+        CK(cudaMemcpyAsync(c->h_pin_out, c->d_out, sizeof(double) * 20,
+                           cudaMemcpyDeviceToHost, st));
+      CK(cudaMemcpyAsync(h_err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    } else {
+      if (!c->hgraph_exec || c->hgraph_src != src || c->hgraph_flags != flags) {
+        if (c->hgraph_exec) cudaGraphExecDestroy(c->hgraph_exec);
+        if (c->hgraph) cudaGraphDestroy(c->hgraph);
+        c->hgraph_exec = nullptr;
+        c->hgraph = nullptr;
+        c->hgraph_src = nullptr;
+        CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e = cudaMemcpyAsync(c->d_hpos, src, bytes, cudaMemcpyHostToDevice, st);
+        rc = e == cudaSuccess ? launch_eval(c, c->d_hpos, c->d_hfrc, c->d_out, flags, 0, st)
+                              : fail(c, PMB200_ECUDA, "copy in: %s", cudaGetErrorString(e));
+        if (!rc) {
+          e = cudaMemcpyAsync(c->h_pin_frc, c->d_hfrc, bytes, cudaMemcpyDeviceToHost, st);
+          if (e == cudaSuccess && flags)
+            e = cudaMemcpyAsync(c->h_pin_out, c->d_out, sizeof(double) * 20,
+                                cudaMemcpyDeviceToHost, st);
+          if (e == cudaSuccess)
+            e = cudaMemcpyAsync(h_err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, st);
+          if (e != cudaSuccess)
+            rc = fail(c, PMB200_ECUDA, "copy out: %s", cudaGetErrorString(e));
+        }
+        cudaGraph_t gr = nullptr;
+        e = cudaStreamEndCapture(st, &gr);
+        if (rc) {
+          if (gr) cudaGraphDestroy(gr);
+          return rc;
+        }
+        if (e != cudaSuccess) return fail(c, PMB200_ECUDA, "capture: %s", cudaGetErrorString(e));
+        c->hgraph = gr;
+        CK(cudaGraphInstantiate(&c->hgraph_exec, gr, 0));
+        c->hgraph_src = src;
+        c->hgraph_flags = flags;
+      }
+      CK(cudaGraphLaunch(c->hgraph_exec, st));
+    }
+  } else {
+    rc = launch_eval(c, c->d_hpos, c->d_hfrc, c->d_out, flags, 0, st);
+    if (rc) return rc;
+    if (flags)
+      CK(cudaMemcpyAsync(c->h_pin_out, c->d_out, sizeof(double) * 20, cudaMemcpyDeviceToHost,
+                         st));
+    CK(cudaMemcpyAsync(h_err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
   }
-  rc = launch_eval(c, c->d_hpos, c->d_hfrc, c->d_out, flags, 0, st);
-  if (rc) return rc;
-  if (c->n > 0) CK(cudaMemcpyAsync(c->h_pin_frc, c->d_hfrc, bytes, cudaMemcpyDeviceToHost, st));
-  if (flags)
-    CK(cudaMemcpyAsync(c->h_pin_out, c->d_out, sizeof(double) * 20, cudaMemcpyDeviceToHost, st));
-  rc = pmb200_sync(c);
+  // the error flag came back with the results: one synchronisation
+  CK(cudaStreamSynchronize(st));
+  rc = device_error(c, *h_err);
   if (rc) return rc;
   {
     const double *src = c->h_pin_frc;
