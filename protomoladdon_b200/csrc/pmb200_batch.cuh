@@ -69,6 +69,7 @@ k_pair_mixed_batch(const BatchSys *__restrict__ sys, const int4 *__restrict__ ta
   __shared__ unsigned short s_st[kMaxHalfCells];
   __shared__ BatchSys s_sys;
   __shared__ int s_task;
+  __shared__ double s_pd[(kEnergy && kForm == FORM_CUTOFF) ? kWarps * 3 * kBatch : 1];
   const int lane = threadIdx.x & 31;
   MixedWarpSmem &sm = s_w[threadIdx.x >> 5];
   for (int t = lane; t < kBatch; t += 32) sm.jf[0][t] = sm.jf[1][t] = sm.jf[2][t] = 0;
@@ -96,7 +97,7 @@ k_pair_mixed_batch(const BatchSys *__restrict__ sys, const int4 *__restrict__ ta
     mixed_task<kForm, kEnergy, kVirial, false>(
         s_sys.g, s_sys.mc, s_st, s_sys.st_n, tk.z, tk.w, s_sys.ntypes, s_lj, tk.y,
         start + s_sys.cell0, spos, smeta, sidx, ex_start, ex, facc, N,
-        partial + (size_t)t * kNacc, s_sys.pb, nullptr, s_w, s_acc, err);
+        partial + (size_t)t * kNacc, s_sys.pb, nullptr, s_w, s_acc, err, s_pd);
     __syncthreads();  // s_task and the staged system are reused
   }
 }

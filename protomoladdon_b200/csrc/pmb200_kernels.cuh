@@ -397,10 +397,16 @@ __device__ __forceinline__ void mixed_task(
     const int *__restrict__ ex_start, const int2 *__restrict__ ex,
     unsigned long long *__restrict__ facc, int n, double *__restrict__ partial_row,
     const PbcRef &pb, const double *__restrict__ com, MixedWarpSmem *s_w,
-    double (*s_acc)[ACC_MV], int *__restrict__ err) {
+    double (*s_acc)[ACC_MV], int *__restrict__ err, double *__restrict__ s_pd) {
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   MixedWarpSmem &sm = s_w[warp];
+  // the energy of the cutoff form is summed from FP64 distances: kEnergy
+  // launches also stage each j position, shifted into the i-cell frame, in
+  // FP64 (s_pd: kWarps x 3 x kBatch doubles)
+  constexpr bool kExactE = kEnergy && kForm == FORM_CUTOFF;
+  double *pdx = kExactE ? s_pd + warp * 3 * kBatch : nullptr;
+  double *pdy = kExactE ? pdx + kBatch : nullptr, *pdz = kExactE ? pdx + 2 * kBatch : nullptr;
   const int cx = cell % g.nx;
   const int cy = (cell / g.nx) % g.ny;
   const int cz = cell / (g.nx * g.ny);
@@ -424,9 +430,22 @@ __device__ __forceinline__ void mixed_task(
     const int oi = sidx[i];
     const int elo = ex_start[oi], ehi = ex_start[oi + 1];
     const int ti = mi.x * ntypes;
+    // the box around the chunk's i atoms (idle lanes hold the chunk's first)
+    float blo_x = pi.x, blo_y = pi.y, blo_z = pi.z, bhi_x = pi.x, bhi_y = pi.y, bhi_z = pi.z;
+    for (int off = 16; off > 0; off >>= 1) {
+      blo_x = fminf(blo_x, __shfl_xor_sync(0xffffffffu, blo_x, off));
+      blo_y = fminf(blo_y, __shfl_xor_sync(0xffffffffu, blo_y, off));
+      blo_z = fminf(blo_z, __shfl_xor_sync(0xffffffffu, blo_z, off));
+      bhi_x = fmaxf(bhi_x, __shfl_xor_sync(0xffffffffu, bhi_x, off));
+      bhi_y = fmaxf(bhi_y, __shfl_xor_sync(0xffffffffu, bhi_y, off));
+      bhi_z = fmaxf(bhi_z, __shfl_xor_sync(0xffffffffu, bhi_z, off));
+    }
     // a batch holds at most kBatch / 2 candidates per lane (the list depth)
     const int batch_cap = min(kBatch, (kBatch / 2) * L);
     long long fx = 0, fy = 0, fz = 0;
+    // FP64 Coulomb sums of the cutoff form (see kExactE)
+    double eU = 0.0, eQ = 0.0, eR = 0.0;
+    const double pid_x = pi.x, pid_y = pi.y, pid_z = pi.z;
     double Ri[3] = {0.0, 0.0, 0.0};
     if (kMolVir)
       for (int k = 0; k < 3; k++) Ri[k] = com[3 * (size_t)mi.y + k];
@@ -570,9 +589,20 @@ __device__ __forceinline__ void mixed_task(
           const float sd = fmaf(dist, mc.c15_3, -mc.c15_1 * rinv);
           fc = ec * fmaf(r2inv, sv, -sd);
           if (kEnergy) {
-            kU.add(qj * rinv);
-            kQ.add(qj);
-            kR.add(qj * r2);
+            // q_j / r, q_j and q_j r^2 from the FP64 distance (the FP32 one
+            // rounds each term by ~1e-7 of q_j / rc while the C1 energy of a
+            // pair near the cutoff is far smaller); 1/r from the FP32 value
+            // and one Newton-Raphson step in FP64
+            const double ex_ = pdx[t] - pid_x;
+            const double ey_ = pdy[t] - pid_y;
+            const double ez_ = pdz[t] - pid_z;
+            const double r2d = fma(ex_, ex_, fma(ey_, ey_, ez_ * ez_));
+            double rid = (double)rinv;
+            rid = rid * fma(-0.5 * r2d, rid * rid, 1.5);
+            const double qjd = (double)qj;
+            eU = fma(qjd, rid, eU);
+            eQ += qjd;
+            eR = fma(qjd, r2d, eR);
           }
         }
         f = flj + fc;
@@ -696,41 +726,64 @@ __device__ __forceinline__ void mixed_task(
         h_cnt = __shfl_sync(0xffffffffu, ccnt, hl);
         h_js = __shfl_sync(0xffffffffu, cjs, hl);
       }
+      // stage the cells' atoms 32 (or the batch's remaining room) at a
+      // time; an atom farther than the cutoff from the box around this
+      // chunk's i atoms is dropped here instead of being tested by every i
+      // lane (home-cell atoms are always kept, so the home run stays whole)
       for (int f0 = 0; f0 < total;) {
-        const int take = min(total - f0, batch_cap - nb);
-        for (int r = 0; r < take; r += 32) {
-          const int t = r + lane;
-          const int f = f0 + t;
-          int c = 0;  // number of cells ending at or before f = f's cell
-          for (int step = 16; step > 0; step >>= 1) {
-            const int v = __shfl_sync(0xffffffffu, incl, c + step - 1);
-            if (v <= f) c += step;
-          }
-          const int js_c = __shfl_sync(0xffffffffu, cjs, c);
-          const int ex_c = __shfl_sync(0xffffffffu, excl, c);
-          const float sx = __shfl_sync(0xffffffffu, csx, c);
-          const float sy = __shfl_sync(0xffffffffu, csy, c);
-          const float sz = __shfl_sync(0xffffffffu, csz, c);
-          if (t < take) {
-            const int jg = js_c + (f - ex_c);
-            float4 p = spos[jg];
-            p.x += sx; p.y += sy; p.z += sz;
-            sm.pos[nb + t] = p;
-            sm.meta[nb + t] = smeta[jg];
-            sm.gidx[nb + t] = jg;
+        const int take = min(min(total - f0, batch_cap - nb), 32);
+        const int f = f0 + lane;
+        int c = 0;  // number of cells ending at or before f = f's cell
+        for (int step = 16; step > 0; step >>= 1) {
+          const int v = __shfl_sync(0xffffffffu, incl, c + step - 1);
+          if (v <= f) c += step;
+        }
+        const int js_c = __shfl_sync(0xffffffffu, cjs, c);
+        const int ex_c = __shfl_sync(0xffffffffu, excl, c);
+        const float sx = __shfl_sync(0xffffffffu, csx, c);
+        const float sy = __shfl_sync(0xffffffffu, csy, c);
+        const float sz = __shfl_sync(0xffffffffu, csz, c);
+        const bool home_atom = hmask && f >= h_excl && f < h_excl + h_cnt;
+        bool keep = false;
+        float4 a = make_float4(0.f, 0.f, 0.f, 0.f), p = a;
+        int jg = 0;
+        if (lane < take) {
+          jg = js_c + (f - ex_c);
+          a = spos[jg];
+          p = a;
+          p.x += sx; p.y += sy; p.z += sz;
+          // squared distance to the box in the pair test's operation order:
+          // per axis it is at most |p - x_i| for every i in the chunk, and
+          // rounding is monotonic, so no pair the test accepts is dropped
+          const float bx = fmaxf(fmaxf(blo_x - p.x, p.x - bhi_x), 0.f);
+          const float by = fmaxf(fmaxf(blo_y - p.y, p.y - bhi_y), 0.f);
+          const float bz = fmaxf(fmaxf(blo_z - p.z, p.z - bhi_z), 0.f);
+          keep = home_atom || fmaf(bx, bx, fmaf(by, by, bz * bz)) <= mc.cut2;
+        }
+        const unsigned km = __ballot_sync(0xffffffffu, keep);
+        if (keep) {
+          const int slot = nb + __popc(km & ((1u << lane) - 1u));
+          sm.pos[slot] = p;
+          sm.meta[slot] = smeta[jg];
+          sm.gidx[slot] = jg;
+          if (kExactE) {  // the shift added in FP64 (exact for these magnitudes)
+            pdx[slot] = (double)a.x + (double)sx;
+            pdy[slot] = (double)a.y + (double)sy;
+            pdz[slot] = (double)a.z + (double)sz;
           }
         }
-        if (hmask) {  // the part of the home cell staged in this batch
-          const int a = max(h_excl, f0), b = min(h_excl + h_cnt, f0 + take);
-          if (a < b) {
-            home_lo = nb + (a - f0);
-            home_hi = nb + (b - f0);
-            home_base = h_js + (a - h_excl);
+        const unsigned hm = __ballot_sync(0xffffffffu, keep && home_atom);
+        if (hm) {  // the part of the home cell staged in this round
+          const int fl = __ffs(hm) - 1, ll = 31 - __clz(hm);
+          if (home_hi == home_lo) {
+            home_lo = nb + __popc(km & ((1u << fl) - 1u));
+            home_base = h_js + (f0 + fl - h_excl);
           }
+          home_hi = nb + __popc(km & ((2u << ll) - 1u));
         }
-        nb += take;
+        nb += __popc(km);
         f0 += take;
-        if (nb == batch_cap) flush_batch();
+        if (batch_cap - nb < 16) flush_batch();
       }
     }
     if (nb > 0) flush_batch();
@@ -760,9 +813,15 @@ __device__ __forceinline__ void mixed_task(
     if (kEnergy && active) {
       // the three Coulomb sums are per i-atom: weight them by q_i (FP64)
       const double qi = (double)pi.w;
-      accU += qi * ((double)kU.s - (double)kU.c);
-      accQ += qi * ((double)kQ.s - (double)kQ.c);
-      accR += qi * ((double)kR.s - (double)kR.c);
+      if (kExactE) {
+        accU += qi * eU;
+        accQ += qi * eQ;
+        accR += qi * eR;
+      } else {
+        accU += qi * ((double)kU.s - (double)kU.c);
+        accQ += qi * ((double)kQ.s - (double)kQ.c);
+        accR += qi * ((double)kR.s - (double)kR.c);
+      }
     }
     kU = KahanF(); kQ = KahanF(); kR = KahanF();
   }
@@ -802,6 +861,7 @@ k_pair_mixed(GridParams g, MixedConsts mc, const HalfStencil st, int ntypes, con
   __shared__ MixedWarpSmem s_w[kWarps];
   __shared__ double s_acc[kWarps][ACC_MV];
   __shared__ unsigned short s_st[kMaxHalfCells];
+  __shared__ double s_pd[(kEnergy && kForm == FORM_CUTOFF) ? kWarps * 3 * kBatch : 1];
   if (kForm == FORM_CUTOFF || kForm == FORM_GENERIC)
     for (int k = threadIdx.x; k < ntypes * ntypes; k += blockDim.x) s_lj[k] = lj32[k];
   for (int k = threadIdx.x; k < st.ncells; k += blockDim.x) s_st[k] = st.off[k];
@@ -813,7 +873,7 @@ k_pair_mixed(GridParams g, MixedConsts mc, const HalfStencil st, int ntypes, con
   if (cell >= g.ncell) return;  // uniform per block
   mixed_task<kForm, kEnergy, kVirial, kMolVir>(
       g, mc, s_st, st.ncells, 0, 1, ntypes, s_lj, cell, start, spos, smeta, sidx, ex_start, ex,
-      facc, n, partial + (size_t)cell * kNacc, pb, com, s_w, s_acc, err);
+      facc, n, partial + (size_t)cell * kNacc, pb, com, s_w, s_acc, err, s_pd);
 }
 
 // Fixed-point force accumulator (sorted order, [3][n], 2^-32 quanta in cell
