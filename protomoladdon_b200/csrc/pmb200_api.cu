@@ -301,10 +301,9 @@ void launch_pair_mixed(pmb200_ctx *c, unsigned flags, cudaStream_t st) {
   const bool energy = (flags & PMB200_ENERGY) != 0;
   const bool virial = (flags & (PMB200_VIRIAL | PMB200_MOLVIRIAL)) != 0;
   const bool molvir = (flags & PMB200_MOLVIRIAL) != 0;
-  const size_t smem =
-      (F == FORM_CUTOFF || F == FORM_GENERIC) ? sizeof(float4) * c->ntypes * c->ntypes : 0;
+  const size_t smem = mixed_smem_bytes(F, c->ntypes, c->half.ncells);
 #define PMB_MIXED_LAUNCH(E, V, M)                                                          \
-  k_pair_mixed<F, E, V, M><<<g.ncell, 32 * kWarps, smem, st>>>(                              \
+  k_pair_mixed<F, E, V, M><<<g.ncell * kCellSlots, 32, smem, st>>>(                          \
       g, c->mc, c->half, c->ntypes, c->d_lj32, c->d_start, c->d_spos32, c->d_smeta,         \
       c->d_sidx, c->d_ex_start, c->d_ex, c->d_facc, c->n, c->d_err, c->d_partial, c->pb,    \
       c->d_com)
@@ -411,7 +410,10 @@ int launch_eval(pmb200_ctx *c, const double *d_pos, double *d_forces, double *d_
     // C1 constants for the mixed Coulomb sums (the Ewald term has none)
     const double rcc = c->p.cutoff_coul / g.unit;
     const bool c1 = c->form == FORM_CUTOFF;
-    k_reduce1<<<kRedBlocks, 256, 0, st>>>(g.ncell, c->d_partial, c->d_red);
+    // partial rows: one per (cell, slot) warp of the mixed kernel, one per
+    // cell of the FP64 kernel
+    k_reduce1<<<kRedBlocks, 256, 0, st>>>(mixed ? g.ncell * kCellSlots : g.ncell,
+                                          c->d_partial, c->d_red);
     // the mixed kernel visits each pair once, the FP64 kernel twice
     k_reduce2<<<1, 256, 0, st>>>(kRedBlocks, c->d_red, mixed ? 1 : 0, mixed ? 1.0 : 0.5,
                                 c1 ? 1.5 / rcc : 0.0, c1 ? 0.5 / (rcc * rcc * rcc) : 0.0,
@@ -807,7 +809,7 @@ int pmb200_set_box(pmb200_ctx *c, const double e1[3], const double e2[3], const 
   if (c->ncell_alloc < g.ncell) {
     CK(dalloc(c->d_count, (size_t)g.ncell));
     CK(dalloc(c->d_start, (size_t)g.ncell + 1));
-    CK(dalloc(c->d_partial, (size_t)g.ncell * kNacc));
+    CK(dalloc(c->d_partial, (size_t)g.ncell * kCellSlots * kNacc));
     c->ncell_alloc = g.ncell;
   }
   // constants
@@ -1432,7 +1434,8 @@ struct NoAllocLayout {  // byte offsets inside the scratch array
   static constexpr size_t count = 0;
   static constexpr size_t start = align256(count + sizeof(int) * kNoAllocCells);
   static constexpr size_t partial = align256(start + sizeof(int) * (kNoAllocCells + 1));
-  static constexpr size_t cell_of = align256(partial + sizeof(double) * kNoAllocCells * kNacc);
+  static constexpr size_t cell_of =
+      align256(partial + sizeof(double) * kNoAllocCells * kCellSlots * kNacc);
   static constexpr size_t slot = align256(cell_of + sizeof(int) * kNoAllocAtoms);
   static constexpr size_t tmp = align256(slot + sizeof(int) * kNoAllocAtoms);
   static constexpr size_t sidx = align256(tmp + sizeof(int) * kNoAllocAtoms);
@@ -1598,18 +1601,19 @@ extern "C" int pmb200_eval_noalloc(const pmb200_params *p, int n, const double *
   if (n > 0) k_scatter<<<(n + 255) / 256, 256, 0, st>>>(n, cell_of, slot, start, tmp);
   k_rank_gather<<<(g.ncell + 3) / 4, 128, 0, st>>>(g.ncell, start, tmp, rel32, nullptr, d_type,
                                                     d_mol, sidx, spos32, nullptr, smeta);
+  const size_t smem = mixed_smem_bytes(FORM_CUTOFF, ntypes, half.ncells);
   if (d_energy)
-    k_pair_mixed<FORM_CUTOFF, true, false, false><<<g.ncell, 32 * kWarps, sizeof(float4) * ntypes * ntypes, st>>>(
+    k_pair_mixed<FORM_CUTOFF, true, false, false><<<g.ncell * kCellSlots, 32, smem, st>>>(
         g, mc, half, ntypes, dlj, start, spos32, smeta, sidx, d_ex_start, d_ex, facc, n, err,
         partial, pb, nullptr);
   else
-    k_pair_mixed<FORM_CUTOFF, false, false, false><<<g.ncell, 32 * kWarps, sizeof(float4) * ntypes * ntypes, st>>>(
+    k_pair_mixed<FORM_CUTOFF, false, false, false><<<g.ncell * kCellSlots, 32, smem, st>>>(
         g, mc, half, ntypes, dlj, start, spos32, smeta, sidx, d_ex_start, d_ex, facc, n, err,
         partial, pb, nullptr);
   if (n > 0)
     k_finalize<<<(n + 255) / 256, 256, 0, st>>>(n, facc, sidx, kFixInv / u, 0, d_forces);
   if (d_energy) {
-    k_reduce1<<<kRedBlocks, 256, 0, st>>>(g.ncell, partial, red);
+    k_reduce1<<<kRedBlocks, 256, 0, st>>>(g.ncell * kCellSlots, partial, red);
     k_reduce2<<<1, 256, 0, st>>>(kRedBlocks, red, 1, 1.0, 1.5 / rq, 0.5 / (rq * rq * rq),
                                 d_energy, pairs);
   }
@@ -1719,7 +1723,7 @@ int batch_build_tasks(pmb200_batch *b) {
   if (b->ntasks < T || !b->d_tasks) {
     BCK(dalloc(b->d_tasks, (size_t)std::max(T, 1)));
     BCK(dalloc(b->d_rows, (size_t)std::max(T, 1)));
-    BCK(dalloc(b->d_partial, (size_t)std::max(T, 1) * kNacc));
+    BCK(dalloc(b->d_partial, (size_t)std::max(T, 1) * kWarps * kNacc));
   }
   b->ntasks = T;
   if (T > 0) {

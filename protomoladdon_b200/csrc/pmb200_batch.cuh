@@ -65,11 +65,11 @@ k_pair_mixed_batch(const BatchSys *__restrict__ sys, const int4 *__restrict__ ta
                    double *__restrict__ partial, int *__restrict__ err) {
   __shared__ float4 s_lj[kMaxTypes * kMaxTypes];
   __shared__ MixedWarpSmem s_w[kWarps];
-  __shared__ double s_acc[kWarps][ACC_MV];
   __shared__ unsigned short s_st[kMaxHalfCells];
   __shared__ BatchSys s_sys;
   __shared__ int s_task;
   __shared__ double s_pd[(kEnergy && kForm == FORM_CUTOFF) ? kWarps * 3 * kBatch : 1];
+  const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   MixedWarpSmem &sm = s_w[threadIdx.x >> 5];
   for (int t = lane; t < kBatch; t += 32) sm.jf[0][t] = sm.jf[1][t] = sm.jf[2][t] = 0;
@@ -94,10 +94,13 @@ k_pair_mixed_batch(const BatchSys *__restrict__ sys, const int4 *__restrict__ ta
       loaded = tk.x;
       __syncthreads();
     }
+    // the block's warps share the task: warp w takes the stencil entries
+    // part * kWarps + w + k * kWarps * parts
     mixed_task<kForm, kEnergy, kVirial, false>(
-        s_sys.g, s_sys.mc, s_st, s_sys.st_n, tk.z, tk.w, s_sys.ntypes, s_lj, tk.y,
-        start + s_sys.cell0, spos, smeta, sidx, ex_start, ex, facc, N,
-        partial + (size_t)t * kNacc, s_sys.pb, nullptr, s_w, s_acc, err, s_pd);
+        s_sys.g, s_sys.mc, s_st, s_sys.st_n, tk.z * kWarps + warp, kWarps * tk.w,
+        s_sys.ntypes, s_lj, tk.y, start + s_sys.cell0, spos, smeta, sidx, ex_start, ex, facc,
+        N, partial + ((size_t)t * kWarps + warp) * kNacc, s_sys.pb, nullptr, s_w[warp], err,
+        (kEnergy && kForm == FORM_CUTOFF) ? s_pd + warp * 3 * kBatch : nullptr);
     __syncthreads();  // s_task and the staged system are reused
   }
 }
@@ -133,7 +136,8 @@ __global__ void k_reduce_batch(int nsys, const int *__restrict__ rows_start,
   double acc = 0.0;  // lane k < ACC_MV sums slot k
   if (lane < ACC_MV)
     for (int r = rows_start[s]; r < rows_start[s + 1]; r++)
-      acc += partial[(size_t)rows[r] * kNacc + lane];
+      for (int w = 0; w < kWarps; w++)
+        acc += partial[((size_t)rows[r] * kWarps + w) * kNacc + lane];
   double v[ACC_MV];
 #pragma unroll
   for (int k = 0; k < ACC_MV; k++) v[k] = __shfl_sync(0xffffffffu, acc, k);

@@ -382,30 +382,27 @@ struct KahanF {
 // straight to the global int64 accumulator at 2^-32 resolution instead.
 // Both sums are exact integer sums.
 
-// One task of the mixed pair kernel for a whole block (kWarps warps): i-cell
-// `cell` and the stencil entries part * kWarps + warp + k * kWarps * nparts
-// (nparts = 1: the cell's whole half shell).  The stencil offsets and the LJ
-// table are read from shared memory; partial_row receives the task's energy
-// and virial partials.  Every thread of the block must call it (it
-// synchronises the block).
+// One task of the mixed pair kernel for one warp: i-cell `cell` and the
+// stencil entries slot + k * nslots (nslots = 1: the cell's whole half
+// shell).  The stencil offsets and the LJ table are read from shared memory;
+// the warp's i forces go straight to facc and its energy and virial partials
+// to partial_row.  Warps never wait for one another.
 template <int kForm, bool kEnergy, bool kVirial, bool kMolVir>
 __device__ __forceinline__ void mixed_task(
     const GridParams &g, const MixedConsts &mc, const unsigned short *st_off, int st_ncells,
-    int part, int nparts, int ntypes, const float4 *s_lj, int cell,
+    int slot, int nslots, int ntypes, const float4 *s_lj, int cell,
     const int *__restrict__ start, const float4 *__restrict__ spos,
     const int2 *__restrict__ smeta, const int *__restrict__ sidx,
     const int *__restrict__ ex_start, const int2 *__restrict__ ex,
     unsigned long long *__restrict__ facc, int n, double *__restrict__ partial_row,
-    const PbcRef &pb, const double *__restrict__ com, MixedWarpSmem *s_w,
-    double (*s_acc)[ACC_MV], int *__restrict__ err, double *__restrict__ s_pd) {
+    const PbcRef &pb, const double *__restrict__ com, MixedWarpSmem &sm,
+    int *__restrict__ err, double *__restrict__ s_pd) {
   const int lane = threadIdx.x & 31;
-  const int warp = threadIdx.x >> 5;
-  MixedWarpSmem &sm = s_w[warp];
   // the energy of the cutoff form is summed from FP64 distances: kEnergy
   // launches also stage each j position, shifted into the i-cell frame, in
-  // FP64 (s_pd: kWarps x 3 x kBatch doubles)
+  // FP64 (s_pd: this warp's 3 x kBatch doubles)
   constexpr bool kExactE = kEnergy && kForm == FORM_CUTOFF;
-  double *pdx = kExactE ? s_pd + warp * 3 * kBatch : nullptr;
+  double *pdx = kExactE ? s_pd : nullptr;
   double *pdy = kExactE ? pdx + kBatch : nullptr, *pdz = kExactE ? pdx + 2 * kBatch : nullptr;
   const int cx = cell % g.nx;
   const int cy = (cell / g.nx) % g.ny;
@@ -683,7 +680,7 @@ __device__ __forceinline__ void mixed_task(
     // lays the cells end to end, and every batch is loaded with independent
     // loads (a binary search over the prefix finds each entry's cell), so the
     // L2 latency is paid once per batch rather than once per cell.
-    const int first = part * kWarps + warp, stride = kWarps * nparts;
+    const int first = slot, stride = nslots;
     const int nmine = first < st_ncells ? (st_ncells - first + stride - 1) / stride : 0;
     for (int g0 = 0; g0 < nmine; g0 += 32) {
       const int myq = g0 + lane;
@@ -788,28 +785,15 @@ __device__ __forceinline__ void mixed_task(
     }
     if (nb > 0) flush_batch();
 
-    // the i forces: lanes of an atom, then warps, then the global accumulator
+    // the i forces: the lanes of an atom, then the global accumulator
     fx = warp_sum_ll(fx, L);
     fy = warp_sum_ll(fy, L);
     fz = warp_sum_ll(fz, L);
-    // the block's i-force sum goes through each warp's staging area, free
-    // once its last batch is flushed
-    {
-      long long *mine = reinterpret_cast<long long *>(sm.pos) + 3 * lane;
-      mine[0] = fx; mine[1] = fy; mine[2] = fz;
+    if (active && sub == 0) {
+      atomicAdd(&facc[i], (unsigned long long)fx);
+      atomicAdd(&facc[(size_t)n + i], (unsigned long long)fy);
+      atomicAdd(&facc[2 * (size_t)n + i], (unsigned long long)fz);
     }
-    __syncthreads();
-    if (warp == 0 && active && sub == 0) {
-      long long tx = 0, ty = 0, tz = 0;
-      for (int q = 0; q < kWarps; q++) {
-        const long long *o = reinterpret_cast<const long long *>(s_w[q].pos) + 3 * lane;
-        tx += o[0]; ty += o[1]; tz += o[2];
-      }
-      atomicAdd(&facc[i], (unsigned long long)tx);
-      atomicAdd(&facc[(size_t)n + i], (unsigned long long)ty);
-      atomicAdd(&facc[2 * (size_t)n + i], (unsigned long long)tz);
-    }
-    __syncthreads();
     if (kEnergy && active) {
       // the three Coulomb sums are per i-atom: weight them by q_i (FP64)
       const double qi = (double)pi.w;
@@ -835,45 +819,54 @@ __device__ __forceinline__ void mixed_task(
 #pragma unroll
     for (int k = 0; k < ACC_MV; k++) {
       const double sum = warp_sum_mask(v[k], 32);
-      if (lane == 0) s_acc[warp][k] = sum;
-    }
-    __syncthreads();
-    if (threadIdx.x < ACC_MV) {
-      double sum = 0.0;
-      for (int q = 0; q < kWarps; q++) sum += s_acc[q][threadIdx.x];
-      partial_row[threadIdx.x] = sum;
+      if (lane == 0) partial_row[k] = sum;
     }
   }
 }
 
-// Forces-only launches (the MD step's) are asked to fit 7 blocks per SM
-// (<= 73 registers, measured 1.4% faster than 6 on the 41k box); the
-// energy / virial variants keep the compiler's register choice.
+// One warp per block, kCellSlots blocks per i-cell (block b: cell b /
+// kCellSlots, stencil entries b % kCellSlots + k * kCellSlots), so a warp
+// that finishes early frees its slot for the next block instead of waiting
+// for the cell's other warps.  Dynamic shared memory: the LJ table (ntypes^2
+// float4, cutoff and generic forms) and then the stencil offsets.
+// Forces-only launches are held to 72 registers, so that shared memory
+// (~8.4 KB per block with the per-block reserve) sets the residency at 27
+// blocks per SM; the energy / virial variants keep the compiler's choice.
+constexpr int kCellSlots = 4;
+
 template <int kForm, bool kEnergy, bool kVirial, bool kMolVir>
-__global__ void __launch_bounds__(128, (kEnergy || kVirial) ? 1 : 7)
+__global__ void __launch_bounds__(32, (kEnergy || kVirial) ? 1 : 27)
 k_pair_mixed(GridParams g, MixedConsts mc, const HalfStencil st, int ntypes, const float4 *__restrict__ lj32,
              const int *__restrict__ start, const float4 *__restrict__ spos,
              const int2 *__restrict__ smeta, const int *__restrict__ sidx,
              const int *__restrict__ ex_start, const int2 *__restrict__ ex,
              unsigned long long *__restrict__ facc, int n, int *__restrict__ err,
              double *__restrict__ partial, const PbcRef pb, const double *__restrict__ com) {
-  extern __shared__ float4 s_lj[];  // ntypes^2 LJ records (dynamic: sized per launch)
-  __shared__ MixedWarpSmem s_w[kWarps];
-  __shared__ double s_acc[kWarps][ACC_MV];
-  __shared__ unsigned short s_st[kMaxHalfCells];
-  __shared__ double s_pd[(kEnergy && kForm == FORM_CUTOFF) ? kWarps * 3 * kBatch : 1];
-  if (kForm == FORM_CUTOFF || kForm == FORM_GENERIC)
-    for (int k = threadIdx.x; k < ntypes * ntypes; k += blockDim.x) s_lj[k] = lj32[k];
-  for (int k = threadIdx.x; k < st.ncells; k += blockDim.x) s_st[k] = st.off[k];
-  const int lane = threadIdx.x & 31;
-  MixedWarpSmem &sm = s_w[threadIdx.x >> 5];
+  extern __shared__ float4 s_dyn[];
+  __shared__ MixedWarpSmem sm;
+  __shared__ double s_pd[(kEnergy && kForm == FORM_CUTOFF) ? 3 * kBatch : 1];
+  constexpr bool kLj = kForm == FORM_CUTOFF || kForm == FORM_GENERIC;
+  const int nlj = kLj ? ntypes * ntypes : 0;
+  float4 *s_lj = s_dyn;
+  unsigned short *s_st = reinterpret_cast<unsigned short *>(s_dyn + nlj);
+  const int lane = threadIdx.x;
+  for (int k = lane; k < nlj; k += 32) s_lj[k] = lj32[k];
+  for (int k = lane; k < st.ncells; k += 32) s_st[k] = st.off[k];
   for (int t = lane; t < kBatch; t += 32) sm.jf[0][t] = sm.jf[1][t] = sm.jf[2][t] = 0;
-  __syncthreads();
-  const int cell = blockIdx.x;
+  __syncwarp();
+  const int cell = blockIdx.x / kCellSlots;
   if (cell >= g.ncell) return;  // uniform per block
   mixed_task<kForm, kEnergy, kVirial, kMolVir>(
-      g, mc, s_st, st.ncells, 0, 1, ntypes, s_lj, cell, start, spos, smeta, sidx, ex_start, ex,
-      facc, n, partial + (size_t)cell * kNacc, pb, com, s_w, s_acc, err, s_pd);
+      g, mc, s_st, st.ncells, blockIdx.x % kCellSlots, kCellSlots, ntypes, s_lj, cell, start,
+      spos, smeta, sidx, ex_start, ex, facc, n, partial + (size_t)blockIdx.x * kNacc, pb, com,
+      sm, err, s_pd);
+}
+
+// Dynamic shared memory of a k_pair_mixed launch.
+inline size_t mixed_smem_bytes(int form, int ntypes, int st_ncells) {
+  const size_t lj = (form == FORM_CUTOFF || form == FORM_GENERIC)
+                        ? sizeof(float4) * (size_t)ntypes * ntypes : 0;
+  return lj + ((sizeof(unsigned short) * (size_t)st_ncells + 15) & ~(size_t)15);
 }
 
 // Fixed-point force accumulator (sorted order, [3][n], 2^-32 quanta in cell
