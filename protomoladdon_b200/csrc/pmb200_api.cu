@@ -302,11 +302,12 @@ void launch_pair_mixed(pmb200_ctx *c, unsigned flags, cudaStream_t st) {
   const bool virial = (flags & (PMB200_VIRIAL | PMB200_MOLVIRIAL)) != 0;
   const bool molvir = (flags & PMB200_MOLVIRIAL) != 0;
   const size_t smem = mixed_smem_bytes(F, c->ntypes, c->half.ncells);
+  const int slots = mixed_cell_slots(energy || virial, c->n, g.ncell);
 #define PMB_MIXED_LAUNCH(E, V, M)                                                          \
-  k_pair_mixed<F, E, V, M><<<g.ncell * kCellSlots, 32, smem, st>>>(                          \
+  k_pair_mixed<F, E, V, M><<<g.ncell * slots, 32, smem, st>>>(                               \
       g, c->mc, c->half, c->ntypes, c->d_lj32, c->d_start, c->d_spos32, c->d_smeta,         \
       c->d_sidx, c->d_ex_start, c->d_ex, c->d_facc, c->n, c->d_err, c->d_partial, c->pb,    \
-      c->d_com)
+      c->d_com, slots)
   if (molvir) PMB_MIXED_LAUNCH(true, true, true);
   else if (energy && virial) PMB_MIXED_LAUNCH(true, true, false);
   else if (energy) PMB_MIXED_LAUNCH(true, false, false);
@@ -412,8 +413,10 @@ int launch_eval(pmb200_ctx *c, const double *d_pos, double *d_forces, double *d_
     const bool c1 = c->form == FORM_CUTOFF;
     // partial rows: one per (cell, slot) warp of the mixed kernel, one per
     // cell of the FP64 kernel
-    k_reduce1<<<kRedBlocks, 256, 0, st>>>(mixed ? g.ncell * kCellSlots : g.ncell,
-                                          c->d_partial, c->d_red);
+    // (energy / virial launches of the mixed kernel use the slot count of
+    // mixed_cell_slots(true, ...))
+    k_reduce1<<<kRedBlocks, 256, 0, st>>>(
+        mixed ? g.ncell * mixed_cell_slots(true, n, g.ncell) : g.ncell, c->d_partial, c->d_red);
     // the mixed kernel visits each pair once, the FP64 kernel twice
     k_reduce2<<<1, 256, 0, st>>>(kRedBlocks, c->d_red, mixed ? 1 : 0, mixed ? 1.0 : 0.5,
                                 c1 ? 1.5 / rcc : 0.0, c1 ? 0.5 / (rcc * rcc * rcc) : 0.0,
@@ -809,7 +812,7 @@ int pmb200_set_box(pmb200_ctx *c, const double e1[3], const double e2[3], const 
   if (c->ncell_alloc < g.ncell) {
     CK(dalloc(c->d_count, (size_t)g.ncell));
     CK(dalloc(c->d_start, (size_t)g.ncell + 1));
-    CK(dalloc(c->d_partial, (size_t)g.ncell * kCellSlots * kNacc));
+    CK(dalloc(c->d_partial, (size_t)g.ncell * kMaxCellSlots * kNacc));
     c->ncell_alloc = g.ncell;
   }
   // constants
@@ -1435,7 +1438,7 @@ struct NoAllocLayout {  // byte offsets inside the scratch array
   static constexpr size_t start = align256(count + sizeof(int) * kNoAllocCells);
   static constexpr size_t partial = align256(start + sizeof(int) * (kNoAllocCells + 1));
   static constexpr size_t cell_of =
-      align256(partial + sizeof(double) * kNoAllocCells * kCellSlots * kNacc);
+      align256(partial + sizeof(double) * kNoAllocCells * kMaxCellSlots * kNacc);
   static constexpr size_t slot = align256(cell_of + sizeof(int) * kNoAllocAtoms);
   static constexpr size_t tmp = align256(slot + sizeof(int) * kNoAllocAtoms);
   static constexpr size_t sidx = align256(tmp + sizeof(int) * kNoAllocAtoms);
@@ -1602,18 +1605,19 @@ extern "C" int pmb200_eval_noalloc(const pmb200_params *p, int n, const double *
   k_rank_gather<<<(g.ncell + 3) / 4, 128, 0, st>>>(g.ncell, start, tmp, rel32, nullptr, d_type,
                                                     d_mol, sidx, spos32, nullptr, smeta);
   const size_t smem = mixed_smem_bytes(FORM_CUTOFF, ntypes, half.ncells);
+  const int slots = mixed_cell_slots(d_energy != nullptr, n, g.ncell);
   if (d_energy)
-    k_pair_mixed<FORM_CUTOFF, true, false, false><<<g.ncell * kCellSlots, 32, smem, st>>>(
+    k_pair_mixed<FORM_CUTOFF, true, false, false><<<g.ncell * slots, 32, smem, st>>>(
         g, mc, half, ntypes, dlj, start, spos32, smeta, sidx, d_ex_start, d_ex, facc, n, err,
-        partial, pb, nullptr);
+        partial, pb, nullptr, slots);
   else
-    k_pair_mixed<FORM_CUTOFF, false, false, false><<<g.ncell * kCellSlots, 32, smem, st>>>(
+    k_pair_mixed<FORM_CUTOFF, false, false, false><<<g.ncell * slots, 32, smem, st>>>(
         g, mc, half, ntypes, dlj, start, spos32, smeta, sidx, d_ex_start, d_ex, facc, n, err,
-        partial, pb, nullptr);
+        partial, pb, nullptr, slots);
   if (n > 0)
     k_finalize<<<(n + 255) / 256, 256, 0, st>>>(n, facc, sidx, kFixInv / u, 0, d_forces);
   if (d_energy) {
-    k_reduce1<<<kRedBlocks, 256, 0, st>>>(g.ncell * kCellSlots, partial, red);
+    k_reduce1<<<kRedBlocks, 256, 0, st>>>(g.ncell * slots, partial, red);
     k_reduce2<<<1, 256, 0, st>>>(kRedBlocks, red, 1, 1.0, 1.5 / rq, 0.5 / (rq * rq * rq),
                                 d_energy, pairs);
   }

@@ -350,7 +350,10 @@ __device__ __forceinline__ int lanes_per_atom(int m) {
 // constants are applied once in FP64 at the end.
 // ---------------------------------------------------------------------------
 constexpr int kWarps = 4;
-constexpr int kBatch = 128;
+#ifndef PMB200_STAGE_BATCH
+#define PMB200_STAGE_BATCH 128
+#endif
+constexpr int kBatch = PMB200_STAGE_BATCH;  // staged j atoms per warp batch (<= 256)
 
 constexpr float kJScale = 262144.0f; // shared j-force quanta (2^-18) per cell-unit force
 constexpr int kJShift = 14;          // to the global 2^-32 quanta
@@ -824,15 +827,18 @@ __device__ __forceinline__ void mixed_task(
   }
 }
 
-// One warp per block, kCellSlots blocks per i-cell (block b: cell b /
-// kCellSlots, stencil entries b % kCellSlots + k * kCellSlots), so a warp
-// that finishes early frees its slot for the next block instead of waiting
-// for the cell's other warps.  Dynamic shared memory: the LJ table (ntypes^2
-// float4, cutoff and generic forms) and then the stencil offsets.
-// Forces-only launches are held to 72 registers, so that shared memory
-// (~8.4 KB per block with the per-block reserve) sets the residency at 27
-// blocks per SM; the energy / virial variants keep the compiler's choice.
-constexpr int kCellSlots = 4;
+// One warp per block, `slots` blocks per i-cell (block b: cell b / slots,
+// stencil entries b % slots + k * slots), so a warp that finishes early
+// frees its slot for the next block instead of waiting for the cell's other
+// warps.  More slots mean more, shorter warps (better balance, more per-warp
+// setup); the host picks 8 for forces-only launches on sparse cells and 4
+// otherwise (kMaxCellSlots bounds the partial rows).  Dynamic shared memory:
+// the LJ table (ntypes^2 float4, cutoff and generic forms) and then the
+// stencil offsets.  Forces-only launches are held to 72 registers, so that
+// shared memory (~8.4 KB per block with the per-block reserve) sets the
+// residency at 27 blocks per SM; the energy / virial variants keep the
+// compiler's choice.
+constexpr int kMaxCellSlots = 8;
 
 template <int kForm, bool kEnergy, bool kVirial, bool kMolVir>
 __global__ void __launch_bounds__(32, (kEnergy || kVirial) ? 1 : 27)
@@ -841,7 +847,8 @@ k_pair_mixed(GridParams g, MixedConsts mc, const HalfStencil st, int ntypes, con
              const int2 *__restrict__ smeta, const int *__restrict__ sidx,
              const int *__restrict__ ex_start, const int2 *__restrict__ ex,
              unsigned long long *__restrict__ facc, int n, int *__restrict__ err,
-             double *__restrict__ partial, const PbcRef pb, const double *__restrict__ com) {
+             double *__restrict__ partial, const PbcRef pb, const double *__restrict__ com,
+             int slots) {
   extern __shared__ float4 s_dyn[];
   __shared__ MixedWarpSmem sm;
   __shared__ double s_pd[(kEnergy && kForm == FORM_CUTOFF) ? 3 * kBatch : 1];
@@ -854,12 +861,19 @@ k_pair_mixed(GridParams g, MixedConsts mc, const HalfStencil st, int ntypes, con
   for (int k = lane; k < st.ncells; k += 32) s_st[k] = st.off[k];
   for (int t = lane; t < kBatch; t += 32) sm.jf[0][t] = sm.jf[1][t] = sm.jf[2][t] = 0;
   __syncwarp();
-  const int cell = blockIdx.x / kCellSlots;
+  const int cell = blockIdx.x / slots;
   if (cell >= g.ncell) return;  // uniform per block
   mixed_task<kForm, kEnergy, kVirial, kMolVir>(
-      g, mc, s_st, st.ncells, blockIdx.x % kCellSlots, kCellSlots, ntypes, s_lj, cell, start,
+      g, mc, s_st, st.ncells, blockIdx.x % slots, slots, ntypes, s_lj, cell, start,
       spos, smeta, sidx, ex_start, ex, facc, n, partial + (size_t)blockIdx.x * kNacc, pb, com,
       sm, err, s_pd);
+}
+
+// Blocks per i-cell of a k_pair_mixed launch: 8 for forces-only launches
+// when cells hold at most 18 atoms on average (measured on water boxes:
+// 15 atoms per cell 4% faster than 4; 24 per cell 5% slower), else 4.
+inline int mixed_cell_slots(bool energy_or_virial, int natoms, int ncell) {
+  return (!energy_or_virial && natoms <= 18LL * ncell) ? 8 : 4;
 }
 
 // Dynamic shared memory of a k_pair_mixed launch.
