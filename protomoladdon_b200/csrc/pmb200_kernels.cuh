@@ -836,12 +836,14 @@ __device__ __forceinline__ void mixed_task(
 // the LJ table (ntypes^2 float4, cutoff and generic forms) and then the
 // stencil offsets.  Forces-only launches are held to 72 registers, so that
 // shared memory (~8.4 KB per block with the per-block reserve) sets the
-// residency at 27 blocks per SM; the energy / virial variants keep the
-// compiler's choice.
+// residency at 27 blocks per SM; energy launches (11.5 KB: 19 blocks) to the
+// ~96 registers that still fit 20 without spills; the virial variants keep
+// the compiler's choice.
 constexpr int kMaxCellSlots = 8;
 
+
 template <int kForm, bool kEnergy, bool kVirial, bool kMolVir>
-__global__ void __launch_bounds__(32, (kEnergy || kVirial) ? 1 : 27)
+__global__ void __launch_bounds__(32, kVirial ? 1 : (kEnergy ? 20 : 27))
 k_pair_mixed(GridParams g, MixedConsts mc, const HalfStencil st, int ntypes, const float4 *__restrict__ lj32,
              const int *__restrict__ start, const float4 *__restrict__ spos,
              const int2 *__restrict__ smeta, const int *__restrict__ sidx,
