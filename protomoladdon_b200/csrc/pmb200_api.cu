@@ -73,6 +73,7 @@ struct pmb200_ctx {
   int n_alloc = 0;
   int *d_cell_of = nullptr, *d_slot = nullptr, *d_tmp = nullptr, *d_sidx = nullptr;
   float4 *d_rel32 = nullptr, *d_spos32 = nullptr;
+  float4 *d_rel_lo = nullptr, *d_spos_lo = nullptr;  // FP32 coordinate residuals
   double4 *d_rel64 = nullptr, *d_spos64 = nullptr;
   int2 *d_smeta = nullptr;
   unsigned long long *d_facc = nullptr;
@@ -284,6 +285,8 @@ int ensure_atom_buffers(pmb200_ctx *c) {
   CK(dalloc(c->d_sidx, n));
   CK(dalloc(c->d_rel32, n));
   CK(dalloc(c->d_spos32, n));
+  CK(dalloc(c->d_rel_lo, n));
+  CK(dalloc(c->d_spos_lo, n));
   CK(dalloc(c->d_rel64, n));
   CK(dalloc(c->d_spos64, n));
   CK(dalloc(c->d_smeta, n));
@@ -307,7 +310,7 @@ void launch_pair_mixed(pmb200_ctx *c, unsigned flags, cudaStream_t st) {
   k_pair_mixed<F, E, V, M><<<g.ncell * slots, 32, smem, st>>>(                               \
       g, c->mc, c->half, c->ntypes, c->d_lj32, c->d_start, c->d_spos32, c->d_smeta,         \
       c->d_sidx, c->d_ex_start, c->d_ex, c->d_facc, c->n, c->d_err, c->d_partial, c->pb,    \
-      c->d_com, slots)
+      c->d_com, slots, c->d_spos_lo)
   if (molvir) PMB_MIXED_LAUNCH(true, true, true);
   else if (energy && virial) PMB_MIXED_LAUNCH(true, true, false);
   else if (energy) PMB_MIXED_LAUNCH(true, false, false);
@@ -341,8 +344,10 @@ void launch_pair_fp64(pmb200_ctx *c, unsigned flags, double *d_forces, int accum
 // overwrite it (0).
 // Counting sort of the atoms into the grid cells (cell index, scan,
 // scatter, in-cell rank order), producing the cell-unit FP32 copies (mixed)
-// or the Angstrom FP64 copies of the sorted positions.
-void launch_cell_build(pmb200_ctx *c, const double *d_pos, bool mixed, cudaStream_t st) {
+// or the Angstrom FP64 copies of the sorted positions; lo: also the FP32
+// coordinates' rounding residuals (energy evaluations of the cutoff form).
+void launch_cell_build(pmb200_ctx *c, const double *d_pos, bool mixed, bool lo,
+                       cudaStream_t st) {
   const int n = c->n;
   const GridParams &g = c->g;
   cudaMemsetAsync(c->d_count, 0, sizeof(int) * g.ncell, st);
@@ -350,7 +355,8 @@ void launch_cell_build(pmb200_ctx *c, const double *d_pos, bool mixed, cudaStrea
     const int tb = 256;
     k_cell_index<<<(n + tb - 1) / tb, tb, 0, st>>>(
         n, d_pos, g, c->d_cell_of, c->d_count, c->d_slot, mixed ? c->d_rel32 : nullptr,
-        mixed ? nullptr : c->d_rel64, c->d_q, (float)(1.0 / std::sqrt(g.unit)), c->d_err);
+        mixed ? nullptr : c->d_rel64, c->d_q, (float)(1.0 / std::sqrt(g.unit)), c->d_err,
+        lo ? c->d_rel_lo : nullptr);
   }
   k_scan<<<1, 1024, 1024 * sizeof(int), st>>>(g.ncell, c->d_count, c->d_start);
   if (n > 0) {
@@ -362,7 +368,8 @@ void launch_cell_build(pmb200_ctx *c, const double *d_pos, bool mixed, cudaStrea
   k_rank_gather<<<blocks, 128, 0, st>>>(
       g.ncell, c->d_start, c->d_tmp, mixed ? c->d_rel32 : nullptr,
       mixed ? nullptr : c->d_rel64, c->d_type, c->d_mol, c->d_sidx,
-      mixed ? c->d_spos32 : nullptr, mixed ? nullptr : c->d_spos64, c->d_smeta);
+      mixed ? c->d_spos32 : nullptr, mixed ? nullptr : c->d_spos64, c->d_smeta,
+      lo ? c->d_rel_lo : nullptr, lo ? c->d_spos_lo : nullptr);
 }
 
 int launch_eval(pmb200_ctx *c, const double *d_pos, double *d_forces, double *d_out,
@@ -373,7 +380,7 @@ int launch_eval(pmb200_ctx *c, const double *d_pos, double *d_forces, double *d_
   const bool virial = (flags & (PMB200_VIRIAL | PMB200_MOLVIRIAL)) != 0;
   const bool molvir = (flags & PMB200_MOLVIRIAL) != 0;
   const GridParams &g = c->g;
-  launch_cell_build(c, d_pos, mixed, st);
+  launch_cell_build(c, d_pos, mixed, mixed && energy && c->form == FORM_CUTOFF, st);
   CK(cudaGetLastError());
   const int blocks = (g.ncell + 3) / 4;
   if (molvir && c->nmol > 0)
@@ -595,7 +602,7 @@ int pmb200_destroy(pmb200_ctx *c) {
   dfree(c->d_lj32); dfree(c->d_lj64);
   dfree(c->d_count); dfree(c->d_start); dfree(c->d_err); dfree(c->d_partial);
   dfree(c->d_cell_of); dfree(c->d_slot); dfree(c->d_tmp); dfree(c->d_sidx);
-  dfree(c->d_rel32); dfree(c->d_spos32); dfree(c->d_rel64); dfree(c->d_spos64);
+  dfree(c->d_rel32); dfree(c->d_spos32); dfree(c->d_rel_lo); dfree(c->d_spos_lo); dfree(c->d_rel64); dfree(c->d_spos64);
   dfree(c->d_smeta); dfree(c->d_com); dfree(c->d_facc);
   dfree(c->d_tpart); dfree(c->d_gq); dfree(c->d_glj);
   dfree(c->d_pairs); dfree(c->d_out); dfree(c->d_red); dfree(c->d_widx); dfree(c->d_fidx);
@@ -913,7 +920,7 @@ static int launch_deriv(pmb200_ctx *c, int mode, const double *d_pos, const doub
     }
     d_dlj = c->d_glj;
   }
-  launch_cell_build(c, d_pos, false, st);
+  launch_cell_build(c, d_pos, false, false, st);
   const size_t smem = sizeof(double) * nt4;
   if (mode == DERIV_PARAMS)
     k_deriv_fp64<DERIV_PARAMS><<<blocks, 128, smem, st>>>(
@@ -1447,7 +1454,9 @@ struct NoAllocLayout {  // byte offsets inside the scratch array
   static constexpr size_t smeta = align256(spos32 + sizeof(float4) * kNoAllocAtoms);
   static constexpr size_t facc = align256(smeta + sizeof(int2) * kNoAllocAtoms);
   static constexpr size_t red = align256(facc + sizeof(unsigned long long) * 3 * kNoAllocAtoms);
-  static constexpr size_t lj32 = align256(red + sizeof(double) * kRedBlocks * ACC_MV);
+  static constexpr size_t rel_lo = align256(red + sizeof(double) * kRedBlocks * ACC_MV);
+  static constexpr size_t spos_lo = align256(rel_lo + sizeof(float4) * kNoAllocAtoms);
+  static constexpr size_t lj32 = align256(spos_lo + sizeof(float4) * kNoAllocAtoms);
   static constexpr size_t pairs = align256(lj32 + sizeof(float4) * kMaxTypes * kMaxTypes);
   static constexpr size_t err = align256(pairs + sizeof(double));
   static constexpr size_t total = align256(err + sizeof(int));
@@ -1581,6 +1590,8 @@ extern "C" int pmb200_eval_noalloc(const pmb200_params *p, int n, const double *
   int *sidx = (int *)(base + Lo::sidx);
   float4 *rel32 = (float4 *)(base + Lo::rel32);
   float4 *spos32 = (float4 *)(base + Lo::spos32);
+  float4 *rel_lo = (float4 *)(base + Lo::rel_lo);
+  float4 *spos_lo = (float4 *)(base + Lo::spos_lo);
   int2 *smeta = (int2 *)(base + Lo::smeta);
   unsigned long long *facc = (unsigned long long *)(base + Lo::facc);
   double *red = (double *)(base + Lo::red);
@@ -1599,21 +1610,23 @@ extern "C" int pmb200_eval_noalloc(const pmb200_params *p, int n, const double *
   if (n > 0)
     k_cell_index<<<(n + 255) / 256, 256, 0, st>>>(n, d_pos, g, cell_of, count, slot, rel32,
                                                    nullptr, d_q, (float)(1.0 / std::sqrt(u)),
-                                                   err);
+                                                   err, d_energy ? rel_lo : nullptr);
   k_scan<<<1, 1024, 1024 * sizeof(int), st>>>(g.ncell, count, start);
   if (n > 0) k_scatter<<<(n + 255) / 256, 256, 0, st>>>(n, cell_of, slot, start, tmp);
   k_rank_gather<<<(g.ncell + 3) / 4, 128, 0, st>>>(g.ncell, start, tmp, rel32, nullptr, d_type,
-                                                    d_mol, sidx, spos32, nullptr, smeta);
+                                                    d_mol, sidx, spos32, nullptr, smeta,
+                                                    d_energy ? rel_lo : nullptr,
+                                                    d_energy ? spos_lo : nullptr);
   const size_t smem = mixed_smem_bytes(FORM_CUTOFF, ntypes, half.ncells);
   const int slots = mixed_cell_slots(d_energy != nullptr, n, g.ncell);
   if (d_energy)
     k_pair_mixed<FORM_CUTOFF, true, false, false><<<g.ncell * slots, 32, smem, st>>>(
         g, mc, half, ntypes, dlj, start, spos32, smeta, sidx, d_ex_start, d_ex, facc, n, err,
-        partial, pb, nullptr, slots);
+        partial, pb, nullptr, slots, spos_lo);
   else
     k_pair_mixed<FORM_CUTOFF, false, false, false><<<g.ncell * slots, 32, smem, st>>>(
         g, mc, half, ntypes, dlj, start, spos32, smeta, sidx, d_ex_start, d_ex, facc, n, err,
-        partial, pb, nullptr, slots);
+        partial, pb, nullptr, slots, spos_lo);
   if (n > 0)
     k_finalize<<<(n + 255) / 256, 256, 0, st>>>(n, facc, sidx, kFixInv / u, 0, d_forces);
   if (d_energy) {
@@ -1658,6 +1671,7 @@ struct pmb200_batch {
   int *d_cell_of = nullptr, *d_count = nullptr, *d_start = nullptr, *d_slot = nullptr;
   int *d_tmp = nullptr, *d_sidx = nullptr, *d_err = nullptr, *d_counter = nullptr;
   float4 *d_rel32 = nullptr, *d_spos32 = nullptr;
+  float4 *d_rel_lo = nullptr, *d_spos_lo = nullptr;
   int2 *d_smeta = nullptr;
   unsigned long long *d_facc = nullptr;
   double *d_partial = nullptr, *d_pairs = nullptr, *d_scratch_f = nullptr;
@@ -1746,7 +1760,7 @@ void batch_launch_pair(pmb200_batch *b, bool energy, bool virial, int grid, cuda
   k_pair_mixed_batch<F, E, V><<<grid, 32 * kWarps, 0, st>>>(                               \
       b->d_sys, b->d_tasks, b->ntasks, b->d_counter, b->d_st, b->d_lj32, b->d_start,       \
       b->d_spos32, b->d_smeta, b->d_sidx, b->d_ex_start, b->d_ex, b->d_facc, b->N,         \
-      b->d_partial, b->d_err)
+      b->d_partial, b->d_err, b->d_spos_lo)
   if (energy && virial) PMB_BATCH_LAUNCH(true, true);
   else if (energy) PMB_BATCH_LAUNCH(true, false);
   else if (virial) PMB_BATCH_LAUNCH(false, true);
@@ -1761,18 +1775,23 @@ int batch_launch_eval(pmb200_batch *b, const double *d_pos, double *d_forces, do
   const int N = b->N;
   const bool energy = (flags & PMB200_ENERGY) != 0;
   const bool virial = (flags & PMB200_VIRIAL) != 0;
+  // the FP32 coordinates' residuals feed the cutoff form's energy sums
+  const bool lo = energy && b->form == FORM_CUTOFF;
   BCK(cudaMemsetAsync(b->d_count, 0, sizeof(int) * b->C, st));
   if (N > 0)
     k_cell_index_batch<<<(N + 255) / 256, 256, 0, st>>>(N, d_pos, b->d_sys, b->d_atom_sys,
                                                         b->d_cell_of, b->d_count, b->d_slot,
-                                                        b->d_rel32, b->d_q, b->d_err);
+                                                        b->d_rel32, b->d_q, b->d_err,
+                                                        lo ? b->d_rel_lo : nullptr);
   k_scan<<<1, 1024, 1024 * sizeof(int), st>>>(b->C, b->d_count, b->d_start);
   if (N > 0)
     k_scatter<<<(N + 255) / 256, 256, 0, st>>>(N, b->d_cell_of, b->d_slot, b->d_start,
                                                  b->d_tmp);
   k_rank_gather<<<(b->C + 3) / 4, 128, 0, st>>>(b->C, b->d_start, b->d_tmp, b->d_rel32,
                                                   nullptr, b->d_type, b->d_mol, b->d_sidx,
-                                                  b->d_spos32, nullptr, b->d_smeta);
+                                                  b->d_spos32, nullptr, b->d_smeta,
+                                                  lo ? b->d_rel_lo : nullptr,
+                                                  lo ? b->d_spos_lo : nullptr);
   if (N > 0)
     BCK(cudaMemsetAsync(b->d_facc, 0, sizeof(unsigned long long) * 3 * (size_t)N, st));
   BCK(cudaMemsetAsync(b->d_counter, 0, sizeof(int), st));
@@ -1808,7 +1827,7 @@ int pmb200_batch_destroy(pmb200_batch *b) {
   dfree(b->d_ex_start); dfree(b->d_ex); dfree(b->d_st); dfree(b->d_lj32);
   dfree(b->d_cell_of); dfree(b->d_count); dfree(b->d_start); dfree(b->d_slot);
   dfree(b->d_tmp); dfree(b->d_sidx); dfree(b->d_err); dfree(b->d_counter);
-  dfree(b->d_rel32); dfree(b->d_spos32); dfree(b->d_smeta); dfree(b->d_facc);
+  dfree(b->d_rel32); dfree(b->d_spos32); dfree(b->d_rel_lo); dfree(b->d_spos_lo); dfree(b->d_smeta); dfree(b->d_facc);
   dfree(b->d_partial); dfree(b->d_pairs); dfree(b->d_scratch_f); dfree(b->d_tasks);
   dfree(b->d_rows_start); dfree(b->d_rows);
   if (b->ev0) cudaEventDestroy(b->ev0);
@@ -1920,6 +1939,8 @@ int pmb200_batch_create(pmb200_ctx *const *systems, int nsys, pmb200_batch **out
   cuda(dalloc(b->d_sidx, n1));
   cuda(dalloc(b->d_rel32, n1));
   cuda(dalloc(b->d_spos32, n1));
+  cuda(dalloc(b->d_rel_lo, n1));
+  cuda(dalloc(b->d_spos_lo, n1));
   cuda(dalloc(b->d_smeta, n1));
   cuda(dalloc(b->d_facc, 3 * n1));
   cuda(dalloc(b->d_scratch_f, 3 * n1));

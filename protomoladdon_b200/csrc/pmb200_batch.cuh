@@ -36,7 +36,7 @@ __global__ void k_cell_index_batch(int N, const double *__restrict__ pos,
                                    const int *__restrict__ atom_sys, int *__restrict__ cell_of,
                                    int *__restrict__ cell_count, int *__restrict__ slot,
                                    float4 *__restrict__ rel32, const double *__restrict__ q,
-                                   int *__restrict__ err) {
+                                   int *__restrict__ err, float4 *__restrict__ rel_lo) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   const BatchSys &b = sys[atom_sys[i]];
@@ -47,8 +47,12 @@ __global__ void k_cell_index_batch(int N, const double *__restrict__ pos,
   cell_of[i] = cid;
   slot[i] = atomicAdd(&cell_count[cid], 1);
   const double inv = 1.0 / b.g.unit;
-  rel32[i] = make_float4((float)(r[0] * inv), (float)(r[1] * inv), (float)(r[2] * inv),
-                         (float)q[i] * b.qscale32);
+  const double v[3] = {r[0] * inv, r[1] * inv, r[2] * inv};
+  const float h[3] = {(float)v[0], (float)v[1], (float)v[2]};
+  rel32[i] = make_float4(h[0], h[1], h[2], (float)q[i] * b.qscale32);
+  if (rel_lo)  // the FP32 coordinates' rounding residuals (energy evaluations)
+    rel_lo[i] = make_float4((float)(v[0] - (double)h[0]), (float)(v[1] - (double)h[1]),
+                            (float)(v[2] - (double)h[2]), 0.f);
 }
 
 // Persistent pair kernel: each block takes tasks from a global counter until
@@ -62,7 +66,8 @@ k_pair_mixed_batch(const BatchSys *__restrict__ sys, const int4 *__restrict__ ta
                    const float4 *__restrict__ spos, const int2 *__restrict__ smeta,
                    const int *__restrict__ sidx, const int *__restrict__ ex_start,
                    const int2 *__restrict__ ex, unsigned long long *__restrict__ facc, int N,
-                   double *__restrict__ partial, int *__restrict__ err) {
+                   double *__restrict__ partial, int *__restrict__ err,
+                   const float4 *__restrict__ spos_lo) {
   __shared__ float4 s_lj[kMaxTypes * kMaxTypes];
   __shared__ MixedWarpSmem s_w[kWarps];
   __shared__ unsigned short s_st[kMaxHalfCells];
@@ -100,7 +105,7 @@ k_pair_mixed_batch(const BatchSys *__restrict__ sys, const int4 *__restrict__ ta
         s_sys.g, s_sys.mc, s_st, s_sys.st_n, tk.z * kWarps + warp, kWarps * tk.w,
         s_sys.ntypes, s_lj, tk.y, start + s_sys.cell0, spos, smeta, sidx, ex_start, ex, facc,
         N, partial + ((size_t)t * kWarps + warp) * kNacc, s_sys.pb, nullptr, s_w[warp], err,
-        (kEnergy && kForm == FORM_CUTOFF) ? s_pd + warp * 3 * kBatch : nullptr);
+        (kEnergy && kForm == FORM_CUTOFF) ? s_pd + warp * 3 * kBatch : nullptr, spos_lo);
     __syncthreads();  // s_task and the staged system are reused
   }
 }

@@ -210,7 +210,8 @@ __global__ void k_cell_index(int n, const double *__restrict__ pos, GridParams g
                              int *__restrict__ cell_of, int *__restrict__ cell_count,
                              int *__restrict__ slot, float4 *__restrict__ rel32,
                              double4 *__restrict__ rel64, const double *__restrict__ q,
-                             float qscale32, int *__restrict__ err) {
+                             float qscale32, int *__restrict__ err,
+                             float4 *__restrict__ rel_lo) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   int c[3];
@@ -222,8 +223,13 @@ __global__ void k_cell_index(int n, const double *__restrict__ pos, GridParams g
   double qi = q[i];
   if (rel32) {
     const double inv = 1.0 / g.unit;
-    rel32[i] = make_float4((float)(r[0] * inv), (float)(r[1] * inv), (float)(r[2] * inv),
-                           (float)qi * qscale32);
+    const double v[3] = {r[0] * inv, r[1] * inv, r[2] * inv};
+    const float h[3] = {(float)v[0], (float)v[1], (float)v[2]};
+    rel32[i] = make_float4(h[0], h[1], h[2], (float)qi * qscale32);
+    // the FP32 coordinates' rounding residuals (energy evaluations)
+    if (rel_lo)
+      rel_lo[i] = make_float4((float)(v[0] - (double)h[0]), (float)(v[1] - (double)h[1]),
+                              (float)(v[2] - (double)h[2]), 0.f);
   }
   if (rel64) rel64[i] = make_double4(r[0], r[1], r[2], qi);
 }
@@ -271,7 +277,8 @@ __global__ void k_rank_gather(int ncell, const int *__restrict__ start,
                               const double4 *__restrict__ rel64, const int *__restrict__ type,
                               const int *__restrict__ mol, int *__restrict__ sidx,
                               float4 *__restrict__ spos32, double4 *__restrict__ spos64,
-                              int2 *__restrict__ smeta) {
+                              int2 *__restrict__ smeta, const float4 *__restrict__ rel_lo,
+                              float4 *__restrict__ spos_lo) {
   const int lane = threadIdx.x & 31;
   const int cell = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (cell >= ncell) return;
@@ -284,6 +291,7 @@ __global__ void k_rank_gather(int ncell, const int *__restrict__ start,
     sidx[d] = me;
     if (spos32) spos32[d] = rel32[me];
     if (spos64) spos64[d] = rel64[me];
+    if (spos_lo) spos_lo[d] = rel_lo[me];
     smeta[d] = make_int2(type[me], mol[me]);
   }
 }
@@ -399,11 +407,12 @@ __device__ __forceinline__ void mixed_task(
     const int *__restrict__ ex_start, const int2 *__restrict__ ex,
     unsigned long long *__restrict__ facc, int n, double *__restrict__ partial_row,
     const PbcRef &pb, const double *__restrict__ com, MixedWarpSmem &sm,
-    int *__restrict__ err, double *__restrict__ s_pd) {
+    int *__restrict__ err, double *__restrict__ s_pd, const float4 *__restrict__ spos_lo) {
   const int lane = threadIdx.x & 31;
   // the energy of the cutoff form is summed from FP64 distances: kEnergy
   // launches also stage each j position, shifted into the i-cell frame, in
-  // FP64 (s_pd: this warp's 3 x kBatch doubles)
+  // FP64 (s_pd: this warp's 3 x kBatch doubles), rebuilt from the FP32
+  // coordinate and its rounding residual (spos_lo, sorted order)
   constexpr bool kExactE = kEnergy && kForm == FORM_CUTOFF;
   double *pdx = kExactE ? s_pd : nullptr;
   double *pdy = kExactE ? pdx + kBatch : nullptr, *pdz = kExactE ? pdx + 2 * kBatch : nullptr;
@@ -445,7 +454,13 @@ __device__ __forceinline__ void mixed_task(
     long long fx = 0, fy = 0, fz = 0;
     // FP64 Coulomb sums of the cutoff form (see kExactE)
     double eU = 0.0, eQ = 0.0, eR = 0.0;
-    const double pid_x = pi.x, pid_y = pi.y, pid_z = pi.z;
+    double pid_x = 0.0, pid_y = 0.0, pid_z = 0.0;
+    if (kExactE) {
+      const float4 li = spos_lo[i];
+      pid_x = (double)pi.x + (double)li.x;
+      pid_y = (double)pi.y + (double)li.y;
+      pid_z = (double)pi.z + (double)li.z;
+    }
     double Ri[3] = {0.0, 0.0, 0.0};
     if (kMolVir)
       for (int k = 0; k < 3; k++) Ri[k] = com[3 * (size_t)mi.y + k];
@@ -766,10 +781,11 @@ __device__ __forceinline__ void mixed_task(
           sm.pos[slot] = p;
           sm.meta[slot] = smeta[jg];
           sm.gidx[slot] = jg;
-          if (kExactE) {  // the shift added in FP64 (exact for these magnitudes)
-            pdx[slot] = (double)a.x + (double)sx;
-            pdy[slot] = (double)a.y + (double)sy;
-            pdz[slot] = (double)a.z + (double)sz;
+          if (kExactE) {  // coordinate, residual and shift added in FP64
+            const float4 lj = spos_lo[jg];
+            pdx[slot] = ((double)a.x + (double)lj.x) + (double)sx;
+            pdy[slot] = ((double)a.y + (double)lj.y) + (double)sy;
+            pdz[slot] = ((double)a.z + (double)lj.z) + (double)sz;
           }
         }
         const unsigned hm = __ballot_sync(0xffffffffu, keep && home_atom);
@@ -850,7 +866,7 @@ k_pair_mixed(GridParams g, MixedConsts mc, const HalfStencil st, int ntypes, con
              const int *__restrict__ ex_start, const int2 *__restrict__ ex,
              unsigned long long *__restrict__ facc, int n, int *__restrict__ err,
              double *__restrict__ partial, const PbcRef pb, const double *__restrict__ com,
-             int slots) {
+             int slots, const float4 *__restrict__ spos_lo) {
   extern __shared__ float4 s_dyn[];
   __shared__ MixedWarpSmem sm;
   __shared__ double s_pd[(kEnergy && kForm == FORM_CUTOFF) ? 3 * kBatch : 1];
@@ -868,7 +884,7 @@ k_pair_mixed(GridParams g, MixedConsts mc, const HalfStencil st, int ntypes, con
   mixed_task<kForm, kEnergy, kVirial, kMolVir>(
       g, mc, s_st, st.ncells, blockIdx.x % slots, slots, ntypes, s_lj, cell, start,
       spos, smeta, sidx, ex_start, ex, facc, n, partial + (size_t)blockIdx.x * kNacc, pb, com,
-      sm, err, s_pd);
+      sm, err, s_pd, spos_lo);
 }
 
 // Blocks per i-cell of a k_pair_mixed launch: 8 for forces-only launches

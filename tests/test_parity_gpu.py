@@ -286,3 +286,41 @@ def test_pinned_host_positions_equal_pageable(water648):
     f.close()
     assert np.array_equal(out[0][0], out[1][0])
     assert out[0][1:] == out[1][1:]
+
+
+@pytest.mark.parametrize("cellsize", [0.0, 3.4, 4.2, 7.0, 10.5, 16.0])
+def test_cell_sizes_keep_every_pair(cellsize):
+    """The mixed kernel drops a staged atom that lies beyond the cutoff of the
+    box around the chunk's i atoms.  At every cell size (rc/3 cells with 1 to 2
+    atoms, cells wider than the cutoff holding several 32-atom chunks and home
+    cells whose atoms can be farther apart than the cutoff) it must still find
+    the oracle's pair set and forces."""
+    s = water.water_box(11, rc=10.0, ron=9.0, seed=11)
+    f, e, v, _ = O.restate_eval(s, s["pos"], virial_mode=1)
+    ref_pairs = O.restate_count_pairs(s, s["pos"])
+    topo = PeriodicTopology.from_dict(s)
+    force = NonbondedCutoffB200SystemForce(s["ron"], s["rc_lj"], s["rc_coul"], s["rc_alg"],
+                                           precision="mixed", cellsize=cellsize)
+    F = np.zeros_like(s["pos"])
+    E = ScalarStructure(virial=True)
+    force.evaluate(topo, s["pos"], F, E)
+    pairs = force.last_pair_count()
+    force.close()
+    # the FP32 cutoff test may decide a pair within ~1e-7 of r = rc either way
+    assert abs(pairs - ref_pairs) <= 2, (pairs, ref_pairs)
+    assert rms_rel(F, f) <= 1e-5
+    # cutoff-form Coulomb energy from FP64 distances, LJ energy in FP32
+    assert abs(E[0] - e[0]) <= 1e-6 * abs(e[0])
+    assert abs(E[1] - e[1]) <= 1e-6 * abs(e[1])
+
+
+@pytest.mark.parametrize("fx", ["water423", "water648", "modified648"])
+def test_mixed_energies_relative(fx, request):
+    """The cutoff-form Coulomb energy of the mixed kernel is summed from FP64
+    distances: within 1e-6 of the reference's own value even on the small
+    lattice-start boxes (whose total cancels to ~1e-4 of the pair sum)."""
+    d = request.getfixturevalue(fx)
+    F, E, _ = run(d, "mixed")
+    e = d["ref_energies"]
+    assert abs(E[0] - e[0]) <= 1e-6 * abs(e[0])
+    assert abs(E[1] - e[1]) <= 1e-6 * abs(e[1])
