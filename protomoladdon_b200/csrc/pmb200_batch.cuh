@@ -78,6 +78,7 @@ k_pair_mixed_batch(const BatchSys *__restrict__ sys, const int4 *__restrict__ ta
   const int lane = threadIdx.x & 31;
   MixedWarpSmem &sm = s_w[threadIdx.x >> 5];
   for (int t = lane; t < kBatch; t += 32) sm.jf[0][t] = sm.jf[1][t] = sm.jf[2][t] = 0;
+  sm.fi[0][lane] = sm.fi[1][lane] = sm.fi[2][lane] = 0;
   int loaded = -1;
   for (;;) {
     if (threadIdx.x == 0) s_task = atomicAdd(counter, 1);

@@ -367,10 +367,14 @@ constexpr float kJScale = 262144.0f; // shared j-force quanta (2^-18) per cell-u
 constexpr int kJShift = 14;          // to the global 2^-32 quanta
 constexpr float kJLimit = 6.7e7f;    // per-contribution bound: 32 contributions fit int32
 constexpr float kJToGlobal = 16384.0f;  // 2^-18 quanta -> the accumulator's 2^-32 quanta
+#ifndef PMB200_SPREAD_COST
+#define PMB200_SPREAD_COST 25   // cost of a round of dealt pairs, in tenths of an own round
+#endif
 
 struct __align__(16) MixedWarpSmem {
   float4 pos[kBatch];                    // staged j atoms, shifted into the i-cell frame
-  int jf[3][kBatch];                     // per-batch j forces, int32 fixed point (2^-16)
+  int jf[3][kBatch];                     // per-batch j forces, int32 fixed point (2^-18)
+  int fi[3][32];                         // per-lane i forces of leftover pairs (2^-18)
   int2 meta[kBatch];                     // their (LJ type, molecule)
   int gidx[kBatch];                      // their sorted indices
   unsigned char list[kBatch / 2][32];    // per-lane in-range candidate indices
@@ -509,22 +513,35 @@ __device__ __forceinline__ void mixed_task(
           }
         }
       }
+      // lists are walked in two phases when that is cheaper: every lane first
+      // takes the first kmin entries of its own list (kmin = the shortest
+      // active list), then the remaining entries of the longer lists are
+      // dealt over the whole warp, so no lane idles while another finishes a
+      // long list; a round of dealt pairs (shuffled i data, shared i-force
+      // sums) is counted as 2.5 rounds of own pairs (the best of 1.5 to 4 on
+      // the 41k and 327k water boxes)
+      const int kmin = __reduce_min_sync(0xffffffffu, active ? cnt : 0x7fffffff);
       const int maxc = __reduce_max_sync(0xffffffffu, cnt);
       float px = 0.f, py = 0.f, pz = 0.f, pE = 0.f;
       float pw0 = 0.f, pw1 = 0.f, pw2 = 0.f, pw3 = 0.f, pw4 = 0.f, pw5 = 0.f;
       float pm0 = 0.f, pm1 = 0.f, pm2 = 0.f, pm3 = 0.f, pm4 = 0.f, pm5 = 0.f;
       int pc = 0;
-      for (int k = 0; k < maxc; k++) {
-        if (k >= cnt) continue;
-        const int t = sm.list[k][lane];
+      // One listed pair: staged j atom t and i atom (a4, moli, exclusion range
+      // elo_..ehi_, LJ row ti_, sorted index ii, FP64 position pix..piz,
+      // molecule centre rx..rz).  own: the lane's own atom (force summed in
+      // px..pz); otherwise the atom of lane src (force to its shared sums).
+      auto pair = [&](const int t, const bool own, const float4 a4, const int moli,
+                      const int elo_, const int ehi_, const int ti_, const size_t ii,
+                      const int src, const double pix, const double piy, const double piz,
+                      const double rx, const double ry, const double rz) {
         const float4 pj = sm.pos[t];
-        const float ddx = pj.x - pi.x, ddy = pj.y - pi.y, ddz = pj.z - pi.z;
+        const float ddx = pj.x - a4.x, ddy = pj.y - a4.y, ddz = pj.z - a4.z;
         const float r2 = fmaf(ddx, ddx, fmaf(ddy, ddy, ddz * ddz));
         const int2 mj = sm.meta[t];
         int kind = 0;
-        if (mj.y == mi.y) {
-          kind = excl_kind(ex, elo, ehi, sidx[sm.gidx[t]]);
-          if (kind == 2) continue;
+        if (mj.y == moli) {
+          kind = excl_kind(ex, elo_, ehi_, sidx[sm.gidx[t]]);
+          if (kind == 2) return;
         }
         // 1/r: hardware reciprocal square root refined by one Newton-Raphson
         // step for 1/sqrt(x).
@@ -537,7 +554,7 @@ __device__ __forceinline__ void mixed_task(
           // (OneAtomPair.h:62-105, OneAtomPairTwo.h:57-125)
           f = 0.0f;
           if (mc.swl.kind != SW_OFF) {
-            const float4 p = s_lj[ti + mj.x];
+            const float4 p = s_lj[ti_ + mj.x];
             const float A = kind == 1 ? p.z : p.x;
             const float B = kind == 1 ? p.w : p.y;
             const float r6 = r2inv * r2inv * r2inv;
@@ -551,11 +568,14 @@ __device__ __forceinline__ void mixed_task(
           if (mc.swc.kind != SW_OFF) {
             float qj = pj.w;
             if (kind == 1) qj *= mc.csf;
-            const float ec = pi.w * qj * rinv;
+            const float ec = a4.w * qj * rinv;
             float S, dS;
             switch_eval(mc.swc, r2, rinv, S, dS);
             f += fmaf(ec * r2inv, S, -ec * dS);
-            if (kEnergy) kU.add(qj * rinv * S);
+            if (kEnergy) {
+              if (own) kU.add(qj * rinv * S);
+              else accU += (double)a4.w * (double)(qj * rinv * S);
+            }
           }
         } else if constexpr (kForm != FORM_CUTOFF) {
           // real-space Ewald (NonbondedFullEwaldSystemForce.h:803-823):
@@ -575,10 +595,13 @@ __device__ __forceinline__ void mixed_task(
           } else {
             g = erfcf(x) * rinv;
           }
-          f = pi.w * qj * fmaf(mc.ea2pi, ex, g) * r2inv;
-          if (kEnergy) kU.add(qj * g);
+          f = a4.w * qj * fmaf(mc.ea2pi, ex, g) * r2inv;
+          if (kEnergy) {
+            if (own) kU.add(qj * g);
+            else accU += (double)a4.w * (double)(qj * g);
+          }
         } else {
-        const float4 p = s_lj[ti + mj.x];
+        const float4 p = s_lj[ti_ + mj.x];
         const float A = kind == 1 ? p.z : p.x;
         const float B = kind == 1 ? p.w : p.y;
         const float r6 = r2inv * r2inv * r2inv;
@@ -598,7 +621,7 @@ __device__ __forceinline__ void mixed_task(
         if (kind == 1) qj *= mc.csf;
         float fc = 0.f;
         if (r2 <= mc.rcc2) {  // C1 switched Coulomb
-          const float ec = pi.w * qj * rinv;
+          const float ec = a4.w * qj * rinv;
           const float dist = r2 * rinv;
           const float sv = 1.0f - dist * fmaf(-r2, mc.c05_3, mc.c15_1);
           const float sd = fmaf(dist, mc.c15_3, -mc.c15_1 * rinv);
@@ -608,16 +631,23 @@ __device__ __forceinline__ void mixed_task(
             // rounds each term by ~1e-7 of q_j / rc while the C1 energy of a
             // pair near the cutoff is far smaller); 1/r from the FP32 value
             // and one Newton-Raphson step in FP64
-            const double ex_ = pdx[t] - pid_x;
-            const double ey_ = pdy[t] - pid_y;
-            const double ez_ = pdz[t] - pid_z;
+            const double ex_ = pdx[t] - pix;
+            const double ey_ = pdy[t] - piy;
+            const double ez_ = pdz[t] - piz;
             const double r2d = fma(ex_, ex_, fma(ey_, ey_, ez_ * ez_));
             double rid = (double)rinv;
             rid = rid * fma(-0.5 * r2d, rid * rid, 1.5);
             const double qjd = (double)qj;
-            eU = fma(qjd, rid, eU);
-            eQ += qjd;
-            eR = fma(qjd, r2d, eR);
+            if (own) {
+              eU = fma(qjd, rid, eU);
+              eQ += qjd;
+              eR = fma(qjd, r2d, eR);
+            } else {  // another lane's atom: weighted by its charge here
+              const double qq = qjd * (double)a4.w;
+              accU = fma(qq, rid, accU);
+              accQ += qq;
+              accR = fma(qq, r2d, accR);
+            }
           }
         }
         f = flj + fc;
@@ -627,34 +657,54 @@ __device__ __forceinline__ void mixed_task(
         // force, virial and molecular virial sums run in the same units
         const float fq = f * kJScale;
         const float fxv = ddx * fq, fyv = ddy * fq, fzv = ddz * fq;
-        px -= fxv;
-        py -= fyv;
-        pz -= fzv;
+        if (own) {
+          px -= fxv;
+          py -= fyv;
+          pz -= fzv;
+        }
         // j force: int32 shared-memory quanta, or, for a contribution too
         // large for 32 of them to fit, straight into the int64 accumulator
-        if (fmaxf(fabsf(fxv), fmaxf(fabsf(fyv), fabsf(fzv))) <= kJLimit) {
+        const float fm = fmaxf(fabsf(fxv), fmaxf(fabsf(fyv), fabsf(fzv)));
+        if (fm <= kJLimit) {
           atomicAdd(&sm.jf[0][t], __float2int_rn(fxv));
           atomicAdd(&sm.jf[1][t], __float2int_rn(fyv));
           atomicAdd(&sm.jf[2][t], __float2int_rn(fzv));
         } else {
           // beyond the int64 accumulator's range (~2^31 cell units), or not
           // finite: the evaluation reports a device error
-          if (!(fmaxf(fabsf(fxv), fmaxf(fabsf(fyv), fabsf(fzv))) < 2.8e14f)) atomicOr(err, 2);
+          if (!(fm < 2.8e14f)) atomicOr(err, 2);
           const size_t jg = (size_t)sm.gidx[t];
           atomicAdd(&facc[jg], (unsigned long long)__float2ll_rn(fxv * kJToGlobal));
           atomicAdd(&facc[(size_t)n + jg], (unsigned long long)__float2ll_rn(fyv * kJToGlobal));
           atomicAdd(&facc[2 * (size_t)n + jg],
                     (unsigned long long)__float2ll_rn(fzv * kJToGlobal));
         }
+        if (!own) {
+          // i force of another lane's atom: int32 shared quanta (at most
+          // kBatch / 2 contributions per lane and batch, each within half
+          // of kJLimit), else straight into the int64 accumulator
+          if (fm <= 0.5f * kJLimit) {
+            atomicAdd(&sm.fi[0][src], -__float2int_rn(fxv));
+            atomicAdd(&sm.fi[1][src], -__float2int_rn(fyv));
+            atomicAdd(&sm.fi[2][src], -__float2int_rn(fzv));
+          } else {
+            atomicAdd(&facc[ii], (unsigned long long)__float2ll_rn(-fxv * kJToGlobal));
+            atomicAdd(&facc[(size_t)n + ii], (unsigned long long)__float2ll_rn(-fyv * kJToGlobal));
+            atomicAdd(&facc[2 * (size_t)n + ii],
+                      (unsigned long long)__float2ll_rn(-fzv * kJToGlobal));
+          }
+        }
         if (kEnergy) pc++;
         if (kVirial) {
           pw0 = fmaf(fxv, ddx, pw0); pw1 = fmaf(fxv, ddy, pw1); pw2 = fmaf(fxv, ddz, pw2);
           pw3 = fmaf(fyv, ddy, pw3); pw4 = fmaf(fyv, ddz, pw4); pw5 = fmaf(fzv, ddz, pw5);
-          if (kMolVir && mj.y != mi.y) {
+          if (kMolVir && mj.y != moli) {
             // ScalarStructure::addVirial(fij, diff, comDiff): comDiff is the
             // minimal image of the two molecule centres (FP64), in cell units
             double cd[3];
-            for (int q = 0; q < 3; q++) cd[q] = com[3 * (size_t)mj.y + q] - Ri[q];
+            cd[0] = com[3 * (size_t)mj.y] - rx;
+            cd[1] = com[3 * (size_t)mj.y + 1] - ry;
+            cd[2] = com[3 * (size_t)mj.y + 2] - rz;
             ref_min_image(pb, cd);
             const float cx_ = (float)(cd[0] * inv_unit), cy_ = (float)(cd[1] * inv_unit),
                         cz_ = (float)(cd[2] * inv_unit);
@@ -662,6 +712,63 @@ __device__ __forceinline__ void mixed_task(
             pm3 = fmaf(fyv, cy_, pm3); pm4 = fmaf(fyv, cz_, pm4); pm5 = fmaf(fzv, cz_, pm5);
           }
         }
+      };
+      int left = active ? cnt - kmin : 0;
+      int linc = left;  // inclusive prefix of the leftover counts
+      for (int off = 1; off < 32; off <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, linc, off);
+        if (lane >= off) linc += v;
+      }
+      int ltot = __shfl_sync(0xffffffffu, linc, 31);
+      if (10 * (maxc - kmin) <= PMB200_SPREAD_COST * ((ltot + 31) >> 5)) {
+        ltot = 0;  // one phase: each lane walks its whole list
+        left = 0;
+      }
+      // (idle lanes, past the chunk's atoms, have no list: they skip phase 1)
+      const int kown = active ? cnt - left : 0;
+      for (int k = 0; k < kown; k++)
+        pair(sm.list[k][lane], true, pi, mi.y, elo, ehi, ti, (size_t)i, lane, pid_x, pid_y,
+             pid_z, Ri[0], Ri[1], Ri[2]);
+      for (int base = 0; base < ltot; base += 32) {
+        const int e = base + lane;
+        int src = 0;  // the lane whose leftovers hold entry e
+        for (int step = 16; step > 0; step >>= 1) {
+          const int v = __shfl_sync(0xffffffffu, linc, src + step - 1);
+          if (v <= e) src += step;
+        }
+        const int k = kmin + e - (__shfl_sync(0xffffffffu, linc, src) -
+                                  __shfl_sync(0xffffffffu, left, src));
+        float4 a4;
+        a4.x = __shfl_sync(0xffffffffu, pi.x, src);
+        a4.y = __shfl_sync(0xffffffffu, pi.y, src);
+        a4.z = __shfl_sync(0xffffffffu, pi.z, src);
+        a4.w = __shfl_sync(0xffffffffu, pi.w, src);
+        const int moli = __shfl_sync(0xffffffffu, mi.y, src);
+        const int elo_ = __shfl_sync(0xffffffffu, elo, src);
+        const int ehi_ = __shfl_sync(0xffffffffu, ehi, src);
+        const int ti_ = __shfl_sync(0xffffffffu, ti, src);
+        const int ii = __shfl_sync(0xffffffffu, i, src);
+        double pix = 0.0, piy = 0.0, piz = 0.0, rx = 0.0, ry = 0.0, rz = 0.0;
+        if (kExactE) {
+          pix = __shfl_sync(0xffffffffu, pid_x, src);
+          piy = __shfl_sync(0xffffffffu, pid_y, src);
+          piz = __shfl_sync(0xffffffffu, pid_z, src);
+        }
+        if (kMolVir) {
+          rx = __shfl_sync(0xffffffffu, Ri[0], src);
+          ry = __shfl_sync(0xffffffffu, Ri[1], src);
+          rz = __shfl_sync(0xffffffffu, Ri[2], src);
+        }
+        if (e < ltot)
+          pair(sm.list[k][src], false, a4, moli, elo_, ehi_, ti_, (size_t)ii, src, pix, piy,
+               piz, rx, ry, rz);
+      }
+      if (ltot > 0) {  // the shared i-force sums of the leftovers, per lane
+        __syncwarp();
+        fx += (long long)sm.fi[0][lane] << kJShift;
+        fy += (long long)sm.fi[1][lane] << kJShift;
+        fz += (long long)sm.fi[2][lane] << kJShift;
+        sm.fi[0][lane] = sm.fi[1][lane] = sm.fi[2][lane] = 0;
       }
       fx += __float2ll_rn(px * kJToGlobal);
       fy += __float2ll_rn(py * kJToGlobal);
@@ -859,7 +966,7 @@ constexpr int kMaxCellSlots = 8;
 
 
 template <int kForm, bool kEnergy, bool kVirial, bool kMolVir>
-__global__ void __launch_bounds__(32, kVirial ? 1 : (kEnergy ? 20 : 27))
+__global__ void __launch_bounds__(32, kVirial ? 1 : (kEnergy ? 19 : 26))
 k_pair_mixed(GridParams g, MixedConsts mc, const HalfStencil st, int ntypes, const float4 *__restrict__ lj32,
              const int *__restrict__ start, const float4 *__restrict__ spos,
              const int2 *__restrict__ smeta, const int *__restrict__ sidx,
@@ -878,6 +985,7 @@ k_pair_mixed(GridParams g, MixedConsts mc, const HalfStencil st, int ntypes, con
   for (int k = lane; k < nlj; k += 32) s_lj[k] = lj32[k];
   for (int k = lane; k < st.ncells; k += 32) s_st[k] = st.off[k];
   for (int t = lane; t < kBatch; t += 32) sm.jf[0][t] = sm.jf[1][t] = sm.jf[2][t] = 0;
+  sm.fi[0][lane] = sm.fi[1][lane] = sm.fi[2][lane] = 0;
   __syncwarp();
   const int cell = blockIdx.x / slots;
   if (cell >= g.ncell) return;  // uniform per block
