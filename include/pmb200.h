@@ -326,7 +326,7 @@ int pmb200_update_params(pmb200_ctx *ctx, const double *q_scaled, const double *
  * d_out[nsys][20] receives each system's {COULOMB, LENNARDJONES, virial 9,
  * molecular virial 9 (zero: not offered)}.  The schedule (stencil parts per
  * cell 1..8, task order 0 = by system / 1 = largest estimated cost first,
- * persistent blocks per SM, 0 = as many as fit) is set directly or chosen
+ * persistent one-warp blocks per SM, 0 = as many as fit) is set directly or chosen
  * by pmb200_batch_autotune, which times every candidate on the given
  * positions (reps timed launches each) and keeps the fastest; sched[4] =
  * {parts, order, blocks per SM, tasks}. */

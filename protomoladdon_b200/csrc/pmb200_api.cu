@@ -1681,6 +1681,8 @@ struct pmb200_batch {
   // largest first), persistent blocks per SM
   int parts = 1, order = 1, bpsm = 0, max_bpsm = 1, nsm = 1;
   int occ[4] = {1, 1, 1, 1};  // resident blocks per SM per variant (energy | virial << 1)
+  int lj_max = 0;             // largest LJ table (records) of any system
+  size_t smem = 0;            // dynamic shared memory of the pair kernel
   // graph of one evaluation (pmb200_batch_eval_device with a stream)
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
@@ -1741,7 +1743,7 @@ int batch_build_tasks(pmb200_batch *b) {
   if (b->ntasks < T || !b->d_tasks) {
     BCK(dalloc(b->d_tasks, (size_t)std::max(T, 1)));
     BCK(dalloc(b->d_rows, (size_t)std::max(T, 1)));
-    BCK(dalloc(b->d_partial, (size_t)std::max(T, 1) * kWarps * kNacc));
+    BCK(dalloc(b->d_partial, (size_t)std::max(T, 1) * kNacc));
   }
   b->ntasks = T;
   if (T > 0) {
@@ -1757,10 +1759,10 @@ int batch_build_tasks(pmb200_batch *b) {
 template <int F>
 void batch_launch_pair(pmb200_batch *b, bool energy, bool virial, int grid, cudaStream_t st) {
 #define PMB_BATCH_LAUNCH(E, V)                                                           \
-  k_pair_mixed_batch<F, E, V><<<grid, 32 * kWarps, 0, st>>>(                               \
+  k_pair_mixed_batch<F, E, V><<<grid, 32, b->smem, st>>>(                                   \
       b->d_sys, b->d_tasks, b->ntasks, b->d_counter, b->d_st, b->d_lj32, b->d_start,       \
       b->d_spos32, b->d_smeta, b->d_sidx, b->d_ex_start, b->d_ex, b->d_facc, b->N,         \
-      b->d_partial, b->d_err, b->d_spos_lo)
+      b->d_partial, b->d_err, b->d_spos_lo, b->lj_max)
   if (energy && virial) PMB_BATCH_LAUNCH(true, true);
   else if (energy) PMB_BATCH_LAUNCH(true, false);
   else if (virial) PMB_BATCH_LAUNCH(false, true);
@@ -1965,12 +1967,20 @@ int pmb200_batch_create(pmb200_ctx *const *systems, int nsys, pmb200_batch **out
     cuda(cudaMemcpy(b->d_lj32, lj.data(), sizeof(float4) * lj.size(), cudaMemcpyHostToDevice));
   cuda(cudaMemset(b->d_err, 0, sizeof(int)));
   if (rc) return done(rc);
+  // dynamic shared memory: the largest LJ table, then the largest stencil
+  int st_max = 0;
+  for (const BatchSys &y : b->h_sys) {
+    b->lj_max = std::max(b->lj_max, y.ntypes * y.ntypes);
+    st_max = std::max(st_max, y.st_n);
+  }
+  b->smem = sizeof(float4) * (size_t)b->lj_max +
+            ((sizeof(unsigned short) * (size_t)st_max + 15) & ~(size_t)15);
   // persistent grid: resident blocks per SM of the pair kernel
   int dev_sm = 1;
   cuda(cudaDeviceGetAttribute(&dev_sm, cudaDevAttrMultiProcessorCount, b->device));
   auto fits = [&](auto kernel, int &out) {
     int o = 1;
-    cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kernel, 32 * kWarps, 0));
+    cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kernel, 32, b->smem));
     out = std::max(1, o);
   };
   // per (energy, virial) variant of the batch's form
@@ -2103,11 +2113,11 @@ int pmb200_batch_autotune(pmb200_batch *b, const double *d_pos, void *stream, in
   if (reps < 1) reps = 5;
   BCK(cudaSetDevice(b->device));
   cudaStream_t st = (cudaStream_t)stream;
-  const int parts_c[3] = {1, 2, 4};
+  const int parts_c[4] = {1, 2, 4, 8};
   const int bpsm_c[2] = {b->occ[0], std::max(1, b->occ[0] / 2)};
   float best = -1.0f;
   int bp = 1, bo = 1, bb = 0;
-  for (int pi = 0; pi < 3; pi++)
+  for (int pi = 0; pi < 4; pi++)
     for (int order = 0; order < 2; order++)
       for (int bi = 0; bi < (bpsm_c[1] != bpsm_c[0] ? 2 : 1); bi++) {
         int rc = pmb200_batch_set_schedule(b, parts_c[pi], order, bpsm_c[bi]);

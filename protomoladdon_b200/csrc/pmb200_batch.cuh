@@ -55,11 +55,14 @@ __global__ void k_cell_index_batch(int N, const double *__restrict__ pos,
                             (float)(v[2] - (double)h[2]), 0.f);
 }
 
-// Persistent pair kernel: each block takes tasks from a global counter until
-// the list is exhausted; a task's system parameters, stencil and LJ table are
-// staged in shared memory when the system changes.
+// Persistent pair kernel, one warp per block: each warp takes tasks (system,
+// i-cell, stencil part, parts) from a global counter until the list is
+// exhausted and never waits for another warp; a task's system parameters,
+// stencil and LJ table are staged in the warp's shared memory when the system
+// changes.  Dynamic shared memory: lj_max float4 LJ records, then st_max
+// stencil offsets (the largest of any system in the batch).
 template <int kForm, bool kEnergy, bool kVirial>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(32, (kEnergy || kVirial) ? 1 : 24)
 k_pair_mixed_batch(const BatchSys *__restrict__ sys, const int4 *__restrict__ tasks, int ntasks,
                    int *__restrict__ counter, const unsigned short *__restrict__ stencils,
                    const float4 *__restrict__ lj32, const int *__restrict__ start,
@@ -67,47 +70,42 @@ k_pair_mixed_batch(const BatchSys *__restrict__ sys, const int4 *__restrict__ ta
                    const int *__restrict__ sidx, const int *__restrict__ ex_start,
                    const int2 *__restrict__ ex, unsigned long long *__restrict__ facc, int N,
                    double *__restrict__ partial, int *__restrict__ err,
-                   const float4 *__restrict__ spos_lo) {
-  __shared__ float4 s_lj[kMaxTypes * kMaxTypes];
-  __shared__ MixedWarpSmem s_w[kWarps];
-  __shared__ unsigned short s_st[kMaxHalfCells];
+                   const float4 *__restrict__ spos_lo, int lj_max) {
+  extern __shared__ float4 s_dyn[];
+  __shared__ MixedWarpSmem sm;
   __shared__ BatchSys s_sys;
-  __shared__ int s_task;
-  __shared__ double s_pd[(kEnergy && kForm == FORM_CUTOFF) ? kWarps * 3 * kBatch : 1];
-  const int warp = threadIdx.x >> 5;
-  const int lane = threadIdx.x & 31;
-  MixedWarpSmem &sm = s_w[threadIdx.x >> 5];
+  __shared__ double s_pd[(kEnergy && kForm == FORM_CUTOFF) ? 3 * kBatch : 1];
+  float4 *s_lj = s_dyn;
+  unsigned short *s_st = reinterpret_cast<unsigned short *>(s_dyn + lj_max);
+  const int lane = threadIdx.x;
   for (int t = lane; t < kBatch; t += 32) sm.jf[0][t] = sm.jf[1][t] = sm.jf[2][t] = 0;
   sm.fi[0][lane] = sm.fi[1][lane] = sm.fi[2][lane] = 0;
   int loaded = -1;
   for (;;) {
-    if (threadIdx.x == 0) s_task = atomicAdd(counter, 1);
-    __syncthreads();
-    const int t = s_task;
-    if (t >= ntasks) break;  // uniform per block
+    int t = 0;
+    if (lane == 0) t = atomicAdd(counter, 1);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    if (t >= ntasks) break;  // uniform per warp
     const int4 tk = tasks[t];
     if (tk.x != loaded) {
       // stage the system: parameters (as 32-bit words), stencil, LJ table
+      __syncwarp();
       const int *src = reinterpret_cast<const int *>(&sys[tk.x]);
       int *dst = reinterpret_cast<int *>(&s_sys);
-      for (int k = threadIdx.x; k < (int)(sizeof(BatchSys) / sizeof(int)); k += blockDim.x)
-        dst[k] = src[k];
+      for (int k = lane; k < (int)(sizeof(BatchSys) / sizeof(int)); k += 32) dst[k] = src[k];
       const BatchSys &gs = sys[tk.x];
-      for (int k = threadIdx.x; k < gs.st_n; k += blockDim.x) s_st[k] = stencils[gs.st0 + k];
+      for (int k = lane; k < gs.st_n; k += 32) s_st[k] = stencils[gs.st0 + k];
       if (kForm == FORM_CUTOFF || kForm == FORM_GENERIC)
-        for (int k = threadIdx.x; k < gs.ntypes * gs.ntypes; k += blockDim.x)
-          s_lj[k] = lj32[gs.lj0 + k];
+        for (int k = lane; k < gs.ntypes * gs.ntypes; k += 32) s_lj[k] = lj32[gs.lj0 + k];
       loaded = tk.x;
-      __syncthreads();
+      __syncwarp();
     }
-    // the block's warps share the task: warp w takes the stencil entries
-    // part * kWarps + w + k * kWarps * parts
+    // the task's stencil entries: part + k * parts
     mixed_task<kForm, kEnergy, kVirial, false>(
-        s_sys.g, s_sys.mc, s_st, s_sys.st_n, tk.z * kWarps + warp, kWarps * tk.w,
-        s_sys.ntypes, s_lj, tk.y, start + s_sys.cell0, spos, smeta, sidx, ex_start, ex, facc,
-        N, partial + ((size_t)t * kWarps + warp) * kNacc, s_sys.pb, nullptr, s_w[warp], err,
-        (kEnergy && kForm == FORM_CUTOFF) ? s_pd + warp * 3 * kBatch : nullptr, spos_lo);
-    __syncthreads();  // s_task and the staged system are reused
+        s_sys.g, s_sys.mc, s_st, s_sys.st_n, tk.z, tk.w, s_sys.ntypes, s_lj, tk.y,
+        start + s_sys.cell0, spos, smeta, sidx, ex_start, ex, facc, N,
+        partial + (size_t)t * kNacc, s_sys.pb, nullptr, sm, err,
+        (kEnergy && kForm == FORM_CUTOFF) ? s_pd : nullptr, spos_lo);
   }
 }
 
@@ -142,8 +140,7 @@ __global__ void k_reduce_batch(int nsys, const int *__restrict__ rows_start,
   double acc = 0.0;  // lane k < ACC_MV sums slot k
   if (lane < ACC_MV)
     for (int r = rows_start[s]; r < rows_start[s + 1]; r++)
-      for (int w = 0; w < kWarps; w++)
-        acc += partial[((size_t)rows[r] * kWarps + w) * kNacc + lane];
+      acc += partial[(size_t)rows[r] * kNacc + lane];
   double v[ACC_MV];
 #pragma unroll
   for (int k = 0; k < ACC_MV; k++) v[k] = __shfl_sync(0xffffffffu, acc, k);

@@ -332,32 +332,34 @@ __device__ __forceinline__ int lanes_per_atom(int m) {
 // ---------------------------------------------------------------------------
 // Mixed-precision pair kernel (Newton's third law, half-shell stencil).
 //
-// One 4-warp block per i-cell.  The half-shell stencil rows (every cell pair
-// once; the home cell pairs i < j) are dealt to the block's warps round-robin.
+// Work unit: one warp, one i-cell and every nslots-th entry of the cell's
+// half-shell stencil (every cell pair once; the home cell pairs i < j).
+// Warps never wait for one another.
 //
 // Per warp: the cell's atoms are taken in chunks of at most 32 / L, each atom
 // served by L lanes that split the candidates by index.  Candidate j atoms
-// are staged in shared memory in batches of kBatch, already shifted into the
-// i-cell's frame (integer cell offsets in cell units, so no per-offset
-// rounding bias).  Each lane first scans the batch and compacts the indices
-// of its in-range partners into a private list, then walks its list (from a
-// lane-dependent starting point, so lanes rarely hit the same j at once):
-// the pair arithmetic runs on dense lanes instead of under a divergent
-// branch.
+// are staged in shared memory in batches of at most kBatch, already shifted
+// into the i-cell's frame (integer cell offsets in cell units, so no
+// per-offset rounding bias); atoms beyond the cutoff of the box around the
+// chunk's i atoms are not staged.  Each lane first scans the batch and
+// compacts the indices of its in-range partners into a private list; the
+// lists are then walked densely (the pair arithmetic never runs under a
+// divergent branch), the longer lists' tails dealt over the whole warp.
 //
 // Forces: the pair force on j is added to a per-batch int32 fixed-point
-// accumulator in shared memory (2^-16 cell-unit force quanta; integer
+// accumulator in shared memory (2^-18 cell-unit force quanta; integer
 // atomics, so the sum is independent of order) and flushed per batch into
 // the global int64 fixed-point accumulator facc (2^-32 quanta, sorted order,
-// [3][n]).  The force on i is summed in FP32 per batch, folded into an int64
-// register, combined over lanes and warps and added to facc once.  Every
-// integer sum is exact, so the result does not depend on scheduling.
+// [3][n]).  The force on i is summed in FP32 per batch (dealt pairs: int32
+// shared quanta), folded into an int64 register, combined over the atom's
+// lanes and added to facc once per warp.  Every integer sum is exact, so
+// the result does not depend on scheduling.
 //
 // Pair arithmetic is FP32 in cell units.  The Coulomb energy is carried as
-// three Kahan-compensated sums (q_j / r, q_j, q_j r^2) so that the C1
-// constants are applied once in FP64 at the end.
+// three per-atom sums (q_j / r, q_j, q_j r^2) so that the C1 constants are
+// applied once in FP64 at the end; the cutoff form takes them from FP64
+// distances, the other forms as Kahan-compensated FP32 sums.
 // ---------------------------------------------------------------------------
-constexpr int kWarps = 4;
 #ifndef PMB200_STAGE_BATCH
 #define PMB200_STAGE_BATCH 128
 #endif
