@@ -131,9 +131,9 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-def committed_traffic():
-    """Pair-kernel DRAM bytes per launch from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "pair_mixed_water41k.md")  # ncu summary
+def committed_traffic(name="pair_mixed_water41k.md"):
+    """Pair-kernel DRAM bytes per launch from a committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", name)  # ncu summary
     try:
         txt = open(path).read()
     except OSError:
@@ -680,7 +680,8 @@ def run_batch(args):
                                   "batched_speedup": t_loop / t_batch},
         "pair_kernel_ms": k_ms,
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak if peak else None, "traffic": None,
+                     "frac": achieved / peak if peak else None,
+                     "traffic": committed_traffic("pair_mixed_batch_512boxes.md"),
                      "peak_source": "FP32 FMA throughput measured in this run"},
         "e2e": {"value": pairs / statistics.mean(e2e) / 1e9, "unit": "Gpairs/s",
                 "ms_per_step": statistics.mean(e2e) * 1e3,
