@@ -1295,8 +1295,9 @@ int pmb200_last_pair_count(pmb200_ctx *c, long long *pairs) {
 }
 
 // SETTLE on the host (same algorithm as settle_water on the device).
-static void host_settle(const SettleParams &sp, const double *A0, const double *B0,
-                        const double *C0, double *A1, double *B1, double *C1) {
+static void host_settle(const SettleParams &sp, double inv_m, double inv_ra, const double *A0,
+                        const double *B0, const double *C0, double *A1, double *B1,
+                        double *C1) {
   auto cross = [](const double a[3], const double b[3], double o[3]) {
     o[0] = a[1] * b[2] - a[2] * b[1];
     o[1] = a[2] * b[0] - a[0] * b[2];
@@ -1306,13 +1307,12 @@ static void host_settle(const SettleParams &sp, const double *A0, const double *
     return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
   };
   auto unit = [&](double a[3]) {
-    const double r = std::sqrt(dot(a, a));
-    a[0] /= r; a[1] /= r; a[2] /= r;
+    const double s = 1.0 / std::sqrt(dot(a, a));
+    a[0] *= s; a[1] *= s; a[2] *= s;
   };
-  const double M = sp.mo + 2.0 * sp.mh;
   double com[3], a1[3], b1[3], c1[3], b0[3], c0[3], ex[3], ey[3], ez[3];
   for (int k = 0; k < 3; k++) {
-    com[k] = (sp.mo * A1[k] + sp.mh * B1[k] + sp.mh * C1[k]) / M;
+    com[k] = (sp.mo * A1[k] + sp.mh * B1[k] + sp.mh * C1[k]) * inv_m;
     a1[k] = A1[k] - com[k];
     b1[k] = B1[k] - com[k];
     c1[k] = C1[k] - com[k];
@@ -1327,7 +1327,7 @@ static void host_settle(const SettleParams &sp, const double *A0, const double *
   const double za1 = dot(ez, a1);
   const double xb1 = dot(ex, b1), yb1 = dot(ey, b1), zb1 = dot(ez, b1);
   const double xc1 = dot(ex, c1), yc1 = dot(ey, c1), zc1 = dot(ez, c1);
-  const double sphi = za1 / sp.ra, cphi = std::sqrt(1.0 - sphi * sphi);
+  const double sphi = za1 * inv_ra, cphi = std::sqrt(1.0 - sphi * sphi);
   const double spsi = (zb1 - zc1) / (2.0 * sp.rc * cphi), cpsi = std::sqrt(1.0 - spsi * spsi);
   const double ya2 = sp.ra * cphi, xb2 = -sp.rc * cpsi;
   const double t1 = -sp.rb * cphi, t2 = sp.rc * spsi * sphi;
@@ -1346,6 +1346,82 @@ static void host_settle(const SettleParams &sp, const double *A0, const double *
     B1[k] = com[k] + xb3 * ex[k] + yb3 * ey[k] + zb3 * ez[k];
     C1[k] = com[k] + xc3 * ex[k] + yc3 * ey[k] + zc3 * ez[k];
   }
+}
+
+// The same for kW waters at once, lane by lane: the loops over lanes
+// vectorise and the waters' dependency chains (seven square roots and
+// divisions each) overlap.
+constexpr int kW = 4;
+static void host_settle_w(const SettleParams &sp, double inv_m, double inv_ra,
+                          const double *const A0[kW], const double *const B0[kW],
+                          const double *const C0[kW], double *const A1[kW],
+                          double *const B1[kW], double *const C1[kW]) {
+#define PMB_LANES for (int l = 0; l < kW; l++)
+  double com[3][kW], a1[3][kW], b1[3][kW], c1[3][kW], b0[3][kW], c0[3][kW];
+  double ex[3][kW], ey[3][kW], ez[3][kW];
+  for (int k = 0; k < 3; k++)
+    PMB_LANES {
+      com[k][l] = (sp.mo * A1[l][k] + sp.mh * B1[l][k] + sp.mh * C1[l][k]) * inv_m;
+      a1[k][l] = A1[l][k] - com[k][l];
+      b1[k][l] = B1[l][k] - com[k][l];
+      c1[k][l] = C1[l][k] - com[k][l];
+      b0[k][l] = B0[l][k] - A0[l][k];
+      c0[k][l] = C0[l][k] - A0[l][k];
+    }
+  auto cross = [](const double a[3][kW], const double b[3][kW], double o[3][kW]) {
+    PMB_LANES {
+      o[0][l] = a[1][l] * b[2][l] - a[2][l] * b[1][l];
+      o[1][l] = a[2][l] * b[0][l] - a[0][l] * b[2][l];
+      o[2][l] = a[0][l] * b[1][l] - a[1][l] * b[0][l];
+    }
+  };
+  auto unit = [](double a[3][kW]) {
+    PMB_LANES {
+      const double s = 1.0 / std::sqrt(a[0][l] * a[0][l] + a[1][l] * a[1][l] + a[2][l] * a[2][l]);
+      a[0][l] *= s; a[1][l] *= s; a[2][l] *= s;
+    }
+  };
+  auto dot = [](const double a[3][kW], const double b[3][kW], double o[kW]) {
+    PMB_LANES o[l] = a[0][l] * b[0][l] + a[1][l] * b[1][l] + a[2][l] * b[2][l];
+  };
+  cross(b0, c0, ez);
+  cross(a1, ez, ex);
+  cross(ez, ex, ey);
+  unit(ex); unit(ey); unit(ez);
+  double xb0[kW], yb0[kW], xc0[kW], yc0[kW], za1[kW], xb1[kW], yb1[kW], zb1[kW], xc1[kW],
+      yc1[kW], zc1[kW];
+  dot(ex, b0, xb0); dot(ey, b0, yb0); dot(ex, c0, xc0); dot(ey, c0, yc0); dot(ez, a1, za1);
+  dot(ex, b1, xb1); dot(ey, b1, yb1); dot(ez, b1, zb1);
+  dot(ex, c1, xc1); dot(ey, c1, yc1); dot(ez, c1, zc1);
+  double ya2[kW], xb2[kW], yb2[kW], yc2[kW], sth[kW], cth[kW];
+  PMB_LANES {
+    const double sphi = za1[l] * inv_ra, cphi = std::sqrt(1.0 - sphi * sphi);
+    const double spsi = (zb1[l] - zc1[l]) / (2.0 * sp.rc * cphi);
+    const double cpsi = std::sqrt(1.0 - spsi * spsi);
+    ya2[l] = sp.ra * cphi;
+    xb2[l] = -sp.rc * cpsi;
+    const double t1 = -sp.rb * cphi, t2 = sp.rc * spsi * sphi;
+    yb2[l] = t1 - t2;
+    yc2[l] = t1 + t2;
+    const double al = xb2[l] * (xb0[l] - xc0[l]) + yb0[l] * yb2[l] + yc0[l] * yc2[l];
+    const double be = xb2[l] * (yc0[l] - yb0[l]) + xb0[l] * yb2[l] + xc0[l] * yc2[l];
+    const double ga = xb0[l] * yb1[l] - xb1[l] * yb0[l] + xc0[l] * yc1[l] - xc1[l] * yc0[l];
+    const double ab = al * al + be * be;
+    sth[l] = (al * ga - be * std::sqrt(ab - ga * ga)) / ab;
+    cth[l] = std::sqrt(1.0 - sth[l] * sth[l]);
+  }
+  PMB_LANES {
+    const double xa3 = -ya2[l] * sth[l], ya3 = ya2[l] * cth[l], za3 = za1[l];
+    const double xb3 = xb2[l] * cth[l] - yb2[l] * sth[l], yb3 = xb2[l] * sth[l] + yb2[l] * cth[l];
+    const double xc3 = -xb2[l] * cth[l] - yc2[l] * sth[l];
+    const double yc3 = -xb2[l] * sth[l] + yc2[l] * cth[l];
+    for (int k = 0; k < 3; k++) {
+      A1[l][k] = com[k][l] + xa3 * ex[k][l] + ya3 * ey[k][l] + za3 * ez[k][l];
+      B1[l][k] = com[k][l] + xb3 * ex[k][l] + yb3 * ey[k][l] + zb1[l] * ez[k][l];
+      C1[l][k] = com[k][l] + xc3 * ex[k][l] + yc3 * ey[k][l] + zc1[l] * ez[k][l];
+    }
+  }
+#undef PMB_LANES
 }
 
 int pmb200_host_kick_drift(int n, double *pos, double *vel, const double *forces,
@@ -1380,17 +1456,37 @@ int pmb200_host_kick_drift(int n, double *pos, double *vel, const double *forces
     sp.mo = mo; sp.mh = mh; sp.rc = rcv;
     sp.ra = 2.0 * mh * t / (mo + 2.0 * mh);
     sp.rb = t - sp.ra;
+    const double inv_m = 1.0 / (mo + 2.0 * mh), inv_ra = 1.0 / sp.ra;
+    const int ngroups = (nwater + kW - 1) / kW;  // kW waters per iteration
 #pragma omp parallel for schedule(static) if (nwater > 1024)
-    for (int w = 0; w < nwater; w++) {
-      const int a = widx[3 * w], b = widx[3 * w + 1], cc = widx[3 * w + 2];
-      host_settle(sp, op + 3 * (size_t)a, op + 3 * (size_t)b, op + 3 * (size_t)cc,
-                  pos + 3 * (size_t)a, pos + 3 * (size_t)b, pos + 3 * (size_t)cc);
-      const int at3[3] = {a, b, cc};
-      for (int m = 0; m < 3; m++)
-        for (int k = 0; k < 3; k++) {
-          const size_t q = 3 * (size_t)at3[m] + k;
-          vel[q] = (pos[q] - op[q]) * inv_h;
+    for (int gidx = 0; gidx < ngroups; gidx++) {
+      const int w0 = gidx * kW, wn = std::min(kW, nwater - w0);
+      if (wn == kW) {
+        const double *A0[kW], *B0[kW], *C0[kW];
+        double *A1[kW], *B1[kW], *C1[kW];
+        for (int l = 0; l < kW; l++) {
+          const int *wi = widx + 3 * (w0 + l);
+          A0[l] = op + 3 * (size_t)wi[0]; B0[l] = op + 3 * (size_t)wi[1];
+          C0[l] = op + 3 * (size_t)wi[2];
+          A1[l] = pos + 3 * (size_t)wi[0]; B1[l] = pos + 3 * (size_t)wi[1];
+          C1[l] = pos + 3 * (size_t)wi[2];
         }
+        host_settle_w(sp, inv_m, inv_ra, A0, B0, C0, A1, B1, C1);
+      } else {
+        for (int l = 0; l < wn; l++) {
+          const int *wi = widx + 3 * (w0 + l);
+          host_settle(sp, inv_m, inv_ra, op + 3 * (size_t)wi[0], op + 3 * (size_t)wi[1],
+                      op + 3 * (size_t)wi[2], pos + 3 * (size_t)wi[0],
+                      pos + 3 * (size_t)wi[1], pos + 3 * (size_t)wi[2]);
+        }
+      }
+      // velocities from the constrained displacement
+      for (int l = 0; l < wn; l++)
+        for (int m = 0; m < 3; m++)
+          for (int k = 0; k < 3; k++) {
+            const size_t q = 3 * (size_t)widx[3 * (w0 + l) + m] + k;
+            vel[q] = (pos[q] - op[q]) * inv_h;
+          }
     }
   }
   return PMB200_OK;
