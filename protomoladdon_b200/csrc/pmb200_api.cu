@@ -819,7 +819,7 @@ int pmb200_set_box(pmb200_ctx *c, const double e1[3], const double e2[3], const 
   if (c->ncell_alloc < g.ncell) {
     CK(dalloc(c->d_count, (size_t)g.ncell));
     CK(dalloc(c->d_start, (size_t)g.ncell + 1));
-    CK(dalloc(c->d_partial, (size_t)g.ncell * kMaxCellSlots * kNacc));
+    CK(dalloc(c->d_partial, (size_t)g.ncell * kEnergyCellSlots * kNacc));
     c->ncell_alloc = g.ncell;
   }
   // constants
@@ -1541,7 +1541,7 @@ struct NoAllocLayout {  // byte offsets inside the scratch array
   static constexpr size_t start = align256(count + sizeof(int) * kNoAllocCells);
   static constexpr size_t partial = align256(start + sizeof(int) * (kNoAllocCells + 1));
   static constexpr size_t cell_of =
-      align256(partial + sizeof(double) * kNoAllocCells * kMaxCellSlots * kNacc);
+      align256(partial + sizeof(double) * kNoAllocCells * kEnergyCellSlots * kNacc);
   static constexpr size_t slot = align256(cell_of + sizeof(int) * kNoAllocAtoms);
   static constexpr size_t tmp = align256(slot + sizeof(int) * kNoAllocAtoms);
   static constexpr size_t sidx = align256(tmp + sizeof(int) * kNoAllocAtoms);

@@ -22,7 +22,7 @@ namespace pmb200 {
 
 constexpr int kMaxRows = 64;          // stencil rows (dy, dz), passed by value
 constexpr int kMaxTypes = 16;         // LJ types held in shared memory
-constexpr int kNacc = 32;             // per-warp accumulator slots
+constexpr int kNacc = 18;             // slots per partial-sum row (ACC_MV)
 constexpr double kFixScale = 4294967296.0;          // 2^32 per force unit
 constexpr double kFixInv = 1.0 / 4294967296.0;
 
@@ -38,6 +38,7 @@ enum {
   ACC_PAIRS = 17,
   ACC_MV = 18,  // number of slots in use
 };
+static_assert(kNacc >= ACC_MV, "partial-sum rows hold every slot");
 
 struct Row {        // one (dy, dz) row of the neighbour-cell stencil
   int dy, dz, dxlo, dxhi;
@@ -965,6 +966,7 @@ __device__ __forceinline__ void mixed_task(
 // ~96 registers that still fit 20 without spills; the virial variants keep
 // the compiler's choice.
 constexpr int kMaxCellSlots = 8;
+constexpr int kEnergyCellSlots = 4;  // energy / virial launches (the ones with partial rows)
 
 
 template <int kForm, bool kEnergy, bool kVirial, bool kMolVir>
@@ -1001,7 +1003,8 @@ k_pair_mixed(GridParams g, MixedConsts mc, const HalfStencil st, int ntypes, con
 // when cells hold at most 18 atoms on average (measured on water boxes:
 // 15 atoms per cell 4% faster than 4; 24 per cell 5% slower), else 4.
 inline int mixed_cell_slots(bool energy_or_virial, int natoms, int ncell) {
-  return (!energy_or_virial && natoms <= 18LL * ncell) ? 8 : 4;
+  if (energy_or_virial) return kEnergyCellSlots;
+  return natoms <= 18LL * ncell ? kMaxCellSlots : 4;
 }
 
 // Dynamic shared memory of a k_pair_mixed launch.
