@@ -18,6 +18,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 namespace pmb200 {
 
 constexpr int kMaxRows = 64;          // stencil rows (dy, dz), passed by value
@@ -487,34 +489,41 @@ __device__ __forceinline__ void mixed_task(
         const float2 nx = make_float2(-pi.x, -pi.x), ny = make_float2(-pi.y, -pi.y),
                      nz = make_float2(-pi.z, -pi.z);
         unsigned char *lst = &sm.list[0][lane];
-        int t = sub;
-        // two candidates per step with packed FP32 (FADD2 / FMUL2 / FFMA2)
-        for (; t + L < nb; t += 2 * L) {
-          const float4 a = sm.pos[t], b = sm.pos[t + L];
-          const float2 dx = __fadd2_rn(make_float2(a.x, b.x), nx);
-          const float2 dy = __fadd2_rn(make_float2(a.y, b.y), ny);
-          const float2 dz = __fadd2_rn(make_float2(a.z, b.z), nz);
-          float2 r2 = __fmul2_rn(dz, dz);
-          r2 = __ffma2_rn(dy, dy, r2);
-          r2 = __ffma2_rn(dx, dx, r2);
-          if (r2.x <= mc.cut2 && (unsigned)(t - ex_lo) >= ex_n) {
-            lst[cnt * 32] = (unsigned char)t;
-            cnt++;
+        // the exclusion-range test only where the batch holds home-cell atoms
+        // (the i < j rule); the other batches scan without it
+        auto scan = [&](auto with_home) {
+          constexpr bool kHome = decltype(with_home)::value;
+          int t = sub;
+          // two candidates per step with packed FP32 (FADD2 / FMUL2 / FFMA2)
+          for (; t + L < nb; t += 2 * L) {
+            const float4 a = sm.pos[t], b = sm.pos[t + L];
+            const float2 dx = __fadd2_rn(make_float2(a.x, b.x), nx);
+            const float2 dy = __fadd2_rn(make_float2(a.y, b.y), ny);
+            const float2 dz = __fadd2_rn(make_float2(a.z, b.z), nz);
+            float2 r2 = __fmul2_rn(dz, dz);
+            r2 = __ffma2_rn(dy, dy, r2);
+            r2 = __ffma2_rn(dx, dx, r2);
+            if (r2.x <= mc.cut2 && (!kHome || (unsigned)(t - ex_lo) >= ex_n)) {
+              lst[cnt * 32] = (unsigned char)t;
+              cnt++;
+            }
+            if (r2.y <= mc.cut2 && (!kHome || (unsigned)(t + L - ex_lo) >= ex_n)) {
+              lst[cnt * 32] = (unsigned char)(t + L);
+              cnt++;
+            }
           }
-          if (r2.y <= mc.cut2 && (unsigned)(t + L - ex_lo) >= ex_n) {
-            lst[cnt * 32] = (unsigned char)(t + L);
-            cnt++;
+          if (t < nb) {
+            const float4 a = sm.pos[t];
+            const float dx = a.x - pi.x, dy = a.y - pi.y, dz = a.z - pi.z;
+            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            if (r2 <= mc.cut2 && (!kHome || (unsigned)(t - ex_lo) >= ex_n)) {
+              lst[cnt * 32] = (unsigned char)t;
+              cnt++;
+            }
           }
-        }
-        if (t < nb) {
-          const float4 a = sm.pos[t];
-          const float dx = a.x - pi.x, dy = a.y - pi.y, dz = a.z - pi.z;
-          const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-          if (r2 <= mc.cut2 && (unsigned)(t - ex_lo) >= ex_n) {
-            lst[cnt * 32] = (unsigned char)t;
-            cnt++;
-          }
-        }
+        };
+        if (home_hi > home_lo) scan(std::true_type{});
+        else scan(std::false_type{});
       }
       // lists are walked in two phases when that is cheaper: every lane first
       // takes the first kmin entries of its own list (kmin = the shortest
