@@ -575,7 +575,7 @@ __device__ __forceinline__ void mixed_task(
             float S, dS;
             switch_eval(mc.swl, r2, rinv, S, dS);
             f = fmaf(flj, S, -elj * dS);
-            if (kEnergy) pE += elj * S;
+            if (kEnergy) pE = fmaf(elj, S, pE);
           }
           if (mc.swc.kind != SW_OFF) {
             float qj = pj.w;
@@ -585,8 +585,9 @@ __device__ __forceinline__ void mixed_task(
             switch_eval(mc.swc, r2, rinv, S, dS);
             f += fmaf(ec * r2inv, S, -ec * dS);
             if (kEnergy) {
-              if (own) kU.add(qj * rinv * S);
-              else accU += (double)a4.w * (double)(qj * rinv * S);
+              const float eS = __fmul_rn(qj * rinv, S);
+              if (own) kU.add(eS);
+              else accU += (double)a4.w * (double)eS;
             }
           }
         } else if constexpr (kForm != FORM_CUTOFF) {
@@ -609,8 +610,9 @@ __device__ __forceinline__ void mixed_task(
           }
           f = a4.w * qj * fmaf(mc.ea2pi, ex, g) * r2inv;
           if (kEnergy) {
-            if (own) kU.add(qj * g);
-            else accU += (double)a4.w * (double)(qj * g);
+            const float eg = __fmul_rn(qj, g);
+            if (own) kU.add(eg);
+            else accU += (double)a4.w * (double)eg;
           }
         } else {
         const float4 p = s_lj[ti_ + mj.x];
@@ -627,18 +629,19 @@ __device__ __forceinline__ void mixed_task(
           const float sv = in ? (on ? mc.s1 * (c2 * c4) : 1.0f) : 0.0f;
           const float sd = (in && on) ? mc.s3 * fmaf(c2, c2, -c4) : 0.0f;
           flj = fmaf(flj, sv, -elj * sd);
-          elj = elj * sv;
+          elj = __fmul_rn(elj, sv);
         }
         float qj = pj.w;
         if (kind == 1) qj *= mc.csf;
-        float fc = 0.f;
-        if (r2 <= mc.rcc2) {  // C1 switched Coulomb
+        float fc;
+        {  // C1 switched Coulomb, branch-free (zero beyond its cutoff)
+          const bool inC = r2 <= mc.rcc2;
           const float ec = a4.w * qj * rinv;
           const float dist = r2 * rinv;
-          const float sv = 1.0f - dist * fmaf(-r2, mc.c05_3, mc.c15_1);
+          const float sv = fmaf(-dist, fmaf(-r2, mc.c05_3, mc.c15_1), 1.0f);
           const float sd = fmaf(dist, mc.c15_3, -mc.c15_1 * rinv);
-          fc = ec * fmaf(r2inv, sv, -sd);
-          if (kEnergy) {
+          fc = inC ? __fmul_rn(ec, fmaf(r2inv, sv, -sd)) : 0.f;
+          if (kEnergy && inC) {
             // q_j / r, q_j and q_j r^2 from the FP64 distance (the FP32 one
             // rounds each term by ~1e-7 of q_j / rc while the C1 energy of a
             // pair near the cutoff is far smaller); 1/r from the FP32 value
@@ -666,22 +669,28 @@ __device__ __forceinline__ void mixed_task(
         if (kEnergy) pE += elj;
         }
         // force on j in 2^-18 quanta (power-of-two scale: exact); the i
-        // force, virial and molecular virial sums run in the same units
+        // force, virial and molecular virial sums run in the same units.
+        // (Every product that meets a sum is rounded explicitly, through
+        // fmaf or __fmul_rn / __fsub_rn, so that no kernel instantiating this
+        // body contracts it differently: the batched and single-system
+        // kernels round every pair alike.)
         const float fq = f * kJScale;
         const float fxv = ddx * fq, fyv = ddy * fq, fzv = ddz * fq;
         if (own) {
-          px -= fxv;
-          py -= fyv;
-          pz -= fzv;
+          px = __fsub_rn(px, fxv);
+          py = __fsub_rn(py, fyv);
+          pz = __fsub_rn(pz, fzv);
         }
         // j force: int32 shared-memory quanta, or, for a contribution too
         // large for 32 of them to fit, straight into the int64 accumulator
         const float fm = fmaxf(fabsf(fxv), fmaxf(fabsf(fyv), fabsf(fzv)));
-        if (fm <= kJLimit) {
-          atomicAdd(&sm.jf[0][t], __float2int_rn(fxv));
-          atomicAdd(&sm.jf[1][t], __float2int_rn(fyv));
-          atomicAdd(&sm.jf[2][t], __float2int_rn(fzv));
-        } else {
+        // (the shared adds are unconditional, zero for a large contribution,
+        // so the common path has no branch)
+        const bool small = fm <= kJLimit;
+        atomicAdd(&sm.jf[0][t], small ? __float2int_rn(fxv) : 0);
+        atomicAdd(&sm.jf[1][t], small ? __float2int_rn(fyv) : 0);
+        atomicAdd(&sm.jf[2][t], small ? __float2int_rn(fzv) : 0);
+        if (!small) {
           // beyond the int64 accumulator's range (~2^31 cell units), or not
           // finite: the evaluation reports a device error
           if (!(fm < 2.8e14f)) atomicOr(err, 2);

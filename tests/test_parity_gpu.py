@@ -155,6 +155,19 @@ def test_errors_are_reported(water648):
     assert ei.value.code == _lib.PMB200_EUNSUPPORTED
 
 
+def test_coincident_atoms_are_reported(water648):
+    """Two atoms of different molecules at one position: the reference
+    divides by zero; the mixed kernel's pair force leaves the fixed-point
+    range and the evaluation reports a device error."""
+    d = dict(water648)
+    pos = d["pos"].copy()
+    pos[9] = pos[0]  # atom 9 belongs to another water than atom 0
+    assert d["mol"][9] != d["mol"][0]
+    with pytest.raises(PmbError) as ei:
+        run(d, "mixed", pos=pos)
+    assert ei.value.code == _lib.PMB200_EDEVICE
+
+
 def test_empty_system(water648):
     d = dict(water648)
     for k in ("type", "qscaled", "mol", "mass"):
