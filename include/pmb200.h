@@ -123,6 +123,30 @@ int pmb200_eval(pmb200_ctx *ctx, const double *pos, double *forces,
 int pmb200_eval_device(pmb200_ctx *ctx, const double *d_pos, double *d_forces,
                        double *d_out, unsigned flags, void *stream);
 
+/* Force decomposition over several GPUs, one process and one context per GPU,
+ * every context holding the same topology, box and positions: the
+ * replicated-data decomposition of the reference's parallel evaluation
+ * (NonbondedCutoffSystemForce::parallelEvaluate, protomol/src/protomol/force/
+ * nonbonded/NonbondedCutoffSystemForce.h:57-77, which deals contiguous runs
+ * of cell pairs to the ranks and sums the forces with MPI; here contiguous
+ * runs of i-cells).  Shard `shard` of `nshards` evaluates the half-shell pairs
+ * of the i-cells [ncell * shard / nshards, ncell * (shard + 1) / nshards)
+ * into d_facc[3n] (int64, overwritten): the forces in the library's fixed
+ * point, an opaque layout whose only use is an element-wise integer sum over
+ * the shards (an all-reduce with ncclInt64 / ncclSum, say), exact whatever
+ * the reduction order.  d_out[20] (overwritten when flags ask for it)
+ * receives the shard's share of the energies and virials, as for
+ * pmb200_eval_device; the caller sums these too.  pmb200_shard_finalize then
+ * adds the forces of the summed accumulator to d_forces[3n] (caller order,
+ * accumulated into, as pmb200_eval_device) using the cell order of this
+ * context's latest shard evaluation (the same on every shard: the cell build
+ * is deterministic).  The summed forces equal a single pmb200_eval_device
+ * bit for bit.  Mixed-precision contexts only. */
+int pmb200_shard_eval_device(pmb200_ctx *ctx, const double *d_pos, int shard, int nshards,
+                             long long *d_facc, double *d_out, unsigned flags, void *stream);
+int pmb200_shard_finalize(pmb200_ctx *ctx, const long long *d_facc, double *d_forces,
+                          void *stream);
+
 /* Waits for the context's work and reports device-side check failures. */
 int pmb200_sync(pmb200_ctx *ctx);
 

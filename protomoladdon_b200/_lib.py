@@ -48,7 +48,7 @@ EXPORTED = (
     "pmb200_batch_eval_device", "pmb200_batch_set_schedule", "pmb200_batch_get_schedule",
     "pmb200_batch_autotune", "pmb200_batch_set_kernel_timing", "pmb200_batch_last_kernel_ms",
     "pmb200_batch_pair_counts", "pmb200_create_pair", "pmb200_set_vacuum_domain",
-    "pmb200_batch_sync",
+    "pmb200_batch_sync", "pmb200_shard_eval_device", "pmb200_shard_finalize",
 )
 
 _P = ctypes.c_void_p
@@ -99,6 +99,8 @@ def lib():
     L.pmb200_set_box.argtypes = [_P, _P, _P, _P, _P]
     L.pmb200_eval.argtypes = [_P, _P, _P, _P, _P, _P, ctypes.c_uint]
     L.pmb200_eval_device.argtypes = [_P, _P, _P, _P, ctypes.c_uint, _P]
+    L.pmb200_shard_eval_device.argtypes = [_P, _P, _I, _I, _P, _P, ctypes.c_uint, _P]
+    L.pmb200_shard_finalize.argtypes = [_P, _P, _P, _P]
     L.pmb200_sync.argtypes = [_P]
     L.pmb200_leapfrog_device.argtypes = [_P, _P, _P, _P, _P, _D, _I, ctypes.c_uint, _P]
     L.pmb200_last_pair_count.argtypes = [_P, ctypes.POINTER(ctypes.c_longlong)]

@@ -297,20 +297,25 @@ int ensure_atom_buffers(pmb200_ctx *c) {
   return PMB200_OK;
 }
 
-// The pair kernels for the flags asked for (template instances per form).
+// The pair kernels for the flags asked for (template instances per form),
+// over the i-cells [cell0, cell0 + ncells) (all by default) into the fixed-
+// point accumulator facc (the context's by default).
 template <int F>
-void launch_pair_mixed(pmb200_ctx *c, unsigned flags, cudaStream_t st) {
+void launch_pair_mixed(pmb200_ctx *c, unsigned flags, cudaStream_t st, int cell0 = 0,
+                       int ncells = -1, unsigned long long *facc = nullptr) {
   const GridParams &g = c->g;
+  if (ncells < 0) ncells = g.ncell;
+  if (!facc) facc = c->d_facc;
   const bool energy = (flags & PMB200_ENERGY) != 0;
   const bool virial = (flags & (PMB200_VIRIAL | PMB200_MOLVIRIAL)) != 0;
   const bool molvir = (flags & PMB200_MOLVIRIAL) != 0;
   const size_t smem = mixed_smem_bytes(F, c->ntypes, c->half.ncells);
   const int slots = mixed_cell_slots(energy || virial, c->n, g.ncell);
 #define PMB_MIXED_LAUNCH(E, V, M)                                                          \
-  k_pair_mixed<F, E, V, M><<<g.ncell * slots, 32, smem, st>>>(                               \
+  k_pair_mixed<F, E, V, M><<<std::max(ncells, 1) * slots, 32, smem, st>>>(                 \
       g, c->mc, c->half, c->ntypes, c->d_lj32, c->d_start, c->d_spos32, c->d_smeta,         \
-      c->d_sidx, c->d_ex_start, c->d_ex, c->d_facc, c->n, c->d_err, c->d_partial, c->pb,    \
-      c->d_com, slots, c->d_spos_lo)
+      c->d_sidx, c->d_ex_start, c->d_ex, facc, c->n, c->d_err, c->d_partial, c->pb,         \
+      c->d_com, slots, c->d_spos_lo, ncells > 0 ? cell0 : g.ncell)
   if (molvir) PMB_MIXED_LAUNCH(true, true, true);
   else if (energy && virial) PMB_MIXED_LAUNCH(true, true, false);
   else if (energy) PMB_MIXED_LAUNCH(true, false, false);
@@ -893,6 +898,78 @@ int pmb200_eval_device(pmb200_ctx *c, const double *d_pos, double *d_forces, dou
   CK(cudaSetDevice(c->p.device));
   cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
   return launch_eval(c, d_pos, d_forces, d_out, flags, 1, st);
+}
+
+// Force decomposition: shard s of nshards takes the i-cells
+// [ncell * s / nshards, ncell * (s + 1) / nshards) of the half-shell walk.
+int pmb200_shard_eval_device(pmb200_ctx *c, const double *d_pos, int shard, int nshards,
+                             long long *d_facc, double *d_out, unsigned flags, void *stream) {
+  int rc = check_ready(c);
+  if (rc) return rc;
+  if (c->p.precision != PMB200_MIXED)
+    return fail(c, PMB200_EUNSUPPORTED, "sharded evaluation needs a mixed-precision context");
+  if (nshards < 1 || shard < 0 || shard >= nshards)
+    return fail(c, PMB200_EINVAL, "shard %d of %d", shard, nshards);
+  if ((flags & PMB200_MOLVIRIAL) && !c->have_mass)
+    return fail(c, PMB200_EINVAL, "molecular virial needs masses");
+  if (c->n > 0 && (!d_pos || !d_facc)) return fail(c, PMB200_EINVAL, "null device buffer");
+  if (flags && !d_out) return fail(c, PMB200_EINVAL, "null output buffer");
+  CK(cudaSetDevice(c->p.device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  const GridParams &g = c->g;
+  const int n = c->n;
+  const bool energy = (flags & PMB200_ENERGY) != 0;
+  const bool virial = (flags & (PMB200_VIRIAL | PMB200_MOLVIRIAL)) != 0;
+  const int lo = (int)((long long)g.ncell * shard / nshards);
+  const int hi = (int)((long long)g.ncell * (shard + 1) / nshards);
+  unsigned long long *facc = reinterpret_cast<unsigned long long *>(d_facc);
+  launch_cell_build(c, d_pos, true, energy && c->form == FORM_CUTOFF, st);
+  if ((flags & PMB200_MOLVIRIAL) && c->nmol > 0)
+    k_com<<<(c->nmol + 127) / 128, 128, 0, st>>>(c->nmol, c->d_mstart, c->d_matoms, c->d_mass,
+                                                  d_pos, c->d_com);
+  if (n > 0) CK(cudaMemsetAsync(facc, 0, sizeof(unsigned long long) * 3 * (size_t)n, st));
+  if (hi > lo) {
+    if (c->form == FORM_GENERIC) launch_pair_mixed<FORM_GENERIC>(c, flags, st, lo, hi - lo, facc);
+    else if (c->form == FORM_EWALD_POLY5)
+      launch_pair_mixed<FORM_EWALD_POLY5>(c, flags, st, lo, hi - lo, facc);
+    else if (c->form == FORM_EWALD_EXACT)
+      launch_pair_mixed<FORM_EWALD_EXACT>(c, flags, st, lo, hi - lo, facc);
+    else launch_pair_mixed<FORM_CUTOFF>(c, flags, st, lo, hi - lo, facc);
+  }
+  CK(cudaGetLastError());
+  if (energy || virial) {
+    if (hi > lo) {
+      // this shard's partial rows: one per (cell, slot) warp
+      const double rcc = c->p.cutoff_coul / g.unit;
+      const bool c1 = c->form == FORM_CUTOFF;
+      k_reduce1<<<kRedBlocks, 256, 0, st>>>((hi - lo) * mixed_cell_slots(true, n, g.ncell),
+                                            c->d_partial, c->d_red);
+      k_reduce2<<<1, 256, 0, st>>>(kRedBlocks, c->d_red, 1, 1.0, c1 ? 1.5 / rcc : 0.0,
+                                  c1 ? 0.5 / (rcc * rcc * rcc) : 0.0, d_out, c->d_pairs);
+    } else {
+      CK(cudaMemsetAsync(d_out, 0, sizeof(double) * 20, st));
+      CK(cudaMemsetAsync(c->d_pairs, 0, sizeof(double), st));
+    }
+    CK(cudaGetLastError());
+  }
+  return PMB200_OK;
+}
+
+int pmb200_shard_finalize(pmb200_ctx *c, const long long *d_facc, double *d_forces,
+                          void *stream) {
+  int rc = check_ready(c);
+  if (rc) return rc;
+  if (c->p.precision != PMB200_MIXED)
+    return fail(c, PMB200_EUNSUPPORTED, "sharded evaluation needs a mixed-precision context");
+  if (c->n > 0 && (!d_facc || !d_forces)) return fail(c, PMB200_EINVAL, "null device buffer");
+  CK(cudaSetDevice(c->p.device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  if (c->n > 0)
+    k_finalize<<<(c->n + 255) / 256, 256, 0, st>>>(
+        c->n, reinterpret_cast<const unsigned long long *>(d_facc), c->d_sidx,
+        kFixInv / c->g.unit, 1, d_forces);
+  CK(cudaGetLastError());
+  return PMB200_OK;
 }
 
 // Derivative kernels (FP64 pair arithmetic whatever the context's
@@ -1718,11 +1795,11 @@ extern "C" int pmb200_eval_noalloc(const pmb200_params *p, int n, const double *
   if (d_energy)
     k_pair_mixed<FORM_CUTOFF, true, false, false><<<g.ncell * slots, 32, smem, st>>>(
         g, mc, half, ntypes, dlj, start, spos32, smeta, sidx, d_ex_start, d_ex, facc, n, err,
-        partial, pb, nullptr, slots, spos_lo);
+        partial, pb, nullptr, slots, spos_lo, 0);
   else
     k_pair_mixed<FORM_CUTOFF, false, false, false><<<g.ncell * slots, 32, smem, st>>>(
         g, mc, half, ntypes, dlj, start, spos32, smeta, sidx, d_ex_start, d_ex, facc, n, err,
-        partial, pb, nullptr, slots, spos_lo);
+        partial, pb, nullptr, slots, spos_lo, 0);
   if (n > 0)
     k_finalize<<<(n + 255) / 256, 256, 0, st>>>(n, facc, sidx, kFixInv / u, 0, d_forces);
   if (d_energy) {

@@ -971,8 +971,8 @@ __device__ __forceinline__ void mixed_task(
   }
 }
 
-// One warp per block, `slots` blocks per i-cell (block b: cell b / slots,
-// stencil entries b % slots + k * slots), so a warp that finishes early
+// One warp per block, `slots` blocks per i-cell (block b: cell cell0 + b /
+// slots, stencil entries b % slots + k * slots), so a warp that finishes early
 // frees its slot for the next block instead of waiting for the cell's other
 // warps.  More slots mean more, shorter warps (better balance, more per-warp
 // setup); the host picks 8 for forces-only launches on sparse cells and 4
@@ -995,7 +995,7 @@ k_pair_mixed(GridParams g, MixedConsts mc, const HalfStencil st, int ntypes, con
              const int *__restrict__ ex_start, const int2 *__restrict__ ex,
              unsigned long long *__restrict__ facc, int n, int *__restrict__ err,
              double *__restrict__ partial, const PbcRef pb, const double *__restrict__ com,
-             int slots, const float4 *__restrict__ spos_lo) {
+             int slots, const float4 *__restrict__ spos_lo, int cell0) {
   extern __shared__ float4 s_dyn[];
   __shared__ MixedWarpSmem sm;
   __shared__ double s_pd[(kEnergy && kForm == FORM_CUTOFF) ? 3 * kBatch : 1];
@@ -1009,7 +1009,7 @@ k_pair_mixed(GridParams g, MixedConsts mc, const HalfStencil st, int ntypes, con
   for (int t = lane; t < kBatch; t += 32) sm.jf[0][t] = sm.jf[1][t] = sm.jf[2][t] = 0;
   sm.fi[0][lane] = sm.fi[1][lane] = sm.fi[2][lane] = 0;
   __syncwarp();
-  const int cell = blockIdx.x / slots;
+  const int cell = cell0 + (int)(blockIdx.x / slots);  // cells cell0.. (a shard's range)
   if (cell >= g.ncell) return;  // uniform per block
   mixed_task<kForm, kEnergy, kVirial, kMolVir>(
       g, mc, s_st, st.ncells, blockIdx.x % slots, slots, ntypes, s_lj, cell, start,

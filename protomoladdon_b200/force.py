@@ -245,6 +245,22 @@ class NonbondedCutoffB200SystemForce:
             self._ctx, _P(pos_ptr), _P(force_ptr), _P(out_ptr) if out_ptr else None,
             int(flags), _P(stream) if stream else None))
 
+    def shard_eval_device(self, topo, pos_ptr, shard, nshards, facc_ptr, out_ptr=None, flags=0,
+                          stream=None):
+        """Shard ``shard`` of ``nshards`` of one evaluation (its run of i-cells)
+        into the int64 fixed-point accumulator ``facc`` (3n, overwritten) and,
+        when flags ask, its share of the energies / virials into out (20);
+        sum both over the shards, then shard_finalize."""
+        self._ensure(topo)
+        self._check(_lib.lib().pmb200_shard_eval_device(
+            self._ctx, _P(pos_ptr), int(shard), int(nshards), _P(facc_ptr),
+            _P(out_ptr) if out_ptr else None, int(flags), _P(stream) if stream else None))
+
+    def shard_finalize(self, facc_ptr, force_ptr, stream=None):
+        """Adds the forces of a summed shard accumulator to ``force`` (3n)."""
+        self._check(_lib.lib().pmb200_shard_finalize(
+            self._ctx, _P(facc_ptr), _P(force_ptr), _P(stream) if stream else None))
+
     def leapfrog_device(self, topo, pos_ptr, vel_ptr, force_ptr, dt_fs, nsteps, out_ptr=None,
                         flags=0, stream=None):
         self._ensure(topo)
