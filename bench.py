@@ -567,6 +567,88 @@ BATCH_METRIC = ("Gpairs/s, 512 uneven water boxes: one persistent graph-captured
                 "launch (autotuned schedule) vs one launch per system")
 
 
+def run_sharded(args):
+    """--workload sharded: the 327,352-atom ion box's LJ+C1 force split over the
+    N GPUs of the job (one process per GPU) by runs of i-cells
+    (pmb200_shard_eval_device), the int64 fixed-point accumulators summed by one
+    NCCL all-reduce, then converted on every rank (pmb200_shard_finalize).
+    value = unique in-cutoff pairs per second of whole evaluations (cell build,
+    shard pair kernel, all-reduce, finalize), device-timed, max over ranks;
+    strong scaling (the box is the same at every N).  Rank 0 also checks that
+    the summed forces equal a one-GPU evaluation bit for bit."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    from protomoladdon_b200 import water
+    from protomoladdon_b200.force import NonbondedCutoffB200SystemForce, PeriodicTopology
+    from protomoladdon_b200.shard import sharded_evaluate
+    world = env_int("WORLD_SIZE", 1)
+    rank = env_int("RANK", 0)
+    dev = torch.device("cuda", env_int("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    if not dist.is_initialized():
+        if "MASTER_ADDR" not in os.environ:  # a plain one-process run
+            os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT="29511", RANK="0",
+                              WORLD_SIZE="1")
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+    s = water.large_331k()
+    topo = PeriodicTopology.from_dict(s)
+    f = NonbondedCutoffB200SystemForce(s["ron"], s["rc_lj"], s["rc_coul"], s["rc_alg"])
+    pos = torch.tensor(s["pos"], dtype=torch.float64, device=dev)
+    frc = torch.zeros_like(pos)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    # the reference result and the pair count: one whole evaluation on this GPU
+    one = torch.zeros_like(pos)
+    out = torch.zeros(20, dtype=torch.float64, device=dev)
+    f.evaluate_device(topo, pos.data_ptr(), one.data_ptr(), out.data_ptr(), 1, 1)
+    torch.cuda.synchronize(dev)
+    f.sync()
+    pairs = f.last_pair_count()
+
+    def step():
+        frc.zero_()
+        sharded_evaluate(f, topo, pos, frc)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    identical = bool(torch.equal(frc, one))
+    steps = min(args.steps, 50)
+    e0 = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    e1 = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    dist.barrier()
+    torch.cuda.synchronize(dev)
+    for k in range(steps):
+        flush.zero_()
+        e0[k].record()
+        step()
+        e1[k].record()
+    torch.cuda.synchronize(dev)
+    dist.barrier()
+    ms = statistics.mean(a.elapsed_time(b) for a, b in zip(e0, e1))
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    f.sync()
+    f.close()
+    dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps({
+            "metric": "Gpairs/s, 327k-atom ion box split over N GPUs (LJ+C1, mixed)",
+            "value": pairs / (ms * 1e-3) / 1e9, "unit": "Gpairs/s", "n_gpus": world,
+            "steps": steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "327,352-atom water box with 2% Na+/Cl-, rc 12 A, one force "
+                                   "evaluation per step split by i-cell runs over the ranks",
+                       "pairs_per_eval": pairs, "l2": "flushed before every timed step",
+                       "parallelism": f"force decomposition over {world} GPU(s)"},
+            "bit_identical_to_one_gpu": identical,
+        }), flush=True)
+    return 0
+
+
 def run_batch(args):
     """All 512 systems' forces per step.  value = unique in-cutoff pairs per
     second over the whole batch, device-resident, one CUDA-graph replay per
@@ -834,11 +916,12 @@ def main():
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--skip-accuracy", action="store_true")
     ap.add_argument("--workload", default="medium",
-                    choices=["medium", "large", "batch", "diff"],
+                    choices=["medium", "large", "batch", "diff", "sharded"],
                     help="medium: the 41,472-atom water box (the headline); large: the "
                          "327,352-atom ion box's LJ+C1 and Ewald real-space kernels; batch: "
                          "512 uneven boxes in one batched launch; diff: the differentiable "
-                         "form (Hessian-vector products, parameter gradients)")
+                         "form (Hessian-vector products, parameter gradients); sharded: "
+                         "the 327k-atom box's force split over the job's GPUs")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -850,6 +933,8 @@ def main():
         return run_batch(args)
     if args.workload == "diff":
         return run_diff(args)
+    if args.workload == "sharded":
+        return run_sharded(args)
     return run_ours(args)
 
 

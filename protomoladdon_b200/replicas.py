@@ -1,11 +1,12 @@
 """Multi-GPU replicas: one independent periodic system per rank.
 
-A 41k-atom box takes ~0.2 ms per step on one B200, so splitting one box over
+A 41k-atom box takes ~0.16 ms per step on one B200, so splitting one box over
 GPUs (replicated-data force decomposition with an all-reduce of the force
 array, the reference's MPI scheme in protomol/src/protomol/parallel/
-Parallel.cpp:122-135) would spend as long in the collective as in the force.
-The path therefore scales by replicas: each rank integrates its own system
-and the only collectives are the timing barrier and a max over ranks.
+Parallel.cpp:122-135; protomoladdon_b200.shard for large systems) would spend
+about as long in the collective as in the force.  The headline workload
+therefore scales by replicas: each rank integrates its own system and the only
+collectives are the timing barrier and a max over ranks.
 """
 from __future__ import annotations
 
