@@ -841,9 +841,11 @@ __device__ __forceinline__ void mixed_task(
         int jx = cx + dx, jy = cy + dy, jz = cz + dz;
         bool inside = true;
         if (g.periodic) {
-          jx %= g.nx; jx += (jx < 0) ? g.nx : 0;
-          jy %= g.ny; jy += (jy < 0) ? g.ny : 0;
-          jz %= g.nz; jz += (jz < 0) ? g.nz : 0;
+          // one wrap suffices: offsets reach at most ceil(rc / edge) <= n / 2
+          // cells, since every box edge is at least twice the cutoff
+          jx += jx < 0 ? g.nx : (jx >= g.nx ? -g.nx : 0);
+          jy += jy < 0 ? g.ny : (jy >= g.ny ? -g.ny : 0);
+          jz += jz < 0 ? g.nz : (jz >= g.nz ? -g.nz : 0);
         } else {
           inside = jx >= 0 && jx < g.nx && jy >= 0 && jy < g.ny && jz >= 0 && jz < g.nz;
         }
@@ -1101,8 +1103,7 @@ k_pair_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes, const dou
       for (int dx = row.dxlo; dx <= row.dxhi; dx++) {
         int jx = cx + dx;
         if (!g.periodic && (jx < 0 || jx >= g.nx)) continue;
-        jx %= g.nx;
-        jx += (jx < 0) ? g.nx : 0;
+        jx += jx < 0 ? g.nx : (jx >= g.nx ? -g.nx : 0);  // |dx| <= n / 2: one wrap
         const int jc = rowbase + jx;
         const int js = start[jc], je = start[jc + 1];
         const double sx = dx * g.edge[0];
@@ -1318,8 +1319,7 @@ k_deriv_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes,
         for (int dx = row.dxlo; dx <= row.dxhi; dx++) {
           int jx = cx + dx;
           if (!g.periodic && (jx < 0 || jx >= g.nx)) continue;
-          jx %= g.nx;
-          jx += (jx < 0) ? g.nx : 0;
+          jx += jx < 0 ? g.nx : (jx >= g.nx ? -g.nx : 0);  // |dx| <= n / 2: one wrap
           const int jc = rowbase + jx;
           const int js = start[jc], je = start[jc + 1];
           const double sx = dx * g.edge[0];
