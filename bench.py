@@ -325,7 +325,7 @@ def run_ours(args):
 
     def host_step():
         rigid.host_kick_drift(xh, vh, F, s["mass"], DT_FS, widx, water.D_OH, water.D_HH)
-        F[:] = 0.0
+        _ft.zero_()  # the integrator zeroes its force array (F is a view of _ft)
         E.clear()
         fmix.evaluate(topo, xh, F, E)
 
