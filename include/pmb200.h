@@ -256,19 +256,26 @@ int pmb200_grid(const pmb200_ctx *ctx, int dims[3], double edge[3]);
  * OneAtomPair<PBC, S, LennardJonesForce>, OneAtomPair<PBC, S, CoulombForce>
  * (a single potential: the other switch PMB200_SW_NONE) and
  * OneAtomPairTwo<PBC, S1, LennardJonesForce, S2, CoulombForce>, with S from
- * C1 (.../switch/C1SwitchingFunction.h), C2 (C2SwitchingFunction.h) and Cn
+ * C1 (.../switch/C1SwitchingFunction.h), C2 (C2SwitchingFunction.h), Cn
  * (CnSwitchingFunction.cpp, orders 2, 3, 4 and 6; the reference's order 5
  * has an all-zero coefficient table and is refused with
+ * PMB200_EUNSUPPORTED) and ComplimentCnCn (CmpCnCnSwitchingFunction.h/.cpp:
+ * 0 below switchon, rising to 1 at switchoff, falling to 0 at the cutoff;
+ * orders 2, 3, 4, 6, and 5 read as 2 as the reference does; non-integer
+ * orders, which the reference truncates, are refused with
  * PMB200_EUNSUPPORTED).  Each potential is multiplied by its own switch,
  * F' = F S - E dS, E' = E S (OneAtomPair.h:80-88).  Per switch the array
  * holds {switchon, cutoff, order, switchoff}: C1 reads the cutoff only, C2
- * switchon and cutoff, Cn all four (switchoff 0 or equal to the cutoff, as
- * CnSwitchingFunction::make requires).  The CmpCnCn switch is not offered.
+ * switchon and cutoff, Cn and ComplimentCnCn all four (Cn: switchoff 0 or
+ * equal to the cutoff, as CnSwitchingFunction::make requires;
+ * ComplimentCnCn: 0 <= switchon < switchoff <= cutoff, as
+ * CmpCnCnSwitchingFunction::make requires).
  * Energies: LENNARDJONES and COULOMB as for the first kind. */
 #define PMB200_SW_NONE 0
 #define PMB200_SW_C1 1
 #define PMB200_SW_C2 2
 #define PMB200_SW_CN 3
+#define PMB200_SW_CMPCNCN 4  /* ComplimentCnCn (CmpCnCnSwitchingFunction) */
 
 typedef struct {
   int precision;       /* PMB200_MIXED or PMB200_FP64 */

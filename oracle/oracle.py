@@ -306,12 +306,13 @@ class RefForce:
                                   _ptr(e), _ptr(v), _ptr(mv), int(virial_mode))
         return f.reshape(-1, 3), float(e[0]), v, mv
 
-    SWITCH_KINDS = {None: 0, "C1": 1, "C2": 2, "Cn": 3}
+    SWITCH_KINDS = {None: 0, "C1": 1, "C2": 2, "Cn": 3, "ComplimentCnCn": 4}
 
     def pair_eval(self, pos, lj, coulomb, rc_alg, virial_mode=2):
         """The reference's NonbondedCutoffSystemForce with OneAtomPair /
         OneAtomPairTwo and the given switches: lj / coulomb are None or
-        (kind, switchon, cutoff, order, switchoff) with kind C1, C2 or Cn.
+        (kind, switchon, cutoff, order, switchoff) with kind C1, C2, Cn or
+        ComplimentCnCn.
         Returns (forces, energies (coulomb, lj), virial, molvirial)."""
         def spec(x):
             if x is None:

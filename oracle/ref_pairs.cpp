@@ -3,7 +3,7 @@
 // 53-82) -- NonbondedCutoffSystemForce<CubicCellManager, P> with
 //   P = OneAtomPair<PBC, S, LennardJonesForce>, OneAtomPair<PBC, S, CoulombForce>,
 //       OneAtomPairTwo<PBC, S1, LennardJonesForce, S2, CoulombForce>
-// and S, S1, S2 among C1, C2 and Cn -- evaluated on the topology pmref_create
+// and S, S1, S2 among C1, C2, Cn and ComplimentCnCn -- evaluated on the topology pmref_create
 // built.  Nothing in the product links this.
 #include <protomol/force/nonbonded/NonbondedCutoffSystemForce.h>
 #include <protomol/force/OneAtomPair.h>
@@ -13,6 +13,7 @@
 #include <protomol/switch/C1SwitchingFunction.h>
 #include <protomol/switch/C2SwitchingFunction.h>
 #include <protomol/switch/CnSwitchingFunction.h>
+#include <protomol/switch/CmpCnCnSwitchingFunction.h>
 #include <protomol/topology/PeriodicBoundaryConditions.h>
 #include <protomol/topology/CubicCellManager.h>
 #include <protomol/topology/CellListEnumeratorPeriodicBoundaries.h>
@@ -31,8 +32,8 @@ typedef PeriodicBoundaryConditions PBC;
 
 namespace {
 
-// switch kinds as in include/pmb200.h: 1 C1, 2 C2, 3 Cn; p = {switchon,
-// cutoff, order, switchoff}
+// switch kinds as in include/pmb200.h: 1 C1, 2 C2, 3 Cn, 4 ComplimentCnCn;
+// p = {switchon, cutoff, order, switchoff}
 C1SwitchingFunction sw(const C1SwitchingFunction *, const double *p) {
   return C1SwitchingFunction(p[1]);
 }
@@ -41,6 +42,9 @@ C2SwitchingFunction sw(const C2SwitchingFunction *, const double *p) {
 }
 CnSwitchingFunction sw(const CnSwitchingFunction *, const double *p) {
   return CnSwitchingFunction(p[2], p[0], p[3], p[1]);
+}
+CmpCnCnSwitchingFunction sw(const CmpCnCnSwitchingFunction *, const double *p) {
+  return CmpCnCnSwitchingFunction(p[0], p[1], p[3], p[2]);
 }
 
 int run(SystemForce *force, PTopo *t, const double *pos, double *forces, double *energies,
@@ -91,6 +95,7 @@ template <class S1>
 SystemForce *two_any(int k2, const double *p1, const double *p2, double rc) {
   if (k2 == 1) return two<S1, C1SwitchingFunction>(p1, p2, rc);
   if (k2 == 2) return two<S1, C2SwitchingFunction>(p1, p2, rc);
+  if (k2 == 4) return two<S1, CmpCnCnSwitchingFunction>(p1, p2, rc);
   return two<S1, CnSwitchingFunction>(p1, p2, rc);
 }
 
@@ -100,7 +105,8 @@ extern "C" {
 
 void *pmref_topology(void *h);
 
-// lj_kind / coul_kind: 0 none, 1 C1, 2 C2, 3 Cn (at least one non-zero);
+// lj_kind / coul_kind: 0 none, 1 C1, 2 C2, 3 Cn, 4 ComplimentCnCn (at least
+// one non-zero);
 // forces accumulated into; energies {COULOMB, LENNARDJONES}; mode 0/1/2 as
 // pmref_eval.  Returns 0, or 1 for an unknown kind.
 int pmref_pair_eval(void *h, int lj_kind, const double *ljp, int coul_kind, const double *cop,
@@ -112,14 +118,17 @@ int pmref_pair_eval(void *h, int lj_kind, const double *ljp, int coul_kind, cons
   if (lj_kind && coul_kind) {
     if (lj_kind == 1) f = two_any<C1SwitchingFunction>(coul_kind, ljp, cop, rc_alg);
     else if (lj_kind == 2) f = two_any<C2SwitchingFunction>(coul_kind, ljp, cop, rc_alg);
+    else if (lj_kind == 4) f = two_any<CmpCnCnSwitchingFunction>(coul_kind, ljp, cop, rc_alg);
     else f = two_any<CnSwitchingFunction>(coul_kind, ljp, cop, rc_alg);
   } else if (lj_kind) {
     if (lj_kind == 1) f = single_lj<C1SwitchingFunction>(ljp, rc_alg);
     else if (lj_kind == 2) f = single_lj<C2SwitchingFunction>(ljp, rc_alg);
+    else if (lj_kind == 4) f = single_lj<CmpCnCnSwitchingFunction>(ljp, rc_alg);
     else f = single_lj<CnSwitchingFunction>(ljp, rc_alg);
   } else if (coul_kind) {
     if (coul_kind == 1) f = single_coul<C1SwitchingFunction>(cop, rc_alg);
     else if (coul_kind == 2) f = single_coul<C2SwitchingFunction>(cop, rc_alg);
+    else if (coul_kind == 4) f = single_coul<CmpCnCnSwitchingFunction>(cop, rc_alg);
     else f = single_coul<CnSwitchingFunction>(cop, rc_alg);
   }
   if (!f) return 1;

@@ -31,6 +31,7 @@ PMB200_SW_NONE = 0
 PMB200_SW_C1 = 1
 PMB200_SW_C2 = 2
 PMB200_SW_CN = 3
+PMB200_SW_CMPCNCN = 4
 
 PMB200_ERFC_POLY5 = 0
 PMB200_ERFC_EXACT = 1

@@ -237,6 +237,19 @@ SwitchSpec<T> make_switch(int kind, const double par[4], double u) {
     w.inv_range = (T)(1.0 / (ron - rc));
     for (int j = 0; j <= n; j++) w.vcoef[j] = (T)binomial(2 * n + 1, n + 1 + j);
     w.dpeak = (T)kCnDeriv[n - 2][0];
+  } else if (kind == SW_CMPCNCN) {  // CmpCnCnSwitchingFunction.cpp:16-33
+    // order 5 is read as 2, as the reference's constructor does
+    const int n = par[2] == 5.0 ? 2 : (int)par[2];
+    const double roff = par[3] / u;
+    w.nord = n;
+    w.ron2 = (T)(ron * ron);
+    w.ron = (T)ron;
+    w.roff2 = (T)(roff * roff);
+    w.roff = (T)roff;
+    w.inv_range = roff < rc ? (T)(1.0 / (roff - rc)) : (T)0;  // empty falling part
+    w.inv_in = (T)(1.0 / (roff - ron));
+    for (int j = 0; j <= n; j++) w.vcoef[j] = (T)binomial(2 * n + 1, n + 1 + j);
+    w.dpeak = (T)kCnDeriv[n - 2][0];
   }
   return w;
 }
@@ -534,7 +547,9 @@ int pmb200_create_pair(const pmb200_pair_params *params, pmb200_ctx **out) {
     const int kd = kinds[k];
     const double *pr = pars[k];
     if (kd == PMB200_SW_NONE) continue;
-    if (kd != PMB200_SW_C1 && kd != PMB200_SW_C2 && kd != PMB200_SW_CN) return PMB200_EINVAL;
+    if (kd != PMB200_SW_C1 && kd != PMB200_SW_C2 && kd != PMB200_SW_CN &&
+        kd != PMB200_SW_CMPCNCN)
+      return PMB200_EINVAL;
     const double ron = pr[0], rc = pr[1], order = pr[2], roff = pr[3];
     if (!(rc > 0.0) || !std::isfinite(rc)) return PMB200_EINVAL;
     if (kd == PMB200_SW_C2 && !(ron >= 0.0 && ron < rc)) return PMB200_EINVAL;
@@ -544,6 +559,18 @@ int pmb200_create_pair(const pmb200_pair_params *params, pmb200_ctx **out) {
         return PMB200_EINVAL;
       // the reference's order 5 has an all-zero coefficient row
       if ((int)order == 5 || order != std::floor(order)) return PMB200_EUNSUPPORTED;
+      static const bool agree = cn_tables_agree();
+      if (!agree) return PMB200_EUNSUPPORTED;
+    }
+    if (kd == PMB200_SW_CMPCNCN) {
+      // CmpCnCnSwitchingFunction::make (CmpCnCnSwitchingFunction.cpp:53-68):
+      // 0 <= switchon < switchoff <= cutoff, 2 <= order <= 6
+      if (!(ron >= 0.0 && roff > 0.0 && ron < roff && roff <= rc) || order < 2.0 ||
+          order > 6.0)
+        return PMB200_EINVAL;
+      // orders 2, 3, 4, 6 and 5 (read as 2); the reference truncates other
+      // orders and its order-5 row is all zero: refused
+      if (order != std::floor(order)) return PMB200_EUNSUPPORTED;
       static const bool agree = cn_tables_agree();
       if (!agree) return PMB200_EUNSUPPORTED;
     }
@@ -566,6 +593,7 @@ int pmb200_create_pair(const pmb200_pair_params *params, pmb200_ctx **out) {
     c->sw_kind[k] = kinds[k] == PMB200_SW_C1   ? SW_C1
                     : kinds[k] == PMB200_SW_C2 ? SW_C2
                     : kinds[k] == PMB200_SW_CN ? SW_CN
+                    : kinds[k] == PMB200_SW_CMPCNCN ? SW_CMPCNCN
                                                : SW_OFF;
     for (int j = 0; j < 4; j++) c->sw_par[k][j] = pars[k][j];
   }

@@ -84,16 +84,18 @@ enum PairForm { FORM_CUTOFF = 0, FORM_EWALD_POLY5 = 1, FORM_EWALD_EXACT = 2, FOR
 
 // Switching functions of the generic form (each potential its own; SW_OFF:
 // the potential is absent).  dS is ProtoMol's "deriv": dS/dr / r.
-enum SwitchKind { SW_OFF = 0, SW_C1 = 1, SW_C2 = 2, SW_CN = 3 };
+enum SwitchKind { SW_OFF = 0, SW_C1 = 1, SW_C2 = 2, SW_CN = 3, SW_CMPCNCN = 4 };
 
 template <class T>
 struct SwitchSpec {
   int kind, nord;    // SwitchKind; Cn: integer order
   T rc2, ron2, rc;   // cutoff^2, switchon^2, cutoff
   T a, b, c;         // C1: 1.5/rc, 0.5/rc^3, 1.5/rc^3; C2: s1, s2, s3 (C2SwitchingFunction.cpp)
-  T ron, inv_range;  // Cn: switchon, 1 / (switchon - cutoff)
-  T vcoef[7];        // Cn: binom(2n+1, n+1+j), j = 0..n
-  T dpeak;           // Cn: (2n+1)! / (n!)^2
+  T ron, inv_range;  // Cn: switchon, 1 / (switchon - cutoff);
+                     // ComplimentCnCn: switchon, 1 / (switchoff - cutoff)
+  T roff2, roff, inv_in;  // ComplimentCnCn: switchoff^2, switchoff, 1 / (switchoff - switchon)
+  T vcoef[7];        // Cn, ComplimentCnCn: binom(2n+1, n+1+j), j = 0..n
+  T dpeak;           // Cn, ComplimentCnCn: (2n+1)! / (n!)^2
 };
 
 // Value S and deriv dS (= dS/dr / r) at r^2 (rinv = 1/r), following
@@ -105,6 +107,10 @@ struct SwitchSpec {
 //   dS/dt = (2n+1)!/(n!)^2 t^n u^n,
 // whose terms are all positive (the power form cancels to ~1e-4 of its
 // terms at order 6, too much for FP32); t and u are both taken from r.
+// ComplimentCnCn (CmpCnCnSwitchingFunction.h:39-84): 0 below switchon, the
+// same polynomial rising on [switchon, switchoff] (the reference's 1 - its
+// falling form, which is the rising one by the polynomial's symmetry) and
+// falling on (switchoff, cutoff].
 template <class T>
 __device__ __forceinline__ void switch_eval(const SwitchSpec<T> &w, T r2, T rinv, T &S, T &dS) {
   S = T(0);
@@ -135,6 +141,24 @@ __device__ __forceinline__ void switch_eval(const SwitchSpec<T> &w, T r2, T rinv
     }
     S = tn * t * acc;
     dS = w.dpeak * tn * un * w.inv_range * rinv;
+  } else if (w.kind == SW_CMPCNCN) {
+    if (r2 < w.ron2) return;
+    const T r = r2 * rinv;
+    const bool fall = r2 > w.roff2;
+    // rising: t = (r - switchon) / (switchoff - switchon); falling:
+    // t = (r - cutoff) / (switchoff - cutoff); u = 1 - t from r in both
+    const T scale = fall ? w.inv_range : w.inv_in;
+    const T t = (r - (fall ? w.rc : w.ron)) * scale;
+    const T u = (w.roff - r) * scale;
+    T tn = T(1), un = T(1);
+    for (int k = 0; k < w.nord; k++) { tn *= t; un *= u; }
+    T acc = w.vcoef[w.nord], up = T(1);
+    for (int j = w.nord - 1; j >= 0; j--) {
+      up *= u;
+      acc = acc * t + w.vcoef[j] * up;
+    }
+    S = tn * t * acc;
+    dS = w.dpeak * tn * un * scale * rinv;
   }
 }
 

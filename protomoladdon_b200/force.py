@@ -428,16 +428,19 @@ class NonbondedCutoffB200PairForce(NonbondedCutoffB200SystemForce):
     (protomol/src/protomol/module/NonbondedCutoffForceModule.cpp:53-82):
     OneAtomPair<PBC, S, LennardJonesForce>, OneAtomPair<PBC, S, CoulombForce>
     and OneAtomPairTwo<PBC, S1, LennardJonesForce, S2, CoulombForce> with S
-    among C1, C2, Cn.  ``lj`` / ``coulomb``: None (term absent) or a tuple
-    (kind, switchon, cutoff, order, switchoff); C1 reads the cutoff, C2
-    switchon and cutoff, Cn all four (see pmb200_create_pair)."""
+    among C1, C2, Cn, ComplimentCnCn.  ``lj`` / ``coulomb``: None (term
+    absent) or a tuple (kind, switchon, cutoff, order, switchoff); C1 reads
+    the cutoff, C2 switchon and cutoff, Cn and ComplimentCnCn all four (see
+    pmb200_create_pair)."""
 
     keyword = "NonbondedCutoffB200"
     _KIND = {None: _lib.PMB200_SW_NONE, "C1": _lib.PMB200_SW_C1, "C2": _lib.PMB200_SW_C2,
-             "Cn": _lib.PMB200_SW_CN}
-    # switch parameters as the reference lists them (getParameters)
+             "Cn": _lib.PMB200_SW_CN, "ComplimentCnCn": _lib.PMB200_SW_CMPCNCN}
+    # switch parameters as the reference lists them (getParameters;
+    # CmpCnCnSwitchingFunction.cpp:35-50 for ComplimentCnCn)
     _PARAMS = {"C1": ["-cutoff"], "C2": ["-switchon", "-cutoff"],
-               "Cn": ["-n", "-switchon", "-switchoff", "-cutoff"]}
+               "Cn": ["-n", "-switchon", "-switchoff", "-cutoff"],
+               "ComplimentCnCn": ["-switchon", "-switchoff", "-cutoff", "-n"]}
 
     def __init__(self, lj=None, coulomb=None, cutoff_alg=None, precision="mixed", device=0,
                  cellsize=0.0):
@@ -445,8 +448,8 @@ class NonbondedCutoffB200PairForce(NonbondedCutoffB200SystemForce):
             if sw is None:
                 return None
             sw = tuple(sw) + (0.0,) * (5 - len(sw))
-            if sw[0] not in ("C1", "C2", "Cn"):
-                raise ValueError(f"switching function {sw[0]!r}: C1, C2 or Cn")
+            if sw[0] not in self._PARAMS:
+                raise ValueError(f"switching function {sw[0]!r}: C1, C2, Cn or ComplimentCnCn")
             return (sw[0],) + tuple(float(x) for x in sw[1:5])
         self.lj = norm(lj)
         self.coulomb = norm(coulomb)
@@ -509,7 +512,7 @@ class NonbondedCutoffB200PairForce(NonbondedCutoffB200SystemForce):
         specs = []
         for sw in sws:
             if sw not in cls._PARAMS:
-                raise ValueError(f"switching function {sw!r}: C1, C2 or Cn")
+                raise ValueError(f"switching function {sw!r}: C1, C2, Cn or ComplimentCnCn")
             vals = {}
             for key in cls._PARAMS[sw]:
                 if not params or params[0][0] != key:

@@ -21,15 +21,21 @@ void ProtoMol::registerB200EwaldRealForce(ForceFactory &factory) {
 
 // The switch combinations NonbondedCutoffForceModule registers for the
 // plain LJ / Coulomb potentials (NonbondedCutoffForceModule.cpp:55-82 and
-// 98-125), CmpCnCn aside; the periodic (C2, C1) pair has its own class.
+// 98-141); the periodic (C2, C1) pair has its own class.
 template <class TBC>
-static void registerPairs(ForceFactory &f, bool withC2C1) {
-  const int C1 = PMB200_SW_C1, C2 = PMB200_SW_C2, CN = PMB200_SW_CN, NO = PMB200_SW_NONE;
-  const int combos[][2] = {{NO, C1}, {NO, C2}, {NO, CN}, {C1, NO}, {C2, NO}, {CN, NO},
-                           {C2, C2}, {C2, CN}, {CN, CN}, {C2, C1}};
-  const int count = withC2C1 ? 10 : 9;
-  for (int k = 0; k < count; k++)
-    f.reg(new B200PairSystemForce<TBC>(combos[k][0], combos[k][1]));
+static void registerPairs(ForceFactory &f, bool vacuum) {
+  const int C1 = PMB200_SW_C1, C2 = PMB200_SW_C2, CN = PMB200_SW_CN, NO = PMB200_SW_NONE,
+            CM = PMB200_SW_CMPCNCN;
+  const int common[][2] = {{NO, C1}, {NO, C2}, {NO, CN}, {NO, CM}, {C1, NO}, {C2, NO},
+                           {CN, NO}, {CM, NO}, {C2, C2}, {C2, CN}, {CN, CN}};
+  for (int k = 0; k < (int)(sizeof(common) / sizeof(common[0])); k++)
+    f.reg(new B200PairSystemForce<TBC>(common[k][0], common[k][1]));
+  if (vacuum) {
+    f.reg(new B200PairSystemForce<TBC>(C2, C1));
+    f.reg(new B200PairSystemForce<TBC>(CM, C1));
+  } else {
+    f.reg(new B200PairSystemForce<TBC>(CM, CM));
+  }
 }
 
 void ProtoMol::registerB200PairForces(ForceFactory &factory, bool vacuum) {

@@ -4,7 +4,8 @@
 // NonbondedCutoffForceModule.cpp:53-134) on a B200 through libpmb200
 // (pmb200_create_pair): OneAtomPair<BC, S, LennardJonesForce>,
 // OneAtomPair<BC, S, CoulombForce> and OneAtomPairTwo<BC, S1,
-// LennardJonesForce, S2, CoulombForce> with S among C1, C2, Cn, for periodic
+// LennardJonesForce, S2, CoulombForce> with S among C1, C2, Cn and
+// ComplimentCnCn (CmpCnCnSwitchingFunction), for periodic
 // boundaries (BC = PeriodicBoundaryConditions) or vacuum
 // (VacuumBoundaryConditions).  One prototype per (LJ switch, Coulomb switch)
 // pair is registered under the algorithm keyword NonbondedCutoffB200; its id
@@ -125,7 +126,10 @@ private:
   B200PairSystemForce &operator=(const B200PairSystemForce &);
 
   static std::string switchName(int kind) {
-    return kind == PMB200_SW_C1 ? "C1" : kind == PMB200_SW_C2 ? "C2" : "Cn";
+    return kind == PMB200_SW_C1   ? "C1"
+           : kind == PMB200_SW_C2 ? "C2"
+           : kind == PMB200_SW_CN ? "Cn"
+                                  : "ComplimentCnCn";
   }
   static int switchArity(int kind) {
     return kind == PMB200_SW_C1 ? 1 : kind == PMB200_SW_C2 ? 2 : 4;
@@ -133,9 +137,20 @@ private:
 
   // The switch's parameters as its getParameters lists them
   // (C1SwitchingFunction.cpp:18-22, C2SwitchingFunction.cpp:20-28,
-  // CnSwitchingFunction.cpp:64-80).
+  // CnSwitchingFunction.cpp:64-80, CmpCnCnSwitchingFunction.cpp:35-50).
   static void switchParameters(int kind, const double *p, std::vector<Parameter> &out) {
     const std::string n = switchName(kind);
+    if (kind == PMB200_SW_CMPCNCN) {
+      out.push_back(Parameter("-switchon", Value(p[0], ConstraintValueType::NotNegative()),
+                              Text("CmpCnCn swf switch on")));
+      out.push_back(Parameter("-switchoff", Value(p[3], ConstraintValueType::Positive()),
+                              Text("CmpCnCn swf switchoff")));
+      out.push_back(Parameter("-cutoff", Value(p[1], ConstraintValueType::Positive()),
+                              Text("CmpCnCn swf cutoff")));
+      out.push_back(Parameter("-n", Value(p[2], ConstraintValueType::Positive()), 2.0,
+                              Text("CmpCnCn swf smoothness")));
+      return;
+    }
     if (kind == PMB200_SW_CN)
       out.push_back(Parameter("-n", Value(p[2], ConstraintValueType::Positive()),
                               Text(n + " swf smoothness")));
@@ -161,7 +176,11 @@ private:
       for (int a = 0; a < switchArity(kinds[s]); a++) values[k++].get(v[a]);
       if (kinds[s] == PMB200_SW_C1) { dst[s][1] = v[0]; }
       else if (kinds[s] == PMB200_SW_C2) { dst[s][0] = v[0]; dst[s][1] = v[1]; }
-      else { dst[s][2] = v[0]; dst[s][0] = v[1]; dst[s][3] = v[2]; dst[s][1] = v[3]; }
+      else if (kinds[s] == PMB200_SW_CN) {
+        dst[s][2] = v[0]; dst[s][0] = v[1]; dst[s][3] = v[2]; dst[s][1] = v[3];
+      } else {  // ComplimentCnCn: switchon, switchoff, cutoff, n
+        dst[s][0] = v[0]; dst[s][3] = v[1]; dst[s][1] = v[2]; dst[s][2] = v[3];
+      }
     }
     Real rc;
     values[k].get(rc);

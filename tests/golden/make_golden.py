@@ -141,13 +141,22 @@ PAIR_CASES = {
     "lj_cn": (("Cn", 6.5, 8.0, 2, 0), None),
     "coul_c2": (None, ("C2", 3.0, 8.0, 0, 0)),
     "coul_cn": (None, ("Cn", 5.0, 8.0, 4, 0)),
+    # ComplimentCnCn: switchon, cutoff, order, switchoff (the periodic LJ+Coulomb
+    # registration; single potentials; order 5 read as 2; switchoff == cutoff).
+    # (A window that keeps only the LJ tail beyond the first shell leaves net
+    # forces ~1e-3 of the pair forces, where a relative force bound measures
+    # FP32 cancellation, not the switch: the LJ case starts at switchon 0.)
+    "cm_cm": (("ComplimentCnCn", 3.0, 8.0, 4, 6.0), ("ComplimentCnCn", 2.0, 8.0, 2, 5.0)),
+    "lj_cm": (("ComplimentCnCn", 0.0, 8.0, 6, 5.0), None),
+    "coul_cm": (None, ("ComplimentCnCn", 1.0, 8.0, 3, 8.0)),
+    "cm5_c1": (("ComplimentCnCn", 3.0, 8.0, 5, 6.5), ("C1", 0.0, 8.0, 0, 0)),
 }
 
 
 def pair_fixtures():
     w = water.small_648()
     out = dict(sysd_arrays(w))
-    codes = {"C1": 1, "C2": 2, "Cn": 3}
+    codes = {"C1": 1, "C2": 2, "Cn": 3, "ComplimentCnCn": 4}
     R = O.RefForce(w)
     for name, (lj, co) in PAIR_CASES.items():
         f, e, v, mv = R.pair_eval(w["pos"], lj, co, 8.0, 2)

@@ -166,16 +166,22 @@ def test_pair_form_create_validates_before_touching_a_device():
     def P(lk, lp, ck, cp, alg=10.0):
         return _lib.PairParams(0, 0, lk, D4(*lp), ck, D4(*cp), alg, 0.0)
     C2, CN, C1, NO = _lib.PMB200_SW_C2, _lib.PMB200_SW_CN, _lib.PMB200_SW_C1, _lib.PMB200_SW_NONE
+    CM = _lib.PMB200_SW_CMPCNCN
     z = (0, 0, 0, 0)
     bad = [P(NO, z, NO, z),                          # no term at all
            P(C2, (9, 9, 0, 0), NO, z),               # C2 switchon == cutoff
            P(CN, (5, 8, 7, 0), NO, z),               # Cn order above 6
            P(CN, (5, 8, 4, 9), NO, z),               # switchoff neither 0 nor the cutoff
            P(C1, (0, -1, 0, 0), NO, z),              # negative cutoff
+           P(CM, (6, 8, 4, 5), NO, z),               # ComplimentCnCn switchon above switchoff
+           P(CM, (3, 8, 4, 9), NO, z),               # ComplimentCnCn switchoff beyond the cutoff
+           P(CM, (3, 8, 7, 6), NO, z),               # ComplimentCnCn order above 6
            P(9, (0, 8, 0, 0), NO, z)]                # unknown switch
     for p in bad:
         assert L.pmb200_create_pair(ctypes.byref(p), ctypes.byref(h)) == _lib.PMB200_EINVAL
     p = P(CN, (5, 8, 5, 0), NO, z)                   # order 5: the reference's zero table
+    assert L.pmb200_create_pair(ctypes.byref(p), ctypes.byref(h)) == _lib.PMB200_EUNSUPPORTED
+    p = P(CM, (3, 8, 2.5, 6), NO, z)                 # an order the reference would truncate
     assert L.pmb200_create_pair(ctypes.byref(p), ctypes.byref(h)) == _lib.PMB200_EUNSUPPORTED
     p = P(C1, (0, 9, 0, 0), C1, (0, 9, 0, 0), alg=8.0)  # algorithm cutoff below a switch
     assert L.pmb200_create_pair(ctypes.byref(p), ctypes.byref(h)) == _lib.PMB200_EUNSUPPORTED
@@ -184,7 +190,8 @@ def test_pair_form_create_validates_before_touching_a_device():
 def test_pair_form_ids_round_trip():
     from protomoladdon_b200.force import NonbondedCutoffB200PairForce as P
     for lj, co in ((("C2", 6.5, 8.0), ("Cn", 5.0, 8.0, 4, 0)), (None, ("C1", 0, 9.0)),
-                   (("Cn", 6, 8, 3, 8), None), (("C2", 7, 9), ("C2", 0, 9))):
+                   (("Cn", 6, 8, 3, 8), None), (("C2", 7, 9), ("C2", 0, 9)),
+                   (("ComplimentCnCn", 3, 8, 4, 6), ("ComplimentCnCn", 2, 8, 2, 5))):
         f = P(lj, co)
         g = P.from_id(f.get_id())
         assert g.get_id() == f.get_id() and g.lj == f.lj and g.coulomb == f.coulomb

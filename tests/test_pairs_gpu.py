@@ -1,11 +1,11 @@
 """The other periodic cutoff registrations (OneAtomPair / OneAtomPairTwo with
-C1, C2, Cn switches; pmb200_create_pair) against the reference's own
+C1, C2, Cn, ComplimentCnCn switches; pmb200_create_pair) against the reference's own
 outputs (tests/golden/pairs_ref.npz, written by make_golden.py from the
 reference compiled from its sources).
 
 Tolerances (written here, checked below): FP64 kernel forces RMS relative
-<= 1e-12, energies relative <= 1e-11 -- <= 1e-10 for both when a Cn switch
-is involved: the reference sums the Cn polynomial in power form, whose terms
+<= 1e-12, energies relative <= 1e-11 -- <= 1e-10 for both when a Cn or
+ComplimentCnCn switch is involved: the reference sums their polynomial in power form, whose terms
 cancel to ~1e-4 of their size at orders 4-6, so its own rounding is
 ~1e-12..1e-11 while the kernel uses the positive Bernstein form; mixed kernel forces RMS relative
 <= 1e-5; energies within 1e-6 of the sum over pairs of |E_pair| (bounded
@@ -22,8 +22,9 @@ from .conftest import load_fixture
 
 pytestmark = pytest.mark.gpu
 
-CASES = ["c2_c2", "c2_cn", "cn_cn", "lj_c1", "lj_cn", "coul_c2", "coul_cn"]
-NAMES = {1: "C1", 2: "C2", 3: "Cn"}
+CASES = ["c2_c2", "c2_cn", "cn_cn", "lj_c1", "lj_cn", "coul_c2", "coul_cn",
+         "cm_cm", "lj_cm", "coul_cm", "cm5_c1"]
+NAMES = {1: "C1", 2: "C2", 3: "Cn", 4: "ComplimentCnCn"}
 
 
 @pytest.fixture(scope="module")
@@ -73,7 +74,7 @@ def test_switch_policies_match_reference(fx, case, precision):
     err = float(np.sqrt(((F - fr) ** 2).sum() / (fr ** 2).sum()))
     vr, mvr = fx[f"{case}_virial"], fx[f"{case}_molvirial"]
     if precision == "fp64":
-        cn = "cn" in case
+        cn = "cn" in case or "cm" in case  # power-form polynomials in the reference
         assert err <= (1e-10 if cn else 1e-12), err
         for k in (0, 1):
             assert abs(E[k] - er[k]) <= (1e-10 if cn else 1e-11) * max(1.0, abs(er[k]))

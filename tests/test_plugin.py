@@ -112,7 +112,7 @@ def _pair_case(name):
     """(force id, values) of a switch-policy fixture case, as a config gives them."""
     from .conftest import load_fixture
     d = load_fixture("pairs_ref.npz")
-    names = {1: "C1", 2: "C2", 3: "Cn"}
+    names = {1: "C1", 2: "C2", 3: "Cn", 4: "ComplimentCnCn"}
     pots, sws, vals = [], [], []
     for pot, key in (("LennardJones", f"{name}_lj"), ("Coulomb", f"{name}_coul")):
         a = d[key]
@@ -122,7 +122,8 @@ def _pair_case(name):
         pots.append(pot)
         sws.append(kind)
         ron, rc, order, roff = (float(x) for x in a[1:])
-        vals += {"C1": [rc], "C2": [ron, rc], "Cn": [order, ron, roff, rc]}[kind]
+        vals += {"C1": [rc], "C2": [ron, rc], "Cn": [order, ron, roff, rc],
+                 "ComplimentCnCn": [ron, roff, rc, order]}[kind]
     vals.append(8.0)  # algorithm cutoff
     fid = " ".join(pots) + "".join(f" -switchingFunction {k}" for k in sws) + \
         " -algorithm NonbondedCutoffB200"
@@ -130,7 +131,7 @@ def _pair_case(name):
 
 
 def test_factory_resolves_switch_policy_ids():
-    for case in ("c2_cn", "lj_c1", "coul_cn"):
+    for case in ("c2_cn", "lj_c1", "coul_cn", "cm_cm", "lj_cm", "coul_cm"):
         d, fid, vals = _pair_case(case)
         R = O.RefForce(d)
         rc, msg, *_ = H.evaluate_pair(R, 0, fid, vals, d["pos"])
@@ -139,7 +140,8 @@ def test_factory_resolves_switch_policy_ids():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", ["c2_c2", "c2_cn", "cn_cn", "lj_c1", "coul_c2"])
+@pytest.mark.parametrize("case", ["c2_c2", "c2_cn", "cn_cn", "lj_c1", "coul_c2", "cm_cm",
+                                  "coul_cm"])
 def test_switch_policy_plugin_matches_reference(case):
     d, fid, vals = _pair_case(case)
     R = O.RefForce(d)
@@ -148,6 +150,19 @@ def test_switch_policy_plugin_matches_reference(case):
     assert rc == 0, msg
     fr = d[f"{case}_forces"]
     assert np.sqrt(((f - fr) ** 2).sum() / (fr ** 2).sum()) <= 1e-5
+
+
+def test_factory_resolves_vacuum_complimentcncn_id():
+    """The vacuum registration OneAtomPairTwo<VBC, CmpCnCn, LJ, C1, Coulomb>
+    (NonbondedCutoffForceModule.cpp:140-141) resolves through the factory."""
+    from .conftest import load_fixture
+    d = load_fixture("vacuum_ref.npz")
+    R = O.RefForce(d)
+    fid = ("LennardJones Coulomb -switchingFunction ComplimentCnCn -switchingFunction C1 "
+           "-algorithm NonbondedCutoffB200")
+    rc, msg, *_ = H.evaluate_pair(R, 1, fid, [3.0, 6.5, 8.0, 4.0, 8.0, 8.0], d["pos"])
+    R.close()
+    assert (rc == 0 and fid in msg) or "B200 cutoff force" in msg, msg
 
 
 @pytest.mark.gpu
