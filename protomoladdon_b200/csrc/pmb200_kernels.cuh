@@ -665,18 +665,20 @@ __device__ __forceinline__ void mixed_task(
           const float sv = fmaf(-dist, fmaf(-r2, mc.c05_3, mc.c15_1), 1.0f);
           const float sd = fmaf(dist, mc.c15_3, -mc.c15_1 * rinv);
           fc = inC ? __fmul_rn(ec, fmaf(r2inv, sv, -sd)) : 0.f;
-          if (kEnergy && inC) {
+          if (kEnergy) {
             // q_j / r, q_j and q_j r^2 from the FP64 distance (the FP32 one
             // rounds each term by ~1e-7 of q_j / rc while the C1 energy of a
             // pair near the cutoff is far smaller); 1/r from the FP32 value
-            // and one Newton-Raphson step in FP64
+            // and one Newton-Raphson step in FP64.  Computed for every pair
+            // and added under the cutoff by selection: no branch, so the FP64
+            // chain overlaps the force arithmetic.
             const double ex_ = pdx[t] - pix;
             const double ey_ = pdy[t] - piy;
             const double ez_ = pdz[t] - piz;
             const double r2d = fma(ex_, ex_, fma(ey_, ey_, ez_ * ez_));
             double rid = (double)rinv;
             rid = rid * fma(-0.5 * r2d, rid * rid, 1.5);
-            const double qjd = (double)qj;
+            const double qjd = inC ? (double)qj : 0.0;
             if (own) {
               eU = fma(qjd, rid, eU);
               eQ += qjd;
