@@ -110,11 +110,16 @@ class _Gradient(torch.autograd.Function):
         h.sync_params(q, table)
         w = w.detach().to(torch.float64).contiguous()
         hv = torch.empty_like(pos)
-        dq = torch.empty(q.shape, dtype=torch.float64, device=pos.device)
-        dt = torch.empty(table.shape, dtype=torch.float64, device=pos.device)
-        h.force.hvp_device(h.topo, pos.data_ptr(), w.data_ptr(), hv.data_ptr(), dq.data_ptr(),
-                           dt.data_ptr(), h.stream())
-        return hv, dq.to(q.dtype), dt.to(table.dtype), None
+        # the parameter derivatives only when asked for (a plain Hessian-vector
+        # product skips their kernel work)
+        need_q, need_t = ctx.needs_input_grad[1], ctx.needs_input_grad[2]
+        dq = torch.empty(q.shape, dtype=torch.float64, device=pos.device) if need_q else None
+        dt = torch.empty(table.shape, dtype=torch.float64, device=pos.device) if need_t else None
+        h.force.hvp_device(h.topo, pos.data_ptr(), w.data_ptr(), hv.data_ptr(),
+                           dq.data_ptr() if need_q else None, dt.data_ptr() if need_t else None,
+                           h.stream())
+        return (hv, dq.to(q.dtype) if need_q else None, dt.to(table.dtype) if need_t else None,
+                None)
 
 
 class _Energy(torch.autograd.Function):

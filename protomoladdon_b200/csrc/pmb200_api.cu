@@ -81,6 +81,8 @@ struct pmb200_ctx {
   // derivative kernels: per-block table rows and scratch outputs
   double *d_tpart = nullptr, *d_gq = nullptr, *d_glj = nullptr;
   size_t tpart_alloc = 0, gq_alloc = 0, glj_alloc = 0;
+  double4 *d_wsorted = nullptr;  // a Hessian-vector product's direction, sorted order
+  size_t ws_alloc = 0;
   double *d_pairs = nullptr, *d_out = nullptr, *d_red = nullptr;
   // rigid waters (SETTLE) for the device integrator
   int nwater = 0, nfree = 0;
@@ -637,7 +639,7 @@ int pmb200_destroy(pmb200_ctx *c) {
   dfree(c->d_cell_of); dfree(c->d_slot); dfree(c->d_tmp); dfree(c->d_sidx);
   dfree(c->d_rel32); dfree(c->d_spos32); dfree(c->d_rel_lo); dfree(c->d_spos_lo); dfree(c->d_rel64); dfree(c->d_spos64);
   dfree(c->d_smeta); dfree(c->d_com); dfree(c->d_facc);
-  dfree(c->d_tpart); dfree(c->d_gq); dfree(c->d_glj);
+  dfree(c->d_tpart); dfree(c->d_gq); dfree(c->d_glj); dfree(c->d_wsorted);
   dfree(c->d_pairs); dfree(c->d_out); dfree(c->d_red); dfree(c->d_widx); dfree(c->d_fidx);
   if (c->h_pin_pos) cudaFreeHost(c->h_pin_pos);
   if (c->h_pin_frc) cudaFreeHost(c->h_pin_frc);
@@ -1007,36 +1009,53 @@ static int launch_deriv(pmb200_ctx *c, int mode, const double *d_pos, const doub
   const GridParams &g = c->g;
   const int blocks = (g.ncell + 3) / 4;
   const size_t nt4 = (size_t)c->ntypes * c->ntypes * 4;
-  if (c->tpart_alloc < (size_t)blocks * nt4) {
-    CK(dalloc(c->d_tpart, (size_t)blocks * nt4));
-    c->tpart_alloc = (size_t)blocks * nt4;
-  }
-  if (!d_dq) {
-    if (c->gq_alloc < (size_t)std::max(c->n, 1)) {
-      CK(dalloc(c->d_gq, (size_t)std::max(c->n, 1)));
-      c->gq_alloc = (size_t)std::max(c->n, 1);
+  // a Hessian-vector product asked for neither parameter derivative skips them
+  const bool params = mode == DERIV_PARAMS || d_dq || d_dlj;
+  if (params) {
+    if (c->tpart_alloc < (size_t)blocks * nt4) {
+      CK(dalloc(c->d_tpart, (size_t)blocks * nt4));
+      c->tpart_alloc = (size_t)blocks * nt4;
     }
-    d_dq = c->d_gq;
-  }
-  if (!d_dlj) {
-    if (c->glj_alloc < nt4) {
-      CK(dalloc(c->d_glj, nt4));
-      c->glj_alloc = nt4;
+    if (!d_dq) {
+      if (c->gq_alloc < (size_t)std::max(c->n, 1)) {
+        CK(dalloc(c->d_gq, (size_t)std::max(c->n, 1)));
+        c->gq_alloc = (size_t)std::max(c->n, 1);
+      }
+      d_dq = c->d_gq;
     }
-    d_dlj = c->d_glj;
+    if (!d_dlj) {
+      if (c->glj_alloc < nt4) {
+        CK(dalloc(c->d_glj, nt4));
+        c->glj_alloc = nt4;
+      }
+      d_dlj = c->d_glj;
+    }
+  }
+  if (mode == DERIV_VJP && c->ws_alloc < (size_t)std::max(c->n, 1)) {
+    CK(dalloc(c->d_wsorted, (size_t)std::max(c->n, 1)));
+    c->ws_alloc = (size_t)std::max(c->n, 1);
   }
   launch_cell_build(c, d_pos, false, false, st);
   const size_t smem = sizeof(double) * nt4;
-  if (mode == DERIV_PARAMS)
+  if (mode == DERIV_PARAMS) {
     k_deriv_fp64<DERIV_PARAMS><<<blocks, 128, smem, st>>>(
         g, c->fc, c->stencil, c->ntypes, c->d_lj64, c->d_start, c->d_spos64, c->d_smeta,
         c->d_sidx, c->d_ex_start, c->d_ex, nullptr, nullptr, d_dq, c->d_tpart);
-  else
-    k_deriv_fp64<DERIV_VJP><<<blocks, 128, smem, st>>>(
-        g, c->fc, c->stencil, c->ntypes, c->d_lj64, c->d_start, c->d_spos64, c->d_smeta,
-        c->d_sidx, c->d_ex_start, c->d_ex, d_w, d_hv, d_dq, c->d_tpart);
-  k_reduce_columns<<<(int)((nt4 + 127) / 128), 128, 0, st>>>(blocks, (int)nt4, c->d_tpart,
-                                                               d_dlj);
+  } else {
+    if (c->n > 0)
+      k_gather_sorted<<<(c->n + 255) / 256, 256, 0, st>>>(c->n, c->d_sidx, d_w, c->d_wsorted);
+    if (params)
+      k_deriv_fp64<DERIV_VJP, true><<<blocks, 128, smem, st>>>(
+          g, c->fc, c->stencil, c->ntypes, c->d_lj64, c->d_start, c->d_spos64, c->d_smeta,
+          c->d_sidx, c->d_ex_start, c->d_ex, c->d_wsorted, d_hv, d_dq, c->d_tpart);
+    else
+      k_deriv_fp64<DERIV_VJP, false><<<blocks, 128, smem, st>>>(
+          g, c->fc, c->stencil, c->ntypes, c->d_lj64, c->d_start, c->d_spos64, c->d_smeta,
+          c->d_sidx, c->d_ex_start, c->d_ex, c->d_wsorted, d_hv, nullptr, nullptr);
+  }
+  if (params)
+    k_reduce_columns<<<(int)((nt4 + 127) / 128), 128, 0, st>>>(blocks, (int)nt4, c->d_tpart,
+                                                                 d_dlj);
   CK(cudaGetLastError());
   return PMB200_OK;
 }

@@ -1297,13 +1297,16 @@ k_pair_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes, const dou
 // ---------------------------------------------------------------------------
 enum DerivMode { DERIV_PARAMS = 0, DERIV_VJP = 1 };
 
-template <int kMode>
+// kParams: also the parameter derivatives (dq, the table partials); a
+// VJP launch without them computes H w alone.  In VJP mode w is read in the
+// sorted order (ws[j] = w of sorted atom j, gathered by k_gather_sorted).
+template <int kMode, bool kParams = true>
 __global__ void __launch_bounds__(128)
 k_deriv_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes,
              const double4 *__restrict__ lj64, const int *__restrict__ start,
              const double4 *__restrict__ spos, const int2 *__restrict__ smeta,
              const int *__restrict__ sidx, const int *__restrict__ ex_start,
-             const int2 *__restrict__ ex, const double *__restrict__ w, double *__restrict__ hv,
+             const int2 *__restrict__ ex, const double4 *__restrict__ ws, double *__restrict__ hv,
              double *__restrict__ dq, double *__restrict__ tpart) {
   extern __shared__ double s_tab[];  // ntypes^2 * 4
   const int nt4 = ntypes * ntypes * 4;
@@ -1329,8 +1332,10 @@ k_deriv_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes,
       const int elo = ex_start[oi], ehi = ex_start[oi + 1];
       const int ti = mi.x * ntypes;
       double wi[3] = {0.0, 0.0, 0.0};
-      if (kMode == DERIV_VJP)
-        for (int k = 0; k < 3; k++) wi[k] = w[3 * (size_t)oi + k];
+      if (kMode == DERIV_VJP) {
+        const double4 wv = ws[i];
+        wi[0] = wv.x; wi[1] = wv.y; wi[2] = wv.z;
+      }
       double hx = 0, hy = 0, hz = 0, gq = 0;
       for (int r = 0; r < g.nrows; r++) {
         const Row row = st.rows[r];
@@ -1393,9 +1398,8 @@ k_deriv_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes,
               atomicAdd(&s_tab[tab], 0.5 * S * is6);
               atomicAdd(&s_tab[tab + 1], -0.5 * S * is3);
             } else {
-              const double wj0 = w[3 * (size_t)sidx[j]], wj1 = w[3 * (size_t)sidx[j] + 1],
-                           wj2 = w[3 * (size_t)sidx[j] + 2];
-              const double dl0 = wi[0] - wj0, dl1 = wi[1] - wj1, dl2 = wi[2] - wj2;
+              const double4 wj = ws[j];
+              const double dl0 = wi[0] - wj.x, dl1 = wi[1] - wj.y, dl2 = wi[2] - wj.z;
               const double dd = ddx * dl0 + ddy * dl1 + ddz * dl2;  // d . (w_i - w_j)
               const double Us = Ss * E + S * Es + pi.w * qf * phis;
               const double Uss = Sss * E + 2.0 * Ss * Es + S * Ess + pi.w * qf * phiss;
@@ -1403,10 +1407,12 @@ k_deriv_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes,
               hx += a * dl0 + b * ddx;
               hy += a * dl1 + b * ddy;
               hz += a * dl2 + b * ddz;
-              const double T = -2.0 * dd;  // 2 d . (w_j - w_i)
-              gq += qf * phis * T;
-              atomicAdd(&s_tab[tab], 0.5 * T * (Ss * is6 - 6.0 * S * is6 * is));
-              atomicAdd(&s_tab[tab + 1], 0.5 * T * (-Ss * is3 + 3.0 * S * is3 * is));
+              if (kParams) {
+                const double T = -2.0 * dd;  // 2 d . (w_j - w_i)
+                gq += qf * phis * T;
+                atomicAdd(&s_tab[tab], 0.5 * T * (Ss * is6 - 6.0 * S * is6 * is));
+                atomicAdd(&s_tab[tab + 1], 0.5 * T * (-Ss * is3 + 3.0 * S * is3 * is));
+              }
             }
           }
         }
@@ -1420,7 +1426,7 @@ k_deriv_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes,
         }
       }
       if (active && sub == 0) {
-        dq[oi] = gq;
+        if (kParams) dq[oi] = gq;
         if (kMode == DERIV_VJP) {
           hv[3 * (size_t)oi] = hx;
           hv[3 * (size_t)oi + 1] = hy;
@@ -1429,9 +1435,21 @@ k_deriv_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes,
       }
     }
   }
-  __syncthreads();
-  for (int k = threadIdx.x; k < nt4; k += blockDim.x)
-    tpart[(size_t)blockIdx.x * nt4 + k] = s_tab[k];
+  if (kParams) {
+    __syncthreads();
+    for (int k = threadIdx.x; k < nt4; k += blockDim.x)
+      tpart[(size_t)blockIdx.x * nt4 + k] = s_tab[k];
+  }
+}
+
+// ws[j] = w[3 sidx[j] ..] for the sorted atoms j (the direction of a
+// Hessian-vector product, read per pair in cell order).
+__global__ void k_gather_sorted(int n, const int *__restrict__ sidx, const double *__restrict__ w,
+                                double4 *__restrict__ ws) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const size_t o = 3 * (size_t)sidx[j];
+  ws[j] = make_double4(w[o], w[o + 1], w[o + 2], 0.0);
 }
 
 // out[k] = sum over rows r of part[r][k], rows added in order (deterministic).
