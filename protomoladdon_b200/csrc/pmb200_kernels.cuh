@@ -1337,6 +1337,23 @@ k_deriv_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes,
         wi[0] = wv.x; wi[1] = wv.y; wi[2] = wv.z;
       }
       double hx = 0, hy = 0, hz = 0, gq = 0;
+      // table derivatives of this lane's plain pairs, per j type, in
+      // registers (with few types the block's shared sums would see every
+      // lane add to the same entry); modified pairs and larger tables go to
+      // the shared sums directly
+      constexpr int kRegTypes = 4;
+      const bool regtab = kParams && ntypes <= kRegTypes;
+      double ta[kRegTypes] = {0.0, 0.0, 0.0, 0.0}, tb[kRegTypes] = {0.0, 0.0, 0.0, 0.0};
+      auto table_add = [&](int tj, int kind_, int tab_, double va, double vb) {
+        if (regtab && kind_ == 0) {
+#pragma unroll
+          for (int k = 0; k < kRegTypes; k++)
+            if (k == tj) { ta[k] += va; tb[k] += vb; }
+        } else {
+          atomicAdd(&s_tab[tab_], va);
+          atomicAdd(&s_tab[tab_ + 1], vb);
+        }
+      };
       for (int r = 0; r < g.nrows; r++) {
         const Row row = st.rows[r];
         int jy = cy + row.dy, jz = cz + row.dz;
@@ -1395,8 +1412,7 @@ k_deriv_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes,
             const int tab = (ti + mj.x) * 4 + (kind == 1 ? 2 : 0);
             if (kMode == DERIV_PARAMS) {
               gq += qf * phi;
-              atomicAdd(&s_tab[tab], 0.5 * S * is6);
-              atomicAdd(&s_tab[tab + 1], -0.5 * S * is3);
+              table_add(mj.x, kind, tab, 0.5 * S * is6, -0.5 * S * is3);
             } else {
               const double4 wj = ws[j];
               const double dl0 = wi[0] - wj.x, dl1 = wi[1] - wj.y, dl2 = wi[2] - wj.z;
@@ -1410,8 +1426,8 @@ k_deriv_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes,
               if (kParams) {
                 const double T = -2.0 * dd;  // 2 d . (w_j - w_i)
                 gq += qf * phis * T;
-                atomicAdd(&s_tab[tab], 0.5 * T * (Ss * is6 - 6.0 * S * is6 * is));
-                atomicAdd(&s_tab[tab + 1], 0.5 * T * (-Ss * is3 + 3.0 * S * is3 * is));
+                table_add(mj.x, kind, tab, 0.5 * T * (Ss * is6 - 6.0 * S * is6 * is),
+                          0.5 * T * (-Ss * is3 + 3.0 * S * is3 * is));
               }
             }
           }
@@ -1423,6 +1439,12 @@ k_deriv_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes,
           hx += __shfl_xor_sync(0xffffffffu, hx, off);
           hy += __shfl_xor_sync(0xffffffffu, hy, off);
           hz += __shfl_xor_sync(0xffffffffu, hz, off);
+        }
+      }
+      if (regtab && active) {  // the lane's register sums into the block's table
+        for (int k = 0; k < ntypes; k++) {
+          if (ta[k] != 0.0) atomicAdd(&s_tab[(ti + k) * 4], ta[k]);
+          if (tb[k] != 0.0) atomicAdd(&s_tab[(ti + k) * 4 + 1], tb[k]);
         }
       }
       if (active && sub == 0) {
