@@ -203,7 +203,10 @@ int pmb200_last_pair_count(pmb200_ctx *ctx, long long *pairs);
  * protomol/src/protomol/integrator/leapfrog/LeapfrogIntegrator.cpp:72-85)
  * followed, for the listed rigid waters, by SETTLE and v = (x_new - x_old)/h
  * (the role of ProtoMol's SHAKE modifier).  kick is 1 for a full kick, 0.5
- * for the first half kick.  Runs on the calling thread; no GPU. */
+ * for the first half kick.  An atom belongs to at most one water
+ * (PMB200_EINVAL otherwise); each water's atoms are kicked, drifted and
+ * constrained in one pass.  Runs on the host (OpenMP threads for large
+ * systems); no GPU. */
 int pmb200_host_kick_drift(int n, double *pos, double *vel,
                            const double *forces, const double *mass,
                            double dt_fs, double kick, int nwater,

@@ -1555,22 +1555,30 @@ int pmb200_host_kick_drift(int n, double *pos, double *vel, const double *forces
     return PMB200_EINVAL;
   if (nwater < 0 || (nwater > 0 && !widx)) return PMB200_EINVAL;
   const double h = dt_fs * 0.02045482828087295;  // Constant::INV_TIMEFACTOR
-  for (int w = 0; w < 3 * nwater; w++)
-    if (widx[w] < 0 || widx[w] >= n) return PMB200_EINVAL;
-  // the host's cores share the atoms and the waters (independent per atom /
-  // per water); the pre-step positions live in a per-thread-reused buffer
-  static thread_local std::vector<double> old;
-  if (nwater > 0) old.resize(3 * (size_t)n);
+  // which atoms the rigid waters hold (each at most once)
+  static thread_local std::vector<unsigned char> in_water;
+  if (nwater > 0) {
+    in_water.assign((size_t)n, 0);
+    for (int w = 0; w < 3 * nwater; w++) {
+      const int a = widx[w];
+      if (a < 0 || a >= n || in_water[a]) return PMB200_EINVAL;
+      in_water[a] = 1;
+    }
+  }
   const double kh = kick * h, inv_h = 1.0 / h;
-  double *op = nwater > 0 ? old.data() : nullptr;
+  // atoms outside the waters: kick and drift (independent per atom, shared
+  // by the host's cores)
+  if (3 * nwater < n) {
+    const unsigned char *inw = nwater > 0 ? in_water.data() : nullptr;
 #pragma omp parallel for schedule(static) if (n > 4096)
-  for (int i = 0; i < n; i++) {
-    const double s = kh / mass[i];
-    for (int k = 0; k < 3; k++) {
-      const size_t q = 3 * (size_t)i + k;
-      if (op) op[q] = pos[q];
-      vel[q] += forces[q] * s;
-      pos[q] += vel[q] * h;
+    for (int i = 0; i < n; i++) {
+      if (inw && inw[i]) continue;
+      const double s = kh / mass[i];
+      for (int k = 0; k < 3; k++) {
+        const size_t q = 3 * (size_t)i + k;
+        vel[q] += forces[q] * s;
+        pos[q] += vel[q] * h;
+      }
     }
   }
   if (nwater > 0) {
@@ -1582,16 +1590,30 @@ int pmb200_host_kick_drift(int n, double *pos, double *vel, const double *forces
     sp.rb = t - sp.ra;
     const double inv_m = 1.0 / (mo + 2.0 * mh), inv_ra = 1.0 / sp.ra;
     const int ngroups = (nwater + kW - 1) / kW;  // kW waters per iteration
+    // one pass per group of waters: kick and drift its atoms (the pre-step
+    // positions kept on the stack), constrain, and take the velocities from
+    // the constrained displacement
 #pragma omp parallel for schedule(static) if (nwater > 1024)
     for (int gidx = 0; gidx < ngroups; gidx++) {
       const int w0 = gidx * kW, wn = std::min(kW, nwater - w0);
+      double old[kW][3][3];
+      for (int l = 0; l < wn; l++)
+        for (int m = 0; m < 3; m++) {
+          const int a = widx[3 * (w0 + l) + m];
+          const double s = kh / mass[a];
+          for (int k = 0; k < 3; k++) {
+            const size_t q = 3 * (size_t)a + k;
+            old[l][m][k] = pos[q];
+            vel[q] += forces[q] * s;
+            pos[q] += vel[q] * h;
+          }
+        }
       if (wn == kW) {
         const double *A0[kW], *B0[kW], *C0[kW];
         double *A1[kW], *B1[kW], *C1[kW];
         for (int l = 0; l < kW; l++) {
           const int *wi = widx + 3 * (w0 + l);
-          A0[l] = op + 3 * (size_t)wi[0]; B0[l] = op + 3 * (size_t)wi[1];
-          C0[l] = op + 3 * (size_t)wi[2];
+          A0[l] = old[l][0]; B0[l] = old[l][1]; C0[l] = old[l][2];
           A1[l] = pos + 3 * (size_t)wi[0]; B1[l] = pos + 3 * (size_t)wi[1];
           C1[l] = pos + 3 * (size_t)wi[2];
         }
@@ -1599,17 +1621,16 @@ int pmb200_host_kick_drift(int n, double *pos, double *vel, const double *forces
       } else {
         for (int l = 0; l < wn; l++) {
           const int *wi = widx + 3 * (w0 + l);
-          host_settle(sp, inv_m, inv_ra, op + 3 * (size_t)wi[0], op + 3 * (size_t)wi[1],
-                      op + 3 * (size_t)wi[2], pos + 3 * (size_t)wi[0],
-                      pos + 3 * (size_t)wi[1], pos + 3 * (size_t)wi[2]);
+          host_settle(sp, inv_m, inv_ra, old[l][0], old[l][1], old[l][2],
+                      pos + 3 * (size_t)wi[0], pos + 3 * (size_t)wi[1],
+                      pos + 3 * (size_t)wi[2]);
         }
       }
-      // velocities from the constrained displacement
       for (int l = 0; l < wn; l++)
         for (int m = 0; m < 3; m++)
           for (int k = 0; k < 3; k++) {
             const size_t q = 3 * (size_t)widx[3 * (w0 + l) + m] + k;
-            vel[q] = (pos[q] - op[q]) * inv_h;
+            vel[q] = (pos[q] - old[l][m][k]) * inv_h;
           }
     }
   }

@@ -141,6 +141,34 @@ def test_host_kick_drift_matches_numpy_settle():
     assert np.abs(p1 - p2).max() < 1e-12 and np.abs(v1 - v2).max() < 1e-9
 
 
+def test_host_kick_drift_free_atoms_and_bad_water_lists():
+    """Atoms outside the listed waters are kicked and drifted only; a water
+    list that names an atom twice, or an atom out of range, is refused
+    before anything is updated."""
+    from protomoladdon_b200 import _lib, rigid
+    s = water.small_648()
+    w = water.rigid_waters(s)
+    rng = np.random.default_rng(2)
+    F = rng.normal(0, 20, s["pos"].shape)
+    # the last 10 waters are left free: their atoms follow plain leapfrog
+    p1, v1 = s["pos"].copy(), s["vel"].copy()
+    p2, v2 = s["pos"].copy(), s["vel"].copy()
+    rigid.kick_drift_settle(p1, v1, F, s["mass"], 1.0, w[:-10], water.D_OH, water.D_HH)
+    rigid.host_kick_drift(p2, v2, F, s["mass"], 1.0, w[:-10], water.D_OH, water.D_HH)
+    assert np.abs(p1 - p2).max() < 1e-12 and np.abs(v1 - v2).max() < 1e-9
+    free = np.asarray(w[-10:]).reshape(-1)
+    h = 1.0 * 0.02045482828087295
+    v_ref = s["vel"][free] + F[free] * (h / s["mass"][free])[:, None]
+    np.testing.assert_allclose(v2[free], v_ref, rtol=1e-14, atol=0)
+    np.testing.assert_allclose(p2[free], s["pos"][free] + v_ref * h, rtol=1e-14, atol=1e-14)
+    for bad in (np.concatenate([w[:2], w[:1]]), np.array([[0, 1, s["n"]]], np.int32)):
+        p3, v3 = s["pos"].copy(), s["vel"].copy()
+        with pytest.raises(_lib.PmbError) as ei:
+            rigid.host_kick_drift(p3, v3, F, s["mass"], 1.0, bad, water.D_OH, water.D_HH)
+        assert ei.value.code == _lib.PMB200_EINVAL
+        assert np.array_equal(p3, s["pos"]) and np.array_equal(v3, s["vel"])
+
+
 def test_lj_table_mixing_matches_the_generator():
     """autograd.lj_table (torch, differentiable) reproduces the water
     generator's table, ions included."""
