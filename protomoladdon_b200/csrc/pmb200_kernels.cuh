@@ -350,6 +350,13 @@ __device__ __forceinline__ long long warp_sum_ll(long long v, int width) {
 
 // Lanes per i-atom for a chunk of m atoms: the largest power of two L <= 8
 // with m * L <= 32.
+// floor(a / d) for 0 <= a <= 32 and 1 <= d <= 32: (a + 1/2) / d lies at
+// least 1 / 64 from an integer, far more than the error of the fast FP32
+// division (a few ulp), so truncation gives the quotient
+__device__ __forceinline__ int small_quot(int a, int d) {
+  return (int)__fdividef((float)a + 0.5f, (float)d);
+}
+
 __device__ __forceinline__ int lanes_per_atom(int m) {
   int L = 1;
   while (L < 8 && m * (L * 2) <= 32) L <<= 1;
@@ -363,8 +370,9 @@ __device__ __forceinline__ int lanes_per_atom(int m) {
 // half-shell stencil (every cell pair once; the home cell pairs i < j).
 // Warps never wait for one another.
 //
-// Per warp: the cell's atoms are taken in chunks of at most 32 / L, each atom
-// served by L lanes that split the candidates by index.  Candidate j atoms
+// Per warp: the cell's atoms are taken in chunks of at most 32, every lane
+// serving one atom (32 / m or 32 / m + 1 lanes per atom of an m-atom chunk,
+// splitting its candidates by index).  Candidate j atoms
 // are staged in shared memory in batches of at most kBatch, already shifted
 // into the i-cell's frame (integer cell offsets in cell units, so no
 // per-offset rounding bias); atoms beyond the cutoff of the box around the
@@ -462,9 +470,16 @@ __device__ __forceinline__ void mixed_task(
 
   for (int c0 = cs; c0 < ce; c0 += 32) {
     const int m = min(32, ce - c0);
-    const int L = lanes_per_atom(m);
-    const int ia = lane / L;
-    const int sub = lane % L;
+    // every lane serves one of the chunk's atoms: atom ia owns the L
+    // contiguous lanes whose first has sub 0 (the first 32 % m atoms one
+    // lane more than the others), and each lane takes every L-th candidate
+    const int base = small_quot(32, m), extra = 32 - base * m, split = extra * (base + 1);
+    const bool wide = lane < split;
+    const int L = wide ? base + 1 : base;
+    const int la = wide ? lane : lane - split;
+    const int q = small_quot(la, L);
+    const int ia = wide ? q : extra + q;
+    const int sub = la - q * L;
     const bool active = ia < m;
     const int i = c0 + (active ? ia : 0);
     const float4 pi = spos[i];
@@ -472,7 +487,7 @@ __device__ __forceinline__ void mixed_task(
     const int oi = sidx[i];
     const int elo = ex_start[oi], ehi = ex_start[oi + 1];
     const int ti = mi.x * ntypes;
-    // the box around the chunk's i atoms (idle lanes hold the chunk's first)
+    // the box around the chunk's i atoms
     float blo_x = pi.x, blo_y = pi.y, blo_z = pi.z, bhi_x = pi.x, bhi_y = pi.y, bhi_z = pi.z;
     for (int off = 16; off > 0; off >>= 1) {
       blo_x = fminf(blo_x, __shfl_xor_sync(0xffffffffu, blo_x, off));
@@ -483,7 +498,7 @@ __device__ __forceinline__ void mixed_task(
       bhi_z = fmaxf(bhi_z, __shfl_xor_sync(0xffffffffu, bhi_z, off));
     }
     // a batch holds at most kBatch / 2 candidates per lane (the list depth)
-    const int batch_cap = min(kBatch, (kBatch / 2) * L);
+    const int batch_cap = min(kBatch, (kBatch / 2) * base);
     long long fx = 0, fy = 0, fz = 0;
     // FP64 Coulomb sums of the cutoff form (see kExactE)
     double eU = 0.0, eQ = 0.0, eR = 0.0;
@@ -960,10 +975,16 @@ __device__ __forceinline__ void mixed_task(
     }
     if (nb > 0) flush_batch();
 
-    // the i forces: the lanes of an atom, then the global accumulator
-    fx = warp_sum_ll(fx, L);
-    fy = warp_sum_ll(fy, L);
-    fz = warp_sum_ll(fz, L);
+    // the i forces: summed over the atom's lanes [lane - sub, seg_end) into
+    // its first lane (after the step with offset d, a lane holds the sum of
+    // its lanes up to 2d ahead, within the atom), then the global accumulator
+    const int seg_end = lane - sub + L;
+    for (int off = 1; off < base + (extra ? 1 : 0); off <<= 1) {
+      const long long vx = __shfl_down_sync(0xffffffffu, fx, off);
+      const long long vy = __shfl_down_sync(0xffffffffu, fy, off);
+      const long long vz = __shfl_down_sync(0xffffffffu, fz, off);
+      if (lane + off < seg_end) { fx += vx; fy += vy; fz += vz; }
+    }
     if (active && sub == 0) {
       atomicAdd(&facc[i], (unsigned long long)fx);
       atomicAdd(&facc[(size_t)n + i], (unsigned long long)fy);
