@@ -404,9 +404,13 @@ constexpr float kJScale = 262144.0f; // shared j-force quanta (2^-18) per cell-u
 constexpr int kJShift = 14;          // to the global 2^-32 quanta
 constexpr float kJLimit = 6.7e7f;    // per-contribution bound: 32 contributions fit int32
 constexpr float kJToGlobal = 16384.0f;  // 2^-18 quanta -> the accumulator's 2^-32 quanta
-#ifndef PMB200_SPREAD_COST
-#define PMB200_SPREAD_COST 25   // cost of a round of dealt pairs, in tenths of an own round
+#ifndef PMB200_DEAL_UNIT
+#define PMB200_DEAL_UNIT 3      // leftover entries dealt to a lane at a time
 #endif
+#ifndef PMB200_SPREAD_COST
+#define PMB200_SPREAD_COST 40   // cost of a round of dealt units, in tenths of an own round
+#endif
+constexpr int kDealUnit = PMB200_DEAL_UNIT;
 
 struct __align__(16) MixedWarpSmem {
   float4 pos[kBatch];                    // staged j atoms, shifted into the i-cell frame
@@ -568,9 +572,12 @@ __device__ __forceinline__ void mixed_task(
       // takes the first kmin entries of its own list (kmin = the shortest
       // active list), then the remaining entries of the longer lists are
       // dealt over the whole warp, so no lane idles while another finishes a
-      // long list; a round of dealt pairs (shuffled i data, shared i-force
-      // sums) is counted as 2.5 rounds of own pairs (the best of 1.5 to 4 on
-      // the 41k and 327k water boxes)
+      // long list.  Leftovers go out in units of up to kDealUnit = 3
+      // consecutive entries of one list (one search and one exchange of i
+      // data per unit); a round of dealt units (shuffled i data, shared
+      // i-force sums) is counted as 4 rounds of own pairs.  (Measured on the
+      // 41k and 327k water boxes: units of 1, 2, 3, 4 and 6 at costs from
+      // 1.5 to 8; 3 at 4 to 5 is best on both.)
       const int kmin = __reduce_min_sync(0xffffffffu, active ? cnt : 0x7fffffff);
       const int maxc = __reduce_max_sync(0xffffffffu, cnt);
       float px = 0.f, py = 0.f, pz = 0.f, pE = 0.f;
@@ -776,30 +783,36 @@ __device__ __forceinline__ void mixed_task(
         }
       };
       int left = active ? cnt - kmin : 0;
-      int linc = left;  // inclusive prefix of the leftover counts
+      // leftovers are dealt in units of up to kDealUnit consecutive entries
+      // of one lane's list, so that one search for the source lane and one
+      // exchange of its atom's data serve several pairs
+      int units = (left + kDealUnit - 1) / kDealUnit;
+      int uinc = units;  // inclusive prefix of the unit counts
       for (int off = 1; off < 32; off <<= 1) {
-        const int v = __shfl_up_sync(0xffffffffu, linc, off);
-        if (lane >= off) linc += v;
+        const int v = __shfl_up_sync(0xffffffffu, uinc, off);
+        if (lane >= off) uinc += v;
       }
-      int ltot = __shfl_sync(0xffffffffu, linc, 31);
-      if (10 * (maxc - kmin) <= PMB200_SPREAD_COST * ((ltot + 31) >> 5)) {
-        ltot = 0;  // one phase: each lane walks its whole list
+      int utot = __shfl_sync(0xffffffffu, uinc, 31);
+      if (10 * (maxc - kmin) <= PMB200_SPREAD_COST * ((utot + 31) >> 5)) {
+        utot = 0;  // one phase: each lane walks its whole list
         left = 0;
       }
-      // (idle lanes, past the chunk's atoms, have no list: they skip phase 1)
       const int kown = active ? cnt - left : 0;
       for (int k = 0; k < kown; k++)
         pair(sm.list[k][lane], true, pi, mi.y, elo, ehi, ti, (size_t)i, lane, pid_x, pid_y,
              pid_z, Ri[0], Ri[1], Ri[2]);
-      for (int base = 0; base < ltot; base += 32) {
-        const int e = base + lane;
-        int src = 0;  // the lane whose leftovers hold entry e
+      for (int base = 0; base < utot; base += 32) {
+        const int u = base + lane;
+        int src = 0;  // the lane whose leftovers hold unit u
         for (int step = 16; step > 0; step >>= 1) {
-          const int v = __shfl_sync(0xffffffffu, linc, src + step - 1);
-          if (v <= e) src += step;
+          const int v = __shfl_sync(0xffffffffu, uinc, src + step - 1);
+          if (v <= u) src += step;
         }
-        const int k = kmin + e - (__shfl_sync(0xffffffffu, linc, src) -
-                                  __shfl_sync(0xffffffffu, left, src));
+        const int u0 = __shfl_sync(0xffffffffu, uinc, src) -
+                       __shfl_sync(0xffffffffu, units, src);  // src's first unit
+        const int lsrc = __shfl_sync(0xffffffffu, left, src);  // (every lane shuffles)
+        const int k = kmin + kDealUnit * (u - u0);
+        const int nk = u < utot ? min(kDealUnit, kmin + lsrc - k) : 0;
         float4 a4;
         a4.x = __shfl_sync(0xffffffffu, pi.x, src);
         a4.y = __shfl_sync(0xffffffffu, pi.y, src);
@@ -821,11 +834,11 @@ __device__ __forceinline__ void mixed_task(
           ry = __shfl_sync(0xffffffffu, Ri[1], src);
           rz = __shfl_sync(0xffffffffu, Ri[2], src);
         }
-        if (e < ltot)
-          pair(sm.list[k][src], false, a4, moli, elo_, ehi_, ti_, (size_t)ii, src, pix, piy,
+        for (int r = 0; r < nk; r++)
+          pair(sm.list[k + r][src], false, a4, moli, elo_, ehi_, ti_, (size_t)ii, src, pix, piy,
                piz, rx, ry, rz);
       }
-      if (ltot > 0) {  // the shared i-force sums of the leftovers, per lane
+      if (utot > 0) {  // the shared i-force sums of the leftovers, per lane
         __syncwarp();
         fx += (long long)sm.fi[0][lane] << kJShift;
         fy += (long long)sm.fi[1][lane] << kJShift;
