@@ -77,6 +77,9 @@ struct pmb200_ctx {
   double4 *d_rel64 = nullptr, *d_spos64 = nullptr;
   int2 *d_smeta = nullptr;
   unsigned long long *d_facc = nullptr;
+  // d_count holds zeros between evaluations (k_scan clears it after reading);
+  // false after a launch sequence broke off, when the next build clears it
+  bool count_zero = false;
   double *d_com = nullptr;
   // derivative kernels: per-block table rows and scratch outputs
   double *d_tpart = nullptr, *d_gq = nullptr, *d_glj = nullptr;
@@ -315,9 +318,13 @@ int ensure_atom_buffers(pmb200_ctx *c) {
 // The pair kernels for the flags asked for (template instances per form),
 // over the i-cells [cell0, cell0 + ncells) (all by default) into the fixed-
 // point accumulator facc (the context's by default).
+// pdl: the previous operation on `st` is the cell build's last kernel; the
+// pair kernel is then launched as its programmatic dependent, so that its
+// launch and prologue overlap that kernel's tail (it waits for it before
+// reading the sorted atoms).
 template <int F>
 void launch_pair_mixed(pmb200_ctx *c, unsigned flags, cudaStream_t st, int cell0 = 0,
-                       int ncells = -1, unsigned long long *facc = nullptr) {
+                       int ncells = -1, unsigned long long *facc = nullptr, bool pdl = false) {
   const GridParams &g = c->g;
   if (ncells < 0) ncells = g.ncell;
   if (!facc) facc = c->d_facc;
@@ -326,11 +333,21 @@ void launch_pair_mixed(pmb200_ctx *c, unsigned flags, cudaStream_t st, int cell0
   const bool molvir = (flags & PMB200_MOLVIRIAL) != 0;
   const size_t smem = mixed_smem_bytes(F, c->ntypes, c->half.ncells);
   const int slots = mixed_cell_slots(energy || virial, c->n, g.ncell);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(std::max(ncells, 1) * slots));
+  cfg.blockDim = dim3(32);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = (pdl && PMB200_PDL) ? 1 : 0;
 #define PMB_MIXED_LAUNCH(E, V, M)                                                          \
-  k_pair_mixed<F, E, V, M><<<std::max(ncells, 1) * slots, 32, smem, st>>>(                 \
-      g, c->mc, c->half, c->ntypes, c->d_lj32, c->d_start, c->d_spos32, c->d_smeta,         \
-      c->d_sidx, c->d_ex_start, c->d_ex, facc, c->n, c->d_err, c->d_partial, c->pb,         \
-      c->d_com, slots, c->d_spos_lo, ncells > 0 ? cell0 : g.ncell)
+  cudaLaunchKernelEx(&cfg, k_pair_mixed<F, E, V, M>, g, c->mc, c->half, c->ntypes,         \
+                     c->d_lj32, c->d_start, c->d_spos32, c->d_smeta, c->d_sidx,             \
+                     c->d_ex_start, c->d_ex, facc, c->n, c->d_err, c->d_partial, c->pb,     \
+                     c->d_com, slots, c->d_spos_lo, ncells > 0 ? cell0 : g.ncell)
   if (molvir) PMB_MIXED_LAUNCH(true, true, true);
   else if (energy && virial) PMB_MIXED_LAUNCH(true, true, false);
   else if (energy) PMB_MIXED_LAUNCH(true, false, false);
@@ -360,6 +377,16 @@ void launch_pair_fp64(pmb200_ctx *c, unsigned flags, double *d_forces, int accum
 #undef PMB_FP64_LAUNCH
 }
 
+// Zeroes d_count when a launch sequence broke off after using it; a captured
+// graph relies on its previous run having left it cleared.
+int ensure_clear(pmb200_ctx *c, cudaStream_t st) {
+  if (!c->count_zero && c->d_count && c->g.ncell > 0) {
+    CK(cudaMemsetAsync(c->d_count, 0, sizeof(int) * (size_t)c->g.ncell, st));
+    c->count_zero = true;
+  }
+  return PMB200_OK;
+}
+
 // Launch one evaluation on `st`.  accumulate: add into d_forces (1) or
 // overwrite it (0).
 // Counting sort of the atoms into the grid cells (cell index, scan,
@@ -370,7 +397,8 @@ void launch_cell_build(pmb200_ctx *c, const double *d_pos, bool mixed, bool lo,
                        cudaStream_t st) {
   const int n = c->n;
   const GridParams &g = c->g;
-  cudaMemsetAsync(c->d_count, 0, sizeof(int) * g.ncell, st);
+  if (!c->count_zero) cudaMemsetAsync(c->d_count, 0, sizeof(int) * g.ncell, st);
+  c->count_zero = false;
   if (n > 0) {
     const int tb = 256;
     k_cell_index<<<(n + tb - 1) / tb, tb, 0, st>>>(
@@ -379,6 +407,7 @@ void launch_cell_build(pmb200_ctx *c, const double *d_pos, bool mixed, bool lo,
         lo ? c->d_rel_lo : nullptr);
   }
   k_scan<<<1, 1024, 1024 * sizeof(int), st>>>(g.ncell, c->d_count, c->d_start);
+  c->count_zero = cudaPeekAtLastError() == cudaSuccess;
   if (n > 0) {
     const int tb = 256;
     k_scatter<<<(n + tb - 1) / tb, tb, 0, st>>>(n, c->d_cell_of, c->d_slot, c->d_start,
@@ -400,6 +429,11 @@ int launch_eval(pmb200_ctx *c, const double *d_pos, double *d_forces, double *d_
   const bool virial = (flags & (PMB200_VIRIAL | PMB200_MOLVIRIAL)) != 0;
   const bool molvir = (flags & PMB200_MOLVIRIAL) != 0;
   const GridParams &g = c->g;
+  // the accumulator is cleared before the cell build (still in L2 when the
+  // pair kernel adds to it), so that the pair kernel follows the build's last
+  // kernel directly
+  if (mixed && n > 0)
+    CK(cudaMemsetAsync(c->d_facc, 0, sizeof(unsigned long long) * 3 * (size_t)n, st));
   launch_cell_build(c, d_pos, mixed, mixed && energy && c->form == FORM_CUTOFF, st);
   CK(cudaGetLastError());
   const int blocks = (g.ncell + 3) / 4;
@@ -414,11 +448,16 @@ int launch_eval(pmb200_ctx *c, const double *d_pos, double *d_forces, double *d_
   if (timed) CK(cudaEventRecord(c->ev0, st));
   if (mixed) {
     const double fscale = 1.0 / g.unit;
-    if (n > 0) CK(cudaMemsetAsync(c->d_facc, 0, sizeof(unsigned long long) * 3 * (size_t)n, st));
-    if (c->form == FORM_GENERIC) launch_pair_mixed<FORM_GENERIC>(c, flags, st);
-    else if (c->form == FORM_EWALD_POLY5) launch_pair_mixed<FORM_EWALD_POLY5>(c, flags, st);
-    else if (c->form == FORM_EWALD_EXACT) launch_pair_mixed<FORM_EWALD_EXACT>(c, flags, st);
-    else launch_pair_mixed<FORM_CUTOFF>(c, flags, st);
+    // (a programmatic dependent of the cell build's last kernel, except in
+    // timed launches, whose events bracket the pair kernel alone)
+    const bool pdl = !timed;
+    if (c->form == FORM_GENERIC)
+      launch_pair_mixed<FORM_GENERIC>(c, flags, st, 0, -1, nullptr, pdl);
+    else if (c->form == FORM_EWALD_POLY5)
+      launch_pair_mixed<FORM_EWALD_POLY5>(c, flags, st, 0, -1, nullptr, pdl);
+    else if (c->form == FORM_EWALD_EXACT)
+      launch_pair_mixed<FORM_EWALD_EXACT>(c, flags, st, 0, -1, nullptr, pdl);
+    else launch_pair_mixed<FORM_CUTOFF>(c, flags, st, 0, -1, nullptr, pdl);
     if (n > 0)
       k_finalize<<<(n + 255) / 256, 256, 0, st>>>(n, c->d_facc, c->d_sidx, fscale * kFixInv,
                                                   accumulate, d_forces);
@@ -853,6 +892,8 @@ int pmb200_set_box(pmb200_ctx *c, const double e1[3], const double e2[3], const 
   }
   if (c->ncell_alloc < g.ncell) {
     CK(dalloc(c->d_count, (size_t)g.ncell));
+    CK(cudaMemset(c->d_count, 0, sizeof(int) * (size_t)g.ncell));
+    c->count_zero = true;
     CK(dalloc(c->d_start, (size_t)g.ncell + 1));
     CK(dalloc(c->d_partial, (size_t)g.ncell * kEnergyCellSlots * kNacc));
     c->ncell_alloc = g.ncell;
@@ -1219,6 +1260,8 @@ int pmb200_eval(pmb200_ctx *c, const double *pos, double *forces, double *energi
         c->hgraph_src = src;
         c->hgraph_flags = flags;
       }
+      rc = ensure_clear(c, st);
+      if (rc) return rc;
       CK(cudaGraphLaunch(c->hgraph_exec, st));
     }
   } else {
@@ -1296,6 +1339,8 @@ int pmb200_leapfrog_device(pmb200_ctx *c, double *d_pos, double *d_vel, double *
       for (int k = 0; k < 4; k++) c->graph_key[k] = key[k];
       c->graph_dt = dt_fs;
     }
+    rc = ensure_clear(c, st);
+    if (rc) return rc;
     for (int s = 0; s < middle; s++) CK(cudaGraphLaunch(c->graph_exec, st));
   }
   if (nsteps >= 2) {
@@ -1345,6 +1390,8 @@ int pmb200_step_device(pmb200_ctx *c, double *d_pos, double *d_vel, double *d_fo
     c->sgraph_dt = dt_fs;
     c->sgraph_flags = flags;
   }
+  rc = ensure_clear(c, st);
+  if (rc) return rc;
   CK(cudaGraphLaunch(c->sgraph_exec, st));
   return PMB200_OK;
 }

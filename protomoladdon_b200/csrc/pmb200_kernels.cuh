@@ -263,7 +263,8 @@ __global__ void k_cell_index(int n, const double *__restrict__ pos, GridParams g
 
 // Exclusive scan of cell counts in one block (C is a few thousand to a few
 // hundred thousand cells; each thread scans a contiguous span).
-__global__ void k_scan(int ncell, const int *__restrict__ count, int *__restrict__ start) {
+// (the counts are cleared once read, ready for the next build's atomics)
+__global__ void k_scan(int ncell, int *__restrict__ count, int *__restrict__ start) {
   extern __shared__ int sh[];
   const int T = blockDim.x;
   const int t = threadIdx.x;
@@ -283,8 +284,10 @@ __global__ void k_scan(int ncell, const int *__restrict__ count, int *__restrict
   }
   int base = sh[t] - s;
   for (int c = lo; c < hi; c++) {
+    const int v = count[c];
     start[c] = base;
-    base += count[c];
+    base += v;
+    count[c] = 0;
   }
   if (t == T - 1) start[ncell] = sh[T - 1];
 }
@@ -306,6 +309,9 @@ __global__ void k_rank_gather(int ncell, const int *__restrict__ start,
                               float4 *__restrict__ spos32, double4 *__restrict__ spos64,
                               int2 *__restrict__ smeta, const float4 *__restrict__ rel_lo,
                               float4 *__restrict__ spos_lo) {
+  // the pair kernel that follows may launch now (it waits for this grid
+  // before it reads anything this grid writes)
+  asm volatile("griddepcontrol.launch_dependents;");
   const int lane = threadIdx.x & 31;
   const int cell = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (cell >= ncell) return;
@@ -411,6 +417,9 @@ constexpr float kJToGlobal = 16384.0f;  // 2^-18 quanta -> the accumulator's 2^-
 #define PMB200_SPREAD_COST 40   // cost of a round of dealt units, in tenths of an own round
 #endif
 constexpr int kDealUnit = PMB200_DEAL_UNIT;
+#ifndef PMB200_PDL
+#define PMB200_PDL 1            // pair kernels launched as programmatic dependents
+#endif
 
 struct __align__(16) MixedWarpSmem {
   float4 pos[kBatch];                    // staged j atoms, shifted into the i-cell frame
@@ -1071,6 +1080,10 @@ k_pair_mixed(GridParams g, MixedConsts mc, const HalfStencil st, int ntypes, con
   for (int t = lane; t < kBatch; t += 32) sm.jf[0][t] = sm.jf[1][t] = sm.jf[2][t] = 0;
   sm.fi[0][lane] = sm.fi[1][lane] = sm.fi[2][lane] = 0;
   __syncwarp();
+  // a launch that overlaps the cell build's last kernel (programmatic
+  // dependent launch) waits for it here, after a prologue that reads only
+  // data written before that kernel started; otherwise a no-op
+  asm volatile("griddepcontrol.wait;" ::: "memory");
   const int cell = cell0 + (int)(blockIdx.x / slots);  // cells cell0.. (a shard's range)
   if (cell >= g.ncell) return;  // uniform per block
   mixed_task<kForm, kEnergy, kVirial, kMolVir>(
