@@ -315,6 +315,25 @@ int ensure_atom_buffers(pmb200_ctx *c) {
   return PMB200_OK;
 }
 
+// Launches kernel k on st; pdl: as a programmatic dependent of the kernel
+// launched just before it on st (k calls pdl_wait before it touches that
+// kernel's data), so that its launch overlaps the predecessor's tail.
+template <class... Exp, class... Act>
+void launch_k(void (*k)(Exp...), unsigned grid, unsigned block, size_t smem, cudaStream_t st,
+              bool pdl, Act &&...args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = (pdl && PMB200_PDL) ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, k, std::forward<Act>(args)...);
+}
+
 // The pair kernels for the flags asked for (template instances per form),
 // over the i-cells [cell0, cell0 + ncells) (all by default) into the fixed-
 // point accumulator facc (the context's by default).
@@ -393,32 +412,30 @@ int ensure_clear(pmb200_ctx *c, cudaStream_t st) {
 // scatter, in-cell rank order), producing the cell-unit FP32 copies (mixed)
 // or the Angstrom FP64 copies of the sorted positions; lo: also the FP32
 // coordinates' rounding residuals (energy evaluations of the cutoff form).
+// clear3: an accumulator of 3n entries the build zeroes on the way (or null).
+// After the first kernel each one is launched as a programmatic dependent of
+// the one before it.
 void launch_cell_build(pmb200_ctx *c, const double *d_pos, bool mixed, bool lo,
-                       cudaStream_t st) {
+                       cudaStream_t st, unsigned long long *clear3 = nullptr) {
   const int n = c->n;
   const GridParams &g = c->g;
   if (!c->count_zero) cudaMemsetAsync(c->d_count, 0, sizeof(int) * g.ncell, st);
   c->count_zero = false;
-  if (n > 0) {
-    const int tb = 256;
-    k_cell_index<<<(n + tb - 1) / tb, tb, 0, st>>>(
-        n, d_pos, g, c->d_cell_of, c->d_count, c->d_slot, mixed ? c->d_rel32 : nullptr,
-        mixed ? nullptr : c->d_rel64, c->d_q, (float)(1.0 / std::sqrt(g.unit)), c->d_err,
-        lo ? c->d_rel_lo : nullptr);
-  }
-  k_scan<<<1, 1024, 1024 * sizeof(int), st>>>(g.ncell, c->d_count, c->d_start);
+  const unsigned nb = (unsigned)((n + 255) / 256);
+  if (n > 0)
+    launch_k(k_cell_index, nb, 256, 0, st, false, n, d_pos, g, c->d_cell_of, c->d_count,
+             c->d_slot, mixed ? c->d_rel32 : nullptr, mixed ? nullptr : c->d_rel64, c->d_q,
+             (float)(1.0 / std::sqrt(g.unit)), c->d_err, lo ? c->d_rel_lo : nullptr, clear3);
+  launch_k(k_scan, 1, 1024, 1024 * sizeof(int), st, n > 0, g.ncell, c->d_count, c->d_start);
   c->count_zero = cudaPeekAtLastError() == cudaSuccess;
-  if (n > 0) {
-    const int tb = 256;
-    k_scatter<<<(n + tb - 1) / tb, tb, 0, st>>>(n, c->d_cell_of, c->d_slot, c->d_start,
-                                                 c->d_tmp);
-  }
-  const int blocks = (g.ncell + 3) / 4;
-  k_rank_gather<<<blocks, 128, 0, st>>>(
-      g.ncell, c->d_start, c->d_tmp, mixed ? c->d_rel32 : nullptr,
-      mixed ? nullptr : c->d_rel64, c->d_type, c->d_mol, c->d_sidx,
-      mixed ? c->d_spos32 : nullptr, mixed ? nullptr : c->d_spos64, c->d_smeta,
-      lo ? c->d_rel_lo : nullptr, lo ? c->d_spos_lo : nullptr);
+  if (n > 0)
+    launch_k(k_scatter, nb, 256, 0, st, true, n, c->d_cell_of, c->d_slot, c->d_start,
+             c->d_tmp);
+  launch_k(k_rank_gather, (unsigned)((g.ncell + 3) / 4), 128, 0, st, true, g.ncell,
+           c->d_start, c->d_tmp, mixed ? c->d_rel32 : nullptr, mixed ? nullptr : c->d_rel64,
+           c->d_type, c->d_mol, c->d_sidx, mixed ? c->d_spos32 : nullptr,
+           mixed ? nullptr : c->d_spos64, c->d_smeta, lo ? c->d_rel_lo : nullptr,
+           lo ? c->d_spos_lo : nullptr);
 }
 
 int launch_eval(pmb200_ctx *c, const double *d_pos, double *d_forces, double *d_out,
@@ -429,12 +446,11 @@ int launch_eval(pmb200_ctx *c, const double *d_pos, double *d_forces, double *d_
   const bool virial = (flags & (PMB200_VIRIAL | PMB200_MOLVIRIAL)) != 0;
   const bool molvir = (flags & PMB200_MOLVIRIAL) != 0;
   const GridParams &g = c->g;
-  // the accumulator is cleared before the cell build (still in L2 when the
+  // the cell build clears the accumulator on the way (still in L2 when the
   // pair kernel adds to it), so that the pair kernel follows the build's last
   // kernel directly
-  if (mixed && n > 0)
-    CK(cudaMemsetAsync(c->d_facc, 0, sizeof(unsigned long long) * 3 * (size_t)n, st));
-  launch_cell_build(c, d_pos, mixed, mixed && energy && c->form == FORM_CUTOFF, st);
+  launch_cell_build(c, d_pos, mixed, mixed && energy && c->form == FORM_CUTOFF, st,
+                    mixed ? c->d_facc : nullptr);
   CK(cudaGetLastError());
   const int blocks = (g.ncell + 3) / 4;
   if (molvir && c->nmol > 0)
@@ -459,8 +475,9 @@ int launch_eval(pmb200_ctx *c, const double *d_pos, double *d_forces, double *d_
       launch_pair_mixed<FORM_EWALD_EXACT>(c, flags, st, 0, -1, nullptr, pdl);
     else launch_pair_mixed<FORM_CUTOFF>(c, flags, st, 0, -1, nullptr, pdl);
     if (n > 0)
-      k_finalize<<<(n + 255) / 256, 256, 0, st>>>(n, c->d_facc, c->d_sidx, fscale * kFixInv,
-                                                  accumulate, d_forces);
+      launch_k(k_finalize, (unsigned)((n + 255) / 256), 256, 0, st, pdl, n,
+               (const unsigned long long *)c->d_facc, (const int *)c->d_sidx, fscale * kFixInv,
+               accumulate, d_forces);
   } else {
     if (c->form == FORM_GENERIC)
       launch_pair_fp64<FORM_GENERIC>(c, flags, d_forces, accumulate, blocks, st);

@@ -213,6 +213,16 @@ struct HalfStencil {
 // The cell of one position: wrapped into the box in FP64, the cell
 // coordinates c and the offset r from the cell's lower corner (Angstrom).
 // Returns false for a non-finite coordinate (binned at the box corner).
+// Programmatic dependent launch (the kernels of one evaluation launched as
+// dependents of the one before them, so that each launch overlaps its
+// predecessor's tail).  pdl_wait: block until the predecessor grid has
+// completed and its writes are visible (a no-op for a kernel launched
+// normally); every kernel that may be launched so calls it before touching
+// data its predecessor reads or writes.  pdl_trigger: this grid's dependent
+// may launch now (it still waits for this grid's completion before use).
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;"); }
+
 __device__ __forceinline__ bool locate_cell(const double *xin, const GridParams &g, int c[3],
                                             double r[3]) {
   const int nd[3] = {g.nx, g.ny, g.nz};
@@ -233,14 +243,18 @@ __device__ __forceinline__ bool locate_cell(const double *xin, const GridParams 
   return ok;
 }
 
+// clear3: an accumulator of 3n entries zeroed on the way (or null).
 __global__ void k_cell_index(int n, const double *__restrict__ pos, GridParams g,
                              int *__restrict__ cell_of, int *__restrict__ cell_count,
                              int *__restrict__ slot, float4 *__restrict__ rel32,
                              double4 *__restrict__ rel64, const double *__restrict__ q,
                              float qscale32, int *__restrict__ err,
-                             float4 *__restrict__ rel_lo) {
+                             float4 *__restrict__ rel_lo,
+                             unsigned long long *__restrict__ clear3 = nullptr) {
+  pdl_trigger();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  if (clear3) clear3[i] = clear3[(size_t)n + i] = clear3[2 * (size_t)n + i] = 0;
   int c[3];
   double r[3];
   if (!locate_cell(pos + 3 * (size_t)i, g, c, r)) atomicOr(err, 1);
@@ -265,6 +279,8 @@ __global__ void k_cell_index(int n, const double *__restrict__ pos, GridParams g
 // hundred thousand cells; each thread scans a contiguous span).
 // (the counts are cleared once read, ready for the next build's atomics)
 __global__ void k_scan(int ncell, int *__restrict__ count, int *__restrict__ start) {
+  pdl_trigger();
+  pdl_wait();
   extern __shared__ int sh[];
   const int T = blockDim.x;
   const int t = threadIdx.x;
@@ -294,6 +310,8 @@ __global__ void k_scan(int ncell, int *__restrict__ count, int *__restrict__ sta
 
 __global__ void k_scatter(int n, const int *__restrict__ cell_of, const int *__restrict__ slot,
                           const int *__restrict__ start, int *__restrict__ tmp) {
+  pdl_trigger();
+  pdl_wait();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   tmp[start[cell_of[i]] + slot[i]] = i;
@@ -309,9 +327,8 @@ __global__ void k_rank_gather(int ncell, const int *__restrict__ start,
                               float4 *__restrict__ spos32, double4 *__restrict__ spos64,
                               int2 *__restrict__ smeta, const float4 *__restrict__ rel_lo,
                               float4 *__restrict__ spos_lo) {
-  // the pair kernel that follows may launch now (it waits for this grid
-  // before it reads anything this grid writes)
-  asm volatile("griddepcontrol.launch_dependents;");
+  pdl_trigger();
+  pdl_wait();
   const int lane = threadIdx.x & 31;
   const int cell = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (cell >= ncell) return;
@@ -1080,10 +1097,9 @@ k_pair_mixed(GridParams g, MixedConsts mc, const HalfStencil st, int ntypes, con
   for (int t = lane; t < kBatch; t += 32) sm.jf[0][t] = sm.jf[1][t] = sm.jf[2][t] = 0;
   sm.fi[0][lane] = sm.fi[1][lane] = sm.fi[2][lane] = 0;
   __syncwarp();
-  // a launch that overlaps the cell build's last kernel (programmatic
-  // dependent launch) waits for it here, after a prologue that reads only
-  // data written before that kernel started; otherwise a no-op
-  asm volatile("griddepcontrol.wait;" ::: "memory");
+  // a launch that overlaps the cell build's last kernel waits for it here,
+  // after a prologue that reads only data written before that kernel started
+  pdl_wait();
   const int cell = cell0 + (int)(blockIdx.x / slots);  // cells cell0.. (a shard's range)
   if (cell >= g.ncell) return;  // uniform per block
   mixed_task<kForm, kEnergy, kVirial, kMolVir>(
@@ -1113,6 +1129,7 @@ inline size_t mixed_smem_bytes(int form, int ntypes, int st_ncells) {
 __global__ void k_finalize(int n, const unsigned long long *__restrict__ facc,
                            const int *__restrict__ sidx, double scale, int accumulate,
                            double *__restrict__ forces) {
+  pdl_wait();
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n) return;
   const int o = sidx[j];
