@@ -1540,6 +1540,9 @@ static void host_settle(const SettleParams &sp, double inv_m, double inv_ra, con
 // vectorise and the waters' dependency chains (seven square roots and
 // divisions each) overlap.
 constexpr int kW = 4;
+// (also built for AVX2, picked at load time where the host has it: four
+// lanes per instruction instead of two; no FMA, so every host rounds alike)
+__attribute__((target_clones("avx2", "default")))
 static void host_settle_w(const SettleParams &sp, double inv_m, double inv_ra,
                           const double *const A0[kW], const double *const B0[kW],
                           const double *const C0[kW], double *const A1[kW],
