@@ -289,23 +289,35 @@ __global__ void k_scan(int ncell, int *__restrict__ count, int *__restrict__ sta
   const int hi = min(ncell, lo + span);
   int s = 0;
   for (int c = lo; c < hi; c++) s += count[c];
-  sh[t] = s;
-  __syncthreads();
-  // Hillis-Steele inclusive scan of the per-thread sums
-  for (int off = 1; off < T; off <<= 1) {
-    int v = (t >= off) ? sh[t - off] : 0;
-    __syncthreads();
-    sh[t] += v;
-    __syncthreads();
+  // inclusive scan of the per-thread sums: within each warp by shuffles,
+  // then over the warps' totals (at most 32 warps; blockDim is a multiple of
+  // 32) by the first warp
+  const int lane = t & 31, w = t >> 5, nw = T >> 5;
+  int x = s;
+  for (int off = 1; off < 32; off <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, x, off);
+    if (lane >= off) x += v;
   }
-  int base = sh[t] - s;
+  if (lane == 31) sh[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    int y = lane < nw ? sh[lane] : 0;
+    for (int off = 1; off < 32; off <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, y, off);
+      if (lane >= off) y += v;
+    }
+    if (lane < nw) sh[lane] = y;
+  }
+  __syncthreads();
+  const int incl = x + (w > 0 ? sh[w - 1] : 0);
+  int base = incl - s;
   for (int c = lo; c < hi; c++) {
     const int v = count[c];
     start[c] = base;
     base += v;
     count[c] = 0;
   }
-  if (t == T - 1) start[ncell] = sh[T - 1];
+  if (t == T - 1) start[ncell] = incl;
 }
 
 __global__ void k_scatter(int n, const int *__restrict__ cell_of, const int *__restrict__ slot,
