@@ -8,15 +8,18 @@ lattice, box 74.496 A, rc 10, C2 from 9).
 
 Default arm (libpmb200 on B200):
   value  -- device-resident steps (positions/velocities/forces in HBM, one
-            CUDA-graph replay per step), L2 flushed (256 MiB write) before
-            every timed step, each step timed with CUDA events on the stream
-            it runs on; sum over K steps, max over ranks.
+            CUDA-graph replay per step) that evaluate the LJ and Coulomb
+            energies every step, as the reference's leapfrog does; L2 flushed
+            (256 MiB write) before every timed step, each step timed with CUDA
+            events on the stream it runs on; sum over K steps, max over ranks.
+            The same steps without energies are reported as forces_only.
   e2e    -- the same steps through the reference-facing host-buffer C-ABI
             call (pmb200_eval: positions and forces copied host->device, forces
             and energies device->host, every step) with the kick/drift done
             on the host as ProtoMol's integrator does; wall clock per step.
   fp64   -- the same device-resident steps with the plain FP64 pair kernel.
-  roofline -- the pair kernel (dominant): 81 algorithmic flops per unique
+  roofline -- the pair kernel of those steps (dominant, energy launch): 81
+            algorithmic flops per unique
             in-cutoff pair over its CUDA-event duration, against the FP32 FMA
             peak measured in-run (the kernel runs on the FP32 pipe; tensor
             cores and HBM are not its bound); traffic from the committed ncu
@@ -61,8 +64,8 @@ sys.path.insert(0, ROOT)
 DT_FS = 1.0
 FLOPS_PER_PAIR = 81          # algorithmic flops per unique in-cutoff pair
 BYTES_PER_ATOM = 84          # algorithmic HBM bytes per atom per evaluation
-KERNELS_PER_STEP = 7         # kick_drift_settle, cell_index, scan, scatter, rank_gather,
-                             # pair, finalize
+KERNELS_PER_STEP = 9         # kick_drift_settle, cell_index, scan, scatter, rank_gather,
+                             # pair, finalize, reduce1, reduce2
 WORKLOAD = ("water box: 41,472 atoms (13,824 TIP3P-geometry waters, 24^3 lattice, "
             "box 74.496 A), LJ C2 switch 9-10 A + Coulomb C1 cutoff 10 A, leapfrog 1 fs")
 METRIC = "ns/day & Gpairs/s, 41k-atom water box: mixed vs FP64 on B200 @<=1e-5 force err"
@@ -142,18 +145,23 @@ def committed_traffic(name="pair_mixed_water41k.md"):
     return float(m.group(1)) if m else None
 
 
-def cpu_reference_time(sysd, steps):
+def cpu_reference_time(sysd, steps, warmup=0):
     """Seconds per leapfrog step of the reference CPU force on this host, one
-    core; (seconds, kind, detail)."""
+    core, after `warmup` untimed steps; (seconds, kind).  The reference's
+    force evaluates energies every step, as its integrator asks."""
     from oracle import oracle as O
     if O.ref_available():
         R = O.RefForce(sysd)
+        if warmup:
+            R.leapfrog(sysd["pos"], sysd["vel"], DT_FS, warmup)
         t0 = time.perf_counter()
         R.leapfrog(sysd["pos"], sysd["vel"], DT_FS, steps)
         dt = time.perf_counter() - t0
         R.close()
         kind = "reference"
     else:
+        if warmup:
+            O.restate_leapfrog(sysd, sysd["pos"], sysd["vel"], DT_FS, warmup)
         t0 = time.perf_counter()
         O.restate_leapfrog(sysd, sysd["pos"], sysd["vel"], DT_FS, steps)
         dt = time.perf_counter() - t0
@@ -162,12 +170,15 @@ def cpu_reference_time(sysd, steps):
 
 
 def _ref_replica(args):
-    steps, seed = args
+    steps, warmup, seed = args
     sys.path.insert(0, ROOT)
     from protomoladdon_b200 import water
     s = water.medium_41k(seed=seed)
-    t, kind = cpu_reference_time(s, steps)
+    t, kind = cpu_reference_time(s, steps, warmup)
     return t, kind
+
+
+REF_MAX_STEPS = 20   # bounded sample: about 9 s of CPU time per replica
 
 
 def run_reference(args):
@@ -176,25 +187,28 @@ def run_reference(args):
         return 0
     import multiprocessing as mp
     cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
-    steps = max(1, min(args.steps, 3))
+    steps = max(1, min(args.steps, REF_MAX_STEPS))
+    warmup = min(args.warmup, 3)
     ctx = mp.get_context("spawn")
     t0 = time.perf_counter()
     with ctx.Pool(cores) as pool:
-        res = pool.map(_ref_replica, [(steps, 1234 + r) for r in range(cores)])
+        res = pool.map(_ref_replica, [(steps, warmup, 1234 + r) for r in range(cores)])
     wall = time.perf_counter() - t0
     per_step = statistics.mean(t for t, _ in res)
     kind = res[0][1]
     value = cores * ns_per_day(per_step)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "ns/day",
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "n_gpus": args.gpus, "steps": steps, "warmup": warmup, "steps_requested": args.steps,
         "ms_per_step": per_step * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "atoms": 41472, "replicas": cores,
-                   "parallelism": f"{cores} independent single-core replicas"},
+                   "parallelism": f"{cores} independent single-core replicas",
+                   "step": "leapfrog step with the reference force (forces and energies)"},
         "cpu_baseline": {"value": value, "unit": "ns/day", "cores": cores, "kind": kind,
-                         "sample": f"{steps} leapfrog steps (+1 initial force) per replica, "
-                                   f"{cores} replicas in parallel, wall {wall:.1f} s"},
+                         "sample": f"{steps} timed leapfrog steps (+1 initial force) after "
+                                   f"{warmup} untimed ones per replica, {cores} replicas in "
+                                   f"parallel, wall {wall:.1f} s"},
         "e2e": {"value": value, "unit": "ns/day", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -232,9 +246,11 @@ def run_ours(args):
         f.set_rigid_waters(topo, widx, water.D_OH, water.D_HH)
         return f
 
-    def device_run(force):
-        """W warm-up + K timed device-resident steps; returns per-step ms list,
-        pair-kernel ms list, pair count."""
+    def device_run(force, flags):
+        """W warm-up + K timed device-resident steps, the force evaluated with
+        `flags` (PMB200_ENERGY: energies every step, as the reference's
+        integrator asks); returns per-step ms list, pair-kernel ms list (the
+        same flags), pair count."""
         pos = torch.tensor(s["pos"], dtype=torch.float64, device=dev)
         vel = torch.tensor(s["vel"], dtype=torch.float64, device=dev)
         frc = torch.zeros_like(pos)
@@ -246,8 +262,10 @@ def run_ours(args):
         force.sync()
         pairs = force.last_pair_count()
         sp = stream.cuda_stream
+        optr = out.data_ptr() if flags else None
         for _ in range(args.warmup):
-            force.step_device(topo, pos.data_ptr(), vel.data_ptr(), frc.data_ptr(), DT_FS, sp)
+            force.step_device(topo, pos.data_ptr(), vel.data_ptr(), frc.data_ptr(), DT_FS, sp,
+                              out_ptr=optr, flags=flags)
         stream.synchronize()
         e0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
         e1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
@@ -259,7 +277,8 @@ def run_ours(args):
             with torch.cuda.stream(stream):
                 flush.zero_()
                 e0[k].record(stream)
-            force.step_device(topo, pos.data_ptr(), vel.data_ptr(), frc.data_ptr(), DT_FS, sp)
+            force.step_device(topo, pos.data_ptr(), vel.data_ptr(), frc.data_ptr(), DT_FS, sp,
+                              out_ptr=optr, flags=flags)
             e1[k].record(stream)
         torch.cuda.synchronize(dev)
         if dist is not None:
@@ -272,7 +291,7 @@ def run_ours(args):
         for k in range(min(args.steps, 50)):
             with torch.cuda.stream(stream):
                 flush.zero_()
-            force.evaluate_device(topo, pos.data_ptr(), frc.data_ptr(), None, 0, sp)
+            force.evaluate_device(topo, pos.data_ptr(), frc.data_ptr(), optr, flags, sp)
             stream.synchronize()
             kms.append(force.last_kernel_ms())
         force.set_kernel_timing(False)
@@ -295,12 +314,15 @@ def run_ours(args):
 
     fmix = make(args.precision)
     with ClockSampler(local) as clk:
-        step_ms, kms, pairs = device_run(fmix)
+        step_ms, kms, pairs = device_run(fmix, _lib.PMB200_ENERGY)
     clocks = clk.summary()
+    # the same steps without energies (the forces an integrator needs when no
+    # energy is asked for), reported beside the headline
+    fo_ms, fo_kms, _ = device_run(fmix, 0)
     fp64 = None
     if args.precision == "mixed" and not args.skip_fp64:
         f64 = make("fp64")
-        s64, k64, _ = device_run(f64)
+        s64, k64, _ = device_run(f64, _lib.PMB200_ENERGY)
         f64.close()
         fp64 = (sum(s64), statistics.mean(k64))
 
@@ -321,13 +343,16 @@ def run_ours(args):
     E = ScalarStructure()
     fmix.evaluate(topo, xh, F, E)
     e2e_steps = min(args.steps, 100)
-    e2e_t = []
+    e2e_t, integ_t, call_t = [], [], []
 
     def host_step():
+        t0 = time.perf_counter()
         rigid.host_kick_drift(xh, vh, F, s["mass"], DT_FS, widx, water.D_OH, water.D_HH)
         _ft.zero_()  # the integrator zeroes its force array (F is a view of _ft)
         E.clear()
+        t1 = time.perf_counter()
         fmix.evaluate(topo, xh, F, E)
+        return t1 - t0, time.perf_counter() - t1
 
     for _ in range(min(args.warmup, 3)):
         host_step()
@@ -337,8 +362,40 @@ def run_ours(args):
         flush.zero_()
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
-        host_step()
+        ti, tc = host_step()
         e2e_t.append(time.perf_counter() - t0)
+        integ_t.append(ti)
+        call_t.append(tc)
+
+    # where an e2e step's force call goes, device-timed with CUDA events on
+    # the same buffers: the pinned host->device copy of the positions, the
+    # evaluation (cell build, pair kernel, finalize, energy reduction), the
+    # device->host copy of forces and energies; the rest of the call is host
+    # work (launch, synchronisation, adding the forces into the caller's array)
+    def ev_ms(fn, reps=20):
+        a = [torch.cuda.Event(enable_timing=True) for _ in range(reps)]
+        b = [torch.cuda.Event(enable_timing=True) for _ in range(reps)]
+        for k in range(reps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                a[k].record(stream)
+                fn()
+                b[k].record(stream)
+        torch.cuda.synchronize(dev)
+        return statistics.mean(x.elapsed_time(y) for x, y in zip(a, b))
+    dpos = torch.empty((n, 3), dtype=torch.float64, device=dev)
+    dfrc = torch.zeros_like(dpos)
+    dout = torch.zeros(20, dtype=torch.float64, device=dev)
+    hout = torch.empty(20, dtype=torch.float64, pin_memory=True)
+    h2d_ms = ev_ms(lambda: dpos.copy_(_xt, non_blocking=True))
+    eval_ms = ev_ms(lambda: fmix.evaluate_device(topo, dpos.data_ptr(), dfrc.data_ptr(),
+                                                 dout.data_ptr(), _lib.PMB200_ENERGY,
+                                                 stream.cuda_stream))
+
+    def d2h():
+        _ft.copy_(dfrc, non_blocking=True)
+        hout.copy_(dout, non_blocking=True)
+    d2h_ms = ev_ms(d2h)
     fmix.close()
 
     tot_ms = sum(step_ms)
@@ -359,6 +416,8 @@ def run_ours(args):
             "dtype": "f32" if args.precision == "mixed" else "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "atoms": n, "pairs_per_eval": pairs,
                        "precision": args.precision,
+                       "step": "kick + drift + SETTLE + cell rebuild + force with LJ and "
+                               "Coulomb energies (every step, as the reference's leapfrog)",
                        "l2": "flushed before every timed step (256 MiB write)",
                        "parallelism": f"{world} independent replica(s), one per GPU"},
             "gpairs_per_s": world * pairs / (ms_step * 1e-3) / 1e9,
@@ -374,6 +433,20 @@ def run_ours(args):
             "e2e": {"value": world * ns_per_day(e2e_s), "unit": "ns/day",
                     "ms_per_step": e2e_s * 1e3,
                     "h2d_bytes_per_step": 24 * n, "d2h_bytes_per_step": 24 * n + 160},
+            "e2e_breakdown": {
+                "host_integrator_ms": statistics.mean(integ_t) * 1e3,
+                "force_call_ms": statistics.mean(call_t) * 1e3,
+                "of_which_device": {"h2d_ms": h2d_ms, "evaluation_ms": eval_ms,
+                                    "d2h_ms": d2h_ms},
+                "host_side_of_call_ms": statistics.mean(call_t) * 1e3 - (h2d_ms + eval_ms
+                                                                         + d2h_ms),
+                "note": "host kick/drift/SETTLE on the host's cores; the force call is one "
+                        "CUDA-graph replay (copy in, evaluate with energies, copy out) and "
+                        "a synchronisation"},
+            "forces_only": {"ns_per_day": world * ns_per_day(statistics.mean(fo_ms) * 1e-3),
+                            "ms_per_step": statistics.mean(fo_ms),
+                            "pair_kernel_ms": statistics.mean(fo_kms),
+                            "note": "the same device steps without energies"},
             "gpu_launches": KERNELS_PER_STEP * args.steps,
             "clocks": clocks,
         }
@@ -389,7 +462,8 @@ def run_ours(args):
             line["cpu_baseline"] = {
                 "value": ns_per_day(t_cpu), "unit": "ns/day", "cores": 1, "kind": kind,
                 "sample": f"{cpu_steps} leapfrog steps (+1 initial force) of the same box, "
-                          f"{t_cpu * 1e3:.0f} ms per step, serial reference force"}
+                          f"{t_cpu * 1e3:.0f} ms per step, serial reference force with "
+                          f"energies"}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()

@@ -235,19 +235,28 @@ int pmb200_measure_fp32_peak(int device, double *tflops);
  * d_ex_start[n+1] offsets into d_ex, which holds int pairs {partner atom,
  * kind} (kind 1 = modified, 2 = full; each pair listed under both of its
  * atoms; 8-byte aligned); host arrays lj[ntypes^2*4]
- * {A, B, A14, B14}, box[3] (orthogonal edges), origin[3].  Outputs:
- * d_forces[3n] is OVERWRITTEN with this evaluation's forces; d_energy[2]
- * (may be NULL) receives {COULOMB, LENNARDJONES}.  Work is queued on
- * `stream`; the first call on a device looks up the array's device address
- * (cudaGetSymbolAddress) and should come before any stream capture.  Every
- * call shares the one array, so calls whose GPU work overlaps (different
- * streams, threads or processes sharing a context) race; serialise them. */
+ * {A, B, A14, B14} (finite), box[3] (orthogonal edges), origin[3].
+ * Outputs: d_forces[3n] is OVERWRITTEN with this evaluation's forces;
+ * d_energy (may be NULL: a forces-only evaluation) receives exactly two
+ * doubles {COULOMB, LENNARDJONES} and nothing beyond them; d_status (may be
+ * NULL) receives one int when the work completes: PMB200_OK, or
+ * PMB200_EDEVICE when a device-side check failed (a non-finite coordinate,
+ * or a pair force beyond the fixed-point range, as for coincident atoms) --
+ * the forces and energies of such a call are not meaningful.  With
+ * d_status NULL those failures go unreported.  The return value covers the
+ * host-side checks and the launches only (the work is asynchronous).  Work
+ * is queued on `stream`; the first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress) and should come before any stream
+ * capture.  Every call shares the one array and it keeps the previous
+ * call's contents, so calls whose GPU work overlaps (different streams,
+ * threads or processes sharing a context) race; serialise them. */
 int pmb200_eval_noalloc(const pmb200_params *params, int n, const double *d_pos,
                         const int *d_type, const double *d_q, const int *d_mol,
                         const int *d_ex_start, const int *d_ex, int ntypes,
                         const double *lj, double coulomb_scaling,
                         const double box[3], const double origin[3],
-                        double *d_forces, double *d_energy, void *stream);
+                        double *d_forces, double *d_energy, int *d_status,
+                        void *stream);
 
 /* Geometry of the device cell grid chosen for the current box. */
 int pmb200_grid(const pmb200_ctx *ctx, int dims[3], double edge[3]);

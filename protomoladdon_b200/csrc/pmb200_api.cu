@@ -1767,8 +1767,32 @@ struct NoAllocLayout {  // byte offsets inside the scratch array
   static constexpr size_t lj32 = align256(spos_lo + sizeof(float4) * kNoAllocAtoms);
   static constexpr size_t pairs = align256(lj32 + sizeof(float4) * kMaxTypes * kMaxTypes);
   static constexpr size_t err = align256(pairs + sizeof(double));
-  static constexpr size_t total = align256(err + sizeof(int));
+  // the final reduction's 20 doubles (energies, virial, molecular virial);
+  // only the two energies are copied to the caller
+  static constexpr size_t out = align256(err + sizeof(int));
+  static constexpr size_t total = align256(out + sizeof(double) * 20);
 };
+
+// The LJ table travels as a kernel parameter (4 KB), so no host buffer is
+// copied and nothing waits for the stream.
+struct NoAllocLj {
+  float4 v[kMaxTypes * kMaxTypes];
+};
+
+// Writes the call's LJ table into the scratch array and clears the device
+// error word (one block).
+__global__ void k_noalloc_setup(const NoAllocLj tbl, int nlj, float4 *__restrict__ dlj,
+                                int *__restrict__ err) {
+  for (int k = threadIdx.x; k < nlj; k += blockDim.x) dlj[k] = tbl.v[k];
+  if (threadIdx.x == 0) *err = 0;
+}
+
+// The caller's status word: PMB200_OK, or PMB200_EDEVICE when a device-side
+// check failed (non-finite coordinate, or a pair force beyond the
+// fixed-point range).
+__global__ void k_noalloc_status(const int *__restrict__ err, int *__restrict__ status) {
+  *status = *err ? PMB200_EDEVICE : PMB200_OK;
+}
 
 // The scratch array itself.  Host code must not pass its name to a kernel
 // (on the host it names a stand-in, not device memory); the device address
@@ -1804,9 +1828,10 @@ extern "C" int pmb200_eval_noalloc(const pmb200_params *p, int n, const double *
                                    const int *d_ex_start, const int *d_ex_pairs, int ntypes,
                                    const double *lj, double coulomb_scaling, const double box[3],
                                    const double origin[3], double *d_forces, double *d_energy,
-                                   void *stream) {
+                                   int *d_status, void *stream) {
   // argument checks first: nothing reaches the device for a rejected call
   if (!p || !box || !origin || !lj) return PMB200_EINVAL;
+  if (!std::isfinite(coulomb_scaling)) return PMB200_EINVAL;
   if (p->precision != PMB200_MIXED) return PMB200_EUNSUPPORTED;
   if (!(p->switchon >= 0.0) || !(p->cutoff_lj > 0.0) || !(p->switchon < p->cutoff_lj) ||
       !(p->cutoff_coul > 0.0) || !(p->cutoff_alg > 0.0))
@@ -1814,6 +1839,8 @@ extern "C" int pmb200_eval_noalloc(const pmb200_params *p, int n, const double *
   if (p->cutoff_alg < rc_max(*p)) return PMB200_EUNSUPPORTED;
   if (n < 0 || n > kNoAllocAtoms) return PMB200_ENOMEM;  // beyond the fixed scratch
   if (ntypes <= 0 || ntypes > kMaxTypes) return PMB200_EUNSUPPORTED;
+  for (int k = 0; k < 4 * ntypes * ntypes; k++)
+    if (!std::isfinite(lj[k])) return PMB200_EINVAL;
   if (n > 0 && (!d_pos || !d_type || !d_q || !d_mol || !d_ex_start || !d_ex_pairs || !d_forces))
     return PMB200_EINVAL;
   if (((uintptr_t)d_ex_pairs & 7u) != 0) return PMB200_EINVAL;  // read as int2
@@ -1879,10 +1906,10 @@ extern "C" int pmb200_eval_noalloc(const pmb200_params *p, int n, const double *
   mc.csf = (float)coulomb_scaling;
   mc.ey = (float)(edge[1] / u);
   mc.ez = (float)(edge[2] / u);
-  float4 lj32[kMaxTypes * kMaxTypes];
+  NoAllocLj lj32{};
   const double u6 = std::pow(u, 6.0), u12 = u6 * u6;
   for (int k = 0; k < ntypes * ntypes; k++)
-    lj32[k] = make_float4((float)(lj[4 * k] / u12), (float)(lj[4 * k + 1] / u6),
+    lj32.v[k] = make_float4((float)(lj[4 * k] / u12), (float)(lj[4 * k + 1] / u6),
                           (float)(lj[4 * k + 2] / u12), (float)(lj[4 * k + 3] / u6));
 
   cudaError_t e = cudaSuccess;
@@ -1906,13 +1933,13 @@ extern "C" int pmb200_eval_noalloc(const pmb200_params *p, int n, const double *
   float4 *dlj = (float4 *)(base + Lo::lj32);
   double *pairs = (double *)(base + Lo::pairs);
   int *err = (int *)(base + Lo::err);
+  double *out = (double *)(base + Lo::out);
   cudaStream_t st = (cudaStream_t)stream;
   // the array keeps the previous call's contents: zero what accumulates
-  e = cudaMemcpyAsync(dlj, lj32, sizeof(float4) * ntypes * ntypes, cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess) e = cudaMemsetAsync(count, 0, sizeof(int) * g.ncell, st);
+  k_noalloc_setup<<<1, 256, 0, st>>>(lj32, ntypes * ntypes, dlj, err);
+  e = cudaMemsetAsync(count, 0, sizeof(int) * g.ncell, st);
   if (e == cudaSuccess && n > 0)
     e = cudaMemsetAsync(facc, 0, sizeof(unsigned long long) * 3 * (size_t)n, st);
-  if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, sizeof(int), st);
   if (e != cudaSuccess) return PMB200_ECUDA;
   const PbcRef pb{};
   if (n > 0)
@@ -1939,9 +1966,14 @@ extern "C" int pmb200_eval_noalloc(const pmb200_params *p, int n, const double *
     k_finalize<<<(n + 255) / 256, 256, 0, st>>>(n, facc, sidx, kFixInv / u, 0, d_forces);
   if (d_energy) {
     k_reduce1<<<kRedBlocks, 256, 0, st>>>(g.ncell * slots, partial, red);
+    // the reduction writes 20 doubles (energies, virial, molecular
+    // virial) into the scratch; the caller's buffer receives the two energies
     k_reduce2<<<1, 256, 0, st>>>(kRedBlocks, red, 1, 1.0, 1.5 / rq, 0.5 / (rq * rq * rq),
-                                d_energy, pairs);
+                                out, pairs);
+    e = cudaMemcpyAsync(d_energy, out, 2 * sizeof(double), cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return PMB200_ECUDA;
   }
+  if (d_status) k_noalloc_status<<<1, 1, 0, st>>>(err, d_status);
   if (cudaGetLastError() != cudaSuccess) return PMB200_ECUDA;
   return PMB200_OK;
 }

@@ -3,7 +3,9 @@
 Run in a tree where the reference sources are available and
 ``make -C oracle ref`` has built oracle/_ref/libpmref.so:
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <reference tree>
+
+(or with the tree in the PROTOMOL_REFERENCE environment variable).
 
 Fixtures (all inputs and outputs FP64):
 
@@ -215,7 +217,10 @@ if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
     only = [a for a in sys.argv[1:] if a.endswith("-only")]
     if not only:
-        main(args[0] if args else "/root/reference")
+        ref = args[0] if args else os.environ.get("PROTOMOL_REFERENCE")
+        if not ref:
+            sys.exit("usage: make_golden.py <reference tree> (or set PROTOMOL_REFERENCE)")
+        main(ref)
     if not only or "--ewald-only" in only:
         ewald_fixtures()
     if not only or "--pairs-only" in only:
