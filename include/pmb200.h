@@ -114,6 +114,21 @@ int pmb200_eval(pmb200_ctx *ctx, const double *pos, double *forces,
                 double *energies, double *virial, double *molvirial,
                 unsigned flags);
 
+/* The share of one rank in the reference's parallel evaluation
+ * (NonbondedCutoffSystemForce::parallelEvaluate,
+ * protomol/src/protomol/force/nonbonded/NonbondedCutoffSystemForce.h:57-77,
+ * which splits its cells into numberOfBlocks() ranges and evaluates the
+ * ranges Parallel::next() grants; Parallel::reduce then sums forces and
+ * energies over the ranks, force/ForceGroup.cpp:79-116).  Evaluates on host
+ * buffers only the pairs whose i-cell (this library's grid, pmb200_grid) lies
+ * in [cell_lo, cell_hi): with the mixed kernel the half-shell pairs of those
+ * cells, with the FP64 kernel the forces on their atoms and half their pair
+ * energies.  Arguments and accumulation as pmb200_eval; over a partition of
+ * [0, number of cells) the shares sum to pmb200_eval's result. */
+int pmb200_eval_cells(pmb200_ctx *ctx, const double *pos, double *forces,
+                      double *energies, double *virial, double *molvirial,
+                      unsigned flags, int cell_lo, int cell_hi);
+
 /* Same evaluation on device buffers, asynchronous on `stream` (a
  * cudaStream_t, NULL = the context's stream).  d_pos[3n], d_forces[3n]
  * (accumulated into), d_out[20] receives {COULOMB, LENNARDJONES, virial[9],

@@ -50,6 +50,7 @@ EXPORTED = (
     "pmb200_batch_autotune", "pmb200_batch_set_kernel_timing", "pmb200_batch_last_kernel_ms",
     "pmb200_batch_pair_counts", "pmb200_create_pair", "pmb200_set_vacuum_domain",
     "pmb200_batch_sync", "pmb200_shard_eval_device", "pmb200_shard_finalize",
+    "pmb200_eval_cells",
 )
 
 _P = ctypes.c_void_p
@@ -120,6 +121,7 @@ def lib():
     L.pmb200_hvp_device.argtypes = [_P, _P, _P, _P, _P, _P, _P]
     L.pmb200_update_params.argtypes = [_P, _P, _P]
     L.pmb200_set_vacuum_domain.argtypes = [_P, _P, _P]
+    L.pmb200_eval_cells.argtypes = [_P, _P, _P, _P, _P, _P, ctypes.c_uint, _I, _I]
     L.pmb200_create_pair.argtypes = [ctypes.POINTER(PairParams), ctypes.POINTER(_P)]
     L.pmb200_batch_create.argtypes = [ctypes.POINTER(_P), _I, ctypes.POINTER(_P)]
     L.pmb200_batch_destroy.argtypes = [_P]

@@ -375,9 +375,10 @@ void launch_pair_mixed(pmb200_ctx *c, unsigned flags, cudaStream_t st, int cell0
 #undef PMB_MIXED_LAUNCH
 }
 
+// (over the i-cells [cell0, cell0 + ncells), all by default)
 template <int F>
 void launch_pair_fp64(pmb200_ctx *c, unsigned flags, double *d_forces, int accumulate,
-                      int blocks, cudaStream_t st) {
+                      int blocks, cudaStream_t st, int cell0 = 0, int ncells = 1 << 30) {
   const GridParams &g = c->g;
   const bool energy = (flags & PMB200_ENERGY) != 0;
   const bool virial = (flags & (PMB200_VIRIAL | PMB200_MOLVIRIAL)) != 0;
@@ -387,7 +388,8 @@ void launch_pair_fp64(pmb200_ctx *c, unsigned flags, double *d_forces, int accum
                                                   c->d_lj64, c->d_start, c->d_spos64,       \
                                                   c->d_smeta, c->d_sidx, c->d_ex_start,     \
                                                   c->d_ex, d_forces, accumulate,            \
-                                                  c->d_partial, c->pb, c->d_com)
+                                                  c->d_partial, c->pb, c->d_com, cell0,     \
+                                                  ncells)
   if (molvir) PMB_FP64_LAUNCH(true, true, true);
   else if (energy && virial) PMB_FP64_LAUNCH(true, true, false);
   else if (energy) PMB_FP64_LAUNCH(true, false, false);
@@ -1299,6 +1301,106 @@ int pmb200_eval(pmb200_ctx *c, const double *pos, double *forces, double *energi
 #pragma omp parallel for schedule(static) if (m > 65536)
     for (long long k = 0; k < m; k++) forces[k] += src[k];
   }
+  const double *out = c->h_pin_out;
+  if (flags & PMB200_ENERGY) {
+    energies[0] += out[0];
+    energies[1] += out[1];
+  }
+  if (flags & PMB200_VIRIAL)
+    for (int k = 0; k < 9; k++) virial[k] += out[2 + k];
+  if (flags & PMB200_MOLVIRIAL)
+    for (int k = 0; k < 9; k++) molvirial[k] += out[11 + k];
+  return PMB200_OK;
+}
+
+// Host-buffer evaluation of the pairs whose i-cell lies in [cell_lo,
+// cell_hi): the share of one block range of the reference's
+// parallelEvaluate.  Direct launches (no graph); forces, energies and
+// virials are accumulated into the caller's arrays.
+int pmb200_eval_cells(pmb200_ctx *c, const double *pos, double *forces, double *energies,
+                      double *virial, double *molvirial, unsigned flags, int cell_lo,
+                      int cell_hi) {
+  int rc = check_ready(c);
+  if (rc) return rc;
+  if (cell_lo < 0 || cell_hi < cell_lo || cell_hi > c->g.ncell)
+    return fail(c, PMB200_EINVAL, "cell range [%d, %d) of %d cells", cell_lo, cell_hi,
+                c->g.ncell);
+  if (c->n > 0 && (!pos || !forces)) return fail(c, PMB200_EINVAL, "null host buffer");
+  if ((flags & PMB200_ENERGY) && !energies) return fail(c, PMB200_EINVAL, "null energies");
+  if ((flags & PMB200_VIRIAL) && !virial) return fail(c, PMB200_EINVAL, "null virial");
+  if ((flags & PMB200_MOLVIRIAL) && !molvirial) return fail(c, PMB200_EINVAL, "null molvirial");
+  if ((flags & PMB200_MOLVIRIAL) && !c->have_mass)
+    return fail(c, PMB200_EINVAL, "molecular virial needs masses");
+  if (cell_hi == cell_lo || c->n == 0) return PMB200_OK;  // nothing in this share
+  CK(cudaSetDevice(c->p.device));
+  const size_t cnt = 3 * (size_t)c->n;
+  const size_t bytes = sizeof(double) * cnt;
+  cudaStream_t st = c->stream;
+  if (c->n_pin < c->n || !c->h_pin_out) {
+    release_graph(c);  // the host-buffer graph copies through these buffers
+    if (c->h_pin_pos) cudaFreeHost(c->h_pin_pos);
+    if (c->h_pin_frc) cudaFreeHost(c->h_pin_frc);
+    if (c->h_pin_out) cudaFreeHost(c->h_pin_out);
+    c->h_pin_pos = c->h_pin_frc = c->h_pin_out = nullptr;
+    CK(cudaMallocHost((void **)&c->h_pin_pos, std::max<size_t>(bytes, 8)));
+    CK(cudaMallocHost((void **)&c->h_pin_frc, std::max<size_t>(bytes, 8)));
+    CK(cudaMallocHost((void **)&c->h_pin_out, sizeof(double) * kPinOut));
+    c->n_pin = c->n;
+  }
+  int *h_err = reinterpret_cast<int *>(c->h_pin_out + 20);
+  std::memcpy(c->h_pin_pos, pos, bytes);
+  CK(cudaMemcpyAsync(c->d_hpos, c->h_pin_pos, bytes, cudaMemcpyHostToDevice, st));
+  const bool mixed = c->p.precision == PMB200_MIXED;
+  const bool energy = (flags & PMB200_ENERGY) != 0;
+  const bool anyvir = (flags & (PMB200_VIRIAL | PMB200_MOLVIRIAL)) != 0;
+  const GridParams &g = c->g;
+  const int nc = cell_hi - cell_lo;
+  launch_cell_build(c, c->d_hpos, mixed, mixed && energy && c->form == FORM_CUTOFF, st,
+                    mixed ? c->d_facc : nullptr);
+  if ((flags & PMB200_MOLVIRIAL) && c->nmol > 0)
+    k_com<<<(c->nmol + 127) / 128, 128, 0, st>>>(c->nmol, c->d_mstart, c->d_matoms, c->d_mass,
+                                                  c->d_hpos, c->d_com);
+  int rows = nc;
+  double *prow = c->d_partial;
+  if (mixed) {
+    if (c->form == FORM_GENERIC) launch_pair_mixed<FORM_GENERIC>(c, flags, st, cell_lo, nc);
+    else if (c->form == FORM_EWALD_POLY5)
+      launch_pair_mixed<FORM_EWALD_POLY5>(c, flags, st, cell_lo, nc);
+    else if (c->form == FORM_EWALD_EXACT)
+      launch_pair_mixed<FORM_EWALD_EXACT>(c, flags, st, cell_lo, nc);
+    else launch_pair_mixed<FORM_CUTOFF>(c, flags, st, cell_lo, nc);
+    k_finalize<<<(c->n + 255) / 256, 256, 0, st>>>(c->n, c->d_facc, c->d_sidx,
+                                                  kFixInv / g.unit, 0, c->d_hfrc);
+    rows = nc * mixed_cell_slots(true, c->n, g.ncell);
+  } else {
+    CK(cudaMemsetAsync(c->d_hfrc, 0, bytes, st));
+    const int blocks = (nc + 3) / 4;
+    if (c->form == FORM_GENERIC)
+      launch_pair_fp64<FORM_GENERIC>(c, flags, c->d_hfrc, 1, blocks, st, cell_lo, nc);
+    else if (c->form == FORM_EWALD_POLY5)
+      launch_pair_fp64<FORM_EWALD_POLY5>(c, flags, c->d_hfrc, 1, blocks, st, cell_lo, nc);
+    else if (c->form == FORM_EWALD_EXACT)
+      launch_pair_fp64<FORM_EWALD_EXACT>(c, flags, c->d_hfrc, 1, blocks, st, cell_lo, nc);
+    else launch_pair_fp64<FORM_CUTOFF>(c, flags, c->d_hfrc, 1, blocks, st, cell_lo, nc);
+    prow = c->d_partial + (size_t)cell_lo * kNacc;  // the FP64 kernel's rows are by cell
+  }
+  CK(cudaGetLastError());
+  if (energy || anyvir) {
+    const double rcc = c->p.cutoff_coul / g.unit;
+    const bool c1 = c->form == FORM_CUTOFF;
+    k_reduce1<<<kRedBlocks, 256, 0, st>>>(rows, prow, c->d_red);
+    k_reduce2<<<1, 256, 0, st>>>(kRedBlocks, c->d_red, mixed ? 1 : 0, mixed ? 1.0 : 0.5,
+                                c1 ? 1.5 / rcc : 0.0, c1 ? 0.5 / (rcc * rcc * rcc) : 0.0,
+                                c->d_out, c->d_pairs);
+    CK(cudaMemcpyAsync(c->h_pin_out, c->d_out, sizeof(double) * 20, cudaMemcpyDeviceToHost,
+                       st));
+  }
+  CK(cudaMemcpyAsync(c->h_pin_frc, c->d_hfrc, bytes, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(h_err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  rc = device_error(c, *h_err);
+  if (rc) return rc;
+  for (size_t k = 0; k < cnt; k++) forces[k] += c->h_pin_frc[k];
   const double *out = c->h_pin_out;
   if (flags & PMB200_ENERGY) {
     energies[0] += out[0];

@@ -1165,10 +1165,13 @@ k_pair_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes, const dou
             const int2 *__restrict__ smeta, const int *__restrict__ sidx,
             const int *__restrict__ ex_start, const int2 *__restrict__ ex,
             double *__restrict__ forces, int accumulate, double *__restrict__ partial,
-            const PbcRef pb, const double *__restrict__ com) {
+            const PbcRef pb, const double *__restrict__ com, int cell0 = 0,
+            int ncells = 1 << 30) {
   const int lane = threadIdx.x & 31;
-  const int cell = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (cell >= g.ncell) return;
+  // one warp per i-cell of [cell0, cell0 + ncells)
+  const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int cell = cell0 + wid;
+  if (wid >= ncells || cell >= g.ncell) return;
   const int cx = cell % g.nx;
   const int cy = (cell / g.nx) % g.ny;
   const int cz = cell / (g.nx * g.ny);

@@ -214,6 +214,32 @@ class NonbondedCutoffB200SystemForce:
     def evaluate(self, topo: PeriodicTopology, positions, forces, energies: ScalarStructure):
         """Accumulates forces (n,3 float64, C-contiguous, modified in place)
         and energies like SystemForce::evaluate."""
+        self._host_eval(topo, positions, forces, energies, None)
+
+    def number_of_blocks(self, topo):
+        """Force::numberOfBlocks: the cells of the device grid (one process,
+        Parallel::getNumberOfPackages(n) == n)."""
+        self._ensure(topo)
+        d, _ = self.grid()
+        return int(d[0] * d[1] * d[2])
+
+    def parallel_evaluate(self, topo, positions, forces, energies, rank, nranks):
+        """SystemForce::parallelEvaluate of one rank in the reference's static
+        mode (Parallel::next() grants block i to rank i mod nranks): block i
+        of numberOfBlocks covers the cells [n i / count, n (i + 1) / count).
+        Summed over the ranks (Parallel::reduce) it is evaluate()."""
+        count = self.number_of_blocks(topo)
+        n = count
+        for i in range(rank, count, nranks):
+            lo, hi = n * i // count, n * (i + 1) // count
+            self.evaluate_cells(topo, positions, forces, energies, lo, hi)
+
+    def evaluate_cells(self, topo, positions, forces, energies, cell_lo, cell_hi):
+        """The pairs whose i-cell lies in [cell_lo, cell_hi) (see
+        pmb200_eval_cells), accumulated like evaluate()."""
+        self._host_eval(topo, positions, forces, energies, (int(cell_lo), int(cell_hi)))
+
+    def _host_eval(self, topo, positions, forces, energies, cells):
         self._ensure(topo)
         pos = np.ascontiguousarray(positions, dtype=np.float64)
         if not (isinstance(forces, np.ndarray) and forces.dtype == np.float64
@@ -227,8 +253,13 @@ class NonbondedCutoffB200SystemForce:
         if energies.molecular_virial:
             flags |= _lib.PMB200_MOLVIRIAL
         e = np.zeros(2)
-        self._check(_lib.lib().pmb200_eval(self._ctx, _ptr(pos), _ptr(forces), _ptr(e), _ptr(vir),
-                                           _ptr(mvir), flags))
+        if cells is None:
+            self._check(_lib.lib().pmb200_eval(self._ctx, _ptr(pos), _ptr(forces), _ptr(e),
+                                               _ptr(vir), _ptr(mvir), flags))
+        else:
+            self._check(_lib.lib().pmb200_eval_cells(self._ctx, _ptr(pos), _ptr(forces), _ptr(e),
+                                                     _ptr(vir), _ptr(mvir), flags, cells[0],
+                                                     cells[1]))
         energies[ScalarStructure.COULOMB] += e[0]
         energies[ScalarStructure.LENNARDJONES] += e[1]
         if energies.virial:

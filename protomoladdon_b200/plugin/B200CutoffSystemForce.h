@@ -62,17 +62,45 @@ public:
   // molecular virial are added when the ScalarStructure asks for them.
   virtual void evaluate(const GenericTopology *topo, const Vector3DBlock *positions,
                         Vector3DBlock *forces, ScalarStructure *energies) {
+    run(topo, positions, forces, energies, false);
+  }
+
+  // SystemForce::parallelEvaluate (the default evaluates everything on every
+  // rank, force/system/SystemForce.h:91-96, which Parallel::reduce would then
+  // count once per rank): this rank's blocks of cells only, as
+  // NonbondedCutoffSystemForce::parallelEvaluate does.
+  virtual void parallelEvaluate(const GenericTopology *topo, const Vector3DBlock *positions,
+                                Vector3DBlock *forces, ScalarStructure *energies) {
+    run(topo, positions, forces, energies, true);
+  }
+
+  // Force::numberOfBlocks: the Parallel::next() calls parallelEvaluate makes.
+  virtual unsigned int numberOfBlocks(const GenericTopology *topo, const Vector3DBlock *) {
+    prepare(topo);
+    return b200NumberOfBlocks(myCtx);
+  }
+
+private:
+  void prepare(const GenericTopology *topo) {
     if (!myCtx) THROW("B200 cutoff force: evaluate called on the factory prototype.");
     const RealTopologyType *t = dynamic_cast<const RealTopologyType *>(topo);
     if (!t) THROW("B200 cutoff force: needs periodic boundaries and the cubic cell manager.");
     if (myCached != topo) upload(*t);
+  }
+
+  void run(const GenericTopology *topo, const Vector3DBlock *positions, Vector3DBlock *forces,
+           ScalarStructure *energies, bool parallel) {
+    prepare(topo);
     unsigned flags = PMB200_ENERGY;
     if (energies->virial()) flags |= PMB200_VIRIAL;
     if (energies->molecularVirial()) flags |= PMB200_MOLVIRIAL;
     double e[2] = {0.0, 0.0};
     double vir[9], mvir[9];
     for (int k = 0; k < 9; k++) vir[k] = mvir[k] = 0.0;
-    check(pmb200_eval(myCtx, positions->c, forces->c, e, vir, mvir, flags));
+    if (parallel)
+      check(b200ParallelEval(myCtx, positions->c, forces->c, e, vir, mvir, flags));
+    else
+      check(pmb200_eval(myCtx, positions->c, forces->c, e, vir, mvir, flags));
     (*energies)[ScalarStructure::COULOMB] += e[0];
     (*energies)[ScalarStructure::LENNARDJONES] += e[1];
     for (int k = 0; k < 9; k++) {
@@ -83,6 +111,7 @@ public:
     }
   }
 
+public:
   // The topology (types, charges, exclusions, box) is re-read after this.
   virtual void uncache() { myCached = 0; }
 

@@ -67,6 +67,26 @@ public:
   // the virial and molecular virial when the ScalarStructure asks for them.
   virtual void evaluate(const GenericTopology *topo, const Vector3DBlock *positions,
                         Vector3DBlock *forces, ScalarStructure *energies) {
+    run(topo, positions, forces, energies, false);
+  }
+
+  // SystemForce::parallelEvaluate: this rank's blocks of cells only (the
+  // reference's Ewald force deals its work through Parallel::next() too,
+  // NonbondedFullEwaldSystemForce.h:115, 518-540); Parallel::reduce sums
+  // the ranks' shares.
+  virtual void parallelEvaluate(const GenericTopology *topo, const Vector3DBlock *positions,
+                                Vector3DBlock *forces, ScalarStructure *energies) {
+    run(topo, positions, forces, energies, true);
+  }
+
+  // Force::numberOfBlocks: the Parallel::next() calls parallelEvaluate makes.
+  virtual unsigned int numberOfBlocks(const GenericTopology *topo, const Vector3DBlock *) {
+    prepare(topo);
+    return b200NumberOfBlocks(myCtx);
+  }
+
+private:
+  void prepare(const GenericTopology *topo) {
     if (!myCtx) THROW("B200 Ewald real-space force: evaluate called on the factory prototype.");
     const RealTopologyType *t = dynamic_cast<const RealTopologyType *>(topo);
     if (!t) THROW("B200 Ewald real-space force: needs periodic boundaries and the cubic cell manager.");
@@ -74,13 +94,21 @@ public:
       check(b200UploadTopology(myCtx, *t));
       myCached = topo;
     }
+  }
+
+  void run(const GenericTopology *topo, const Vector3DBlock *positions, Vector3DBlock *forces,
+           ScalarStructure *energies, bool parallel) {
+    prepare(topo);
     unsigned flags = PMB200_ENERGY;
     if (energies->virial()) flags |= PMB200_VIRIAL;
     if (energies->molecularVirial()) flags |= PMB200_MOLVIRIAL;
     double e[2] = {0.0, 0.0};
     double vir[9], mvir[9];
     for (int k = 0; k < 9; k++) vir[k] = mvir[k] = 0.0;
-    check(pmb200_eval(myCtx, positions->c, forces->c, e, vir, mvir, flags));
+    if (parallel)
+      check(b200ParallelEval(myCtx, positions->c, forces->c, e, vir, mvir, flags));
+    else
+      check(pmb200_eval(myCtx, positions->c, forces->c, e, vir, mvir, flags));
     (*energies)[ScalarStructure::COULOMB] += e[0];
     for (int k = 0; k < 9; k++) {
       if (flags & PMB200_VIRIAL)
@@ -90,6 +118,7 @@ public:
     }
   }
 
+public:
   virtual void uncache() { myCached = 0; }
 
   virtual std::string getKeyword() const { return "FullEwaldB200"; }

@@ -72,6 +72,27 @@ public:
 
   virtual void evaluate(const GenericTopology *topo, const Vector3DBlock *positions,
                         Vector3DBlock *forces, ScalarStructure *energies) {
+    run(topo, positions, forces, energies, false);
+  }
+
+  // SystemForce::parallelEvaluate: this rank's blocks of cells only, as
+  // NonbondedCutoffSystemForce::parallelEvaluate does; Parallel::reduce sums
+  // the ranks' shares.
+  virtual void parallelEvaluate(const GenericTopology *topo, const Vector3DBlock *positions,
+                                Vector3DBlock *forces, ScalarStructure *energies) {
+    run(topo, positions, forces, energies, true);
+  }
+
+  // Force::numberOfBlocks: the Parallel::next() calls parallelEvaluate makes.
+  // (For vacuum boundaries the grid follows the atoms' bounding box, which
+  // ForceGroup fixes before it asks; every rank holds the same positions.)
+  virtual unsigned int numberOfBlocks(const GenericTopology *topo, const Vector3DBlock *pos) {
+    prepare(topo, pos);
+    return b200NumberOfBlocks(myCtx);
+  }
+
+private:
+  void prepare(const GenericTopology *topo, const Vector3DBlock *positions) {
     if (!myCtx) THROW("B200 cutoff force: evaluate called on the factory prototype.");
     const RealTopologyType *t = dynamic_cast<const RealTopologyType *>(topo);
     if (!t) THROW("B200 cutoff force: topology type does not match the force's boundaries.");
@@ -80,13 +101,21 @@ public:
       myCached = topo;
     }
     if (TBC::VACUUM) updateDomain(positions);
+  }
+
+  void run(const GenericTopology *topo, const Vector3DBlock *positions, Vector3DBlock *forces,
+           ScalarStructure *energies, bool parallel) {
+    prepare(topo, positions);
     unsigned flags = PMB200_ENERGY;
     if (energies->virial()) flags |= PMB200_VIRIAL;
     if (energies->molecularVirial()) flags |= PMB200_MOLVIRIAL;
     double e[2] = {0.0, 0.0};
     double vir[9], mvir[9];
     for (int k = 0; k < 9; k++) vir[k] = mvir[k] = 0.0;
-    check(pmb200_eval(myCtx, positions->c, forces->c, e, vir, mvir, flags));
+    if (parallel)
+      check(b200ParallelEval(myCtx, positions->c, forces->c, e, vir, mvir, flags));
+    else
+      check(pmb200_eval(myCtx, positions->c, forces->c, e, vir, mvir, flags));
     (*energies)[ScalarStructure::COULOMB] += e[0];
     (*energies)[ScalarStructure::LENNARDJONES] += e[1];
     for (int k = 0; k < 9; k++) {
@@ -97,6 +126,7 @@ public:
     }
   }
 
+public:
   virtual void uncache() { myCached = 0; }
   virtual std::string getKeyword() const { return "NonbondedCutoffB200"; }
 

@@ -12,6 +12,7 @@
 #include <protomol/topology/Topology.h>
 #include <protomol/topology/PeriodicBoundaryConditions.h>
 #include <protomol/topology/CubicCellManager.h>
+#include <protomol/parallel/Parallel.h>
 
 #include <vector>
 
@@ -58,6 +59,51 @@ inline int b200UploadTopology(pmb200_ctx *ctx,
   if (rc) return rc;
   const PeriodicBoundaryConditions &bc = t.boundaryConditions;
   return pmb200_set_box(ctx, bc.e1().c, bc.e2().c, bc.e3().c, bc.origin().c);
+}
+
+// Force::numberOfBlocks for the B200 forces: the cells of the device grid,
+// grouped as Parallel::getNumberOfPackages groups the reference's cells
+// (NonbondedCutoffForce::numberOfBlocks,
+// protomol/src/protomol/force/nonbonded/NonbondedCutoffForce.h:60-65).
+inline unsigned int b200NumberOfBlocks(pmb200_ctx *ctx) {
+  int dims[3];
+  double edge[3];
+  if (pmb200_grid(ctx, dims, edge) != PMB200_OK) return 1;
+  return Parallel::getNumberOfPackages((unsigned int)(dims[0] * dims[1] * dims[2]));
+}
+
+// SystemForce::parallelEvaluate's share of one rank, as
+// NonbondedCutoffSystemForce::parallelEvaluate splits it
+// (protomol/src/protomol/force/nonbonded/NonbondedCutoffSystemForce.h:57-77):
+// block i of count = b200NumberOfBlocks covers the cells
+// [n i / count, n (i + 1) / count), Parallel::next() is called once per
+// block in order, and the blocks it grants are evaluated (runs of adjacent
+// blocks in one pmb200_eval_cells call).  Forces and e/vir/mvir are
+// accumulated into; Parallel::reduce then sums the ranks' shares
+// (force/ForceGroup.cpp:116).  Returns the first non-zero libpmb200 status
+// (every next() call is still made).
+inline int b200ParallelEval(pmb200_ctx *ctx, const double *pos, double *forces, double *e,
+                            double *vir, double *mvir, unsigned flags) {
+  int dims[3];
+  double edge[3];
+  int rc = pmb200_grid(ctx, dims, edge);
+  if (rc) return rc;
+  const unsigned long long n = (unsigned long long)dims[0] * dims[1] * dims[2];
+  const unsigned int count = Parallel::getNumberOfPackages((unsigned int)n);
+  int lo = -1, hi = -1;
+  for (unsigned int i = 0; i < count; i++) {
+    const int a = (int)(n * i / count), b = (int)(n * (i + 1) / count);
+    if (!Parallel::next()) continue;
+    if (lo >= 0 && a == hi) {
+      hi = b;
+      continue;
+    }
+    if (lo >= 0 && !rc) rc = pmb200_eval_cells(ctx, pos, forces, e, vir, mvir, flags, lo, hi);
+    lo = a;
+    hi = b;
+  }
+  if (lo >= 0 && !rc) rc = pmb200_eval_cells(ctx, pos, forces, e, vir, mvir, flags, lo, hi);
+  return rc;
 }
 
 }  // namespace ProtoMol

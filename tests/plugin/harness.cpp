@@ -23,6 +23,7 @@
 #include <protomol/force/OneAtomPair.h>
 #include <protomol/topology/TopologyUtilities.h>
 #include <protomol/config/Value.h>
+#include <protomol/parallel/Parallel.h>
 
 #include <cstring>
 #include <exception>
@@ -42,8 +43,28 @@ typedef NonbondedFullEwaldSystemForce<PeriodicBoundaryConditions, CubicCellManag
     RefEwaldReal;
 
 static char g_msg[1024];
+// parallel mode: forces are called through SystemForce::parallelEvaluate
+// (with Force::numberOfBlocks asked first, as ForceGroup does) instead of
+// evaluate; without MPI, Parallel::next() grants every block
+static int g_parallel = 0;
+static unsigned int g_blocks = 0;
 
 extern "C" const char *harness_message() { return g_msg; }
+extern "C" void harness_set_parallel(int on) { g_parallel = on; }
+extern "C" unsigned int harness_last_blocks() { return g_blocks; }
+
+template <class TTopo>
+static void call_force(Force *force, TTopo *t, Vector3DBlock *p, Vector3DBlock *fr,
+                       ScalarStructure *en) {
+  SystemForce *sf = dynamic_cast<SystemForce *>(force);
+  if (g_parallel) {
+    Parallel::resetNext();
+    g_blocks = sf->numberOfBlocks(t, p);
+    sf->parallelEvaluate(t, p, fr, en);
+  } else {
+    sf->evaluate(t, p, fr, en);
+  }
+}
 
 static Force *make_force(ForceFactory &f, const std::string &id, double ron, double rclj,
                          double rcc, double rc) {
@@ -65,7 +86,7 @@ static void eval_force(Force *force, PTopo *t, const double *pos, int n, double 
   en.virial(true);
   en.molecularVirial(true);
   buildMolecularCenterOfMass(&p, t);
-  dynamic_cast<SystemForce *>(force)->evaluate(t, &p, &fr, &en);
+  call_force(force, t, &p, &fr, &en);
   std::memcpy(f, fr.c, sizeof(double) * 3 * n);
   e[0] = en[ScalarStructure::COULOMB];
   e[1] = en[ScalarStructure::LENNARDJONES];
@@ -171,7 +192,7 @@ static int pair_eval_on(Topology<TBC, CubicCellManager> *t, bool vacuum, const c
   en.virial(true);
   en.molecularVirial(true);
   buildMolecularCenterOfMass(&p, t);
-  dynamic_cast<SystemForce *>(force)->evaluate(t, &p, &fr, &en);
+  call_force(force, t, &p, &fr, &en);
   std::memcpy(forces, fr.c, sizeof(double) * 3 * n);
   energies[0] = en[ScalarStructure::COULOMB];
   energies[1] = en[ScalarStructure::LENNARDJONES];

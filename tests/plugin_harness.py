@@ -20,7 +20,19 @@ def lib():
     L.harness_eval.argtypes = [_P, _I, _I, _P, _D, _D, _D, _D, _P, _P, _P, _P]
     L.harness_eval.restype = _I
     L.harness_message.restype = ctypes.c_char_p
+    L.harness_set_parallel.argtypes = [_I]
+    L.harness_last_blocks.restype = ctypes.c_uint
     return L
+
+
+def set_parallel(on):
+    """Call the forces through SystemForce::parallelEvaluate (after
+    Force::numberOfBlocks, as ForceGroup does) instead of evaluate."""
+    lib().harness_set_parallel(1 if on else 0)
+
+
+def last_blocks():
+    return int(lib().harness_last_blocks())
 
 
 def evaluate(ref_force, which, sysd, pos):

@@ -178,3 +178,76 @@ def test_vacuum_plugin_matches_reference():
     fr = d["ref_forces"]
     assert np.sqrt(((f - fr) ** 2).sum() / (fr ** 2).sum()) <= 1e-5
     assert np.abs(e - d["ref_energies"]).max() <= 2e-3
+
+
+def _parallel_vs_plain(call):
+    """(plain result, parallelEvaluate result, blocks) of one harness call."""
+    H.set_parallel(False)
+    plain = call()
+    H.set_parallel(True)
+    try:
+        par = call()
+        blocks = H.last_blocks()
+    finally:
+        H.set_parallel(False)
+    return plain, par, blocks
+
+
+def test_reference_parallel_evaluate_equals_evaluate(water648):
+    """The harness's parallel mode on the reference prototype: without MPI
+    Parallel::next() grants every block, so parallelEvaluate == evaluate."""
+    R = O.RefForce(water648)
+    plain, par, blocks = _parallel_vs_plain(
+        lambda: H.evaluate(R, 0, water648, water648["pos"]))
+    R.close()
+    assert plain[0] == 0 and par[0] == 0, par[1]
+    assert blocks >= 1
+    np.testing.assert_allclose(par[2], plain[2], rtol=0, atol=1e-12)
+    np.testing.assert_allclose(par[3], plain[3], rtol=1e-13)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("which", [1, 2])
+def test_plugin_parallel_evaluate_matches_evaluate(water648, which):
+    """The B200 forces override parallelEvaluate / numberOfBlocks (the
+    default would evaluate everything on every rank); under the reference's
+    sequential Parallel every block is granted, so the result is evaluate's,
+    and numberOfBlocks is the number of device grid cells."""
+    R = O.RefForce(water648)
+    plain, par, blocks = _parallel_vs_plain(
+        lambda: H.evaluate(R, which, water648, water648["pos"]))
+    R.close()
+    assert plain[0] == 0 and par[0] == 0, par[1]
+    from protomoladdon_b200.force import NonbondedCutoffB200SystemForce, PeriodicTopology
+    f = NonbondedCutoffB200SystemForce(water648["ron"], water648["rc_lj"], water648["rc_coul"],
+                                       water648["rc_alg"])
+    assert blocks == f.number_of_blocks(PeriodicTopology.from_dict(water648))
+    f.close()
+    np.testing.assert_allclose(par[2], plain[2], rtol=0, atol=1e-12 * np.abs(plain[2]).max())
+    np.testing.assert_allclose(par[3], plain[3], rtol=1e-12)
+    np.testing.assert_allclose(par[4], plain[4], rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(par[5], plain[5], rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.gpu
+def test_plugin_ewald_and_pair_parallel_evaluate(water648):
+    """parallelEvaluate == evaluate for the Ewald real-space force, a
+    periodic switch-policy force and the vacuum force (sequential Parallel)."""
+    from .conftest import load_fixture
+    acc = float(np.exp(-(0.35 * 8.0) ** 2))
+    dp, fid, vals = _pair_case("c2_cn")
+    dv = load_fixture("vacuum_ref.npz")
+    vid = ("LennardJones Coulomb -switchingFunction C2 -switchingFunction C1 "
+           "-algorithm NonbondedCutoffB200")
+    cases = ((water648, lambda R: H.evaluate_ewald(R, 1, water648, water648["pos"], 0.35, acc)),
+             (dp, lambda R: H.evaluate_pair(R, 0, fid, vals, dp["pos"])),
+             (dv, lambda R: H.evaluate_pair(R, 1, vid, [7.0, 8.0, 8.0, 8.0], dv["pos"])))
+    for d, call in cases:
+        R = O.RefForce(d)
+        plain, par, blocks = _parallel_vs_plain(lambda: call(R))
+        R.close()
+        assert plain[0] == 0 and par[0] == 0, par[1]
+        assert blocks >= 1
+        np.testing.assert_allclose(par[2], plain[2], rtol=0,
+                                   atol=1e-12 * np.abs(plain[2]).max())
+        np.testing.assert_allclose(par[3], plain[3], rtol=1e-12, atol=1e-12)
