@@ -85,7 +85,8 @@ const char *pmb200_last_error(const pmb200_ctx *ctx);
  *   mass[n]      Atom::scaledMass (may be NULL; needed for PMB200_MOLVIRIAL
  *                and the integrator)
  *   lj[ntypes*ntypes*4]  LennardJonesParameterTable {A, B, A14, B14}
- *                (protomol/src/protomol/topology/LennardJonesParameterTable.h:34-36)
+ *                (protomol/src/protomol/topology/LennardJonesParameterTable.h:34-36);
+ *                ntypes <= 1024 (the derivative kernels: <= 39; batches: <= 16)
  *   excl[nexcl*3]  ExclusionTable entries {a1, a2, kind}, kind 1 =
  *                EXCLUSION_MODIFIED, 2 = EXCLUSION_FULL; later duplicates
  *                override earlier ones like ExclusionTable::add

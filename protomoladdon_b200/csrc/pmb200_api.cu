@@ -362,16 +362,26 @@ void launch_pair_mixed(pmb200_ctx *c, unsigned flags, cudaStream_t st, int cell0
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
   cfg.numAttrs = (pdl && PMB200_PDL) ? 1 : 0;
-#define PMB_MIXED_LAUNCH(E, V, M)                                                          \
-  cudaLaunchKernelEx(&cfg, k_pair_mixed<F, E, V, M>, g, c->mc, c->half, c->ntypes,         \
+  // tables of more than kMaxTypes types are read through L1 (forms with LJ)
+  constexpr bool kLjForm = F == FORM_CUTOFF || F == FORM_GENERIC;
+  const bool big = kLjForm && c->ntypes > kMaxTypes;
+#define PMB_MIXED_LAUNCH(E, V, M, G)                                                       \
+  cudaLaunchKernelEx(&cfg, k_pair_mixed<F, E, V, M, G>, g, c->mc, c->half, c->ntypes,      \
                      c->d_lj32, c->d_start, c->d_spos32, c->d_smeta, c->d_sidx,             \
                      c->d_ex_start, c->d_ex, facc, c->n, c->d_err, c->d_partial, c->pb,     \
                      c->d_com, slots, c->d_spos_lo, ncells > 0 ? cell0 : g.ncell)
-  if (molvir) PMB_MIXED_LAUNCH(true, true, true);
-  else if (energy && virial) PMB_MIXED_LAUNCH(true, true, false);
-  else if (energy) PMB_MIXED_LAUNCH(true, false, false);
-  else if (virial) PMB_MIXED_LAUNCH(false, true, false);
-  else PMB_MIXED_LAUNCH(false, false, false);
+#define PMB_MIXED_FLAGS(G)                                                                 \
+  if (molvir) PMB_MIXED_LAUNCH(true, true, true, G);                                       \
+  else if (energy && virial) PMB_MIXED_LAUNCH(true, true, false, G);                       \
+  else if (energy) PMB_MIXED_LAUNCH(true, false, false, G);                                \
+  else if (virial) PMB_MIXED_LAUNCH(false, true, false, G);                                \
+  else PMB_MIXED_LAUNCH(false, false, false, G)
+  if (!big) {
+    PMB_MIXED_FLAGS(false);
+  } else if constexpr (kLjForm) {
+    PMB_MIXED_FLAGS(true);
+  }
+#undef PMB_MIXED_FLAGS
 #undef PMB_MIXED_LAUNCH
 }
 
@@ -722,8 +732,9 @@ int pmb200_set_topology(pmb200_ctx *c, int n, const int *type, const double *q_s
   if (n > 0 && (!type || !q_scaled || !molecule)) return fail(c, PMB200_EINVAL, "null array");
   if (!lj) return fail(c, PMB200_EINVAL, "null LJ table");
   if (nexcl > 0 && !excl) return fail(c, PMB200_EINVAL, "null exclusion array");
-  if (ntypes > kMaxTypes)
-    return fail(c, PMB200_EUNSUPPORTED, "%d LJ types; at most %d supported", ntypes, kMaxTypes);
+  if (ntypes > kMaxTypesTable)
+    return fail(c, PMB200_EUNSUPPORTED, "%d LJ types; at most %d supported", ntypes,
+                kMaxTypesTable);
   CK(cudaSetDevice(c->p.device));
   int nmol = 0;
   for (int i = 0; i < n; i++) {
@@ -1125,6 +1136,10 @@ static int deriv_ready(pmb200_ctx *c) {
   if (rc) return rc;
   if (c->form != FORM_CUTOFF)
     return fail(c, PMB200_EUNSUPPORTED, "derivative kernels cover the cutoff LJ + Coulomb force");
+  // the table derivatives are summed per block in shared memory (48 KB)
+  if (sizeof(double) * 4 * (size_t)c->ntypes * c->ntypes > 48 * 1024)
+    return fail(c, PMB200_EUNSUPPORTED, "derivative kernels: at most 39 LJ types (%d given)",
+                c->ntypes);
   return PMB200_OK;
 }
 
@@ -2290,6 +2305,7 @@ int pmb200_batch_create(pmb200_ctx *const *systems, int nsys, pmb200_batch **out
     if (!c) return PMB200_EINVAL;
     if (!c->have_topo || !c->have_box) return PMB200_ESTATE;
     if (c->p.precision != PMB200_MIXED) return PMB200_EUNSUPPORTED;
+    if (c->ntypes > kMaxTypes) return PMB200_EUNSUPPORTED;  // tables staged in shared memory
     if (c->form != systems[0]->form || c->p.device != systems[0]->p.device)
       return PMB200_EINVAL;
   }

@@ -24,6 +24,8 @@ namespace pmb200 {
 
 constexpr int kMaxRows = 64;          // stencil rows (dy, dz), passed by value
 constexpr int kMaxTypes = 16;         // LJ types held in shared memory
+constexpr int kMaxTypesTable = 1024;  // LJ types of a context (more than kMaxTypes:
+                                      // the mixed kernel reads the table through L1)
 constexpr int kNacc = 18;             // slots per partial-sum row (ACC_MV)
 constexpr double kFixScale = 4294967296.0;          // 2^32 per force unit
 constexpr double kFixInv = 1.0 / 4294967296.0;
@@ -1087,7 +1089,9 @@ constexpr int kMaxCellSlots = 8;
 constexpr int kEnergyCellSlots = 4;  // energy / virial launches (the ones with partial rows)
 
 
-template <int kForm, bool kEnergy, bool kVirial, bool kMolVir>
+// kGlobalLj: the LJ table (more than kMaxTypes types) is read from global
+// memory through L1 instead of being staged in shared memory.
+template <int kForm, bool kEnergy, bool kVirial, bool kMolVir, bool kGlobalLj = false>
 __global__ void __launch_bounds__(32, kVirial ? 1 : (kEnergy ? 19 : 26))
 k_pair_mixed(GridParams g, MixedConsts mc, const HalfStencil st, int ntypes, const float4 *__restrict__ lj32,
              const int *__restrict__ start, const float4 *__restrict__ spos,
@@ -1100,7 +1104,7 @@ k_pair_mixed(GridParams g, MixedConsts mc, const HalfStencil st, int ntypes, con
   __shared__ MixedWarpSmem sm;
   __shared__ double s_pd[(kEnergy && kForm == FORM_CUTOFF) ? 3 * kBatch : 1];
   constexpr bool kLj = kForm == FORM_CUTOFF || kForm == FORM_GENERIC;
-  const int nlj = kLj ? ntypes * ntypes : 0;
+  const int nlj = (kLj && !kGlobalLj) ? ntypes * ntypes : 0;
   float4 *s_lj = s_dyn;
   unsigned short *s_st = reinterpret_cast<unsigned short *>(s_dyn + nlj);
   const int lane = threadIdx.x;
@@ -1115,7 +1119,8 @@ k_pair_mixed(GridParams g, MixedConsts mc, const HalfStencil st, int ntypes, con
   const int cell = cell0 + (int)(blockIdx.x / slots);  // cells cell0.. (a shard's range)
   if (cell >= g.ncell) return;  // uniform per block
   mixed_task<kForm, kEnergy, kVirial, kMolVir>(
-      g, mc, s_st, st.ncells, blockIdx.x % slots, slots, ntypes, s_lj, cell, start,
+      g, mc, s_st, st.ncells, blockIdx.x % slots, slots, ntypes, kGlobalLj ? lj32 : s_lj, cell,
+      start,
       spos, smeta, sidx, ex_start, ex, facc, n, partial + (size_t)blockIdx.x * kNacc, pb, com,
       sm, err, s_pd, spos_lo);
 }
@@ -1130,7 +1135,7 @@ inline int mixed_cell_slots(bool energy_or_virial, int natoms, int ncell) {
 
 // Dynamic shared memory of a k_pair_mixed launch.
 inline size_t mixed_smem_bytes(int form, int ntypes, int st_ncells) {
-  const size_t lj = (form == FORM_CUTOFF || form == FORM_GENERIC)
+  const size_t lj = ((form == FORM_CUTOFF || form == FORM_GENERIC) && ntypes <= kMaxTypes)
                         ? sizeof(float4) * (size_t)ntypes * ntypes : 0;
   return lj + ((sizeof(unsigned short) * (size_t)st_ncells + 15) & ~(size_t)15);
 }

@@ -174,6 +174,39 @@ def rigid_waters(sysd) -> np.ndarray:
     return np.asarray(out, dtype=np.int32).reshape(-1, 3)
 
 
+def many_types(sysd, n_o_types=14, n_h_types=10, n_unused=6, seed=7):
+    """The same atoms spread over many Lennard-Jones types, as a force-field
+    topology has them: each oxygen gets one of ``n_o_types`` O-like types
+    (sigma 3.0-3.3 A, epsilon 0.12-0.18 kcal/mol), each hydrogen one of
+    ``n_h_types`` H-like types with a small LJ term (sigma 0.9-1.5 A,
+    epsilon 0.02-0.05), and ``n_unused`` more types appear only in the table
+    (like the unused types of a parameter file); Lorentz-Berthelot mixing,
+    A14/B14 at half strength.  Charges, geometry and exclusions unchanged."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    d = dict(sysd)
+    typ = np.asarray(sysd["type"]).copy()
+    o = typ == T_O
+    h = typ == T_H
+    typ[o] = rng.integers(0, n_o_types, size=int(o.sum()))
+    typ[h] = n_o_types + rng.integers(0, n_h_types, size=int(h.sum()))
+    nt = n_o_types + n_h_types + n_unused
+    sig = np.concatenate([rng.uniform(3.0, 3.3, n_o_types), rng.uniform(0.9, 1.5, n_h_types),
+                          rng.uniform(1.0, 4.0, n_unused)])
+    eps = np.concatenate([rng.uniform(0.12, 0.18, n_o_types),
+                          rng.uniform(0.02, 0.05, n_h_types), rng.uniform(0.01, 0.2, n_unused)])
+    t = np.zeros((nt, nt, 4))
+    for a in range(nt):
+        for b in range(nt):
+            sg = 0.5 * (sig[a] + sig[b])
+            ep = math.sqrt(eps[a] * eps[b])
+            A = 4.0 * ep * sg ** 12
+            B = 4.0 * ep * sg ** 6
+            t[a, b] = (A, B, 0.5 * A, 0.5 * B)
+    d["type"] = typ.astype(np.int32)
+    d["lj"] = t
+    return d
+
+
 # Named workloads (sizes from the reference-facing benchmark definitions).
 def small_648(seed=1234):
     """216 waters, 6^3 lattice, box 18.624 A, rc 8, C2 from 7."""

@@ -108,7 +108,23 @@ def main(ref_root):
     np.savez_compressed(os.path.join(HERE, "modified_ref.npz"), **sysd_arrays(m),
                         ref_forces=f, ref_energies=e, ref_virial=v, ref_molvirial=mv)
     R.close()
+    many_types_fixture()
     print("wrote fixtures to", HERE)
+
+
+def many_types_fixture():
+    """The 648-atom box over 30 LJ types (24 used) with the H-H pair of each
+    water modified (A14/B14, Coulomb scaling 0.5) and O-H fully excluded."""
+    t = water.many_types(water.small_648())
+    ex = t["excl"].copy()
+    ex[t["type"][ex[:, 0]] >= 14, 2] = 1  # H-H modified, O-H full
+    t["excl"] = ex
+    t["coulomb_scaling"] = 0.5
+    R = O.RefForce(t)
+    f, e, v, mv = R.evaluate(t["pos"], 2)
+    np.savez_compressed(os.path.join(HERE, "manytypes_ref.npz"), **sysd_arrays(t),
+                        ref_forces=f, ref_energies=e, ref_virial=v, ref_molvirial=mv)
+    R.close()
 
 
 def ewald_fixtures():
@@ -227,3 +243,5 @@ if __name__ == "__main__":
         pair_fixtures()
     if not only or "--vacuum-only" in only:
         vacuum_fixture()
+    if "--manytypes-only" in only:
+        many_types_fixture()

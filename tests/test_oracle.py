@@ -207,3 +207,13 @@ def test_ewald_restatement_bitexact_vs_compiled_reference(seed, exact):
     g, ee, vv, mm = O.restate_ewald_real(s, s["pos"], 0.33, acc, exact, 2)
     assert np.array_equal(f, g) and e == ee
     assert np.array_equal(v, vv) and np.array_equal(mv, mm)
+
+
+def test_restatement_bitexact_vs_many_types_fixture():
+    """A 30-type table (24 used) with modified H-H pairs: the restatement
+    equals the reference's own output bit for bit."""
+    from tests.conftest import load_fixture
+    d = load_fixture("manytypes_ref.npz")
+    f, e, v, mv = O.restate_eval(d, d["pos"], 2)
+    assert np.array_equal(f, d["ref_forces"]) and np.array_equal(e, d["ref_energies"])
+    assert np.array_equal(v, d["ref_virial"]) and np.array_equal(mv, d["ref_molvirial"])
