@@ -119,6 +119,10 @@ def ref_lib(exact_erfc: bool = False):
         lib.pmref_hessian.restype = _I
         lib.pmref_pair_eval.argtypes = [_P, _I, _P, _I, _P, _D, _P, _P, _P, _P, _P, _I]
         lib.pmref_pair_eval.restype = _I
+        lib.pmref_set_box.argtypes = [_P, _P, _P, _P, _P]
+        lib.pmref_set_box.restype = _I
+        lib.pmref_eval_allpairs.argtypes = [_P, _P, _P, _P, _P, _P, _I]
+        lib.pmref_eval_allpairs.restype = _I
         if exact_erfc:
             _ref_exact = lib
         else:
@@ -275,7 +279,9 @@ class RefForce:
         self._sys = {k: sysd[k] for k in ("ron", "rc_lj", "rc_coul", "rc_alg")}
         self.ar = _Arrays(sysd)
         ar = self.ar
-        box = np.ascontiguousarray(sysd["box"], dtype=np.float64)
+        basis = np.asarray(sysd["box"], dtype=np.float64)
+        # a 3x3 box holds the basis vectors as rows (a general periodic cell)
+        box = np.ascontiguousarray(np.diag(basis) if basis.shape == (3, 3) else basis)
         org = np.ascontiguousarray(sysd.get("origin", (0.0, 0.0, 0.0)), dtype=np.float64)
         self._keep = (box, org)
         self.n = ar.n
@@ -284,6 +290,8 @@ class RefForce:
             _ptr(ar.lj), ar.nexcl, _ptr(ar.excl), float(sysd.get("coulomb_scaling", 1.0)),
             _ptr(box), _ptr(org), float(sysd["cellsize"]), float(sysd["ron"]),
             float(sysd["rc_lj"]), float(sysd["rc_coul"]), float(sysd["rc_alg"]))
+        if basis.shape == (3, 3):
+            self.set_box(basis[0], basis[1], basis[2], org)
 
     def evaluate(self, pos, virial_mode=2):
         p = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1)
@@ -292,6 +300,25 @@ class RefForce:
         v = np.zeros(9)
         mv = np.zeros(9)
         self.lib.pmref_eval(self.h, _ptr(p), _ptr(f), _ptr(e), _ptr(v), _ptr(mv), int(virial_mode))
+        return f.reshape(-1, 3), e, v, mv
+
+    def set_box(self, e1, e2, e3, origin):
+        """PeriodicBoundaryConditions::set with a general basis (the
+        reference's non-orthogonal minimal image)."""
+        vec = [np.ascontiguousarray(x, dtype=np.float64) for x in (e1, e2, e3, origin)]
+        self._keep_box = vec
+        self.lib.pmref_set_box(self.h, *[_ptr(x) for x in vec])
+
+    def evaluate_allpairs(self, pos, virial_mode=2):
+        """The same pair function over every pair i < j at the minimal image
+        (NonbondedSimpleFullSystemForce): no cell list."""
+        p = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1)
+        f = np.zeros(p.size)
+        e = np.zeros(2)
+        v = np.zeros(9)
+        mv = np.zeros(9)
+        self.lib.pmref_eval_allpairs(self.h, _ptr(p), _ptr(f), _ptr(e), _ptr(v), _ptr(mv),
+                                     int(virial_mode))
         return f.reshape(-1, 3), e, v, mv
 
     def ewald_real(self, pos, alpha, accuracy, virial_mode=2):

@@ -12,6 +12,7 @@
 // on a Topology<PeriodicBoundaryConditions, CubicCellManager> filled from flat
 // arrays (protomol/src/protomol/topology/Topology.h:26-31).
 #include <protomol/force/nonbonded/NonbondedCutoffSystemForce.h>
+#include <protomol/force/nonbonded/NonbondedSimpleFullSystemForce.h>
 #include <protomol/force/OneAtomPairTwo.h>
 #include <protomol/force/LennardJonesForce.h>
 #include <protomol/force/CoulombForce.h>
@@ -52,6 +53,7 @@ struct pmref_sys {
   Vector3DBlock pos, frc, vel;
   ScalarStructure energies;
   int n;
+  double ron, rc_lj, rc_coul;  // the switches, for pmref_eval_allpairs
 };
 
 extern "C" {
@@ -107,11 +109,60 @@ void *pmref_create(int n, const int *type, const double *qscaled,
   s->pos.resize(n);
   s->frc.resize(n);
   s->vel.resize(n);
+  s->ron = ron;
+  s->rc_lj = rc_lj;
+  s->rc_coul = rc_coul;
   s->force = new PForce(rc_alg, PPair(LennardJonesForce(),
                                       C2SwitchingFunction(ron, rc_lj),
                                       CoulombForce(),
                                       C1SwitchingFunction(rc_coul)));
   return s;
+}
+
+// A general periodic cell: PeriodicBoundaryConditions::set with any basis
+// (the non-orthogonal minimal image of
+// protomol/src/protomol/topology/PeriodicBoundaryConditions.h:62-67, 95-100);
+// the cell lists are rebuilt at the next evaluation.
+int pmref_set_box(void *h, const double e1[3], const double e2[3], const double e3[3],
+                  const double origin[3]) {
+  pmref_sys *s = (pmref_sys *)h;
+  s->topo->boundaryConditions.set(Vector3D(e1[0], e1[1], e1[2]), Vector3D(e2[0], e2[1], e2[2]),
+                                  Vector3D(e3[0], e3[1], e3[2]),
+                                  Vector3D(origin[0], origin[1], origin[2]));
+  s->topo->uncacheCellList();
+  return 0;
+}
+
+// The same pair function over every pair i < j
+// (NonbondedSimpleFullSystemForce, protomol/src/protomol/force/nonbonded/
+// NonbondedSimpleFullSystemForce.h): no cell list, each pair at the minimal
+// image of PeriodicBoundaryConditions::minimalDifference.  Arguments as
+// pmref_eval.
+int pmref_eval_allpairs(void *h, const double *pos, double *forces, double *energies,
+                        double *virial, double *molvirial, int virial_mode) {
+  pmref_sys *s = (pmref_sys *)h;
+  const int n = s->n;
+  NonbondedSimpleFullSystemForce<PPair> full(
+      PPair(LennardJonesForce(), C2SwitchingFunction(s->ron, s->rc_lj), CoulombForce(),
+            C1SwitchingFunction(s->rc_coul)));
+  memcpy(s->pos.c, pos, sizeof(double) * 3 * n);
+  memcpy(s->frc.c, forces, sizeof(double) * 3 * n);
+  s->energies.clear();
+  s->energies.virial(virial_mode >= 1);
+  s->energies.molecularVirial(virial_mode >= 2);
+  if (virial_mode >= 2) buildMolecularCenterOfMass(&s->pos, s->topo);
+  full.evaluate(s->topo, &s->pos, &s->frc, &s->energies);
+  memcpy(forces, s->frc.c, sizeof(double) * 3 * n);
+  energies[0] = s->energies[ScalarStructure::COULOMB];
+  energies[1] = s->energies[ScalarStructure::LENNARDJONES];
+  if (virial)
+    for (int k = 0; k < 9; k++)
+      virial[k] = s->energies[(ScalarStructure::Index)(ScalarStructure::VIRIALXX + k)];
+  if (molvirial)
+    for (int k = 0; k < 9; k++)
+      molvirial[k] =
+        s->energies[(ScalarStructure::Index)(ScalarStructure::MOLVIRIALXX + k)];
+  return 0;
 }
 
 // The Topology<PeriodicBoundaryConditions, CubicCellManager> built by

@@ -263,10 +263,10 @@ SwitchSpec<T> make_switch(int kind, const double par[4], double u) {
 // (protomol/src/protomol/force/nonbonded/NonbondedFullEwaldSystemForce.h:
 // 586-598): alpha (default sqrt(pi) (5.5 N / V^2)^(1/6), V = |(e1 x e2) . e3|)
 // and rc = sqrt(-log(accuracy)) / alpha.
-void ewald_derive(pmb200_ctx *c, const double L[3]) {
+void ewald_derive(pmb200_ctx *c, double volume) {
   double alpha = c->ew_alpha_in;
   if (alpha <= 0.0) {
-    const double v = std::fabs((L[0] * L[1]) * L[2]);
+    const double v = volume;
     alpha = std::sqrt(M_PI) * std::pow(5.5 * (unsigned)c->n / (v * v), 1.0 / 6.0);
   }
   c->ew_alpha = alpha;
@@ -414,6 +414,62 @@ int ensure_clear(pmb200_ctx *c, cudaStream_t st) {
   if (!c->count_zero && c->d_count && c->g.ncell > 0) {
     CK(cudaMemsetAsync(c->d_count, 0, sizeof(int) * (size_t)c->g.ncell, st));
     c->count_zero = true;
+  }
+  return PMB200_OK;
+}
+
+// Neighbour-cell stencils of the current grid for the cutoff rc: rows (dy,
+// dz) with their dx span (full shell) and the half shell by cell (offsets
+// with dz > 0, or dz == 0 and dy > 0, or dz == dy == 0 and dx >= 0; dx == 0
+// is the home cell, pairs i < j) in a fixed pseudo-random order --
+// consecutive cells of a warp's share then lie in different directions, so
+// each staged batch holds a similar number of partners for every i atom.
+// Orthogonal grid: every cell whose nearest point can lie within rc of the
+// home cell.  General cell: every offset up to ceil(rc n_k / width_k) cells
+// along each basis vector (the fractional extent of the cutoff sphere).
+int build_stencils(pmb200_ctx *c, double rc, std::vector<Row> &rows, HalfStencil &half) {
+  const GridParams &g = c->g;
+  rows.clear();
+  if (g.tric) {
+    int R[3];
+    for (int k = 0; k < 3; k++) R[k] = (int)std::ceil(rc / g.edge[k] - 1e-12);
+    for (int dz = -R[2]; dz <= R[2]; dz++)
+      for (int dy = -R[1]; dy <= R[1]; dy++) rows.push_back(Row{dy, dz, -R[0], R[0]});
+  } else {
+    int R[3];
+    for (int a = 0; a < 3; a++) R[a] = (int)std::ceil(rc / g.edge[a] - 1e-12);
+    const double rc2 = rc * rc * (1.0 + 1e-12);
+    for (int dz = -R[2]; dz <= R[2]; dz++)
+      for (int dy = -R[1]; dy <= R[1]; dy++) {
+        const double yz = std::pow(std::max(std::abs(dy) - 1, 0) * g.edge[1], 2) +
+                          std::pow(std::max(std::abs(dz) - 1, 0) * g.edge[2], 2);
+        if (yz > rc2) continue;
+        int hi = 0;
+        for (int dx = 0; dx <= R[0]; dx++)
+          if (yz + std::pow(std::max(dx - 1, 0) * g.edge[0], 2) <= rc2) hi = dx;
+        rows.push_back(Row{dy, dz, -hi, hi});
+      }
+  }
+  if ((int)rows.size() > kMaxRows)
+    return fail(c, PMB200_EUNSUPPORTED, "stencil of %d rows (cell size too small)",
+                (int)rows.size());
+  half = HalfStencil{};
+  for (const Row &rw : rows)
+    for (int dx = rw.dxlo; dx <= rw.dxhi; dx++) {
+      const bool keep = rw.dz > 0 || (rw.dz == 0 && rw.dy > 0) ||
+                        (rw.dz == 0 && rw.dy == 0 && dx >= 0);
+      if (!keep) continue;
+      if (half.ncells >= kMaxHalfCells || std::abs(dx) > 8 || std::abs(rw.dy) > 8 ||
+          std::abs(rw.dz) > 8)
+        return fail(c, PMB200_EUNSUPPORTED, "neighbour stencil too large (cell size too small)");
+      half.off[half.ncells++] =
+          (unsigned short)((dx + 8) | ((rw.dy + 8) << 5) | ((rw.dz + 8) << 10));
+    }
+  unsigned long long x = 0x9E3779B97F4A7C15ull;
+  for (int k = half.ncells - 1; k > 0; k--) {
+    x = x * 6364136223846793005ull + 1442695040888963407ull;
+    const int j = (int)((x >> 33) % (unsigned long long)(k + 1));
+    std::swap(half.off[k], half.off[j]);
   }
   return PMB200_OK;
 }
@@ -827,12 +883,38 @@ int pmb200_set_box(pmb200_ctx *c, const double e1[3], const double e2[3], const 
   c->vacuum_pending = false;
   if (!e1 || !e2 || !e3 || !origin) return fail(c, PMB200_EINVAL, "null box vector");
   c->vacuum = vacuum;
-  if (e1[1] != 0.0 || e1[2] != 0.0 || e2[0] != 0.0 || e2[2] != 0.0 || e3[0] != 0.0 ||
-      e3[1] != 0.0)
-    return fail(c, PMB200_EUNSUPPORTED, "only orthogonal periodic boxes are supported");
+  // PeriodicBoundaryConditions::set (PeriodicBoundaryConditions.cpp:38-66):
+  // orthogonal when every off-diagonal component is zero; the reciprocal
+  // vectors e_k^r = (e_{k+1} x e_{k+2}) / (e_k . (e_{k+1} x e_{k+2}))
+  const bool ortho = !(e1[1] != 0.0 || e1[2] != 0.0 || e2[0] != 0.0 || e2[2] != 0.0 ||
+                       e3[0] != 0.0 || e3[1] != 0.0);
+  const double *ev[3] = {e1, e2, e3};
+  for (int k = 0; k < 3; k++)
+    for (int a = 0; a < 3; a++)
+      if (!std::isfinite(ev[k][a])) return fail(c, PMB200_EINVAL, "box vector %d", k + 1);
+  if (!ortho && vacuum)
+    return fail(c, PMB200_EINVAL, "a vacuum domain is an axis-aligned box");
+  auto cross = [](const double *a, const double *b, double *o) {
+    o[0] = a[1] * b[2] - a[2] * b[1];
+    o[1] = a[2] * b[0] - a[0] * b[2];
+    o[2] = a[0] * b[1] - a[1] * b[0];
+  };
+  auto dot = [](const double *a, const double *b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; };
+  double er[3][3], width[3];
+  for (int k = 0; k < 3; k++) {
+    double x[3];
+    cross(ev[(k + 1) % 3], ev[(k + 2) % 3], x);
+    const double den = dot(ev[k], x);
+    for (int a = 0; a < 3; a++) er[k][a] = x[a] / den;
+    width[k] = 1.0 / std::sqrt(dot(er[k], er[k]));  // distance between the faces
+  }
+  double cr[3];
+  cross(e1, e2, cr);
+  const double volume = std::fabs(dot(cr, e3));
+  if (!(volume > 0.0) || !std::isfinite(volume)) return fail(c, PMB200_EINVAL, "box has no volume");
   const double L[3] = {std::fabs(e1[0]), std::fabs(e2[1]), std::fabs(e3[2])};
   for (int a = 0; a < 3; a++) {
-    if (!(L[a] > 0.0) || !std::isfinite(L[a]))
+    if (ortho && (!(L[a] > 0.0) || !std::isfinite(L[a])))
       return fail(c, PMB200_EINVAL, "box edge %d is %g", a, L[a]);
     if (!std::isfinite(origin[a])) return fail(c, PMB200_EINVAL, "origin");
   }
@@ -846,80 +928,72 @@ int pmb200_set_box(pmb200_ctx *c, const double e1[3], const double e2[3], const 
       c->have_box = false;
       return PMB200_OK;
     }
-    ewald_derive(c, L);
+    ewald_derive(c, volume);
   }
   const double rc = ctx_rc(c);
   for (int a = 0; a < 3; a++) {
-    if (L[a] < 2.0 * rc && !c->vacuum)
+    if (width[a] < 2.0 * rc && !c->vacuum)
       return fail(c, PMB200_EUNSUPPORTED,
-                  "box edge %g is below twice the cutoff %g (minimum image would need more "
-                  "than one image per pair)", L[a], rc);
+                  "box width %g is below twice the cutoff %g (minimum image would need more "
+                  "than one image per pair)", width[a], rc);
   }
   CK(cudaSetDevice(c->p.device));
   release_graph(c);
   GridParams &g = c->g;
-  const double target = c->p.cellsize > 0.0 ? std::max(c->p.cellsize, rc / 3.0) : rc / 2.0;
+  g.tric = ortho ? 0 : 1;
   int nd[3];
-  for (int a = 0; a < 3; a++) {
-    nd[a] = std::max(1, (int)std::floor(L[a] / target));
-    g.edge[a] = L[a] / nd[a];
-    g.boxlen[a] = L[a];
-    g.boxmin[a] = origin[a] - 0.5 * L[a];
+  if (ortho) {
+    const double target = c->p.cellsize > 0.0 ? std::max(c->p.cellsize, rc / 3.0) : rc / 2.0;
+    for (int a = 0; a < 3; a++) {
+      nd[a] = std::max(1, (int)std::floor(L[a] / target));
+      g.edge[a] = L[a] / nd[a];
+      g.boxlen[a] = L[a];
+      g.boxmin[a] = origin[a] - 0.5 * L[a];
+    }
+    g.unit = g.edge[0];
+  } else {
+    // cells along each basis vector, a third of the cutoff wide by default;
+    // every neighbour-cell offset must be distinct modulo the grid, which
+    // also makes the image a cell offset gives a pair within the cutoff the
+    // reference's (fractional rounding) image
+    const double target = c->p.cellsize > 0.0 ? std::max(c->p.cellsize, rc / 4.0) : rc / 3.0;
+    double unit = 1e300;
+    for (int k = 0; k < 3; k++) {
+      nd[k] = std::max(1, (int)std::floor(width[k] / target));
+      const int R = (int)std::ceil(rc * nd[k] / width[k] - 1e-12);
+      if (2 * R + 1 > nd[k])
+        return fail(c, PMB200_EUNSUPPORTED,
+                    "general periodic cell: width %g along basis vector %d holds %d cells of "
+                    "%g A, but the cutoff %g needs %d on each side of a cell (widths of about "
+                    "3 cutoffs or more are supported)", width[k], k + 1, nd[k],
+                    width[k] / nd[k], rc, R);
+      g.edge[k] = width[k] / nd[k];
+      unit = std::min(unit, g.edge[k]);
+      for (int a = 0; a < 3; a++) {
+        g.lat[3 * k + a] = nd[k] * er[k][a];
+        g.ec[3 * a + k] = ev[k][a] / nd[k];
+      }
+    }
+    g.unit = unit;
+    for (int q = 0; q < 9; q++) g.m[q] = g.ec[q] / unit;
+    for (int a = 0; a < 3; a++) {
+      g.org[a] = origin[a];
+      g.boxmin[a] = origin[a] - 0.5 * (e1[a] + e2[a] + e3[a]);
+      g.boxlen[a] = 0.0;  // (not used by the lattice cell build)
+    }
   }
   g.nx = nd[0]; g.ny = nd[1]; g.nz = nd[2];
   g.periodic = c->vacuum ? 0 : 1;
   const long long ncell = (long long)nd[0] * nd[1] * nd[2];
   if (ncell > (1 << 24)) return fail(c, PMB200_EUNSUPPORTED, "%lld cells", ncell);
   g.ncell = (int)ncell;
-  g.unit = g.edge[0];
-  // stencil: rows (dy, dz) and their dx span, keeping every cell whose
-  // nearest point can lie within the cutoff of the home cell
-  int R[3];
-  for (int a = 0; a < 3; a++) R[a] = (int)std::ceil(rc / g.edge[a] - 1e-12);
-  c->rows.clear();
-  const double rc2 = rc * rc * (1.0 + 1e-12);
-  for (int dz = -R[2]; dz <= R[2]; dz++)
-    for (int dy = -R[1]; dy <= R[1]; dy++) {
-      const double yz = std::pow(std::max(std::abs(dy) - 1, 0) * g.edge[1], 2) +
-                        std::pow(std::max(std::abs(dz) - 1, 0) * g.edge[2], 2);
-      if (yz > rc2) continue;
-      int lo = 0, hi = 0;
-      for (int dx = 0; dx <= R[0]; dx++)
-        if (yz + std::pow(std::max(dx - 1, 0) * g.edge[0], 2) <= rc2) hi = dx;
-      lo = -hi;
-      c->rows.push_back(Row{dy, dz, lo, hi});
-    }
-  if ((int)c->rows.size() > kMaxRows)
-    return fail(c, PMB200_EUNSUPPORTED, "stencil of %d rows (cell size too small)",
-                (int)c->rows.size());
+  // stencils for the cutoff: the FP64 kernel's full shell and the mixed
+  // kernel's half shell
+  int src = build_stencils(c, rc, c->rows, c->half);
+  if (src) return src;
   g.nrows = (int)c->rows.size();
   c->stencil = Stencil{};
   for (size_t r = 0; r < c->rows.size(); r++) c->stencil.rows[r] = c->rows[r];
-  // half shell by cell: offsets with dz > 0, or dz == 0 and dy > 0, or
-  // dz == dy == 0 and dx >= 0 (dx == 0 is the home cell, pairs i < j)
-  c->half = HalfStencil{};
-  for (const Row &rw : c->rows)
-    for (int dx = rw.dxlo; dx <= rw.dxhi; dx++) {
-      const bool keep = rw.dz > 0 || (rw.dz == 0 && rw.dy > 0) ||
-                        (rw.dz == 0 && rw.dy == 0 && dx >= 0);
-      if (!keep) continue;
-      if (c->half.ncells >= kMaxHalfCells || std::abs(dx) > 8 || std::abs(rw.dy) > 8 ||
-          std::abs(rw.dz) > 8)
-        return fail(c, PMB200_EUNSUPPORTED, "neighbour stencil too large (cell size too small)");
-      c->half.off[c->half.ncells++] =
-          (unsigned short)((dx + 8) | ((rw.dy + 8) << 5) | ((rw.dz + 8) << 10));
-    }
-  // Fixed pseudo-random order: consecutive cells of a warp's share then lie
-  // in different directions, so each staged batch holds a similar number of
-  // in-range partners for every i atom and the per-lane lists stay balanced.
-  {
-    unsigned long long x = 0x9E3779B97F4A7C15ull;
-    for (int k = c->half.ncells - 1; k > 0; k--) {
-      x = x * 6364136223846793005ull + 1442695040888963407ull;
-      const int r = (int)((x >> 33) % (unsigned long long)(k + 1));
-      std::swap(c->half.off[k], c->half.off[r]);
-    }
-  }
   if (c->ncell_alloc < g.ncell) {
     CK(dalloc(c->d_count, (size_t)g.ncell));
     CK(cudaMemset(c->d_count, 0, sizeof(int) * (size_t)g.ncell));
@@ -972,6 +1046,7 @@ int pmb200_set_box(pmb200_ctx *c, const double e1[3], const double e2[3], const 
   // PeriodicBoundaryConditions::set, orthogonal case (min/max corners,
   // myH, myH2, reciprocal basis, myD), for the molecule-centre image
   PbcRef &b = c->pb;
+  b = PbcRef{};
   for (int a = 0; a < 3; a++) {
     const double lo = origin[a] - L[a] * 0.5, hi = origin[a] + L[a] * 0.5;
     b.e[a] = L[a];
@@ -983,6 +1058,14 @@ int pmb200_set_box(pmb200_ctx *c, const double e1[3], const double e2[3], const 
   b.er[2] = (L[0] * L[1]) / (L[2] * (L[0] * L[1]));
   b.d = std::min((L[0] * 0.5) * (L[0] * 0.5),
                  std::min((L[1] * 0.5) * (L[1] * 0.5), (L[2] * 0.5) * (L[2] * 0.5)));
+  if (!ortho) {  // the general branch of minimalDifference
+    b.tric = 1;
+    for (int k = 0; k < 3; k++)
+      for (int a = 0; a < 3; a++) {
+        b.ev[3 * k + a] = ev[k][a];
+        b.erv[3 * k + a] = er[k][a];
+      }
+  }
   if (c->vacuum) b.d = std::numeric_limits<double>::infinity();  // no images
   c->have_box = true;
   if (c->have_topo) return upload_lj(c);
@@ -2306,6 +2389,7 @@ int pmb200_batch_create(pmb200_ctx *const *systems, int nsys, pmb200_batch **out
     if (!c->have_topo || !c->have_box) return PMB200_ESTATE;
     if (c->p.precision != PMB200_MIXED) return PMB200_EUNSUPPORTED;
     if (c->ntypes > kMaxTypes) return PMB200_EUNSUPPORTED;  // tables staged in shared memory
+    if (c->g.tric) return PMB200_EUNSUPPORTED;  // the batch bins orthogonal boxes only
     if (c->form != systems[0]->form || c->p.device != systems[0]->p.device)
       return PMB200_EINVAL;
   }

@@ -22,7 +22,7 @@
 
 namespace pmb200 {
 
-constexpr int kMaxRows = 64;          // stencil rows (dy, dz), passed by value
+constexpr int kMaxRows = 128;         // stencil rows (dy, dz), passed by value
 constexpr int kMaxTypes = 16;         // LJ types held in shared memory
 constexpr int kMaxTypesTable = 1024;  // LJ types of a context (more than kMaxTypes:
                                       // the mixed kernel reads the table through L1)
@@ -50,13 +50,39 @@ struct Row {        // one (dy, dz) row of the neighbour-cell stencil
 
 struct GridParams {
   int nx, ny, nz, ncell;
-  double edge[3];    // cell edges (A)
+  double edge[3];    // cell edges (A); general cells: the cells' widths
   double boxmin[3];  // lower box corner
   double boxlen[3];  // box edges
-  double unit;       // cell-unit length scale (= edge[0])
+  double unit;       // cell-unit length scale (= edge[0]; general cells: the smallest width)
   int nrows;
   int periodic;      // 1: periodic box (wrap, minimum image); 0: vacuum domain
+  // General (non-orthogonal) periodic cell: the grid is n_k cells along each
+  // basis vector e_k; an atom is binned by its fractional coordinates and
+  // stored as its Cartesian offset from its cell's lattice corner, so the
+  // pair kernels see Cartesian differences as for an orthogonal box and only
+  // the shift of a neighbour cell (a lattice vector) changes.
+  int tric;          // 1: general basis (the fields below)
+  double org[3];     // box centre (PeriodicBoundaryConditions origin)
+  double lat[9];     // rows: n_k times the reciprocal vector e_k^r (lattice coordinates)
+  double ec[9];      // ec[3 r + k] = component r of e_k / n_k (a cell's edge vectors, A)
+  double m[9];       // ec / unit: the shift of a cell offset in cell units
 };
+
+// Cartesian shift (A when `mat` is ec, cell units when it is m) of the cell
+// offset (dx, dy, dz): for an orthogonal grid (dx edge0, dy edge1, dz edge2).
+__host__ __device__ __forceinline__ void cell_shift(const GridParams &g, const double *mat,
+                                                   double scale, int dx, int dy, int dz,
+                                                   double &sx, double &sy, double &sz) {
+  if (g.tric) {
+    sx = mat[0] * dx + mat[1] * dy + mat[2] * dz;
+    sy = mat[3] * dx + mat[4] * dy + mat[5] * dz;
+    sz = mat[6] * dx + mat[7] * dy + mat[8] * dz;
+  } else {
+    sx = dx * g.edge[0] * scale;
+    sy = dy * g.edge[1] * scale;
+    sz = dz * g.edge[2] * scale;
+  }
+}
 
 // PeriodicBoundaryConditions constants for minimalDifference
 // (protomol/src/protomol/topology/PeriodicBoundaryConditions.cpp:32-77,
@@ -64,11 +90,25 @@ struct GridParams {
 // molecular virial.
 struct PbcRef {
   double e[3], er[3], h[3], h2[3], d;
+  int tric;                 // general basis: the vectors below
+  double ev[9], erv[9];     // rows: e1, e2, e3 and e1r, e2r, e3r
 };
 
-// PeriodicBoundaryConditions::minimalDifference, orthogonal branch
-// (protomol/src/protomol/topology/PeriodicBoundaryConditions.h:53-70).
+// PeriodicBoundaryConditions::minimalDifference
+// (protomol/src/protomol/topology/PeriodicBoundaryConditions.h:53-70, and the
+// general branch 62-67: diff -= e1 rint(e1r.diff) + e2 rint(e2r.diff) +
+// e3 rint(e3r.diff)).
 __device__ __forceinline__ void ref_min_image(const PbcRef &b, double v[3]) {
+  if (b.tric) {
+    double k[3];
+    for (int a = 0; a < 3; a++)
+      k[a] = rint(b.erv[3 * a] * v[0] + b.erv[3 * a + 1] * v[1] + b.erv[3 * a + 2] * v[2]);
+    double w[3];
+    for (int c = 0; c < 3; c++)
+      w[c] = b.ev[c] * k[0] + b.ev[3 + c] * k[1] + b.ev[6 + c] * k[2];
+    for (int c = 0; c < 3; c++) v[c] -= w[c];
+    return;
+  }
   if (v[0] * v[0] + v[1] * v[1] + v[2] * v[2] > b.d) {
     for (int k = 0; k < 3; k++) {
       if (v[k] < -b.h2[k]) v[k] += b.h[k];
@@ -229,6 +269,28 @@ __device__ __forceinline__ bool locate_cell(const double *xin, const GridParams 
                                             double r[3]) {
   const int nd[3] = {g.nx, g.ny, g.nz};
   bool ok = true;
+  if (g.tric) {
+    // lattice coordinates t_k = n_k (e_k^r . (x - origin) + 1/2), wrapped
+    // into [0, n_k); the offset from the cell's lattice corner, in A
+    double x[3];
+    for (int a = 0; a < 3; a++) {
+      x[a] = xin[a] - g.org[a];
+      if (!isfinite(xin[a])) { ok = false; x[a] = 0.0; }
+    }
+    double u[3];
+    for (int k = 0; k < 3; k++) {
+      double t = g.lat[3 * k] * x[0] + g.lat[3 * k + 1] * x[1] + g.lat[3 * k + 2] * x[2] +
+                 0.5 * nd[k];
+      t -= nd[k] * floor(t / nd[k]);
+      int ck = (int)floor(t);
+      ck = ck < 0 ? 0 : (ck >= nd[k] ? nd[k] - 1 : ck);
+      c[k] = ck;
+      u[k] = t - ck;
+    }
+    for (int a = 0; a < 3; a++)
+      r[a] = g.ec[3 * a] * u[0] + g.ec[3 * a + 1] * u[1] + g.ec[3 * a + 2] * u[2];
+    return ok;
+  }
   for (int a = 0; a < 3; a++) {
     double x = xin[a];
     if (!isfinite(x)) { ok = false; x = g.boxmin[a]; }
@@ -926,6 +988,7 @@ __device__ __forceinline__ void mixed_task(
       const int myq = g0 + lane;
       int cjs = 0, ccnt = 0;
       float csx = 0.f, csy = 0.f, csz = 0.f;
+      double dsx = 0.0, dsy = 0.0, dsz = 0.0;  // the same shift in FP64 (energies)
       bool chome = false;
       if (myq < nmine) {
         const unsigned o = st_off[first + myq * stride];
@@ -948,7 +1011,14 @@ __device__ __forceinline__ void mixed_task(
           cjs = start[jc];
           ccnt = start[jc + 1] - cjs;
         }
-        csx = (float)dx; csy = (float)dy * mc.ey; csz = (float)dz * mc.ez;
+        if (g.tric) {
+          // a lattice vector: rounded to FP32 once per cell offset
+          cell_shift(g, g.m, 1.0, dx, dy, dz, dsx, dsy, dsz);
+          csx = (float)dsx; csy = (float)dsy; csz = (float)dsz;
+        } else {
+          csx = (float)dx; csy = (float)dy * mc.ey; csz = (float)dz * mc.ez;
+          dsx = csx; dsy = csy; dsz = csz;
+        }
       }
       int incl = ccnt;  // inclusive prefix of the cells' atom counts
       for (int off = 1; off < 32; off <<= 1) {
@@ -982,6 +1052,12 @@ __device__ __forceinline__ void mixed_task(
         const float sx = __shfl_sync(0xffffffffu, csx, c);
         const float sy = __shfl_sync(0xffffffffu, csy, c);
         const float sz = __shfl_sync(0xffffffffu, csz, c);
+        double dshx = sx, dshy = sy, dshz = sz;  // (the FP32 shift is exact unless triclinic)
+        if (kExactE && g.tric) {
+          dshx = __shfl_sync(0xffffffffu, dsx, c);
+          dshy = __shfl_sync(0xffffffffu, dsy, c);
+          dshz = __shfl_sync(0xffffffffu, dsz, c);
+        }
         const bool home_atom = hmask && f >= h_excl && f < h_excl + h_cnt;
         bool keep = false;
         float4 a = make_float4(0.f, 0.f, 0.f, 0.f), p = a;
@@ -1007,9 +1083,9 @@ __device__ __forceinline__ void mixed_task(
           sm.gidx[slot] = jg;
           if (kExactE) {  // coordinate, residual and shift added in FP64
             const float4 lj = spos_lo[jg];
-            pdx[slot] = ((double)a.x + (double)lj.x) + (double)sx;
-            pdy[slot] = ((double)a.y + (double)lj.y) + (double)sy;
-            pdz[slot] = ((double)a.z + (double)lj.z) + (double)sz;
+            pdx[slot] = ((double)a.x + (double)lj.x) + dshx;
+            pdy[slot] = ((double)a.y + (double)lj.y) + dshy;
+            pdz[slot] = ((double)a.z + (double)lj.z) + dshz;
           }
         }
         const unsigned hm = __ballot_sync(0xffffffffu, keep && home_atom);
@@ -1209,14 +1285,14 @@ k_pair_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes, const dou
       while (jz < 0) jz += g.nz;
       while (jz >= g.nz) jz -= g.nz;
       const int rowbase = (jz * g.ny + jy) * g.nx;
-      const double sy = row.dy * g.edge[1], sz = row.dz * g.edge[2];
       for (int dx = row.dxlo; dx <= row.dxhi; dx++) {
         int jx = cx + dx;
         if (!g.periodic && (jx < 0 || jx >= g.nx)) continue;
         jx += jx < 0 ? g.nx : (jx >= g.nx ? -g.nx : 0);  // |dx| <= n / 2: one wrap
         const int jc = rowbase + jx;
         const int js = start[jc], je = start[jc + 1];
-        const double sx = dx * g.edge[0];
+        double sx, sy, sz;  // the neighbour cell's shift (A)
+        cell_shift(g, g.ec, 1.0, dx, row.dy, row.dz, sx, sy, sz);
         for (int j = js + sub; j < je; j += L) {
           const double4 pj = spos[j];
           const double ddx = (pj.x + sx) - pi.x;
@@ -1447,14 +1523,14 @@ k_deriv_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes,
         while (jz < 0) jz += g.nz;
         while (jz >= g.nz) jz -= g.nz;
         const int rowbase = (jz * g.ny + jy) * g.nx;
-        const double sy = row.dy * g.edge[1], sz = row.dz * g.edge[2];
         for (int dx = row.dxlo; dx <= row.dxhi; dx++) {
           int jx = cx + dx;
           if (!g.periodic && (jx < 0 || jx >= g.nx)) continue;
           jx += jx < 0 ? g.nx : (jx >= g.nx ? -g.nx : 0);  // |dx| <= n / 2: one wrap
           const int jc = rowbase + jx;
           const int js = start[jc], je = start[jc + 1];
-          const double sx = dx * g.edge[0];
+          double sx, sy, sz;  // the neighbour cell's shift (A)
+          cell_shift(g, g.ec, 1.0, dx, row.dy, row.dz, sx, sy, sz);
           for (int j = js + sub; j < je; j += L) {
             const double4 pj = spos[j];
             const double ddx = (pj.x + sx) - pi.x;

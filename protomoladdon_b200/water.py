@@ -207,6 +207,28 @@ def many_types(sysd, n_o_types=14, n_h_types=10, n_unused=6, seed=7):
     return d
 
 
+def sheared(sysd, sxy=0.3, sxz=0.0, syz=0.0):
+    """The box made a general periodic cell by shear: basis e1 = (L, 0, 0),
+    e2 = (sxy L, L, 0), e3 = (sxz L, syz L, L) (rows of the 3x3 "box"); each
+    molecule moves rigidly with the shear of its first atom, so the geometry
+    and the density stay the water box's.  The origin is the cell's centre."""
+    d = dict(sysd)
+    L = float(np.asarray(sysd["box"])[0])
+    mol = np.asarray(sysd["mol"])
+    pos = np.array(sysd["pos"], dtype=np.float64)
+    first = np.full(mol.max() + 1, -1)
+    for i in range(len(mol) - 1, -1, -1):
+        first[mol[i]] = i
+    a = pos[first[mol]]
+    pos[:, 0] += sxy * a[:, 1] + sxz * a[:, 2]
+    pos[:, 1] += syz * a[:, 2]
+    e = np.array([[L, 0.0, 0.0], [sxy * L, L, 0.0], [sxz * L, syz * L, L]])
+    d["pos"] = pos
+    d["box"] = e
+    d["origin"] = 0.5 * e.sum(0)
+    return d
+
+
 # Named workloads (sizes from the reference-facing benchmark definitions).
 def small_648(seed=1234):
     """216 waters, 6^3 lattice, box 18.624 A, rc 8, C2 from 7."""

@@ -112,6 +112,20 @@ def main(ref_root):
     print("wrote fixtures to", HERE)
 
 
+def triclinic_fixture():
+    """A sheared 9^3 water box (2,187 atoms; e2 = (0.3 L, L, 0), e3 =
+    (0.1 L, -0.2 L, L)), rc 6, C2 from 5, with the reference's pair function
+    over all pairs at its minimal image (NonbondedSimpleFullSystemForce).  Its
+    cell-list force is not used: on general cells it misses pairs across the
+    sheared faces, and on this box it stops on an array-bounds assertion."""
+    t = water.sheared(water.water_box(9, rc=6.0, ron=5.0, seed=17), 0.3, 0.1, -0.2)
+    R = O.RefForce(t)
+    f, e, v, mv = R.evaluate_allpairs(t["pos"], 2)
+    np.savez_compressed(os.path.join(HERE, "triclinic_ref.npz"), **sysd_arrays(t),
+                        ref_forces=f, ref_energies=e, ref_virial=v, ref_molvirial=mv)
+    R.close()
+
+
 def many_types_fixture():
     """The 648-atom box over 30 LJ types (24 used) with the H-H pair of each
     water modified (A14/B14, Coulomb scaling 0.5) and O-H fully excluded."""
@@ -245,3 +259,5 @@ if __name__ == "__main__":
         vacuum_fixture()
     if "--manytypes-only" in only:
         many_types_fixture()
+    if not only or "--triclinic-only" in only:
+        triclinic_fixture()

@@ -217,3 +217,23 @@ def test_restatement_bitexact_vs_many_types_fixture():
     f, e, v, mv = O.restate_eval(d, d["pos"], 2)
     assert np.array_equal(f, d["ref_forces"]) and np.array_equal(e, d["ref_energies"])
     assert np.array_equal(v, d["ref_virial"]) and np.array_equal(mv, d["ref_molvirial"])
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference oracle library not built")
+def test_triclinic_fixture_is_the_reference_all_pairs_force():
+    """The committed general-cell fixture equals a fresh evaluation of the
+    reference's all-pairs force, and on an orthogonal box that force equals
+    the reference's cell-list force (to summation order)."""
+    from tests.conftest import load_fixture
+    d = load_fixture("triclinic_ref.npz")
+    R = O.RefForce(d)
+    f, e, v, mv = R.evaluate_allpairs(d["pos"], 2)
+    R.close()
+    assert np.array_equal(f, d["ref_forces"]) and np.array_equal(e, d["ref_energies"])
+    s = water.water_box(6, rc=8.0, ron=7.0, seed=3)
+    R = O.RefForce(s)
+    f1, e1, _, _ = R.evaluate(s["pos"], 1)
+    f2, e2, _, _ = R.evaluate_allpairs(s["pos"], 1)
+    R.close()
+    assert np.abs(f1 - f2).max() <= 1e-12 * np.abs(f1).max()
+    assert np.allclose(e1, e2, rtol=1e-13)
