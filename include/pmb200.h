@@ -100,7 +100,13 @@ int pmb200_set_topology(pmb200_ctx *ctx, int n, const int *type,
 
 /* Periodic cell (replaces PeriodicBoundaryConditions::set,
  * protomol/src/protomol/topology/PeriodicBoundaryConditions.cpp:32-77).
- * Only orthogonal boxes; every edge must be >= 2 * max switch cutoff. */
+ * Any basis e1, e2, e3 (origin = the cell's centre).  Orthogonal boxes: every
+ * edge >= 2 * max switch cutoff.  General cells: pairs are taken at the
+ * reference's minimal image (PeriodicBoundaryConditions.h:62-67: fractional
+ * differences rounded to the nearest lattice vector); the distance between
+ * opposite faces must be about 3 cutoffs or more (each axis must hold
+ * 2 ceil(rc / cell width) + 1 cells of at least rc / 4; PMB200_EUNSUPPORTED
+ * otherwise).  Batches take orthogonal boxes only. */
 int pmb200_set_box(pmb200_ctx *ctx, const double e1[3], const double e2[3],
                    const double e3[3], const double origin[3]);
 

@@ -14,8 +14,9 @@ stops on an array-bounds assertion.
 
 Tolerances (written here, checked below): FP64 kernel forces RMS relative
 <= 1e-12, energies relative <= 1e-11, virials <= 1e-11 relative; mixed
-kernel forces RMS relative <= 1e-5, energies within 2e-3 kcal/mol (1e-6 of
-the summed pair magnitudes on this 2,187-atom box), virials <= 1e-5.
+kernel forces RMS relative <= 1e-5, LJ + C1 energies within 2e-3 kcal/mol
+(1e-6 of the summed pair magnitudes on this 2,187-atom box), the Ewald
+term's energy within 1e-6 of its summed pair magnitudes, virials <= 1e-5.
 """
 import numpy as np
 import pytest
@@ -100,6 +101,7 @@ def _ewald_brute(d, alpha, rc):
     n = len(q)
     F = np.zeros_like(pos)
     E = 0.0
+    A = 0.0  # sum of the pair energies' magnitudes
     for i in range(n - 1):
         dv = pos[i + 1:] - pos[i]
         dv -= np.rint(dv @ er) @ e
@@ -111,11 +113,12 @@ def _ewald_brute(d, alpha, rc):
         qq = q[i] * q[js[m]]
         g = erfc(alpha * r) / r
         E += (qq * g).sum()
+        A += np.abs(qq * g).sum()
         fr = qq * (g + 2 * alpha / np.sqrt(np.pi) * np.exp(-(alpha * r) ** 2)) / r2[m]
         fv = dv[m] * fr[:, None]
         F[i] -= fv.sum(0)
         np.add.at(F, js[m], fv)
-    return F, E
+    return F, E, A
 
 
 @pytest.mark.parametrize("precision", ["mixed", "fp64"])
@@ -123,15 +126,19 @@ def test_ewald_real_term_on_a_general_cell(tric, precision):
     d = tric
     alpha = 0.45
     acc = float(np.exp(-(alpha * 6.0) ** 2))  # rc = 6 A
-    f = EwaldRealB200SystemForce(alpha, acc, precision=precision)
+    # erfc itself (the reference's -DUSE_EWALD_EXACT_ERF build), as in the
+    # brute force below
+    f = EwaldRealB200SystemForce(alpha, acc, precision=precision, erfc="exact")
     F = np.zeros_like(d["pos"])
     E = ScalarStructure()
     f.evaluate(PeriodicTopology.from_dict(d), d["pos"], F, E)
     f.close()
-    Fb, Eb = _ewald_brute(d, alpha, 6.0)
+    Fb, Eb, Ab = _ewald_brute(d, alpha, 6.0)
     tol = 1e-12 if precision == "fp64" else 1e-5
     assert rms_rel(F, Fb) <= tol
-    assert abs(E[0] - Eb) <= (1e-10 * abs(Eb) + 1e-9 if precision == "fp64" else 2e-3)
+    # the mixed Ewald energy is judged on the summed pair magnitudes, as on
+    # the orthogonal boxes (tests/test_ewald_gpu.py)
+    assert abs(E[0] - Eb) <= (1e-10 * abs(Eb) + 1e-9 if precision == "fp64" else 1e-6 * Ab)
 
 
 def test_large_sheared_box_mixed_against_fp64():
@@ -147,8 +154,14 @@ def test_large_sheared_box_mixed_against_fp64():
 
 
 def test_too_narrow_a_general_cell_is_refused(tric):
+    """Widths of 12.6-13.4 A for a 6 A cutoff: wider than twice the cutoff,
+    but 6 cells of ~2.1 A per axis cannot hold 3 cells on each side of a
+    cell plus the cell itself, so the set-up refuses the box (before any
+    evaluation: the positions are not rescaled)."""
     d = dict(tric)
-    d["box"] = np.asarray(d["box"]) * 0.55  # widths ~15 A for a 6 A cutoff
+    d["box"] = np.asarray(d["box"]) * 0.48
+    w = 1.0 / np.linalg.norm(np.linalg.inv(d["box"]).T, axis=1)
+    assert (w > 2 * d["rc_lj"]).all() and (w < 2.5 * d["rc_lj"]).all()
     with pytest.raises(PmbError) as ei:
         run(d, "mixed")
     assert ei.value.code == _lib.PMB200_EUNSUPPORTED
