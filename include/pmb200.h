@@ -304,12 +304,26 @@ int pmb200_grid(const pmb200_ctx *ctx, int dims[3], double edge[3]);
  * equal to the cutoff, as CnSwitchingFunction::make requires;
  * ComplimentCnCn: 0 <= switchon < switchoff <= cutoff, as
  * CmpCnCnSwitchingFunction::make requires).
- * Energies: LENNARDJONES and COULOMB as for the first kind. */
+ * Energies: LENNARDJONES and COULOMB as for the first kind.
+ *
+ * Tabulated LJ: lj_switch = PMB200_SW_TABLE | S (S = C2, Cn or
+ * ComplimentCnCn) with coulomb_switch = PMB200_SW_NONE stands for
+ * OneAtomPair<BC, UniversalSwitchingFunction, LennardJonesTableForce<S, 7,
+ * Real>> (NonbondedCutoffForceModule.cpp:67-72 periodic, 121-126 vacuum;
+ * .../force/table/LennardJonesTableForce.h, LookupTable.h): the switched LJ
+ * potential tabulated over r^2 from 1/16 A^2 with 128 cubic Hermite
+ * intervals per octave, pairs beyond the switch's cutoff skipped and no
+ * further switch applied.  The FP64 kernel reads that table (built from the
+ * same recipe at creation); the mixed kernel evaluates the switched LJ the
+ * table approximates (the table's own interpolation error is below 2e-6 of
+ * the force and 3e-8 of the energy, measured over r^2 in [2, 64] A^2).
+ * Other combinations with PMB200_SW_TABLE: PMB200_EUNSUPPORTED. */
 #define PMB200_SW_NONE 0
 #define PMB200_SW_C1 1
 #define PMB200_SW_C2 2
 #define PMB200_SW_CN 3
 #define PMB200_SW_CMPCNCN 4  /* ComplimentCnCn (CmpCnCnSwitchingFunction) */
+#define PMB200_SW_TABLE 16   /* flag on lj_switch: LennardJonesTableForce */
 
 typedef struct {
   int precision;       /* PMB200_MIXED or PMB200_FP64 */

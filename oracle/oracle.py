@@ -335,11 +335,13 @@ class RefForce:
 
     SWITCH_KINDS = {None: 0, "C1": 1, "C2": 2, "Cn": 3, "ComplimentCnCn": 4}
 
-    def pair_eval(self, pos, lj, coulomb, rc_alg, virial_mode=2):
+    def pair_eval(self, pos, lj, coulomb, rc_alg, virial_mode=2, lj_table=False):
         """The reference's NonbondedCutoffSystemForce with OneAtomPair /
         OneAtomPairTwo and the given switches: lj / coulomb are None or
         (kind, switchon, cutoff, order, switchoff) with kind C1, C2, Cn or
-        ComplimentCnCn.
+        ComplimentCnCn.  lj_table: OneAtomPair<PBC, Universal,
+        LennardJonesTableForce<S, 7, Real>> with S = lj's switch (C2, Cn or
+        ComplimentCnCn; no Coulomb term).
         Returns (forces, energies (coulomb, lj), virial, molvirial)."""
         def spec(x):
             if x is None:
@@ -347,6 +349,8 @@ class RefForce:
             return self.SWITCH_KINDS[x[0]], np.asarray(x[1:5], dtype=np.float64)
         kl, pl = spec(lj)
         kc, pc = spec(coulomb)
+        if lj_table:
+            kl |= 16
         p = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1)
         f = np.zeros(p.size)
         e = np.zeros(2)
@@ -409,6 +413,33 @@ def ref_vacuum_eval(sysd, pos, virial_mode=2):
                           float(sysd["ron"]), float(sysd["rc_lj"]), float(sysd["rc_coul"]),
                           float(sysd["rc_alg"]), _ptr(p), _ptr(f), _ptr(e), _ptr(v), _ptr(mv),
                           int(virial_mode))
+    return f.reshape(-1, 3), e, v, mv
+
+
+def ref_vacuum_table_eval(sysd, pos, lj, rc_alg, virial_mode=2):
+    """The reference's vacuum tabulated LJ (OneAtomPair<VacuumBoundary
+    Conditions, Universal, LennardJonesTableForce<S, 7, Real>>), lj = (kind,
+    switchon, cutoff, order, switchoff) with kind C2, Cn or ComplimentCnCn:
+    (forces, energies (coulomb, lj), virial, molvirial)."""
+    lib = ref_lib()
+    lib.pmref_vacuum_table_eval.argtypes = [_I, _P, _P, _P, _P, _I, _P, _I, _P, _D, _D, _I, _P,
+                                            _D, _P, _P, _P, _P, _P, _I]
+    lib.pmref_vacuum_table_eval.restype = _I
+    ar = _Arrays(sysd)
+    p = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1)
+    sp = np.asarray(lj[1:5], dtype=np.float64)
+    f = np.zeros(p.size)
+    e = np.zeros(2)
+    v = np.zeros(9)
+    mv = np.zeros(9)
+    rc = lib.pmref_vacuum_table_eval(ar.n, _ptr(ar.type), _ptr(ar.q), _ptr(ar.mol), _ptr(ar.mass),
+                                     ar.ntypes, _ptr(ar.lj), ar.nexcl, _ptr(ar.excl),
+                                     float(sysd.get("coulomb_scaling", 1.0)),
+                                     float(sysd["cellsize"]), RefForce.SWITCH_KINDS[lj[0]],
+                                     _ptr(sp), float(rc_alg), _ptr(p), _ptr(f), _ptr(e), _ptr(v),
+                                     _ptr(mv), int(virial_mode))
+    if rc:
+        raise RuntimeError("pmref_vacuum_table_eval failed")
     return f.reshape(-1, 3), e, v, mv
 
 

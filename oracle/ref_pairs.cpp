@@ -2,7 +2,8 @@
 // registrations (protomol/src/protomol/module/NonbondedCutoffForceModule.cpp:
 // 53-82) -- NonbondedCutoffSystemForce<CubicCellManager, P> with
 //   P = OneAtomPair<PBC, S, LennardJonesForce>, OneAtomPair<PBC, S, CoulombForce>,
-//       OneAtomPairTwo<PBC, S1, LennardJonesForce, S2, CoulombForce>
+//       OneAtomPairTwo<PBC, S1, LennardJonesForce, S2, CoulombForce>,
+//       OneAtomPair<PBC, UniversalSwitchingFunction, LennardJonesTableForce<S, 7, Real>>
 // and S, S1, S2 among C1, C2, Cn and ComplimentCnCn -- evaluated on the topology pmref_create
 // built.  Nothing in the product links this.
 #include <protomol/force/nonbonded/NonbondedCutoffSystemForce.h>
@@ -10,6 +11,8 @@
 #include <protomol/force/OneAtomPairTwo.h>
 #include <protomol/force/LennardJonesForce.h>
 #include <protomol/force/CoulombForce.h>
+#include <protomol/force/table/LennardJonesTableForce.h>
+#include <protomol/switch/UniversalSwitchingFunction.h>
 #include <protomol/switch/C1SwitchingFunction.h>
 #include <protomol/switch/C2SwitchingFunction.h>
 #include <protomol/switch/CnSwitchingFunction.h>
@@ -91,6 +94,13 @@ SystemForce *two(const double *p1, const double *p2, double rc) {
   return new NonbondedCutoffSystemForce<CubicCellManager, P>(
       rc, P(LennardJonesForce(), sw((S1 *)0, p1), CoulombForce(), sw((S2 *)0, p2)));
 }
+template <class S>
+SystemForce *table_lj(const double *p, double rc) {
+  typedef LennardJonesTableForce<S, 7, Real> T;
+  typedef OneAtomPair<PBC, UniversalSwitchingFunction, T> P;
+  return new NonbondedCutoffSystemForce<CubicCellManager, P>(
+      rc, P(T(sw((S *)0, p)), UniversalSwitchingFunction()));
+}
 template <class S1>
 SystemForce *two_any(int k2, const double *p1, const double *p2, double rc) {
   if (k2 == 1) return two<S1, C1SwitchingFunction>(p1, p2, rc);
@@ -106,7 +116,8 @@ extern "C" {
 void *pmref_topology(void *h);
 
 // lj_kind / coul_kind: 0 none, 1 C1, 2 C2, 3 Cn, 4 ComplimentCnCn (at least
-// one non-zero);
+// one non-zero); lj_kind 16 + S: the tabulated LJ with switch S (2, 3, 4),
+// alone;
 // forces accumulated into; energies {COULOMB, LENNARDJONES}; mode 0/1/2 as
 // pmref_eval.  Returns 0, or 1 for an unknown kind.
 int pmref_pair_eval(void *h, int lj_kind, const double *ljp, int coul_kind, const double *cop,
@@ -115,7 +126,12 @@ int pmref_pair_eval(void *h, int lj_kind, const double *ljp, int coul_kind, cons
   Report::report << Report::reportlevel(-4);
   PTopo *t = (PTopo *)pmref_topology(h);
   SystemForce *f = 0;
-  if (lj_kind && coul_kind) {
+  if (lj_kind & 16) {
+    if (coul_kind) return 1;
+    if (lj_kind == 18) f = table_lj<C2SwitchingFunction>(ljp, rc_alg);
+    else if (lj_kind == 19) f = table_lj<CnSwitchingFunction>(ljp, rc_alg);
+    else if (lj_kind == 20) f = table_lj<CmpCnCnSwitchingFunction>(ljp, rc_alg);
+  } else if (lj_kind && coul_kind) {
     if (lj_kind == 1) f = two_any<C1SwitchingFunction>(coul_kind, ljp, cop, rc_alg);
     else if (lj_kind == 2) f = two_any<C2SwitchingFunction>(coul_kind, ljp, cop, rc_alg);
     else if (lj_kind == 4) f = two_any<CmpCnCnSwitchingFunction>(coul_kind, ljp, cop, rc_alg);

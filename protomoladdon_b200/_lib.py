@@ -32,6 +32,7 @@ PMB200_SW_C1 = 1
 PMB200_SW_C2 = 2
 PMB200_SW_CN = 3
 PMB200_SW_CMPCNCN = 4
+PMB200_SW_TABLE = 16  # flag on the LJ switch: LennardJonesTableForce
 
 PMB200_ERFC_POLY5 = 0
 PMB200_ERFC_EXACT = 1

@@ -40,6 +40,10 @@ struct pmb200_ctx {
   // potential (LJ, Coulomb)
   int sw_kind[2] = {0, 0};
   double sw_par[2][4] = {};
+  // tabulated LJ (LennardJonesTableForce under UniversalSwitchingFunction):
+  // the FP64 grid on the device (null: analytic LJ)
+  double4 *d_ljtab = nullptr;
+  int tab_first = 0, tab_last = 0;
   // vacuum boundaries: the box is only the cell domain (no wrap, no images)
   bool vacuum = false, vacuum_pending = false;
   // the box as last given (re-applied when an Ewald default alpha changes)
@@ -257,6 +261,77 @@ SwitchSpec<T> make_switch(int kind, const double par[4], double u) {
     w.dpeak = (T)kCnDeriv[n - 2][0];
   }
   return w;
+}
+
+// The grid of LennardJonesTableForce<S, 7, double>(swf): LookupTable's
+// construction (protomol/src/protomol/force/table/LookupTable.h:71-158) with
+// LennardJonesLookupValues::assign (LennardJonesTableForce.h:24-34).  Grid
+// points run over r^2 from lowerboundExp2(0.1) = 1/16, 128 per octave, up to
+// the octave holding the switch's cutoff^2; point p holds, for the switched
+// r^-12 part (A) and the switched -r^-6 part (B), the value, its derivative
+// in r^2 and the cubic Hermite coefficients c, d of the interval starting at
+// p (refined twice against the next point, as the reference does).  Output:
+// two double4 per point ({v, g, c, d} of A, then of B); first = the biased
+// exponent-and-top-mantissa hash of 1/16; last = the final point's index.
+void build_lj_table(const SwitchSpec<double> &w, std::vector<double4> &tab, int &first,
+                    int &last) {
+  auto bits = [](double x) {
+    long long b;
+    std::memcpy(&b, &x, sizeof b);
+    return b;
+  };
+  auto lb2 = [](double r) {  // MathUtilities.cpp:52-61
+    double res = 1.0;
+    while (res < r) res *= 2.0;
+    while (res > r) res /= 2.0;
+    return res;
+  };
+  constexpr int kN = 1 << kTabPre;
+  const double lo = lb2(0.1);
+  const int octaves = (int)((bits(lb2(w.rc2)) >> 52) + 1 - (bits(lo) >> 52));
+  const int npt = octaves * kN + 1;
+  first = (int)(bits(lo) >> kTabShift);
+  last = octaves * kN;
+  std::vector<double> t((size_t)8 * npt, 0.0);
+  for (int i = 0; i < npt; i++) {
+    const double base = lo * (double)(1 << (i / kN));
+    const double del = base / (double)kN;
+    const double r = base + del * (double)(i % kN);
+    const double r1 = std::sqrt(r);
+    double v, d;
+    switch_eval(w, r, 1.0 / r1, v, d);
+    // powers of 1/r1 by squaring, in the order MathUtilities.h:79-90 uses
+    const double ip = 1.0 / r1;
+    const double p3 = (ip * ip) * ip, p6 = p3 * p3, p4 = (ip * ip) * (ip * ip);
+    const double p7 = p6 * ip;
+    double *e = &t[(size_t)8 * i];
+    double ev = p6 * p6, fv = 12.0 * (p7 * p7);
+    e[0] = ev * v;
+    e[1] = -0.5 * (fv * v - ev * d);
+    ev = -p6;
+    fv = -6.0 * (p4 * p4);
+    e[4] = ev * v;
+    e[5] = -0.5 * (fv * v - ev * d);
+    if (i == 0) continue;
+    const double x = lo * (double)(1 << ((i - 1) / kN)) / (double)kN;
+    double *pr = &t[(size_t)8 * (i - 1)];
+    for (int j = 0; j < 8; j += 4) {
+      const double v1 = pr[j], g1 = pr[j + 1], v2 = e[j], g2 = e[j + 1];
+      double c = (3.0 * (v2 - v1) - x * (2.0 * g1 + g2)) / (x * x);
+      double dd = (-2.0 * (v2 - v1) + x * (g1 + g2)) / (x * x * x);
+      for (int k = 0; k < 2; k++) {
+        const double dv = (v1 - v2) + ((dd * x + c) * x + g1) * x;
+        const double dg = (g1 - g2) + (3.0 * dd * x + 2.0 * c) * x;
+        c -= (3.0 * dv - x * dg) / (x * x);
+        dd -= (-2.0 * dv + x * dg) / (x * x * x);
+      }
+      pr[j + 2] = c;
+      pr[j + 3] = dd;
+    }
+  }
+  tab.resize((size_t)2 * npt);
+  for (int i = 0; i < 2 * npt; i++)
+    tab[i] = make_double4(t[4 * i], t[4 * i + 1], t[4 * i + 2], t[4 * i + 3]);
 }
 
 // NonbondedFullEwaldSystemForce::initialize
@@ -665,7 +740,17 @@ int pmb200_create_pair(const pmb200_pair_params *params, pmb200_ctx **out) {
   if (!params || !out) return PMB200_EINVAL;
   *out = nullptr;
   const pmb200_pair_params &q = *params;
-  const int kinds[2] = {q.lj_switch, q.coulomb_switch};
+  // LennardJonesTableForce<S, 7, Real> under UniversalSwitchingFunction: the
+  // reference registers it for S = C2, Cn, ComplimentCnCn and alone
+  // (NonbondedCutoffForceModule.cpp:67-72, 121-126)
+  const bool table = (q.lj_switch & PMB200_SW_TABLE) != 0;
+  if (table) {
+    const int s = q.lj_switch & ~PMB200_SW_TABLE;
+    if (q.coulomb_switch != PMB200_SW_NONE ||
+        (s != PMB200_SW_C2 && s != PMB200_SW_CN && s != PMB200_SW_CMPCNCN))
+      return PMB200_EUNSUPPORTED;
+  }
+  const int kinds[2] = {q.lj_switch & ~PMB200_SW_TABLE, q.coulomb_switch};
   const double *pars[2] = {q.lj, q.coulomb};
   double rcmax = 0.0;
   if (kinds[0] == PMB200_SW_NONE && kinds[1] == PMB200_SW_NONE) return PMB200_EINVAL;
@@ -723,6 +808,19 @@ int pmb200_create_pair(const pmb200_pair_params *params, pmb200_ctx **out) {
                                                : SW_OFF;
     for (int j = 0; j < 4; j++) c->sw_par[k][j] = pars[k][j];
   }
+  if (table) {
+    std::vector<double4> tab;
+    build_lj_table(make_switch<double>(c->sw_kind[0], c->sw_par[0], 1.0), tab, c->tab_first,
+                   c->tab_last);
+    const bool ok = cudaSetDevice(c->p.device) == cudaSuccess &&
+                    dalloc(c->d_ljtab, tab.size()) == cudaSuccess &&
+                    cudaMemcpy(c->d_ljtab, tab.data(), sizeof(double4) * tab.size(),
+                               cudaMemcpyHostToDevice) == cudaSuccess;
+    if (!ok) {
+      pmb200_destroy(c);
+      return PMB200_ECUDA;
+    }
+  }
   *out = c;
   return PMB200_OK;
 }
@@ -758,7 +856,7 @@ int pmb200_destroy(pmb200_ctx *c) {
   release_graph(c);
   dfree(c->d_type); dfree(c->d_mol); dfree(c->d_q); dfree(c->d_mass);
   dfree(c->d_ex_start); dfree(c->d_ex); dfree(c->d_mstart); dfree(c->d_matoms);
-  dfree(c->d_lj32); dfree(c->d_lj64);
+  dfree(c->d_lj32); dfree(c->d_lj64); dfree(c->d_ljtab);
   dfree(c->d_count); dfree(c->d_start); dfree(c->d_err); dfree(c->d_partial);
   dfree(c->d_cell_of); dfree(c->d_slot); dfree(c->d_tmp); dfree(c->d_sidx);
   dfree(c->d_rel32); dfree(c->d_spos32); dfree(c->d_rel_lo); dfree(c->d_spos_lo); dfree(c->d_rel64); dfree(c->d_spos64);
@@ -1040,6 +1138,9 @@ int pmb200_set_box(pmb200_ctx *c, const double e1[3], const double e2[3], const 
   f.csf = c->csf;
   f.swl = make_switch<double>(c->sw_kind[0], c->sw_par[0], 1.0);
   f.swc = make_switch<double>(c->sw_kind[1], c->sw_par[1], 1.0);
+  f.ljtab = c->d_ljtab;
+  f.tfirst = c->tab_first;
+  f.tlast = c->tab_last;
   f.ea = c->ew_alpha;
   f.ea2 = c->ew_alpha * c->ew_alpha;
   f.ea2pi = 2.0 * c->ew_alpha / std::sqrt(M_PI);

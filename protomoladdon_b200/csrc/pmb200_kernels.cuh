@@ -154,7 +154,8 @@ struct SwitchSpec {
 // falling form, which is the rising one by the polynomial's symmetry) and
 // falling on (switchoff, cutoff].
 template <class T>
-__device__ __forceinline__ void switch_eval(const SwitchSpec<T> &w, T r2, T rinv, T &S, T &dS) {
+__host__ __device__ __forceinline__ void switch_eval(const SwitchSpec<T> &w, T r2, T rinv, T &S,
+                                                    T &dS) {
   S = T(0);
   dS = T(0);
   if (r2 > w.rc2) return;
@@ -229,7 +230,39 @@ struct Fp64Consts {
   double csf;
   double ea, ea2, ea2pi;     // Ewald alpha, alpha^2, 2 alpha / sqrt(pi) (1/A)
   SwitchSpec<double> swl, swc;  // generic form: LJ and Coulomb switches
+  // generic form, tabulated LJ (LennardJonesTableForce): two double4 per grid
+  // point, the hash of the first point and the last point (null: analytic)
+  const double4 *ljtab;
+  int tfirst, tlast;
 };
+
+// LookupTable<..., PRE = 7, double>: 2^7 intervals per octave of r^2, so the
+// hash of r^2 is its top 64 - 45 bits (sign, exponent, 7 mantissa bits)
+constexpr int kTabPre = 7;
+constexpr int kTabShift = 52 - kTabPre;
+
+// LennardJonesTableForce::operator() with LookupTable::index / interpolate
+// (LennardJonesTableForce.h:68-89, LookupTable.h:196-214): the grid point of
+// r^2 from its bit pattern, dt = r^2 minus r^2 with its low 45 bits cleared
+// (0 outside the grid, clamped to its ends), then the cubic in dt.  e: the
+// energy; f: force / r.
+__device__ __forceinline__ void lj_table_eval(const double4 *__restrict__ tab, int first, int last,
+                                              double r2, double A, double B, double &e,
+                                              double &f) {
+  const long long b = __double_as_longlong(r2);
+  int i = (int)(b >> kTabShift) - first;
+  double dt = 0.0;
+  if (i < 0) i = 0;
+  else if (i > last) i = last;
+  else dt = r2 - __longlong_as_double(b & ~((1LL << kTabShift) - 1));
+  const double4 ta = tab[2 * i], tb = tab[2 * i + 1];
+  const double a = ta.x * A + tb.x * B;
+  const double bb = ta.y * A + tb.y * B;
+  const double c = ta.z * A + tb.z * B;
+  const double d = ta.w * A + tb.w * B;
+  e = ((dt * d + c) * dt + bb) * dt + a;
+  f = -2.0 * ((3.0 * dt * d + 2.0 * c) * dt + bb);
+}
 
 // The stencil travels by value in the kernel parameters (per launch, so
 // contexts with different grids never share it).
@@ -1311,7 +1344,11 @@ k_pair_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes, const dou
             f = 0.0;
             const double rd2 = 1.0 / r2;
             const double rinv = sqrt(rd2);
-            if (mc.swl.kind != SW_OFF) {
+            if (mc.ljtab) {  // no Coulomb term beside the table
+              const double4 p = lj64[ti + mj.x];
+              lj_table_eval(mc.ljtab, mc.tfirst, mc.tlast, r2, kind == 1 ? p.z : p.x,
+                            kind == 1 ? p.w : p.y, e1, f);
+            } else if (mc.swl.kind != SW_OFF) {
               const double4 p = lj64[ti + mj.x];
               const double A = kind == 1 ? p.z : p.x;
               const double B = kind == 1 ? p.w : p.y;

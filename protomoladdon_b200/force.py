@@ -462,7 +462,10 @@ class NonbondedCutoffB200PairForce(NonbondedCutoffB200SystemForce):
     among C1, C2, Cn, ComplimentCnCn.  ``lj`` / ``coulomb``: None (term
     absent) or a tuple (kind, switchon, cutoff, order, switchoff); C1 reads
     the cutoff, C2 switchon and cutoff, Cn and ComplimentCnCn all four (see
-    pmb200_create_pair)."""
+    pmb200_create_pair).  ``lj_table``: the tabulated registrations
+    OneAtomPair<PBC, UniversalSwitchingFunction, LennardJonesTableForce<S, 7,
+    Real>> (NonbondedCutoffForceModule.cpp:67-72; id ``LennardJonesTable``),
+    S = ``lj``'s switch among C2, Cn, ComplimentCnCn, with no Coulomb term."""
 
     keyword = "NonbondedCutoffB200"
     _KIND = {None: _lib.PMB200_SW_NONE, "C1": _lib.PMB200_SW_C1, "C2": _lib.PMB200_SW_C2,
@@ -474,7 +477,7 @@ class NonbondedCutoffB200PairForce(NonbondedCutoffB200SystemForce):
                "ComplimentCnCn": ["-switchon", "-switchoff", "-cutoff", "-n"]}
 
     def __init__(self, lj=None, coulomb=None, cutoff_alg=None, precision="mixed", device=0,
-                 cellsize=0.0):
+                 cellsize=0.0, lj_table=False):
         def norm(sw):
             if sw is None:
                 return None
@@ -486,6 +489,11 @@ class NonbondedCutoffB200PairForce(NonbondedCutoffB200SystemForce):
         self.coulomb = norm(coulomb)
         if self.lj is None and self.coulomb is None:
             raise ValueError("need a Lennard-Jones or a Coulomb term")
+        self.lj_table = bool(lj_table)
+        if self.lj_table and (self.lj is None or self.coulomb is not None
+                              or self.lj[0] not in ("C2", "Cn", "ComplimentCnCn")):
+            raise ValueError("LennardJonesTable: a C2, Cn or ComplimentCnCn switch and no "
+                             "Coulomb term")
         rcs = [s[2] for s in (self.lj, self.coulomb) if s is not None]
         self.cutoff_alg = float(cutoff_alg if cutoff_alg is not None else max(rcs))
         self.precision = precision
@@ -500,7 +508,8 @@ class NonbondedCutoffB200PairForce(NonbondedCutoffB200SystemForce):
             return (ctypes.c_double * 4)(*(sw[1:5] if sw else (0.0,) * 4))
         p = _lib.PairParams(
             _lib.PMB200_MIXED if self.precision == "mixed" else _lib.PMB200_FP64, self.device,
-            self._KIND[self.lj[0] if self.lj else None], arr(self.lj),
+            self._KIND[self.lj[0] if self.lj else None]
+            | (_lib.PMB200_SW_TABLE if self.lj_table else 0), arr(self.lj),
             self._KIND[self.coulomb[0] if self.coulomb else None], arr(self.coulomb),
             self.cutoff_alg, self.cellsize or topo.cellsize)
         h = _P()
@@ -516,7 +525,8 @@ class NonbondedCutoffB200PairForce(NonbondedCutoffB200SystemForce):
         return " ".join(f"{k} {vals[k]:g}" for k in cls._PARAMS[kind])
 
     def get_id(self):
-        pots = [n for n, s in (("LennardJones", self.lj), ("Coulomb", self.coulomb)) if s]
+        pots = [n for n, s in (("LennardJonesTable" if self.lj_table else "LennardJones",
+                               self.lj), ("Coulomb", self.coulomb)) if s]
         sws = [s for s in (self.lj, self.coulomb) if s]
         head = " ".join(pots) + f" -algorithm {self.keyword} " + " ".join(
             f"-switchingFunction {s[0]}" for s in sws)
@@ -529,8 +539,13 @@ class NonbondedCutoffB200PairForce(NonbondedCutoffB200SystemForce):
         pots = []
         while toks and not toks[0].startswith("-"):
             pots.append(toks.pop(0))
+        table = pots == ["LennardJonesTable"]
+        if table:
+            pots = ["LennardJones"]
+            kw = dict(kw, lj_table=True)
         if pots not in (["LennardJones"], ["Coulomb"], ["LennardJones", "Coulomb"]):
-            raise ValueError(f"potentials {pots}: LennardJones and/or Coulomb")
+            raise ValueError(f"potentials {pots}: LennardJones and/or Coulomb, or "
+                             "LennardJonesTable")
         pairs = list(zip(toks[0::2], toks[1::2]))
         if len(toks) % 2:
             raise ValueError(f"cannot parse force id {force_id!r}")

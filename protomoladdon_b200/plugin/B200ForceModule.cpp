@@ -20,8 +20,8 @@ void ProtoMol::registerB200EwaldRealForce(ForceFactory &factory) {
 }
 
 // The switch combinations NonbondedCutoffForceModule registers for the
-// plain LJ / Coulomb potentials (NonbondedCutoffForceModule.cpp:55-82 and
-// 98-141); the periodic (C2, C1) pair has its own class.
+// plain and tabulated LJ / Coulomb potentials (NonbondedCutoffForceModule.cpp:
+// 55-82 and 98-141); the periodic (C2, C1) pair has its own class.
 template <class TBC>
 static void registerPairs(ForceFactory &f, bool vacuum) {
   const int C1 = PMB200_SW_C1, C2 = PMB200_SW_C2, CN = PMB200_SW_CN, NO = PMB200_SW_NONE,
@@ -30,6 +30,12 @@ static void registerPairs(ForceFactory &f, bool vacuum) {
                            {CN, NO}, {CM, NO}, {C2, C2}, {C2, CN}, {CN, CN}};
   for (int k = 0; k < (int)(sizeof(common) / sizeof(common[0])); k++)
     f.reg(new B200PairSystemForce<TBC>(common[k][0], common[k][1]));
+  // OneAtomPair<BC, Universal, LennardJonesTableForce<S, 7, Real>>
+  // (NonbondedCutoffForceModule.cpp:67-72, 121-126)
+  const int TB = PMB200_SW_TABLE;
+  f.reg(new B200PairSystemForce<TBC>(TB | C2, NO));
+  f.reg(new B200PairSystemForce<TBC>(TB | CN, NO));
+  f.reg(new B200PairSystemForce<TBC>(TB | CM, NO));
   if (vacuum) {
     f.reg(new B200PairSystemForce<TBC>(C2, C1));
     f.reg(new B200PairSystemForce<TBC>(CM, C1));

@@ -5,7 +5,10 @@
 // (pmb200_create_pair): OneAtomPair<BC, S, LennardJonesForce>,
 // OneAtomPair<BC, S, CoulombForce> and OneAtomPairTwo<BC, S1,
 // LennardJonesForce, S2, CoulombForce> with S among C1, C2, Cn and
-// ComplimentCnCn (CmpCnCnSwitchingFunction), for periodic
+// ComplimentCnCn (CmpCnCnSwitchingFunction), and OneAtomPair<BC,
+// UniversalSwitchingFunction, LennardJonesTableForce<S, 7, Real>> with S
+// among C2, Cn, ComplimentCnCn (id LennardJonesTable; NonbondedCutoffForce
+// Module.cpp:67-72, 121-126), for periodic
 // boundaries (BC = PeriodicBoundaryConditions) or vacuum
 // (VacuumBoundaryConditions).  One prototype per (LJ switch, Coulomb switch)
 // pair is registered under the algorithm keyword NonbondedCutoffB200; its id
@@ -43,7 +46,8 @@ class B200PairSystemForce : public SystemForce {
   typedef Topology<TBC, CubicCellManager> RealTopologyType;
 
 public:
-  // Prototype for (ljSwitch, coulombSwitch), each PMB200_SW_* (NONE: term absent).
+  // Prototype for (ljSwitch, coulombSwitch), each PMB200_SW_* (NONE: term
+  // absent; ljSwitch | PMB200_SW_TABLE: the tabulated LJ).
   B200PairSystemForce(int ljSwitch, int coulombSwitch) : myCtx(0), myCached(0) {
     init(ljSwitch, coulombSwitch);
   }
@@ -132,10 +136,11 @@ public:
 
   virtual std::string getIdNoAlias() const {
     std::string id;
-    if (myParams.lj_switch != PMB200_SW_NONE) id = "LennardJones";
+    if (myParams.lj_switch != PMB200_SW_NONE)
+      id = (myParams.lj_switch & PMB200_SW_TABLE) ? "LennardJonesTable" : "LennardJones";
     if (myParams.coulomb_switch != PMB200_SW_NONE) id += id.empty() ? "Coulomb" : " Coulomb";
     if (myParams.lj_switch != PMB200_SW_NONE)
-      id += " -switchingFunction " + switchName(myParams.lj_switch);
+      id += " -switchingFunction " + switchName(base(myParams.lj_switch));
     if (myParams.coulomb_switch != PMB200_SW_NONE)
       id += " -switchingFunction " + switchName(myParams.coulomb_switch);
     return id + " -algorithm " + getKeyword();
@@ -143,7 +148,7 @@ public:
 
   virtual void getParameters(std::vector<Parameter> &parameters) const {
     if (myParams.lj_switch != PMB200_SW_NONE)
-      switchParameters(myParams.lj_switch, myParams.lj, parameters);
+      switchParameters(base(myParams.lj_switch), myParams.lj, parameters);
     if (myParams.coulomb_switch != PMB200_SW_NONE)
       switchParameters(myParams.coulomb_switch, myParams.coulomb, parameters);
     parameters.push_back(Parameter("-cutoff",
@@ -155,6 +160,7 @@ private:
   B200PairSystemForce(const B200PairSystemForce &);
   B200PairSystemForce &operator=(const B200PairSystemForce &);
 
+  static int base(int kind) { return kind & ~PMB200_SW_TABLE; }
   static std::string switchName(int kind) {
     return kind == PMB200_SW_C1   ? "C1"
            : kind == PMB200_SW_C2 ? "C2"
@@ -203,10 +209,11 @@ private:
     for (int s = 0; s < 2; s++) {
       if (kinds[s] == PMB200_SW_NONE) continue;
       Real v[4] = {0, 0, 0, 0};
-      for (int a = 0; a < switchArity(kinds[s]); a++) values[k++].get(v[a]);
-      if (kinds[s] == PMB200_SW_C1) { dst[s][1] = v[0]; }
-      else if (kinds[s] == PMB200_SW_C2) { dst[s][0] = v[0]; dst[s][1] = v[1]; }
-      else if (kinds[s] == PMB200_SW_CN) {
+      const int kd = base(kinds[s]);
+      for (int a = 0; a < switchArity(kd); a++) values[k++].get(v[a]);
+      if (kd == PMB200_SW_C1) { dst[s][1] = v[0]; }
+      else if (kd == PMB200_SW_C2) { dst[s][0] = v[0]; dst[s][1] = v[1]; }
+      else if (kd == PMB200_SW_CN) {
         dst[s][2] = v[0]; dst[s][0] = v[1]; dst[s][3] = v[2]; dst[s][1] = v[3];
       } else {  // ComplimentCnCn: switchon, switchoff, cutoff, n
         dst[s][0] = v[0]; dst[s][3] = v[1]; dst[s][1] = v[2]; dst[s][2] = v[3];

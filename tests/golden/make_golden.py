@@ -40,6 +40,13 @@ Fixtures (all inputs and outputs FP64):
   whole molecules of the 648-atom box within 8.5 A of its centre, unwrapped
   around it), rc 8 / C2 from 7: forces, energies, virials.
   ``--vacuum-only`` writes just this.
+* ljtable_{water,modified,vacuum}_ref.npz -- the reference's tabulated LJ
+  registrations (OneAtomPair<BC, UniversalSwitchingFunction,
+  LennardJonesTableForce<S, 7, Real>>, S = C2, Cn, ComplimentCnCn) on the
+  648-atom box, on the modified box (A14/B14 through the table) and, with
+  vacuum boundaries, on the droplet: per case
+  ``<case>_{forces,energies,virial,molvirial}`` and ``<case>_lj`` (the
+  switch spec as in pairs_ref.npz).  ``--ljtable-only`` writes just these.
 """
 from __future__ import annotations
 
@@ -243,6 +250,43 @@ def vacuum_fixture():
     print("wrote the vacuum fixture to", HERE)
 
 
+LJTABLE_CASES = {
+    # file: {case: (switch kind, switchon, cutoff, order, switchoff)}
+    "water": {"t_c2": ("C2", 6.5, 8.0, 0, 0), "t_cn": ("Cn", 6.0, 8.0, 3, 8.0),
+              "t_cm": ("ComplimentCnCn", 0.0, 8.0, 6, 5.0)},
+    "modified": {"t_c2": ("C2", 7.0, 8.0, 0, 0)},
+    "vacuum": {"t_c2": ("C2", 7.0, 8.0, 0, 0), "t_cn": ("Cn", 6.0, 8.0, 4, 0),
+               "t_cm": ("ComplimentCnCn", 0.0, 8.0, 4, 6.0)},
+}
+
+
+def ljtable_fixtures():
+    codes = {"C2": 2, "Cn": 3, "ComplimentCnCn": 4}
+    w = water.small_648()
+    m = dict(w)
+    ex = np.asarray(m["excl"]).copy()
+    ex[m["type"][ex[:, 0]] == water.T_O, 2] = 1  # the O-H pairs modified (A14/B14)
+    m["excl"] = ex
+    m["coulomb_scaling"] = 0.5
+    systems = {"water": w, "modified": m, "vacuum": droplet()}
+    for name, cases in LJTABLE_CASES.items():
+        d = systems[name]
+        out = dict(sysd_arrays(d))
+        R = None if name == "vacuum" else O.RefForce(d)
+        for case, sw in cases.items():
+            if R is None:
+                f, e, v, mv = O.ref_vacuum_table_eval(d, d["pos"], sw, 8.0, 2)
+            else:
+                f, e, v, mv = R.pair_eval(d["pos"], sw, None, 8.0, 2, lj_table=True)
+            out.update({f"{case}_forces": f, f"{case}_energies": e, f"{case}_virial": v,
+                        f"{case}_molvirial": mv,
+                        f"{case}_lj": np.array([codes[sw[0]], *sw[1:]], dtype=np.float64)})
+        if R is not None:
+            R.close()
+        np.savez_compressed(os.path.join(HERE, f"ljtable_{name}_ref.npz"), **out)
+    print("wrote the tabulated-LJ fixtures to", HERE)
+
+
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
     only = [a for a in sys.argv[1:] if a.endswith("-only")]
@@ -261,3 +305,5 @@ if __name__ == "__main__":
         many_types_fixture()
     if not only or "--triclinic-only" in only:
         triclinic_fixture()
+    if not only or "--ljtable-only" in only:
+        ljtable_fixtures()

@@ -180,6 +180,44 @@ def test_vacuum_plugin_matches_reference():
     assert np.abs(e - d["ref_energies"]).max() <= 2e-3
 
 
+def _table_case(fname, case):
+    """(fixture, force id, values) of a tabulated-LJ fixture case."""
+    from .conftest import load_fixture
+    d = load_fixture(f"ljtable_{fname}_ref.npz")
+    a = d[f"{case}_lj"]
+    kind = {2: "C2", 3: "Cn", 4: "ComplimentCnCn"}[int(a[0])]
+    ron, rc, order, roff = (float(x) for x in a[1:])
+    vals = {"C2": [ron, rc], "Cn": [order, ron, roff, rc],
+            "ComplimentCnCn": [ron, roff, rc, order]}[kind] + [8.0]
+    return d, f"LennardJonesTable -switchingFunction {kind} -algorithm NonbondedCutoffB200", vals
+
+
+def test_factory_resolves_ljtable_ids():
+    """OneAtomPair<BC, Universal, LennardJonesTableForce<S, 7, Real>>
+    (NonbondedCutoffForceModule.cpp:67-72, 121-126) for both boundaries."""
+    for fname, case, vac in (("water", "t_c2", 0), ("water", "t_cn", 0), ("water", "t_cm", 0),
+                             ("vacuum", "t_cm", 1)):
+        d, fid, vals = _table_case(fname, case)
+        R = O.RefForce(d)
+        rc, msg, *_ = H.evaluate_pair(R, vac, fid, vals, d["pos"])
+        R.close()
+        assert (rc == 0 and fid in msg) or "B200 cutoff force" in msg, (case, msg)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("fname,case,vac", [("water", "t_c2", 0), ("modified", "t_c2", 0),
+                                            ("water", "t_cm", 0), ("vacuum", "t_cn", 1)])
+def test_ljtable_plugin_matches_reference(fname, case, vac):
+    d, fid, vals = _table_case(fname, case)
+    R = O.RefForce(d)
+    rc, msg, f, e, v, mv = H.evaluate_pair(R, vac, fid, vals, d["pos"])
+    R.close()
+    assert rc == 0, msg
+    fr = d[f"{case}_forces"]
+    assert np.sqrt(((f - fr) ** 2).sum() / (fr ** 2).sum()) <= 1e-5
+    assert e[0] == 0.0 and abs(e[1] - d[f"{case}_energies"][1]) <= 1e-3
+
+
 def _parallel_vs_plain(call):
     """(plain result, parallelEvaluate result, blocks) of one harness call."""
     H.set_parallel(False)
