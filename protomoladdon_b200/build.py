@@ -12,9 +12,11 @@ SOURCES = [os.path.join(CSRC, "pmb200_api.cu")]
 DEPS = SOURCES + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))] + [
     os.path.join(HERE, "..", "include", "pmb200.h")]
 
-# (-fno-math-errno: the host code's square roots vectorise)
+# (-fno-math-errno: the host code's square roots vectorise; -ffp-contract=off:
+# no fused multiply-adds in host code, so hosts with and without FMA round alike)
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-fopenmp", "-Xcompiler", "-fno-math-errno",
+              "-Xcompiler", "-ffp-contract=off",
               "-shared", "-cudart", "static",
               "-lgomp"]
 

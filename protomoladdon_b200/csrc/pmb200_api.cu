@@ -1783,82 +1783,30 @@ int pmb200_last_pair_count(pmb200_ctx *c, long long *pairs) {
   return PMB200_OK;
 }
 
-// SETTLE on the host (same algorithm as settle_water on the device).
-static void host_settle(const SettleParams &sp, double inv_m, double inv_ra, const double *A0,
-                        const double *B0, const double *C0, double *A1, double *B1,
-                        double *C1) {
-  auto cross = [](const double a[3], const double b[3], double o[3]) {
-    o[0] = a[1] * b[2] - a[2] * b[1];
-    o[1] = a[2] * b[0] - a[0] * b[2];
-    o[2] = a[0] * b[1] - a[1] * b[0];
-  };
-  auto dot = [](const double a[3], const double b[3]) {
-    return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
-  };
-  auto unit = [&](double a[3]) {
-    const double s = 1.0 / std::sqrt(dot(a, a));
-    a[0] *= s; a[1] *= s; a[2] *= s;
-  };
-  double com[3], a1[3], b1[3], c1[3], b0[3], c0[3], ex[3], ey[3], ez[3];
-  for (int k = 0; k < 3; k++) {
-    com[k] = (sp.mo * A1[k] + sp.mh * B1[k] + sp.mh * C1[k]) * inv_m;
-    a1[k] = A1[k] - com[k];
-    b1[k] = B1[k] - com[k];
-    c1[k] = C1[k] - com[k];
-    b0[k] = B0[k] - A0[k];
-    c0[k] = C0[k] - A0[k];
-  }
-  cross(b0, c0, ez);
-  cross(a1, ez, ex);
-  cross(ez, ex, ey);
-  unit(ex); unit(ey); unit(ez);
-  const double xb0 = dot(ex, b0), yb0 = dot(ey, b0), xc0 = dot(ex, c0), yc0 = dot(ey, c0);
-  const double za1 = dot(ez, a1);
-  const double xb1 = dot(ex, b1), yb1 = dot(ey, b1), zb1 = dot(ez, b1);
-  const double xc1 = dot(ex, c1), yc1 = dot(ey, c1), zc1 = dot(ez, c1);
-  const double sphi = za1 * inv_ra, cphi = std::sqrt(1.0 - sphi * sphi);
-  const double spsi = (zb1 - zc1) / (2.0 * sp.rc * cphi), cpsi = std::sqrt(1.0 - spsi * spsi);
-  const double ya2 = sp.ra * cphi, xb2 = -sp.rc * cpsi;
-  const double t1 = -sp.rb * cphi, t2 = sp.rc * spsi * sphi;
-  const double yb2 = t1 - t2, yc2 = t1 + t2;
-  const double al = xb2 * (xb0 - xc0) + yb0 * yb2 + yc0 * yc2;
-  const double be = xb2 * (yc0 - yb0) + xb0 * yb2 + xc0 * yc2;
-  const double ga = xb0 * yb1 - xb1 * yb0 + xc0 * yc1 - xc1 * yc0;
-  const double ab = al * al + be * be;
-  const double sth = (al * ga - be * std::sqrt(ab - ga * ga)) / ab;
-  const double cth = std::sqrt(1.0 - sth * sth);
-  const double xa3 = -ya2 * sth, ya3 = ya2 * cth, za3 = za1;
-  const double xb3 = xb2 * cth - yb2 * sth, yb3 = xb2 * sth + yb2 * cth, zb3 = zb1;
-  const double xc3 = -xb2 * cth - yc2 * sth, yc3 = -xb2 * sth + yc2 * cth, zc3 = zc1;
-  for (int k = 0; k < 3; k++) {
-    A1[k] = com[k] + xa3 * ex[k] + ya3 * ey[k] + za3 * ez[k];
-    B1[k] = com[k] + xb3 * ex[k] + yb3 * ey[k] + zb3 * ez[k];
-    C1[k] = com[k] + xc3 * ex[k] + yc3 * ey[k] + zc3 * ez[k];
-  }
-}
-
-// The same for kW waters at once, lane by lane: the loops over lanes
-// vectorise and the waters' dependency chains (seven square roots and
-// divisions each) overlap.
-constexpr int kW = 4;
-// (also built for AVX2, picked at load time where the host has it: four
-// lanes per instruction instead of two; no FMA, so every host rounds alike)
-__attribute__((target_clones("avx2", "default")))
+// SETTLE on the host (the algorithm of settle_water on the device) for kW
+// waters at once, structure of arrays: X0 the pre-step positions, X1 the
+// unconstrained new ones (in) and the constrained ones (out), rows
+// {O, H1, H2} x {x, y, z}.  Every loop runs over the lanes with no
+// dependence between them, so it vectorises; the waters' dependency chains
+// (seven square roots and divisions each) overlap.  Built for AVX-512 and
+// AVX2 as well, picked at load time where the host has them (eight or four
+// lanes per instruction instead of two); floating-point contraction is off
+// in this build, so every host rounds alike.
+constexpr int kW = 8;
+__attribute__((target_clones("avx512f", "avx2", "default")))
 static void host_settle_w(const SettleParams &sp, double inv_m, double inv_ra,
-                          const double *const A0[kW], const double *const B0[kW],
-                          const double *const C0[kW], double *const A1[kW],
-                          double *const B1[kW], double *const C1[kW]) {
-#define PMB_LANES for (int l = 0; l < kW; l++)
+                          const double (&X0)[9][kW], double (&X1)[9][kW]) {
+#define PMB_LANES _Pragma("omp simd") for (int l = 0; l < kW; l++)
   double com[3][kW], a1[3][kW], b1[3][kW], c1[3][kW], b0[3][kW], c0[3][kW];
   double ex[3][kW], ey[3][kW], ez[3][kW];
   for (int k = 0; k < 3; k++)
     PMB_LANES {
-      com[k][l] = (sp.mo * A1[l][k] + sp.mh * B1[l][k] + sp.mh * C1[l][k]) * inv_m;
-      a1[k][l] = A1[l][k] - com[k][l];
-      b1[k][l] = B1[l][k] - com[k][l];
-      c1[k][l] = C1[l][k] - com[k][l];
-      b0[k][l] = B0[l][k] - A0[l][k];
-      c0[k][l] = C0[l][k] - A0[l][k];
+      com[k][l] = (sp.mo * X1[k][l] + sp.mh * X1[3 + k][l] + sp.mh * X1[6 + k][l]) * inv_m;
+      a1[k][l] = X1[k][l] - com[k][l];
+      b1[k][l] = X1[3 + k][l] - com[k][l];
+      c1[k][l] = X1[6 + k][l] - com[k][l];
+      b0[k][l] = X0[3 + k][l] - X0[k][l];
+      c0[k][l] = X0[6 + k][l] - X0[k][l];
     }
   auto cross = [](const double a[3][kW], const double b[3][kW], double o[3][kW]) {
     PMB_LANES {
@@ -1902,17 +1850,17 @@ static void host_settle_w(const SettleParams &sp, double inv_m, double inv_ra,
     sth[l] = (al * ga - be * std::sqrt(ab - ga * ga)) / ab;
     cth[l] = std::sqrt(1.0 - sth[l] * sth[l]);
   }
-  PMB_LANES {
-    const double xa3 = -ya2[l] * sth[l], ya3 = ya2[l] * cth[l], za3 = za1[l];
-    const double xb3 = xb2[l] * cth[l] - yb2[l] * sth[l], yb3 = xb2[l] * sth[l] + yb2[l] * cth[l];
-    const double xc3 = -xb2[l] * cth[l] - yc2[l] * sth[l];
-    const double yc3 = -xb2[l] * sth[l] + yc2[l] * cth[l];
-    for (int k = 0; k < 3; k++) {
-      A1[l][k] = com[k][l] + xa3 * ex[k][l] + ya3 * ey[k][l] + za3 * ez[k][l];
-      B1[l][k] = com[k][l] + xb3 * ex[k][l] + yb3 * ey[k][l] + zb1[l] * ez[k][l];
-      C1[l][k] = com[k][l] + xc3 * ex[k][l] + yc3 * ey[k][l] + zc1[l] * ez[k][l];
+  for (int k = 0; k < 3; k++)
+    PMB_LANES {
+      const double xa3 = -ya2[l] * sth[l], ya3 = ya2[l] * cth[l];
+      const double xb3 = xb2[l] * cth[l] - yb2[l] * sth[l];
+      const double yb3 = xb2[l] * sth[l] + yb2[l] * cth[l];
+      const double xc3 = -xb2[l] * cth[l] - yc2[l] * sth[l];
+      const double yc3 = -xb2[l] * sth[l] + yc2[l] * cth[l];
+      X1[k][l] = com[k][l] + xa3 * ex[k][l] + ya3 * ey[k][l] + za1[l] * ez[k][l];
+      X1[3 + k][l] = com[k][l] + xb3 * ex[k][l] + yb3 * ey[k][l] + zb1[l] * ez[k][l];
+      X1[6 + k][l] = com[k][l] + xc3 * ex[k][l] + yc3 * ey[k][l] + zc1[l] * ez[k][l];
     }
-  }
 #undef PMB_LANES
 }
 
@@ -1921,85 +1869,100 @@ int pmb200_host_kick_drift(int n, double *pos, double *vel, const double *forces
                            const int *widx, double d_oh, double d_hh) {
   if (n < 0 || (n > 0 && (!pos || !vel || !forces || !mass)) || !(dt_fs > 0.0))
     return PMB200_EINVAL;
-  if (nwater < 0 || (nwater > 0 && !widx)) return PMB200_EINVAL;
+  if (nwater < 0 || (nwater > 0 && !widx) || 3LL * nwater > n) return PMB200_EINVAL;
   const double h = dt_fs * 0.02045482828087295;  // Constant::INV_TIMEFACTOR
-  // which atoms the rigid waters hold (each at most once)
+  // which atoms the rigid waters hold: each index in range and at most once,
+  // checked before anything is written.  Strictly increasing indices (the
+  // usual listing) are checked on all cores with no shared writes; when the
+  // waters hold every atom nothing else is needed, otherwise the atoms they
+  // hold are marked.  Any other order: the marks, one index at a time.
   static thread_local std::vector<unsigned char> in_water;
+  bool mark = false;
   if (nwater > 0) {
-    in_water.assign((size_t)n, 0);
-    for (int w = 0; w < 3 * nwater; w++) {
+    const int nw3 = 3 * nwater;
+    int bad = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad) if (nwater > 1024)
+    for (int w = 0; w < nw3; w++) {
       const int a = widx[w];
-      if (a < 0 || a >= n || in_water[a]) return PMB200_EINVAL;
-      in_water[a] = 1;
+      bad |= (a < 0 || a >= n || (w + 1 < nw3 && widx[w + 1] <= a)) ? 1 : 0;
+    }
+    mark = nw3 < n;
+    if (bad) {
+      in_water.assign((size_t)n, 0);
+      for (int w = 0; w < nw3; w++) {
+        const int a = widx[w];
+        if (a < 0 || a >= n || in_water[a]) return PMB200_EINVAL;
+        in_water[a] = 1;
+      }
+      mark = false;  // already marked
+    } else if (mark) {
+      in_water.assign((size_t)n, 0);
     }
   }
   const double kh = kick * h, inv_h = 1.0 / h;
-  // atoms outside the waters: kick and drift (independent per atom, shared
-  // by the host's cores)
-  if (3 * nwater < n) {
-    const unsigned char *inw = nwater > 0 ? in_water.data() : nullptr;
-#pragma omp parallel for schedule(static) if (n > 4096)
-    for (int i = 0; i < n; i++) {
-      if (inw && inw[i]) continue;
-      const double s = kh / mass[i];
-      for (int k = 0; k < 3; k++) {
-        const size_t q = 3 * (size_t)i + k;
-        vel[q] += forces[q] * s;
-        pos[q] += vel[q] * h;
-      }
-    }
-  }
+  SettleParams sp{};
+  double inv_m = 0.0, inv_ra = 0.0;
   if (nwater > 0) {
-    SettleParams sp{};
     const double mo = mass[widx[0]], mh = mass[widx[1]];
     const double rcv = 0.5 * d_hh, t = std::sqrt(d_oh * d_oh - rcv * rcv);
     sp.mo = mo; sp.mh = mh; sp.rc = rcv;
     sp.ra = 2.0 * mh * t / (mo + 2.0 * mh);
     sp.rb = t - sp.ra;
-    const double inv_m = 1.0 / (mo + 2.0 * mh), inv_ra = 1.0 / sp.ra;
-    const int ngroups = (nwater + kW - 1) / kW;  // kW waters per iteration
-    // one pass per group of waters: kick and drift its atoms (the pre-step
-    // positions kept on the stack), constrain, and take the velocities from
-    // the constrained displacement
-#pragma omp parallel for schedule(static) if (nwater > 1024)
+    inv_m = 1.0 / (mo + 2.0 * mh);
+    inv_ra = 1.0 / sp.ra;
+  }
+  const int ngroups = (nwater + kW - 1) / kW;  // kW waters per group
+  const int nchunk = 3 * nwater < n ? (n + 4095) / 4096 : 0;  // atoms outside the waters
+  unsigned char *inw = nchunk > 0 && nwater > 0 ? in_water.data() : nullptr;
+#pragma omp parallel if (n > 4096)
+  {
+    if (mark) {  // distinct indices: no two threads write the same byte
+#pragma omp for schedule(static)
+      for (int w = 0; w < 3 * nwater; w++) inw[widx[w]] = 1;
+    }
+    // atoms outside the waters: kick and drift (independent per atom)
+#pragma omp for schedule(static) nowait
+    for (int cidx = 0; cidx < nchunk; cidx++) {
+      const int i1 = std::min(n, (cidx + 1) * 4096);
+      for (int i = cidx * 4096; i < i1; i++) {
+        if (inw && inw[i]) continue;
+        const double s = kh / mass[i];
+        for (int k = 0; k < 3; k++) {
+          const size_t q = 3 * (size_t)i + k;
+          vel[q] += forces[q] * s;
+          pos[q] += vel[q] * h;
+        }
+      }
+    }
+    // one pass per group of waters: kick and drift into the group's arrays,
+    // constrain, write the positions and take the velocities from the
+    // constrained displacement; a short last group repeats its first water
+    // in the spare lanes and writes only its own
+#pragma omp for schedule(static)
     for (int gidx = 0; gidx < ngroups; gidx++) {
       const int w0 = gidx * kW, wn = std::min(kW, nwater - w0);
-      double old[kW][3][3];
-      for (int l = 0; l < wn; l++)
+      double X0[9][kW], X1[9][kW];
+      for (int l = 0; l < kW; l++)
         for (int m = 0; m < 3; m++) {
-          const int a = widx[3 * (w0 + l) + m];
+          const int a = widx[3 * (w0 + (l < wn ? l : 0)) + m];
           const double s = kh / mass[a];
           for (int k = 0; k < 3; k++) {
             const size_t q = 3 * (size_t)a + k;
-            old[l][m][k] = pos[q];
-            vel[q] += forces[q] * s;
-            pos[q] += vel[q] * h;
+            const double v = vel[q] + forces[q] * s;
+            X0[3 * m + k][l] = pos[q];
+            X1[3 * m + k][l] = pos[q] + v * h;
           }
         }
-      if (wn == kW) {
-        const double *A0[kW], *B0[kW], *C0[kW];
-        double *A1[kW], *B1[kW], *C1[kW];
-        for (int l = 0; l < kW; l++) {
-          const int *wi = widx + 3 * (w0 + l);
-          A0[l] = old[l][0]; B0[l] = old[l][1]; C0[l] = old[l][2];
-          A1[l] = pos + 3 * (size_t)wi[0]; B1[l] = pos + 3 * (size_t)wi[1];
-          C1[l] = pos + 3 * (size_t)wi[2];
-        }
-        host_settle_w(sp, inv_m, inv_ra, A0, B0, C0, A1, B1, C1);
-      } else {
-        for (int l = 0; l < wn; l++) {
-          const int *wi = widx + 3 * (w0 + l);
-          host_settle(sp, inv_m, inv_ra, old[l][0], old[l][1], old[l][2],
-                      pos + 3 * (size_t)wi[0], pos + 3 * (size_t)wi[1],
-                      pos + 3 * (size_t)wi[2]);
-        }
-      }
+      host_settle_w(sp, inv_m, inv_ra, X0, X1);
       for (int l = 0; l < wn; l++)
-        for (int m = 0; m < 3; m++)
+        for (int m = 0; m < 3; m++) {
+          const int a = widx[3 * (w0 + l) + m];
           for (int k = 0; k < 3; k++) {
-            const size_t q = 3 * (size_t)widx[3 * (w0 + l) + m] + k;
-            vel[q] = (pos[q] - old[l][m][k]) * inv_h;
+            const size_t q = 3 * (size_t)a + k;
+            pos[q] = X1[3 * m + k][l];
+            vel[q] = (X1[3 * m + k][l] - X0[3 * m + k][l]) * inv_h;
           }
+        }
     }
   }
   return PMB200_OK;

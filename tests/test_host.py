@@ -169,6 +169,24 @@ def test_host_kick_drift_free_atoms_and_bad_water_lists():
         assert np.array_equal(p3, s["pos"]) and np.array_equal(v3, s["vel"])
 
 
+def test_host_kick_drift_any_water_order():
+    """Waters listed in any order (not increasing: the one-by-one check) and
+    with some waters free give the same result as the increasing listing."""
+    from protomoladdon_b200 import rigid
+    s = water.small_648()
+    w = np.asarray(water.rigid_waters(s)).reshape(-1, 3)
+    rng = np.random.default_rng(3)
+    F = rng.normal(0, 20, s["pos"].shape)
+    for keep in (len(w), len(w) - 7):
+        sub = w[:keep]
+        p1, v1 = s["pos"].copy(), s["vel"].copy()
+        rigid.host_kick_drift(p1, v1, F, s["mass"], 1.0, sub, water.D_OH, water.D_HH)
+        p2, v2 = s["pos"].copy(), s["vel"].copy()
+        rigid.host_kick_drift(p2, v2, F, s["mass"], 1.0, sub[rng.permutation(keep)],
+                              water.D_OH, water.D_HH)
+        assert np.array_equal(p1, p2) and np.array_equal(v1, v2)
+
+
 def test_lj_table_mixing_matches_the_generator():
     """autograd.lj_table (torch, differentiable) reproduces the water
     generator's table, ions included."""
