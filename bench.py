@@ -347,8 +347,10 @@ def run_ours(args):
 
     def host_step():
         t0 = time.perf_counter()
-        rigid.host_kick_drift(xh, vh, F, s["mass"], DT_FS, widx, water.D_OH, water.D_HH)
-        _ft.zero_()  # the integrator zeroes its force array (F is a view of _ft)
+        # kick, drift, SETTLE, and the force array zeroed for the next
+        # evaluation to add into (StandardIntegrator::calculateForces), in one pass
+        rigid.host_kick_drift(xh, vh, F, s["mass"], DT_FS, widx, water.D_OH, water.D_HH,
+                              clear_forces=True)
         E.clear()
         t1 = time.perf_counter()
         fmix.evaluate(topo, xh, F, E)

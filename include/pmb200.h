@@ -227,12 +227,16 @@ int pmb200_last_pair_count(pmb200_ctx *ctx, long long *pairs);
  * (the role of ProtoMol's SHAKE modifier).  kick is 1 for a full kick, 0.5
  * for the first half kick.  An atom belongs to at most one water
  * (PMB200_EINVAL otherwise); each water's atoms are kicked, drifted and
- * constrained in one pass.  Runs on the host (OpenMP threads for large
- * systems); no GPU. */
+ * constrained in one pass.  clear_forces != 0: each force entry is set to
+ * zero once it has been used, ready for the next evaluation to add into (the
+ * myForces->zero() of StandardIntegrator::calculateForces,
+ * .../integrator/StandardIntegrator.cpp:44-48), in the same pass.  Runs on the host (OpenMP threads for
+ * large systems); no GPU. */
 int pmb200_host_kick_drift(int n, double *pos, double *vel,
-                           const double *forces, const double *mass,
+                           double *forces, const double *mass,
                            double dt_fs, double kick, int nwater,
-                           const int *widx, double d_oh, double d_hh);
+                           const int *widx, double d_oh, double d_hh,
+                           int clear_forces);
 
 /* Measurement helper (no counterpart in the reference): FP32 FMA throughput
  * of `device` in TFLOP/s (2 flops per FMA), from a 148-SM-filling chain of

@@ -113,7 +113,7 @@ def lib():
     L.pmb200_last_kernel_ms.argtypes = [_P, ctypes.POINTER(ctypes.c_float)]
     L.pmb200_measure_fp32_peak.argtypes = [_I, ctypes.POINTER(_D)]
     L.pmb200_set_rigid_waters.argtypes = [_P, _I, _P, _D, _D]
-    L.pmb200_host_kick_drift.argtypes = [_I, _P, _P, _P, _P, _D, _D, _I, _P, _D, _D]
+    L.pmb200_host_kick_drift.argtypes = [_I, _P, _P, _P, _P, _D, _D, _I, _P, _D, _D, _I]
     L.pmb200_eval_noalloc.argtypes = [ctypes.POINTER(Params), _I, _P, _P, _P, _P, _P, _P, _I, _P,
                                       _D, _P, _P, _P, _P, _P, _P]
     L.pmb200_create_ewald_real.argtypes = [ctypes.POINTER(EwaldParams), ctypes.POINTER(_P)]

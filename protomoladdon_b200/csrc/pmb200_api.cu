@@ -1864,9 +1864,9 @@ static void host_settle_w(const SettleParams &sp, double inv_m, double inv_ra,
 #undef PMB_LANES
 }
 
-int pmb200_host_kick_drift(int n, double *pos, double *vel, const double *forces,
+int pmb200_host_kick_drift(int n, double *pos, double *vel, double *forces,
                            const double *mass, double dt_fs, double kick, int nwater,
-                           const int *widx, double d_oh, double d_hh) {
+                           const int *widx, double d_oh, double d_hh, int clear_forces) {
   if (n < 0 || (n > 0 && (!pos || !vel || !forces || !mass)) || !(dt_fs > 0.0))
     return PMB200_EINVAL;
   if (nwater < 0 || (nwater > 0 && !widx) || 3LL * nwater > n) return PMB200_EINVAL;
@@ -1931,6 +1931,7 @@ int pmb200_host_kick_drift(int n, double *pos, double *vel, const double *forces
           const size_t q = 3 * (size_t)i + k;
           vel[q] += forces[q] * s;
           pos[q] += vel[q] * h;
+          if (clear_forces) forces[q] = 0.0;
         }
       }
     }
@@ -1953,6 +1954,10 @@ int pmb200_host_kick_drift(int n, double *pos, double *vel, const double *forces
             X1[3 * m + k][l] = pos[q] + v * h;
           }
         }
+      if (clear_forces)  // after the gather: a short group reads its first water twice
+        for (int l = 0; l < wn; l++)
+          for (int m = 0; m < 3; m++)
+            for (int k = 0; k < 3; k++) forces[3 * (size_t)widx[3 * (w0 + l) + m] + k] = 0.0;
       host_settle_w(sp, inv_m, inv_ra, X0, X1);
       for (int l = 0; l < wn; l++)
         for (int m = 0; m < 3; m++) {

@@ -85,9 +85,11 @@ def kick_drift_settle(pos, vel, forces, mass, dt_fs, widx, d_oh, d_hh, kick=1.0)
         vel[w] = (pos[w] - old[w]) / h
 
 
-def host_kick_drift(pos, vel, forces, mass, dt_fs, widx, d_oh, d_hh, kick=1.0):
+def host_kick_drift(pos, vel, forces, mass, dt_fs, widx, d_oh, d_hh, kick=1.0,
+                    clear_forces=False):
     """kick_drift_settle through libpmb200's native host helper
-    (pmb200_host_kick_drift); arrays are C-contiguous float64, updated in place."""
+    (pmb200_host_kick_drift); arrays are C-contiguous float64, updated in place.
+    clear_forces: zero ``forces`` once used (for the next evaluation to add into)."""
     import ctypes
     from . import _lib
     w = np.ascontiguousarray(widx, dtype=np.int32).reshape(-1)
@@ -96,6 +98,6 @@ def host_kick_drift(pos, vel, forces, mass, dt_fs, widx, d_oh, d_hh, kick=1.0):
     rc = _lib.lib().pmb200_host_kick_drift(
         int(pos.shape[0]), P(pos.ctypes.data), P(vel.ctypes.data), P(forces.ctypes.data),
         P(m.ctypes.data), float(dt_fs), float(kick), w.size // 3,
-        P(w.ctypes.data) if w.size else None, float(d_oh), float(d_hh))
+        P(w.ctypes.data) if w.size else None, float(d_oh), float(d_hh), int(bool(clear_forces)))
     if rc:
         raise _lib.PmbError(rc, "pmb200_host_kick_drift")

@@ -187,6 +187,23 @@ def test_host_kick_drift_any_water_order():
         assert np.array_equal(p1, p2) and np.array_equal(v1, v2)
 
 
+def test_host_kick_drift_clears_forces_after_use():
+    """clear_forces: the same positions and velocities, and every force entry
+    (waters and free atoms, including a short last group of waters) zero."""
+    from protomoladdon_b200 import rigid
+    s = water.small_648()
+    w = np.asarray(water.rigid_waters(s)).reshape(-1, 3)[:-5]  # 211 waters, 5 free
+    rng = np.random.default_rng(4)
+    F = rng.normal(0, 20, s["pos"].shape)
+    p1, v1 = s["pos"].copy(), s["vel"].copy()
+    rigid.host_kick_drift(p1, v1, F, s["mass"], 1.0, w, water.D_OH, water.D_HH)
+    p2, v2, F2 = s["pos"].copy(), s["vel"].copy(), F.copy()
+    rigid.host_kick_drift(p2, v2, F2, s["mass"], 1.0, w, water.D_OH, water.D_HH,
+                          clear_forces=True)
+    assert np.array_equal(p1, p2) and np.array_equal(v1, v2)
+    assert not F2.any()
+
+
 def test_lj_table_mixing_matches_the_generator():
     """autograd.lj_table (torch, differentiable) reproduces the water
     generator's table, ions included."""
