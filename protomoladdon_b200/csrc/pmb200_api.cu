@@ -634,9 +634,6 @@ int launch_eval(pmb200_ctx *c, const double *d_pos, double *d_forces, double *d_
   CK(cudaGetLastError());
   if (timed) CK(cudaEventRecord(c->ev1, st));
   if (energy || virial) {
-    // C1 constants for the mixed Coulomb sums (the Ewald term has none)
-    const double rcc = c->p.cutoff_coul / g.unit;
-    const bool c1 = c->form == FORM_CUTOFF;
     // partial rows: one per (cell, slot) warp of the mixed kernel, one per
     // cell of the FP64 kernel
     // (energy / virial launches of the mixed kernel use the slot count of
@@ -644,8 +641,7 @@ int launch_eval(pmb200_ctx *c, const double *d_pos, double *d_forces, double *d_
     k_reduce1<<<kRedBlocks, 256, 0, st>>>(
         mixed ? g.ncell * mixed_cell_slots(true, n, g.ncell) : g.ncell, c->d_partial, c->d_red);
     // the mixed kernel visits each pair once, the FP64 kernel twice
-    k_reduce2<<<1, 256, 0, st>>>(kRedBlocks, c->d_red, mixed ? 1 : 0, mixed ? 1.0 : 0.5,
-                                c1 ? 1.5 / rcc : 0.0, c1 ? 0.5 / (rcc * rcc * rcc) : 0.0,
+    k_reduce2<<<1, 256, 0, st>>>(kRedBlocks, c->d_red, mixed ? 1.0 : 0.5,
                                 d_out ? d_out : c->d_out, c->d_pairs);
     CK(cudaGetLastError());
   }
@@ -1116,6 +1112,8 @@ int pmb200_set_box(pmb200_ctx *c, const double e1[3], const double e2[3], const 
   m.c15_1 = (float)(1.5 / rq);
   m.c05_3 = (float)(0.5 / (rq * rq * rq));
   m.c15_3 = (float)(1.5 / (rq * rq * rq));
+  m.e15 = 1.5 / rq;
+  m.e05 = 0.5 / (rq * rq * rq);
   m.csf = (float)c->csf;
   m.ey = (float)(g.edge[1] / u);
   m.ez = (float)(g.edge[2] / u);
@@ -1225,12 +1223,9 @@ int pmb200_shard_eval_device(pmb200_ctx *c, const double *d_pos, int shard, int 
   if (energy || virial) {
     if (hi > lo) {
       // this shard's partial rows: one per (cell, slot) warp
-      const double rcc = c->p.cutoff_coul / g.unit;
-      const bool c1 = c->form == FORM_CUTOFF;
       k_reduce1<<<kRedBlocks, 256, 0, st>>>((hi - lo) * mixed_cell_slots(true, n, g.ncell),
                                             c->d_partial, c->d_red);
-      k_reduce2<<<1, 256, 0, st>>>(kRedBlocks, c->d_red, 1, 1.0, c1 ? 1.5 / rcc : 0.0,
-                                  c1 ? 0.5 / (rcc * rcc * rcc) : 0.0, d_out, c->d_pairs);
+      k_reduce2<<<1, 256, 0, st>>>(kRedBlocks, c->d_red, 1.0, d_out, c->d_pairs);
     } else {
       CK(cudaMemsetAsync(d_out, 0, sizeof(double) * 20, st));
       CK(cudaMemsetAsync(c->d_pairs, 0, sizeof(double), st));
@@ -1585,12 +1580,9 @@ int pmb200_eval_cells(pmb200_ctx *c, const double *pos, double *forces, double *
   }
   CK(cudaGetLastError());
   if (energy || anyvir) {
-    const double rcc = c->p.cutoff_coul / g.unit;
-    const bool c1 = c->form == FORM_CUTOFF;
     k_reduce1<<<kRedBlocks, 256, 0, st>>>(rows, prow, c->d_red);
-    k_reduce2<<<1, 256, 0, st>>>(kRedBlocks, c->d_red, mixed ? 1 : 0, mixed ? 1.0 : 0.5,
-                                c1 ? 1.5 / rcc : 0.0, c1 ? 0.5 / (rcc * rcc * rcc) : 0.0,
-                                c->d_out, c->d_pairs);
+    k_reduce2<<<1, 256, 0, st>>>(kRedBlocks, c->d_red, mixed ? 1.0 : 0.5, c->d_out,
+                                c->d_pairs);
     CK(cudaMemcpyAsync(c->h_pin_out, c->d_out, sizeof(double) * 20, cudaMemcpyDeviceToHost,
                        st));
   }
@@ -2172,6 +2164,8 @@ extern "C" int pmb200_eval_noalloc(const pmb200_params *p, int n, const double *
   mc.c15_1 = (float)(1.5 / rq);
   mc.c05_3 = (float)(0.5 / (rq * rq * rq));
   mc.c15_3 = (float)(1.5 / (rq * rq * rq));
+  mc.e15 = 1.5 / rq;
+  mc.e05 = 0.5 / (rq * rq * rq);
   mc.csf = (float)coulomb_scaling;
   mc.ey = (float)(edge[1] / u);
   mc.ez = (float)(edge[2] / u);
@@ -2237,8 +2231,7 @@ extern "C" int pmb200_eval_noalloc(const pmb200_params *p, int n, const double *
     k_reduce1<<<kRedBlocks, 256, 0, st>>>(g.ncell * slots, partial, red);
     // the reduction writes 20 doubles (energies, virial, molecular
     // virial) into the scratch; the caller's buffer receives the two energies
-    k_reduce2<<<1, 256, 0, st>>>(kRedBlocks, red, 1, 1.0, 1.5 / rq, 0.5 / (rq * rq * rq),
-                                out, pairs);
+    k_reduce2<<<1, 256, 0, st>>>(kRedBlocks, red, 1.0, out, pairs);
     e = cudaMemcpyAsync(d_energy, out, 2 * sizeof(double), cudaMemcpyDeviceToDevice, st);
     if (e != cudaSuccess) return PMB200_ECUDA;
   }
@@ -2485,9 +2478,6 @@ int pmb200_batch_create(pmb200_ctx *const *systems, int nsys, pmb200_batch **out
     y.mc = c->mc;
     y.pb = c->pb;
     y.fscale = kFixInv / c->g.unit;
-    const double rcc = c->p.cutoff_coul / c->g.unit;
-    y.c15_1 = c->form == FORM_CUTOFF ? 1.5 / rcc : 0.0;
-    y.c05_3 = c->form == FORM_CUTOFF ? 0.5 / (rcc * rcc * rcc) : 0.0;
     y.qscale32 = (float)(1.0 / std::sqrt(c->g.unit));
     y.cell0 = (int)C;
     y.atom0 = (int)N;

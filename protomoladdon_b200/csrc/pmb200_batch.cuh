@@ -24,7 +24,6 @@ struct BatchSys {
   MixedConsts mc;
   PbcRef pb;
   double fscale;         // fixed point -> force: 2^-32 / cell edge
-  double c15_1, c05_3;   // C1 constants in cell units (energy), 0 for the Ewald term
   float qscale32;        // 1 / sqrt(cell edge)
   int cell0, atom0, natoms;
   int st0, st_n;         // stencil slice
@@ -74,7 +73,7 @@ k_pair_mixed_batch(const BatchSys *__restrict__ sys, const int4 *__restrict__ ta
   extern __shared__ float4 s_dyn[];
   __shared__ MixedWarpSmem sm;
   __shared__ BatchSys s_sys;
-  __shared__ double s_pd[(kEnergy && kForm == FORM_CUTOFF) ? 3 * kBatch : 1];
+  __shared__ float s_res[(kEnergy && kForm == FORM_CUTOFF) ? 3 * kBatch : 1];
   float4 *s_lj = s_dyn;
   unsigned short *s_st = reinterpret_cast<unsigned short *>(s_dyn + lj_max);
   const int lane = threadIdx.x;
@@ -105,7 +104,7 @@ k_pair_mixed_batch(const BatchSys *__restrict__ sys, const int4 *__restrict__ ta
         s_sys.g, s_sys.mc, s_st, s_sys.st_n, tk.z, tk.w, s_sys.ntypes, s_lj, tk.y,
         start + s_sys.cell0, spos, smeta, sidx, ex_start, ex, facc, N,
         partial + (size_t)t * kNacc, s_sys.pb, nullptr, sm, err,
-        (kEnergy && kForm == FORM_CUTOFF) ? s_pd : nullptr, spos_lo);
+        (kEnergy && kForm == FORM_CUTOFF) ? s_res : nullptr, spos_lo);
   }
 }
 
@@ -145,9 +144,8 @@ __global__ void k_reduce_batch(int nsys, const int *__restrict__ rows_start,
 #pragma unroll
   for (int k = 0; k < ACC_MV; k++) v[k] = __shfl_sync(0xffffffffu, acc, k);
   if (lane != 0) return;
-  const BatchSys &b = sys[s];
   double *o = out + 20 * (size_t)s;
-  o[0] = v[ACC_U] - b.c15_1 * v[ACC_Q] + b.c05_3 * v[ACC_R];
+  o[0] = v[ACC_ECOUL];
   o[1] = v[ACC_ELJ];
   const int map[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
   for (int k = 0; k < 9; k++) {

@@ -26,21 +26,18 @@ constexpr int kMaxRows = 128;         // stencil rows (dy, dz), passed by value
 constexpr int kMaxTypes = 16;         // LJ types held in shared memory
 constexpr int kMaxTypesTable = 1024;  // LJ types of a context (more than kMaxTypes:
                                       // the mixed kernel reads the table through L1)
-constexpr int kNacc = 18;             // slots per partial-sum row (ACC_MV)
+constexpr int kNacc = 16;             // slots per partial-sum row (>= ACC_MV)
 constexpr double kFixScale = 4294967296.0;          // 2^32 per force unit
 constexpr double kFixInv = 1.0 / 4294967296.0;
 
 // accumulator slot indices (partial[w][k])
 enum {
-  ACC_U = 0,    // sum q_i q_j / r        (Coulomb 1/r term, cell units)
-  ACC_Q = 1,    // sum q_i q_j            (C1 constant term)
-  ACC_R = 2,    // sum q_i q_j r^2        (C1 r^2 term)
-  ACC_ELJ = 3,  // Lennard-Jones energy
-  ACC_ECOUL = 4,// Coulomb energy, direct (FP64 kernel)
-  ACC_W = 5,    // 6 virial components xx xy xz yy yz zz (5..10)
-  ACC_MW = 11,  // 6 molecular-virial components f_a comDiff_b, a <= b (11..16)
-  ACC_PAIRS = 17,
-  ACC_MV = 18,  // number of slots in use
+  ACC_ECOUL = 0,// Coulomb energy
+  ACC_ELJ = 1,  // Lennard-Jones energy
+  ACC_W = 2,    // 6 virial components xx xy xz yy yz zz (2..7)
+  ACC_MW = 8,   // 6 molecular-virial components f_a comDiff_b, a <= b (8..13)
+  ACC_PAIRS = 14,
+  ACC_MV = 15,  // number of slots in use
 };
 static_assert(kNacc >= ACC_MV, "partial-sum rows hold every slot");
 
@@ -219,6 +216,7 @@ struct MixedConsts {   // FP32 constants in cell units
   float c15_1, c05_3, c15_3; // C1 (force path)
   float csf;                 // coulombScalingFactor
   float ey, ez;              // edge[1] / unit, edge[2] / unit (1 for cubic cells)
+  double e15, e05;           // C1 energy (FP64): 1.5 / rc_coul and 0.5 / rc_coul^3 (cell units)
   float ea, ea2pi;           // Ewald alpha and 2 alpha / sqrt(pi), per cell unit
   SwitchSpec<float> swl, swc;  // generic form: LJ and Coulomb switches
 };
@@ -587,22 +585,24 @@ __device__ __forceinline__ void mixed_task(
     const int *__restrict__ ex_start, const int2 *__restrict__ ex,
     unsigned long long *__restrict__ facc, int n, double *__restrict__ partial_row,
     const PbcRef &pb, const double *__restrict__ com, MixedWarpSmem &sm,
-    int *__restrict__ err, double *__restrict__ s_pd, const float4 *__restrict__ spos_lo) {
+    int *__restrict__ err, float *__restrict__ s_res, const float4 *__restrict__ spos_lo) {
   const int lane = threadIdx.x & 31;
   // the energy of the cutoff form is summed from FP64 distances: kEnergy
-  // launches also stage each j position, shifted into the i-cell frame, in
-  // FP64 (s_pd: this warp's 3 x kBatch doubles), rebuilt from the FP32
-  // coordinate and its rounding residual (spos_lo, sorted order)
+  // launches also stage, for each j position shifted into the i-cell frame,
+  // what the FP32 staged value lacks of the FP64 one (s_res: this warp's
+  // 3 x kBatch floats), from the FP32 coordinate, its rounding residual
+  // (spos_lo, sorted order) and the shift; FP32 staged value + that
+  // remainder = the FP64 position to ~1e-13 of a cell
   constexpr bool kExactE = kEnergy && kForm == FORM_CUTOFF;
-  double *pdx = kExactE ? s_pd : nullptr;
-  double *pdy = kExactE ? pdx + kBatch : nullptr, *pdz = kExactE ? pdx + 2 * kBatch : nullptr;
+  float *rsx = kExactE ? s_res : nullptr;
+  float *rsy = kExactE ? rsx + kBatch : nullptr, *rsz = kExactE ? rsx + 2 * kBatch : nullptr;
   const int cx = cell % g.nx;
   const int cy = (cell / g.nx) % g.ny;
   const int cz = cell / (g.nx * g.ny);
   const int cs = start[cell], ce = start[cell + 1];
 
-  KahanF kU, kQ, kR;
-  double accU = 0, accQ = 0, accR = 0, accE = 0, accP = 0;
+  KahanF kU;
+  double accU = 0, accE = 0, accP = 0;
   double w[6] = {0, 0, 0, 0, 0, 0};
   double mw[6] = {0, 0, 0, 0, 0, 0};
   const double inv_unit = 1.0 / g.unit;
@@ -639,8 +639,8 @@ __device__ __forceinline__ void mixed_task(
     // a batch holds at most kBatch / 2 candidates per lane (the list depth)
     const int batch_cap = min(kBatch, (kBatch / 2) * base);
     long long fx = 0, fy = 0, fz = 0;
-    // FP64 Coulomb sums of the cutoff form (see kExactE)
-    double eU = 0.0, eQ = 0.0, eR = 0.0;
+    // FP64 Coulomb energy sum of the cutoff form (see kExactE)
+    double eU = 0.0;
     double pid_x = 0.0, pid_y = 0.0, pid_z = 0.0;
     if (kExactE) {
       const float4 li = spos_lo[i];
@@ -823,29 +823,25 @@ __device__ __forceinline__ void mixed_task(
           const float sd = fmaf(dist, mc.c15_3, -mc.c15_1 * rinv);
           fc = inC ? __fmul_rn(ec, fmaf(r2inv, sv, -sd)) : 0.f;
           if (kEnergy) {
-            // q_j / r, q_j and q_j r^2 from the FP64 distance (the FP32 one
-            // rounds each term by ~1e-7 of q_j / rc while the C1 energy of a
-            // pair near the cutoff is far smaller); 1/r from the FP32 value
-            // and one Newton-Raphson step in FP64.  Computed for every pair
-            // and added under the cutoff by selection: no branch, so the FP64
-            // chain overlaps the force arithmetic.
-            const double ex_ = pdx[t] - pix;
-            const double ey_ = pdy[t] - piy;
-            const double ez_ = pdz[t] - piz;
+            // q_j g(r), g = 1/r - 1.5/rc + 0.5 r^2/rc^3 (the C1-switched
+            // 1/r), from the FP64 distance: the FP32 one rounds each term by
+            // ~1e-7 of q_j / rc while the energy of a pair near the cutoff
+            // is far smaller, and the total cancels to ~1e-4 of the pair
+            // magnitudes on lattice-start boxes.  1/r from the FP32 value and
+            // one Newton-Raphson step in FP64; g in FP64 keeps its absolute
+            // error at ~1e-16 / r where it vanishes at the cutoff.  Computed
+            // for every pair and added under the cutoff by selection: no
+            // branch, so the FP64 chain overlaps the force arithmetic.
+            const double ex_ = ((double)pj.x + (double)rsx[t]) - pix;
+            const double ey_ = ((double)pj.y + (double)rsy[t]) - piy;
+            const double ez_ = ((double)pj.z + (double)rsz[t]) - piz;
             const double r2d = fma(ex_, ex_, fma(ey_, ey_, ez_ * ez_));
             double rid = (double)rinv;
             rid = rid * fma(-0.5 * r2d, rid * rid, 1.5);
+            const double gd = fma(mc.e05, r2d, rid - mc.e15);
             const double qjd = inC ? (double)qj : 0.0;
-            if (own) {
-              eU = fma(qjd, rid, eU);
-              eQ += qjd;
-              eR = fma(qjd, r2d, eR);
-            } else {  // another lane's atom: weighted by its charge here
-              const double qq = qjd * (double)a4.w;
-              accU = fma(qq, rid, accU);
-              accQ += qq;
-              accR = fma(qq, r2d, accR);
-            }
+            if (own) eU = fma(qjd, gd, eU);
+            else accU = fma(qjd * (double)a4.w, gd, accU);  // weighted by q_i here
           }
         }
         f = flj + fc;
@@ -1114,11 +1110,11 @@ __device__ __forceinline__ void mixed_task(
           sm.pos[slot] = p;
           sm.meta[slot] = smeta[jg];
           sm.gidx[slot] = jg;
-          if (kExactE) {  // coordinate, residual and shift added in FP64
+          if (kExactE) {  // coordinate, residual and shift in FP64, less the staged value
             const float4 lj = spos_lo[jg];
-            pdx[slot] = ((double)a.x + (double)lj.x) + dshx;
-            pdy[slot] = ((double)a.y + (double)lj.y) + dshy;
-            pdz[slot] = ((double)a.z + (double)lj.z) + dshz;
+            rsx[slot] = (float)((((double)a.x + (double)lj.x) + dshx) - (double)p.x);
+            rsy[slot] = (float)((((double)a.y + (double)lj.y) + dshy) - (double)p.y);
+            rsz[slot] = (float)((((double)a.z + (double)lj.z) + dshz) - (double)p.z);
           }
         }
         const unsigned hm = __ballot_sync(0xffffffffu, keep && home_atom);
@@ -1153,25 +1149,18 @@ __device__ __forceinline__ void mixed_task(
       atomicAdd(&facc[2 * (size_t)n + i], (unsigned long long)fz);
     }
     if (kEnergy && active) {
-      // the three Coulomb sums are per i-atom: weight them by q_i (FP64)
+      // the own-pair Coulomb sum is per i-atom: weight it by q_i (FP64)
       const double qi = (double)pi.w;
-      if (kExactE) {
-        accU += qi * eU;
-        accQ += qi * eQ;
-        accR += qi * eR;
-      } else {
-        accU += qi * ((double)kU.s - (double)kU.c);
-        accQ += qi * ((double)kQ.s - (double)kQ.c);
-        accR += qi * ((double)kR.s - (double)kR.c);
-      }
+      if (kExactE) accU += qi * eU;
+      else accU += qi * ((double)kU.s - (double)kU.c);
     }
-    kU = KahanF(); kQ = KahanF(); kR = KahanF();
+    kU = KahanF();
   }
   if (kEnergy || kVirial) {
     double v[ACC_MV];
 #pragma unroll
     for (int k = 0; k < ACC_MV; k++) v[k] = 0.0;
-    v[ACC_U] = accU; v[ACC_Q] = accQ; v[ACC_R] = accR; v[ACC_ELJ] = accE; v[ACC_PAIRS] = accP;
+    v[ACC_ECOUL] = accU; v[ACC_ELJ] = accE; v[ACC_PAIRS] = accP;
 #pragma unroll
     for (int k = 0; k < 6; k++) { v[ACC_W + k] = w[k]; v[ACC_MW + k] = mw[k]; }
 #pragma unroll
@@ -1191,9 +1180,10 @@ __device__ __forceinline__ void mixed_task(
 // the LJ table (ntypes^2 float4, cutoff and generic forms) and then the
 // stencil offsets.  Forces-only launches are held to 72 registers, so that
 // shared memory (~8.4 KB per block with the per-block reserve) sets the
-// residency at 27 blocks per SM; energy launches (11.5 KB: 19 blocks) to the
-// ~96 registers that still fit 20 without spills; the virial variants keep
-// the compiler's choice.
+// residency at 27 blocks per SM; energy launches (~10 KB) to the registers
+// of 19 blocks per SM (measured on the 41k water box: 19, 20, 21, 22 blocks
+// took 167, 171, 171, 179 us, the higher counts through spilled registers);
+// the virial variants keep the compiler's choice.
 constexpr int kMaxCellSlots = 8;
 constexpr int kEnergyCellSlots = 4;  // energy / virial launches (the ones with partial rows)
 
@@ -1201,7 +1191,10 @@ constexpr int kEnergyCellSlots = 4;  // energy / virial launches (the ones with 
 // kGlobalLj: the LJ table (more than kMaxTypes types) is read from global
 // memory through L1 instead of being staged in shared memory.
 template <int kForm, bool kEnergy, bool kVirial, bool kMolVir, bool kGlobalLj = false>
-__global__ void __launch_bounds__(32, kVirial ? 1 : (kEnergy ? 19 : 26))
+#ifndef PMB200_ENERGY_BLOCKS
+#define PMB200_ENERGY_BLOCKS 19  // resident blocks per SM asked of energy launches
+#endif
+__global__ void __launch_bounds__(32, kVirial ? 1 : (kEnergy ? PMB200_ENERGY_BLOCKS : 26))
 k_pair_mixed(GridParams g, MixedConsts mc, const HalfStencil st, int ntypes, const float4 *__restrict__ lj32,
              const int *__restrict__ start, const float4 *__restrict__ spos,
              const int2 *__restrict__ smeta, const int *__restrict__ sidx,
@@ -1211,7 +1204,7 @@ k_pair_mixed(GridParams g, MixedConsts mc, const HalfStencil st, int ntypes, con
              int slots, const float4 *__restrict__ spos_lo, int cell0) {
   extern __shared__ float4 s_dyn[];
   __shared__ MixedWarpSmem sm;
-  __shared__ double s_pd[(kEnergy && kForm == FORM_CUTOFF) ? 3 * kBatch : 1];
+  __shared__ float s_res[(kEnergy && kForm == FORM_CUTOFF) ? 3 * kBatch : 1];
   constexpr bool kLj = kForm == FORM_CUTOFF || kForm == FORM_GENERIC;
   const int nlj = (kLj && !kGlobalLj) ? ntypes * ntypes : 0;
   float4 *s_lj = s_dyn;
@@ -1231,7 +1224,7 @@ k_pair_mixed(GridParams g, MixedConsts mc, const HalfStencil st, int ntypes, con
       g, mc, s_st, st.ncells, blockIdx.x % slots, slots, ntypes, kGlobalLj ? lj32 : s_lj, cell,
       start,
       spos, smeta, sidx, ex_start, ex, facc, n, partial + (size_t)blockIdx.x * kNacc, pb, com,
-      sm, err, s_pd, spos_lo);
+      sm, err, s_res, spos_lo);
 }
 
 // Blocks per i-cell of a k_pair_mixed launch: 8 for forces-only launches
@@ -1740,9 +1733,8 @@ __global__ void k_reduce1(int ncell, const double *__restrict__ partial,
   if (t < ACC_MV) red[blockIdx.x * ACC_MV + t] = sh[t][0];
 }
 
-__global__ void k_reduce2(int nred, const double *__restrict__ red, int mixed, double visit,
-                          double c15_1, double c05_3, double *__restrict__ out,
-                          double *__restrict__ pairs_out) {
+__global__ void k_reduce2(int nred, const double *__restrict__ red, double visit,
+                          double *__restrict__ out, double *__restrict__ pairs_out) {
   // all threads stage the block sums; then each of ACC_MV threads adds one
   // column in block order (fixed order: deterministic)
   __shared__ double sh[kRedBlocks * ACC_MV];
@@ -1759,9 +1751,7 @@ __global__ void k_reduce2(int nred, const double *__restrict__ red, int mixed, d
   double r[ACC_MV];
   for (int k = 0; k < ACC_MV; k++) r[k] = col[k];
   // visit = 1 / (times each pair was evaluated)
-  const double ec = mixed ? visit * (r[ACC_U] - c15_1 * r[ACC_Q] + c05_3 * r[ACC_R])
-                          : visit * r[ACC_ECOUL];
-  out[0] = ec;
+  out[0] = visit * r[ACC_ECOUL];
   out[1] = visit * r[ACC_ELJ];
   // symmetric atomic virial from xx xy xz yy yz zz
   // Both tables hold xx xy xz yy yz zz.  The reference stores the molecular
