@@ -80,6 +80,8 @@ struct pmb200_ctx {
   float4 *d_rel_lo = nullptr, *d_spos_lo = nullptr;  // FP32 coordinate residuals
   double4 *d_rel64 = nullptr, *d_spos64 = nullptr;
   int2 *d_smeta = nullptr;
+  // force accumulator, sorted order: [3][n] 2^-32 quanta (mixed) or [6][n]
+  // two-word fixed point (FP64 evaluation kernel)
   unsigned long long *d_facc = nullptr;
   // d_count holds zeros between evaluations (k_scan clears it after reading);
   // false after a launch sequence broke off, when the next build clears it
@@ -383,7 +385,7 @@ int ensure_atom_buffers(pmb200_ctx *c) {
   CK(dalloc(c->d_rel64, n));
   CK(dalloc(c->d_spos64, n));
   CK(dalloc(c->d_smeta, n));
-  CK(dalloc(c->d_facc, 3 * n));
+  CK(dalloc(c->d_facc, 6 * n));
   CK(dalloc(c->d_hpos, 3 * n));
   CK(dalloc(c->d_hfrc, 3 * n));
   c->n_alloc = c->n;
@@ -483,6 +485,31 @@ void launch_pair_fp64(pmb200_ctx *c, unsigned flags, double *d_forces, int accum
 #undef PMB_FP64_LAUNCH
 }
 
+// The FP64 evaluation kernel (half shell, kFp64Slots warps per i-cell) into
+// the sorted-order accumulator d_facc (two-word fixed point, cleared by the
+// cell build).
+constexpr int kFp64Slots = kEnergyCellSlots;
+template <int F>
+void launch_pair_fp64_half(pmb200_ctx *c, unsigned flags, cudaStream_t st) {
+  const GridParams &g = c->g;
+  const bool energy = (flags & PMB200_ENERGY) != 0;
+  const bool virial = (flags & (PMB200_VIRIAL | PMB200_MOLVIRIAL)) != 0;
+  const bool molvir = (flags & PMB200_MOLVIRIAL) != 0;
+  const unsigned blocks = (unsigned)g.ncell * kFp64Slots;
+  if (blocks == 0) return;
+#define PMB_FP64H_LAUNCH(E, V, M)                                                          \
+  k_pair_fp64_half<F, E, V, M><<<blocks, 32, 0, st>>>(                                    \
+      g, c->fc, c->half, kFp64Slots, c->ntypes, c->d_lj64, c->d_start, c->d_spos64,         \
+      c->d_smeta, c->d_sidx, c->d_ex_start, c->d_ex, c->d_facc, c->n, c->d_partial, c->pb,  \
+      c->d_com, c->d_err)
+  if (molvir) PMB_FP64H_LAUNCH(true, true, true);
+  else if (energy && virial) PMB_FP64H_LAUNCH(true, true, false);
+  else if (energy) PMB_FP64H_LAUNCH(true, false, false);
+  else if (virial) PMB_FP64H_LAUNCH(false, true, false);
+  else PMB_FP64H_LAUNCH(false, false, false);
+#undef PMB_FP64H_LAUNCH
+}
+
 // Zeroes d_count when a launch sequence broke off after using it; a captured
 // graph relies on its previous run having left it cleared.
 int ensure_clear(pmb200_ctx *c, cudaStream_t st) {
@@ -555,11 +582,12 @@ int build_stencils(pmb200_ctx *c, double rc, std::vector<Row> &rows, HalfStencil
 // scatter, in-cell rank order), producing the cell-unit FP32 copies (mixed)
 // or the Angstrom FP64 copies of the sorted positions; lo: also the FP32
 // coordinates' rounding residuals (energy evaluations of the cutoff form).
-// clear3: an accumulator of 3n entries the build zeroes on the way (or null).
+// clear: an accumulator of nclear x n entries the build zeroes on the way
+// (or null).
 // After the first kernel each one is launched as a programmatic dependent of
 // the one before it.
 void launch_cell_build(pmb200_ctx *c, const double *d_pos, bool mixed, bool lo,
-                       cudaStream_t st, unsigned long long *clear3 = nullptr) {
+                       cudaStream_t st, unsigned long long *clear = nullptr, int nclear = 3) {
   const int n = c->n;
   const GridParams &g = c->g;
   if (!c->count_zero) cudaMemsetAsync(c->d_count, 0, sizeof(int) * g.ncell, st);
@@ -568,7 +596,8 @@ void launch_cell_build(pmb200_ctx *c, const double *d_pos, bool mixed, bool lo,
   if (n > 0)
     launch_k(k_cell_index, nb, 256, 0, st, false, n, d_pos, g, c->d_cell_of, c->d_count,
              c->d_slot, mixed ? c->d_rel32 : nullptr, mixed ? nullptr : c->d_rel64, c->d_q,
-             (float)(1.0 / std::sqrt(g.unit)), c->d_err, lo ? c->d_rel_lo : nullptr, clear3);
+             (float)(1.0 / std::sqrt(g.unit)), c->d_err, lo ? c->d_rel_lo : nullptr, clear,
+             nclear);
   launch_k(k_scan, 1, 1024, 1024 * sizeof(int), st, n > 0, g.ncell, c->d_count, c->d_start);
   c->count_zero = cudaPeekAtLastError() == cudaSuccess;
   if (n > 0)
@@ -592,10 +621,9 @@ int launch_eval(pmb200_ctx *c, const double *d_pos, double *d_forces, double *d_
   // the cell build clears the accumulator on the way (still in L2 when the
   // pair kernel adds to it), so that the pair kernel follows the build's last
   // kernel directly
-  launch_cell_build(c, d_pos, mixed, mixed && energy && c->form == FORM_CUTOFF, st,
-                    mixed ? c->d_facc : nullptr);
+  launch_cell_build(c, d_pos, mixed, mixed && energy && c->form == FORM_CUTOFF, st, c->d_facc,
+                    mixed ? 3 : 6);
   CK(cudaGetLastError());
-  const int blocks = (g.ncell + 3) / 4;
   if (molvir && c->nmol > 0)
     k_com<<<(c->nmol + 127) / 128, 128, 0, st>>>(c->nmol, c->d_mstart, c->d_matoms, c->d_mass,
                                                   d_pos, c->d_com);
@@ -622,27 +650,25 @@ int launch_eval(pmb200_ctx *c, const double *d_pos, double *d_forces, double *d_
                (const unsigned long long *)c->d_facc, (const int *)c->d_sidx, fscale * kFixInv,
                accumulate, d_forces);
   } else {
-    if (c->form == FORM_GENERIC)
-      launch_pair_fp64<FORM_GENERIC>(c, flags, d_forces, accumulate, blocks, st);
-    else if (c->form == FORM_EWALD_POLY5)
-      launch_pair_fp64<FORM_EWALD_POLY5>(c, flags, d_forces, accumulate, blocks, st);
-    else if (c->form == FORM_EWALD_EXACT)
-      launch_pair_fp64<FORM_EWALD_EXACT>(c, flags, d_forces, accumulate, blocks, st);
-    else
-      launch_pair_fp64<FORM_CUTOFF>(c, flags, d_forces, accumulate, blocks, st);
+    if (c->form == FORM_GENERIC) launch_pair_fp64_half<FORM_GENERIC>(c, flags, st);
+    else if (c->form == FORM_EWALD_POLY5) launch_pair_fp64_half<FORM_EWALD_POLY5>(c, flags, st);
+    else if (c->form == FORM_EWALD_EXACT) launch_pair_fp64_half<FORM_EWALD_EXACT>(c, flags, st);
+    else launch_pair_fp64_half<FORM_CUTOFF>(c, flags, st);
+    if (n > 0)
+      k_finalize64<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, c->d_facc, c->d_sidx,
+                                                                 accumulate, d_forces);
   }
   CK(cudaGetLastError());
   if (timed) CK(cudaEventRecord(c->ev1, st));
   if (energy || virial) {
-    // partial rows: one per (cell, slot) warp of the mixed kernel, one per
-    // cell of the FP64 kernel
-    // (energy / virial launches of the mixed kernel use the slot count of
-    // mixed_cell_slots(true, ...))
+    // partial rows: one per (cell, slot) warp (energy / virial launches of
+    // the mixed kernel use the slot count of mixed_cell_slots(true, ...));
+    // both kernels visit each pair once
     k_reduce1<<<kRedBlocks, 256, 0, st>>>(
-        mixed ? g.ncell * mixed_cell_slots(true, n, g.ncell) : g.ncell, c->d_partial, c->d_red);
-    // the mixed kernel visits each pair once, the FP64 kernel twice
-    k_reduce2<<<1, 256, 0, st>>>(kRedBlocks, c->d_red, mixed ? 1.0 : 0.5,
-                                d_out ? d_out : c->d_out, c->d_pairs);
+        g.ncell * (mixed ? mixed_cell_slots(true, n, g.ncell) : kFp64Slots), c->d_partial,
+        c->d_red);
+    k_reduce2<<<1, 256, 0, st>>>(kRedBlocks, c->d_red, 1.0, d_out ? d_out : c->d_out,
+                                c->d_pairs);
     CK(cudaGetLastError());
   }
   return PMB200_OK;

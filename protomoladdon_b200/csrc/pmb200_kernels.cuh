@@ -338,18 +338,19 @@ __device__ __forceinline__ bool locate_cell(const double *xin, const GridParams 
   return ok;
 }
 
-// clear3: an accumulator of 3n entries zeroed on the way (or null).
+// clear: an accumulator of nclear x n entries zeroed on the way (or null).
 __global__ void k_cell_index(int n, const double *__restrict__ pos, GridParams g,
                              int *__restrict__ cell_of, int *__restrict__ cell_count,
                              int *__restrict__ slot, float4 *__restrict__ rel32,
                              double4 *__restrict__ rel64, const double *__restrict__ q,
                              float qscale32, int *__restrict__ err,
                              float4 *__restrict__ rel_lo,
-                             unsigned long long *__restrict__ clear3 = nullptr) {
+                             unsigned long long *__restrict__ clear = nullptr, int nclear = 3) {
   pdl_trigger();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  if (clear3) clear3[i] = clear3[(size_t)n + i] = clear3[2 * (size_t)n + i] = 0;
+  if (clear)
+    for (int k = 0; k < nclear; k++) clear[(size_t)k * n + i] = 0;
   int c[3];
   double r[3];
   if (!locate_cell(pos + 3 * (size_t)i, g, c, r)) atomicOr(err, 1);
@@ -1260,6 +1261,108 @@ __global__ void k_finalize(int n, const unsigned long long *__restrict__ facc,
   }
 }
 
+// The reference's per-pair arithmetic in FP64 for a pair at squared
+// distance r2 (A^2): OneAtomPairTwo::doOneAtomPair's LJ(C2) + Coulomb(C1)
+// (OneAtomPairTwo.h:57-125) for the cutoff form, the generic switches and
+// the tabulated LJ (OneAtomPair.h:56-111) for the generic form, the
+// real-space Ewald term otherwise.  ti = type_i * ntypes, tj = type_j, kind
+// the pair's exclusion class (1: modified), qi / qj the scaled charges.  Out:
+// f = force / r, e1 the LJ energy, e2 the Coulomb energy.  Shared by the FP64
+// kernels so that they round every pair alike.
+template <int kForm>
+__device__ __forceinline__ void fp64_pair(const Fp64Consts &mc, const double4 *__restrict__ lj64,
+                                          int ti, int tj, int kind, double r2, double qi,
+                                          double qj, double &f, double &e1, double &e2) {
+  e1 = 0.0;
+  e2 = 0.0;
+  if constexpr (kForm == FORM_GENERIC) {
+    f = 0.0;
+    const double rd2 = 1.0 / r2;
+    const double rinv = sqrt(rd2);
+    if (mc.ljtab) {  // no Coulomb term beside the table
+      const double4 p = lj64[ti + tj];
+      lj_table_eval(mc.ljtab, mc.tfirst, mc.tlast, r2, kind == 1 ? p.z : p.x,
+                    kind == 1 ? p.w : p.y, e1, f);
+    } else if (mc.swl.kind != SW_OFF) {
+      const double4 p = lj64[ti + tj];
+      const double A = kind == 1 ? p.z : p.x;
+      const double B = kind == 1 ? p.w : p.y;
+      const double r6 = rd2 * rd2 * rd2;
+      const double r12 = r6 * r6;
+      const double r6B = B * r6, r12A = A * r12;
+      e1 = r12A - r6B;
+      double f1 = 12.0 * r12A * rd2 - 6.0 * r6B * rd2;
+      double S, dS;
+      switch_eval(mc.swl, r2, rinv, S, dS);
+      f1 = f1 * S - e1 * dS;
+      e1 = e1 * S;
+      f += f1;
+    }
+    if (mc.swc.kind != SW_OFF) {
+      e2 = qi * qj * rinv;
+      if (kind == 1) e2 *= mc.csf;
+      double f2 = e2 * rd2;
+      double S, dS;
+      switch_eval(mc.swc, r2, rinv, S, dS);
+      f2 = f2 * S - e2 * dS;
+      e2 = e2 * S;
+      f += f2;
+    }
+  } else if constexpr (kForm != FORM_CUTOFF) {
+    // NonbondedFullEwaldSystemForce::realTerm's pair arithmetic
+    // (NonbondedFullEwaldSystemForce.h:803-823)
+    const double r = sqrt(r2);
+    double qq = qi * qj;
+    if (kind == 1) qq *= mc.csf;
+    if constexpr (kForm == FORM_EWALD_POLY5) {
+      const double rr = 1.0 / r;
+      const double ar = mc.ea * r;
+      const double e = qq * exp(-ar * ar);
+      const double t = 1.0 / (1.0 + kAsP * ar);
+      const double poly =
+          (t) * (kAsA1 + (t) * (kAsA2 + (t) * (kAsA3 + (t) * (kAsA4 + (t) * kAsA5))));
+      e2 = poly * e * rr;
+      f = ((e2 + mc.ea2pi * e) * rr * rr);
+    } else {
+      const double a = erfc(mc.ea * r) / r;
+      e2 = qq * a;
+      f = qq * (a + mc.ea2pi * exp(-mc.ea2 * r2)) / r2;
+    }
+  } else {
+    const double rd2 = 1.0 / r2;
+    const double4 p = lj64[ti + tj];
+    const double A = kind == 1 ? p.z : p.x;
+    const double B = kind == 1 ? p.w : p.y;
+    const double r6 = rd2 * rd2 * rd2;
+    const double r12 = r6 * r6;
+    const double r6B = B * r6, r12A = A * r12;
+    e1 = r12A - r6B;
+    double f1 = 12.0 * r12A * rd2 - 6.0 * r6B * rd2;
+    double sv = 1.0, sd = 0.0;
+    if (r2 > mc.rclj2) sv = 0.0;
+    else if (r2 >= mc.ron2) {
+      const double c2 = mc.rclj2 - r2;
+      const double c4 = c2 * (mc.s2 + 2.0 * r2);
+      sv = mc.s1 * (c2 * c4);
+      sd = mc.s3 * (c2 * c2 - c4);
+    }
+    f1 = f1 * sv - e1 * sd;
+    e1 = e1 * sv;
+    e2 = qi * qj * sqrt(rd2);
+    if (kind == 1) e2 *= mc.csf;
+    double f2 = e2 * rd2;
+    if (r2 > mc.rcc2) { e2 = 0.0; f2 = 0.0; }
+    else {
+      const double dist = sqrt(r2);
+      const double v = 1.0 - dist * (mc.c15_1 - r2 * mc.c05_3);
+      const double dv = -mc.c15_1 / dist + dist * mc.c15_3;
+      f2 = f2 * v - e2 * dv;
+      e2 = e2 * v;
+    }
+    f = f1 + f2;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Plain FP64 pair kernel: the same cell-pair walk and lane mapping as the
 // mixed kernel, with the reference's FP64 per-pair arithmetic
@@ -1332,93 +1435,8 @@ k_pair_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes, const dou
             kind = excl_kind(ex, elo, ehi, sidx[j]);
             if (kind == 2) continue;
           }
-          double f, e1 = 0.0, e2 = 0.0;
-          if constexpr (kForm == FORM_GENERIC) {
-            f = 0.0;
-            const double rd2 = 1.0 / r2;
-            const double rinv = sqrt(rd2);
-            if (mc.ljtab) {  // no Coulomb term beside the table
-              const double4 p = lj64[ti + mj.x];
-              lj_table_eval(mc.ljtab, mc.tfirst, mc.tlast, r2, kind == 1 ? p.z : p.x,
-                            kind == 1 ? p.w : p.y, e1, f);
-            } else if (mc.swl.kind != SW_OFF) {
-              const double4 p = lj64[ti + mj.x];
-              const double A = kind == 1 ? p.z : p.x;
-              const double B = kind == 1 ? p.w : p.y;
-              const double r6 = rd2 * rd2 * rd2;
-              const double r12 = r6 * r6;
-              const double r6B = B * r6, r12A = A * r12;
-              e1 = r12A - r6B;
-              double f1 = 12.0 * r12A * rd2 - 6.0 * r6B * rd2;
-              double S, dS;
-              switch_eval(mc.swl, r2, rinv, S, dS);
-              f1 = f1 * S - e1 * dS;
-              e1 = e1 * S;
-              f += f1;
-            }
-            if (mc.swc.kind != SW_OFF) {
-              e2 = pi.w * pj.w * rinv;
-              if (kind == 1) e2 *= mc.csf;
-              double f2 = e2 * rd2;
-              double S, dS;
-              switch_eval(mc.swc, r2, rinv, S, dS);
-              f2 = f2 * S - e2 * dS;
-              e2 = e2 * S;
-              f += f2;
-            }
-          } else if constexpr (kForm != FORM_CUTOFF) {
-            // NonbondedFullEwaldSystemForce::realTerm's pair arithmetic
-            // (NonbondedFullEwaldSystemForce.h:803-823)
-            const double r = sqrt(r2);
-            double qq = pi.w * pj.w;
-            if (kind == 1) qq *= mc.csf;
-            if constexpr (kForm == FORM_EWALD_POLY5) {
-              const double rr = 1.0 / r;
-              const double ar = mc.ea * r;
-              const double e = qq * exp(-ar * ar);
-              const double t = 1.0 / (1.0 + kAsP * ar);
-              const double poly =
-                  (t) * (kAsA1 + (t) * (kAsA2 + (t) * (kAsA3 + (t) * (kAsA4 + (t) * kAsA5))));
-              e2 = poly * e * rr;
-              f = ((e2 + mc.ea2pi * e) * rr * rr);
-            } else {
-              const double a = erfc(mc.ea * r) / r;
-              e2 = qq * a;
-              f = qq * (a + mc.ea2pi * exp(-mc.ea2 * r2)) / r2;
-            }
-          } else {
-          const double rd2 = 1.0 / r2;
-          const double4 p = lj64[ti + mj.x];
-          const double A = kind == 1 ? p.z : p.x;
-          const double B = kind == 1 ? p.w : p.y;
-          const double r6 = rd2 * rd2 * rd2;
-          const double r12 = r6 * r6;
-          const double r6B = B * r6, r12A = A * r12;
-          e1 = r12A - r6B;
-          double f1 = 12.0 * r12A * rd2 - 6.0 * r6B * rd2;
-          double sv = 1.0, sd = 0.0;
-          if (r2 > mc.rclj2) sv = 0.0;
-          else if (r2 >= mc.ron2) {
-            const double c2 = mc.rclj2 - r2;
-            const double c4 = c2 * (mc.s2 + 2.0 * r2);
-            sv = mc.s1 * (c2 * c4);
-            sd = mc.s3 * (c2 * c2 - c4);
-          }
-          f1 = f1 * sv - e1 * sd;
-          e1 = e1 * sv;
-          e2 = pi.w * pj.w * sqrt(rd2);
-          if (kind == 1) e2 *= mc.csf;
-          double f2 = e2 * rd2;
-          if (r2 > mc.rcc2) { e2 = 0.0; f2 = 0.0; }
-          else {
-            const double dist = sqrt(r2);
-            const double v = 1.0 - dist * (mc.c15_1 - r2 * mc.c05_3);
-            const double dv = -mc.c15_1 / dist + dist * mc.c15_3;
-            f2 = f2 * v - e2 * dv;
-            e2 = e2 * v;
-          }
-          f = f1 + f2;
-          }
+          double f, e1, e2;
+          fp64_pair<kForm>(mc, lj64, ti, mj.x, kind, r2, pi.w, pj.w, f, e1, e2);
           fx -= ddx * f; fy -= ddy * f; fz -= ddz * f;
           if (kEnergy) { accE += e1; accC += e2; accP += 1.0; }
           if (kVirial) {
@@ -1459,6 +1477,228 @@ k_pair_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes, const dou
       double s = warp_sum_mask(v[k], 32);
       if (lane == 0) partial[(size_t)cell * kNacc + k] = s;
     }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FP64 pair kernel on the half shell (the evaluation kernel of FP64
+// contexts): the mixed kernel's task split -- one warp per block, each warp
+// one i-cell and one share of the half-shell cell offsets (the same
+// HalfStencil; home-cell pairs taken for i < j) -- with fp64_pair's
+// arithmetic and each pair evaluated once, its force added to both atoms
+// (Newton's third law, as NonbondedCutoffForce's cell-pair loop does).  No
+// candidate culling or list building: the warp stages the atoms of its
+// cells (positions in the i-cell frame, FP64) kB64 at a time in shared
+// memory and every i atom meets every staged atom.  The lanes of i atom ia
+// take the batch in blocks of L entries, block (ia + k) mod nsteps at step k,
+// so that at each step no two lanes touch the same staged atom: j forces are
+// summed in shared memory without atomics, in step order, and i forces in
+// registers.  Both reach the global accumulator as exact two-word
+// fixed-point numbers (fix2_split: multiples of 2^-20 and of 2^-68
+// kcal/mol/A), whose integer sums are the same in any order: the results are
+// deterministic.  Accumulator acc[6][n] int64, sorted order, words {hi x,
+// hi y, hi z, lo x, lo y, lo z}.  Energy and virial partials: one row per
+// block.
+constexpr int kB64 = 64;
+constexpr double kFix2Hi = 1048576.0;            // 2^20
+constexpr double kFix2Lo = 281474976710656.0;    // 2^48 (below 2^-20)
+constexpr double kFix2Max = 6.0e10;              // < 2^36 kcal/mol/A
+struct Fp64WarpSmem {
+  double4 pos[kB64];  // staged j: position in the i-cell frame (A), charge
+  int2 meta[kB64];    // type, molecule
+  int jidx[kB64];     // sorted index; bit 31: an atom of the home cell
+  double jf[3][kB64]; // j force sums of the batch
+};
+
+// v = (hi + lo 2^-48) 2^-20 exactly: hi = rint(v 2^20); the remainder
+// v 2^20 - hi (exact, |.| <= 1/2) scaled by 2^48 and rounded (error <= 2^-69
+// kcal/mol/A).  A summed force component of kFix2Max or more (or not finite)
+// makes the evaluation report a device error: below it every word sum stays
+// within int64 for up to 2^13 such contributions.
+__device__ __forceinline__ void fix2_add(unsigned long long *__restrict__ acc, size_t n, size_t j,
+                                         int q, double v, int *__restrict__ err) {
+  if (!(fabs(v) < kFix2Max)) {
+    atomicOr(err, 2);
+    return;
+  }
+  const double s = v * kFix2Hi;
+  const double h = rint(s);
+  const long long hi = (long long)h;
+  const long long lo = __double2ll_rn((s - h) * kFix2Lo);
+  if (hi) atomicAdd(&acc[(size_t)q * n + j], (unsigned long long)hi);
+  if (lo) atomicAdd(&acc[(size_t)(3 + q) * n + j], (unsigned long long)lo);
+}
+
+template <int kForm, bool kEnergy, bool kVirial, bool kMolVir>
+__global__ void __launch_bounds__(32)
+k_pair_fp64_half(GridParams g, Fp64Consts mc, const HalfStencil st, int slots, int ntypes,
+                 const double4 *__restrict__ lj64, const int *__restrict__ start,
+                 const double4 *__restrict__ spos, const int2 *__restrict__ smeta,
+                 const int *__restrict__ sidx, const int *__restrict__ ex_start,
+                 const int2 *__restrict__ ex, unsigned long long *__restrict__ acc, int n,
+                 double *__restrict__ partial, const PbcRef pb, const double *__restrict__ com,
+                 int *__restrict__ err) {
+  __shared__ Fp64WarpSmem sm;
+  const int lane = threadIdx.x;
+  const int cell = (int)(blockIdx.x / slots), slot = (int)(blockIdx.x % slots);
+  if (cell >= g.ncell) return;  // uniform per block
+  const int cx = cell % g.nx;
+  const int cy = (cell / g.nx) % g.ny;
+  const int cz = cell / (g.nx * g.ny);
+  const int cs = start[cell], ce = start[cell + 1];
+  for (int t = lane; t < kB64; t += 32) sm.jf[0][t] = sm.jf[1][t] = sm.jf[2][t] = 0.0;
+  double accC = 0, accE = 0, accP = 0;
+  double w[6] = {0, 0, 0, 0, 0, 0};
+  double mw[6] = {0, 0, 0, 0, 0, 0};
+  for (int c0 = cs; c0 < ce; c0 += 32) {
+    const int m = min(32, ce - c0);
+    const int L = lanes_per_atom(m);
+    const int ia = lane / L;
+    const int sub = lane % L;
+    const bool active = ia < m;
+    const int i = c0 + (active ? ia : 0);
+    const double4 pi = spos[i];
+    const int2 mi = smeta[i];
+    const int oi = sidx[i];
+    const int elo = ex_start[oi], ehi = ex_start[oi + 1];
+    const int ti = mi.x * ntypes;
+    double fx = 0, fy = 0, fz = 0;
+    double Ri[3] = {0.0, 0.0, 0.0};
+    if (kMolVir)
+      for (int k = 0; k < 3; k++) Ri[k] = com[3 * (size_t)mi.y + k];
+    int nb = 0;
+    // every i atom of the chunk against the nb staged atoms, then the j
+    // forces out and the batch emptied
+    auto process = [&]() {
+      __syncwarp();
+      const int nblk = (nb + L - 1) / L;
+      const int nsteps = max(nblk, m);  // >= m: the atoms' blocks differ at every step
+      for (int k = 0; k < nsteps; k++) {
+        int blk = ia + k;
+        if (blk >= nsteps) blk -= nsteps;
+        const int t = blk * L + sub;
+        if (active && t < nb) {
+          const int jw = sm.jidx[t];
+          const int j = jw & 0x7fffffff;
+          const double4 pj = sm.pos[t];
+          const double ddx = pj.x - pi.x;
+          const double ddy = pj.y - pi.y;
+          const double ddz = pj.z - pi.z;
+          const double r2 = ddx * ddx + ddy * ddy + ddz * ddz;
+          const int2 mj = sm.meta[t];
+          int kind = (jw < 0 && j <= i) ? 2 : 0;  // home cell: pairs i < j only
+          if (kind == 0 && r2 <= mc.cut2 && mj.y == mi.y) kind = excl_kind(ex, elo, ehi, sidx[j]);
+          if (kind != 2 && r2 <= mc.cut2) {
+            double f, e1, e2;
+            fp64_pair<kForm>(mc, lj64, ti, mj.x, kind, r2, pi.w, pj.w, f, e1, e2);
+            const double fxv = ddx * f, fyv = ddy * f, fzv = ddz * f;
+            fx -= fxv; fy -= fyv; fz -= fzv;
+            sm.jf[0][t] += fxv;
+            sm.jf[1][t] += fyv;
+            sm.jf[2][t] += fzv;
+            if (kEnergy) { accE += e1; accC += e2; accP += 1.0; }
+            if (kVirial) {
+              w[0] += fxv * ddx; w[1] += fxv * ddy; w[2] += fxv * ddz;
+              w[3] += fyv * ddy; w[4] += fyv * ddz; w[5] += fzv * ddz;
+              if (kMolVir && mj.y != mi.y) {
+                double cd[3];
+                for (int qq = 0; qq < 3; qq++) cd[qq] = com[3 * (size_t)mj.y + qq] - Ri[qq];
+                ref_min_image(pb, cd);
+                mw[0] += fxv * cd[0]; mw[1] += fxv * cd[1]; mw[2] += fxv * cd[2];
+                mw[3] += fyv * cd[1]; mw[4] += fyv * cd[2]; mw[5] += fzv * cd[2];
+              }
+            }
+          }
+        }
+        __syncwarp();
+      }
+      for (int t = lane; t < nb; t += 32) {
+        const size_t j = (size_t)(sm.jidx[t] & 0x7fffffff);
+#pragma unroll
+        for (int qq = 0; qq < 3; qq++) {
+          const double v = sm.jf[qq][t];
+          if (v != 0.0) fix2_add(acc, (size_t)n, j, qq, v, err);
+          sm.jf[qq][t] = 0.0;
+        }
+      }
+      nb = 0;
+      __syncwarp();
+    };
+    for (int q = slot; q < st.ncells; q += slots) {
+      const unsigned o = st.off[q];
+      const int dx = (int)(o & 31u) - 8, dy = (int)((o >> 5) & 31u) - 8,
+                dz = (int)((o >> 10) & 31u) - 8;
+      const int homebit = (dx | dy | dz) == 0 ? (int)0x80000000u : 0;
+      int jx = cx + dx, jy = cy + dy, jz = cz + dz;
+      if (g.periodic) {
+        // one wrap suffices: offsets reach at most ceil(rc / edge) <= n / 2
+        jx += jx < 0 ? g.nx : (jx >= g.nx ? -g.nx : 0);
+        jy += jy < 0 ? g.ny : (jy >= g.ny ? -g.ny : 0);
+        jz += jz < 0 ? g.nz : (jz >= g.nz ? -g.nz : 0);
+      } else if (jx < 0 || jx >= g.nx || jy < 0 || jy >= g.ny || jz < 0 || jz >= g.nz) {
+        continue;  // uniform per warp
+      }
+      const int jc = (jz * g.ny + jy) * g.nx + jx;
+      const int js = start[jc], cnt = start[jc + 1] - js;
+      double sx, sy, sz;  // the neighbour cell's shift (A)
+      cell_shift(g, g.ec, 1.0, dx, dy, dz, sx, sy, sz);
+      for (int f0 = 0; f0 < cnt;) {
+        const int take = min(min(cnt - f0, kB64 - nb), 32);
+        if (lane < take) {
+          const int j = js + f0 + lane;
+          double4 p = spos[j];
+          p.x += sx; p.y += sy; p.z += sz;
+          sm.pos[nb + lane] = p;
+          sm.meta[nb + lane] = smeta[j];
+          sm.jidx[nb + lane] = j | homebit;
+        }
+        nb += take;
+        f0 += take;
+        if (nb == kB64) process();
+      }
+    }
+    if (nb > 0) process();
+    for (int off = 1; off < L; off <<= 1) {
+      fx += __shfl_xor_sync(0xffffffffu, fx, off);
+      fy += __shfl_xor_sync(0xffffffffu, fy, off);
+      fz += __shfl_xor_sync(0xffffffffu, fz, off);
+    }
+    if (active && sub == 0) {
+      fix2_add(acc, (size_t)n, (size_t)i, 0, fx, err);
+      fix2_add(acc, (size_t)n, (size_t)i, 1, fy, err);
+      fix2_add(acc, (size_t)n, (size_t)i, 2, fz, err);
+    }
+  }
+  if (kEnergy || kVirial) {
+    double v[ACC_MV];
+#pragma unroll
+    for (int k = 0; k < ACC_MV; k++) v[k] = 0.0;
+    v[ACC_ECOUL] = accC; v[ACC_ELJ] = accE; v[ACC_PAIRS] = accP;
+#pragma unroll
+    for (int k = 0; k < 6; k++) { v[ACC_W + k] = w[k]; v[ACC_MW + k] = mw[k]; }
+#pragma unroll
+    for (int k = 0; k < ACC_MV; k++) {
+      const double sum = warp_sum_mask(v[k], 32);
+      if (lane == 0) partial[(size_t)blockIdx.x * kNacc + k] = sum;
+    }
+  }
+}
+
+// The FP64 half-shell kernel's accumulator (sorted order, fix2 words
+// [6][n]) -> forces in the caller's atom order, accumulated or overwritten.
+__global__ void k_finalize64(int n, const unsigned long long *__restrict__ acc,
+                             const int *__restrict__ sidx, int accumulate,
+                             double *__restrict__ forces) {
+  pdl_wait();
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  double *fo = forces + 3 * (size_t)sidx[j];
+#pragma unroll
+  for (int q = 0; q < 3; q++) {
+    const double hi = (double)(long long)acc[(size_t)q * n + j];
+    const double lo = (double)(long long)acc[(size_t)(3 + q) * n + j];
+    const double v = (hi + lo * (1.0 / kFix2Lo)) * (1.0 / kFix2Hi);
+    fo[q] = accumulate ? fo[q] + v : v;
   }
 }
 
