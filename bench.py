@@ -457,7 +457,11 @@ def run_ours(args):
             t64 = fp64[0] / args.steps
             line["fp64"] = {"ns_per_day": world * ns_per_day(t64 * 1e-3), "ms_per_step": t64,
                             "pair_kernel_ms": fp64[1],
-                            "mixed_speedup": t64 / ms_step}
+                            "mixed_speedup": t64 / ms_step,
+                            "pair_kernel_speedup": fp64[1] / mean_k,
+                            "kernel": "k_pair_fp64_half: the mixed kernel's half-shell task "
+                                      "split and box culling in FP64, each pair once, exact "
+                                      "fixed-point force sums; the same device steps"}
         if world == 1 and not args.skip_cpu:
             cpu_steps = args.cpu_steps
             t_cpu, kind = cpu_reference_time(s, cpu_steps)

@@ -1486,10 +1486,11 @@ k_pair_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes, const dou
 // one i-cell and one share of the half-shell cell offsets (the same
 // HalfStencil; home-cell pairs taken for i < j) -- with fp64_pair's
 // arithmetic and each pair evaluated once, its force added to both atoms
-// (Newton's third law, as NonbondedCutoffForce's cell-pair loop does).  No
-// candidate culling or list building: the warp stages the atoms of its
-// cells (positions in the i-cell frame, FP64) kB64 at a time in shared
-// memory and every i atom meets every staged atom.  The lanes of i atom ia
+// (Newton's third law, as NonbondedCutoffForce's cell-pair loop does).  The
+// warp stages the atoms of its cells (positions in the i-cell frame, FP64)
+// kB64 at a time in shared memory, leaving out those farther than the
+// cutoff from the box around the chunk's i atoms (no pair of theirs is
+// within it), and every i atom meets every staged atom.  The lanes of i atom ia
 // take the batch in blocks of L entries, block (ia + k) mod nsteps at step k,
 // so that at each step no two lanes touch the same staged atom: j forces are
 // summed in shared memory without atomics, in step order, and i forces in
@@ -1529,8 +1530,11 @@ __device__ __forceinline__ void fix2_add(unsigned long long *__restrict__ acc, s
   if (lo) atomicAdd(&acc[(size_t)(3 + q) * n + j], (unsigned long long)lo);
 }
 
+#ifndef PMB200_FP64_BLOCKS
+#define PMB200_FP64_BLOCKS 20  // resident blocks per SM asked of the FP64 kernel
+#endif
 template <int kForm, bool kEnergy, bool kVirial, bool kMolVir>
-__global__ void __launch_bounds__(32)
+__global__ void __launch_bounds__(32, kVirial ? 1 : PMB200_FP64_BLOCKS)
 k_pair_fp64_half(GridParams g, Fp64Consts mc, const HalfStencil st, int slots, int ntypes,
                  const double4 *__restrict__ lj64, const int *__restrict__ start,
                  const double4 *__restrict__ spos, const int2 *__restrict__ smeta,
@@ -1566,6 +1570,16 @@ k_pair_fp64_half(GridParams g, Fp64Consts mc, const HalfStencil st, int slots, i
     double Ri[3] = {0.0, 0.0, 0.0};
     if (kMolVir)
       for (int k = 0; k < 3; k++) Ri[k] = com[3 * (size_t)mi.y + k];
+    // the box around the chunk's i atoms
+    double blo_x = pi.x, blo_y = pi.y, blo_z = pi.z, bhi_x = pi.x, bhi_y = pi.y, bhi_z = pi.z;
+    for (int off = 16; off > 0; off >>= 1) {
+      blo_x = fmin(blo_x, __shfl_xor_sync(0xffffffffu, blo_x, off));
+      blo_y = fmin(blo_y, __shfl_xor_sync(0xffffffffu, blo_y, off));
+      blo_z = fmin(blo_z, __shfl_xor_sync(0xffffffffu, blo_z, off));
+      bhi_x = fmax(bhi_x, __shfl_xor_sync(0xffffffffu, bhi_x, off));
+      bhi_y = fmax(bhi_y, __shfl_xor_sync(0xffffffffu, bhi_y, off));
+      bhi_z = fmax(bhi_z, __shfl_xor_sync(0xffffffffu, bhi_z, off));
+    }
     int nb = 0;
     // every i atom of the chunk against the nb staged atoms, then the j
     // forces out and the batch emptied
@@ -1644,17 +1658,30 @@ k_pair_fp64_half(GridParams g, Fp64Consts mc, const HalfStencil st, int slots, i
       cell_shift(g, g.ec, 1.0, dx, dy, dz, sx, sy, sz);
       for (int f0 = 0; f0 < cnt;) {
         const int take = min(min(cnt - f0, kB64 - nb), 32);
+        bool keep = false;
+        double4 p = make_double4(0.0, 0.0, 0.0, 0.0);
+        const int j = js + f0 + lane;
         if (lane < take) {
-          const int j = js + f0 + lane;
-          double4 p = spos[j];
+          p = spos[j];
           p.x += sx; p.y += sy; p.z += sz;
-          sm.pos[nb + lane] = p;
-          sm.meta[nb + lane] = smeta[j];
-          sm.jidx[nb + lane] = j | homebit;
+          // squared distance to the box in the pair test's operation order:
+          // per axis at most |p - x_i| for every i in the chunk, and rounding
+          // is monotonic, so no pair the test accepts is dropped
+          const double bx = fmax(fmax(blo_x - p.x, p.x - bhi_x), 0.0);
+          const double by = fmax(fmax(blo_y - p.y, p.y - bhi_y), 0.0);
+          const double bz = fmax(fmax(blo_z - p.z, p.z - bhi_z), 0.0);
+          keep = bx * bx + by * by + bz * bz <= mc.cut2;
         }
-        nb += take;
+        const unsigned km = __ballot_sync(0xffffffffu, keep);
+        if (keep) {
+          const int slot = nb + __popc(km & ((1u << lane) - 1u));
+          sm.pos[slot] = p;
+          sm.meta[slot] = smeta[j];
+          sm.jidx[slot] = j | homebit;
+        }
+        nb += __popc(km);
         f0 += take;
-        if (nb == kB64) process();
+        if (nb > kB64 - 32) process();  // less than a full round of room left
       }
     }
     if (nb > 0) process();
