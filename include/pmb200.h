@@ -145,6 +145,42 @@ int pmb200_eval_cells(pmb200_ctx *ctx, const double *pos, double *forces,
 int pmb200_eval_device(pmb200_ctx *ctx, const double *d_pos, double *d_forces,
                        double *d_out, unsigned flags, void *stream);
 
+/* Autotuner of one context's evaluation.  Times the whole evaluation (cell
+ * build, pair kernel, force finalisation, reductions) on the device
+ * positions d_pos[3n], reps timed launches per configuration (median), with
+ * and without energies, over the grid's cell size (hints cutoff / 1.5, / 2,
+ * / 2.5, / 3, / 3.5, / 4, each as pmb200_params::cellsize; hints that give
+ * the same grid are timed once, grids the stencil limits refuse are skipped)
+ * and, for PMB200_MIXED contexts, the pair kernel (search or cluster-pair,
+ * see pmb200_set_pair_kernel) and its warps per i-cell (2, 4, 8), chosen
+ * separately for energy launches and forces-only launches; keeps the grid
+ * with the fastest evaluation with energies (the reference's integrators
+ * ask for energies every step) and applies it.  The choice is cached for the
+ * process under a key of the device, the force (kind, precision, cutoffs,
+ * switches), the atom and type counts and the box: a later context with the
+ * same key takes it without timing.  result[8] (may be NULL) = {cell-size
+ * hint, warps per i-cell with energies, warps per i-cell forces-only (0 for
+ * FP64), ms with energies, ms forces-only, configurations timed (0: taken
+ * from the cache), pair kernel with energies, pair kernel forces-only
+ * (PMB200_KERNEL_*)}.  Forces and energies after tuning agree with the
+ * untuned ones to the kernel's precision (the cell grid sets the FP32
+ * cell-unit coordinates).  The device work runs on `stream` (NULL: the
+ * context's) and is synchronised. */
+int pmb200_autotune(pmb200_ctx *ctx, const double *d_pos, void *stream, int reps,
+                    double result[8]);
+
+/* The mixed pair kernel of a context.  PMB200_KERNEL_SEARCH (the default):
+ * per-atom candidate search in every evaluation (culled staging, per-lane
+ * lists).  PMB200_KERNEL_TILES: cluster pairs -- runs of 4 atoms of a cell
+ * (sorted by height) as clusters, one bounding-box test per cluster pair,
+ * and 4 x 4 tiles of atom pairs evaluated with masks; the same pair set and
+ * pair arithmetic.  The tile kernel serves the cutoff and real-space Ewald
+ * forms of mixed contexts without virial on orthogonal grids with at most
+ * 16 LJ types; other evaluations of the context use the search kernel. */
+#define PMB200_KERNEL_SEARCH 0
+#define PMB200_KERNEL_TILES 1
+int pmb200_set_pair_kernel(pmb200_ctx *ctx, int kernel);
+
 /* Force decomposition over several GPUs, one process and one context per GPU,
  * every context holding the same topology, box and positions: the
  * replicated-data decomposition of the reference's parallel evaluation

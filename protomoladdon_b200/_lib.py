@@ -34,6 +34,9 @@ PMB200_SW_CN = 3
 PMB200_SW_CMPCNCN = 4
 PMB200_SW_TABLE = 16  # flag on the LJ switch: LennardJonesTableForce
 
+PMB200_KERNEL_SEARCH = 0
+PMB200_KERNEL_TILES = 1
+
 PMB200_ERFC_POLY5 = 0
 PMB200_ERFC_EXACT = 1
 
@@ -44,6 +47,7 @@ EXPORTED = (
     "pmb200_leapfrog_device", "pmb200_last_pair_count", "pmb200_grid",
     "pmb200_step_device", "pmb200_set_kernel_timing", "pmb200_last_kernel_ms",
     "pmb200_measure_fp32_peak", "pmb200_set_rigid_waters", "pmb200_host_kick_drift",
+    "pmb200_autotune", "pmb200_set_pair_kernel",
     "pmb200_eval_noalloc", "pmb200_create_ewald_real", "pmb200_ewald_info",
     "pmb200_param_grad_device", "pmb200_hvp_device", "pmb200_update_params",
     "pmb200_batch_create", "pmb200_batch_destroy", "pmb200_batch_last_error",
@@ -114,6 +118,8 @@ def lib():
     L.pmb200_measure_fp32_peak.argtypes = [_I, ctypes.POINTER(_D)]
     L.pmb200_set_rigid_waters.argtypes = [_P, _I, _P, _D, _D]
     L.pmb200_host_kick_drift.argtypes = [_I, _P, _P, _P, _P, _D, _D, _I, _P, _D, _D, _I]
+    L.pmb200_autotune.argtypes = [_P, _P, _P, _I, _P]
+    L.pmb200_set_pair_kernel.argtypes = [_P, _I]
     L.pmb200_eval_noalloc.argtypes = [ctypes.POINTER(Params), _I, _P, _P, _P, _P, _P, _P, _I, _P,
                                       _D, _P, _P, _P, _P, _P, _P]
     L.pmb200_create_ewald_real.argtypes = [ctypes.POINTER(EwaldParams), ctypes.POINTER(_P)]

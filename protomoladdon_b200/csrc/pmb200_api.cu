@@ -9,6 +9,7 @@
 // all on the context's stream.
 #include "../../include/pmb200.h"
 #include "pmb200_kernels.cuh"
+#include "pmb200_tiles.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -40,6 +41,14 @@ struct pmb200_ctx {
   // potential (LJ, Coulomb)
   int sw_kind[2] = {0, 0};
   double sw_par[2][4] = {};
+  // mixed kernel warps per i-cell for forces-only and for energy / virial
+  // launches (0: mixed_cell_slots' choice; set by pmb200_autotune)
+  int slots_f = 0, slots_e = 0;
+  // mixed pair kernel for energy and for forces-only launches: the
+  // cluster-pair (tile) kernel where it applies (pmb200_set_pair_kernel,
+  // pmb200_autotune), else the search kernel
+  bool tiles_e = false, tiles_f = false;
+  float4 *d_cblo = nullptr, *d_cbhi = nullptr;  // cluster boxes (tile kernel)
   // tabulated LJ (LennardJonesTableForce under UniversalSwitchingFunction):
   // the FP64 grid on the device (null: analytic LJ)
   double4 *d_ljtab = nullptr;
@@ -173,6 +182,12 @@ void release_graph(pmb200_ctx *c) {
 }
 
 double rc_max(const pmb200_params &p) { return std::max(p.cutoff_lj, p.cutoff_coul); }
+
+// Warps per i-cell of the context's mixed launches.
+int ctx_slots(const pmb200_ctx *c, bool energy_or_virial) {
+  const int s = energy_or_virial ? c->slots_e : c->slots_f;
+  return s > 0 ? s : mixed_cell_slots(energy_or_virial, c->n, c->g.ncell);
+}
 
 // Pair cutoff of the context's potential.
 double ctx_rc(const pmb200_ctx *c) {
@@ -386,6 +401,8 @@ int ensure_atom_buffers(pmb200_ctx *c) {
   CK(dalloc(c->d_spos64, n));
   CK(dalloc(c->d_smeta, n));
   CK(dalloc(c->d_facc, 6 * n));
+  CK(dalloc(c->d_cblo, n));
+  CK(dalloc(c->d_cbhi, n));
   CK(dalloc(c->d_hpos, 3 * n));
   CK(dalloc(c->d_hfrc, 3 * n));
   c->n_alloc = c->n;
@@ -428,7 +445,7 @@ void launch_pair_mixed(pmb200_ctx *c, unsigned flags, cudaStream_t st, int cell0
   const bool virial = (flags & (PMB200_VIRIAL | PMB200_MOLVIRIAL)) != 0;
   const bool molvir = (flags & PMB200_MOLVIRIAL) != 0;
   const size_t smem = mixed_smem_bytes(F, c->ntypes, c->half.ncells);
-  const int slots = mixed_cell_slots(energy || virial, c->n, g.ncell);
+  const int slots = ctx_slots(c, energy || virial);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)(std::max(ncells, 1) * slots));
   cfg.blockDim = dim3(32);
@@ -460,6 +477,45 @@ void launch_pair_mixed(pmb200_ctx *c, unsigned flags, cudaStream_t st, int cell0
   }
 #undef PMB_MIXED_FLAGS
 #undef PMB_MIXED_LAUNCH
+}
+
+// Whether an evaluation with these flags runs on the cluster-pair kernel:
+// the context asked for it, mixed precision, the cutoff or real-space Ewald
+// form with its LJ table in shared memory, no virial, an orthogonal grid.
+bool tiles_apply(const pmb200_ctx *c, unsigned flags) {
+  return ((flags & PMB200_ENERGY) ? c->tiles_e : c->tiles_f) && c->p.precision == PMB200_MIXED &&
+         (c->form == FORM_CUTOFF || c->form == FORM_EWALD_POLY5 || c->form == FORM_EWALD_EXACT) &&
+         !(flags & (PMB200_VIRIAL | PMB200_MOLVIRIAL)) && c->ntypes <= kMaxTypes && !c->g.tric &&
+         c->n < (1 << 29);
+}
+
+// The cluster boxes and the cluster-pair kernel (see pmb200_tiles.cuh), as
+// programmatic dependents of the cell build when pdl.
+template <int F>
+void launch_pair_tiles(pmb200_ctx *c, unsigned flags, cudaStream_t st, bool pdl) {
+  const GridParams &g = c->g;
+  const bool energy = (flags & PMB200_ENERGY) != 0;
+  const int slots = ctx_slots(c, energy);
+  launch_k(k_cluster_boxes, (unsigned)((g.ncell + 3) / 4), 128, 0, st, pdl, g.ncell,
+           (const int *)c->d_start, (const float4 *)c->d_spos32, c->d_cblo, c->d_cbhi);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(std::max(g.ncell, 1) * slots));
+  cfg.blockDim = dim3(32);
+  cfg.dynamicSmemBytes = mixed_smem_bytes(F, c->ntypes, c->half.ncells);
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = (pdl && PMB200_PDL) ? 1 : 0;
+#define PMB_TILES_LAUNCH(E)                                                                \
+  cudaLaunchKernelEx(&cfg, k_pair_tiles<F, E>, g, c->mc, c->half, c->ntypes, c->d_lj32,      \
+                     c->d_start, c->d_spos32, c->d_smeta, c->d_sidx, c->d_ex_start, c->d_ex,  \
+                     c->d_cblo, c->d_cbhi, c->d_facc, c->n, c->d_err, c->d_partial, slots,   \
+                     c->d_spos_lo)
+  if (energy) PMB_TILES_LAUNCH(true);
+  else PMB_TILES_LAUNCH(false);
+#undef PMB_TILES_LAUNCH
 }
 
 // (over the i-cells [cell0, cell0 + ncells), all by default)
@@ -607,7 +663,7 @@ void launch_cell_build(pmb200_ctx *c, const double *d_pos, bool mixed, bool lo,
            c->d_start, c->d_tmp, mixed ? c->d_rel32 : nullptr, mixed ? nullptr : c->d_rel64,
            c->d_type, c->d_mol, c->d_sidx, mixed ? c->d_spos32 : nullptr,
            mixed ? nullptr : c->d_spos64, c->d_smeta, lo ? c->d_rel_lo : nullptr,
-           lo ? c->d_spos_lo : nullptr);
+           lo ? c->d_spos_lo : nullptr, (mixed && (c->tiles_e || c->tiles_f)) ? 1 : 0);
 }
 
 int launch_eval(pmb200_ctx *c, const double *d_pos, double *d_forces, double *d_out,
@@ -638,7 +694,11 @@ int launch_eval(pmb200_ctx *c, const double *d_pos, double *d_forces, double *d_
     // (a programmatic dependent of the cell build's last kernel, except in
     // timed launches, whose events bracket the pair kernel alone)
     const bool pdl = !timed;
-    if (c->form == FORM_GENERIC)
+    if (tiles_apply(c, flags)) {
+      if (c->form == FORM_EWALD_POLY5) launch_pair_tiles<FORM_EWALD_POLY5>(c, flags, st, pdl);
+      else if (c->form == FORM_EWALD_EXACT) launch_pair_tiles<FORM_EWALD_EXACT>(c, flags, st, pdl);
+      else launch_pair_tiles<FORM_CUTOFF>(c, flags, st, pdl);
+    } else if (c->form == FORM_GENERIC)
       launch_pair_mixed<FORM_GENERIC>(c, flags, st, 0, -1, nullptr, pdl);
     else if (c->form == FORM_EWALD_POLY5)
       launch_pair_mixed<FORM_EWALD_POLY5>(c, flags, st, 0, -1, nullptr, pdl);
@@ -661,12 +721,10 @@ int launch_eval(pmb200_ctx *c, const double *d_pos, double *d_forces, double *d_
   CK(cudaGetLastError());
   if (timed) CK(cudaEventRecord(c->ev1, st));
   if (energy || virial) {
-    // partial rows: one per (cell, slot) warp (energy / virial launches of
-    // the mixed kernel use the slot count of mixed_cell_slots(true, ...));
-    // both kernels visit each pair once
-    k_reduce1<<<kRedBlocks, 256, 0, st>>>(
-        g.ncell * (mixed ? mixed_cell_slots(true, n, g.ncell) : kFp64Slots), c->d_partial,
-        c->d_red);
+    // partial rows: one per (cell, slot) warp; both kernels visit each pair
+    // once
+    k_reduce1<<<kRedBlocks, 256, 0, st>>>(g.ncell * (mixed ? ctx_slots(c, true) : kFp64Slots),
+                                          c->d_partial, c->d_red);
     k_reduce2<<<1, 256, 0, st>>>(kRedBlocks, c->d_red, 1.0, d_out ? d_out : c->d_out,
                                 c->d_pairs);
     CK(cudaGetLastError());
@@ -878,7 +936,7 @@ int pmb200_destroy(pmb200_ctx *c) {
   release_graph(c);
   dfree(c->d_type); dfree(c->d_mol); dfree(c->d_q); dfree(c->d_mass);
   dfree(c->d_ex_start); dfree(c->d_ex); dfree(c->d_mstart); dfree(c->d_matoms);
-  dfree(c->d_lj32); dfree(c->d_lj64); dfree(c->d_ljtab);
+  dfree(c->d_lj32); dfree(c->d_lj64); dfree(c->d_ljtab); dfree(c->d_cblo); dfree(c->d_cbhi);
   dfree(c->d_count); dfree(c->d_start); dfree(c->d_err); dfree(c->d_partial);
   dfree(c->d_cell_of); dfree(c->d_slot); dfree(c->d_tmp); dfree(c->d_sidx);
   dfree(c->d_rel32); dfree(c->d_spos32); dfree(c->d_rel_lo); dfree(c->d_spos_lo); dfree(c->d_rel64); dfree(c->d_spos64);
@@ -1038,12 +1096,12 @@ int pmb200_set_box(pmb200_ctx *c, const double e1[3], const double e2[3], const 
       return fail(c, PMB200_EINVAL, "box edge %d is %g", a, L[a]);
     if (!std::isfinite(origin[a])) return fail(c, PMB200_EINVAL, "origin");
   }
+  for (int k = 0; k < 3; k++) {
+    c->box_e[0][k] = e1[k]; c->box_e[1][k] = e2[k]; c->box_e[2][k] = e3[k];
+    c->box_origin[k] = origin[k];
+  }
+  c->box_given = true;
   if (c->form != FORM_CUTOFF) {
-    for (int k = 0; k < 3; k++) {
-      c->box_e[0][k] = e1[k]; c->box_e[1][k] = e2[k]; c->box_e[2][k] = e3[k];
-      c->box_origin[k] = origin[k];
-    }
-    c->box_given = true;
     if (!c->have_topo) {  // alpha may need N: finish when the topology arrives
       c->have_box = false;
       return PMB200_OK;
@@ -1119,7 +1177,7 @@ int pmb200_set_box(pmb200_ctx *c, const double e1[3], const double e2[3], const 
     CK(cudaMemset(c->d_count, 0, sizeof(int) * (size_t)g.ncell));
     c->count_zero = true;
     CK(dalloc(c->d_start, (size_t)g.ncell + 1));
-    CK(dalloc(c->d_partial, (size_t)g.ncell * kEnergyCellSlots * kNacc));
+    CK(dalloc(c->d_partial, (size_t)g.ncell * kMaxCellSlots * kNacc));
     c->ncell_alloc = g.ncell;
   }
   // constants
@@ -1209,6 +1267,187 @@ int pmb200_eval_device(pmb200_ctx *c, const double *d_pos, double *d_forces, dou
   return launch_eval(c, d_pos, d_forces, d_out, flags, 1, st);
 }
 
+}  // extern "C"
+
+namespace {
+
+// ---- single-context autotuner ----
+// Choices found for a workload, kept for the process: contexts with the same
+// key take them without timing again.
+struct TuneChoice {
+  double cellsize;         // the cell-size hint applied (0: the default)
+  int slots_e, slots_f;    // mixed warps per i-cell (0 for FP64 contexts)
+  bool tiles_e, tiles_f;   // the cluster-pair kernel with / without energies
+  double ms_e, ms_f;       // median evaluation times with and without energies
+  int tried;               // configurations timed
+};
+std::mutex g_tune_mutex;
+std::map<std::string, TuneChoice> g_tune_cache;
+
+std::string tune_key(const pmb200_ctx *c) {
+  cudaDeviceProp prop{};
+  cudaGetDeviceProperties(&prop, c->p.device);
+  char buf[512];
+  std::snprintf(buf, sizeof buf,
+                "%s|%d|form%d|prec%d|n%d|t%d|vac%d|rc%.6g|%.6g %.6g %.6g|%.6g %.6g %.6g|"
+                "%.6g %.6g %.6g|sw%d,%d|%.6g %.6g %.6g %.6g|tab%d",
+                prop.name, prop.multiProcessorCount, c->form, c->p.precision, c->n, c->ntypes,
+                c->vacuum ? 1 : 0, ctx_rc(c), c->box_e[0][0], c->box_e[0][1], c->box_e[0][2],
+                c->box_e[1][0], c->box_e[1][1], c->box_e[1][2], c->box_e[2][0], c->box_e[2][1],
+                c->box_e[2][2], c->sw_kind[0], c->sw_kind[1], c->sw_par[0][0], c->sw_par[0][1],
+                c->sw_par[1][0], c->sw_par[1][1], c->d_ljtab ? 1 : 0);
+  return buf;
+}
+
+// Re-applies the context's box (or vacuum domain) under its current hint.
+int reapply_box(pmb200_ctx *c) {
+  if (c->vacuum) c->vacuum_pending = true;
+  return pmb200_set_box(c, c->box_e[0], c->box_e[1], c->box_e[2], c->box_origin);
+}
+
+}  // namespace
+
+extern "C" {
+
+int pmb200_set_pair_kernel(pmb200_ctx *c, int kernel) {
+  if (!c) return PMB200_EINVAL;
+  if (kernel != PMB200_KERNEL_SEARCH && kernel != PMB200_KERNEL_TILES)
+    return fail(c, PMB200_EINVAL, "pair kernel %d", kernel);
+  c->tiles_e = c->tiles_f = kernel == PMB200_KERNEL_TILES;
+  release_graph(c);  // graphs hold the previous kernel
+  return PMB200_OK;
+}
+
+int pmb200_autotune(pmb200_ctx *c, const double *d_pos, void *stream, int reps,
+                    double result[8]) {
+  int rc = check_ready(c);
+  if (rc) return rc;
+  if (c->n > 0 && !d_pos) return fail(c, PMB200_EINVAL, "null device buffer");
+  if (reps < 1 || reps > 1000) return fail(c, PMB200_EINVAL, "reps %d (1..1000)", reps);
+  CK(cudaSetDevice(c->p.device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  const bool mixed = c->p.precision == PMB200_MIXED;
+  const std::string key = tune_key(c);
+  TuneChoice best{};
+  bool cached = false;
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      best = it->second;
+      cached = true;
+    }
+  }
+  const double hint0 = c->p.cellsize;
+  if (!cached) {
+    // candidate cell sizes (as hints; the grid takes the largest cell of at
+    // most the hint that divides each box edge, so some give the same grid)
+    const double rc_cut = ctx_rc(c);
+    const double divs[] = {1.5, 2.0, 2.5, 3.0, 3.5, 4.0};
+    const int slot_opts[] = {2, 4, 8};
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    auto timed = [&](unsigned flags, double &ms) -> int {
+      std::vector<float> t((size_t)reps);
+      int r = launch_eval(c, d_pos, c->d_hfrc, c->d_out, flags, 0, st);  // warm-up
+      if (r) return r;
+      for (int k = 0; k < reps; k++) {
+        if (cudaEventRecord(e0, st) != cudaSuccess) return PMB200_ECUDA;
+        r = launch_eval(c, d_pos, c->d_hfrc, c->d_out, flags, 0, st);
+        if (r) return r;
+        if (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+            cudaEventElapsedTime(&t[k], e0, e1) != cudaSuccess)
+          return PMB200_ECUDA;
+      }
+      std::nth_element(t.begin(), t.begin() + reps / 2, t.end());
+      ms = t[reps / 2];
+      return PMB200_OK;
+    };
+    int last_dims[3] = {-1, -1, -1};
+    best.ms_e = 1e300;
+    int status = PMB200_OK;
+    for (double dv : divs) {
+      c->p.cellsize = rc_cut / dv;
+      c->tiles_e = c->tiles_f = false;
+      if (reapply_box(c) != PMB200_OK) continue;  // a grid the stencil limits refuse
+      const int dims[3] = {c->g.nx, c->g.ny, c->g.nz};
+      if (dims[0] == last_dims[0] && dims[1] == last_dims[1] && dims[2] == last_dims[2])
+        continue;  // the same grid as the previous hint
+      for (int a = 0; a < 3; a++) last_dims[a] = dims[a];
+      TuneChoice cand{};
+      cand.cellsize = c->p.cellsize;
+      cand.ms_e = cand.ms_f = 1e300;
+      // the search kernel, and the cluster-pair kernel where it applies
+      for (int kern = 0; kern < 2 && !status; kern++) {
+        c->tiles_e = c->tiles_f = kern == 1;
+        if (kern == 1 && !tiles_apply(c, PMB200_ENERGY) && !tiles_apply(c, 0u)) break;
+        for (int so : slot_opts) {
+          if (!mixed && so != slot_opts[0]) break;  // the FP64 kernel's split is fixed
+          double me = 0.0, mf = 0.0;
+          c->slots_e = c->slots_f = mixed ? so : 0;
+          status = timed(PMB200_ENERGY, me);
+          if (!status) status = timed(0u, mf);
+          if (status) break;
+          best.tried++;
+          if (me < cand.ms_e) {
+            cand.ms_e = me;
+            cand.slots_e = mixed ? so : 0;
+            cand.tiles_e = kern == 1;
+          }
+          if (mf < cand.ms_f) {
+            cand.ms_f = mf;
+            cand.slots_f = mixed ? so : 0;
+            cand.tiles_f = kern == 1;
+          }
+        }
+      }
+      c->tiles_e = c->tiles_f = false;
+      if (status) break;
+      if (cand.ms_e < best.ms_e) {
+        const int tried = best.tried;
+        best = cand;
+        best.tried = tried;
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (status || best.ms_e >= 1e300) {
+      c->p.cellsize = hint0;
+      c->slots_e = c->slots_f = 0;
+      c->tiles_e = c->tiles_f = false;
+      const int r2 = reapply_box(c);
+      return status ? status : (r2 ? r2 : fail(c, PMB200_EUNSUPPORTED, "no grid to tune"));
+    }
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    g_tune_cache[key] = best;
+  }
+  // apply the choice
+  c->p.cellsize = best.cellsize;
+  rc = reapply_box(c);
+  if (rc) {
+    c->p.cellsize = hint0;
+    reapply_box(c);
+    return rc;
+  }
+  c->slots_e = best.slots_e;
+  c->slots_f = best.slots_f;
+  c->tiles_e = best.tiles_e;
+  c->tiles_f = best.tiles_f;
+  release_graph(c);  // graphs hold the previous launch shapes
+  if (result) {
+    result[0] = best.cellsize;
+    result[1] = best.slots_e;
+    result[2] = best.slots_f;
+    result[3] = best.ms_e;
+    result[4] = best.ms_f;
+    result[5] = cached ? 0.0 : best.tried;
+    result[6] = best.tiles_e ? PMB200_KERNEL_TILES : PMB200_KERNEL_SEARCH;
+    result[7] = best.tiles_f ? PMB200_KERNEL_TILES : PMB200_KERNEL_SEARCH;
+  }
+  return PMB200_OK;
+}
+
 // Force decomposition: shard s of nshards takes the i-cells
 // [ncell * s / nshards, ncell * (s + 1) / nshards) of the half-shell walk.
 int pmb200_shard_eval_device(pmb200_ctx *c, const double *d_pos, int shard, int nshards,
@@ -1249,7 +1488,7 @@ int pmb200_shard_eval_device(pmb200_ctx *c, const double *d_pos, int shard, int 
   if (energy || virial) {
     if (hi > lo) {
       // this shard's partial rows: one per (cell, slot) warp
-      k_reduce1<<<kRedBlocks, 256, 0, st>>>((hi - lo) * mixed_cell_slots(true, n, g.ncell),
+      k_reduce1<<<kRedBlocks, 256, 0, st>>>((hi - lo) * ctx_slots(c, true),
                                             c->d_partial, c->d_red);
       k_reduce2<<<1, 256, 0, st>>>(kRedBlocks, c->d_red, 1.0, d_out, c->d_pairs);
     } else {
@@ -1591,7 +1830,7 @@ int pmb200_eval_cells(pmb200_ctx *c, const double *pos, double *forces, double *
     else launch_pair_mixed<FORM_CUTOFF>(c, flags, st, cell_lo, nc);
     k_finalize<<<(c->n + 255) / 256, 256, 0, st>>>(c->n, c->d_facc, c->d_sidx,
                                                   kFixInv / g.unit, 0, c->d_hfrc);
-    rows = nc * mixed_cell_slots(true, c->n, g.ncell);
+    rows = nc * ctx_slots(c, true);
   } else {
     CK(cudaMemsetAsync(c->d_hfrc, 0, bytes, st));
     const int blocks = (nc + 3) / 4;

@@ -434,7 +434,7 @@ __global__ void k_rank_gather(int ncell, const int *__restrict__ start,
                               const int *__restrict__ mol, int *__restrict__ sidx,
                               float4 *__restrict__ spos32, double4 *__restrict__ spos64,
                               int2 *__restrict__ smeta, const float4 *__restrict__ rel_lo,
-                              float4 *__restrict__ spos_lo) {
+                              float4 *__restrict__ spos_lo, int zorder = 0) {
   pdl_trigger();
   pdl_wait();
   const int lane = threadIdx.x & 31;
@@ -444,7 +444,16 @@ __global__ void k_rank_gather(int ncell, const int *__restrict__ start,
   for (int k = s + lane; k < e; k += 32) {
     const int me = tmp[k];
     int rank = 0;
-    for (int m = s; m < e; m++) rank += (tmp[m] < me);
+    if (zorder) {  // by height in the cell (FP32 coordinate), then by index
+      const float zme = rel32[me].z;
+      for (int m = s; m < e; m++) {
+        const int o = tmp[m];
+        const float zo = rel32[o].z;
+        rank += (zo < zme || (zo == zme && o < me));
+      }
+    } else {
+      for (int m = s; m < e; m++) rank += (tmp[m] < me);
+    }
     const int d = s + rank;
     sidx[d] = me;
     if (spos32) spos32[d] = rel32[me];
@@ -521,10 +530,9 @@ __device__ __forceinline__ int lanes_per_atom(int m) {
 // lanes and added to facc once per warp.  Every integer sum is exact, so
 // the result does not depend on scheduling.
 //
-// Pair arithmetic is FP32 in cell units.  The Coulomb energy is carried as
-// three per-atom sums (q_j / r, q_j, q_j r^2) so that the C1 constants are
-// applied once in FP64 at the end; the cutoff form takes them from FP64
-// distances, the other forms as Kahan-compensated FP32 sums.
+// Pair arithmetic is FP32 in cell units.  The Coulomb energy of the cutoff
+// form is summed in FP64 from FP64 distances (q_j g(r) per pair, g the
+// C1-switched 1/r); the other forms' as Kahan-compensated FP32 sums.
 // ---------------------------------------------------------------------------
 #ifndef PMB200_STAGE_BATCH
 #define PMB200_STAGE_BATCH 128

@@ -174,6 +174,8 @@ class NonbondedCutoffB200SystemForce:
         L = _lib.lib()
         if self._ctx is None:
             self._ctx = self._create(topo)
+            if getattr(self, "_pair_kernel", _lib.PMB200_KERNEL_SEARCH):
+                self._check(L.pmb200_set_pair_kernel(self._ctx, self._pair_kernel))
         key = (id(topo), topo.version)
         if self._topo_key != key:
             ex = topo.excl.reshape(-1)
@@ -275,6 +277,28 @@ class NonbondedCutoffB200SystemForce:
         self._check(_lib.lib().pmb200_eval_device(
             self._ctx, _P(pos_ptr), _P(force_ptr), _P(out_ptr) if out_ptr else None,
             int(flags), _P(stream) if stream else None))
+
+    def autotune(self, topo, pos_ptr, reps=10, stream=None):
+        """pmb200_autotune on device positions (a raw pointer): times the
+        evaluation over cell sizes and, for mixed precision, warps per i-cell,
+        applies the fastest and returns the choice as a dict."""
+        self._ensure(topo)
+        r = (ctypes.c_double * 8)()
+        self._check(_lib.lib().pmb200_autotune(self._ctx, _P(pos_ptr),
+                                               _P(stream) if stream else None, int(reps), r))
+        names = {_lib.PMB200_KERNEL_SEARCH: "search", _lib.PMB200_KERNEL_TILES: "tiles"}
+        return {"cellsize_hint": r[0], "warps_per_cell_energy": int(r[1]),
+                "warps_per_cell_forces": int(r[2]), "ms_energy": r[3], "ms_forces": r[4],
+                "configurations_timed": int(r[5]), "kernel_energy": names[int(r[6])],
+                "kernel_forces": names[int(r[7])]}
+
+    def set_pair_kernel(self, kernel):
+        """The mixed pair kernel: "search" (default) or "tiles" (cluster pairs;
+        pmb200_set_pair_kernel)."""
+        k = {"search": _lib.PMB200_KERNEL_SEARCH, "tiles": _lib.PMB200_KERNEL_TILES}[kernel]
+        self._pair_kernel = k
+        if self._ctx is not None:
+            self._check(_lib.lib().pmb200_set_pair_kernel(self._ctx, k))
 
     def shard_eval_device(self, topo, pos_ptr, shard, nshards, facc_ptr, out_ptr=None, flags=0,
                           stream=None):
