@@ -313,10 +313,13 @@ def run_ours(args):
                "energy_rel_err_lj": float(abs(E[1] - eo[1]) / abs(eo[1]))}
 
     def tune(force):
-        """pmb200_autotune on the start positions: the grid's cell size and
-        the pair kernel's warps per i-cell, applied to the context."""
+        """pmb200_autotune on the start positions: the grid's cell size, the
+        pair kernel and its warps per i-cell, applied to the context."""
         pos = torch.tensor(s["pos"], dtype=torch.float64, device=dev)
-        choice = force.autotune(topo, pos.data_ptr(), reps=10, stream=stream.cuda_stream)
+        if args.autotune_reps <= 0:
+            return {"tuned": False}
+        choice = force.autotune(topo, pos.data_ptr(), reps=args.autotune_reps,
+                                stream=stream.cuda_stream)
         choice["grid"] = list(force.grid()[0])
         return choice
 
@@ -1028,6 +1031,9 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--skip-accuracy", action="store_true")
+    ap.add_argument("--autotune-reps", type=int, default=10,
+                    help="timed launches per configuration of pmb200_autotune (0: no tuning, "
+                         "the library's default grid and kernel)")
     ap.add_argument("--workload", default="medium",
                     choices=["medium", "large", "batch", "diff", "sharded"],
                     help="medium: the 41,472-atom water box (the headline); large: the "
