@@ -155,7 +155,9 @@ int pmb200_eval_device(pmb200_ctx *ctx, const double *d_pos, double *d_forces,
  * see pmb200_set_pair_kernel) and its warps per i-cell (2, 4, 8), chosen
  * separately for energy launches and forces-only launches; keeps the grid
  * with the fastest evaluation with energies (the reference's integrators
- * ask for energies every step) and applies it.  The choice is cached for the
+ * ask for energies every step) and applies it.  The library's defaults are
+ * timed first and another configuration replaces them only when it is 2%
+ * faster (timing noise between near-equal ones does not move the choice).  The choice is cached for the
  * process under a key of the device, the force (kind, precision, cutoffs,
  * switches), the atom and type counts and the box: a later context with the
  * same key takes it without timing.  result[8] (may be NULL) = {cell-size
