@@ -723,10 +723,11 @@ int launch_eval(pmb200_ctx *c, const double *d_pos, double *d_forces, double *d_
   if (energy || virial) {
     // partial rows: one per (cell, slot) warp; both kernels visit each pair
     // once
+    const int ns = virial ? ACC_MV : ACC_E;  // the slots the launch filled
     k_reduce1<<<kRedBlocks, 256, 0, st>>>(g.ncell * (mixed ? ctx_slots(c, true) : kFp64Slots),
-                                          c->d_partial, c->d_red);
+                                          c->d_partial, c->d_red, ns);
     k_reduce2<<<1, 256, 0, st>>>(kRedBlocks, c->d_red, 1.0, d_out ? d_out : c->d_out,
-                                c->d_pairs);
+                                c->d_pairs, ns);
     CK(cudaGetLastError());
   }
   return PMB200_OK;
@@ -1497,9 +1498,10 @@ int pmb200_shard_eval_device(pmb200_ctx *c, const double *d_pos, int shard, int 
   if (energy || virial) {
     if (hi > lo) {
       // this shard's partial rows: one per (cell, slot) warp
+      const int ns = (flags & (PMB200_VIRIAL | PMB200_MOLVIRIAL)) ? ACC_MV : ACC_E;
       k_reduce1<<<kRedBlocks, 256, 0, st>>>((hi - lo) * ctx_slots(c, true),
-                                            c->d_partial, c->d_red);
-      k_reduce2<<<1, 256, 0, st>>>(kRedBlocks, c->d_red, 1.0, d_out, c->d_pairs);
+                                            c->d_partial, c->d_red, ns);
+      k_reduce2<<<1, 256, 0, st>>>(kRedBlocks, c->d_red, 1.0, d_out, c->d_pairs, ns);
     } else {
       CK(cudaMemsetAsync(d_out, 0, sizeof(double) * 20, st));
       CK(cudaMemsetAsync(c->d_pairs, 0, sizeof(double), st));
@@ -1854,9 +1856,10 @@ int pmb200_eval_cells(pmb200_ctx *c, const double *pos, double *forces, double *
   }
   CK(cudaGetLastError());
   if (energy || anyvir) {
-    k_reduce1<<<kRedBlocks, 256, 0, st>>>(rows, prow, c->d_red);
+    const int ns = anyvir ? ACC_MV : ACC_E;
+    k_reduce1<<<kRedBlocks, 256, 0, st>>>(rows, prow, c->d_red, ns);
     k_reduce2<<<1, 256, 0, st>>>(kRedBlocks, c->d_red, mixed ? 1.0 : 0.5, c->d_out,
-                                c->d_pairs);
+                                c->d_pairs, ns);
     CK(cudaMemcpyAsync(c->h_pin_out, c->d_out, sizeof(double) * 20, cudaMemcpyDeviceToHost,
                        st));
   }
@@ -2502,10 +2505,10 @@ extern "C" int pmb200_eval_noalloc(const pmb200_params *p, int n, const double *
   if (n > 0)
     k_finalize<<<(n + 255) / 256, 256, 0, st>>>(n, facc, sidx, kFixInv / u, 0, d_forces);
   if (d_energy) {
-    k_reduce1<<<kRedBlocks, 256, 0, st>>>(g.ncell * slots, partial, red);
+    k_reduce1<<<kRedBlocks, 256, 0, st>>>(g.ncell * slots, partial, red, ACC_E);
     // the reduction writes 20 doubles (energies, virial, molecular
     // virial) into the scratch; the caller's buffer receives the two energies
-    k_reduce2<<<1, 256, 0, st>>>(kRedBlocks, red, 1.0, out, pairs);
+    k_reduce2<<<1, 256, 0, st>>>(kRedBlocks, red, 1.0, out, pairs, ACC_E);
     e = cudaMemcpyAsync(d_energy, out, 2 * sizeof(double), cudaMemcpyDeviceToDevice, st);
     if (e != cudaSuccess) return PMB200_ECUDA;
   }
@@ -2688,7 +2691,8 @@ int batch_launch_eval(pmb200_batch *b, const double *d_pos, double *d_forces, do
                                                       b->d_sys, accumulate, d_forces);
   if ((energy || virial) && d_out)
     k_reduce_batch<<<(b->nsys + 3) / 4, 128, 0, st>>>(b->nsys, b->d_rows_start, b->d_rows,
-                                                       b->d_partial, b->d_sys, d_out, b->d_pairs);
+                                                       b->d_partial, b->d_sys, d_out, b->d_pairs,
+                                                       virial ? ACC_MV : ACC_E);
   BCK(cudaGetLastError());
   return PMB200_OK;
 }

@@ -132,12 +132,12 @@ __global__ void k_finalize_batch(int N, const unsigned long long *__restrict__ f
 __global__ void k_reduce_batch(int nsys, const int *__restrict__ rows_start,
                                const int *__restrict__ rows, const double *__restrict__ partial,
                                const BatchSys *__restrict__ sys, double *__restrict__ out,
-                               double *__restrict__ pairs) {
+                               double *__restrict__ pairs, int ns) {
   const int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (s >= nsys) return;
-  double acc = 0.0;  // lane k < ACC_MV sums slot k
-  if (lane < ACC_MV)
+  double acc = 0.0;  // lane k < ns sums slot k (the slots the launch filled; the rest 0)
+  if (lane < ns)
     for (int r = rows_start[s]; r < rows_start[s + 1]; r++)
       acc += partial[(size_t)rows[r] * kNacc + lane];
   double v[ACC_MV];

@@ -34,11 +34,13 @@ constexpr double kFixInv = 1.0 / 4294967296.0;
 enum {
   ACC_ECOUL = 0,// Coulomb energy
   ACC_ELJ = 1,  // Lennard-Jones energy
-  ACC_W = 2,    // 6 virial components xx xy xz yy yz zz (2..7)
-  ACC_MW = 8,   // 6 molecular-virial components f_a comDiff_b, a <= b (8..13)
-  ACC_PAIRS = 14,
+  ACC_PAIRS = 2,// in-cutoff pairs
+  ACC_W = 3,    // 6 virial components xx xy xz yy yz zz (3..8)
+  ACC_MW = 9,   // 6 molecular-virial components f_a comDiff_b, a <= b (9..14)
   ACC_MV = 15,  // number of slots in use
+  ACC_E = 3,    // the slots an energy launch without virial fills
 };
+
 static_assert(kNacc >= ACC_MV, "partial-sum rows hold every slot");
 
 struct Row {        // one (dy, dz) row of the neighbour-cell stencil
@@ -483,6 +485,20 @@ __device__ __forceinline__ double warp_sum_mask(double v, int width) {
   for (int off = 1; off < width; off <<= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
   return v;
 }
+
+// The per-warp partial row of a pair kernel: warp sums of the first ns slots
+// of v (ns = ACC_E or ACC_MV), written by lane 0; the rest of the row is left
+// as it is (the reductions read only the first ns slots).
+template <int ns>
+__device__ __forceinline__ void write_partial_row(const double (&v)[ACC_MV], int lane,
+                                                  double *__restrict__ row) {
+#pragma unroll
+  for (int k = 0; k < ns; k++) {
+    const double sum = warp_sum_mask(v[k], 32);
+    if (lane == 0) row[k] = sum;
+  }
+}
+
 __device__ __forceinline__ long long warp_sum_ll(long long v, int width) {
   for (int off = 1; off < width; off <<= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
   return v;
@@ -1172,11 +1188,7 @@ __device__ __forceinline__ void mixed_task(
     v[ACC_ECOUL] = accU; v[ACC_ELJ] = accE; v[ACC_PAIRS] = accP;
 #pragma unroll
     for (int k = 0; k < 6; k++) { v[ACC_W + k] = w[k]; v[ACC_MW + k] = mw[k]; }
-#pragma unroll
-    for (int k = 0; k < ACC_MV; k++) {
-      const double sum = warp_sum_mask(v[k], 32);
-      if (lane == 0) partial_row[k] = sum;
-    }
+    write_partial_row<kVirial ? ACC_MV : ACC_E>(v, lane, partial_row);
   }
 }
 
@@ -1480,11 +1492,7 @@ k_pair_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes, const dou
     v[ACC_ECOUL] = accC; v[ACC_ELJ] = accE; v[ACC_PAIRS] = accP;
 #pragma unroll
     for (int k = 0; k < 6; k++) { v[ACC_W + k] = w[k]; v[ACC_MW + k] = mw[k]; }
-#pragma unroll
-    for (int k = 0; k < ACC_MV; k++) {
-      double s = warp_sum_mask(v[k], 32);
-      if (lane == 0) partial[(size_t)cell * kNacc + k] = s;
-    }
+    write_partial_row<kVirial ? ACC_MV : ACC_E>(v, lane, partial + (size_t)cell * kNacc);
   }
 }
 
@@ -1713,11 +1721,7 @@ k_pair_fp64_half(GridParams g, Fp64Consts mc, const HalfStencil st, int slots, i
     v[ACC_ECOUL] = accC; v[ACC_ELJ] = accE; v[ACC_PAIRS] = accP;
 #pragma unroll
     for (int k = 0; k < 6; k++) { v[ACC_W + k] = w[k]; v[ACC_MW + k] = mw[k]; }
-#pragma unroll
-    for (int k = 0; k < ACC_MV; k++) {
-      const double sum = warp_sum_mask(v[k], 32);
-      if (lane == 0) partial[(size_t)blockIdx.x * kNacc + k] = sum;
-    }
+    write_partial_row<kVirial ? ACC_MV : ACC_E>(v, lane, partial + (size_t)blockIdx.x * kNacc);
   }
 }
 
@@ -1991,37 +1995,46 @@ __global__ void k_com(int nmol, const int *__restrict__ mstart, const int *__res
 constexpr int kRedBlocks = 64;
 
 __global__ void k_reduce1(int ncell, const double *__restrict__ partial,
-                          double *__restrict__ red) {
-  __shared__ double sh[ACC_MV][256];
-  const int t = threadIdx.x;
+                          double *__restrict__ red, int ns) {
+  // each thread sums its rows' first ns slots; warp shuffles, then the
+  // block's warps in order (fixed order: deterministic)
+  __shared__ double sh[8][ACC_MV];
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
   const int span = (ncell + gridDim.x - 1) / gridDim.x;
   const int lo = blockIdx.x * span, hi = min(ncell, lo + span);
   double v[ACC_MV];
+#pragma unroll
   for (int k = 0; k < ACC_MV; k++) v[k] = 0.0;
   for (int c = lo + t; c < hi; c += blockDim.x)
-    for (int k = 0; k < ACC_MV; k++) v[k] += partial[(size_t)c * kNacc + k];
-  for (int k = 0; k < ACC_MV; k++) sh[k][t] = v[k];
+#pragma unroll
+    for (int k = 0; k < ACC_MV; k++)
+      if (k < ns) v[k] += partial[(size_t)c * kNacc + k];
+#pragma unroll
+  for (int k = 0; k < ACC_MV; k++)
+    if (k < ns) {
+      const double s = warp_sum_mask(v[k], 32);
+      if (lane == 0) sh[w][k] = s;
+    }
   __syncthreads();
-  for (int off = blockDim.x / 2; off > 0; off >>= 1) {
-    if (t < off)
-      for (int k = 0; k < ACC_MV; k++) sh[k][t] += sh[k][t + off];
-    __syncthreads();
+  if (t < ns) {
+    double acc = 0.0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); q++) acc += sh[q][t];
+    red[blockIdx.x * ACC_MV + t] = acc;
   }
-  if (t < ACC_MV) red[blockIdx.x * ACC_MV + t] = sh[t][0];
 }
 
 __global__ void k_reduce2(int nred, const double *__restrict__ red, double visit,
-                          double *__restrict__ out, double *__restrict__ pairs_out) {
-  // all threads stage the block sums; then each of ACC_MV threads adds one
-  // column in block order (fixed order: deterministic)
-  __shared__ double sh[kRedBlocks * ACC_MV];
+                          double *__restrict__ out, double *__restrict__ pairs_out, int ns) {
+  // each of the first ns slots summed over the blocks in block order by one
+  // warp (fixed order: deterministic); slots beyond ns are zero
   __shared__ double col[ACC_MV];
-  for (int k = threadIdx.x; k < nred * ACC_MV; k += blockDim.x) sh[k] = red[k];
-  __syncthreads();
-  if (threadIdx.x < ACC_MV) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int k = w; k < ACC_MV; k += (int)(blockDim.x >> 5)) {
     double acc = 0.0;
-    for (int b = 0; b < nred; b++) acc += sh[b * ACC_MV + threadIdx.x];
-    col[threadIdx.x] = acc;
+    if (k < ns)
+      for (int b = lane; b < nred; b += 32) acc += red[b * ACC_MV + k];
+    acc = warp_sum_mask(acc, 32);
+    if (lane == 0) col[k] = acc;
   }
   __syncthreads();
   if (threadIdx.x != 0) return;

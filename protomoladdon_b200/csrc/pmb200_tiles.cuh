@@ -350,11 +350,7 @@ k_pair_tiles(GridParams g, MixedConsts mc, const HalfStencil st, int ntypes,
 #pragma unroll
     for (int k = 0; k < ACC_MV; k++) v[k] = 0.0;
     v[ACC_ECOUL] = accU; v[ACC_ELJ] = accE; v[ACC_PAIRS] = accP;
-#pragma unroll
-    for (int k = 0; k < ACC_MV; k++) {
-      const double sum = warp_sum_mask(v[k], 32);
-      if (lane == 0) partial[(size_t)blockIdx.x * kNacc + k] = sum;
-    }
+    write_partial_row<ACC_E>(v, lane, partial + (size_t)blockIdx.x * kNacc);
   }
 }
 
