@@ -404,7 +404,7 @@ int ensure_atom_buffers(pmb200_ctx *c) {
   CK(dalloc(c->d_cblo, n));
   CK(dalloc(c->d_cbhi, n));
   CK(dalloc(c->d_hpos, 3 * n));
-  CK(dalloc(c->d_hfrc, 3 * n));
+  CK(dalloc(c->d_hfrc, 3 * n + kPinOut + 3));  // forces, then the results (pmb200_eval)
   c->n_alloc = c->n;
   return PMB200_OK;
 }
@@ -665,6 +665,9 @@ void launch_cell_build(pmb200_ctx *c, const double *d_pos, bool mixed, bool lo,
            mixed ? nullptr : c->d_spos64, c->d_smeta, lo ? c->d_rel_lo : nullptr,
            lo ? c->d_spos_lo : nullptr, (mixed && (c->tiles_e || c->tiles_f)) ? 1 : 0);
 }
+
+// One word copied on the device (the error flag into the results' copy).
+__global__ void k_copy_word(const int *__restrict__ src, int *__restrict__ dst) { *dst = *src; }
 
 int launch_eval(pmb200_ctx *c, const double *d_pos, double *d_forces, double *d_out,
                 unsigned flags, int accumulate, cudaStream_t st) {
@@ -1679,12 +1682,16 @@ int pmb200_eval(pmb200_ctx *c, const double *pos, double *forces, double *energi
     if (c->h_pin_out) cudaFreeHost(c->h_pin_out);
     c->h_pin_pos = c->h_pin_frc = c->h_pin_out = nullptr;
     CK(cudaMallocHost((void **)&c->h_pin_pos, std::max<size_t>(bytes, 8)));
-    CK(cudaMallocHost((void **)&c->h_pin_frc, std::max<size_t>(bytes, 8)));
+    CK(cudaMallocHost((void **)&c->h_pin_frc, bytes + sizeof(double) * (kPinOut + 3)));
     CK(cudaMallocHost((void **)&c->h_pin_out, sizeof(double) * kPinOut));
     c->n_pin = c->n;
   }
-  // the device error flag's page-locked copy, behind the 20 result words
-  int *h_err = reinterpret_cast<int *>(c->h_pin_out + 20);
+  // the results travel behind the forces in one copy: d_hfrc holds the 3n
+  // forces, then the 20 result words, then the device error flag
+  double *d_hout = c->d_hfrc + cnt;
+  const double *h_res = c->h_pin_frc + cnt;
+  const size_t res_bytes = bytes + sizeof(double) * kPinOut;
+  int *h_err = reinterpret_cast<int *>(c->h_pin_frc + cnt + 20);
   // positions through pinned staging; this evaluation's forces are computed
   // on the device (overwrite), read back, and added to the caller's array
   if (c->n > 0) {
@@ -1706,16 +1713,23 @@ int pmb200_eval(pmb200_ctx *c, const double *pos, double *forces, double *energi
     }
     // copy in, evaluate, copy out: one graph per (source array, flags),
     // replayed while the context's box and topology stay the same (the
-    // pair-kernel timing mode launches directly)
+    // pair-kernel timing mode launches directly).  The results and the
+    // error flag follow the forces in d_hfrc, so one copy brings all back.
+    auto sequence = [&]() -> int {
+      cudaError_t e = cudaMemcpyAsync(c->d_hpos, src, bytes, cudaMemcpyHostToDevice, st);
+      if (e != cudaSuccess) return fail(c, PMB200_ECUDA, "copy in: %s", cudaGetErrorString(e));
+      int r = launch_eval(c, c->d_hpos, c->d_hfrc, d_hout, flags, 0, st);
+      if (r) return r;
+      k_copy_word<<<1, 1, 0, st>>>(c->d_err, reinterpret_cast<int *>(d_hout + 20));
+      e = cudaGetLastError();
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(c->h_pin_frc, c->d_hfrc, res_bytes, cudaMemcpyDeviceToHost, st);
+      if (e != cudaSuccess) return fail(c, PMB200_ECUDA, "copy out: %s", cudaGetErrorString(e));
+      return PMB200_OK;
+    };
     if (c->timing) {
-      CK(cudaMemcpyAsync(c->d_hpos, src, bytes, cudaMemcpyHostToDevice, st));
-      rc = launch_eval(c, c->d_hpos, c->d_hfrc, c->d_out, flags, 0, st);
+      rc = sequence();
       if (rc) return rc;
-      CK(cudaMemcpyAsync(c->h_pin_frc, c->d_hfrc, bytes, cudaMemcpyDeviceToHost, st));
-      if (flags)
-        CK(cudaMemcpyAsync(c->h_pin_out, c->d_out, sizeof(double) * 20,
-                           cudaMemcpyDeviceToHost, st));
-      CK(cudaMemcpyAsync(h_err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
     } else {
       if (!c->hgraph_exec || c->hgraph_src != src || c->hgraph_flags != flags) {
         if (c->hgraph_exec) cudaGraphExecDestroy(c->hgraph_exec);
@@ -1724,21 +1738,9 @@ int pmb200_eval(pmb200_ctx *c, const double *pos, double *forces, double *energi
         c->hgraph = nullptr;
         c->hgraph_src = nullptr;
         CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        cudaError_t e = cudaMemcpyAsync(c->d_hpos, src, bytes, cudaMemcpyHostToDevice, st);
-        rc = e == cudaSuccess ? launch_eval(c, c->d_hpos, c->d_hfrc, c->d_out, flags, 0, st)
-                              : fail(c, PMB200_ECUDA, "copy in: %s", cudaGetErrorString(e));
-        if (!rc) {
-          e = cudaMemcpyAsync(c->h_pin_frc, c->d_hfrc, bytes, cudaMemcpyDeviceToHost, st);
-          if (e == cudaSuccess && flags)
-            e = cudaMemcpyAsync(c->h_pin_out, c->d_out, sizeof(double) * 20,
-                                cudaMemcpyDeviceToHost, st);
-          if (e == cudaSuccess)
-            e = cudaMemcpyAsync(h_err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, st);
-          if (e != cudaSuccess)
-            rc = fail(c, PMB200_ECUDA, "copy out: %s", cudaGetErrorString(e));
-        }
+        rc = sequence();
         cudaGraph_t gr = nullptr;
-        e = cudaStreamEndCapture(st, &gr);
+        const cudaError_t e = cudaStreamEndCapture(st, &gr);
         if (rc) {
           if (gr) cudaGraphDestroy(gr);
           return rc;
@@ -1754,12 +1756,12 @@ int pmb200_eval(pmb200_ctx *c, const double *pos, double *forces, double *energi
       CK(cudaGraphLaunch(c->hgraph_exec, st));
     }
   } else {
-    rc = launch_eval(c, c->d_hpos, c->d_hfrc, c->d_out, flags, 0, st);
+    rc = launch_eval(c, c->d_hpos, c->d_hfrc, d_hout, flags, 0, st);
     if (rc) return rc;
-    if (flags)
-      CK(cudaMemcpyAsync(c->h_pin_out, c->d_out, sizeof(double) * 20, cudaMemcpyDeviceToHost,
-                         st));
-    CK(cudaMemcpyAsync(h_err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    k_copy_word<<<1, 1, 0, st>>>(c->d_err, reinterpret_cast<int *>(d_hout + 20));
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(c->h_pin_frc, d_hout, sizeof(double) * kPinOut, cudaMemcpyDeviceToHost,
+                       st));
   }
   // the error flag came back with the results: one synchronisation
   CK(cudaStreamSynchronize(st));
@@ -1771,7 +1773,7 @@ int pmb200_eval(pmb200_ctx *c, const double *pos, double *forces, double *energi
 #pragma omp parallel for schedule(static) if (m > 65536)
     for (long long k = 0; k < m; k++) forces[k] += src[k];
   }
-  const double *out = c->h_pin_out;
+  const double *out = h_res;
   if (flags & PMB200_ENERGY) {
     energies[0] += out[0];
     energies[1] += out[1];
