@@ -554,6 +554,12 @@ __device__ __forceinline__ int lanes_per_atom(int m) {
 #define PMB200_STAGE_BATCH 128
 #endif
 constexpr int kBatch = PMB200_STAGE_BATCH;  // staged j atoms per warp batch (<= 256)
+#ifndef PMB200_STAGE_BATCH_E
+#define PMB200_STAGE_BATCH_E PMB200_STAGE_BATCH
+#endif
+// the same for the single-system kernel's energy launches (shared memory,
+// with the FP64 energy staging, sets their residency)
+constexpr int kBatchE = PMB200_STAGE_BATCH_E;
 
 constexpr float kJScale = 262144.0f; // shared j-force quanta (2^-18) per cell-unit force
 constexpr int kJShift = 14;          // to the global 2^-32 quanta
@@ -570,14 +576,17 @@ constexpr int kDealUnit = PMB200_DEAL_UNIT;
 #define PMB200_PDL 1            // pair kernels launched as programmatic dependents
 #endif
 
-struct __align__(16) MixedWarpSmem {
-  float4 pos[kBatch];                    // staged j atoms, shifted into the i-cell frame
-  int jf[3][kBatch];                     // per-batch j forces, int32 fixed point (2^-18)
+template <int kB>
+struct __align__(16) MixedWarpSmemT {
+  static constexpr int kCap = kB;        // staged atoms per batch
+  float4 pos[kB];                        // staged j atoms, shifted into the i-cell frame
+  int jf[3][kB];                         // per-batch j forces, int32 fixed point (2^-18)
   int fi[3][32];                         // per-lane i forces of leftover pairs (2^-18)
-  int2 meta[kBatch];                     // their (LJ type, molecule)
-  int gidx[kBatch];                      // their sorted indices
-  unsigned char list[kBatch / 2][32];    // per-lane in-range candidate indices
+  int2 meta[kB];                         // their (LJ type, molecule)
+  int gidx[kB];                          // their sorted indices
+  unsigned char list[kB / 2][32];        // per-lane in-range candidate indices
 };
+using MixedWarpSmem = MixedWarpSmemT<kBatch>;
 
 struct KahanF {
   float s = 0.f, c = 0.f;
@@ -601,7 +610,7 @@ struct KahanF {
 // shell).  The stencil offsets and the LJ table are read from shared memory;
 // the warp's i forces go straight to facc and its energy and virial partials
 // to partial_row.  Warps never wait for one another.
-template <int kForm, bool kEnergy, bool kVirial, bool kMolVir>
+template <int kForm, bool kEnergy, bool kVirial, bool kMolVir, class Smem = MixedWarpSmem>
 __device__ __forceinline__ void mixed_task(
     const GridParams &g, const MixedConsts &mc, const unsigned short *st_off, int st_ncells,
     int slot, int nslots, int ntypes, const float4 *s_lj, int cell,
@@ -609,7 +618,7 @@ __device__ __forceinline__ void mixed_task(
     const int2 *__restrict__ smeta, const int *__restrict__ sidx,
     const int *__restrict__ ex_start, const int2 *__restrict__ ex,
     unsigned long long *__restrict__ facc, int n, double *__restrict__ partial_row,
-    const PbcRef &pb, const double *__restrict__ com, MixedWarpSmem &sm,
+    const PbcRef &pb, const double *__restrict__ com, Smem &sm,
     int *__restrict__ err, float *__restrict__ s_res, const float4 *__restrict__ spos_lo) {
   const int lane = threadIdx.x & 31;
   // the energy of the cutoff form is summed from FP64 distances: kEnergy
@@ -620,6 +629,7 @@ __device__ __forceinline__ void mixed_task(
   // remainder = the FP64 position to ~1e-13 of a cell
   constexpr bool kExactE = kEnergy && kForm == FORM_CUTOFF;
   float *rsx = kExactE ? s_res : nullptr;
+  constexpr int kBatch = Smem::kCap;  // this kernel's staging batch
   float *rsy = kExactE ? rsx + kBatch : nullptr, *rsz = kExactE ? rsx + 2 * kBatch : nullptr;
   const int cx = cell % g.nx;
   const int cy = (cell / g.nx) % g.ny;
@@ -1224,8 +1234,9 @@ k_pair_mixed(GridParams g, MixedConsts mc, const HalfStencil st, int ntypes, con
              double *__restrict__ partial, const PbcRef pb, const double *__restrict__ com,
              int slots, const float4 *__restrict__ spos_lo, int cell0) {
   extern __shared__ float4 s_dyn[];
-  __shared__ MixedWarpSmem sm;
-  __shared__ float s_res[(kEnergy && kForm == FORM_CUTOFF) ? 3 * kBatch : 1];
+  constexpr int kB = kEnergy ? kBatchE : kBatch;
+  __shared__ MixedWarpSmemT<kB> sm;
+  __shared__ float s_res[(kEnergy && kForm == FORM_CUTOFF) ? 3 * kB : 1];
   constexpr bool kLj = kForm == FORM_CUTOFF || kForm == FORM_GENERIC;
   const int nlj = (kLj && !kGlobalLj) ? ntypes * ntypes : 0;
   float4 *s_lj = s_dyn;
@@ -1233,7 +1244,7 @@ k_pair_mixed(GridParams g, MixedConsts mc, const HalfStencil st, int ntypes, con
   const int lane = threadIdx.x;
   for (int k = lane; k < nlj; k += 32) s_lj[k] = lj32[k];
   for (int k = lane; k < st.ncells; k += 32) s_st[k] = st.off[k];
-  for (int t = lane; t < kBatch; t += 32) sm.jf[0][t] = sm.jf[1][t] = sm.jf[2][t] = 0;
+  for (int t = lane; t < kB; t += 32) sm.jf[0][t] = sm.jf[1][t] = sm.jf[2][t] = 0;
   sm.fi[0][lane] = sm.fi[1][lane] = sm.fi[2][lane] = 0;
   __syncwarp();
   // a launch that overlaps the cell build's last kernel waits for it here,
@@ -1241,7 +1252,7 @@ k_pair_mixed(GridParams g, MixedConsts mc, const HalfStencil st, int ntypes, con
   pdl_wait();
   const int cell = cell0 + (int)(blockIdx.x / slots);  // cells cell0.. (a shard's range)
   if (cell >= g.ncell) return;  // uniform per block
-  mixed_task<kForm, kEnergy, kVirial, kMolVir>(
+  mixed_task<kForm, kEnergy, kVirial, kMolVir, MixedWarpSmemT<kB>>(
       g, mc, s_st, st.ncells, blockIdx.x % slots, slots, ntypes, kGlobalLj ? lj32 : s_lj, cell,
       start,
       spos, smeta, sidx, ex_start, ex, facc, n, partial + (size_t)blockIdx.x * kNacc, pb, com,
