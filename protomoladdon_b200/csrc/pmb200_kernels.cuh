@@ -553,7 +553,9 @@ __device__ __forceinline__ int lanes_per_atom(int m) {
 #ifndef PMB200_STAGE_BATCH
 #define PMB200_STAGE_BATCH 128
 #endif
-constexpr int kBatch = PMB200_STAGE_BATCH;  // staged j atoms per warp batch (<= 256)
+// staged j atoms per warp batch: at most 128, for the byte-wide list indices
+// and the int32 shared force sums (checked where the batch is used)
+constexpr int kBatch = PMB200_STAGE_BATCH;
 #ifndef PMB200_STAGE_BATCH_E
 #define PMB200_STAGE_BATCH_E PMB200_STAGE_BATCH
 #endif
@@ -630,6 +632,13 @@ __device__ __forceinline__ void mixed_task(
   constexpr bool kExactE = kEnergy && kForm == FORM_CUTOFF;
   float *rsx = kExactE ? s_res : nullptr;
   constexpr int kBatch = Smem::kCap;  // this kernel's staging batch
+  // the int32 shared sums: a staged j atom meets each of a chunk's (at most
+  // 32) i atoms once per batch, each contribution within kJLimit quanta; a
+  // lane's dealt i-force sums take at most kBatch / 2 contributions per batch,
+  // each within kJLimit / 2
+  static_assert(32.0 * (double)kJLimit < 2147483648.0, "j-force sums fit int32");
+  static_assert((double)(kBatch / 2) * 0.5 * (double)kJLimit < 2147483648.0,
+                "dealt i-force sums fit int32");
   float *rsy = kExactE ? rsx + kBatch : nullptr, *rsz = kExactE ? rsx + 2 * kBatch : nullptr;
   const int cx = cell % g.nx;
   const int cy = (cell / g.nx) % g.ny;
