@@ -1533,6 +1533,10 @@ int pmb200_shard_finalize(pmb200_ctx *c, const long long *d_facc, double *d_forc
 
 // Derivative kernels (FP64 pair arithmetic whatever the context's
 // precision; cutoff form only).
+#ifndef PMB200_HVP_SLOTS
+#define PMB200_HVP_SLOTS 4
+#endif
+constexpr int kHvpSlots = PMB200_HVP_SLOTS;  // warps per i-cell of k_hvp_fp64_half
 static int launch_deriv(pmb200_ctx *c, int mode, const double *d_pos, const double *d_w,
                         double *d_hv, double *d_dq, double *d_dlj, cudaStream_t st) {
   const GridParams &g = c->g;
@@ -1564,9 +1568,22 @@ static int launch_deriv(pmb200_ctx *c, int mode, const double *d_pos, const doub
     CK(dalloc(c->d_wsorted, (size_t)std::max(c->n, 1)));
     c->ws_alloc = (size_t)std::max(c->n, 1);
   }
-  launch_cell_build(c, d_pos, false, false, st);
+  // a plain Hessian-vector product: the half-shell kernel into the
+  // fixed-point accumulator (cleared by the cell build)
+  const bool half = mode == DERIV_VJP && !params;
+  launch_cell_build(c, d_pos, false, false, st, half ? c->d_facc : nullptr, 6);
   const size_t smem = sizeof(double) * nt4;
-  if (mode == DERIV_PARAMS) {
+  if (half) {
+    if (c->n > 0) {
+      k_gather_sorted<<<(c->n + 255) / 256, 256, 0, st>>>(c->n, c->d_sidx, d_w, c->d_wsorted);
+      k_hvp_fp64_half<<<(unsigned)g.ncell * kHvpSlots, 32, 0, st>>>(
+          g, c->fc, c->half, kHvpSlots, c->ntypes, c->d_lj64, c->d_start, c->d_spos64,
+          c->d_smeta, c->d_sidx, c->d_ex_start, c->d_ex, c->d_wsorted, c->d_facc, c->n,
+          c->d_err);
+      k_finalize64<<<(unsigned)((c->n + 255) / 256), 256, 0, st>>>(c->n, c->d_facc, c->d_sidx,
+                                                                   0, d_hv);
+    }
+  } else if (mode == DERIV_PARAMS) {
     k_deriv_fp64<DERIV_PARAMS><<<blocks, 128, smem, st>>>(
         g, c->fc, c->stencil, c->ntypes, c->d_lj64, c->d_start, c->d_spos64, c->d_smeta,
         c->d_sidx, c->d_ex_start, c->d_ex, nullptr, nullptr, d_dq, c->d_tpart);
@@ -1649,7 +1666,7 @@ static int device_error(pmb200_ctx *c, int e) {
   CK(cudaMemset(c->d_err, 0, sizeof(int)));
   if (e & 1) return fail(c, PMB200_EDEVICE, "non-finite atom position in an evaluation");
   return fail(c, PMB200_EDEVICE,
-              "a pair force exceeded the mixed kernel's fixed-point range (atoms overlap)");
+              "a pair term exceeded the fixed-point accumulator's range (atoms overlap)");
 }
 
 int pmb200_sync(pmb200_ctx *c) {

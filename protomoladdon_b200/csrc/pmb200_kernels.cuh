@@ -1788,6 +1788,46 @@ __global__ void k_finalize64(int n, const unsigned long long *__restrict__ acc,
 // ---------------------------------------------------------------------------
 enum DerivMode { DERIV_PARAMS = 0, DERIV_VJP = 1 };
 
+// One pair's terms in s = r^2: the LJ energy E = A s^-6 - B s^-3 and its
+// s-derivatives, the C2 switch S and its derivatives (polynomials in s), f q_j
+// and the C1-shifted Coulomb phi with its derivatives (zero beyond rc).
+// Shared by the derivative kernels, so that they round every pair alike.
+struct DerivTerms {
+  double is, is3, is6, E, Es, Ess, S, Ss, Sss, qf, phi, phis, phiss;
+};
+__device__ __forceinline__ DerivTerms deriv_terms(const Fp64Consts &mc,
+                                                  const double4 *__restrict__ lj64, int tab,
+                                                  int kind, double s, double qj) {
+  DerivTerms u;
+  const double4 p = lj64[tab];
+  const double A = kind == 1 ? p.z : p.x;
+  const double B = kind == 1 ? p.w : p.y;
+  u.is = 1.0 / s;
+  u.is3 = u.is * u.is * u.is;
+  u.is6 = u.is3 * u.is3;
+  u.E = A * u.is6 - B * u.is3;
+  u.Es = (-6.0 * A * u.is6 + 3.0 * B * u.is3) * u.is;
+  u.Ess = (42.0 * A * u.is6 - 12.0 * B * u.is3) * u.is * u.is;
+  u.S = 1.0; u.Ss = 0.0; u.Sss = 0.0;
+  if (s > mc.rclj2) {
+    u.S = 0.0;
+  } else if (s >= mc.ron2) {
+    const double c2 = mc.rclj2 - s;
+    u.S = mc.s1 * c2 * c2 * (mc.s2 + 2.0 * s);
+    u.Ss = 2.0 * mc.s1 * c2 * (c2 - mc.s2 - 2.0 * s);
+    u.Sss = 2.0 * mc.s1 * (mc.s2 + 2.0 * s - 4.0 * c2);
+  }
+  u.qf = qj * (kind == 1 ? mc.csf : 1.0);  // f q_j
+  u.phi = 0.0; u.phis = 0.0; u.phiss = 0.0;
+  if (s <= mc.rcc2) {
+    const double ir = 1.0 / sqrt(s);
+    u.phi = ir - mc.c15_1 + mc.c05_3 * s;
+    u.phis = -0.5 * ir * u.is + mc.c05_3;
+    u.phiss = 0.75 * ir * u.is * u.is;
+  }
+  return u;
+}
+
 // kParams: also the parameter derivatives (dq, the table partials); a
 // VJP launch without them computes H w alone.  In VJP mode w is read in the
 // sorted order (ws[j] = w of sorted atom j, gathered by k_gather_sorted).
@@ -1875,31 +1915,10 @@ k_deriv_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes,
               kind = excl_kind(ex, elo, ehi, sidx[j]);
               if (kind == 2) continue;
             }
-            const double4 p = lj64[ti + mj.x];
-            const double A = kind == 1 ? p.z : p.x;
-            const double B = kind == 1 ? p.w : p.y;
-            const double is = 1.0 / s;
-            const double is3 = is * is * is, is6 = is3 * is3;
-            const double E = A * is6 - B * is3;
-            const double Es = (-6.0 * A * is6 + 3.0 * B * is3) * is;
-            const double Ess = (42.0 * A * is6 - 12.0 * B * is3) * is * is;
-            double S = 1.0, Ss = 0.0, Sss = 0.0;
-            if (s > mc.rclj2) {
-              S = 0.0;
-            } else if (s >= mc.ron2) {
-              const double c2 = mc.rclj2 - s;
-              S = mc.s1 * c2 * c2 * (mc.s2 + 2.0 * s);
-              Ss = 2.0 * mc.s1 * c2 * (c2 - mc.s2 - 2.0 * s);
-              Sss = 2.0 * mc.s1 * (mc.s2 + 2.0 * s - 4.0 * c2);
-            }
-            const double qf = pj.w * (kind == 1 ? mc.csf : 1.0);  // f q_j
-            double phi = 0.0, phis = 0.0, phiss = 0.0;
-            if (s <= mc.rcc2) {
-              const double ir = 1.0 / sqrt(s);
-              phi = ir - mc.c15_1 + mc.c05_3 * s;
-              phis = -0.5 * ir * is + mc.c05_3;
-              phiss = 0.75 * ir * is * is;
-            }
+            const DerivTerms u = deriv_terms(mc, lj64, ti + mj.x, kind, s, pj.w);
+            const double E = u.E, Es = u.Es, Ess = u.Ess, S = u.S, Ss = u.Ss, Sss = u.Sss;
+            const double is = u.is, is3 = u.is3, is6 = u.is6;
+            const double qf = u.qf, phi = u.phi, phis = u.phis, phiss = u.phiss;
             const int tab = (ti + mj.x) * 4 + (kind == 1 ? 2 : 0);
             if (kMode == DERIV_PARAMS) {
               gq += qf * phi;
@@ -1952,6 +1971,185 @@ k_deriv_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes,
     __syncthreads();
     for (int k = threadIdx.x; k < nt4; k += blockDim.x)
       tpart[(size_t)blockIdx.x * nt4 + k] = s_tab[k];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Hessian-vector product on the half shell (the kernel of products asked for
+// no parameter derivative): k_pair_fp64_half's task split -- one warp per
+// block, `slots` warps per i-cell, each a share of the half-shell cell
+// offsets (home-cell pairs i < j) -- its staging (j atoms in the i-cell
+// frame, with their direction, kB64 at a time, those farther than the cutoff
+// from the box around the chunk's i atoms left out) and its conflict-free
+// block rotation, with deriv_terms' per-pair arithmetic.  Each pair is
+// evaluated once: its block K (w_i - w_j), K = 2 U_s I + 4 U_ss d d^T, goes
+// to hv_i and, K being even in d = x_j - x_i, its negative to hv_j.  Both
+// sums reach acc[6][n] (sorted order, cleared by the cell build) as the
+// exact two-word fixed point of fix2_add, so the product does not depend on
+// the order of the sums; k_finalize64 writes it in the caller's order.
+// ---------------------------------------------------------------------------
+struct HvpWarpSmem {
+  double4 pos[kB64];   // staged j: position in the i-cell frame (A), charge
+  double4 w[kB64];     // its direction (w.w unused)
+  int2 meta[kB64];     // type, molecule
+  int jidx[kB64];      // sorted index; bit 31: an atom of the home cell
+  double jh[3][kB64];  // the batch's hv_j sums
+};
+
+#ifndef PMB200_HVP_BLOCKS
+#define PMB200_HVP_BLOCKS 24
+#endif
+__global__ void __launch_bounds__(32, PMB200_HVP_BLOCKS)
+k_hvp_fp64_half(GridParams g, Fp64Consts mc, const HalfStencil st, int slots, int ntypes,
+                const double4 *__restrict__ lj64, const int *__restrict__ start,
+                const double4 *__restrict__ spos, const int2 *__restrict__ smeta,
+                const int *__restrict__ sidx, const int *__restrict__ ex_start,
+                const int2 *__restrict__ ex, const double4 *__restrict__ ws,
+                unsigned long long *__restrict__ acc, int n, int *__restrict__ err) {
+  __shared__ HvpWarpSmem sm;
+  const int lane = threadIdx.x;
+  const int cell = (int)(blockIdx.x / slots), slot = (int)(blockIdx.x % slots);
+  if (cell >= g.ncell) return;  // uniform per block
+  const int cx = cell % g.nx;
+  const int cy = (cell / g.nx) % g.ny;
+  const int cz = cell / (g.nx * g.ny);
+  const int cs = start[cell], ce = start[cell + 1];
+  for (int t = lane; t < kB64; t += 32) sm.jh[0][t] = sm.jh[1][t] = sm.jh[2][t] = 0.0;
+  for (int c0 = cs; c0 < ce; c0 += 32) {
+    const int m = min(32, ce - c0);
+    const int L = lanes_per_atom(m);
+    const int ia = lane / L;
+    const int sub = lane % L;
+    const bool active = ia < m;
+    const int i = c0 + (active ? ia : 0);
+    const double4 pi = spos[i];
+    const double4 wi = ws[i];
+    const int2 mi = smeta[i];
+    const int oi = sidx[i];
+    const int elo = ex_start[oi], ehi = ex_start[oi + 1];
+    const int ti = mi.x * ntypes;
+    double hx = 0, hy = 0, hz = 0;
+    // the box around the chunk's i atoms
+    double blo_x = pi.x, blo_y = pi.y, blo_z = pi.z, bhi_x = pi.x, bhi_y = pi.y, bhi_z = pi.z;
+    for (int off = 16; off > 0; off >>= 1) {
+      blo_x = fmin(blo_x, __shfl_xor_sync(0xffffffffu, blo_x, off));
+      blo_y = fmin(blo_y, __shfl_xor_sync(0xffffffffu, blo_y, off));
+      blo_z = fmin(blo_z, __shfl_xor_sync(0xffffffffu, blo_z, off));
+      bhi_x = fmax(bhi_x, __shfl_xor_sync(0xffffffffu, bhi_x, off));
+      bhi_y = fmax(bhi_y, __shfl_xor_sync(0xffffffffu, bhi_y, off));
+      bhi_z = fmax(bhi_z, __shfl_xor_sync(0xffffffffu, bhi_z, off));
+    }
+    int nb = 0;
+    // every i atom of the chunk against the nb staged atoms (atom ia's lanes
+    // take block (ia + k) mod nsteps at step k: no two lanes meet one staged
+    // atom in a step), then the hv_j sums out and the batch emptied
+    auto process = [&]() {
+      __syncwarp();
+      const int nblk = (nb + L - 1) / L;
+      const int nsteps = max(nblk, m);
+      for (int k = 0; k < nsteps; k++) {
+        int blk = ia + k;
+        if (blk >= nsteps) blk -= nsteps;
+        const int t = blk * L + sub;
+        if (active && t < nb) {
+          const int jw = sm.jidx[t];
+          const int j = jw & 0x7fffffff;
+          const double4 pj = sm.pos[t];
+          const double ddx = pj.x - pi.x;
+          const double ddy = pj.y - pi.y;
+          const double ddz = pj.z - pi.z;
+          const double s = ddx * ddx + ddy * ddy + ddz * ddz;
+          const int2 mj = sm.meta[t];
+          int kind = (jw < 0 && j <= i) ? 2 : 0;  // home cell: pairs i < j only
+          const bool near = s <= mc.cut2 && s > 0.0;
+          if (kind == 0 && near && mj.y == mi.y) kind = excl_kind(ex, elo, ehi, sidx[j]);
+          if (kind != 2 && near) {
+            const DerivTerms u = deriv_terms(mc, lj64, ti + mj.x, kind, s, pj.w);
+            const double4 wj = sm.w[t];
+            const double dl0 = wi.x - wj.x, dl1 = wi.y - wj.y, dl2 = wi.z - wj.z;
+            const double dd = ddx * dl0 + ddy * dl1 + ddz * dl2;  // d . (w_i - w_j)
+            const double Us = u.Ss * u.E + u.S * u.Es + pi.w * u.qf * u.phis;
+            const double Uss =
+                u.Sss * u.E + 2.0 * u.Ss * u.Es + u.S * u.Ess + pi.w * u.qf * u.phiss;
+            const double a = 2.0 * Us, b = 4.0 * Uss * dd;
+            const double vx = a * dl0 + b * ddx, vy = a * dl1 + b * ddy, vz = a * dl2 + b * ddz;
+            hx += vx; hy += vy; hz += vz;
+            sm.jh[0][t] -= vx;
+            sm.jh[1][t] -= vy;
+            sm.jh[2][t] -= vz;
+          }
+        }
+        __syncwarp();
+      }
+      for (int t = lane; t < nb; t += 32) {
+        const size_t j = (size_t)(sm.jidx[t] & 0x7fffffff);
+#pragma unroll
+        for (int qq = 0; qq < 3; qq++) {
+          const double v = sm.jh[qq][t];
+          if (v != 0.0) fix2_add(acc, (size_t)n, j, qq, v, err);
+          sm.jh[qq][t] = 0.0;
+        }
+      }
+      nb = 0;
+      __syncwarp();
+    };
+    for (int q = slot; q < st.ncells; q += slots) {
+      const unsigned o = st.off[q];
+      const int dx = (int)(o & 31u) - 8, dy = (int)((o >> 5) & 31u) - 8,
+                dz = (int)((o >> 10) & 31u) - 8;
+      const int homebit = (dx | dy | dz) == 0 ? (int)0x80000000u : 0;
+      int jx = cx + dx, jy = cy + dy, jz = cz + dz;
+      if (g.periodic) {
+        // one wrap suffices: offsets reach at most ceil(rc / edge) <= n / 2
+        jx += jx < 0 ? g.nx : (jx >= g.nx ? -g.nx : 0);
+        jy += jy < 0 ? g.ny : (jy >= g.ny ? -g.ny : 0);
+        jz += jz < 0 ? g.nz : (jz >= g.nz ? -g.nz : 0);
+      } else if (jx < 0 || jx >= g.nx || jy < 0 || jy >= g.ny || jz < 0 || jz >= g.nz) {
+        continue;  // uniform per warp
+      }
+      const int jc = (jz * g.ny + jy) * g.nx + jx;
+      const int js = start[jc], cnt = start[jc + 1] - js;
+      double sx, sy, sz;  // the neighbour cell's shift (A)
+      cell_shift(g, g.ec, 1.0, dx, dy, dz, sx, sy, sz);
+      for (int f0 = 0; f0 < cnt;) {
+        const int take = min(min(cnt - f0, kB64 - nb), 32);
+        bool keep = false;
+        double4 p = make_double4(0.0, 0.0, 0.0, 0.0);
+        const int j = js + f0 + lane;
+        if (lane < take) {
+          p = spos[j];
+          p.x += sx; p.y += sy; p.z += sz;
+          // squared distance to the box (no pair the test accepts is dropped:
+          // per axis at most |p - x_i| for every i of the chunk)
+          const double bx = fmax(fmax(blo_x - p.x, p.x - bhi_x), 0.0);
+          const double by = fmax(fmax(blo_y - p.y, p.y - bhi_y), 0.0);
+          const double bz = fmax(fmax(blo_z - p.z, p.z - bhi_z), 0.0);
+          keep = bx * bx + by * by + bz * bz <= mc.cut2;
+        }
+        const unsigned km = __ballot_sync(0xffffffffu, keep);
+        if (keep) {
+          const int slot_ = nb + __popc(km & ((1u << lane) - 1u));
+          sm.pos[slot_] = p;
+          sm.w[slot_] = ws[j];
+          sm.meta[slot_] = smeta[j];
+          sm.jidx[slot_] = j | homebit;
+        }
+        nb += __popc(km);
+        f0 += take;
+        if (nb > kB64 - 32) process();  // less than a full round of room left
+      }
+    }
+    if (nb > 0) process();
+    for (int off = 1; off < L; off <<= 1) {
+      hx += __shfl_xor_sync(0xffffffffu, hx, off);
+      hy += __shfl_xor_sync(0xffffffffu, hy, off);
+      hz += __shfl_xor_sync(0xffffffffu, hz, off);
+    }
+    if (active && sub == 0) {
+      fix2_add(acc, (size_t)n, (size_t)i, 0, hx, err);
+      fix2_add(acc, (size_t)n, (size_t)i, 1, hy, err);
+      fix2_add(acc, (size_t)n, (size_t)i, 2, hz, err);
+    }
   }
 }
 

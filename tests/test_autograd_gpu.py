@@ -211,5 +211,33 @@ def test_medium_box_hvp_and_charge_gradient_against_fd():
     assert abs(dq[100].item() - fd) <= 1e-6 * abs(fd)
 
 
+@pytest.fixture(scope="module")
+def medium():
+    return water.medium_41k()
+
+
+@pytest.mark.parametrize("fx", ["small", "ions", "medium"])
+def test_hvp_half_shell_kernel(fx, request):
+    """A plain Hessian-vector product (the half-shell kernel, each pair once,
+    fixed-point sums) against the same product asked with dE/dq (the
+    full-shell kernel, each pair from both atoms): relative <= 1e-12; two
+    plain products bit-identical."""
+    s = request.getfixturevalue(fx)
+    m, pos, q, t = make(s)
+    rng = np.random.default_rng(11)
+    v = rng.standard_normal(s["pos"].shape)
+    vt = torch.tensor(v / np.linalg.norm(v), device="cuda")
+    h1, h2, hf = (torch.empty_like(pos) for _ in range(3))
+    m.force.hvp_device(m.topo, pos.data_ptr(), vt.data_ptr(), h1.data_ptr())
+    m.force.hvp_device(m.topo, pos.data_ptr(), vt.data_ptr(), h2.data_ptr())
+    dq = torch.empty_like(q)
+    m.force.hvp_device(m.topo, pos.data_ptr(), vt.data_ptr(), hf.data_ptr(), dq.data_ptr())
+    torch.cuda.synchronize()
+    m.force.sync()
+    m.close()
+    assert torch.equal(h1, h2)
+    assert rel(h1.cpu().numpy(), hf.cpu().numpy()) <= 1e-12
+
+
 def test_charge_units_constant():
     assert SQRTCOULOMBCONSTANT ** 2 == pytest.approx(332.0636, rel=1e-6)
