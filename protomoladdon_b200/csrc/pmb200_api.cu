@@ -400,7 +400,7 @@ int ensure_atom_buffers(pmb200_ctx *c) {
   CK(dalloc(c->d_rel64, n));
   CK(dalloc(c->d_spos64, n));
   CK(dalloc(c->d_smeta, n));
-  CK(dalloc(c->d_facc, 6 * n));
+  CK(dalloc(c->d_facc, 8 * n));  // FP64 forces: 6 words per atom; derivatives: 8
   CK(dalloc(c->d_cblo, n));
   CK(dalloc(c->d_cbhi, n));
   CK(dalloc(c->d_hpos, 3 * n));
@@ -1532,27 +1532,32 @@ int pmb200_shard_finalize(pmb200_ctx *c, const long long *d_facc, double *d_forc
 }
 
 // Derivative kernels (FP64 pair arithmetic whatever the context's
-// precision; cutoff form only).
+// precision; cutoff form only): the half-shell kernel for Hessian-vector
+// products and, with at most kDerivRegTypes LJ types, for the parameter
+// derivatives; the full-shell kernel for the parameter derivatives of larger
+// tables.
 #ifndef PMB200_HVP_SLOTS
 #define PMB200_HVP_SLOTS 4
 #endif
-constexpr int kHvpSlots = PMB200_HVP_SLOTS;  // warps per i-cell of k_hvp_fp64_half
+constexpr int kDerivSlots = PMB200_HVP_SLOTS;  // warps per i-cell of k_deriv_fp64_half
 static int launch_deriv(pmb200_ctx *c, int mode, const double *d_pos, const double *d_w,
                         double *d_hv, double *d_dq, double *d_dlj, cudaStream_t st) {
   const GridParams &g = c->g;
-  const int blocks = (g.ncell + 3) / 4;
   const size_t nt4 = (size_t)c->ntypes * c->ntypes * 4;
+  const int n = c->n;
   // a Hessian-vector product asked for neither parameter derivative skips them
   const bool params = mode == DERIV_PARAMS || d_dq || d_dlj;
+  const bool half = !params || c->ntypes <= kDerivRegTypes;
+  const int blocks = half ? g.ncell * kDerivSlots : (g.ncell + 3) / 4;
   if (params) {
     if (c->tpart_alloc < (size_t)blocks * nt4) {
       CK(dalloc(c->d_tpart, (size_t)blocks * nt4));
       c->tpart_alloc = (size_t)blocks * nt4;
     }
     if (!d_dq) {
-      if (c->gq_alloc < (size_t)std::max(c->n, 1)) {
-        CK(dalloc(c->d_gq, (size_t)std::max(c->n, 1)));
-        c->gq_alloc = (size_t)std::max(c->n, 1);
+      if (c->gq_alloc < (size_t)std::max(n, 1)) {
+        CK(dalloc(c->d_gq, (size_t)std::max(n, 1)));
+        c->gq_alloc = (size_t)std::max(n, 1);
       }
       d_dq = c->d_gq;
     }
@@ -1564,44 +1569,45 @@ static int launch_deriv(pmb200_ctx *c, int mode, const double *d_pos, const doub
       d_dlj = c->d_glj;
     }
   }
-  if (mode == DERIV_VJP && c->ws_alloc < (size_t)std::max(c->n, 1)) {
-    CK(dalloc(c->d_wsorted, (size_t)std::max(c->n, 1)));
-    c->ws_alloc = (size_t)std::max(c->n, 1);
+  if (mode == DERIV_VJP && c->ws_alloc < (size_t)std::max(n, 1)) {
+    CK(dalloc(c->d_wsorted, (size_t)std::max(n, 1)));
+    c->ws_alloc = (size_t)std::max(n, 1);
   }
-  // a plain Hessian-vector product: the half-shell kernel into the
-  // fixed-point accumulator (cleared by the cell build)
-  const bool half = mode == DERIV_VJP && !params;
-  launch_cell_build(c, d_pos, false, false, st, half ? c->d_facc : nullptr, 6);
-  const size_t smem = sizeof(double) * nt4;
-  if (half) {
-    if (c->n > 0) {
-      k_gather_sorted<<<(c->n + 255) / 256, 256, 0, st>>>(c->n, c->d_sidx, d_w, c->d_wsorted);
-      k_hvp_fp64_half<<<(unsigned)g.ncell * kHvpSlots, 32, 0, st>>>(
-          g, c->fc, c->half, kHvpSlots, c->ntypes, c->d_lj64, c->d_start, c->d_spos64,
-          c->d_smeta, c->d_sidx, c->d_ex_start, c->d_ex, c->d_wsorted, c->d_facc, c->n,
-          c->d_err);
-      k_finalize64<<<(unsigned)((c->n + 255) / 256), 256, 0, st>>>(c->n, c->d_facc, c->d_sidx,
-                                                                   0, d_hv);
-    }
-  } else if (mode == DERIV_PARAMS) {
-    k_deriv_fp64<DERIV_PARAMS><<<blocks, 128, smem, st>>>(
-        g, c->fc, c->stencil, c->ntypes, c->d_lj64, c->d_start, c->d_spos64, c->d_smeta,
-        c->d_sidx, c->d_ex_start, c->d_ex, nullptr, nullptr, d_dq, c->d_tpart);
-  } else {
-    if (c->n > 0)
-      k_gather_sorted<<<(c->n + 255) / 256, 256, 0, st>>>(c->n, c->d_sidx, d_w, c->d_wsorted);
+  // the half-shell kernel sums into the fixed-point accumulator, which the
+  // cell build clears (hv words 0-5, dq words 6-7)
+  launch_cell_build(c, d_pos, false, false, st, half ? c->d_facc : nullptr, params ? 8 : 6);
+  if (mode == DERIV_VJP && n > 0)
+    k_gather_sorted<<<(n + 255) / 256, 256, 0, st>>>(n, c->d_sidx, d_w, c->d_wsorted);
+  if (half && n == 0) {
+    if (params) CK(cudaMemsetAsync(d_dlj, 0, sizeof(double) * nt4, st));
+  } else if (half) {
+#define PMB_DERIV_HALF(M, P)                                                                 \
+  k_deriv_fp64_half<M, P><<<(unsigned)blocks, 32, 0, st>>>(                                 \
+      g, c->fc, c->half, kDerivSlots, c->ntypes, c->d_lj64, c->d_start, c->d_spos64,         \
+      c->d_smeta, c->d_sidx, c->d_ex_start, c->d_ex, c->d_wsorted, c->d_facc, n, c->d_tpart, \
+      c->d_err)
+    if (mode == DERIV_PARAMS) PMB_DERIV_HALF(DERIV_PARAMS, true);
+    else if (params) PMB_DERIV_HALF(DERIV_VJP, true);
+    else PMB_DERIV_HALF(DERIV_VJP, false);
+#undef PMB_DERIV_HALF
+    if (mode == DERIV_VJP)
+      k_finalize64<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, c->d_facc, c->d_sidx, 0,
+                                                                 d_hv);
     if (params)
+      k_finalize_q<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, c->d_facc, c->d_sidx, d_dq);
+  } else {
+    const size_t smem = sizeof(double) * nt4;
+    if (mode == DERIV_PARAMS)
+      k_deriv_fp64<DERIV_PARAMS><<<blocks, 128, smem, st>>>(
+          g, c->fc, c->stencil, c->ntypes, c->d_lj64, c->d_start, c->d_spos64, c->d_smeta,
+          c->d_sidx, c->d_ex_start, c->d_ex, nullptr, nullptr, d_dq, c->d_tpart);
+    else
       k_deriv_fp64<DERIV_VJP, true><<<blocks, 128, smem, st>>>(
           g, c->fc, c->stencil, c->ntypes, c->d_lj64, c->d_start, c->d_spos64, c->d_smeta,
           c->d_sidx, c->d_ex_start, c->d_ex, c->d_wsorted, d_hv, d_dq, c->d_tpart);
-    else
-      k_deriv_fp64<DERIV_VJP, false><<<blocks, 128, smem, st>>>(
-          g, c->fc, c->stencil, c->ntypes, c->d_lj64, c->d_start, c->d_spos64, c->d_smeta,
-          c->d_sidx, c->d_ex_start, c->d_ex, c->d_wsorted, d_hv, nullptr, nullptr);
   }
-  if (params)
-    k_reduce_columns<<<(int)((nt4 + 127) / 128), 128, 0, st>>>(blocks, (int)nt4, c->d_tpart,
-                                                                 d_dlj);
+  if (params && !(half && n == 0))
+    k_reduce_columns<<<(unsigned)nt4, 256, 0, st>>>(blocks, (int)nt4, c->d_tpart, d_dlj);
   CK(cudaGetLastError());
   return PMB200_OK;
 }

@@ -1783,8 +1783,8 @@ __global__ void k_finalize64(int n, const unsigned long long *__restrict__ acc,
 // DERIV_VJP: for a direction w (3n), hv = H w (hv_i = sum_j K (w_i - w_j)),
 //   and the derivatives of w . grad E = sum_pairs 2 U_s d.(w_j - w_i) with
 //   respect to q_i (dq) and to the table entries (tpart), as above.
-// Table sums go through shared memory to per-block rows of tpart
-// ([gridDim.x][ntypes^2 * 4]); k_reduce_columns adds the rows in order.
+// Table sums go through shared memory to one column entry per block of
+// tpart ([ntypes^2 * 4][gridDim.x]); k_reduce_columns adds them up.
 // ---------------------------------------------------------------------------
 enum DerivMode { DERIV_PARAMS = 0, DERIV_VJP = 1 };
 
@@ -1970,43 +1970,80 @@ k_deriv_fp64(GridParams g, Fp64Consts mc, const Stencil st, int ntypes,
   if (kParams) {
     __syncthreads();
     for (int k = threadIdx.x; k < nt4; k += blockDim.x)
-      tpart[(size_t)blockIdx.x * nt4 + k] = s_tab[k];
+      tpart[(size_t)k * gridDim.x + blockIdx.x] = s_tab[k];
   }
 }
 
 // ---------------------------------------------------------------------------
-// Hessian-vector product on the half shell (the kernel of products asked for
-// no parameter derivative): k_pair_fp64_half's task split -- one warp per
-// block, `slots` warps per i-cell, each a share of the half-shell cell
-// offsets (home-cell pairs i < j) -- its staging (j atoms in the i-cell
-// frame, with their direction, kB64 at a time, those farther than the cutoff
-// from the box around the chunk's i atoms left out) and its conflict-free
-// block rotation, with deriv_terms' per-pair arithmetic.  Each pair is
-// evaluated once: its block K (w_i - w_j), K = 2 U_s I + 4 U_ss d d^T, goes
-// to hv_i and, K being even in d = x_j - x_i, its negative to hv_j.  Both
-// sums reach acc[6][n] (sorted order, cleared by the cell build) as the
-// exact two-word fixed point of fix2_add, so the product does not depend on
-// the order of the sums; k_finalize64 writes it in the caller's order.
+// The derivative kernel on the half shell: k_pair_fp64_half's task split --
+// one warp per block, `slots` warps per i-cell, each a share of the
+// half-shell cell offsets (home-cell pairs i < j) -- its staging (j atoms in
+// the i-cell frame, kB64 at a time, with their direction in DERIV_VJP mode;
+// those farther than the cutoff from the box around the chunk's i atoms left
+// out) and its conflict-free block rotation, with deriv_terms' per-pair
+// arithmetic.  Each pair is evaluated once and its terms go to both atoms:
+// DERIV_VJP: K (w_i - w_j), K = 2 U_s I + 4 U_ss d d^T, to hv_i and, K being
+//   even in d = x_j - x_i, its negative to hv_j;
+// kParams: c = f phi (DERIV_PARAMS) or f phi_s T, T = 2 d.(w_j - w_i) (even
+//   in d too): q_j c to dq_i and q_i c to dq_j; the table terms (halved) to
+//   the entries (a, b) and (b, a) of the pair's types -- the terms of
+//   k_deriv_fp64's two visits of the pair.
+// hv and dq reach acc (sorted order, cleared by the cell build: words
+// {hi x, hi y, hi z, lo x, lo y, lo z} of hv, then {hi, lo} of dq) as the
+// exact two-word fixed point of fix2_add, so they do not depend on the order
+// of the sums; k_finalize64 and k_finalize_q write them in the caller's order.
+// Table sums (kParams; at most kDerivRegTypes types, summed per lane in
+// registers by j type, modified pairs in shared memory) leave one column
+// entry per block: tpart[entry][block], added up by k_reduce_columns.
 // ---------------------------------------------------------------------------
-struct HvpWarpSmem {
-  double4 pos[kB64];   // staged j: position in the i-cell frame (A), charge
-  double4 w[kB64];     // its direction (w.w unused)
-  int2 meta[kB64];     // type, molecule
-  int jidx[kB64];      // sorted index; bit 31: an atom of the home cell
-  double jh[3][kB64];  // the batch's hv_j sums
+constexpr int kDerivRegTypes = 4;
+constexpr int kDerivTab = kDerivRegTypes * kDerivRegTypes * 4;
+struct DerivWarpSmem {
+  double4 pos[kB64];    // staged j: position in the i-cell frame (A), charge
+  double4 w[kB64];      // its direction (w.w unused; DERIV_VJP)
+  int2 meta[kB64];      // type, molecule
+  int jidx[kB64];       // sorted index; bit 31: an atom of the home cell
+  double jh[3][kB64];   // the batch's hv_j sums
+  double jq[kB64];      // the batch's dq_j sums
+  double tab[kDerivTab];  // the block's table sums
 };
 
+// v into the two-word fixed-point words rhi, rlo of atom j (fix2_add's split)
+__device__ __forceinline__ void fix2_add_rows(unsigned long long *__restrict__ acc, size_t n,
+                                              size_t j, int rhi, int rlo, double v,
+                                              int *__restrict__ err) {
+  if (!(fabs(v) < kFix2Max)) {
+    atomicOr(err, 2);
+    return;
+  }
+  const double s = v * kFix2Hi;
+  const double h = rint(s);
+  const long long hi = (long long)h;
+  const long long lo = __double2ll_rn((s - h) * kFix2Lo);
+  if (hi) atomicAdd(&acc[(size_t)rhi * n + j], (unsigned long long)hi);
+  if (lo) atomicAdd(&acc[(size_t)rlo * n + j], (unsigned long long)lo);
+}
+
 #ifndef PMB200_HVP_BLOCKS
+// resident blocks per SM asked of the Hessian-vector product kernel
+// (measured on the 41k water box: 12, 16, 20, 24 blocks 0.468, 0.473, 0.455,
+// 0.446 ms per product)
 #define PMB200_HVP_BLOCKS 24
 #endif
-__global__ void __launch_bounds__(32, PMB200_HVP_BLOCKS)
-k_hvp_fp64_half(GridParams g, Fp64Consts mc, const HalfStencil st, int slots, int ntypes,
-                const double4 *__restrict__ lj64, const int *__restrict__ start,
-                const double4 *__restrict__ spos, const int2 *__restrict__ smeta,
-                const int *__restrict__ sidx, const int *__restrict__ ex_start,
-                const int2 *__restrict__ ex, const double4 *__restrict__ ws,
-                unsigned long long *__restrict__ acc, int n, int *__restrict__ err) {
-  __shared__ HvpWarpSmem sm;
+#ifndef PMB200_DERIV_PARAM_BLOCKS
+#define PMB200_DERIV_PARAM_BLOCKS 16
+#endif
+template <int kMode, bool kParams>
+__global__ void __launch_bounds__(32, kParams ? PMB200_DERIV_PARAM_BLOCKS : PMB200_HVP_BLOCKS)
+k_deriv_fp64_half(GridParams g, Fp64Consts mc, const HalfStencil st, int slots, int ntypes,
+                  const double4 *__restrict__ lj64, const int *__restrict__ start,
+                  const double4 *__restrict__ spos, const int2 *__restrict__ smeta,
+                  const int *__restrict__ sidx, const int *__restrict__ ex_start,
+                  const int2 *__restrict__ ex, const double4 *__restrict__ ws,
+                  unsigned long long *__restrict__ acc, int n, double *__restrict__ tpart,
+                  int *__restrict__ err) {
+  constexpr bool kVjp = kMode == DERIV_VJP;
+  __shared__ DerivWarpSmem sm;
   const int lane = threadIdx.x;
   const int cell = (int)(blockIdx.x / slots), slot = (int)(blockIdx.x % slots);
   if (cell >= g.ncell) return;  // uniform per block
@@ -2014,7 +2051,12 @@ k_hvp_fp64_half(GridParams g, Fp64Consts mc, const HalfStencil st, int slots, in
   const int cy = (cell / g.nx) % g.ny;
   const int cz = cell / (g.nx * g.ny);
   const int cs = start[cell], ce = start[cell + 1];
-  for (int t = lane; t < kB64; t += 32) sm.jh[0][t] = sm.jh[1][t] = sm.jh[2][t] = 0.0;
+  for (int t = lane; t < kB64; t += 32) {
+    sm.jh[0][t] = sm.jh[1][t] = sm.jh[2][t] = 0.0;
+    sm.jq[t] = 0.0;
+  }
+  if (kParams)
+    for (int t = lane; t < kDerivTab; t += 32) sm.tab[t] = 0.0;
   for (int c0 = cs; c0 < ce; c0 += 32) {
     const int m = min(32, ce - c0);
     const int L = lanes_per_atom(m);
@@ -2023,12 +2065,14 @@ k_hvp_fp64_half(GridParams g, Fp64Consts mc, const HalfStencil st, int slots, in
     const bool active = ia < m;
     const int i = c0 + (active ? ia : 0);
     const double4 pi = spos[i];
-    const double4 wi = ws[i];
+    const double4 wi = kVjp ? ws[i] : make_double4(0.0, 0.0, 0.0, 0.0);
     const int2 mi = smeta[i];
     const int oi = sidx[i];
     const int elo = ex_start[oi], ehi = ex_start[oi + 1];
     const int ti = mi.x * ntypes;
-    double hx = 0, hy = 0, hz = 0;
+    double hx = 0, hy = 0, hz = 0, gq = 0;
+    // the lane's plain pairs' table terms by j type
+    double ta[kDerivRegTypes] = {0.0, 0.0, 0.0, 0.0}, tb[kDerivRegTypes] = {0.0, 0.0, 0.0, 0.0};
     // the box around the chunk's i atoms
     double blo_x = pi.x, blo_y = pi.y, blo_z = pi.z, bhi_x = pi.x, bhi_y = pi.y, bhi_z = pi.z;
     for (int off = 16; off > 0; off >>= 1) {
@@ -2042,7 +2086,7 @@ k_hvp_fp64_half(GridParams g, Fp64Consts mc, const HalfStencil st, int slots, in
     int nb = 0;
     // every i atom of the chunk against the nb staged atoms (atom ia's lanes
     // take block (ia + k) mod nsteps at step k: no two lanes meet one staged
-    // atom in a step), then the hv_j sums out and the batch emptied
+    // atom in a step), then the j sums out and the batch emptied
     auto process = [&]() {
       __syncwarp();
       const int nblk = (nb + L - 1) / L;
@@ -2065,29 +2109,65 @@ k_hvp_fp64_half(GridParams g, Fp64Consts mc, const HalfStencil st, int slots, in
           if (kind == 0 && near && mj.y == mi.y) kind = excl_kind(ex, elo, ehi, sidx[j]);
           if (kind != 2 && near) {
             const DerivTerms u = deriv_terms(mc, lj64, ti + mj.x, kind, s, pj.w);
-            const double4 wj = sm.w[t];
-            const double dl0 = wi.x - wj.x, dl1 = wi.y - wj.y, dl2 = wi.z - wj.z;
-            const double dd = ddx * dl0 + ddy * dl1 + ddz * dl2;  // d . (w_i - w_j)
-            const double Us = u.Ss * u.E + u.S * u.Es + pi.w * u.qf * u.phis;
-            const double Uss =
-                u.Sss * u.E + 2.0 * u.Ss * u.Es + u.S * u.Ess + pi.w * u.qf * u.phiss;
-            const double a = 2.0 * Us, b = 4.0 * Uss * dd;
-            const double vx = a * dl0 + b * ddx, vy = a * dl1 + b * ddy, vz = a * dl2 + b * ddz;
-            hx += vx; hy += vy; hz += vz;
-            sm.jh[0][t] -= vx;
-            sm.jh[1][t] -= vy;
-            sm.jh[2][t] -= vz;
+            double T = 0.0;
+            if (kVjp) {
+              const double4 wj = sm.w[t];
+              const double dl0 = wi.x - wj.x, dl1 = wi.y - wj.y, dl2 = wi.z - wj.z;
+              const double dd = ddx * dl0 + ddy * dl1 + ddz * dl2;  // d . (w_i - w_j)
+              const double Us = u.Ss * u.E + u.S * u.Es + pi.w * u.qf * u.phis;
+              const double Uss =
+                  u.Sss * u.E + 2.0 * u.Ss * u.Es + u.S * u.Ess + pi.w * u.qf * u.phiss;
+              const double a = 2.0 * Us, b = 4.0 * Uss * dd;
+              const double vx = a * dl0 + b * ddx, vy = a * dl1 + b * ddy,
+                           vz = a * dl2 + b * ddz;
+              hx += vx; hy += vy; hz += vz;
+              sm.jh[0][t] -= vx;
+              sm.jh[1][t] -= vy;
+              sm.jh[2][t] -= vz;
+              T = -2.0 * dd;
+            }
+            if (kParams) {
+              const double c = kVjp ? u.phis * T : u.phi;
+              gq += u.qf * c;                                      // f q_j c
+              sm.jq[t] += pi.w * (kind == 1 ? mc.csf : 1.0) * c;  // f q_i c
+              double va, vb;
+              if (kVjp) {
+                va = 0.5 * T * (u.Ss * u.is6 - 6.0 * u.S * u.is6 * u.is);
+                vb = 0.5 * T * (-u.Ss * u.is3 + 3.0 * u.S * u.is3 * u.is);
+              } else {
+                va = 0.5 * u.S * u.is6;
+                vb = -0.5 * u.S * u.is3;
+              }
+              if (kind == 0) {
+#pragma unroll
+                for (int q = 0; q < kDerivRegTypes; q++)
+                  if (q == mj.x) { ta[q] += va; tb[q] += vb; }
+              } else {  // a modified pair: entries 2, 3 of both orders
+                const int e1 = (ti + mj.x) * 4 + 2, e2 = (mj.x * ntypes + mi.x) * 4 + 2;
+                atomicAdd(&sm.tab[e1], va);
+                atomicAdd(&sm.tab[e1 + 1], vb);
+                atomicAdd(&sm.tab[e2], va);
+                atomicAdd(&sm.tab[e2 + 1], vb);
+              }
+            }
           }
         }
         __syncwarp();
       }
       for (int t = lane; t < nb; t += 32) {
         const size_t j = (size_t)(sm.jidx[t] & 0x7fffffff);
+        if (kVjp) {
 #pragma unroll
-        for (int qq = 0; qq < 3; qq++) {
-          const double v = sm.jh[qq][t];
-          if (v != 0.0) fix2_add(acc, (size_t)n, j, qq, v, err);
-          sm.jh[qq][t] = 0.0;
+          for (int qq = 0; qq < 3; qq++) {
+            const double v = sm.jh[qq][t];
+            if (v != 0.0) fix2_add_rows(acc, (size_t)n, j, qq, 3 + qq, v, err);
+            sm.jh[qq][t] = 0.0;
+          }
+        }
+        if (kParams) {
+          const double v = sm.jq[t];
+          if (v != 0.0) fix2_add_rows(acc, (size_t)n, j, 6, 7, v, err);
+          sm.jq[t] = 0.0;
         }
       }
       nb = 0;
@@ -2130,7 +2210,7 @@ k_hvp_fp64_half(GridParams g, Fp64Consts mc, const HalfStencil st, int slots, in
         if (keep) {
           const int slot_ = nb + __popc(km & ((1u << lane) - 1u));
           sm.pos[slot_] = p;
-          sm.w[slot_] = ws[j];
+          if (kVjp) sm.w[slot_] = ws[j];
           sm.meta[slot_] = smeta[j];
           sm.jidx[slot_] = j | homebit;
         }
@@ -2141,16 +2221,52 @@ k_hvp_fp64_half(GridParams g, Fp64Consts mc, const HalfStencil st, int slots, in
     }
     if (nb > 0) process();
     for (int off = 1; off < L; off <<= 1) {
-      hx += __shfl_xor_sync(0xffffffffu, hx, off);
-      hy += __shfl_xor_sync(0xffffffffu, hy, off);
-      hz += __shfl_xor_sync(0xffffffffu, hz, off);
+      if (kVjp) {
+        hx += __shfl_xor_sync(0xffffffffu, hx, off);
+        hy += __shfl_xor_sync(0xffffffffu, hy, off);
+        hz += __shfl_xor_sync(0xffffffffu, hz, off);
+      }
+      if (kParams) gq += __shfl_xor_sync(0xffffffffu, gq, off);
     }
     if (active && sub == 0) {
-      fix2_add(acc, (size_t)n, (size_t)i, 0, hx, err);
-      fix2_add(acc, (size_t)n, (size_t)i, 1, hy, err);
-      fix2_add(acc, (size_t)n, (size_t)i, 2, hz, err);
+      if (kVjp) {
+        fix2_add_rows(acc, (size_t)n, (size_t)i, 0, 3, hx, err);
+        fix2_add_rows(acc, (size_t)n, (size_t)i, 1, 4, hy, err);
+        fix2_add_rows(acc, (size_t)n, (size_t)i, 2, 5, hz, err);
+      }
+      if (kParams) fix2_add_rows(acc, (size_t)n, (size_t)i, 6, 7, gq, err);
+    }
+    if (kParams && active) {  // the lane's register sums, to both orders
+#pragma unroll
+      for (int q = 0; q < kDerivRegTypes; q++) {
+        if (q >= ntypes) break;
+        if (ta[q] != 0.0) {
+          atomicAdd(&sm.tab[(ti + q) * 4], ta[q]);
+          atomicAdd(&sm.tab[(q * ntypes + mi.x) * 4], ta[q]);
+        }
+        if (tb[q] != 0.0) {
+          atomicAdd(&sm.tab[(ti + q) * 4 + 1], tb[q]);
+          atomicAdd(&sm.tab[(q * ntypes + mi.x) * 4 + 1], tb[q]);
+        }
+      }
     }
   }
+  if (kParams) {
+    __syncwarp();
+    const int nt4 = ntypes * ntypes * 4;
+    for (int k = lane; k < nt4; k += 32) tpart[(size_t)k * gridDim.x + blockIdx.x] = sm.tab[k];
+  }
+}
+
+// dq from the derivative accumulator's words {hi, lo} (rows 6, 7), in the
+// caller's atom order.
+__global__ void k_finalize_q(int n, const unsigned long long *__restrict__ acc,
+                             const int *__restrict__ sidx, double *__restrict__ dq) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const double hi = (double)(long long)acc[6 * (size_t)n + j];
+  const double lo = (double)(long long)acc[7 * (size_t)n + j];
+  dq[sidx[j]] = (hi + lo * (1.0 / kFix2Lo)) * (1.0 / kFix2Hi);
 }
 
 // ws[j] = w[3 sidx[j] ..] for the sorted atoms j (the direction of a
@@ -2166,11 +2282,21 @@ __global__ void k_gather_sorted(int n, const int *__restrict__ sidx, const doubl
 // out[k] = sum over rows r of part[r][k], rows added in order (deterministic).
 __global__ void k_reduce_columns(int rows, int cols, const double *__restrict__ part,
                                  double *__restrict__ out) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  // one block per column (part[col][row]): strided per-thread sums, then a
+  // fixed tree, so the order of the additions is the same every launch
+  __shared__ double red[256];
+  const int k = blockIdx.x;
   if (k >= cols) return;
+  const double *col = part + (size_t)k * rows;
   double acc = 0.0;
-  for (int r = 0; r < rows; r++) acc += part[(size_t)r * cols + k];
-  out[k] = acc;
+  for (int r = threadIdx.x; r < rows; r += blockDim.x) acc += col[r];
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[k] = red[0];
 }
 
 // ---------------------------------------------------------------------------

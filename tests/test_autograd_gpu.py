@@ -220,8 +220,8 @@ def medium():
 def test_hvp_half_shell_kernel(fx, request):
     """A plain Hessian-vector product (the half-shell kernel, each pair once,
     fixed-point sums) against the same product asked with dE/dq (the
-    full-shell kernel, each pair from both atoms): relative <= 1e-12; two
-    plain products bit-identical."""
+    kernel's parameter instance): relative <= 1e-12; two plain products
+    bit-identical."""
     s = request.getfixturevalue(fx)
     m, pos, q, t = make(s)
     rng = np.random.default_rng(11)
@@ -237,6 +237,61 @@ def test_hvp_half_shell_kernel(fx, request):
     m.close()
     assert torch.equal(h1, h2)
     assert rel(h1.cpu().numpy(), hf.cpu().numpy()) <= 1e-12
+
+
+def split_types(d, extra=((0, 4), (1, 5))):
+    """The same atoms over more LJ types: every other atom of type a moves to
+    a new type b carrying a's parameters (the table's rows and columns
+    copied), so the energy, the forces, dE/dq and H w are unchanged and the
+    table derivative folds back onto the original entries.  Returns the
+    system and each type's original type."""
+    typ = np.asarray(d["type"]).copy()
+    nt = d["lj"].shape[0]
+    orig = np.array(list(range(nt)) + [a for a, _ in extra])
+    for a, b in extra:
+        typ[np.flatnonzero(typ == a)[::2]] = b
+    out = dict(d)
+    out["type"] = typ.astype(np.int32)
+    out["lj"] = d["lj"][np.ix_(orig, orig)].copy()
+    return out, orig
+
+
+@pytest.mark.parametrize("mode", ["params", "vjp"])
+def test_derivative_kernels_agree_across_type_counts(ions, mode):
+    """The ion box over its four LJ types (parameter derivatives by the
+    half-shell kernel, each pair once) against the same box over six types
+    (the full-shell kernel, each pair from both atoms): dE/dq, the table
+    derivative folded back onto the four types and, in VJP mode, H w, all
+    within 1e-12 relative."""
+    s6, orig = split_types(ions)
+    assert len(orig) == 6 and (np.bincount(s6["type"], minlength=6) > 0).all()
+    res = []
+    for s in (ions, s6):
+        m, pos, q, t = make(s)
+        dq = torch.empty_like(q)
+        dt = torch.empty(t.shape, dtype=torch.float64, device="cuda")
+        hv = torch.zeros_like(pos)
+        if mode == "params":
+            m.force.param_grad_device(m.topo, pos.data_ptr(), dq.data_ptr(), dt.data_ptr())
+        else:
+            v = np.random.default_rng(3).standard_normal(s["pos"].shape)
+            vt = torch.tensor(v / np.linalg.norm(v), device="cuda")
+            m.force.hvp_device(m.topo, pos.data_ptr(), vt.data_ptr(), hv.data_ptr(),
+                               dq.data_ptr(), dt.data_ptr())
+        torch.cuda.synchronize()
+        m.force.sync()
+        m.close()
+        res.append((dq.cpu().numpy(), dt.cpu().numpy().reshape(len(s["lj"]), -1, 4),
+                    hv.cpu().numpy()))
+    (dq4, dt4, hv4), (dq6, dt6, hv6) = res
+    folded = np.zeros_like(dt4)
+    for a in range(6):
+        for b in range(6):
+            folded[orig[a], orig[b]] += dt6[a, b]
+    assert rel(dq4, dq6) <= 1e-12
+    assert rel(dt4, folded) <= 1e-12
+    if mode == "vjp":
+        assert rel(hv4, hv6) <= 1e-12
 
 
 def test_charge_units_constant():
