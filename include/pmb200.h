@@ -403,7 +403,12 @@ int pmb200_set_vacuum_domain(pmb200_ctx *ctx, const double lo[3], const double h
  * ones set_topology takes: q_scaled, and the LJ table entries
  * {A, B, A14, B14} per ordered type pair (a, b) as the pair loop reads them
  * (an unordered pair's derivative is split half to (a, b), half to (b, a)).
- * Work is queued on `stream` (NULL: the context's stream).
+ * Work is queued on `stream` (NULL: the context's stream).  H w and dE/dq
+ * are summed in exact fixed point (bitwise reproducible) except for the
+ * parameter derivatives of tables of more than four types, which take a
+ * full-shell kernel summing in FP64 per atom; table derivatives are FP64
+ * sums.  A term beyond the fixed-point range (atoms overlapping) sets the
+ * device error flag (pmb200_sync reports PMB200_EDEVICE).
  *
  * Parameter gradients: d_dq[n] = dE/dq_scaled per atom, d_dlj[ntypes^2 * 4]
  * = dE/d{A, B, A14, B14}, both overwritten (E = LJ + Coulomb energy).  The
