@@ -1802,7 +1802,10 @@ __device__ __forceinline__ DerivTerms deriv_terms(const Fp64Consts &mc,
   const double4 p = lj64[tab];
   const double A = kind == 1 ? p.z : p.x;
   const double B = kind == 1 ? p.w : p.y;
-  u.is = 1.0 / s;
+  // one reciprocal square root serves both 1/s and s^-1/2 (the Coulomb
+  // terms): 1/s as its square, within 2 ulp of the quotient
+  const double ir = rsqrt(s);
+  u.is = ir * ir;
   u.is3 = u.is * u.is * u.is;
   u.is6 = u.is3 * u.is3;
   u.E = A * u.is6 - B * u.is3;
@@ -1820,7 +1823,6 @@ __device__ __forceinline__ DerivTerms deriv_terms(const Fp64Consts &mc,
   u.qf = qj * (kind == 1 ? mc.csf : 1.0);  // f q_j
   u.phi = 0.0; u.phis = 0.0; u.phiss = 0.0;
   if (s <= mc.rcc2) {
-    const double ir = 1.0 / sqrt(s);
     u.phi = ir - mc.c15_1 + mc.c05_3 * s;
     u.phis = -0.5 * ir * u.is + mc.c05_3;
     u.phiss = 0.75 * ir * u.is * u.is;

@@ -18,6 +18,9 @@ import torch
 from oracle import oracle as O
 from protomoladdon_b200 import water
 from protomoladdon_b200.autograd import NonbondedEnergy, SQRTCOULOMBCONSTANT, lj_table
+from protomoladdon_b200.force import PeriodicTopology
+
+from .conftest import load_fixture
 
 pytestmark = pytest.mark.gpu
 
@@ -237,6 +240,41 @@ def test_hvp_half_shell_kernel(fx, request):
     m.close()
     assert torch.equal(h1, h2)
     assert rel(h1.cpu().numpy(), hf.cpu().numpy()) <= 1e-12
+
+
+def test_vacuum_hvp_and_charge_gradient():
+    """Vacuum boundaries (the water droplet of the reference's vacuum
+    fixture): H w and dE/dq against central differences of the reference's
+    own vacuum cutoff force and energy (oracle/_ref), h = 1e-4."""
+    d = dict(load_fixture("vacuum_ref.npz"))
+    topo = PeriodicTopology.from_dict(d)
+    topo.domain = (d["pos"].min(0) - 1.0, d["pos"].max(0) + 1.0)
+    m = NonbondedEnergy(topo, d["ron"], d["rc_lj"], d["rc_coul"], d["rc_alg"], precision="fp64")
+    q, _ = m.initial_params()
+    pos = torch.tensor(d["pos"], dtype=torch.float64, device="cuda")
+    rng = np.random.default_rng(9)
+    v = rng.standard_normal(d["pos"].shape)
+    v /= np.linalg.norm(v)
+    vt = torch.tensor(v, device="cuda")
+    hv = torch.empty_like(pos)
+    m.force.hvp_device(m.topo, pos.data_ptr(), vt.data_ptr(), hv.data_ptr())
+    dq = torch.empty_like(q)
+    dt = torch.empty(len(d["lj"]) ** 2 * 4, dtype=torch.float64, device="cuda")
+    m.force.param_grad_device(m.topo, pos.data_ptr(), dq.data_ptr(), dt.data_ptr())
+    torch.cuda.synchronize()
+    m.force.sync()
+    m.close()
+    fp = O.ref_vacuum_eval(d, d["pos"] + H * v, virial_mode=0)[0]
+    fm = O.ref_vacuum_eval(d, d["pos"] - H * v, virial_mode=0)[0]
+    assert rel(hv.cpu().numpy(), -(fp - fm) / (2 * H)) <= 1e-6
+    qh = np.asarray(d["qscaled"], float)
+    for i in (0, 1, 100):
+        dd = np.zeros_like(qh)
+        dd[i] = H
+        ep = O.ref_vacuum_eval(dict(d, qscaled=qh + dd), d["pos"], virial_mode=0)[1].sum()
+        em = O.ref_vacuum_eval(dict(d, qscaled=qh - dd), d["pos"], virial_mode=0)[1].sum()
+        fd = (ep - em) / (2 * H)
+        assert abs(dq[i].item() - fd) <= 1e-6 * max(abs(fd), 1.0), (i, dq[i].item(), fd)
 
 
 def split_types(d, extra=((0, 4), (1, 5))):
