@@ -434,6 +434,17 @@ int pmb200_hvp_device(pmb200_ctx *ctx, const double *d_pos, const double *d_w, d
  * Replaces rebuilding the topology to change force-field parameters. */
 int pmb200_update_params(pmb200_ctx *ctx, const double *q_scaled, const double *lj);
 
+/* The same from DEVICE buffers, queued on `stream` (NULL: the context's
+ * stream) with no host round trip: d_q_scaled[n] and/or d_lj[ntypes^2 * 4]
+ * (either may be NULL) are copied into the context in stream order, so work
+ * queued after it on the same stream sees them.  A non-finite value sets the
+ * device error flag (the next pmb200_sync reports PMB200_EDEVICE).  A table
+ * needs the box (PMB200_ESTATE otherwise).  For callers whose parameters live
+ * on the device, such as the differentiable form's autograd functions, which
+ * pass theirs before every kernel call. */
+int pmb200_update_params_device(pmb200_ctx *ctx, const double *d_q_scaled, const double *d_lj,
+                                void *stream);
+
 /* ---- batches of independent systems ----
  * Many periodic systems of uneven size evaluated together: one counting sort
  * over all their atoms, one persistent pair kernel that takes (system,

@@ -50,6 +50,7 @@ EXPORTED = (
     "pmb200_autotune", "pmb200_set_pair_kernel",
     "pmb200_eval_noalloc", "pmb200_create_ewald_real", "pmb200_ewald_info",
     "pmb200_param_grad_device", "pmb200_hvp_device", "pmb200_update_params",
+    "pmb200_update_params_device",
     "pmb200_batch_create", "pmb200_batch_destroy", "pmb200_batch_last_error",
     "pmb200_batch_eval_device", "pmb200_batch_set_schedule", "pmb200_batch_get_schedule",
     "pmb200_batch_autotune", "pmb200_batch_set_kernel_timing", "pmb200_batch_last_kernel_ms",
@@ -127,6 +128,7 @@ def lib():
     L.pmb200_param_grad_device.argtypes = [_P, _P, _P, _P, _P]
     L.pmb200_hvp_device.argtypes = [_P, _P, _P, _P, _P, _P, _P]
     L.pmb200_update_params.argtypes = [_P, _P, _P]
+    L.pmb200_update_params_device.argtypes = [_P, _P, _P, _P]
     L.pmb200_set_vacuum_domain.argtypes = [_P, _P, _P]
     L.pmb200_eval_cells.argtypes = [_P, _P, _P, _P, _P, _P, ctypes.c_uint, _I, _I]
     L.pmb200_create_pair.argtypes = [ctypes.POINTER(PairParams), ctypes.POINTER(_P)]

@@ -52,28 +52,26 @@ def lj_table(sigma, epsilon):
 
 
 class _Handle:
-    """One device force context plus the parameter values it holds."""
+    """One device force context; the autograd functions hand it their
+    parameter tensors before every kernel call."""
 
     def __init__(self, topo: PeriodicTopology, force: NonbondedCutoffB200SystemForce):
         self.topo = topo
         self.force = force
-        self.q_key = None
-        self.t_key = None
 
     def sync_params(self, q, table):
-        """Uploads charges / table when they differ from what the context
-        holds (a host round trip per call: this form serves parameter fitting
-        and normal-mode analysis, not the MD step loop)."""
+        """Copies the charges and the table into the context on the device,
+        queued on torch's stream ahead of the kernels that read them (no
+        host round trip; a non-finite value is reported by the next sync)."""
         self.force._ensure(self.topo)
-        qh = q.detach().to("cpu", torch.float64).contiguous().numpy()
-        th = table.detach().to("cpu", torch.float64).contiguous().numpy()
-        qk, tk = qh.tobytes(), th.tobytes()
-        if qk != self.q_key or tk != self.t_key:
-            torch.cuda.current_stream().synchronize()  # no kernel may still read them
-            self.force.sync()
-            self.force.update_params(self.topo, qh if qk != self.q_key else None,
-                                     th.reshape(-1) if tk != self.t_key else None)
-            self.q_key, self.t_key = qk, tk
+        dev = torch.device("cuda", self.force.device)
+        qd = q.detach().to(device=dev, dtype=torch.float64).contiguous()
+        td = table.detach().to(device=dev, dtype=torch.float64).contiguous()
+        if qd.numel() != self.topo.n or td.numel() != self.topo.ntypes ** 2 * 4:
+            raise ValueError("charges must hold n values and the table ntypes^2 * 4")
+        # (the temporaries' memory is reused only by work queued later on
+        # this stream, after the copies)
+        self.force.update_params_device(self.topo, qd.data_ptr(), td.data_ptr(), self.stream())
 
     def stream(self):
         """torch's current stream as a CUDA stream handle.  torch's default

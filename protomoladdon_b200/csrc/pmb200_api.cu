@@ -129,6 +129,10 @@ struct pmb200_ctx {
   // pair-kernel timing
   int timing = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // the LJ table was last set on the device (pmb200_update_params_device):
+  // h_lj is refreshed from d_lj64 after ev_lj before a host consumer reads it
+  bool lj_dev_newer = false;
+  cudaEvent_t ev_lj = nullptr;
 };
 
 namespace {
@@ -365,8 +369,21 @@ void ewald_derive(pmb200_ctx *c, double volume) {
   c->ew_rc = std::sqrt(-std::log(c->ew_accuracy)) / alpha;
 }
 
+// The host copy of the LJ table, brought up to date after a device-side
+// update (for the rare host consumers: box changes, batch creation).
+int pull_lj(pmb200_ctx *c) {
+  if (!c->lj_dev_newer) return PMB200_OK;
+  CK(cudaEventSynchronize(c->ev_lj));
+  const size_t t2 = (size_t)c->ntypes * c->ntypes;
+  CK(cudaMemcpy(c->h_lj.data(), c->d_lj64, sizeof(double4) * t2, cudaMemcpyDeviceToHost));
+  c->lj_dev_newer = false;
+  return PMB200_OK;
+}
+
 // LJ tables: FP64 in Angstrom units, FP32 in cell units (A / u^12, B / u^6).
 int upload_lj(pmb200_ctx *c) {
+  int rc = pull_lj(c);
+  if (rc) return rc;
   const int t2 = c->ntypes * c->ntypes;
   std::vector<double4> l64(t2);
   std::vector<float4> l32(t2);
@@ -952,6 +969,7 @@ int pmb200_destroy(pmb200_ctx *c) {
   if (c->h_pin_out) cudaFreeHost(c->h_pin_out); dfree(c->d_hpos); dfree(c->d_hfrc);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->ev_lj) cudaEventDestroy(c->ev_lj);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return PMB200_OK;
@@ -1024,6 +1042,7 @@ int pmb200_set_topology(pmb200_ctx *c, int n, const int *type, const double *q_s
   c->csf = coulomb_scaling;
   c->have_mass = mass != nullptr;
   c->h_lj.assign(lj, lj + 4 * ntypes * ntypes);
+  c->lj_dev_newer = false;
   const size_t nn = (size_t)std::max(n, 1);
   CK(dalloc(c->d_type, nn));
   CK(dalloc(c->d_mol, nn));
@@ -1660,8 +1679,55 @@ int pmb200_update_params(pmb200_ctx *c, const double *q_scaled, const double *lj
     for (int k = 0; k < t4; k++)
       if (!std::isfinite(lj[k])) return fail(c, PMB200_EINVAL, "LJ table entry %d", k);
     c->h_lj.assign(lj, lj + t4);
+    c->lj_dev_newer = false;
     if (c->have_box) return upload_lj(c);
   }
+  return PMB200_OK;
+}
+
+// Parameters from device buffers: charges copied, the table copied to the
+// FP64 table and scaled into the FP32 one (the quotients upload_lj takes);
+// a non-finite value sets error bit 4.
+__global__ void k_update_q(int n, const double *__restrict__ src, double *__restrict__ dst,
+                           int *__restrict__ err) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double v = src[i];
+  if (!isfinite(v)) atomicOr(err, 4);
+  dst[i] = v;
+}
+
+__global__ void k_update_lj(int t2, const double *__restrict__ src, double u6, double u12,
+                            double4 *__restrict__ lj64, float4 *__restrict__ lj32,
+                            int *__restrict__ err) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= t2) return;
+  const double a = src[4 * k], b = src[4 * k + 1], a14 = src[4 * k + 2], b14 = src[4 * k + 3];
+  if (!(isfinite(a) && isfinite(b) && isfinite(a14) && isfinite(b14))) atomicOr(err, 4);
+  lj64[k] = make_double4(a, b, a14, b14);
+  lj32[k] = make_float4((float)(a / u12), (float)(b / u6), (float)(a14 / u12), (float)(b14 / u6));
+}
+
+int pmb200_update_params_device(pmb200_ctx *c, const double *d_q_scaled, const double *d_lj,
+                                void *stream) {
+  if (!c) return PMB200_EINVAL;
+  if (!c->have_topo) return fail(c, PMB200_ESTATE, "pmb200_set_topology has not been called");
+  if (d_lj && !c->have_box)
+    return fail(c, PMB200_ESTATE, "a device LJ table needs the box (pmb200_set_box)");
+  CK(cudaSetDevice(c->p.device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  if (d_q_scaled && c->n > 0)
+    k_update_q<<<(c->n + 255) / 256, 256, 0, st>>>(c->n, d_q_scaled, c->d_q, c->d_err);
+  if (d_lj) {
+    const int t2 = c->ntypes * c->ntypes;
+    const double u6 = std::pow(c->g.unit, 6.0), u12 = u6 * u6;
+    k_update_lj<<<(t2 + 127) / 128, 128, 0, st>>>(t2, d_lj, u6, u12, c->d_lj64, c->d_lj32,
+                                                  c->d_err);
+    if (!c->ev_lj) CK(cudaEventCreateWithFlags(&c->ev_lj, cudaEventDisableTiming));
+    CK(cudaEventRecord(c->ev_lj, st));
+    c->lj_dev_newer = true;
+  }
+  CK(cudaGetLastError());
   return PMB200_OK;
 }
 
@@ -1671,6 +1737,7 @@ static int device_error(pmb200_ctx *c, int e) {
   if (!e) return PMB200_OK;
   CK(cudaMemset(c->d_err, 0, sizeof(int)));
   if (e & 1) return fail(c, PMB200_EDEVICE, "non-finite atom position in an evaluation");
+  if (e & 4) return fail(c, PMB200_EDEVICE, "non-finite charge or LJ table entry (device update)");
   return fail(c, PMB200_EDEVICE,
               "a pair term exceeded the fixed-point accumulator's range (atoms overlap)");
 }
@@ -2775,7 +2842,8 @@ int pmb200_batch_create(pmb200_ctx *const *systems, int nsys, pmb200_batch **out
   std::vector<int> atom_sys;
   long long N = 0, C = 0;
   for (int s = 0; s < nsys; s++) {
-    const pmb200_ctx *c = systems[s];
+    pmb200_ctx *c = systems[s];
+    if (pull_lj(c)) return done(PMB200_ECUDA);
     BatchSys y{};
     y.g = c->g;
     y.mc = c->mc;

@@ -358,6 +358,16 @@ class NonbondedCutoffB200SystemForce:
         if t is not None:
             topo.lj = t.copy()
 
+    def update_params_device(self, topo, q_ptr=None, lj_ptr=None, stream=None):
+        """New charges (n doubles) and/or LJ table (ntypes^2 * 4 doubles)
+        from device pointers, queued on ``stream`` (see
+        pmb200_update_params_device); the topology's host arrays are left as
+        they are."""
+        self._ensure(topo)
+        self._check(_lib.lib().pmb200_update_params_device(
+            self._ctx, _P(q_ptr) if q_ptr else None, _P(lj_ptr) if lj_ptr else None,
+            _P(stream) if stream else None))
+
     def set_rigid_waters(self, topo, widx, d_oh, d_hh):
         """SETTLE constraints for the device integrator (see pmb200.h)."""
         self._ensure(topo)

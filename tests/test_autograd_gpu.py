@@ -277,6 +277,56 @@ def test_vacuum_hvp_and_charge_gradient():
         assert abs(dq[i].item() - fd) <= 1e-6 * max(abs(fd), 1.0), (i, dq[i].item(), fd)
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_device_parameter_update(small, precision):
+    """pmb200_update_params_device against pmb200_update_params (host): the
+    same forces and energies bit for bit, again after a box change (which
+    rebuilds the FP32 table from the device-updated one); a non-finite
+    charge is reported by the next sync, and the context stays usable."""
+    from protomoladdon_b200._lib import PmbError
+    from protomoladdon_b200.force import NonbondedCutoffB200SystemForce, ScalarStructure
+    s = small
+    q2 = np.asarray(s["qscaled"]) * 1.05
+    lj2 = np.asarray(s["lj"]) * np.array([1.1, 0.9, 1.2, 0.8])
+    out = []
+    for mode in ("host", "device"):
+        topo = PeriodicTopology.from_dict(s)
+        f = NonbondedCutoffB200SystemForce(s["ron"], s["rc_lj"], s["rc_coul"], s["rc_alg"],
+                                           precision=precision)
+        if mode == "host":
+            f.update_params(topo, q2, lj2)
+        else:
+            qd = torch.tensor(q2, device="cuda")
+            td = torch.tensor(lj2, device="cuda")
+            torch.cuda.synchronize()
+            f.update_params_device(topo, qd.data_ptr(), td.data_ptr())  # the context's stream
+        res = []
+        e0 = topo.e.copy()
+        for scale in (1.0, 1.01):
+            topo.e = np.ascontiguousarray(e0 * scale)
+            F = np.zeros_like(s["pos"])
+            E = ScalarStructure()
+            f.evaluate(topo, s["pos"], F, E)
+            res.append((F, E[0], E[1]))
+        if mode == "device":
+            bad = qd.clone()
+            bad[5] = float("nan")
+            f.update_params_device(topo, bad.data_ptr(), None)
+            with pytest.raises(PmbError):
+                f.sync()
+            f.update_params_device(topo, qd.data_ptr(), None)
+            F = np.zeros_like(s["pos"])
+            E = ScalarStructure()
+            f.evaluate(topo, s["pos"], F, E)
+            res.append((F, E[0], E[1]))
+        f.close()
+        out.append(res)
+    host, dev = out
+    for (Fh, ch, lh), (Fd, cd, ld) in zip(host, dev):
+        assert np.array_equal(Fh, Fd) and ch == cd and lh == ld
+    assert np.array_equal(dev[2][0], dev[1][0]) and dev[2][1] == dev[1][1]
+
+
 def split_types(d, extra=((0, 4), (1, 5))):
     """The same atoms over more LJ types: every other atom of type a moves to
     a new type b carrying a's parameters (the table's rows and columns
