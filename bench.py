@@ -66,6 +66,12 @@ FLOPS_PER_PAIR = 81          # algorithmic flops per unique in-cutoff pair
 BYTES_PER_ATOM = 84          # algorithmic HBM bytes per atom per evaluation
 KERNELS_PER_STEP = 9         # kick_drift_settle, cell_index, scan, scatter, rank_gather,
                              # pair, finalize, reduce1, reduce2
+KERNELS_PER_STEP_CLUSTERS = 13  # kick_drift_settle, sc_index, scan, scatter, rank_gather,
+                             # sc_columns, sc_build, sc_list, sc_tasks, sc_pair,
+                             # sc_finalize, sc_reduce1, reduce2
+# ncu summaries holding each energy launch's DRAM bytes (traffic_bytes_per_launch)
+TRAFFIC_PROFILE = {"search": "pair_mixed_water41k.md", "clusters": "pair_clusters_water41k.md",
+                   "tiles": None}
 WORKLOAD = ("water box: 41,472 atoms (13,824 TIP3P-geometry waters, 24^3 lattice, "
             "box 74.496 A), LJ C2 switch 9-10 A + Coulomb C1 cutoff 10 A, leapfrog 1 fs")
 METRIC = "ns/day & Gpairs/s, 41k-atom water box: mixed vs FP64 on B200 @<=1e-5 force err"
@@ -422,7 +428,9 @@ def run_ours(args):
     if rank == 0:
         peak = ctypes_peak(local)
         achieved = FLOPS_PER_PAIR * pairs / (mean_k * 1e-3) / 1e12
-        traffic = committed_traffic()
+        kern_e = tuned.get(args.precision, {}).get("kernel_energy", "search")
+        prof = TRAFFIC_PROFILE.get(kern_e)
+        traffic = committed_traffic(prof) if prof else None
         line = {
             "metric": METRIC, "value": value, "unit": "ns/day", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
@@ -462,7 +470,8 @@ def run_ours(args):
                             "pair_kernel_ms": statistics.mean(fo_kms),
                             "note": "the same device steps without energies"},
             "autotune": tuned,
-            "gpu_launches": KERNELS_PER_STEP * args.steps,
+            "gpu_launches": (KERNELS_PER_STEP_CLUSTERS if kern_e == "clusters"
+                             else KERNELS_PER_STEP) * args.steps,
             "clocks": clocks,
         }
         line.update(acc)

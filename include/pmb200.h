@@ -153,7 +153,8 @@ int pmb200_eval_device(pmb200_ctx *ctx, const double *d_pos, double *d_forces,
  * the same grid are timed once, grids the stencil limits refuse are skipped)
  * and, for PMB200_MIXED contexts, the pair kernel (search or cluster-pair,
  * see pmb200_set_pair_kernel) and its warps per i-cell (2, 4, 8), chosen
- * separately for energy launches and forces-only launches; keeps the grid
+ * separately for energy launches and forces-only launches, then the
+ * supercluster kernel on the chosen grid where it applies; keeps the grid
  * with the fastest evaluation with energies (the reference's integrators
  * ask for energies every step) and applies it.  The library's defaults are
  * timed first and another configuration replaces them only when it is 2%
@@ -178,9 +179,22 @@ int pmb200_autotune(pmb200_ctx *ctx, const double *d_pos, void *stream, int reps
  * and 4 x 4 tiles of atom pairs evaluated with masks; the same pair set and
  * pair arithmetic.  The tile kernel serves the cutoff and real-space Ewald
  * forms of mixed contexts without virial on orthogonal grids with at most
- * 16 LJ types; other evaluations of the context use the search kernel. */
+ * 16 LJ types; other evaluations of the context use the search kernel.
+ * PMB200_KERNEL_CLUSTERS: superclusters -- each super-column's atoms cut by
+ * height into groups of 32, each split into eight 4-atom clusters (2 x 2 x 2);
+ * per group a list of the clusters within the cutoff with atom-pair masks
+ * (exclusions, each pair once), built on the device at every evaluation;
+ * 4 x 4 tiles evaluated with the exact cutoff test and the same pair
+ * arithmetic.  It serves energy and forces-only evaluations of the mixed
+ * cutoff form (LJ(C2) + Coulomb(C1)) without virial, in orthogonal periodic
+ * boxes whose x and y edges hold at least five 32-atom columns across the
+ * cutoff (about 2 rc + 14 A at water density), with at most 16 LJ types and
+ * no modified (1-4) pairs; other evaluations use the search kernel.  A
+ * system packed too densely or sparsely for its lists makes the evaluation
+ * report PMB200_EDEVICE (PMB200_KERNEL_SEARCH then serves it). */
 #define PMB200_KERNEL_SEARCH 0
 #define PMB200_KERNEL_TILES 1
+#define PMB200_KERNEL_CLUSTERS 2
 int pmb200_set_pair_kernel(pmb200_ctx *ctx, int kernel);
 
 /* Force decomposition over several GPUs, one process and one context per GPU,

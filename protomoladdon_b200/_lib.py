@@ -36,6 +36,7 @@ PMB200_SW_TABLE = 16  # flag on the LJ switch: LennardJonesTableForce
 
 PMB200_KERNEL_SEARCH = 0
 PMB200_KERNEL_TILES = 1
+PMB200_KERNEL_CLUSTERS = 2
 
 PMB200_ERFC_POLY5 = 0
 PMB200_ERFC_EXACT = 1

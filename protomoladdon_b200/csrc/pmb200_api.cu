@@ -10,6 +10,7 @@
 #include "../../include/pmb200.h"
 #include "pmb200_kernels.cuh"
 #include "pmb200_tiles.cuh"
+#include "pmb200_clusters.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -49,6 +50,28 @@ struct pmb200_ctx {
   // pmb200_autotune), else the search kernel
   bool tiles_e = false, tiles_f = false;
   float4 *d_cblo = nullptr, *d_cbhi = nullptr;  // cluster boxes (tile kernel)
+  // supercluster pair kernel (pmb200_clusters.cuh) for energy and forces-only
+  // launches, where it applies (sc_ok: mixed cutoff form, orthogonal
+  // periodic box wide enough, at most kMaxTypes types, no modified pairs)
+  bool clu_e = false, clu_f = false, sc_ok = false;
+  bool has_modified = false;  // the exclusion list holds modified (1-4) pairs
+  ScGrid sg{};
+  ScStencil sst{};
+  MixedConsts mca{};          // the pair constants in A
+  int sc_grid_e = 0, sc_grid_f = 0;  // persistent pair-kernel blocks
+  double sc_side = 1.0;       // column width / edge of a cube of 32 atoms (pmb200_autotune)
+  int sc_ncell_alloc = 0, sc_ncol_alloc = 0, sc_nsup_alloc = 0;
+  bool sc_count_zero = false;
+  int *d_sc_count = nullptr, *d_sc_start = nullptr, *d_sc_supbase = nullptr;
+  int *d_sc_ctl = nullptr, *d_sc_atom = nullptr, *d_sc_type = nullptr, *d_sc_mol = nullptr;
+  int *d_sc_cnt = nullptr;
+  float4 *d_sc_xi = nullptr, *d_sc_xj = nullptr, *d_sc_xilo = nullptr, *d_sc_xjlo = nullptr;
+  float4 *d_sc_clo = nullptr, *d_sc_chi = nullptr, *d_sc_sbox = nullptr;
+  int4 *d_sc_corg = nullptr, *d_sc_sorg = nullptr, *d_sc_tasks = nullptr;
+  int2 *d_sc_cmol = nullptr;
+  ScEntry *d_sc_ent = nullptr;
+  unsigned long long *d_sc_facc = nullptr;
+  double *d_sc_part = nullptr;
   // tabulated LJ (LennardJonesTableForce under UniversalSwitchingFunction):
   // the FP64 grid on the device (null: analytic LJ)
   double4 *d_ljtab = nullptr;
@@ -686,6 +709,202 @@ void launch_cell_build(pmb200_ctx *c, const double *d_pos, bool mixed, bool lo,
 // One word copied on the device (the error flag into the results' copy).
 __global__ void k_copy_word(const int *__restrict__ src, int *__restrict__ dst) { *dst = *src; }
 
+// The supercluster kernel's grid, stencil, constants and buffers for the
+// current box and topology (sc_ok = false where it does not apply: the
+// other kernels then run).  Called when the box, the topology or the pair
+// kernel choice changes.
+int sc_prepare(pmb200_ctx *c) {
+  c->sc_ok = false;
+  if (!(c->clu_e || c->clu_f) || !c->have_box || !c->have_topo) return PMB200_OK;
+  if (c->p.precision != PMB200_MIXED || c->form != FORM_CUTOFF || c->g.tric || c->vacuum ||
+      c->ntypes > kMaxTypes || c->has_modified || c->n <= 0 || c->n >= (1 << 24))
+    return PMB200_OK;
+  const GridParams &gp = c->g;
+  const double rc = ctx_rc(c);
+  const double rlist = rc * (1.0 + 1e-5) + 1e-3;  // box tests with a margin
+  ScGrid g{};
+  double vol = 1.0;
+  for (int a = 0; a < 3; a++) {
+    g.boxmin[a] = gp.boxmin[a];
+    g.boxlen[a] = gp.boxlen[a];
+    g.L[a] = (float)gp.boxlen[a];
+    vol *= gp.boxlen[a];
+    // a lattice of about 3 A whose step divides the edge
+    g.m[a] = std::max(1, (int)std::lround(gp.boxlen[a] / 3.0));
+    g.h[a] = gp.boxlen[a] / g.m[a];
+    g.hf[a] = (float)g.h[a];
+  }
+  // columns about the edge of a cube holding 32 atoms; slabs of about 1 A
+  const double side = c->sc_side * std::cbrt(kScAtoms * vol / c->n);
+  int ns[2];
+  for (int a = 0; a < 2; a++) {
+    ns[a] = std::max(1, (int)std::lround(gp.boxlen[a] / side));
+    g.colw[a] = gp.boxlen[a] / ns[a];
+    const int R = (int)std::ceil(rlist / g.colw[a]);
+    if (ns[a] < 2 * R + 1) return PMB200_OK;  // columns must be distinct images
+  }
+  g.nsx = ns[0];
+  g.nsy = ns[1];
+  g.ncol = ns[0] * ns[1];
+  g.nsz = std::max(1, (int)std::lround(gp.boxlen[2] / 1.0));
+  g.slabw = gp.boxlen[2] / g.nsz;
+  g.zmax_ext = (float)(0.5 * (gp.boxlen[2] - 2.0 * rlist) - 0.01);
+  if (g.zmax_ext < 2.0f) return PMB200_OK;
+  const long long ncell = (long long)g.ncol * g.nsz;
+  if (ncell > (1 << 24)) return PMB200_OK;
+  g.nsup_max = (c->n + kScAtoms - 1) / kScAtoms + g.ncol;
+  g.nslot_max = g.nsup_max * kScAtoms;
+  g.rlist2 = (float)(rlist * rlist);
+  ScStencil st{};
+  const int R0 = (int)std::ceil(rlist / g.colw[0]), R1 = (int)std::ceil(rlist / g.colw[1]);
+  for (int dx = -R0; dx <= R0; dx++)
+    for (int dy = -R1; dy <= R1; dy++) {
+      const double gx = std::max(std::abs(dx) - 1, 0) * g.colw[0];
+      const double gy = std::max(std::abs(dy) - 1, 0) * g.colw[1];
+      if (gx * gx + gy * gy >= rlist * rlist) continue;
+      if (st.n >= kScMaxCols) return PMB200_OK;
+      st.off[st.n++] = make_short2((short)dx, (short)dy);
+    }
+  // buffers
+  if (c->sc_ncell_alloc < (int)ncell) {
+    CK(dalloc(c->d_sc_count, (size_t)ncell));
+    CK(dalloc(c->d_sc_start, (size_t)ncell + 1));
+    c->sc_ncell_alloc = (int)ncell;
+  }
+  CK(cudaMemset(c->d_sc_count, 0, sizeof(int) * (size_t)ncell));
+  c->sc_count_zero = true;
+  if (c->sc_ncol_alloc < g.ncol) {
+    CK(dalloc(c->d_sc_supbase, (size_t)g.ncol + 1));
+    c->sc_ncol_alloc = g.ncol;
+  }
+  if (!c->d_sc_ctl) CK(dalloc(c->d_sc_ctl, 4));
+  if (c->sc_nsup_alloc < g.nsup_max) {
+    const size_t ns_ = (size_t)g.nsup_max, nsl = ns_ * kScAtoms, ncl = ns_ * 8;
+    const size_t ntask = ns_ * ((kScCap + kScChunk - 1) / kScChunk);
+    CK(dalloc(c->d_sc_atom, nsl));
+    CK(dalloc(c->d_sc_type, nsl));
+    CK(dalloc(c->d_sc_mol, nsl));
+    CK(dalloc(c->d_sc_xi, nsl));
+    CK(dalloc(c->d_sc_xj, nsl));
+    CK(dalloc(c->d_sc_xilo, nsl));
+    CK(dalloc(c->d_sc_xjlo, nsl));
+    CK(dalloc(c->d_sc_facc, 3 * nsl));
+    CK(dalloc(c->d_sc_clo, ncl));
+    CK(dalloc(c->d_sc_chi, ncl));
+    CK(dalloc(c->d_sc_corg, ncl));
+    CK(dalloc(c->d_sc_cmol, ncl));
+    CK(dalloc(c->d_sc_sorg, ns_));
+    CK(dalloc(c->d_sc_sbox, 2 * ns_));
+    CK(dalloc(c->d_sc_cnt, ns_));
+    CK(dalloc(c->d_sc_ent, ns_ * kScCap));
+    CK(dalloc(c->d_sc_tasks, ntask));
+    CK(dalloc(c->d_sc_part, ntask * kNacc));
+    c->sc_nsup_alloc = g.nsup_max;
+  }
+  // the pair constants in A (the search kernel's, with unit 1)
+  const pmb200_params &p = c->p;
+  MixedConsts m = c->mc;
+  {
+    const double rl = p.cutoff_lj, ro = p.switchon, rq = p.cutoff_coul;
+    const double t = rl * rl - ro * ro;
+    m.cut2 = (float)(rc * rc);
+    m.rclj2 = (float)(rl * rl);
+    m.ron2 = (float)(ro * ro);
+    m.rcc2 = (float)(rq * rq);
+    m.s1 = (float)(1.0 / (t * t * t));
+    m.s2 = (float)(rl * rl - 3.0 * ro * ro);
+    m.s3 = (float)(4.0 / (t * t * t));
+    m.c15_1 = (float)(1.5 / rq);
+    m.c05_3 = (float)(0.5 / (rq * rq * rq));
+    m.c15_3 = (float)(1.5 / (rq * rq * rq));
+    m.e15 = 1.5 / rq;
+    m.e05 = 0.5 / (rq * rq * rq);
+  }
+  int dev = 0, sms = 0, be = 0, bf = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&be, k_sc_pair<true>, 32, 0));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf, k_sc_pair<false>, 32, 0));
+  c->sc_grid_e = sms * std::max(be, 1);
+  c->sc_grid_f = sms * std::max(bf, 1);
+  c->sg = g;
+  c->sst = st;
+  c->mca = m;
+  c->sc_ok = true;
+  release_graph(c);
+  return PMB200_OK;
+}
+
+bool clusters_apply(const pmb200_ctx *c, unsigned flags) {
+  return c->sc_ok && ((flags & PMB200_ENERGY) ? c->clu_e : c->clu_f) &&
+         !(flags & (PMB200_VIRIAL | PMB200_MOLVIRIAL));
+}
+
+// One evaluation on the supercluster kernel: column sort, superclusters,
+// lists, tasks, pair kernel, forces back to the original order, energies.
+// Every kernel after the first is a programmatic dependent of the one before
+// (except a timed pair kernel, whose events bracket it alone).
+int launch_eval_clusters(pmb200_ctx *c, const double *d_pos, double *d_forces, double *d_out,
+                         unsigned flags, int accumulate, cudaStream_t st, bool timed) {
+  const int n = c->n;
+  const ScGrid &g = c->sg;
+  const bool energy = (flags & PMB200_ENERGY) != 0;
+  const int ncell = g.ncol * g.nsz;
+  // every kernel after the first as a programmatic dependent of the one
+  // before it (the kernels read the counts their predecessors write through
+  // volatile loads after their wait: sc_ctl)
+  constexpr bool kChain = true;
+  if (!c->sc_count_zero) cudaMemsetAsync(c->d_sc_count, 0, sizeof(int) * (size_t)ncell, st);
+  c->sc_count_zero = false;
+  const unsigned nb = (unsigned)((n + 255) / 256);
+  launch_k(k_sc_index, nb, 256, 0, st, false, n, d_pos, g, c->d_cell_of, c->d_sc_count,
+           c->d_slot, c->d_err);
+  launch_k(k_scan, 1, 1024, 1024 * sizeof(int), st, kChain, ncell, c->d_sc_count, c->d_sc_start);
+  c->sc_count_zero = cudaPeekAtLastError() == cudaSuccess;
+  launch_k(k_scatter, nb, 256, 0, st, kChain, n, c->d_cell_of, c->d_slot, c->d_sc_start,
+           c->d_tmp);
+  launch_k(k_rank_gather, (unsigned)((ncell + 3) / 4), 128, 0, st, kChain, ncell, c->d_sc_start,
+           c->d_tmp, (const float4 *)nullptr, (const double4 *)nullptr, c->d_type, c->d_mol,
+           c->d_sidx, (float4 *)nullptr, (double4 *)nullptr, c->d_smeta,
+           (const float4 *)nullptr, (float4 *)nullptr, 0);
+  launch_k(k_sc_columns, 1, 1024, 0, st, kChain, g.ncol, g.nsz, c->d_sc_start, c->d_sc_supbase,
+           c->d_sc_ctl);
+  launch_k(k_sc_build, (unsigned)((g.nsup_max + kScBuildWarps - 1) / kScBuildWarps),
+           32 * kScBuildWarps, 0, st, kChain, g, d_pos, c->d_sc_start, c->d_sidx, c->d_smeta,
+           c->d_sc_supbase, c->d_sc_ctl, c->d_q, c->d_sc_atom, c->d_sc_type, c->d_sc_mol,
+           c->d_sc_xi, c->d_sc_xj, energy ? c->d_sc_xilo : nullptr,
+           energy ? c->d_sc_xjlo : nullptr, c->d_sc_clo, c->d_sc_chi, c->d_sc_corg,
+           c->d_sc_cmol, c->d_sc_sorg, c->d_sc_sbox, c->d_sc_facc, c->d_err);
+  launch_k(k_sc_list, (unsigned)g.nsup_max, 32, 0, st, kChain, g, c->sst, c->d_sc_supbase,
+           c->d_sc_ctl, c->d_sc_clo, c->d_sc_chi, c->d_sc_corg, c->d_sc_cmol, c->d_sc_sorg,
+           c->d_sc_sbox, c->d_sc_atom, c->d_sc_mol, c->d_ex_start, c->d_ex, c->d_sc_ent,
+           c->d_sc_cnt, c->d_err);
+  launch_k(k_sc_tasks, 1, 1024, 0, st, kChain, c->d_sc_cnt, c->d_sc_ctl, c->d_sc_tasks);
+  CK(cudaGetLastError());
+  if (timed) CK(cudaEventRecord(c->ev0, st));
+  const bool pdl = !timed && kChain;
+  if (energy)
+    launch_k(k_sc_pair<true>, (unsigned)c->sc_grid_e, 32, 0, st, pdl, c->mca, c->ntypes,
+             c->d_lj64, c->d_sc_tasks, c->d_sc_ctl, c->d_sc_xi, c->d_sc_xj, c->d_sc_type,
+             c->d_sc_ent, c->d_sc_xilo, c->d_sc_xjlo, g, c->d_sc_facc, c->d_sc_part, c->d_err);
+  else
+    launch_k(k_sc_pair<false>, (unsigned)c->sc_grid_f, 32, 0, st, pdl, c->mca, c->ntypes,
+             c->d_lj64, c->d_sc_tasks, c->d_sc_ctl, c->d_sc_xi, c->d_sc_xj, c->d_sc_type,
+             c->d_sc_ent, c->d_sc_xilo, c->d_sc_xjlo, g, c->d_sc_facc, c->d_sc_part, c->d_err);
+  CK(cudaGetLastError());
+  if (timed) CK(cudaEventRecord(c->ev1, st));
+  launch_k(k_sc_finalize, (unsigned)((g.nslot_max + 255) / 256), 256, 0, st, pdl,
+           (const int *)c->d_sc_ctl, g.nslot_max, (const int *)c->d_sc_atom,
+           (const unsigned long long *)c->d_sc_facc, accumulate, d_forces);
+  if (energy) {
+    k_sc_reduce1<<<kRedBlocks, 256, 0, st>>>(c->d_sc_ctl + 1, c->d_sc_part, c->d_red, ACC_E);
+    k_reduce2<<<1, 256, 0, st>>>(kRedBlocks, c->d_red, 1.0, d_out ? d_out : c->d_out,
+                                c->d_pairs, ACC_E);
+  }
+  CK(cudaGetLastError());
+  return PMB200_OK;
+}
+
 int launch_eval(pmb200_ctx *c, const double *d_pos, double *d_forces, double *d_out,
                 unsigned flags, int accumulate, cudaStream_t st) {
   const int n = c->n;
@@ -694,6 +913,12 @@ int launch_eval(pmb200_ctx *c, const double *d_pos, double *d_forces, double *d_
   const bool virial = (flags & (PMB200_VIRIAL | PMB200_MOLVIRIAL)) != 0;
   const bool molvir = (flags & PMB200_MOLVIRIAL) != 0;
   const GridParams &g = c->g;
+  if (mixed && clusters_apply(c, flags)) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(st, &cs));
+    return launch_eval_clusters(c, d_pos, d_forces, d_out, flags, accumulate, st,
+                                c->timing && cs == cudaStreamCaptureStatusNone);
+  }
   // the cell build clears the accumulator on the way (still in L2 when the
   // pair kernel adds to it), so that the pair kernel follows the build's last
   // kernel directly
@@ -964,6 +1189,12 @@ int pmb200_destroy(pmb200_ctx *c) {
   dfree(c->d_smeta); dfree(c->d_com); dfree(c->d_facc);
   dfree(c->d_tpart); dfree(c->d_gq); dfree(c->d_glj); dfree(c->d_wsorted);
   dfree(c->d_pairs); dfree(c->d_out); dfree(c->d_red); dfree(c->d_widx); dfree(c->d_fidx);
+  dfree(c->d_sc_count); dfree(c->d_sc_start); dfree(c->d_sc_supbase); dfree(c->d_sc_ctl);
+  dfree(c->d_sc_atom); dfree(c->d_sc_type); dfree(c->d_sc_mol); dfree(c->d_sc_cnt);
+  dfree(c->d_sc_xi); dfree(c->d_sc_xj); dfree(c->d_sc_xilo); dfree(c->d_sc_xjlo);
+  dfree(c->d_sc_clo); dfree(c->d_sc_chi); dfree(c->d_sc_sbox); dfree(c->d_sc_corg);
+  dfree(c->d_sc_sorg); dfree(c->d_sc_tasks); dfree(c->d_sc_cmol); dfree(c->d_sc_ent);
+  dfree(c->d_sc_facc); dfree(c->d_sc_part);
   if (c->h_pin_pos) cudaFreeHost(c->h_pin_pos);
   if (c->h_pin_frc) cudaFreeHost(c->h_pin_frc);
   if (c->h_pin_out) cudaFreeHost(c->h_pin_out); dfree(c->d_hpos); dfree(c->d_hfrc);
@@ -1014,8 +1245,10 @@ int pmb200_set_topology(pmb200_ctx *c, int n, const int *type, const double *q_s
     kinds[std::make_pair(std::min(a, b), std::max(a, b))] = k;
   }
   std::vector<std::vector<int2>> per(n);
+  bool modified = false;
   for (const auto &kv : kinds) {
     if (kv.second == 0) continue;
+    modified = modified || kv.second == 1;
     per[kv.first.first].push_back(make_int2(kv.first.second, kv.second));
     per[kv.first.second].push_back(make_int2(kv.first.first, kv.second));
   }
@@ -1040,6 +1273,7 @@ int pmb200_set_topology(pmb200_ctx *c, int n, const int *type, const double *q_s
   c->ntypes = ntypes;
   c->nmol = nmol;
   c->csf = coulomb_scaling;
+  c->has_modified = modified;
   c->have_mass = mass != nullptr;
   c->h_lj.assign(lj, lj + 4 * ntypes * ntypes);
   c->lj_dev_newer = false;
@@ -1072,7 +1306,10 @@ int pmb200_set_topology(pmb200_ctx *c, int n, const int *type, const double *q_s
   // an Ewald context's cutoff may depend on N (default alpha): rebuild the grid
   if (c->form != FORM_CUTOFF && c->box_given)
     return pmb200_set_box(c, c->box_e[0], c->box_e[1], c->box_e[2], c->box_origin);
-  if (c->have_box) return upload_lj(c);
+  if (c->have_box) {
+    const int r = upload_lj(c);
+    return r ? r : sc_prepare(c);
+  }
   return PMB200_OK;
 }
 
@@ -1274,7 +1511,10 @@ int pmb200_set_box(pmb200_ctx *c, const double e1[3], const double e2[3], const 
   }
   if (c->vacuum) b.d = std::numeric_limits<double>::infinity();  // no images
   c->have_box = true;
-  if (c->have_topo) return upload_lj(c);
+  if (c->have_topo) {
+    const int r = upload_lj(c);
+    return r ? r : sc_prepare(c);
+  }
   return PMB200_OK;
 }
 
@@ -1301,6 +1541,8 @@ struct TuneChoice {
   double cellsize;         // the cell-size hint applied (0: the default)
   int slots_e, slots_f;    // mixed warps per i-cell (0 for FP64 contexts)
   bool tiles_e, tiles_f;   // the cluster-pair kernel with / without energies
+  bool clu_e, clu_f;       // the supercluster kernel with / without energies
+  double sc_side;          // its column width factor (sc_prepare)
   double ms_e, ms_f;       // median evaluation times with and without energies
   int tried;               // configurations timed
 };
@@ -1334,11 +1576,14 @@ extern "C" {
 
 int pmb200_set_pair_kernel(pmb200_ctx *c, int kernel) {
   if (!c) return PMB200_EINVAL;
-  if (kernel != PMB200_KERNEL_SEARCH && kernel != PMB200_KERNEL_TILES)
+  if (kernel != PMB200_KERNEL_SEARCH && kernel != PMB200_KERNEL_TILES &&
+      kernel != PMB200_KERNEL_CLUSTERS)
     return fail(c, PMB200_EINVAL, "pair kernel %d", kernel);
+  CK(cudaSetDevice(c->p.device));
   c->tiles_e = c->tiles_f = kernel == PMB200_KERNEL_TILES;
+  c->clu_e = c->clu_f = kernel == PMB200_KERNEL_CLUSTERS;
   release_graph(c);  // graphs hold the previous kernel
-  return PMB200_OK;
+  return sc_prepare(c);
 }
 
 int pmb200_autotune(pmb200_ctx *c, const double *d_pos, void *stream, int reps,
@@ -1379,18 +1624,34 @@ int pmb200_autotune(pmb200_ctx *c, const double *d_pos, void *stream, int reps,
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
+    // one evaluation as the library runs it in a step or a host-buffer call:
+    // captured once as a graph and replayed (launching its kernels one by one
+    // from the host would time the host's launch rate for the paths with
+    // more kernels)
     auto timed = [&](unsigned flags, double &ms) -> int {
       std::vector<float> t((size_t)reps);
-      int r = launch_eval(c, d_pos, c->d_hfrc, c->d_out, flags, 0, st);  // warm-up
+      int r = ensure_clear(c, st);
       if (r) return r;
-      for (int k = 0; k < reps; k++) {
-        if (cudaEventRecord(e0, st) != cudaSuccess) return PMB200_ECUDA;
-        r = launch_eval(c, d_pos, c->d_hfrc, c->d_out, flags, 0, st);
-        if (r) return r;
-        if (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
-            cudaEventElapsedTime(&t[k], e0, e1) != cudaSuccess)
-          return PMB200_ECUDA;
+      cudaGraph_t gr = nullptr;
+      cudaGraphExec_t ge = nullptr;
+      if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        return fail(c, PMB200_ECUDA, "autotune: capture failed");
+      r = launch_eval(c, d_pos, c->d_hfrc, c->d_out, flags, 0, st);
+      const cudaError_t ce = cudaStreamEndCapture(st, &gr);
+      if (r || ce != cudaSuccess || cudaGraphInstantiate(&ge, gr, 0) != cudaSuccess) {
+        if (gr) cudaGraphDestroy(gr);
+        return r ? r : fail(c, PMB200_ECUDA, "autotune: capture failed");
       }
+      if (cudaGraphLaunch(ge, st) != cudaSuccess) r = PMB200_ECUDA;  // warm-up
+      for (int k = 0; k < reps && !r; k++) {
+        if (cudaEventRecord(e0, st) != cudaSuccess || cudaGraphLaunch(ge, st) != cudaSuccess ||
+            cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+            cudaEventElapsedTime(&t[k], e0, e1) != cudaSuccess)
+          r = PMB200_ECUDA;
+      }
+      cudaGraphExecDestroy(ge);
+      cudaGraphDestroy(gr);
+      if (r) return fail(c, r, "autotune: timed replay failed");
       std::nth_element(t.begin(), t.begin() + reps / 2, t.end());
       ms = t[reps / 2];
       return PMB200_OK;
@@ -1442,12 +1703,65 @@ int pmb200_autotune(pmb200_ctx *c, const double *d_pos, void *stream, int reps,
         best.tried = tried;
       }
     }
+    if (!status && best.ms_e < 1e300 && mixed) {
+      // the supercluster kernel where it applies (its own grid: the cell size
+      // and the warps per i-cell do not concern it), on the best cell grid
+      // column widths of 0.8 to 1.15 times the edge of a cube of 32 atoms (how
+      // many superclusters a column's atoms fill, and so the padding, varies
+      // with it)
+      c->p.cellsize = best.cellsize;
+      c->clu_e = c->clu_f = true;
+      double bme = 1e300, bmf = 1e300, bside = 1.0;
+      int last_cols = -1;
+      for (double side : {1.0, 0.9, 0.8, 1.15}) {
+        c->sc_side = side;
+        if (reapply_box(c) != PMB200_OK || !c->sc_ok) continue;
+        if (c->sg.ncol == last_cols) continue;  // the same columns as the previous width
+        last_cols = c->sg.ncol;
+        double me = 0.0, mf = 0.0;
+        int r = timed(PMB200_ENERGY, me);
+        if (!r) r = timed(0u, mf);
+        int e = 0;
+        if (!r && (cudaStreamSynchronize(st) != cudaSuccess ||
+                   cudaMemcpy(&e, c->d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess))
+          r = PMB200_ECUDA;
+        if (e) cudaMemset(c->d_err, 0, sizeof(int));  // (lists too long: not a candidate)
+        if (r) {
+          status = r;
+          break;
+        }
+        if (e) continue;
+        best.tried += 2;
+        if (me < bme) {
+          bme = me;
+          bmf = mf;
+          bside = side;
+        }
+      }
+      if (!status && bme < 1e300) {
+        if (faster(bme, best.ms_e)) {
+          best.ms_e = bme;
+          best.clu_e = true;
+          best.tiles_e = false;
+        }
+        if (faster(bmf, best.ms_f)) {
+          best.ms_f = bmf;
+          best.clu_f = true;
+          best.tiles_f = false;
+        }
+        best.sc_side = bside;
+      }
+      c->clu_e = c->clu_f = false;
+      c->sc_side = 1.0;
+      c->sc_ok = false;
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (status || best.ms_e >= 1e300) {
       c->p.cellsize = hint0;
       c->slots_e = c->slots_f = 0;
       c->tiles_e = c->tiles_f = false;
+      c->clu_e = c->clu_f = false;
       const int r2 = reapply_box(c);
       return status ? status : (r2 ? r2 : fail(c, PMB200_EUNSUPPORTED, "no grid to tune"));
     }
@@ -1466,6 +1780,11 @@ int pmb200_autotune(pmb200_ctx *c, const double *d_pos, void *stream, int reps,
   c->slots_f = best.slots_f;
   c->tiles_e = best.tiles_e;
   c->tiles_f = best.tiles_f;
+  c->clu_e = best.clu_e;
+  c->clu_f = best.clu_f;
+  c->sc_side = best.sc_side > 0.0 ? best.sc_side : 1.0;
+  rc = sc_prepare(c);
+  if (rc) return rc;
   release_graph(c);  // graphs hold the previous launch shapes
   if (result) {
     result[0] = best.cellsize;
@@ -1474,8 +1793,10 @@ int pmb200_autotune(pmb200_ctx *c, const double *d_pos, void *stream, int reps,
     result[3] = best.ms_e;
     result[4] = best.ms_f;
     result[5] = cached ? 0.0 : best.tried;
-    result[6] = best.tiles_e ? PMB200_KERNEL_TILES : PMB200_KERNEL_SEARCH;
-    result[7] = best.tiles_f ? PMB200_KERNEL_TILES : PMB200_KERNEL_SEARCH;
+    result[6] = best.clu_e ? PMB200_KERNEL_CLUSTERS
+                           : (best.tiles_e ? PMB200_KERNEL_TILES : PMB200_KERNEL_SEARCH);
+    result[7] = best.clu_f ? PMB200_KERNEL_CLUSTERS
+                           : (best.tiles_f ? PMB200_KERNEL_TILES : PMB200_KERNEL_SEARCH);
   }
   return PMB200_OK;
 }
@@ -1738,6 +2059,13 @@ static int device_error(pmb200_ctx *c, int e) {
   CK(cudaMemset(c->d_err, 0, sizeof(int)));
   if (e & 1) return fail(c, PMB200_EDEVICE, "non-finite atom position in an evaluation");
   if (e & 4) return fail(c, PMB200_EDEVICE, "non-finite charge or LJ table entry (device update)");
+  if (e & 8)
+    return fail(c, PMB200_EDEVICE, "supercluster kernel: a cluster list exceeded %d entries "
+                "(atoms packed denser than the kernel supports; use PMB200_KERNEL_SEARCH)",
+                kScCap);
+  if (e & (16 | 32))
+    return fail(c, PMB200_EDEVICE, "supercluster kernel: a supercluster is taller than the box "
+                "allows for a unique periodic image (sparse system; use PMB200_KERNEL_SEARCH)");
   return fail(c, PMB200_EDEVICE,
               "a pair term exceeded the fixed-point accumulator's range (atoms overlap)");
 }

@@ -286,16 +286,18 @@ class NonbondedCutoffB200SystemForce:
         r = (ctypes.c_double * 8)()
         self._check(_lib.lib().pmb200_autotune(self._ctx, _P(pos_ptr),
                                                _P(stream) if stream else None, int(reps), r))
-        names = {_lib.PMB200_KERNEL_SEARCH: "search", _lib.PMB200_KERNEL_TILES: "tiles"}
+        names = {_lib.PMB200_KERNEL_SEARCH: "search", _lib.PMB200_KERNEL_TILES: "tiles",
+                 _lib.PMB200_KERNEL_CLUSTERS: "clusters"}
         return {"cellsize_hint": r[0], "warps_per_cell_energy": int(r[1]),
                 "warps_per_cell_forces": int(r[2]), "ms_energy": r[3], "ms_forces": r[4],
                 "configurations_timed": int(r[5]), "kernel_energy": names[int(r[6])],
                 "kernel_forces": names[int(r[7])]}
 
     def set_pair_kernel(self, kernel):
-        """The mixed pair kernel: "search" (default) or "tiles" (cluster pairs;
-        pmb200_set_pair_kernel)."""
-        k = {"search": _lib.PMB200_KERNEL_SEARCH, "tiles": _lib.PMB200_KERNEL_TILES}[kernel]
+        """The mixed pair kernel: "search" (default), "tiles" (cluster pairs of a
+        cell) or "clusters" (supercluster lists; pmb200_set_pair_kernel)."""
+        k = {"search": _lib.PMB200_KERNEL_SEARCH, "tiles": _lib.PMB200_KERNEL_TILES,
+             "clusters": _lib.PMB200_KERNEL_CLUSTERS}[kernel]
         self._pair_kernel = k
         if self._ctx is not None:
             self._check(_lib.lib().pmb200_set_pair_kernel(self._ctx, k))
