@@ -320,8 +320,13 @@ def run_ours(args):
 
     def tune(force):
         """pmb200_autotune on the start positions: the grid's cell size, the
-        pair kernel and its warps per i-cell, applied to the context."""
+        pair kernel and its warps per i-cell, applied to the context (or the
+        pair kernel --pair-kernel names, untuned)."""
         pos = torch.tensor(s["pos"], dtype=torch.float64, device=dev)
+        if args.pair_kernel != "auto" and force.precision == "mixed":
+            force.set_pair_kernel(args.pair_kernel)
+            return {"tuned": False, "kernel_energy": args.pair_kernel,
+                    "kernel_forces": args.pair_kernel}
         if args.autotune_reps <= 0:
             return {"tuned": False}
         choice = force.autotune(topo, pos.data_ptr(), reps=args.autotune_reps,
@@ -1039,6 +1044,8 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--skip-accuracy", action="store_true")
+    ap.add_argument("--pair-kernel", default="auto", choices=["auto", "search", "clusters"],
+                    help="mixed pair kernel: auto (pmb200_autotune) or a fixed one")
     ap.add_argument("--autotune-reps", type=int, default=10,
                     help="timed launches per configuration of pmb200_autotune (0: no tuning, "
                          "the library's default grid and kernel)")

@@ -59,6 +59,7 @@ struct pmb200_ctx {
   ScStencil sst{};
   MixedConsts mca{};          // the pair constants in A
   int sc_grid_e = 0, sc_grid_f = 0;  // persistent pair-kernel blocks
+  bool sc_full = false;       // both switch cutoffs equal the pair cutoff
   double sc_side = 1.0;       // column width / edge of a cube of 32 atoms (pmb200_autotune)
   int sc_ncell_alloc = 0, sc_ncol_alloc = 0, sc_nsup_alloc = 0;
   bool sc_count_zero = false;
@@ -823,8 +824,15 @@ int sc_prepare(pmb200_ctx *c) {
   int dev = 0, sms = 0, be = 0, bf = 0;
   CK(cudaGetDevice(&dev));
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&be, k_sc_pair<true>, 32, 0));
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf, k_sc_pair<false>, 32, 0));
+  const bool full = m.rclj2 >= m.cut2 && m.rcc2 >= m.cut2;
+  if (full) {
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&be, k_sc_pair<true, true>, 32, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf, k_sc_pair<false, true>, 32, 0));
+  } else {
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&be, k_sc_pair<true, false>, 32, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf, k_sc_pair<false, false>, 32, 0));
+  }
+  c->sc_full = full;
   c->sc_grid_e = sms * std::max(be, 1);
   c->sc_grid_f = sms * std::max(bf, 1);
   c->sg = g;
@@ -875,7 +883,8 @@ int launch_eval_clusters(pmb200_ctx *c, const double *d_pos, double *d_forces, d
            c->d_sc_xi, c->d_sc_xj, energy ? c->d_sc_xilo : nullptr,
            energy ? c->d_sc_xjlo : nullptr, c->d_sc_clo, c->d_sc_chi, c->d_sc_corg,
            c->d_sc_cmol, c->d_sc_sorg, c->d_sc_sbox, c->d_sc_facc, c->d_err);
-  launch_k(k_sc_list, (unsigned)g.nsup_max, 32, 0, st, kChain, g, c->sst, c->d_sc_supbase,
+  launch_k(k_sc_list, (unsigned)g.nsup_max, 32 * kScListWarps, kScListSmem, st, kChain, g,
+           c->sst, c->d_sc_supbase,
            c->d_sc_ctl, c->d_sc_clo, c->d_sc_chi, c->d_sc_corg, c->d_sc_cmol, c->d_sc_sorg,
            c->d_sc_sbox, c->d_sc_atom, c->d_sc_mol, c->d_ex_start, c->d_ex, c->d_sc_ent,
            c->d_sc_cnt, c->d_err);
@@ -883,14 +892,16 @@ int launch_eval_clusters(pmb200_ctx *c, const double *d_pos, double *d_forces, d
   CK(cudaGetLastError());
   if (timed) CK(cudaEventRecord(c->ev0, st));
   const bool pdl = !timed && kChain;
-  if (energy)
-    launch_k(k_sc_pair<true>, (unsigned)c->sc_grid_e, 32, 0, st, pdl, c->mca, c->ntypes,
-             c->d_lj64, c->d_sc_tasks, c->d_sc_ctl, c->d_sc_xi, c->d_sc_xj, c->d_sc_type,
-             c->d_sc_ent, c->d_sc_xilo, c->d_sc_xjlo, g, c->d_sc_facc, c->d_sc_part, c->d_err);
-  else
-    launch_k(k_sc_pair<false>, (unsigned)c->sc_grid_f, 32, 0, st, pdl, c->mca, c->ntypes,
-             c->d_lj64, c->d_sc_tasks, c->d_sc_ctl, c->d_sc_xi, c->d_sc_xj, c->d_sc_type,
-             c->d_sc_ent, c->d_sc_xilo, c->d_sc_xjlo, g, c->d_sc_facc, c->d_sc_part, c->d_err);
+#define PMB_SC_PAIR(E, F)                                                                   \
+  launch_k(k_sc_pair<E, F>, (unsigned)(E ? c->sc_grid_e : c->sc_grid_f), 32, 0, st, pdl,     \
+           c->mca, c->ntypes, c->d_lj64, c->d_sc_tasks, c->d_sc_ctl, c->d_sc_xi, c->d_sc_xj, \
+           c->d_sc_type, c->d_sc_ent, c->d_sc_xilo, c->d_sc_xjlo, g, c->d_sc_facc,           \
+           c->d_sc_part, c->d_err)
+  if (energy && c->sc_full) PMB_SC_PAIR(true, true);
+  else if (energy) PMB_SC_PAIR(true, false);
+  else if (c->sc_full) PMB_SC_PAIR(false, true);
+  else PMB_SC_PAIR(false, false);
+#undef PMB_SC_PAIR
   CK(cudaGetLastError());
   if (timed) CK(cudaEventRecord(c->ev1, st));
   launch_k(k_sc_finalize, (unsigned)((g.nslot_max + 255) / 256), 256, 0, st, pdl,

@@ -5,7 +5,7 @@
 //
 // Layout, rebuilt on the device at every evaluation:
 //   * the box is cut into super-columns along x and y (about the edge of a
-//     cube holding 32 atoms) and each column into thin z slabs; a counting
+//     cube holding 32 atoms) and each column into 1 A slabs; a counting
 //     sort by (column, slab, index) orders every column's atoms by height;
 //   * each column's atoms are cut, bottom to top, into superclusters of 32
 //     slots (the last one padded); a supercluster's atoms are split in halves
@@ -38,6 +38,7 @@ constexpr int kScAtoms = 32;      // slots per supercluster
 constexpr int kScCap = 640;       // list entries per supercluster
 constexpr int kScChunk = 16;      // entries per warp task
 constexpr int kScMaxCols = 128;   // column offsets of the stencil
+constexpr int kScTaskSups = 4096; // superclusters per round of the task kernel
 constexpr float kScFar = 1.0e4f;  // pad slots' coordinate (beyond any cutoff)
 constexpr float kScForceLim = 2.0e9f;  // |F| (kcal/mol/A) within the int64 2^-32 range
 
@@ -135,8 +136,8 @@ __device__ __forceinline__ int sc_block_scan(int x, int *sh) {
 // task count) and ctl[2] (the task counter) cleared.  One block.
 __global__ void k_sc_columns(int ncol, int nsz, const int *__restrict__ start,
                              int *__restrict__ supbase, int *__restrict__ ctl) {
-  pdl_trigger();
   pdl_wait();
+  pdl_trigger();  // (after the wait: see k_sc_tasks)
   __shared__ int sh[32];
   const int T = blockDim.x, t = threadIdx.x;
   const int span = (ncol + T - 1) / T;
@@ -170,7 +171,7 @@ __device__ __forceinline__ int sc_column(const int *supbase, int ncol, int s) {
 }
 
 // One warp per supercluster: the 2 x 2 x 2 split, the slot arrays, cluster
-// boxes and lattice corners, the molecule-index range of each cluster, the
+// boxes and lattice corners, the molecule signature of each cluster, the
 // supercluster's box; the slots' force accumulator cleared.
 constexpr int kScBuildWarps = 4;
 __global__ void __launch_bounds__(32 * kScBuildWarps)
@@ -183,8 +184,8 @@ k_sc_build(ScGrid g, const double *__restrict__ pos, const int *__restrict__ sta
            float4 *__restrict__ chi, int4 *__restrict__ corg, int2 *__restrict__ cmol,
            int4 *__restrict__ sorg, float4 *__restrict__ sbox,
            unsigned long long *__restrict__ facc, int *__restrict__ err) {
-  pdl_trigger();
   pdl_wait();
+  pdl_trigger();  // (after the wait: see k_sc_tasks)
   __shared__ double s_w[kScBuildWarps][3][32];
   __shared__ int s_at[kScBuildWarps][32];
   __shared__ int2 s_me[kScBuildWarps][32];
@@ -255,11 +256,10 @@ k_sc_build(ScGrid g, const double *__restrict__ pos, const int *__restrict__ sta
     for (int off = 4; off < 32; off <<= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, off));
     os[a] = v == 0x7fffffff ? 0 : v;
   }
-  int mlo = rs ? me.y : 0x7fffffff, mhi = rs ? me.y : -1;
-  for (int off = 1; off < 4; off <<= 1) {
-    mlo = min(mlo, __shfl_xor_sync(0xffffffffu, mlo, off));
-    mhi = max(mhi, __shfl_xor_sync(0xffffffffu, mhi, off));
-  }
+  // the cluster's molecule signature: bit (molecule mod 64) of each atom
+  // (two clusters can share a molecule only where their signatures meet)
+  unsigned long long sig = rs ? 1ull << (me.y & 63) : 0ull;
+  for (int off = 1; off < 4; off <<= 1) sig |= __shfl_xor_sync(0xffffffffu, sig, off);
   float xlo = lo[0], xhi = hi[0], ylo = lo[1], yhi = hi[1], zlo = lo[2], zhi = hi[2];
   for (int off = 4; off < 32; off <<= 1) {
     xlo = fminf(xlo, __shfl_xor_sync(0xffffffffu, xlo, off));
@@ -308,7 +308,7 @@ k_sc_build(ScGrid g, const double *__restrict__ pos, const int *__restrict__ sta
     clo[cl] = make_float4(lo[0], lo[1], lo[2], 0.f);
     chi[cl] = make_float4(hi[0], hi[1], hi[2], 0.f);
     corg[cl] = make_int4(og[0], og[1], og[2], 0);
-    cmol[cl] = make_int2(mlo, mhi);
+    cmol[cl] = make_int2((int)(unsigned)sig, (int)(unsigned)(sig >> 32));
   }
   if (lane == 0) {
     sorg[s] = make_int4(os[0], os[1], os[2], 0);
@@ -325,9 +325,17 @@ __device__ __forceinline__ float sc_gap2(float alo, float ahi, float blo, float 
   return d * d;
 }
 
-// One warp per supercluster: its cluster list (entries written at
-// s * kScCap, count in cnt[s]).
-__global__ void __launch_bounds__(32)
+// One block of kScListWarps warps per supercluster: its cluster list
+// (entries written at s * kScCap, count in cnt[s]).  The stencil's columns
+// that this supercluster lists are dealt to the warps in turn, each into its own shared-memory
+// buffer; the buffers are then concatenated in warp order (a fixed order,
+// so the lists, the tasks and every sum over them are the same on every
+// run).  (With one warp per supercluster, the chain of dependent loads over
+// all its columns took ~150 us on the 41k box.)
+constexpr int kScListWarps = 4;
+constexpr int kScWarpCap = 192;  // entries per warp buffer
+constexpr size_t kScListSmem = sizeof(ScEntry) * kScListWarps * kScWarpCap;
+__global__ void __launch_bounds__(32 * kScListWarps)
 k_sc_list(ScGrid g, const ScStencil st, const int *__restrict__ supbase,
           const int *__restrict__ ctl, const float4 *__restrict__ clo,
           const float4 *__restrict__ chi, const int4 *__restrict__ corg,
@@ -336,29 +344,35 @@ k_sc_list(ScGrid g, const ScStencil st, const int *__restrict__ supbase,
           const int *__restrict__ smol, const int *__restrict__ ex_start,
           const int2 *__restrict__ ex, ScEntry *__restrict__ ent, int *__restrict__ cnt,
           int *__restrict__ err) {
-  pdl_trigger();
   pdl_wait();
+  pdl_trigger();  // (after the wait: see k_sc_tasks)
+  extern __shared__ __align__(16) unsigned char s_raw[];
+  ScEntry *s_ent = reinterpret_cast<ScEntry *>(s_raw);
   __shared__ float4 s_lo[8], s_hi[8];
   __shared__ int2 s_mr[8];
   __shared__ int s_at[32], s_mo[32];
-  const int lane = threadIdx.x;
+  __shared__ int s_cnt[kScListWarps];
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
   const int s = blockIdx.x;
-  if (s >= sc_ctl(ctl)) return;
-  if (lane < 8) {
-    s_lo[lane] = clo[(size_t)s * 8 + lane];
-    s_hi[lane] = chi[(size_t)s * 8 + lane];
-    s_mr[lane] = cmol[(size_t)s * 8 + lane];
+  if (s >= sc_ctl(ctl)) return;  // uniform per block
+  if (threadIdx.x < 8) {
+    s_lo[threadIdx.x] = clo[(size_t)s * 8 + threadIdx.x];
+    s_hi[threadIdx.x] = chi[(size_t)s * 8 + threadIdx.x];
+    s_mr[threadIdx.x] = cmol[(size_t)s * 8 + threadIdx.x];
   }
-  s_at[lane] = satom[(size_t)s * kScAtoms + lane];
-  s_mo[lane] = smol[(size_t)s * kScAtoms + lane];
-  __syncwarp();
+  if (threadIdx.x < 32) {
+    s_at[threadIdx.x] = satom[(size_t)s * kScAtoms + threadIdx.x];
+    s_mo[threadIdx.x] = smol[(size_t)s * kScAtoms + threadIdx.x];
+  }
+  __syncthreads();
   const float4 bl = sbox[2 * (size_t)s], bh = sbox[2 * (size_t)s + 1];
   const int4 os = sorg[s];
   const int col = sc_column(supbase, g.ncol, s);
   const int cx = col / g.nsy, cy = col % g.nsy;
   const float zc = 0.5f * (bl.z + bh.z);
   int count = 0;
-  ScEntry *out = ent + (size_t)s * kScCap;
+  ScEntry *out = s_ent + wp * kScWarpCap;
+  int valid = 0;  // the columns this supercluster lists, dealt to the warps in turn
   for (int q = 0; q < st.n; q++) {
     int nx = cx + st.off[q].x, ny = cy + st.off[q].y;
     int imx = 0, imy = 0;
@@ -366,6 +380,7 @@ k_sc_list(ScGrid g, const ScStencil st, const int *__restrict__ supbase,
     if (ny < 0) { ny += g.nsy; imy = -1; } else if (ny >= g.nsy) { ny -= g.nsy; imy = 1; }
     const int col2 = nx * g.nsy + ny;
     if (col2 < col) continue;  // that column lists the pairs with this one
+    if (valid++ % kScListWarps != wp) continue;
     const float shx = imx * g.L[0], shy = imy * g.L[1];
     const int s0 = col2 == col ? s : supbase[col2], s1 = supbase[col2 + 1];
     for (int b0 = s0; b0 < s1; b0 += 32) {
@@ -394,14 +409,21 @@ k_sc_list(ScGrid g, const ScStencil st, const int *__restrict__ supbase,
         const int izs = __shfl_sync(0xffffffffu, imz, pick >= 0 ? pick : 0);
         unsigned imask = 0;
         unsigned words[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) words[k] = 0xFFFFu;
         int c = -1;
+        int4 oc = make_int4(0, 0, 0, 0);
         if (pick >= 0) {
           c = (b0 + pick) * 8 + (lane & 7);
+          // everything the candidate needs, in one round of loads
           const float4 jl = clo[c], jh = chi[c];
+          const int2 jm = cmol[c];
+          oc = corg[c];
+          const int4 a4 = *reinterpret_cast<const int4 *>(satom + (size_t)c * 4);
+          const int4 m4 = *reinterpret_cast<const int4 *>(smol + (size_t)c * 4);
           const float shz = izs * g.L[2];
 #pragma unroll
           for (int k = 0; k < 8; k++) {
-            words[k] = 0xFFFFu;
             if (c < s * 8 + k) continue;
             const float4 il = s_lo[k], ih = s_hi[k];
             const float d2 = sc_gap2(il.x, ih.x, jl.x + shx, jh.x + shx) +
@@ -410,31 +432,30 @@ k_sc_list(ScGrid g, const ScStencil st, const int *__restrict__ supbase,
             if (d2 < g.rlist2) imask |= 1u << k;
           }
           if (imask) {
-            const int2 jm = cmol[c];
-            int jat[4] = {-1, -1, -1, -1}, jmo[4] = {0, 0, 0, 0};
-            bool loaded = false;
+            const int jat[4] = {a4.x, a4.y, a4.z, a4.w};
+            const int jmo[4] = {m4.x, m4.y, m4.z, m4.w};
 #pragma unroll
             for (int k = 0; k < 8; k++) {
               if (!((imask >> k) & 1u)) continue;
               const bool self = c == s * 8 + k;
               const int2 im = s_mr[k];
-              if (!self && (im.y < jm.x || jm.y < im.x)) continue;  // no common molecule
-              if (!loaded) {
-                for (int b = 0; b < 4; b++) {
-                  jat[b] = satom[(size_t)c * 4 + b];
-                  jmo[b] = smol[(size_t)c * 4 + b];
-                }
-                loaded = true;
-              }
-              unsigned wd = 0;
+              if (!self && !((im.x & jm.x) | (im.y & jm.y))) continue;  // no common molecule
+              // pairs of one molecule (pads hold molecule -1 and never match
+              // a real atom's)
+              unsigned same = 0;
               for (int a = 0; a < 4; a++) {
-                const int ai = s_at[k * 4 + a], mi = s_mo[k * 4 + a];
-                for (int b = 0; b < 4; b++) {
-                  bool ok = !(self && b <= a);
-                  if (ok && ai >= 0 && jat[b] >= 0 && mi == jmo[b])
-                    ok = excl_kind(ex, ex_start[ai], ex_start[ai + 1], jat[b]) == 0;
-                  if (ok) wd |= 1u << (a * 4 + b);
-                }
+                const int mi = s_mo[k * 4 + a];
+                for (int b = 0; b < 4; b++)
+                  same |= (mi == jmo[b] && mi >= 0) ? 1u << (a * 4 + b) : 0u;
+              }
+              unsigned wd = self ? 0x08CEu /* bits a * 4 + b with b > a */ : 0xFFFFu;
+              wd &= ~same;
+              while (same) {  // same-molecule pairs: allowed unless excluded
+                const int bit = __ffs((int)same) - 1;
+                same &= same - 1u;
+                if (self && (bit & 3) <= (bit >> 2)) continue;
+                const int ai = s_at[k * 4 + (bit >> 2)], aj = jat[bit & 3];
+                if (excl_kind(ex, ex_start[ai], ex_start[ai + 1], aj) == 0) wd |= 1u << bit;
               }
               words[k] = wd;
             }
@@ -443,8 +464,7 @@ k_sc_list(ScGrid g, const ScStencil st, const int *__restrict__ supbase,
         const unsigned has = __ballot_sync(0xffffffffu, imask != 0);
         if (imask) {
           const int slot = count + __popc(has & ((1u << lane) - 1u));
-          if (slot < kScCap) {
-            const int4 oc = corg[c];
+          if (slot < kScWarpCap) {
             const int sx = oc.x - os.x + imx * g.m[0] + 512;
             const int sy = oc.y - os.y + imy * g.m[1] + 512;
             const int sz = oc.z - os.z + izs * g.m[2] + 512;
@@ -465,32 +485,84 @@ k_sc_list(ScGrid g, const ScStencil st, const int *__restrict__ supbase,
       }
     }
   }
-  if (lane == 0) {
-    if (count > kScCap) atomicOr(err, 8);
-    cnt[s] = min(count, kScCap);
+  if (lane == 0) s_cnt[wp] = count;
+  __syncthreads();
+  // concatenate the warps' buffers in warp order
+  int base = 0, total = 0;
+  bool over = false;
+  for (int v = 0; v < kScListWarps; v++) {
+    const int cv = s_cnt[v];
+    over = over || cv > kScWarpCap;
+    if (v < wp) base += min(cv, kScWarpCap);
+    total += min(cv, kScWarpCap);
+  }
+  const int mine = min(count, kScWarpCap);
+  ScEntry *dst = ent + (size_t)s * kScCap;
+  for (int i = lane; i < mine; i += 32)
+    if (base + i < kScCap) dst[base + i] = out[i];
+  if (threadIdx.x == 0) {
+    if (over || total > kScCap) atomicOr(err, 8);
+    cnt[s] = min(total, kScCap);
   }
 }
 
 // Tasks (supercluster, first entry, end) of at most kScChunk entries, in
 // supercluster order; ctl[1] = their number.  One block.
-__global__ void k_sc_tasks(const int *__restrict__ cnt, int *__restrict__ ctl,
-                           int4 *__restrict__ tasks) {
-  pdl_trigger();
+// Every kernel of the chain signals its dependent only once its own
+// predecessor is complete: the persistent pair kernel fills every SM slot
+// while it waits, and launched earlier it kept the list kernel's blocks from
+// the SMs (a step then took twice as long).
+__global__ void __launch_bounds__(1024)
+k_sc_tasks(const int *__restrict__ cnt, int *__restrict__ ctl, int4 *__restrict__ tasks) {
   pdl_wait();
+  pdl_trigger();  // (after the wait: the pair kernel's blocks may now take the SMs)
   __shared__ int sh[32];
+  __shared__ int s_base[kScTaskSups + 1];
+  __shared__ int s_cnt[kScTaskSups];
   const int ns = sc_ctl(ctl);
   const int T = blockDim.x, t = threadIdx.x;
-  const int span = (ns + T - 1) / T;
-  const int lo = t * span, hi = min(ns, lo + span);
-  int sum = 0;
-  for (int s = lo; s < hi; s++) sum += (cnt[s] + kScChunk - 1) / kScChunk;
-  const int incl = sc_block_scan(sum, sh);
-  int base = incl - sum;
-  for (int s = lo; s < hi; s++) {
-    const int e0 = s * kScCap, e1 = e0 + cnt[s];
-    for (int e = e0; e < e1; e += kScChunk) tasks[base++] = make_int4(s, e, min(e1, e + kScChunk), 0);
+  int done = 0;  // tasks of the superclusters before this round
+  // rounds of kScTaskSups superclusters: their task counts scanned, then
+  // the tasks written by the whole block (task i of the round found by a
+  // binary search over the round's prefix)
+  for (int r0 = 0; r0 < ns; r0 += kScTaskSups) {
+    const int nr = min(kScTaskSups, ns - r0);
+    const int per = (kScTaskSups + T - 1) / T;
+    int sum = 0;
+    int mine[4];
+    for (int q = 0; q < per; q++) {
+      const int sI = t * per + q;
+      const int cv = sI < nr ? cnt[r0 + sI] : 0;
+      if (sI < nr) s_cnt[sI] = cv;
+      mine[q] = (cv + kScChunk - 1) / kScChunk;
+      sum += mine[q];
+    }
+    const int incl = sc_block_scan(sum, sh);
+    int b = incl - sum;
+    for (int q = 0; q < per; q++) {
+      const int sI = t * per + q;
+      if (sI < nr) s_base[sI] = b;
+      b += mine[q];
+    }
+    if (t == T - 1) s_base[nr] = incl;
+    __syncthreads();
+    const int total = s_base[nr];
+    for (int i = t; i < total; i += T) {
+      int lo = 0, hi = nr;  // the last supercluster whose first task is <= i
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (s_base[mid] <= i) lo = mid;
+        else hi = mid;
+      }
+      const int sI = r0 + lo, q = i - s_base[lo];
+      const int e0 = sI * kScCap, e1 = e0 + s_cnt[lo];
+      const int e = e0 + q * kScChunk;
+      tasks[done + i] = make_int4(sI, e, min(e1, e + kScChunk), 0);
+    }
+    done += total;
+    __syncthreads();
   }
-  if (t == T - 1) ctl[1] = incl;
+  if (t == 0) ctl[1] = done;
 }
 
 // Persistent pair kernel: each one-warp block takes tasks from the counter
@@ -502,7 +574,9 @@ __global__ void k_sc_tasks(const int *__restrict__ cnt, int *__restrict__ ctl,
 #ifndef PMB200_SC_BLOCKS_E
 #define PMB200_SC_BLOCKS_E 20
 #endif
-template <bool kEnergy>
+// kFull: both switches end at the pair cutoff (a pair that passes the
+// cutoff test is within both), so no per-switch range selects are needed.
+template <bool kEnergy, bool kFull>
 __global__ void __launch_bounds__(32, kEnergy ? PMB200_SC_BLOCKS_E : PMB200_SC_BLOCKS)
 k_sc_pair(MixedConsts mc, int ntypes, const double4 *__restrict__ lj64,
           const int4 *__restrict__ tasks, int *__restrict__ ctl,
@@ -608,19 +682,18 @@ k_sc_pair(MixedConsts mc, int ntypes, const double4 *__restrict__ lj64,
             const float c2 = mc.rclj2 - r2;
             const float c4 = c2 * fmaf(2.0f, r2, mc.s2);
             const bool on = r2 >= mc.ron2;
-            const bool in = r2 <= mc.rclj2;
+            const bool in = kFull || r2 <= mc.rclj2;
             svl = in ? (on ? mc.s1 * (c2 * c4) : 1.0f) : 0.0f;
             const float sd = (in && on) ? mc.s3 * fmaf(c2, c2, -c4) : 0.0f;
             flj = fmaf(flj, svl, -elj * sd);
           }
           float fc;
-          {  // C1 switched Coulomb, branch-free (zero beyond its cutoff)
-            const bool inC = r2 <= mc.rcc2;
-            const float ec = pi.w * pj.w * rinv;
-            const float dist = r2 * rinv;
-            const float sv = fmaf(-dist, fmaf(-r2, mc.c05_3, mc.c15_1), 1.0f);
-            const float sd = fmaf(dist, mc.c15_3, -mc.c15_1 * rinv);
-            fc = inC ? __fmul_rn(ec, fmaf(r2inv, sv, -sd)) : 0.f;
+          {  // C1 switched Coulomb, branch-free (zero beyond its cutoff):
+             // E S = q q (1/r - 1.5/rc + 0.5 r^2/rc^3), so F S - E dS over r
+             // is q q (1/r^3 - 1/rc^3)
+            const bool inC = kFull || r2 <= mc.rcc2;
+            const float qq = pi.w * pj.w;
+            fc = inC ? __fmul_rn(qq, fmaf(r2inv, rinv, -2.0f * mc.c05_3)) : 0.f;
             if (kEnergy) {
               // q_i q_j g(r) from the FP64 distance (as the search kernel)
               const double ex_ = pdx - s_d[0][k * 4 + ti];
@@ -632,7 +705,7 @@ k_sc_pair(MixedConsts mc, int ntypes, const double4 *__restrict__ lj64,
               const double gd = fma(mc.e05, r2d, rid - mc.e15);
               // (selected, not multiplied by zero: a masked pair's terms
               // need not be finite)
-              const double eu = fma((double)__fmul_rn(pi.w, pj.w), gd, eU);
+              const double eu = fma((double)qq, gd, eU);
               eU = (ok && inC) ? eu : eU;
               // LJ: (A s^-6 - B s^-3) S with s^-1 = (1/r)^2 in FP64
               const double2 ab = s_ljd[row + tjt];
