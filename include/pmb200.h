@@ -116,7 +116,9 @@ int pmb200_set_box(pmb200_ctx *ctx, const double e1[3], const double e2[3],
  * ACCUMULATED into, like the reference.  energies[2] = {COULOMB,
  * LENNARDJONES}: accumulated into (may be NULL when !(flags&ENERGY)).
  * virial[9], molvirial[9] row-major xx..zz: accumulated into when the flag is
- * set (else may be NULL). */
+ * set (else may be NULL).  A PMB200_MIXED context's forces reach the host in
+ * FP32 (its kernels' forces are good to ~1e-6; the device entry points return
+ * them in FP64). */
 int pmb200_eval(pmb200_ctx *ctx, const double *pos, double *forces,
                 double *energies, double *virial, double *molvirial,
                 unsigned flags);

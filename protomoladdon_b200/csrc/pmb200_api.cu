@@ -132,6 +132,8 @@ struct pmb200_ctx {
   SettleParams sp{};
   // host-buffer evaluation scratch: device copies and pinned staging
   double *d_hpos = nullptr, *d_hfrc = nullptr;
+  // host-buffer calls of mixed contexts read the forces back in FP32
+  float *d_hf32 = nullptr;
   double *h_pin_pos = nullptr, *h_pin_frc = nullptr, *h_pin_out = nullptr;
   int n_pin = 0;
   // leapfrog graph
@@ -446,6 +448,7 @@ int ensure_atom_buffers(pmb200_ctx *c) {
   CK(dalloc(c->d_cbhi, n));
   CK(dalloc(c->d_hpos, 3 * n));
   CK(dalloc(c->d_hfrc, 3 * n + kPinOut + 3));  // forces, then the results (pmb200_eval)
+  CK(dalloc(c->d_hf32, 3 * n + 2 + 2 * (kPinOut + 3)));  // FP32 forces, then the results
   c->n_alloc = c->n;
   return PMB200_OK;
 }
@@ -709,6 +712,21 @@ void launch_cell_build(pmb200_ctx *c, const double *d_pos, bool mixed, bool lo,
 
 // One word copied on the device (the error flag into the results' copy).
 __global__ void k_copy_word(const int *__restrict__ src, int *__restrict__ dst) { *dst = *src; }
+
+// Host-buffer calls of mixed contexts read the forces back in FP32 (the
+// mixed kernels' forces are good to ~1e-6; FP32 keeps 6e-8 of each, and the
+// copy is half as long), then the result words.  (Sending the positions as
+// 32-bit box fractions was measured too: the host's encoding pass cost what
+// the shorter copy saved.)
+__global__ void k_pack_out(size_t n3, const double *__restrict__ frc,
+                           const double *__restrict__ res, float *__restrict__ out) {
+  const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n3) out[k] = (float)frc[k];
+  // the result words (and the error flag behind them) after the forces, at
+  // a double boundary
+  double *tail = reinterpret_cast<double *>(out + ((n3 + 1) & ~(size_t)1));
+  if (k < (size_t)kPinOut) tail[k] = res[k];
+}
 
 // The supercluster kernel's grid, stencil, constants and buffers for the
 // current box and topology (sc_ok = false where it does not apply: the
@@ -1209,6 +1227,7 @@ int pmb200_destroy(pmb200_ctx *c) {
   if (c->h_pin_pos) cudaFreeHost(c->h_pin_pos);
   if (c->h_pin_frc) cudaFreeHost(c->h_pin_frc);
   if (c->h_pin_out) cudaFreeHost(c->h_pin_out); dfree(c->d_hpos); dfree(c->d_hfrc);
+  dfree(c->d_hf32);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->ev_lj) cudaEventDestroy(c->ev_lj);
@@ -2118,14 +2137,15 @@ int pmb200_eval(pmb200_ctx *c, const double *pos, double *forces, double *energi
   // the results travel behind the forces in one copy: d_hfrc holds the 3n
   // forces, then the 20 result words, then the device error flag
   double *d_hout = c->d_hfrc + cnt;
-  const double *h_res = c->h_pin_frc + cnt;
   const size_t res_bytes = bytes + sizeof(double) * kPinOut;
-  int *h_err = reinterpret_cast<int *>(c->h_pin_frc + cnt + 20);
+  bool f32out = false;  // FP32 forces back this call (set below)
   // positions through pinned staging; this evaluation's forces are computed
   // on the device (overwrite), read back, and added to the caller's array
   if (c->n > 0) {
     // page-locked caller arrays are transferred directly; pageable ones go
     // through the pinned staging copy, made on the host's cores
+    // FP32 forces back for mixed contexts (see k_pack_out)
+    f32out = c->p.precision == PMB200_MIXED;
     cudaPointerAttributes attr{};
     const bool pinned = cudaPointerGetAttributes(&attr, pos) == cudaSuccess &&
                         attr.type == cudaMemoryTypeHost;
@@ -2144,15 +2164,24 @@ int pmb200_eval(pmb200_ctx *c, const double *pos, double *forces, double *energi
     // replayed while the context's box and topology stay the same (the
     // pair-kernel timing mode launches directly).  The results and the
     // error flag follow the forces in d_hfrc, so one copy brings all back.
+    const size_t f32_slots = (cnt + 1) & ~(size_t)1;  // FP32 forces, to a double boundary
+    const size_t res32_bytes = sizeof(float) * f32_slots + sizeof(double) * kPinOut;
     auto sequence = [&]() -> int {
+      const unsigned eb = (unsigned)((cnt + 255) / 256);
       cudaError_t e = cudaMemcpyAsync(c->d_hpos, src, bytes, cudaMemcpyHostToDevice, st);
       if (e != cudaSuccess) return fail(c, PMB200_ECUDA, "copy in: %s", cudaGetErrorString(e));
       int r = launch_eval(c, c->d_hpos, c->d_hfrc, d_hout, flags, 0, st);
       if (r) return r;
       k_copy_word<<<1, 1, 0, st>>>(c->d_err, reinterpret_cast<int *>(d_hout + 20));
       e = cudaGetLastError();
-      if (e == cudaSuccess)
+      if (e == cudaSuccess && f32out) {
+        k_pack_out<<<eb, 256, 0, st>>>(cnt, c->d_hfrc, d_hout, c->d_hf32);
+        e = cudaGetLastError();
+        if (e == cudaSuccess)
+          e = cudaMemcpyAsync(c->h_pin_frc, c->d_hf32, res32_bytes, cudaMemcpyDeviceToHost, st);
+      } else if (e == cudaSuccess) {
         e = cudaMemcpyAsync(c->h_pin_frc, c->d_hfrc, res_bytes, cudaMemcpyDeviceToHost, st);
+      }
       if (e != cudaSuccess) return fail(c, PMB200_ECUDA, "copy out: %s", cudaGetErrorString(e));
       return PMB200_OK;
     };
@@ -2160,7 +2189,8 @@ int pmb200_eval(pmb200_ctx *c, const double *pos, double *forces, double *energi
       rc = sequence();
       if (rc) return rc;
     } else {
-      if (!c->hgraph_exec || c->hgraph_src != src || c->hgraph_flags != flags) {
+      const unsigned gkey = flags | (f32out ? 0x80000000u : 0u);
+      if (!c->hgraph_exec || c->hgraph_src != src || c->hgraph_flags != gkey) {
         if (c->hgraph_exec) cudaGraphExecDestroy(c->hgraph_exec);
         if (c->hgraph) cudaGraphDestroy(c->hgraph);
         c->hgraph_exec = nullptr;
@@ -2178,7 +2208,7 @@ int pmb200_eval(pmb200_ctx *c, const double *pos, double *forces, double *energi
         c->hgraph = gr;
         CK(cudaGraphInstantiate(&c->hgraph_exec, gr, 0));
         c->hgraph_src = src;
-        c->hgraph_flags = flags;
+        c->hgraph_flags = gkey;
       }
       rc = ensure_clear(c, st);
       if (rc) return rc;
@@ -2194,15 +2224,22 @@ int pmb200_eval(pmb200_ctx *c, const double *pos, double *forces, double *energi
   }
   // the error flag came back with the results: one synchronisation
   CK(cudaStreamSynchronize(st));
-  rc = device_error(c, *h_err);
+  const size_t res_at = f32out ? ((cnt + 1) & ~(size_t)1) / 2 : cnt;  // (in doubles)
+  const double *out = c->h_pin_frc + res_at;
+  rc = device_error(c, *reinterpret_cast<const int *>(out + 20));
   if (rc) return rc;
   {
-    const double *src = c->h_pin_frc;
     const long long m = (long long)cnt;
+    if (f32out) {
+      const float *src = reinterpret_cast<const float *>(c->h_pin_frc);
 #pragma omp parallel for schedule(static) if (m > 65536)
-    for (long long k = 0; k < m; k++) forces[k] += src[k];
+      for (long long k = 0; k < m; k++) forces[k] += (double)src[k];
+    } else {
+      const double *src = c->h_pin_frc;
+#pragma omp parallel for schedule(static) if (m > 65536)
+      for (long long k = 0; k < m; k++) forces[k] += src[k];
+    }
   }
-  const double *out = h_res;
   if (flags & PMB200_ENERGY) {
     energies[0] += out[0];
     energies[1] += out[1];

@@ -32,10 +32,20 @@ def _make(kind, s, precision):
 def test_ranks_sum_to_one_evaluation(kind, precision):
     s = water.water_box(9, rc=8.0, ron=7.0, seed=33)
     topo = PeriodicTopology.from_dict(s)
+    import torch
     f = _make(kind, s, precision)
     F1 = np.zeros_like(s["pos"])
     E1 = ScalarStructure(virial=True, molecular_virial=True)
     f.evaluate(topo, s["pos"], F1, E1)
+    # the forces of one evaluation in FP64 (the host-buffer call of a mixed
+    # context returns them in FP32)
+    # (an energy launch, as the shares are: the same task split)
+    pos = torch.tensor(s["pos"], dtype=torch.float64, device="cuda:0")
+    frc = torch.zeros_like(pos)
+    out = torch.zeros(20, dtype=torch.float64, device="cuda:0")
+    f.evaluate_device(topo, pos.data_ptr(), frc.data_ptr(), out.data_ptr(), 1)
+    f.sync()
+    F1 = frc.cpu().numpy()
     blocks = f.number_of_blocks(topo)
     assert blocks == int(np.prod(f.grid()[0]))
     for nranks in (1, 2, 3, 7, blocks + 3):  # the last: some ranks get no block

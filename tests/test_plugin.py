@@ -261,7 +261,9 @@ def test_plugin_parallel_evaluate_matches_evaluate(water648, which):
                                        water648["rc_alg"])
     assert blocks == f.number_of_blocks(PeriodicTopology.from_dict(water648))
     f.close()
-    np.testing.assert_allclose(par[2], plain[2], rtol=0, atol=1e-12 * np.abs(plain[2]).max())
+    # (evaluate's host-buffer call returns the mixed forces rounded to FP32;
+    # the block shares come back in FP64)
+    np.testing.assert_allclose(par[2], plain[2], rtol=0, atol=1e-7 * np.abs(plain[2]).max())
     np.testing.assert_allclose(par[3], plain[3], rtol=1e-12)
     np.testing.assert_allclose(par[4], plain[4], rtol=1e-12, atol=1e-12)
     np.testing.assert_allclose(par[5], plain[5], rtol=1e-12, atol=1e-12)
@@ -286,6 +288,7 @@ def test_plugin_ewald_and_pair_parallel_evaluate(water648):
         R.close()
         assert plain[0] == 0 and par[0] == 0, par[1]
         assert blocks >= 1
+        # (mixed forces: FP32 from evaluate's host-buffer call, FP64 shares)
         np.testing.assert_allclose(par[2], plain[2], rtol=0,
-                                   atol=1e-12 * np.abs(plain[2]).max())
+                                   atol=1e-7 * np.abs(plain[2]).max())
         np.testing.assert_allclose(par[3], plain[3], rtol=1e-12, atol=1e-12)
