@@ -366,7 +366,7 @@ def run_ours(args):
     _ft, F = pinned_copy(np.zeros_like(s["pos"]))
     E = ScalarStructure()
     fmix.evaluate(topo, xh, F, E)
-    e2e_steps = min(args.steps, 100)
+    e2e_steps = min(args.steps, 500)
     e2e_t, integ_t, call_t = [], [], []
 
     def host_step():
