@@ -171,3 +171,32 @@ def test_autotune_may_choose_it(medium):
     f.close()
     assert rms_rel(F, fo) <= 1e-5
     assert abs(E[0] - eo[0]) <= 1e-6 * abs(eo[0])
+
+
+def test_dense_system_reports_list_overflow():
+    """Atoms packed ~5x denser than water: a supercluster's list outgrows its
+    buffer, the list kernel stops writing at the bound and flags it, and the
+    evaluation reports PMB200_EDEVICE; the search kernel then serves the same
+    context."""
+    from protomoladdon_b200._lib import PmbError
+    s = water.water_box(16, rc=10.0, ron=9.0, seed=5)
+    scale = 0.6
+    s["pos"] = s["pos"] * scale
+    s["box"] = s["box"] * scale
+    s["origin"] = s["origin"] * scale
+    topo = PeriodicTopology.from_dict(s)
+    f = NonbondedCutoffB200SystemForce(s["ron"], s["rc_lj"], s["rc_coul"], s["rc_alg"],
+                                       precision="mixed")
+    f.set_pair_kernel("clusters")
+    F = np.zeros_like(s["pos"])
+    E = ScalarStructure()
+    with pytest.raises(PmbError) as ei:
+        f.evaluate(topo, s["pos"], F, E)
+    assert ei.value.code == _lib.PMB200_EDEVICE and "supercluster kernel" in str(ei.value)
+    f.set_pair_kernel("search")
+    F = np.zeros_like(s["pos"])
+    E = ScalarStructure()
+    f.evaluate(topo, s["pos"], F, E)
+    f.close()
+    fo, eo, _, _ = O.restate_eval(s, s["pos"], virial_mode=0)
+    assert rms_rel(F, fo) <= 1e-5
