@@ -349,6 +349,19 @@ def run_ours(args):
         s64, k64, _ = device_run(f64, _lib.PMB200_ENERGY)
         f64.close()
         fp64 = (sum(s64), statistics.mean(k64))
+    # the other pair kernel of mixed contexts, the supercluster kernel, on
+    # the same steps (the autotuner's choice is the headline; this is its
+    # alternative, reported beside it)
+    other = None
+    if (args.precision == "mixed" and not args.skip_alternative and args.pair_kernel == "auto"
+            and tuned["mixed"].get("kernel_energy") != "clusters"):
+        fc = make("mixed")
+        fc.set_pair_kernel("clusters")
+        ce_ms, ce_k, _ = device_run(fc, _lib.PMB200_ENERGY)
+        cf_ms, cf_k, _ = device_run(fc, 0)
+        fc.close()
+        other = (statistics.mean(ce_ms), statistics.mean(ce_k), statistics.mean(cf_ms),
+                 statistics.mean(cf_k))
 
     # end to end through the host-buffer C-ABI call (SystemForce::evaluate's
     # replacement): the host integrator does kick + drift + SETTLE, as
@@ -480,6 +493,15 @@ def run_ours(args):
                             "pair_kernel_ms": statistics.mean(fo_kms),
                             "note": "the same device steps without energies"},
             "autotune": tuned,
+            **({"alternative_pair_kernel": {
+                "kernel": "clusters (k_sc_pair: device-built supercluster lists, 4x4 tiles)",
+                "ms_per_step": other[0], "pair_kernel_ms": other[1],
+                "forces_only_ms_per_step": other[2], "forces_only_pair_kernel_ms": other[3],
+                "pair_kernel_fp32_frac": (FLOPS_PER_PAIR * pairs / (other[1] * 1e-3) / 1e12
+                                          / peak) if peak else None,
+                "note": "the same device steps on the supercluster kernel: its pair kernel is "
+                        "faster, its per-step list build costs more; the autotuner keeps "
+                        "the faster whole step"}} if other else {}),
             "gpu_launches": (KERNELS_PER_STEP_CLUSTERS if kern_e == "clusters"
                              else KERNELS_PER_STEP) * args.steps,
             "clocks": clocks,
@@ -1048,6 +1070,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=20)
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-fp64", action="store_true")
+    ap.add_argument("--skip-alternative", action="store_true",
+                    help="do not time the supercluster kernel beside the autotuned one")
     ap.add_argument("--skip-accuracy", action="store_true")
     ap.add_argument("--pair-kernel", default="auto", choices=["auto", "search", "clusters"],
                     help="mixed pair kernel: auto (pmb200_autotune) or a fixed one")
