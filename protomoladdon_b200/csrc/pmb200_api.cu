@@ -1664,8 +1664,24 @@ int pmb200_autotune(pmb200_ctx *c, const double *d_pos, void *stream, int reps,
       if (r) return r;
       cudaGraph_t gr = nullptr;
       cudaGraphExec_t ge = nullptr;
-      if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
-        return fail(c, PMB200_ECUDA, "autotune: capture failed");
+      if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        // a stream that cannot be captured (the legacy default stream):
+        // direct launches, timed the same way
+        cudaGetLastError();
+        r = launch_eval(c, d_pos, c->d_hfrc, c->d_out, flags, 0, st);  // warm-up
+        for (int k = 0; k < reps && !r; k++) {
+          if (cudaEventRecord(e0, st) != cudaSuccess) return PMB200_ECUDA;
+          r = launch_eval(c, d_pos, c->d_hfrc, c->d_out, flags, 0, st);
+          if (!r && (cudaEventRecord(e1, st) != cudaSuccess ||
+                     cudaEventSynchronize(e1) != cudaSuccess ||
+                     cudaEventElapsedTime(&t[k], e0, e1) != cudaSuccess))
+            r = PMB200_ECUDA;
+        }
+        if (r) return r;
+        std::nth_element(t.begin(), t.begin() + reps / 2, t.end());
+        ms = t[reps / 2];
+        return PMB200_OK;
+      }
       r = launch_eval(c, d_pos, c->d_hfrc, c->d_out, flags, 0, st);
       const cudaError_t ce = cudaStreamEndCapture(st, &gr);
       if (r || ce != cudaSuccess || cudaGraphInstantiate(&ge, gr, 0) != cudaSuccess) {

@@ -73,3 +73,26 @@ def test_tuned_fp64_context_matches_reference(water648):
     assert rms_rel(F, d["ref_forces"]) <= 1e-12
     e = d["ref_energies"]
     assert abs(E[0] - e[0]) <= 1e-11 * abs(e[0]) and abs(E[1] - e[1]) <= 1e-11 * abs(e[1])
+
+
+def test_tuning_on_the_legacy_default_stream():
+    """The tuner times graph replays of an evaluation; on a stream that
+    cannot be captured (the legacy default stream, handle 0x1) it times
+    direct launches instead, with the same result structure.  (A fresh box
+    size, so that no cached choice is taken.)"""
+    import torch
+    from protomoladdon_b200 import water
+    d = water.water_box(7, rc=8.0, ron=7.0, seed=21)
+    topo = PeriodicTopology.from_dict(d)
+    f = NonbondedCutoffB200SystemForce(d["ron"], d["rc_lj"], d["rc_coul"], d["rc_alg"])
+    pos = torch.tensor(d["pos"], dtype=torch.float64, device="cuda:0")
+    torch.cuda.synchronize()
+    choice = f.autotune(topo, pos.data_ptr(), reps=2, stream=0x1)
+    assert choice["configurations_timed"] > 0 and choice["ms_energy"] > 0.0
+    F = np.zeros_like(d["pos"])
+    E = ScalarStructure()
+    f.evaluate(topo, d["pos"], F, E)
+    f.close()
+    from oracle import oracle as O
+    fo, eo, _, _ = O.restate_eval(d, d["pos"], virial_mode=0)
+    assert rms_rel(F, fo) <= 1e-5
