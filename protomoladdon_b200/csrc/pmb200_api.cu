@@ -126,6 +126,7 @@ struct pmb200_ctx {
   double4 *d_wsorted = nullptr;  // a Hessian-vector product's direction, sorted order
   size_t ws_alloc = 0;
   double *d_pairs = nullptr, *d_out = nullptr, *d_red = nullptr;
+  unsigned *d_redctr = nullptr;  // k_finalize_reduce's arrival counter (wraps to 0)
   // rigid waters (SETTLE) for the device integrator
   int nwater = 0, nfree = 0;
   int *d_widx = nullptr, *d_fidx = nullptr;
@@ -979,6 +980,17 @@ int launch_eval(pmb200_ctx *c, const double *d_pos, double *d_forces, double *d_
     else if (c->form == FORM_EWALD_EXACT)
       launch_pair_mixed<FORM_EWALD_EXACT>(c, flags, st, 0, -1, nullptr, pdl);
     else launch_pair_mixed<FORM_CUTOFF>(c, flags, st, 0, -1, nullptr, pdl);
+    if (n > 0 && (energy || virial) && !timed) {
+      // forces and the reduction of the partial rows in one launch
+      const int ns = virial ? ACC_MV : ACC_E;  // the slots the launch filled
+      launch_k(k_finalize_reduce, (unsigned)std::max((n + 255) / 256, kRedBlocks), 256, 0, st,
+               pdl, n, (const unsigned long long *)c->d_facc, (const int *)c->d_sidx,
+               fscale * kFixInv, accumulate, d_forces, g.ncell * ctx_slots(c, true),
+               (const double *)c->d_partial, c->d_red, c->d_redctr, 1.0,
+               d_out ? d_out : c->d_out, c->d_pairs, ns);
+      CK(cudaGetLastError());
+      return PMB200_OK;
+    }
     if (n > 0)
       launch_k(k_finalize, (unsigned)((n + 255) / 256), 256, 0, st, pdl, n,
                (const unsigned long long *)c->d_facc, (const int *)c->d_sidx, fscale * kFixInv,
@@ -1056,6 +1068,8 @@ int pmb200_create(const pmb200_params *params, pmb200_ctx **out) {
   if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_out, sizeof(double) * 20);
   if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_pairs, sizeof(double));
   if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_red, sizeof(double) * kRedBlocks * ACC_MV);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_redctr, sizeof(unsigned));
+  if (e == cudaSuccess) e = cudaMemset(c->d_redctr, 0, sizeof(unsigned));
   if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
   if (e != cudaSuccess) {
@@ -1217,7 +1231,7 @@ int pmb200_destroy(pmb200_ctx *c) {
   dfree(c->d_rel32); dfree(c->d_spos32); dfree(c->d_rel_lo); dfree(c->d_spos_lo); dfree(c->d_rel64); dfree(c->d_spos64);
   dfree(c->d_smeta); dfree(c->d_com); dfree(c->d_facc);
   dfree(c->d_tpart); dfree(c->d_gq); dfree(c->d_glj); dfree(c->d_wsorted);
-  dfree(c->d_pairs); dfree(c->d_out); dfree(c->d_red); dfree(c->d_widx); dfree(c->d_fidx);
+  dfree(c->d_pairs); dfree(c->d_out); dfree(c->d_red); dfree(c->d_redctr); dfree(c->d_widx); dfree(c->d_fidx);
   dfree(c->d_sc_count); dfree(c->d_sc_start); dfree(c->d_sc_supbase); dfree(c->d_sc_ctl);
   dfree(c->d_sc_atom); dfree(c->d_sc_type); dfree(c->d_sc_mol); dfree(c->d_sc_cnt);
   dfree(c->d_sc_xi); dfree(c->d_sc_xj); dfree(c->d_sc_xilo); dfree(c->d_sc_xjlo);

@@ -2342,14 +2342,16 @@ __global__ void k_com(int nmol, const int *__restrict__ mstart, const int *__res
 // with the C1 constants (cell units) applied here in FP64.
 constexpr int kRedBlocks = 64;
 
-__global__ void k_reduce1(int ncell, const double *__restrict__ partial,
-                          double *__restrict__ red, int ns) {
+// k_reduce1's work for block b of kRedBlocks (256 threads): the first ns
+// slots of rows [b * span, (b + 1) * span) summed, written to red[b][.]
+__device__ __forceinline__ void reduce1_block(int b, int nrows, const double *__restrict__ partial,
+                                              double *__restrict__ red, int ns,
+                                              double (*sh)[ACC_MV]) {
   // each thread sums its rows' first ns slots; warp shuffles, then the
   // block's warps in order (fixed order: deterministic)
-  __shared__ double sh[8][ACC_MV];
   const int t = threadIdx.x, lane = t & 31, w = t >> 5;
-  const int span = (ncell + gridDim.x - 1) / gridDim.x;
-  const int lo = blockIdx.x * span, hi = min(ncell, lo + span);
+  const int span = (nrows + kRedBlocks - 1) / kRedBlocks;
+  const int lo = b * span, hi = min(nrows, lo + span);
   double v[ACC_MV];
 #pragma unroll
   for (int k = 0; k < ACC_MV; k++) v[k] = 0.0;
@@ -2367,20 +2369,24 @@ __global__ void k_reduce1(int ncell, const double *__restrict__ partial,
   if (t < ns) {
     double acc = 0.0;
     for (int q = 0; q < (int)(blockDim.x >> 5); q++) acc += sh[q][t];
-    red[blockIdx.x * ACC_MV + t] = acc;
+    red[b * ACC_MV + t] = acc;
   }
 }
 
-__global__ void k_reduce2(int nred, const double *__restrict__ red, double visit,
-                          double *__restrict__ out, double *__restrict__ pairs_out, int ns) {
+// k_reduce2's work (one block): the kRedBlocks block totals summed and the
+// results written (red read through L2: written by other blocks of the same
+// launch in k_finalize_reduce).
+__device__ __forceinline__ void reduce2_block(int nred, const double *red, double visit,
+                                              double *__restrict__ out,
+                                              double *__restrict__ pairs_out, int ns,
+                                              double *col) {
   // each of the first ns slots summed over the blocks in block order by one
   // warp (fixed order: deterministic); slots beyond ns are zero
-  __shared__ double col[ACC_MV];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   for (int k = w; k < ACC_MV; k += (int)(blockDim.x >> 5)) {
     double acc = 0.0;
     if (k < ns)
-      for (int b = lane; b < nred; b += 32) acc += red[b * ACC_MV + k];
+      for (int b = lane; b < nred; b += 32) acc += __ldcg(red + b * ACC_MV + k);
     acc = warp_sum_mask(acc, 32);
     if (lane == 0) col[k] = acc;
   }
@@ -2402,6 +2408,60 @@ __global__ void k_reduce2(int nred, const double *__restrict__ red, double visit
     out[11 + k] = visit * r[ACC_MW + map[k]];
   }
   if (pairs_out) *pairs_out = visit * r[ACC_PAIRS];
+}
+
+// Launched with kRedBlocks blocks of 256 threads.
+__global__ void k_reduce1(int nrows, const double *__restrict__ partial,
+                          double *__restrict__ red, int ns) {
+  __shared__ double sh[8][ACC_MV];
+  reduce1_block(blockIdx.x, nrows, partial, red, ns, sh);
+}
+
+// One block of 256 threads; nred = kRedBlocks.
+__global__ void k_reduce2(int nred, const double *__restrict__ red, double visit,
+                          double *__restrict__ out, double *__restrict__ pairs_out, int ns) {
+  __shared__ double col[ACC_MV];
+  reduce2_block(nred, red, visit, out, pairs_out, ns, col);
+}
+
+// k_finalize, k_reduce1 and k_reduce2 of one evaluation in one launch (the
+// energy and virial evaluations of the mixed kernels): every block finalizes
+// its 256 atoms; blocks 0 .. kRedBlocks - 1 also do k_reduce1's work for
+// their index, and the last of them to finish (an arrival counter that
+// atomicInc wraps back to zero for the next launch) does k_reduce2's -- the
+// same sums in the same order, so the results equal those of the three
+// kernels bit for bit, without two launches and their gaps.  Launch:
+// max(ceil(n / 256), kRedBlocks) blocks of 256 threads.
+__global__ void __launch_bounds__(256)
+k_finalize_reduce(int n, const unsigned long long *__restrict__ facc,
+                  const int *__restrict__ sidx, double scale, int accumulate,
+                  double *__restrict__ forces, int nrows, const double *__restrict__ partial,
+                  double *red, unsigned *__restrict__ arrivals, double visit,
+                  double *__restrict__ out, double *__restrict__ pairs_out, int ns) {
+  pdl_wait();
+  __shared__ double sh[8][ACC_MV];
+  __shared__ double col[ACC_MV];
+  __shared__ unsigned s_arrived;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < n) {
+    const int o = sidx[j];
+    double *fo = forces + 3 * (size_t)o;
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      const double v = (double)(long long)facc[(size_t)q * n + j] * scale;
+      fo[q] = accumulate ? fo[q] + v : v;
+    }
+  }
+  if (blockIdx.x >= kRedBlocks) return;  // uniform per block
+  reduce1_block(blockIdx.x, nrows, partial, red, ns, sh);
+  // this block's totals visible device-wide before its arrival is counted
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_arrived = atomicInc(arrivals, kRedBlocks - 1);
+  __syncthreads();
+  if (s_arrived != kRedBlocks - 1) return;  // uniform per block
+  __threadfence();
+  reduce2_block(kRedBlocks, red, visit, out, pairs_out, ns, col);
 }
 
 // Leapfrog kick + drift (LeapfrogIntegrator::doKickdoDrift without modifiers,

@@ -109,6 +109,36 @@ def test_deterministic_and_accumulates(water648, precision):
     assert np.allclose(F3, 2 * F1, rtol=1e-15, atol=1e-12)
 
 
+@pytest.mark.parametrize("box,virial", [("water648", True), ("water648", False),
+                                        ("medium", False)])
+def test_fused_reduction_equals_separate_kernels(box, virial, request):
+    """Mixed energy evaluations finalize the forces and reduce the partial
+    rows in one launch (k_finalize_reduce); the kernel-timing mode runs
+    k_finalize, k_reduce1 and k_reduce2 instead.  Same sums in the same order:
+    forces, energies, virials and pair counts equal bit for bit, on a box of
+    fewer atoms than reduction blocks and on one of more, twice in a row (the
+    arrival counter starts from zero again)."""
+    d = request.getfixturevalue(box)
+    topo = PeriodicTopology.from_dict(d)
+    res = []
+    for timing in (False, True, False):
+        f = NonbondedCutoffB200SystemForce(d["ron"], d["rc_lj"], d["rc_coul"], d["rc_alg"],
+                                           precision="mixed")
+        f.set_pair_kernel("search")
+        f._ensure(topo)
+        f.set_kernel_timing(timing)
+        for _ in range(2):
+            F = np.zeros_like(d["pos"])
+            E = ScalarStructure(virial=virial, molecular_virial=virial)
+            f.evaluate(topo, d["pos"], F, E)
+            res.append((F, E.table.copy(), f.last_pair_count()))
+        f.close()
+    for F, T, p in res[1:]:
+        assert np.array_equal(F, res[0][0])
+        assert np.array_equal(T, res[0][1])
+        assert p == res[0][2]
+
+
 @pytest.mark.parametrize("precision", ["mixed", "fp64"])
 def test_unwrapped_and_translated_positions(water648, precision):
     L = water648["box"]
