@@ -176,14 +176,16 @@ class NonbondedCutoffB200SystemForce:
             self._ctx = self._create(topo)
             if getattr(self, "_pair_kernel", _lib.PMB200_KERNEL_SEARCH):
                 self._check(L.pmb200_set_pair_kernel(self._ctx, self._pair_kernel))
-        key = (id(topo), topo.version)
-        if self._topo_key != key:
+        # the cached topology is held by reference with its version: an id()
+        # alone can be handed to a new topology once the old one is freed
+        key = self._topo_key
+        if key is None or key[0] is not topo or key[1] != topo.version:
             ex = topo.excl.reshape(-1)
             self._check(L.pmb200_set_topology(
                 self._ctx, topo.n, _ptr(topo.type), _ptr(topo.qscaled), _ptr(topo.mol),
                 _ptr(topo.mass), topo.ntypes, _ptr(topo.lj), topo.excl.shape[0],
                 _ptr(ex) if ex.size else None, topo.coulomb_scaling))
-            self._topo_key = key
+            self._topo_key = (topo, topo.version)
             self._box_key = None
         dom = None if topo.domain is None else tuple(
             np.ascontiguousarray(x, dtype=np.float64) for x in topo.domain)

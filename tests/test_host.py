@@ -263,3 +263,35 @@ def test_pair_form_ids_round_trip():
                   "-cutoff 8")  # C2 wants -switchon first
     with pytest.raises(ValueError):
         P(("C3", 1, 2), None)
+
+
+def test_topology_cache_follows_the_object_not_its_id(monkeypatch):
+    """A force sends the topology again whenever it is handed another
+    topology object -- also one that Python places at the address of a freed
+    one, where an id()-keyed cache would keep the old atoms -- and not again
+    for the same unchanged object (the C-ABI calls recorded by a fake)."""
+    calls = []
+
+    class FakeLib:
+        def __getattr__(self, name):
+            def call(*args):
+                calls.append(name)
+                return _lib.PMB200_OK
+            return call
+
+    monkeypatch.setattr(_lib, "lib", lambda: FakeLib())
+    f = NonbondedCutoffB200SystemForce(7.0, 8.0, 8.0, 8.0, precision="mixed")
+    f._ctx = ctypes.c_void_p(1)  # (no context is created: the fake serves every call)
+    try:
+        boxes = [water.water_box(k, rc=8.0, ron=7.0, seed=k) for k in (3, 4)]
+        for s in boxes + boxes:
+            topo = PeriodicTopology.from_dict(s)
+            f._ensure(topo)
+            del topo
+        assert calls.count("pmb200_set_topology") == 4
+        topo = PeriodicTopology.from_dict(boxes[0])
+        f._ensure(topo)
+        f._ensure(topo)
+        assert calls.count("pmb200_set_topology") == 5
+    finally:
+        f._ctx = None
