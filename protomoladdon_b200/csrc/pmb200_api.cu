@@ -720,13 +720,15 @@ __global__ void k_copy_word(const int *__restrict__ src, int *__restrict__ dst) 
 // 32-bit box fractions was measured too: the host's encoding pass cost what
 // the shorter copy saved.)
 __global__ void k_pack_out(size_t n3, const double *__restrict__ frc,
-                           const double *__restrict__ res, float *__restrict__ out) {
+                           const double *__restrict__ res, const int *__restrict__ err,
+                           float *__restrict__ out) {
   const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k < n3) out[k] = (float)frc[k];
-  // the result words (and the error flag behind them) after the forces, at
-  // a double boundary
+  // the 20 result words and the device error flag behind them, after the
+  // forces at a double boundary
   double *tail = reinterpret_cast<double *>(out + ((n3 + 1) & ~(size_t)1));
-  if (k < (size_t)kPinOut) tail[k] = res[k];
+  if (k < 20) tail[k] = res[k];
+  else if (k == 20) *reinterpret_cast<int *>(tail + 20) = *err;
 }
 
 // The supercluster kernel's grid, stencil, constants and buffers for the
@@ -2202,15 +2204,17 @@ int pmb200_eval(pmb200_ctx *c, const double *pos, double *forces, double *energi
       if (e != cudaSuccess) return fail(c, PMB200_ECUDA, "copy in: %s", cudaGetErrorString(e));
       int r = launch_eval(c, c->d_hpos, c->d_hfrc, d_hout, flags, 0, st);
       if (r) return r;
-      k_copy_word<<<1, 1, 0, st>>>(c->d_err, reinterpret_cast<int *>(d_hout + 20));
-      e = cudaGetLastError();
-      if (e == cudaSuccess && f32out) {
-        k_pack_out<<<eb, 256, 0, st>>>(cnt, c->d_hfrc, d_hout, c->d_hf32);
+      if (f32out) {
+        // (the error flag goes into the packed copy's tail)
+        k_pack_out<<<eb, 256, 0, st>>>(cnt, c->d_hfrc, d_hout, c->d_err, c->d_hf32);
         e = cudaGetLastError();
         if (e == cudaSuccess)
           e = cudaMemcpyAsync(c->h_pin_frc, c->d_hf32, res32_bytes, cudaMemcpyDeviceToHost, st);
-      } else if (e == cudaSuccess) {
-        e = cudaMemcpyAsync(c->h_pin_frc, c->d_hfrc, res_bytes, cudaMemcpyDeviceToHost, st);
+      } else {
+        k_copy_word<<<1, 1, 0, st>>>(c->d_err, reinterpret_cast<int *>(d_hout + 20));
+        e = cudaGetLastError();
+        if (e == cudaSuccess)
+          e = cudaMemcpyAsync(c->h_pin_frc, c->d_hfrc, res_bytes, cudaMemcpyDeviceToHost, st);
       }
       if (e != cudaSuccess) return fail(c, PMB200_ECUDA, "copy out: %s", cudaGetErrorString(e));
       return PMB200_OK;
