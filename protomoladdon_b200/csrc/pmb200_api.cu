@@ -937,8 +937,13 @@ int launch_eval_clusters(pmb200_ctx *c, const double *d_pos, double *d_forces, d
   return PMB200_OK;
 }
 
+// f32 / tail (host-buffer calls of mixed contexts, or null): where the
+// evaluation may put its forces in FP32 and the results with the error flag
+// (k_finalize_reduce); *packed tells whether it did.
 int launch_eval(pmb200_ctx *c, const double *d_pos, double *d_forces, double *d_out,
-                unsigned flags, int accumulate, cudaStream_t st) {
+                unsigned flags, int accumulate, cudaStream_t st, float *f32 = nullptr,
+                double *tail = nullptr, bool *packed = nullptr) {
+  if (packed) *packed = false;
   const int n = c->n;
   const bool mixed = c->p.precision == PMB200_MIXED;
   const bool energy = (flags & PMB200_ENERGY) != 0;
@@ -989,8 +994,10 @@ int launch_eval(pmb200_ctx *c, const double *d_pos, double *d_forces, double *d_
                pdl, n, (const unsigned long long *)c->d_facc, (const int *)c->d_sidx,
                fscale * kFixInv, accumulate, d_forces, g.ncell * ctx_slots(c, true),
                (const double *)c->d_partial, c->d_red, c->d_redctr, 1.0,
-               d_out ? d_out : c->d_out, c->d_pairs, ns);
+               d_out ? d_out : c->d_out, c->d_pairs, ns, f32, f32 ? tail : nullptr,
+               (const int *)c->d_err);
       CK(cudaGetLastError());
+      if (packed) *packed = f32 != nullptr;
       return PMB200_OK;
     }
     if (n > 0)
@@ -2202,9 +2209,16 @@ int pmb200_eval(pmb200_ctx *c, const double *pos, double *forces, double *energi
       const unsigned eb = (unsigned)((cnt + 255) / 256);
       cudaError_t e = cudaMemcpyAsync(c->d_hpos, src, bytes, cudaMemcpyHostToDevice, st);
       if (e != cudaSuccess) return fail(c, PMB200_ECUDA, "copy in: %s", cudaGetErrorString(e));
-      int r = launch_eval(c, c->d_hpos, c->d_hfrc, d_hout, flags, 0, st);
+      // (a mixed energy evaluation packs the FP32 forces, results and error
+      // flag itself)
+      double *tail = reinterpret_cast<double *>(c->d_hf32 + f32_slots);
+      bool packed = false;
+      int r = launch_eval(c, c->d_hpos, c->d_hfrc, d_hout, flags, 0, st,
+                          f32out ? c->d_hf32 : nullptr, tail, &packed);
       if (r) return r;
-      if (f32out) {
+      if (packed) {
+        e = cudaMemcpyAsync(c->h_pin_frc, c->d_hf32, res32_bytes, cudaMemcpyDeviceToHost, st);
+      } else if (f32out) {
         // (the error flag goes into the packed copy's tail)
         k_pack_out<<<eb, 256, 0, st>>>(cnt, c->d_hfrc, d_hout, c->d_err, c->d_hf32);
         e = cudaGetLastError();

@@ -2432,12 +2432,17 @@ __global__ void k_reduce2(int nred, const double *__restrict__ red, double visit
 // same sums in the same order, so the results equal those of the three
 // kernels bit for bit, without two launches and their gaps.  Launch:
 // max(ceil(n / 256), kRedBlocks) blocks of 256 threads.
+// f32 (host-buffer calls of mixed contexts, or null): the forces are written
+// there in FP32 (the FP64 values rounded once) instead of to `forces`, and
+// the 20 result words and the device error flag `err` to `tail` after them,
+// for one copy back to the host.
 __global__ void __launch_bounds__(256)
 k_finalize_reduce(int n, const unsigned long long *__restrict__ facc,
                   const int *__restrict__ sidx, double scale, int accumulate,
                   double *__restrict__ forces, int nrows, const double *__restrict__ partial,
                   double *red, unsigned *__restrict__ arrivals, double visit,
-                  double *__restrict__ out, double *__restrict__ pairs_out, int ns) {
+                  double *__restrict__ out, double *__restrict__ pairs_out, int ns,
+                  float *__restrict__ f32, double *__restrict__ tail, const int *err) {
   pdl_wait();
   __shared__ double sh[8][ACC_MV];
   __shared__ double col[ACC_MV];
@@ -2445,11 +2450,17 @@ k_finalize_reduce(int n, const unsigned long long *__restrict__ facc,
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j < n) {
     const int o = sidx[j];
-    double *fo = forces + 3 * (size_t)o;
+    if (f32) {
 #pragma unroll
-    for (int q = 0; q < 3; q++) {
-      const double v = (double)(long long)facc[(size_t)q * n + j] * scale;
-      fo[q] = accumulate ? fo[q] + v : v;
+      for (int q = 0; q < 3; q++)
+        f32[3 * (size_t)o + q] = (float)((double)(long long)facc[(size_t)q * n + j] * scale);
+    } else {
+      double *fo = forces + 3 * (size_t)o;
+#pragma unroll
+      for (int q = 0; q < 3; q++) {
+        const double v = (double)(long long)facc[(size_t)q * n + j] * scale;
+        fo[q] = accumulate ? fo[q] + v : v;
+      }
     }
   }
   if (blockIdx.x >= kRedBlocks) return;  // uniform per block
@@ -2462,6 +2473,10 @@ k_finalize_reduce(int n, const unsigned long long *__restrict__ facc,
   if (s_arrived != kRedBlocks - 1) return;  // uniform per block
   __threadfence();
   reduce2_block(kRedBlocks, red, visit, out, pairs_out, ns, col);
+  if (tail && threadIdx.x == 0) {  // (out was written by this thread)
+    for (int k = 0; k < 20; k++) tail[k] = out[k];
+    *reinterpret_cast<int *>(tail + 20) = *(const volatile int *)err;
+  }
 }
 
 // Leapfrog kick + drift (LeapfrogIntegrator::doKickdoDrift without modifiers,
