@@ -64,8 +64,8 @@ sys.path.insert(0, ROOT)
 DT_FS = 1.0
 FLOPS_PER_PAIR = 81          # algorithmic flops per unique in-cutoff pair
 BYTES_PER_ATOM = 84          # algorithmic HBM bytes per atom per evaluation
-KERNELS_PER_STEP = 9         # kick_drift_settle, cell_index, scan, scatter, rank_gather,
-                             # pair, finalize, reduce1, reduce2
+KERNELS_PER_STEP = 7         # kick_drift_settle, cell_index, scan, scatter, rank_gather,
+                             # pair, finalize_reduce (forces and energy sums)
 KERNELS_PER_STEP_CLUSTERS = 13  # kick_drift_settle, sc_index, scan, scatter, rank_gather,
                              # sc_columns, sc_build, sc_list, sc_tasks, sc_pair,
                              # sc_finalize, sc_reduce1, reduce2
